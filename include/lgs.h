@@ -1,0 +1,115 @@
+/* LigeSIS / Basefold prover for B200 (sm_100a) — the C ABI of liblgs.so.
+ *
+ * Each entry point stands in for a function of the reference Rust crate paulguoyanpei/ligesis
+ * (paths are inside that project).  Plain pointers and sizes only: BF (Goldilocks) values are
+ * uint64_t (reduced mod p = 2^64 - 2^32 + 1 on input), EF (BinomialExtensionField<BF,2>) values
+ * are two consecutive uint64_t (c0, c1).  Nothing throws across this boundary: every call
+ * returns an lgs_status, and lgs_last_error() describes the last failure on the calling thread.
+ * A context owns one CUDA stream on one device; use one context per host thread.
+ */
+#ifndef LGS_H
+#define LGS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  LGS_OK = 0,
+  LGS_ERR_BAD_SHAPE = 1,        /* setup's shared-domain precondition, or an unsupported size */
+  LGS_ERR_OOM = 2,              /* device allocation failed */
+  LGS_ERR_ORACLE_EXHAUSTED = 3, /* the randomness oracle has too few fields/ints left */
+  LGS_ERR_DEVICE_TIMEOUT = 4,   /* a bounded device wait gave up */
+  LGS_ERR_BAD_ARG = 5,          /* null pointer, wrong length, mismatched key/commitment */
+  LGS_ERR_CUDA = 6,             /* any other CUDA error */
+  LGS_ERR_INTERNAL = 7,
+  LGS_ERR_BUFFER_TOO_SMALL = 8  /* *len holds the size needed */
+} lgs_status;
+
+typedef struct lgs_ctx lgs_ctx;
+typedef struct lgs_pk lgs_pk;                   /* ProvingKey (pcs/src/ligesis.rs:67-74) */
+typedef struct lgs_commit_data lgs_commit_data; /* CommitData (pcs/src/ligesis.rs:88-97) */
+
+const char* lgs_last_error(void);
+const char* lgs_version(void);
+
+/* Context: device, stream, twiddle table, scratch arena.  `flags` is reserved (pass 0). */
+lgs_status lgs_ctx_create(int device, unsigned flags, lgs_ctx** out);
+void lgs_ctx_destroy(lgs_ctx* ctx);
+/* The cudaStream_t every call of this context enqueues on (for event timing). */
+lgs_status lgs_ctx_stream(lgs_ctx* ctx, void** stream);
+
+/* Ligesis::setup (pcs/src/ligesis.rs:239-273).  A: the 32 x (64 * 2^log_m) subset-sum matrix,
+ * row-major (SubsetSumHash::new, pcs/src/subset_sum.rs:31-39, sampled by the caller).
+ * com_a receives the Basefold commitment to the flattened A. */
+lgs_status lgs_setup(lgs_ctx* ctx, unsigned log_m, unsigned log_n, const uint64_t* A,
+                     lgs_pk** pk, uint8_t com_a[32]);
+void lgs_pk_free(lgs_pk* pk);
+
+/* Ligesis::commit (pcs/src/ligesis.rs:277-325).  f: 2^(log_m+log_n) BF evaluations in host
+ * memory (MlPoly<BF>, utils/src/poly.rs:4).  root receives the LigesisCommit. */
+lgs_status lgs_commit(lgs_ctx* ctx, const lgs_pk* pk, const uint64_t* f, size_t len,
+                      uint8_t root[32], lgs_commit_data** out);
+/* Same, with f already in device memory of the context's device. */
+lgs_status lgs_commit_device(lgs_ctx* ctx, const lgs_pk* pk, const uint64_t* f_dev, size_t len,
+                             uint8_t root[32], lgs_commit_data** out);
+void lgs_commit_data_free(lgs_commit_data* cd);
+/* Copy a commitment intermediate to host memory: which = 0 the RS codeword F' (m x 2n),
+ * 1 the digest H (32 x 2n).  count must equal the element count. */
+lgs_status lgs_commit_read(lgs_ctx* ctx, const lgs_commit_data* cd, int which, uint64_t* out,
+                           size_t count);
+
+/* Oracle draws one prove/verify consumes (RandomOracle cursors, utils/src/oracle.rs:94-116). */
+lgs_status lgs_oracle_need(unsigned log_m, unsigned log_n, size_t* fields, size_t* ints);
+
+/* Ligesis::prove (pcs/src/ligesis.rs:347-549).  z: log_m + log_n EF (z2 = the low log_n).
+ * fields/ints: the RandomOracle arrays (EF and u64); cursors[0..2] = (fields, ints) positions,
+ * advanced on success.  *proof points at the encoded LigesisProof (layout in proof.hpp),
+ * owned by the context and valid until its next lgs_prove. */
+lgs_status lgs_prove(lgs_ctx* ctx, const lgs_pk* pk, const lgs_commit_data* cd,
+                     const uint64_t* z, size_t zlen, const uint64_t* fields, size_t nfields,
+                     const uint64_t* ints, size_t nints, uint64_t cursors[2],
+                     const uint8_t** proof, size_t* proof_len);
+
+/* Ligesis::verify (pcs/src/ligesis.rs:569-756), on the host.  *accept = 1 or 0. */
+lgs_status lgs_verify(unsigned log_m, unsigned log_n, const uint8_t com_a[32],
+                      const uint8_t root[32], const uint64_t* z, size_t zlen,
+                      const uint8_t* proof, size_t proof_len, const uint64_t* fields,
+                      size_t nfields, const uint64_t* ints, size_t nints, uint64_t cursors[2],
+                      int* accept);
+
+/* ---- the individual device operations of the path (host buffers in and out) ---- */
+
+/* Radix2Dit::dft of `batch` vectors (p3-dft 0.5.3; pcs/src/ligesis.rs:231-235): in holds
+ * batch x n_in BF, each zero-padded to 2^log_size; out holds batch x 2^log_size. */
+lgs_status lgs_dft(lgs_ctx* ctx, const uint64_t* in, size_t n_in, size_t batch,
+                   unsigned log_size, uint64_t* out);
+/* SubsetSumHash::hash_columns (pcs/src/subset_sum.rs:58-67) on bit columns given as the RS
+ * codeword: cw is m x cols BF; column j's bits are bit b of cw[i][j] at row 64 i + b.
+ * A is 32 x 64m; H receives 32 x cols. */
+lgs_status lgs_subset_sum_hash(lgs_ctx* ctx, const uint64_t* A, size_t m, const uint64_t* cw,
+                               size_t cols, uint64_t* H);
+/* MerkleTreeProver::new + commit (utils/src/merkle.rs:49-85): leaves are nleaves x words
+ * u64 serialized little-endian; nleaves a power of two, words * 8 <= 1024. */
+lgs_status lgs_merkle_root(lgs_ctx* ctx, const uint64_t* leaves, size_t nleaves, unsigned words,
+                           uint8_t root[32]);
+/* sumcheck::prove (utils/src/sumcheck.rs:37-84): d factors (1..3) of 2^k EF each,
+ * factor-major; challenges: k EF (the oracle fields it draws, in order).  rounds_out receives
+ * k x (d+1) EF, finals_out d EF. */
+lgs_status lgs_sumcheck_prove(lgs_ctx* ctx, const uint64_t* polys, unsigned d, unsigned k,
+                              const uint64_t* challenges, uint64_t* rounds_out,
+                              uint64_t* finals_out);
+/* MlPoly::eval (utils/src/poly.rs:7-18): 2^k EF at a k-EF point. */
+lgs_status lgs_mle_eval(lgs_ctx* ctx, const uint64_t* evals, unsigned k, const uint64_t* point,
+                        uint64_t out[2]);
+/* MlPoly::new_eq (utils/src/poly.rs:44-53): 2^k EF. */
+lgs_status lgs_new_eq(lgs_ctx* ctx, const uint64_t* point, unsigned k, uint64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LGS_H */

@@ -1,0 +1,35 @@
+"""LigeSIS / Basefold prover for NVIDIA B200 (sm_100a).
+
+The compute path is liblgs.so (hand-written CUDA, C ABI in include/lgs.h); this package is the
+Python host mirror of the reference's API for the path (paulguoyanpei/ligesis:
+pcs/src/ligesis.rs, pcs/src/subset_sum.rs, utils/src/poly.rs, utils/src/oracle.rs).
+"""
+from ._lib import Context, LgsError, OracleExhausted, ShapeError, load
+from .ligesis import (
+    CODE_RATE,
+    C_ROWS,
+    ETA,
+    NUM_COLS_OPENED,
+    CommitData,
+    Ligesis,
+    LigesisCommit,
+    LigesisProof,
+    MlPoly,
+    ProvingKey,
+    RandomOracle,
+    SubsetSumHash,
+    VerifyingKey,
+    dft,
+    merkle_root,
+    oracle_need,
+    shape_ok,
+    sumcheck_prove,
+)
+from .rng import SeededRng
+
+__all__ = [
+    "CODE_RATE", "C_ROWS", "ETA", "NUM_COLS_OPENED", "CommitData", "Context", "LgsError",
+    "Ligesis", "LigesisCommit", "LigesisProof", "MlPoly", "OracleExhausted", "ProvingKey",
+    "RandomOracle", "SeededRng", "ShapeError", "SubsetSumHash", "VerifyingKey", "dft", "load",
+    "merkle_root", "oracle_need", "shape_ok", "sumcheck_prove",
+]

@@ -1,0 +1,153 @@
+"""ctypes binding of liblgs.so (include/lgs.h).  The library is the only compute path: if it is
+missing or cannot be loaded, every call raises; there is no CPU fallback."""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "liblgs.so"
+
+STATUS = {
+    0: "ok",
+    1: "bad shape",
+    2: "out of memory",
+    3: "oracle exhausted",
+    4: "device timeout",
+    5: "bad argument",
+    6: "cuda error",
+    7: "internal error",
+    8: "buffer too small",
+}
+
+
+class LgsError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class ShapeError(LgsError):
+    pass
+
+
+class OracleExhausted(LgsError):
+    pass
+
+
+_lib = None
+_lock = threading.Lock()
+
+u64p = C.POINTER(C.c_uint64)
+u8p = C.POINTER(C.c_uint8)
+vp = C.c_void_p
+
+_SIGS = {
+    "lgs_last_error": (C.c_char_p, []),
+    "lgs_version": (C.c_char_p, []),
+    "lgs_ctx_create": (C.c_int, [C.c_int, C.c_uint, C.POINTER(vp)]),
+    "lgs_ctx_destroy": (None, [vp]),
+    "lgs_ctx_stream": (C.c_int, [vp, C.POINTER(vp)]),
+    "lgs_setup": (C.c_int, [vp, C.c_uint, C.c_uint, u64p, C.POINTER(vp), u8p]),
+    "lgs_pk_free": (None, [vp]),
+    "lgs_commit": (C.c_int, [vp, vp, u64p, C.c_size_t, u8p, C.POINTER(vp)]),
+    "lgs_commit_device": (C.c_int, [vp, vp, vp, C.c_size_t, u8p, C.POINTER(vp)]),
+    "lgs_commit_data_free": (None, [vp]),
+    "lgs_commit_read": (C.c_int, [vp, vp, C.c_int, u64p, C.c_size_t]),
+    "lgs_oracle_need": (C.c_int, [C.c_uint, C.c_uint, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "lgs_prove": (C.c_int, [vp, vp, vp, u64p, C.c_size_t, u64p, C.c_size_t, u64p, C.c_size_t,
+                            u64p, C.POINTER(u8p), C.POINTER(C.c_size_t)]),
+    "lgs_verify": (C.c_int, [C.c_uint, C.c_uint, u8p, u8p, u64p, C.c_size_t, u8p, C.c_size_t,
+                             u64p, C.c_size_t, u64p, C.c_size_t, u64p, C.POINTER(C.c_int)]),
+    "lgs_dft": (C.c_int, [vp, u64p, C.c_size_t, C.c_size_t, C.c_uint, u64p]),
+    "lgs_subset_sum_hash": (C.c_int, [vp, u64p, C.c_size_t, u64p, C.c_size_t, u64p]),
+    "lgs_merkle_root": (C.c_int, [vp, u64p, C.c_size_t, C.c_uint, u8p]),
+    "lgs_sumcheck_prove": (C.c_int, [vp, u64p, C.c_uint, C.c_uint, u64p, u64p, u64p]),
+    "lgs_mle_eval": (C.c_int, [vp, u64p, C.c_uint, u64p, u64p]),
+    "lgs_new_eq": (C.c_int, [vp, u64p, C.c_uint, u64p]),
+}
+
+
+def load(path: Path | None = None):
+    """Load liblgs.so (building it first if the CUDA toolkit is here and it is absent)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        p = Path(path) if path else LIB_PATH
+        if not p.exists():
+            from . import build as _build
+
+            _build.build()
+        lib = C.CDLL(str(p))
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def check(status: int) -> None:
+    if status == 0:
+        return
+    msg = (load().lgs_last_error() or b"").decode(errors="replace")
+    if status == 1:
+        raise ShapeError(status, msg)
+    if status == 3:
+        raise OracleExhausted(status, msg)
+    raise LgsError(status, msg)
+
+
+def ptr64(a: np.ndarray):
+    assert a.dtype == np.uint64 and a.flags["C_CONTIGUOUS"], "expected a contiguous uint64 array"
+    return a.ctypes.data_as(u64p)
+
+
+def ptr8(a: np.ndarray):
+    assert a.dtype == np.uint8 and a.flags["C_CONTIGUOUS"], "expected a contiguous uint8 array"
+    return a.ctypes.data_as(u8p)
+
+
+def u64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint64))
+
+
+class Context:
+    """One device, one CUDA stream (lgs_ctx).  Not shared between host threads."""
+
+    _default: dict[int, "Context"] = {}
+
+    def __init__(self, device: int = 0):
+        lib = load()
+        h = vp()
+        check(lib.lgs_ctx_create(int(device), 0, C.byref(h)))
+        self.handle = h
+        self.device = device
+        self._lib = lib
+
+    @classmethod
+    def default(cls, device: int = 0) -> "Context":
+        ctx = cls._default.get(device)
+        if ctx is None:
+            ctx = cls._default[device] = cls(device)
+        return ctx
+
+    @property
+    def stream_ptr(self) -> int:
+        s = vp()
+        check(self._lib.lgs_ctx_stream(self.handle, C.byref(s)))
+        return int(s.value or 0)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.lgs_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

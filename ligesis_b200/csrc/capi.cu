@@ -1,0 +1,353 @@
+// The extern "C" boundary of liblgs.so (declared in include/lgs.h).  Every entry point catches
+// all C++ exceptions and maps them to an lgs_status; the message is kept per host thread.
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/lgs.h"
+#include "prover.cuh"
+
+namespace lgs {
+void ctx_init(lgs_ctx* c, int device);
+void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lgs_pk* pk);
+void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device, lgs_commit_data* cd);
+void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u64* z_host,
+               size_t zlen, const u64* fields_host, size_t nfields, const uint64_t* ints_host,
+               size_t nints, uint64_t cursors[2], std::vector<uint8_t>* proof_out);
+int verify_host(unsigned log_m, unsigned log_n, const Hash32& com_a, const Hash32& root,
+                const u64* z_in, size_t zlen, const uint8_t* proof, size_t proof_len,
+                const u64* fields, size_t nfields, const uint64_t* ints, size_t nints,
+                uint64_t cursors[2]);
+}  // namespace lgs
+
+using namespace lgs;
+
+namespace {
+thread_local std::string g_err;
+
+lgs_status fail(lgs_status s, const std::string& m) {
+  g_err = m;
+  return s;
+}
+
+template <class F>
+lgs_status guarded(F&& f) {
+  try {
+    f();
+    return LGS_OK;
+  } catch (const ShapeError& e) {
+    return fail(LGS_ERR_BAD_SHAPE, e.what());
+  } catch (const OracleError& e) {
+    return fail(LGS_ERR_ORACLE_EXHAUSTED, e.what());
+  } catch (const CudaError& e) {
+    std::string m = e.what();
+    if (m.find("out of memory") != std::string::npos) return fail(LGS_ERR_OOM, m);
+    return fail(LGS_ERR_CUDA, m);
+  } catch (const std::bad_alloc&) {
+    return fail(LGS_ERR_OOM, "host allocation failed");
+  } catch (const std::invalid_argument& e) {
+    return fail(LGS_ERR_BAD_ARG, e.what());
+  } catch (const std::exception& e) {
+    return fail(LGS_ERR_INTERNAL, e.what());
+  } catch (...) {
+    return fail(LGS_ERR_INTERNAL, "unknown exception");
+  }
+}
+
+void need(bool c, const char* what) {
+  if (!c) throw std::invalid_argument(what);
+}
+
+struct CtxDevice {  // make the context's device current for the duration of a call
+  int prev = -1;
+  explicit CtxDevice(const lgs_ctx* c) {
+    cudaGetDevice(&prev);
+    if (prev != c->device) LGS_CUDA(cudaSetDevice(c->device));
+  }
+  ~CtxDevice() {
+    int cur;
+    if (cudaGetDevice(&cur) == cudaSuccess && prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+}  // namespace
+
+extern "C" {
+
+const char* lgs_last_error(void) { return g_err.c_str(); }
+const char* lgs_version(void) { return "ligesis-b200 0.1 (sm_100a)"; }
+
+lgs_status lgs_ctx_create(int device, unsigned flags, lgs_ctx** out) {
+  (void)flags;
+  return guarded([&] {
+    need(out != nullptr, "lgs_ctx_create: out is null");
+    int ndev = 0;
+    LGS_CUDA(cudaGetDeviceCount(&ndev));
+    need(device >= 0 && device < ndev, "lgs_ctx_create: no such device");
+    auto* c = new lgs_ctx;
+    try {
+      ctx_init(c, device);
+    } catch (...) {
+      delete c;
+      throw;
+    }
+    *out = c;
+  });
+}
+
+void lgs_ctx_destroy(lgs_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->st) {
+    cudaStreamSynchronize(ctx->st);
+    cudaStreamDestroy(ctx->st);
+  }
+  delete ctx;
+}
+
+lgs_status lgs_ctx_stream(lgs_ctx* ctx, void** stream) {
+  return guarded([&] {
+    need(ctx && stream, "lgs_ctx_stream: null argument");
+    *stream = (void*)ctx->st;
+  });
+}
+
+lgs_status lgs_setup(lgs_ctx* ctx, unsigned log_m, unsigned log_n, const uint64_t* A,
+                     lgs_pk** pk, uint8_t com_a[32]) {
+  return guarded([&] {
+    need(ctx && A && pk && com_a, "lgs_setup: null argument");
+    need(log_m <= 13 && log_n <= 21, "lgs_setup: shape too large");
+    CtxDevice dg(ctx);
+    auto* k = new lgs_pk;
+    try {
+      setup_dev(ctx, log_m, log_n, A, k);
+    } catch (...) {
+      delete k;
+      throw;
+    }
+    std::memcpy(com_a, k->com_a.b, 32);
+    *pk = k;
+  });
+}
+void lgs_pk_free(lgs_pk* pk) { delete pk; }
+
+static lgs_status commit_impl(lgs_ctx* ctx, const lgs_pk* pk, const uint64_t* f, size_t len,
+                              uint8_t root[32], lgs_commit_data** out, bool dev) {
+  return guarded([&] {
+    need(ctx && pk && f && root && out, "lgs_commit: null argument");
+    need(len == pk->shape.m() * pk->shape.n(), "lgs_commit: f must hold 2^(log_m+log_n) values");
+    CtxDevice dg(ctx);
+    auto* cd = new lgs_commit_data;
+    try {
+      commit_dev(ctx, pk, f, dev, cd);
+    } catch (...) {
+      delete cd;
+      throw;
+    }
+    std::memcpy(root, cd->root.b, 32);
+    *out = cd;
+  });
+}
+lgs_status lgs_commit(lgs_ctx* ctx, const lgs_pk* pk, const uint64_t* f, size_t len,
+                      uint8_t root[32], lgs_commit_data** out) {
+  return commit_impl(ctx, pk, f, len, root, out, false);
+}
+lgs_status lgs_commit_device(lgs_ctx* ctx, const lgs_pk* pk, const uint64_t* f_dev, size_t len,
+                             uint8_t root[32], lgs_commit_data** out) {
+  return commit_impl(ctx, pk, f_dev, len, root, out, true);
+}
+void lgs_commit_data_free(lgs_commit_data* cd) { delete cd; }
+
+lgs_status lgs_commit_read(lgs_ctx* ctx, const lgs_commit_data* cd, int which, uint64_t* out,
+                           size_t count) {
+  return guarded([&] {
+    need(ctx && cd && out, "lgs_commit_read: null argument");
+    const DevMem& src = which == 0 ? cd->cw : cd->H;
+    need(which == 0 || which == 1, "lgs_commit_read: which must be 0 or 1");
+    need(count * 8 == src.bytes, "lgs_commit_read: wrong element count");
+    CtxDevice dg(ctx);
+    LGS_CUDA(cudaMemcpyAsync(out, src.p, src.bytes, cudaMemcpyDeviceToHost, ctx->st));
+    LGS_CUDA(cudaStreamSynchronize(ctx->st));
+  });
+}
+
+lgs_status lgs_oracle_need(unsigned log_m, unsigned log_n, size_t* fields, size_t* ints) {
+  return guarded([&] {
+    need(fields && ints, "lgs_oracle_need: null argument");
+    Shape s{log_m, log_n};
+    if (!s.eval_ok()) throw ShapeError("shape outside the shared-domain window");
+    *fields = FieldPlan(s).total;
+    *ints = INTS_PER_PROOF;
+  });
+}
+
+lgs_status lgs_prove(lgs_ctx* ctx, const lgs_pk* pk, const lgs_commit_data* cd,
+                     const uint64_t* z, size_t zlen, const uint64_t* fields, size_t nfields,
+                     const uint64_t* ints, size_t nints, uint64_t cursors[2],
+                     const uint8_t** proof, size_t* proof_len) {
+  return guarded([&] {
+    need(ctx && pk && cd && z && fields && ints && cursors && proof && proof_len,
+         "lgs_prove: null argument");
+    CtxDevice dg(ctx);
+    uint64_t cur[2] = {cursors[0], cursors[1]};
+    std::vector<uint8_t>& buf = ctx->proof_buf;
+    std::vector<uint8_t> out;
+    prove_dev(ctx, pk, cd, z, zlen, fields, nfields, ints, nints, cur, &out);
+    buf.swap(out);
+    *proof = buf.data();
+    *proof_len = buf.size();
+    cursors[0] = cur[0];
+    cursors[1] = cur[1];
+  });
+}
+
+lgs_status lgs_verify(unsigned log_m, unsigned log_n, const uint8_t com_a[32],
+                      const uint8_t root[32], const uint64_t* z, size_t zlen,
+                      const uint8_t* proof, size_t proof_len, const uint64_t* fields,
+                      size_t nfields, const uint64_t* ints, size_t nints, uint64_t cursors[2],
+                      int* accept) {
+  return guarded([&] {
+    need(com_a && root && z && proof && fields && ints && cursors && accept,
+         "lgs_verify: null argument");
+    Hash32 ca, rt;
+    std::memcpy(ca.b, com_a, 32);
+    std::memcpy(rt.b, root, 32);
+    *accept = verify_host(log_m, log_n, ca, rt, z, zlen, proof, proof_len, fields, nfields, ints,
+                          nints, cursors);
+  });
+}
+
+// ---- individual operations ----------------------------------------------------------------
+
+lgs_status lgs_dft(lgs_ctx* ctx, const uint64_t* in, size_t n_in, size_t batch,
+                   unsigned log_size, uint64_t* out) {
+  return guarded([&] {
+    need(ctx && in && out, "lgs_dft: null argument");
+    need(log_size >= 1 && log_size <= TW_LOG, "lgs_dft: size out of range");
+    const size_t N = (size_t)1 << log_size;
+    need(n_in >= 1 && n_in <= N && batch >= 1, "lgs_dft: bad lengths");
+    CtxDevice dg(ctx);
+    ctx->arena.begin();
+    u64* d_in = ctx->arena.get<u64>(batch * n_in);
+    u64* d_out = ctx->arena.get<u64>(batch * N);
+    u64* scr = log_size > 12 ? ctx->arena.get<u64>(batch * N) : nullptr;
+    std::vector<u64> canon(in, in + batch * n_in);
+    for (auto& x : canon) x = gl_canon(x);
+    LGS_CUDA(cudaMemcpyAsync(d_in, canon.data(), canon.size() * 8, cudaMemcpyHostToDevice, ctx->st));
+    ntt_batch(d_in, n_in, n_in, d_out, N, log_size, batch, scr, ctx->tw.as<u64>(), ctx->st);
+    LGS_CUDA(cudaMemcpyAsync(out, d_out, batch * N * 8, cudaMemcpyDeviceToHost, ctx->st));
+    LGS_CUDA(cudaStreamSynchronize(ctx->st));
+  });
+}
+
+lgs_status lgs_subset_sum_hash(lgs_ctx* ctx, const uint64_t* A, size_t m, const uint64_t* cw,
+                               size_t cols, uint64_t* H) {
+  return guarded([&] {
+    need(ctx && A && cw && H, "lgs_subset_sum_hash: null argument");
+    need(m >= 1 && cols >= 1 && cols % 128 == 0, "lgs_subset_sum_hash: cols must be a multiple of 128");
+    CtxDevice dg(ctx);
+    const size_t W = 64 * m;
+    ctx->arena.begin();
+    u64* dA = ctx->arena.get<u64>(DIGEST_ROWS * W);
+    uint8_t* dL = ctx->arena.get<uint8_t>(DIGEST_ROWS * W * 8);
+    u64* dC = ctx->arena.get<u64>(m * cols);
+    u64* dH = ctx->arena.get<u64>(DIGEST_ROWS * cols);
+    std::vector<u64> a(A, A + DIGEST_ROWS * W), c(cw, cw + m * cols);
+    for (auto& x : a) x = gl_canon(x);
+    for (auto& x : c) x = gl_canon(x);
+    LGS_CUDA(cudaMemcpyAsync(dA, a.data(), a.size() * 8, cudaMemcpyHostToDevice, ctx->st));
+    LGS_CUDA(cudaMemcpyAsync(dC, c.data(), c.size() * 8, cudaMemcpyHostToDevice, ctx->st));
+    alimb_from_a(dA, dL, W, ctx->st);
+    subset_sum_hash(dL, dC, dH, (unsigned)m, cols, ctx->st);
+    LGS_CUDA(cudaMemcpyAsync(H, dH, DIGEST_ROWS * cols * 8, cudaMemcpyDeviceToHost, ctx->st));
+    LGS_CUDA(cudaStreamSynchronize(ctx->st));
+  });
+}
+
+lgs_status lgs_merkle_root(lgs_ctx* ctx, const uint64_t* leaves, size_t nleaves, unsigned words,
+                           uint8_t root[32]) {
+  return guarded([&] {
+    need(ctx && leaves && root, "lgs_merkle_root: null argument");
+    need(nleaves >= 1 && (nleaves & (nleaves - 1)) == 0, "lgs_merkle_root: nleaves must be a power of two");
+    need(words >= 1 && words * 8 <= 1024, "lgs_merkle_root: leaf must be 8..1024 bytes");
+    CtxDevice dg(ctx);
+    ctx->arena.begin();
+    u64* d = ctx->arena.get<u64>(nleaves * words);
+    u32* nodes = ctx->arena.get<u32>((2 * nleaves - 1) * 8);
+    LGS_CUDA(cudaMemcpyAsync(d, leaves, nleaves * words * 8, cudaMemcpyHostToDevice, ctx->st));
+    merkle_leaves_contig(d, words, nleaves, nodes, ctx->st);
+    merkle_build_from_leaves(nodes, nleaves, ctx->st);
+    LGS_CUDA(cudaMemcpyAsync(root, nodes + (2 * nleaves - 2) * 8, 32, cudaMemcpyDeviceToHost, ctx->st));
+    LGS_CUDA(cudaStreamSynchronize(ctx->st));
+  });
+}
+
+lgs_status lgs_sumcheck_prove(lgs_ctx* ctx, const uint64_t* polys, unsigned d, unsigned k,
+                              const uint64_t* challenges, uint64_t* rounds_out,
+                              uint64_t* finals_out) {
+  return guarded([&] {
+    need(ctx && polys && challenges && rounds_out && finals_out, "lgs_sumcheck_prove: null argument");
+    need(d >= 1 && d <= 3 && k >= 1 && k <= 30, "lgs_sumcheck_prove: 1..3 factors, 1..30 variables");
+    CtxDevice dg(ctx);
+    const size_t len = (size_t)1 << k;
+    ctx->arena.begin();
+    ef2* p[3];
+    for (unsigned j = 0; j < d; ++j) p[j] = ctx->arena.get<ef2>(len);
+    ef2* ch = ctx->arena.get<ef2>(k);
+    ef2* ro = ctx->arena.get<ef2>((size_t)k * (d + 1));
+    ef2* fo = ctx->arena.get<ef2>(d);
+    ef2* part = ctx->arena.get<ef2>(sumcheck_partials_elems(k, d));
+    std::vector<u64> hp(polys, polys + 2 * len * d), hc(challenges, challenges + 2 * k);
+    for (auto& x : hp) x = gl_canon(x);
+    for (auto& x : hc) x = gl_canon(x);
+    for (unsigned j = 0; j < d; ++j)
+      LGS_CUDA(cudaMemcpyAsync(p[j], hp.data() + 2 * len * j, len * 16, cudaMemcpyHostToDevice, ctx->st));
+    LGS_CUDA(cudaMemcpyAsync(ch, hc.data(), k * 16, cudaMemcpyHostToDevice, ctx->st));
+    sumcheck_prove_dev(p, d, k, ch, ro, fo, part, ctx->st);
+    LGS_CUDA(cudaMemcpyAsync(rounds_out, ro, (size_t)k * (d + 1) * 16, cudaMemcpyDeviceToHost, ctx->st));
+    LGS_CUDA(cudaMemcpyAsync(finals_out, fo, d * 16, cudaMemcpyDeviceToHost, ctx->st));
+    LGS_CUDA(cudaStreamSynchronize(ctx->st));
+  });
+}
+
+lgs_status lgs_mle_eval(lgs_ctx* ctx, const uint64_t* evals, unsigned k, const uint64_t* point,
+                        uint64_t out[2]) {
+  return guarded([&] {
+    need(ctx && evals && point && out, "lgs_mle_eval: null argument");
+    need(k >= 1 && k <= 30, "lgs_mle_eval: 1..30 variables");
+    CtxDevice dg(ctx);
+    const size_t len = (size_t)1 << k;
+    ctx->arena.begin();
+    ef2* v = ctx->arena.get<ef2>(len);
+    ef2* pt = ctx->arena.get<ef2>(k);
+    ef2* o = ctx->arena.get<ef2>(1);
+    ef2* part = ctx->arena.get<ef2>(eqdot_partials_elems(k));
+    std::vector<u64> hv(evals, evals + 2 * len), hp(point, point + 2 * k);
+    for (auto& x : hv) x = gl_canon(x);
+    for (auto& x : hp) x = gl_canon(x);
+    LGS_CUDA(cudaMemcpyAsync(v, hv.data(), len * 16, cudaMemcpyHostToDevice, ctx->st));
+    LGS_CUDA(cudaMemcpyAsync(pt, hp.data(), k * 16, cudaMemcpyHostToDevice, ctx->st));
+    eq_dot_dev(v, 0, pt, k, o, part, ctx->st);
+    LGS_CUDA(cudaMemcpyAsync(out, o, 16, cudaMemcpyDeviceToHost, ctx->st));
+    LGS_CUDA(cudaStreamSynchronize(ctx->st));
+  });
+}
+
+lgs_status lgs_new_eq(lgs_ctx* ctx, const uint64_t* point, unsigned k, uint64_t* out) {
+  return guarded([&] {
+    need(ctx && point && out, "lgs_new_eq: null argument");
+    need(k >= 1 && k <= 30, "lgs_new_eq: 1..30 variables");
+    CtxDevice dg(ctx);
+    const size_t len = (size_t)1 << k;
+    ctx->arena.begin();
+    ef2* pt = ctx->arena.get<ef2>(k);
+    ef2* o = ctx->arena.get<ef2>(len);
+    std::vector<u64> hp(point, point + 2 * k);
+    for (auto& x : hp) x = gl_canon(x);
+    LGS_CUDA(cudaMemcpyAsync(pt, hp.data(), k * 16, cudaMemcpyHostToDevice, ctx->st));
+    new_eq_dev(pt, k, o, ctx->st);
+    LGS_CUDA(cudaMemcpyAsync(out, o, len * 16, cudaMemcpyDeviceToHost, ctx->st));
+    LGS_CUDA(cudaStreamSynchronize(ctx->st));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,461 @@
+// Eval-path kernels of the LigeSIS prover (pcs/src/ligesis.rs:347-567) and of the Basefold
+// shared-domain batched open (pcs/src/basefold.rs:201-218, 648-856): eq tables, eq-weighted
+// dot products (MLE evaluations), the a-bar GEMV, the bit-column gather B_I, the sumcheck
+// inputs g1/g2/v/sel, RS-link weights, and the batched-FRI channel rounds and codeword folds.
+#include "kernels.cuh"
+
+namespace lgs {
+
+namespace {
+constexpr unsigned EQ_TILE_LOG = 10;  // eq tables are built per 1024-entry tile
+
+__device__ __forceinline__ ef2 shfl_xor_ef(ef2 v, int m) {
+  ef2 r;
+  r.c0 = __shfl_xor_sync(0xffffffffu, v.c0, m);
+  r.c1 = __shfl_xor_sync(0xffffffffu, v.c1, m);
+  return r;
+}
+// CTA-wide sum of one EF value; valid in every thread afterwards.  red: >= 32 entries.
+__device__ ef2 block_sum(ef2 v, ef2* red) {
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int m = 16; m; m >>= 1) v = ef_add(v, shfl_xor_ef(v, m));
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  ef2 t = lane < nw ? red[lane] : ef_zero();
+#pragma unroll
+  for (int m = 16; m; m >>= 1) t = ef_add(t, shfl_xor_ef(t, m));
+  return t;
+}
+
+// tab[j] = prod_{t < b} (bit t of j ? p[t] : 1 - p[t]) for j < 2^b, built by doubling.
+__device__ void eq_table_smem(const ef2* p, unsigned b, ef2* tab) {
+  if (threadIdx.x == 0) tab[0] = ef_one();
+  __syncthreads();
+  for (unsigned t = 0; t < b; ++t) {
+    const unsigned h = 1u << t;
+    const ef2 pt = p[t], qt = ef_sub(ef_one(), pt);
+    for (unsigned j = threadIdx.x; j < h; j += blockDim.x) {
+      ef2 x = tab[j];
+      tab[j + h] = ef_mul(x, pt);
+      tab[j] = ef_mul(x, qt);
+    }
+    __syncthreads();
+  }
+}
+// prod_{t in [b, k)} (bit t of idx ? p[t] : 1 - p[t])
+__device__ ef2 eq_high(const ef2* p, unsigned b, unsigned k, size_t idx) {
+  ef2 acc = ef_one();
+  for (unsigned t = b; t < k; ++t)
+    acc = ef_mul(acc, ((idx >> t) & 1) ? p[t] : ef_sub(ef_one(), p[t]));
+  return acc;
+}
+}  // namespace
+
+// ---- gather ------------------------------------------------------------------------------
+__global__ void gather_segments_kernel(const GatherSeg* __restrict__ segs) {
+  const GatherSeg s = segs[blockIdx.x];
+  const size_t total = s.count * s.words;
+  for (size_t t = threadIdx.x; t < total; t += blockDim.x) {
+    size_t i = t / s.words, w = t % s.words;
+    s.dst[t] = s.src[s.idx[i] * s.words + w];
+  }
+}
+void gather_segments(const GatherSeg* segs_dev, unsigned nseg, cudaStream_t st) {
+  if (!nseg) return;
+  gather_segments_kernel<<<nseg, 256, 0, st>>>(segs_dev);
+  LGS_LAUNCH_CHECK();
+}
+
+// ---- eq tables ----------------------------------------------------------------------------
+// MlPoly::new_eq (utils/src/poly.rs:44-53): point[0] is the lowest index bit.
+__global__ void new_eq_kernel(const ef2* __restrict__ point, unsigned k, ef2* __restrict__ out) {
+  __shared__ ef2 p[64];
+  __shared__ ef2 tab[1 << EQ_TILE_LOG];
+  __shared__ ef2 hi;
+  if (threadIdx.x < k) p[threadIdx.x] = point[threadIdx.x];
+  __syncthreads();
+  const unsigned b = k < EQ_TILE_LOG ? k : EQ_TILE_LOG;
+  const size_t base = (size_t)blockIdx.x << b;
+  if (threadIdx.x == 0) hi = eq_high(p, b, k, base);
+  eq_table_smem(p, b, tab);
+  for (unsigned j = threadIdx.x; j < (1u << b); j += blockDim.x) out[base + j] = ef_mul(hi, tab[j]);
+}
+void new_eq_dev(const ef2* point, unsigned k, ef2* out, cudaStream_t st) {
+  if (k > 40) throw ShapeError("new_eq: too many variables");
+  unsigned b = k < EQ_TILE_LOG ? k : EQ_TILE_LOG;
+  new_eq_kernel<<<(unsigned)((size_t)1 << (k - b)), 256, 0, st>>>(point, k, out);
+  LGS_LAUNCH_CHECK();
+}
+
+// combine_eq (pcs/src/ligesis.rs:159-171): out = sum_j gamma^j eq_{points[j]}.
+__global__ void combine_eq_kernel(const ef2* __restrict__ points, unsigned npts, unsigned k,
+                                  const ef2* __restrict__ gamma, ef2* __restrict__ out) {
+  __shared__ ef2 p[4 * 64];
+  __shared__ ef2 tab[1 << EQ_TILE_LOG];
+  __shared__ ef2 coef;
+  constexpr unsigned PER = (1u << EQ_TILE_LOG) / 256;  // entries per thread (blockDim 256)
+  for (unsigned i = threadIdx.x; i < npts * k; i += blockDim.x) p[i] = points[i];
+  __syncthreads();
+  const unsigned b = k < EQ_TILE_LOG ? k : EQ_TILE_LOG;
+  const size_t base = (size_t)blockIdx.x << b;
+  ef2 acc[PER];
+#pragma unroll
+  for (unsigned q = 0; q < PER; ++q) acc[q] = ef_zero();
+  ef2 g = ef_one();
+  for (unsigned j = 0; j < npts; ++j) {
+    if (threadIdx.x == 0) coef = ef_mul(g, eq_high(p + j * k, b, k, base));
+    eq_table_smem(p + j * k, b, tab);  // ends with a barrier, so coef is visible
+#pragma unroll
+    for (unsigned q = 0; q < PER; ++q) {
+      unsigned i = threadIdx.x + q * 256;
+      if (i < (1u << b)) acc[q] = ef_add(acc[q], ef_mul(coef, tab[i]));
+    }
+    __syncthreads();
+    g = ef_mul(g, *gamma);
+  }
+#pragma unroll
+  for (unsigned q = 0; q < PER; ++q) {
+    unsigned i = threadIdx.x + q * 256;
+    if (i < (1u << b)) out[base + i] = acc[q];
+  }
+}
+void combine_eq_dev(const ef2* points, unsigned npts, unsigned k, const ef2* gamma, ef2* out,
+                    cudaStream_t st) {
+  if (npts > 4 || k > 64) throw ShapeError("combine_eq: at most 4 points of 64 variables");
+  unsigned b = k < EQ_TILE_LOG ? k : EQ_TILE_LOG;
+  combine_eq_kernel<<<(unsigned)((size_t)1 << (k - b)), 256, 0, st>>>(points, npts, k, gamma, out);
+  LGS_LAUNCH_CHECK();
+}
+
+// ---- eq-weighted dot: MlPoly(vec).eval(point) = sum_i vec[i] eq_point(i) -------------------
+template <bool BF>
+__global__ void eq_dot_kernel(const void* __restrict__ vec, const ef2* __restrict__ point,
+                              unsigned k, ef2* __restrict__ partials) {
+  __shared__ ef2 p[64];
+  __shared__ ef2 tab[1 << EQ_TILE_LOG];
+  __shared__ ef2 red[32];
+  if (threadIdx.x < k) p[threadIdx.x] = point[threadIdx.x];
+  __syncthreads();
+  const unsigned b = k < EQ_TILE_LOG ? k : EQ_TILE_LOG;
+  const size_t base = (size_t)blockIdx.x << b;
+  eq_table_smem(p, b, tab);
+  ef2 acc = ef_zero();
+  for (unsigned j = threadIdx.x; j < (1u << b); j += blockDim.x) {
+    if (BF) {
+      u64 x = ((const u64*)vec)[base + j];
+      acc = ef_add(acc, ef_scale(tab[j], x));
+    } else {
+      acc = ef_add(acc, ef_mul(((const ef2*)vec)[base + j], tab[j]));
+    }
+  }
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) partials[blockIdx.x] = ef_mul(acc, eq_high(p, b, k, base));
+}
+__global__ void sum_partials_kernel(const ef2* __restrict__ partials, size_t n, ef2* out) {
+  __shared__ ef2 red[32];
+  ef2 acc = ef_zero();
+  for (size_t i = threadIdx.x; i < n; i += blockDim.x) acc = ef_add(acc, partials[i]);
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) *out = acc;
+}
+size_t eqdot_partials_elems(unsigned k) {
+  return k > EQ_TILE_LOG ? ((size_t)1 << (k - EQ_TILE_LOG)) : 1;
+}
+void eq_dot_dev(const void* vec, int is_bf, const ef2* point, unsigned k, ef2* out,
+                ef2* partials, cudaStream_t st) {
+  if (k > 40) throw ShapeError("eq_dot: too many variables");
+  unsigned b = k < EQ_TILE_LOG ? k : EQ_TILE_LOG;
+  unsigned grid = (unsigned)((size_t)1 << (k - b));
+  if (is_bf)
+    eq_dot_kernel<true><<<grid, 256, 0, st>>>(vec, point, k, partials);
+  else
+    eq_dot_kernel<false><<<grid, 256, 0, st>>>(vec, point, k, partials);
+  LGS_LAUNCH_CHECK();
+  sum_partials_kernel<<<1, 256, 0, st>>>(partials, grid, out);
+  LGS_LAUNCH_CHECK();
+}
+
+// ---- a-bar = eq_{z1}^T F (pcs/src/ligesis.rs:372-379) --------------------------------------
+__global__ void gemv_eq_rows_kernel(const u64* __restrict__ f, const ef2* __restrict__ eq,
+                                    size_t m, size_t n, ef2* __restrict__ out) {
+  size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  ef2 acc = ef_zero();
+  for (size_t i = 0; i < m; ++i) acc = ef_add(acc, ef_scale(eq[i], __ldg(f + i * n + j)));
+  out[j] = acc;
+}
+void gemv_eq_rows(const u64* f, const ef2* eq, size_t m, size_t n, ef2* out, cudaStream_t st) {
+  gemv_eq_rows_kernel<<<cdiv(n, 256), 256, 0, st>>>(f, eq, m, n, out);
+  LGS_LAUNCH_CHECK();
+}
+
+__global__ void lift_bf_kernel(const u64* __restrict__ in, ef2* __restrict__ out, size_t n,
+                               u64 minus) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = ef_make(gl_sub(in[i], minus), 0);
+}
+void lift_bf(const u64* in, ef2* out, size_t n, u64 minus, cudaStream_t st) {
+  lift_bf_kernel<<<cdiv(n, 256), 256, 0, st>>>(in, out, n, minus);
+  LGS_LAUNCH_CHECK();
+}
+
+// ---- B_I: bi[i*s + k] = bit (i % 64) of F'[i / 64][idx[k]] (pcs/src/ligesis.rs:403-410) -----
+__global__ void bits_gather_kernel(const u64* __restrict__ cw, size_t two_n,
+                                   const uint64_t* __restrict__ idx, unsigned s, size_t rows,
+                                   u64* __restrict__ bi) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= rows * s) return;
+  size_t q = t / s;
+  unsigned k = (unsigned)(t % s);
+  u64 word = cw[q * two_n + idx[k]];
+  for (unsigned b = 0; b < 64; ++b) bi[(q * 64 + b) * s + k] = (word >> b) & 1;
+}
+void bits_gather(const u64* cw, size_t two_n, const uint64_t* idx, unsigned s, size_t W,
+                 u64* bi, cudaStream_t st) {
+  size_t rows = W / 64;
+  bits_gather_kernel<<<cdiv(rows * s, 128), 128, 0, st>>>(cw, two_n, idx, s, rows, bi);
+  LGS_LAUNCH_CHECK();
+}
+
+// g1 = eq_{alpha2}^T A (pcs/src/ligesis.rs:436-444)
+__global__ void g1_kernel(const u64* __restrict__ A, size_t W, const ef2* __restrict__ eq,
+                          unsigned C, ef2* __restrict__ g1) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= W) return;
+  ef2 acc = ef_zero();
+  for (unsigned r = 0; r < C; ++r) acc = ef_add(acc, ef_scale(eq[r], A[(size_t)r * W + i]));
+  g1[i] = acc;
+}
+void g1_build(const u64* A, size_t W, const ef2* eq_a2, unsigned C, ef2* g1, cudaStream_t st) {
+  g1_kernel<<<cdiv(W, 256), 256, 0, st>>>(A, W, eq_a2, C, g1);
+  LGS_LAUNCH_CHECK();
+}
+// g2[i] = sum_k eq_{r2}[k] B[i][idx[k]] (pcs/src/ligesis.rs:445-455); one warp per i.
+__global__ void g2_kernel(const u64* __restrict__ bi, size_t W, unsigned s,
+                          const ef2* __restrict__ eq, ef2* __restrict__ g2) {
+  size_t i = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  unsigned lane = threadIdx.x & 31;
+  if (i >= W) return;
+  ef2 acc = ef_zero();
+  for (unsigned k = lane; k < s; k += 32)
+    if (bi[i * s + k]) acc = ef_add(acc, eq[k]);
+#pragma unroll
+  for (int m = 16; m; m >>= 1) acc = ef_add(acc, shfl_xor_ef(acc, m));
+  if (lane == 0) g2[i] = acc;
+}
+void g2_build(const u64* bi, size_t W, unsigned s, const ef2* eq_r2, ef2* g2, cudaStream_t st) {
+  g2_kernel<<<cdiv(W * 32, 256), 256, 0, st>>>(bi, W, s, eq_r2, g2);
+  LGS_LAUNCH_CHECK();
+}
+// v[i] = eq_{z1}[i / 64] * 2^(i % 64) (pcs/src/ligesis.rs:474-476)
+__global__ void v_kernel(const ef2* __restrict__ eqz1, size_t W, ef2* __restrict__ v) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= W) return;
+  ef2 e = eqz1[i / 64];
+  unsigned sh = (unsigned)(i % 64);
+  v[i] = ef_make(gl_shl(e.c0, sh), gl_shl(e.c1, sh));
+}
+void v_build(const ef2* eqz1, size_t W, ef2* v, cudaStream_t st) {
+  v_kernel<<<cdiv(W, 256), 256, 0, st>>>(eqz1, W, v);
+  LGS_LAUNCH_CHECK();
+}
+// y4 = sum_k eq_{r2}[k] RS(a)[idx[k]] (pcs/src/ligesis.rs:458)
+__global__ void y4_kernel(const ef2* __restrict__ eq, const ef2* __restrict__ ra,
+                          const uint64_t* __restrict__ idx, unsigned s, ef2* out) {
+  __shared__ ef2 red[32];
+  ef2 acc = ef_zero();
+  for (unsigned k = threadIdx.x; k < s; k += blockDim.x) acc = ef_add(acc, ef_mul(eq[k], ra[idx[k]]));
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) *out = acc;
+}
+void y4_dev(const ef2* eq_r2, const ef2* ra, const uint64_t* idx, unsigned s, ef2* out,
+            cudaStream_t st) {
+  y4_kernel<<<1, 128, 0, st>>>(eq_r2, ra, idx, s, out);
+  LGS_LAUNCH_CHECK();
+}
+__global__ void sel_scatter_kernel(const uint64_t* __restrict__ idx, const ef2* __restrict__ eq,
+                                   unsigned s, ef2* __restrict__ sel) {
+  unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < s) sel[idx[k]] = eq[k];
+}
+void sel_build(const uint64_t* idx, const ef2* eq_r2, unsigned s, size_t two_n, ef2* sel,
+               cudaStream_t st) {
+  LGS_CUDA(cudaMemsetAsync(sel, 0, two_n * sizeof(ef2), st));
+  sel_scatter_kernel<<<cdiv(s, 128), 128, 0, st>>>(idx, eq_r2, s, sel);
+  LGS_LAUNCH_CHECK();
+}
+// w[k] = prod_t (1 - r3[t] + r3[t] g^((2^t k) mod 2n)) (pcs/src/ligesis.rs:553-567)
+__global__ void rs_weights_kernel(const ef2* __restrict__ r3, unsigned log2n, size_t n,
+                                  const u64* __restrict__ tw, ef2* __restrict__ w) {
+  __shared__ ef2 r[64];
+  if (threadIdx.x < log2n) r[threadIdx.x] = r3[threadIdx.x];
+  __syncthreads();
+  size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const size_t mask = ((size_t)2 << (log2n - 1)) - 1;
+  const unsigned shift = TW_LOG - log2n;
+  ef2 prod = ef_one();
+  for (unsigned t = 0; t < log2n; ++t) {
+    size_t e = (k << t) & mask;
+    u64 gp = __ldg(tw + (e << shift));
+    ef2 term = ef_add(ef_sub(ef_one(), r[t]), ef_scale(r[t], gp));
+    prod = ef_mul(prod, term);
+  }
+  w[k] = prod;
+}
+void rs_weights_dev(const ef2* r3, unsigned log2n, size_t n, const u64* tw, ef2* w,
+                    cudaStream_t st) {
+  if (log2n > TW_LOG || log2n > 64) throw ShapeError("rs_weights: domain too large");
+  rs_weights_kernel<<<cdiv(n, 256), 256, 0, st>>>(r3, log2n, n, tw, w);
+  LGS_LAUNCH_CHECK();
+}
+
+// ---- Basefold batched open ------------------------------------------------------------------
+// Level-0 combined codeword (pcs/src/basefold.rs:660-666, 735-741):
+// combined[i] = sum_ch coeffs[ch] sum_j eq4_ch[j] codes_ch[i][j].
+__global__ void bf_combine_kernel(const BfChannelDev* __restrict__ chs, unsigned nch,
+                                  const ef2* __restrict__ coeffs, size_t D,
+                                  ef2* __restrict__ combined) {
+  __shared__ ef2 wts[4][64];
+  __shared__ ef2 pts[4][8];
+  for (unsigned c = 0; c < nch; ++c) {
+    if (threadIdx.x < chs[c].li) pts[c][threadIdx.x] = chs[c].point[threadIdx.x];
+  }
+  __syncthreads();
+  for (unsigned c = 0; c < nch; ++c) {
+    eq_table_smem(pts[c], chs[c].li, wts[c]);
+    for (unsigned j = threadIdx.x; j < (1u << chs[c].li); j += blockDim.x)
+      wts[c][j] = ef_mul(wts[c][j], coeffs[c]);
+    __syncthreads();
+  }
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D) return;
+  ef2 acc = ef_zero();
+  for (unsigned c = 0; c < nch; ++c) {
+    const unsigned L = 1u << chs[c].li;
+    if (chs[c].is_ef) {
+      const ef2* row = (const ef2*)chs[c].codes + i * L;
+      for (unsigned j = 0; j < L; ++j) acc = ef_add(acc, ef_mul(wts[c][j], row[j]));
+    } else {
+      const u64* row = chs[c].codes + i * L;
+      for (unsigned j = 0; j < L; ++j) acc = ef_add(acc, ef_scale(wts[c][j], row[j]));
+    }
+  }
+  combined[i] = acc;
+}
+void bf_combine_dev(const BfChannelDev* chs_dev, unsigned nch, const ef2* coeffs, size_t D,
+                    ef2* combined, cudaStream_t st) {
+  if (nch > 4) throw ShapeError("basefold: at most 4 channels per launch");
+  bf_combine_kernel<<<cdiv(D, 256), 256, 0, st>>>(chs_dev, nch, coeffs, D, combined);
+  LGS_LAUNCH_CHECK();
+}
+
+// m = poly.fold(point[0..li]) (pcs/src/basefold.rs:667-668): m[t] = sum_j eq4[j] poly[t 2^li + j].
+__global__ void bf_fold_poly_kernel(const u64* __restrict__ poly, int is_ef, unsigned li,
+                                    const ef2* __restrict__ point, size_t out_len,
+                                    ef2* __restrict__ m) {
+  __shared__ ef2 pts[8];
+  __shared__ ef2 wts[64];
+  if (threadIdx.x < li) pts[threadIdx.x] = point[threadIdx.x];
+  __syncthreads();
+  eq_table_smem(pts, li, wts);
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= out_len) return;
+  const unsigned L = 1u << li;
+  ef2 acc = ef_zero();
+  if (is_ef) {
+    const ef2* row = (const ef2*)poly + t * L;
+    for (unsigned j = 0; j < L; ++j) acc = ef_add(acc, ef_mul(wts[j], row[j]));
+  } else {
+    const u64* row = poly + t * L;
+    for (unsigned j = 0; j < L; ++j) acc = ef_add(acc, ef_scale(wts[j], row[j]));
+  }
+  m[t] = acc;
+}
+void bf_fold_poly_dev(const u64* poly, int is_ef, unsigned li, const ef2* point, size_t out_len,
+                      ef2* m, cudaStream_t st) {
+  if (li > 6) throw ShapeError("basefold: log_interleave above 6");
+  bf_fold_poly_kernel<<<cdiv(out_len, 256), 256, 0, st>>>(poly, is_ef, li, point, out_len, m);
+  LGS_LAUNCH_CHECK();
+}
+
+// CTA c < nch: the R evaluation-reduction rounds of channel c (pcs/src/basefold.rs:746-769):
+//   l0 = MLE(m[even])(zp[t+1..]), l1 = MLE(m[odd])(zp[t+1..]); msg = l0; m <- fold(m, r_t).
+// CTA nch: the R codeword folds (eq_fold_codeword, pcs/src/basefold.rs:201-218) on `levels`
+// (level k of length D >> k stored at offset D * (2 - 2^(1-k))).
+struct BfRoundsArgs {
+  ef2* m[4];
+  ef2* tmp[4];
+  const ef2* zp[4];
+};
+__global__ void __launch_bounds__(1024)
+    bf_rounds_kernel(BfRoundsArgs a, unsigned nch, unsigned R, const ef2* __restrict__ ch,
+                     ef2* __restrict__ msgs, ef2* __restrict__ levels, size_t D,
+                     const u64* __restrict__ tw) {
+  extern __shared__ ef2 sm[];  // lo table (64) + hi table (2^(R-7))
+  __shared__ ef2 red[32];
+  __shared__ ef2 zp[64];
+  const unsigned c = blockIdx.x;
+  if (c == nch) {
+    const u64 inv2 = 0x7FFFFFFF80000001ULL;  // (p + 1) / 2
+    size_t off = 0, len = D;
+    for (unsigned t = 0; t < R; ++t) {
+      const ef2 r = ch[t];
+      const size_t h = len >> 1;
+      const unsigned lg = 63 - __clzll((long long)len);
+      for (size_t i = threadIdx.x; i < h; i += blockDim.x) {
+        ef2 x = levels[off + i], nx = levels[off + i + h];
+        u64 ginv = i ? __ldg(tw + ((len - i) << (TW_LOG - lg))) : 1;
+        ef2 pe = ef_scale(ef_add(x, nx), inv2);
+        ef2 po = ef_scale(ef_scale(ef_sub(x, nx), ginv), inv2);
+        levels[off + len + i] = ef_add(ef_mul(ef_sub(ef_one(), r), pe), ef_mul(r, po));
+      }
+      __syncthreads();
+      off += len;
+      len = h;
+    }
+    return;
+  }
+  if (threadIdx.x < R) zp[threadIdx.x] = a.zp[c][threadIdx.x];
+  __syncthreads();
+  ef2* m = a.m[c];
+  ef2* tmp = a.tmp[c];
+  ef2* lo_tab = sm;
+  ef2* hi_tab = sm + 64;
+  for (unsigned t = 0; t < R; ++t) {
+    const unsigned nrest = R - t - 1;  // variables of the rest point
+    const size_t half = (size_t)1 << nrest;
+    const unsigned blo = nrest < 6 ? nrest : 6, bhi = nrest - blo;
+    eq_table_smem(zp + t + 1, blo, lo_tab);
+    eq_table_smem(zp + t + 1 + blo, bhi, hi_tab);
+    ef2 l0 = ef_zero(), l1 = ef_zero();
+    for (size_t i = threadIdx.x; i < half; i += blockDim.x) {
+      ef2 e = ef_mul(lo_tab[i & ((1u << blo) - 1)], hi_tab[i >> blo]);
+      l0 = ef_add(l0, ef_mul(m[2 * i], e));
+      l1 = ef_add(l1, ef_mul(m[2 * i + 1], e));
+    }
+    l0 = block_sum(l0, red);
+    if (threadIdx.x == 0) msgs[(size_t)c * R + t] = l0;
+    (void)l1;
+    const ef2 r = ch[t];
+    for (size_t i = threadIdx.x; i < half; i += blockDim.x) tmp[i] = ef_lerp(m[2 * i], m[2 * i + 1], r);
+    __syncthreads();
+    ef2* sw = m;
+    m = tmp;
+    tmp = sw;
+  }
+}
+void bf_rounds_dev(ef2* const* ms, ef2* const* tmps, const ef2* const* zps, unsigned nch,
+                   unsigned R, const ef2* ch, ef2* msgs_out, ef2* levels, size_t D,
+                   const u64* tw, void*, cudaStream_t st) {
+  if (nch > 4 || R > 17 || R < 1) throw ShapeError("basefold: unsupported round count");
+  BfRoundsArgs a;
+  for (unsigned c = 0; c < nch; ++c) a.m[c] = ms[c], a.tmp[c] = tmps[c], a.zp[c] = zps[c];
+  size_t smem = (64 + ((size_t)1 << (R > 7 ? R - 7 : 0))) * sizeof(ef2);
+  bf_rounds_kernel<<<nch + 1, 1024, smem, st>>>(a, nch, R, ch, msgs_out, levels, D, tw);
+  LGS_LAUNCH_CHECK();
+}
+
+}  // namespace lgs

@@ -1,0 +1,107 @@
+// Goldilocks field p = 2^64 - 2^32 + 1 and its quadratic extension F_p[x]/(x^2 - 7), for host
+// and device.  These are the `BF` / `EF = BinomialExtensionField<BF, 2>` of the reference prover
+// (pcs/src/ligesis.rs:205-210, :787).  Values are always kept canonical (< p); an EF element is
+// (c0, c1) = c0 + c1 x and is stored as two consecutive u64 (c0 first), which is also its
+// serialized byte order (utils/src/merkle.rs:24-35).
+#pragma once
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define GL_HD __host__ __device__ __forceinline__
+#else
+#define GL_HD inline
+#endif
+
+namespace lgs {
+
+typedef uint64_t u64;
+typedef uint32_t u32;
+
+constexpr u64 GL_P = 0xFFFFFFFF00000001ULL;
+constexpr u64 GL_EPS = 0xFFFFFFFFULL;  // 2^64 mod p
+constexpr u64 GL_W = 7;                // extension non-residue
+// Generator of the order-2^32 subgroup (p3-goldilocks' published value); the order-2^k
+// generator is its 2^(32-k)-th power.
+constexpr u64 GL_G32 = 1753635133440165772ULL;
+
+GL_HD u64 gl_mulhi(u64 a, u64 b) {
+#ifdef __CUDA_ARCH__
+  return __umul64hi(a, b);
+#else
+  return (u64)(((unsigned __int128)a * b) >> 64);
+#endif
+}
+
+// (hi * 2^64 + lo) mod p with 2^64 = 2^32 - 1 and 2^96 = -1.
+GL_HD u64 gl_reduce(u64 lo, u64 hi) {
+  u64 hh = hi >> 32, hl = hi & GL_EPS;
+  u64 t0 = lo - hh;
+  if (lo < hh) t0 -= GL_EPS;
+  u64 t1 = (hl << 32) - hl;
+  u64 t2 = t0 + t1;
+  if (t2 < t1) t2 += GL_EPS;
+  return t2 >= GL_P ? t2 - GL_P : t2;
+}
+GL_HD u64 gl_add(u64 a, u64 b) {
+  u64 s = a + b;
+  if (s < a) s += GL_EPS;
+  return s >= GL_P ? s - GL_P : s;
+}
+GL_HD u64 gl_sub(u64 a, u64 b) { return a >= b ? a - b : a + (GL_P - b); }
+GL_HD u64 gl_neg(u64 a) { return a ? GL_P - a : 0; }
+GL_HD u64 gl_mul(u64 a, u64 b) { return gl_reduce(a * b, gl_mulhi(a, b)); }
+GL_HD u64 gl_canon(u64 a) { return a >= GL_P ? a - GL_P : a; }
+GL_HD u64 gl_pow(u64 a, u64 e) {
+  u64 r = 1;
+  while (e) {
+    if (e & 1) r = gl_mul(r, a);
+    a = gl_mul(a, a);
+    e >>= 1;
+  }
+  return r;
+}
+GL_HD u64 gl_inv(u64 a) { return gl_pow(a, GL_P - 2); }
+GL_HD u64 gl_two_adic_generator(unsigned bits) {
+  u64 g = GL_G32;
+  for (unsigned i = bits; i < 32; ++i) g = gl_mul(g, g);
+  return g;
+}
+// x * 2^s mod p for 0 <= s < 64.
+GL_HD u64 gl_shl(u64 x, unsigned s) {
+  if (s == 0) return x;
+  return gl_reduce(x << s, x >> (64 - s));
+}
+
+struct ef2 {
+  u64 c0, c1;
+};
+GL_HD ef2 ef_make(u64 a, u64 b) {
+  ef2 r;
+  r.c0 = a;
+  r.c1 = b;
+  return r;
+}
+GL_HD ef2 ef_zero() { return ef_make(0, 0); }
+GL_HD ef2 ef_one() { return ef_make(1, 0); }
+GL_HD ef2 ef_from(u64 a) { return ef_make(a, 0); }
+GL_HD bool ef_eq(ef2 a, ef2 b) { return a.c0 == b.c0 && a.c1 == b.c1; }
+GL_HD ef2 ef_add(ef2 a, ef2 b) { return ef_make(gl_add(a.c0, b.c0), gl_add(a.c1, b.c1)); }
+GL_HD ef2 ef_sub(ef2 a, ef2 b) { return ef_make(gl_sub(a.c0, b.c0), gl_sub(a.c1, b.c1)); }
+GL_HD ef2 ef_scale(ef2 a, u64 s) { return ef_make(gl_mul(a.c0, s), gl_mul(a.c1, s)); }
+// 7 * x: x*8 - x through the 128-bit path (x < p, so x*8 < 2^67).
+GL_HD u64 gl_mul7(u64 x) { return gl_sub(gl_reduce(x << 3, x >> 61), x); }
+GL_HD ef2 ef_mul(ef2 a, ef2 b) {
+  // Karatsuba: c0 = a0 b0 + 7 a1 b1, c1 = (a0 + a1)(b0 + b1) - a0 b0 - a1 b1
+  u64 p0 = gl_mul(a.c0, b.c0), p1 = gl_mul(a.c1, b.c1);
+  u64 pm = gl_mul(gl_add(a.c0, a.c1), gl_add(b.c0, b.c1));
+  return ef_make(gl_add(p0, gl_mul7(p1)), gl_sub(gl_sub(pm, p0), p1));
+}
+// (1 - r) a + r b = a + r (b - a)
+GL_HD ef2 ef_lerp(ef2 a, ef2 b, ef2 r) { return ef_add(a, ef_mul(r, ef_sub(b, a))); }
+GL_HD ef2 ef_inv(ef2 a) {
+  u64 norm = gl_sub(gl_mul(a.c0, a.c0), gl_mul7(gl_mul(a.c1, a.c1)));
+  u64 ni = gl_inv(norm);
+  return ef_make(gl_mul(a.c0, ni), gl_mul(gl_neg(a.c1), ni));
+}
+
+}  // namespace lgs

@@ -1,0 +1,86 @@
+// Host-side launchers for every device kernel of the prover library.  All of them enqueue on
+// the given stream and never synchronize.
+#pragma once
+#include <algorithm>
+#include <cstddef>
+#include <vector>
+
+#include "common.cuh"
+
+namespace lgs {
+
+constexpr unsigned SC_MAX_BLOCKS = 296;  // 2 CTAs per SM on a 148-SM B200
+
+// ntt.cu
+void build_twiddles(u64* d_tw, cudaStream_t st);
+void ntt_batch(const u64* in, size_t in_stride, size_t n_in, u64* out, size_t out_stride,
+               unsigned logN, size_t batch, u64* scratch, const u64* tw, cudaStream_t st);
+void transpose_u64(const u64* in, u64* out, size_t rows, size_t cols, size_t batch,
+                   cudaStream_t st);
+
+// hash_mma.cu
+void alimb_from_a(const u64* A, uint8_t* alimb, size_t W, cudaStream_t st);
+void subset_sum_hash(const uint8_t* alimb, const u64* cw, u64* H, unsigned m, size_t two_n,
+                     cudaStream_t st);
+
+// merkle.cu
+size_t merkle_node_count(size_t nleaves);
+size_t merkle_layer_offset(size_t nleaves, unsigned layer);
+void merkle_build_from_leaves(u32* nodes, size_t nleaves, cudaStream_t st);
+void merkle_leaves_cols(const u64* H, unsigned rows, size_t ncols, u32* nodes, cudaStream_t st);
+void merkle_leaves_contig(const u64* data, unsigned words, size_t nleaves, u32* nodes,
+                          cudaStream_t st);
+void gather_u64(const u64* src, const uint64_t* idx, size_t count, unsigned words, u64* dst,
+                cudaStream_t st);
+
+// sumcheck.cu
+size_t sumcheck_partials_elems(unsigned k, unsigned d);
+void sumcheck_prove_dev(ef2* const* polys, unsigned d, unsigned k, const ef2* ch, ef2* rounds_out,
+                        ef2* final_out, ef2* partials, cudaStream_t st);
+
+// eval.cu
+struct GatherSeg {
+  const u64* src;
+  const uint64_t* idx;  // item indices into src (units of `words`)
+  uint64_t count;
+  uint32_t words;
+  u64* dst;
+};
+void gather_segments(const GatherSeg* segs_dev, unsigned nseg, cudaStream_t st);
+void new_eq_dev(const ef2* point, unsigned k, ef2* out, cudaStream_t st);
+void combine_eq_dev(const ef2* points, unsigned npts, unsigned k, const ef2* gamma, ef2* out,
+                    cudaStream_t st);
+size_t eqdot_partials_elems(unsigned k);
+// out = sum_i vec[i] * eq_point(i); vec is EF (is_bf = 0) or BF (is_bf = 1).
+void eq_dot_dev(const void* vec, int is_bf, const ef2* point, unsigned k, ef2* out,
+                ef2* partials, cudaStream_t st);
+void gemv_eq_rows(const u64* f, const ef2* eq, size_t m, size_t n, ef2* out, cudaStream_t st);
+void lift_bf(const u64* in, ef2* out, size_t n, u64 minus, cudaStream_t st);
+void bits_gather(const u64* cw, size_t two_n, const uint64_t* idx, unsigned s, size_t W,
+                 u64* bi, cudaStream_t st);
+void g1_build(const u64* A, size_t W, const ef2* eq_a2, unsigned C, ef2* g1, cudaStream_t st);
+void g2_build(const u64* bi, size_t W, unsigned s, const ef2* eq_r2, ef2* g2, cudaStream_t st);
+void v_build(const ef2* eqz1, size_t W, ef2* v, cudaStream_t st);
+void y4_dev(const ef2* eq_r2, const ef2* ra, const uint64_t* idx, unsigned s, ef2* out,
+            cudaStream_t st);
+void sel_build(const uint64_t* idx, const ef2* eq_r2, unsigned s, size_t two_n, ef2* sel,
+               cudaStream_t st);
+void rs_weights_dev(const ef2* r3, unsigned log2n, size_t n, const u64* tw, ef2* w,
+                    cudaStream_t st);
+// Basefold batched-open helpers.
+struct BfChannelDev {
+  const u64* codes;  // leaf-major: D x 2^li elements (1 u64 per BF, 2 per EF)
+  const u64* poly;   // full polynomial, BF or EF
+  int is_ef;
+  unsigned li;
+  const ef2* point;  // num_vars = li + R coordinates
+};
+void bf_combine_dev(const BfChannelDev* chs_dev, unsigned nch, const ef2* coeffs, size_t D,
+                    ef2* combined, cudaStream_t st);
+void bf_fold_poly_dev(const u64* poly, int is_ef, unsigned li, const ef2* point, size_t out_len,
+                      ef2* m, cudaStream_t st);
+void bf_rounds_dev(ef2* const* ms, ef2* const* tmps, const ef2* const* zps, unsigned nch,
+                   unsigned R, const ef2* ch, ef2* msgs_out, ef2* levels, size_t D,
+                   const u64* tw, void* scratch_ptrs, cudaStream_t st);
+
+}  // namespace lgs

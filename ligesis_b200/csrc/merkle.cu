@@ -1,0 +1,170 @@
+// Blake3 Merkle trees on the device, byte-compatible with the reference's
+// `MerkleTreeProver` (utils/src/merkle.rs:49-85 over rs_merkle 1.5.0): a leaf is
+// blake3(serialized field elements), a parent is blake3(left || right).  Nodes are stored as
+// 8 little-endian u32 words, all layers in one buffer: layer 0 (leaves) first, then each parent
+// layer, the root last.  Every tree on this path has a power-of-two leaf count.
+#include "blake3.cuh"
+#include "kernels.cuh"
+
+namespace lgs {
+
+// Leaf j is the C-row column (H[0][j], ..., H[rows-1][j]) of a row-major rows x ncols matrix.
+__global__ void leaf_hash_cols_kernel(const u64* __restrict__ H, unsigned rows, size_t ncols,
+                                      u32* __restrict__ out) {
+  size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ncols) return;
+  u32 cv[8];
+  b3_init(cv);
+  const unsigned len = rows * 8;
+  const unsigned nblocks = (len + 63) / 64;
+  for (unsigned b = 0; b < nblocks; ++b) {
+    u32 blk[16];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      unsigned r = b * 8 + q;
+      u64 v = r < rows ? H[(size_t)r * ncols + j] : 0;
+      blk[2 * q] = (u32)v;
+      blk[2 * q + 1] = (u32)(v >> 32);
+    }
+    unsigned bl = len - b * 64 < 64 ? len - b * 64 : 64;
+    u32 flags = (b == 0 ? B3_CHUNK_START : 0) | (b + 1 == nblocks ? (B3_CHUNK_END | B3_ROOT) : 0);
+    b3_compress(cv, blk, bl, flags);
+  }
+#pragma unroll
+  for (int q = 0; q < 8; ++q) out[j * 8 + q] = cv[q];
+}
+
+// Leaf p is the `words` consecutive u64 starting at data[p * words] (leaf-major layouts).
+__global__ void leaf_hash_contig_kernel(const u64* __restrict__ data, unsigned words,
+                                        size_t nleaves, u32* __restrict__ out) {
+  size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nleaves) return;
+  const u64* src = data + p * words;
+  u32 cv[8];
+  b3_init(cv);
+  const unsigned len = words * 8;
+  const unsigned nblocks = (len + 63) / 64;
+  for (unsigned b = 0; b < nblocks; ++b) {
+    u32 blk[16];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      unsigned w = b * 8 + q;
+      u64 v = w < words ? src[w] : 0;
+      blk[2 * q] = (u32)v;
+      blk[2 * q + 1] = (u32)(v >> 32);
+    }
+    unsigned bl = len - b * 64 < 64 ? len - b * 64 : 64;
+    u32 flags = (b == 0 ? B3_CHUNK_START : 0) | (b + 1 == nblocks ? (B3_CHUNK_END | B3_ROOT) : 0);
+    b3_compress(cv, blk, bl, flags);
+  }
+#pragma unroll
+  for (int q = 0; q < 8; ++q) out[p * 8 + q] = cv[q];
+}
+
+// One CTA turns 2^q consecutive nodes of one layer into the q layers above them.
+// in: first node of the input layer; out_layers[t] = first node of layer +t+1.
+__global__ void tree_reduce_kernel(u32* __restrict__ nodes, size_t in_off, size_t in_count,
+                                   unsigned q) {
+  extern __shared__ u32 sh[];  // 2^(q-1) nodes x 8 words
+  const unsigned half0 = 1u << (q - 1);
+  const size_t base = (size_t)blockIdx.x << q;
+  size_t layer_off = in_off, layer_count = in_count;
+  unsigned cnt = half0;
+  size_t local_base = base;  // index of this CTA's first node within the current layer
+  // level 1: read children from global
+  for (unsigned i = threadIdx.x; i < cnt; i += blockDim.x) {
+    const u32* l = nodes + (layer_off + local_base + 2 * i) * 8;
+    u32 lw[8], rw[8], o[8];
+#pragma unroll
+    for (int w = 0; w < 8; ++w) lw[w] = l[w], rw[w] = l[8 + w];
+    b3_parent(lw, rw, o);
+#pragma unroll
+    for (int w = 0; w < 8; ++w) sh[i * 8 + w] = o[w];
+  }
+  __syncthreads();
+  for (unsigned lev = 1; lev <= q; ++lev) {
+    size_t next_off = layer_off + layer_count;
+    size_t next_base = local_base >> 1;
+    // write this level's nodes (held in sh[0..cnt)) to global
+    for (unsigned i = threadIdx.x; i < cnt * 8; i += blockDim.x)
+      nodes[(next_off + next_base) * 8 + i] = sh[i];
+    if (lev == q) break;
+    __syncthreads();
+    unsigned ncnt = cnt >> 1;
+    u32 o[8];
+    bool act = threadIdx.x < ncnt;
+    if (act) {
+      u32 lw[8], rw[8];
+#pragma unroll
+      for (int w = 0; w < 8; ++w) lw[w] = sh[threadIdx.x * 16 + w], rw[w] = sh[threadIdx.x * 16 + 8 + w];
+      b3_parent(lw, rw, o);
+    }
+    __syncthreads();
+    if (act)
+#pragma unroll
+      for (int w = 0; w < 8; ++w) sh[threadIdx.x * 8 + w] = o[w];
+    __syncthreads();
+    layer_off = next_off;
+    layer_count >>= 1;
+    local_base = next_base;
+    cnt = ncnt;
+  }
+}
+
+size_t merkle_node_count(size_t nleaves) { return 2 * nleaves - 1; }
+size_t merkle_layer_offset(size_t nleaves, unsigned layer) {
+  size_t off = 0, cnt = nleaves;
+  for (unsigned l = 0; l < layer; ++l) {
+    off += cnt;
+    cnt >>= 1;
+  }
+  return off;
+}
+
+// Build parents for a tree whose leaf hashes are already in nodes[0 .. nleaves).
+void merkle_build_from_leaves(u32* nodes, size_t nleaves, cudaStream_t st) {
+  if (nleaves & (nleaves - 1)) throw ShapeError("merkle: leaf count must be a power of two");
+  size_t off = 0, count = nleaves;
+  while (count > 1) {
+    unsigned logc = ilog2(count);
+    unsigned q = logc < 9 ? logc : 9;
+    unsigned half0 = 1u << (q - 1);
+    unsigned threads = half0 < 256 ? (half0 < 32 ? 32 : half0) : 256;
+    size_t grid = count >> q;
+    tree_reduce_kernel<<<(unsigned)grid, threads, half0 * 32, st>>>(nodes, off, count, q);
+    LGS_LAUNCH_CHECK();
+    // advance q layers
+    for (unsigned t = 0; t < q; ++t) {
+      off += count;
+      count >>= 1;
+    }
+  }
+}
+
+void merkle_leaves_cols(const u64* H, unsigned rows, size_t ncols, u32* nodes, cudaStream_t st) {
+  leaf_hash_cols_kernel<<<cdiv(ncols, 128), 128, 0, st>>>(H, rows, ncols, nodes);
+  LGS_LAUNCH_CHECK();
+}
+void merkle_leaves_contig(const u64* data, unsigned words, size_t nleaves, u32* nodes,
+                          cudaStream_t st) {
+  if (words * 8 > 1024) throw ShapeError("merkle: leaf larger than one blake3 chunk");
+  leaf_hash_contig_kernel<<<cdiv(nleaves, 128), 128, 0, st>>>(data, words, nleaves, nodes);
+  LGS_LAUNCH_CHECK();
+}
+
+// dst[i] = src[idx[i]] for `count` items of `words` u64 each.
+__global__ void gather_kernel(const u64* __restrict__ src, const uint64_t* __restrict__ idx,
+                              size_t count, unsigned words, u64* __restrict__ dst) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count * words) return;
+  size_t i = t / words, w = t % words;
+  dst[t] = src[idx[i] * words + w];
+}
+void gather_u64(const u64* src, const uint64_t* idx, size_t count, unsigned words, u64* dst,
+                cudaStream_t st) {
+  if (!count) return;
+  gather_kernel<<<cdiv(count * words, 256), 256, 0, st>>>(src, idx, count, words, dst);
+  LGS_LAUNCH_CHECK();
+}
+
+}  // namespace lgs

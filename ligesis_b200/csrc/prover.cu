@@ -1,0 +1,541 @@
+// The LigeSIS prover on one GPU: Ligesis::setup / commit / prove (pcs/src/ligesis.rs:239-549)
+// with the Basefold interleaved commit (pcs/src/basefold.rs:257-382) and shared-domain batched
+// open (pcs/src/basefold.rs:648-856).  Every challenge of the pre-drawn oracle is known before
+// the first kernel runs, so `prove` uploads one parameter block, enqueues the whole dataflow on
+// the context stream, and reads back one staging buffer from which the proof is assembled.
+#include <cstring>
+
+#include "prover.cuh"
+
+namespace lgs {
+
+namespace {
+
+void h2d(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (bytes) LGS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+}
+void d2d(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (bytes) LGS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st));
+}
+
+// Basefold commit of `poly` (len elements, BF or EF) split into 2^li interleaved chunks
+// (MlPoly::split, utils/src/poly.rs:20-31), each zero-padded to 2 len/2^li and DFT'd; leaves are
+// the columns across chunks.  `out` receives codes (leaf-major) and the tree.
+void bf_commit(lgs_ctx* c, const u64* poly, int is_ef, size_t len, unsigned li,
+               BasefoldDev* out) {
+  Arena& ar = c->arena;
+  const size_t rows = len >> li;
+  const size_t cols = ((size_t)1 << li) * (is_ef ? 2 : 1);
+  const size_t L = rows << CODE_RATE;
+  const unsigned logL = ilog2(L);
+  u64* tT = ar.get<u64>(cols * rows);
+  u64* cT = ar.get<u64>(cols * L);
+  u64* scr = logL > 12 ? ar.get<u64>(cols * L) : nullptr;
+  transpose_u64(poly, tT, rows, cols, 1, c->st);
+  ntt_batch(tT, rows, rows, cT, L, logL, cols, scr, c->tw.as<u64>(), c->st);
+  transpose_u64(cT, out->codes, cols, L, 1, c->st);
+  merkle_leaves_contig(out->codes, (unsigned)cols, L, out->nodes, c->st);
+  merkle_build_from_leaves(out->nodes, L, c->st);
+  out->poly = poly;
+  out->is_ef = is_ef;
+  out->li = li;
+  out->num_vars = ilog2(len);
+  out->L = L;
+}
+
+Hash32 read_root(const u32* nodes, size_t nleaves, cudaStream_t st) {
+  Hash32 h;
+  LGS_CUDA(cudaMemcpyAsync(h.b, nodes + (2 * nleaves - 2) * 8, 32, cudaMemcpyDeviceToHost, st));
+  LGS_CUDA(cudaStreamSynchronize(st));
+  return h;
+}
+
+}  // namespace
+
+void ctx_init(lgs_ctx* c, int device) {
+  c->device = device;
+  LGS_CUDA(cudaSetDevice(device));
+  LGS_CUDA(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+  c->tw.alloc(((size_t)1 << TW_LOG) * sizeof(u64));
+  build_twiddles(c->tw.as<u64>(), c->st);
+  LGS_CUDA(cudaStreamSynchronize(c->st));
+}
+
+void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lgs_pk* pk) {
+  Shape s{log_m, log_n};
+  if (!s.eval_ok())
+    throw ShapeError("batched LigeSIS needs the {A, B_I, a} var counts within LOG_INTERLEAVE");
+  pk->shape = s;
+  const size_t W = s.W(), len = (size_t)DIGEST_ROWS * W;
+  c->arena.begin();
+  pk->A.alloc(len * 8);
+  std::vector<u64> canon(A_host, A_host + len);
+  for (auto& x : canon) x = gl_canon(x);
+  h2d(pk->A.p, canon.data(), len * 8, c->st);
+  pk->alimb.alloc(len * 8);
+  alimb_from_a(pk->A.as<u64>(), pk->alimb.as<uint8_t>(), W, c->st);
+  const unsigned li = s.li(s.na());
+  const size_t L = (len >> li) << CODE_RATE;
+  pk->a_codes.alloc(L * ((size_t)1 << li) * 8);
+  pk->a_nodes.alloc((2 * L - 1) * 32);
+  pk->a_state.codes = pk->a_codes.as<u64>();
+  pk->a_state.nodes = pk->a_nodes.as<u32>();
+  bf_commit(c, pk->A.as<u64>(), 0, len, li, &pk->a_state);
+  pk->com_a = read_root(pk->a_state.nodes, L, c->st);
+}
+
+// Ligesis::commit (pcs/src/ligesis.rs:277-325): RS-encode rows, hash B's columns, Merkle the
+// digest columns.  `f` may be a host or a device pointer (f_on_device).
+void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
+                lgs_commit_data* cd) {
+  const Shape& s = pk->shape;
+  const size_t m = s.m(), n = s.n(), two_n = 2 * n;
+  if (two_n % 128) throw ShapeError("commit: 2n must be a multiple of 128");
+  cd->shape = s;
+  c->arena.begin();
+  if (cd->f.bytes != m * n * 8) cd->f.alloc(m * n * 8);
+  if (cd->cw.bytes != m * two_n * 8) cd->cw.alloc(m * two_n * 8);
+  if (cd->H.bytes != DIGEST_ROWS * two_n * 8) cd->H.alloc(DIGEST_ROWS * two_n * 8);
+  if (cd->nodes.bytes != (2 * two_n - 1) * 32) cd->nodes.alloc((2 * two_n - 1) * 32);
+  if (f_on_device)
+    d2d(cd->f.p, f, m * n * 8, c->st);
+  else
+    h2d(cd->f.p, f, m * n * 8, c->st);
+  const unsigned logN = ilog2(two_n);
+  u64* scr = logN > 12 ? c->arena.get<u64>(m * two_n) : nullptr;
+  ntt_batch(cd->f.as<u64>(), n, n, cd->cw.as<u64>(), two_n, logN, m, scr, c->tw.as<u64>(), c->st);
+  subset_sum_hash(pk->alimb.as<uint8_t>(), cd->cw.as<u64>(), cd->H.as<u64>(), (unsigned)m, two_n,
+                  c->st);
+  merkle_leaves_cols(cd->H.as<u64>(), DIGEST_ROWS, two_n, cd->nodes.as<u32>(), c->st);
+  merkle_build_from_leaves(cd->nodes.as<u32>(), two_n, c->st);
+  cd->root = read_root(cd->nodes.as<u32>(), two_n, c->st);
+}
+
+// ---------------------------------------------------------------------------------------------
+// prove
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+// Staging buffer layout (u64 offsets) for everything the proof reads back from the device.
+struct Stage {
+  size_t total = 0;
+  size_t take(size_t words) {
+    size_t o = total;
+    total += words;
+    return o;
+  }
+};
+
+struct SegPlan {
+  std::vector<GatherSeg> segs;  // idx and dst hold offsets until relocated
+  std::vector<uint64_t> idx;    // all index lists, concatenated
+  void add(const u64* src, const std::vector<uint64_t>& items, unsigned words, size_t dst_off) {
+    GatherSeg g;
+    g.src = src;
+    g.idx = (const uint64_t*)(uintptr_t)idx.size();
+    g.count = items.size();
+    g.words = words;
+    g.dst = (u64*)(uintptr_t)dst_off;
+    idx.insert(idx.end(), items.begin(), items.end());
+    segs.push_back(g);
+  }
+};
+
+struct OpenPlan {  // one Merkle opening read back from the device
+  size_t node_off, nnodes, val_off;
+  std::vector<uint64_t> keys;
+  unsigned words;
+};
+
+const size_t SC_D[7] = {3, 2, 2, 2, 2, 2, 2};
+
+}  // namespace
+
+void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u64* z_host,
+               size_t zlen, const u64* fields_host, size_t nfields, const uint64_t* ints_host,
+               size_t nints, uint64_t cursors[2], std::vector<uint8_t>* proof_out) {
+  const Shape& s = pk->shape;
+  if (cd->shape.log_m != s.log_m || cd->shape.log_n != s.log_n)
+    throw ShapeError("prove: commitment shape differs from the key");
+  if (zlen != s.log_m + s.log_n) throw ShapeError("prove: point length must be log_m + log_n");
+  const size_t m = s.m(), n = s.n(), two_n = 2 * n, W = s.W(), S = NUM_COLS;
+  const unsigned log_n = s.log_n, log_w = s.log_w(), log_s = s.log_s();
+  const unsigned nb = log_w + log_s, R = s.R();
+  const size_t D = s.D(), WS = W * S;
+  const FieldPlan fp(s);
+  const uint64_t f0 = cursors[0], i0 = cursors[1];
+  if (f0 > nfields || nfields - f0 < fp.total) throw OracleError("oracle exhausted (fields)");
+  if (i0 > nints || nints - i0 < INTS_PER_PROOF) throw OracleError("oracle exhausted (ints)");
+  cudaStream_t st = c->st;
+  Arena& ar = c->arena;
+  ar.begin();
+
+  // ---- host transcript: indices and points --------------------------------------------------
+  std::vector<uint64_t> idx;
+  if (!sample_columns(ints_host + i0, two_n, &idx))
+    throw OracleError("not enough distinct columns sampled from oracle");
+  std::vector<uint64_t> sorted_idx(idx);
+  std::sort(sorted_idx.begin(), sorted_idx.end());
+  const std::vector<uint64_t> base = query_base(ints_host + i0 + 4 * NUM_COLS, D / 2);
+  const std::vector<uint64_t> bpos = level_positions(base, D / 2);
+
+  const u64* F = fields_host + 2 * f0;  // EF fields from the cursor
+  auto fld = [&](unsigned off) { return ef_make(F[2 * off], F[2 * off + 1]); };
+  auto slice = [&](unsigned off, unsigned len) {
+    std::vector<ef2> v(len);
+    for (unsigned i = 0; i < len; ++i) v[i] = fld(off + i);
+    return v;
+  };
+  auto rev = [](std::vector<ef2> v) {
+    std::reverse(v.begin(), v.end());
+    return v;
+  };
+  auto cat = [](std::vector<ef2> a, const std::vector<ef2>& b) {
+    a.insert(a.end(), b.begin(), b.end());
+    return a;
+  };
+  std::vector<ef2> z(zlen);
+  for (size_t i = 0; i < zlen; ++i) z[i] = ef_make(gl_canon(z_host[2 * i]), gl_canon(z_host[2 * i + 1]));
+  const std::vector<ef2> z2(z.begin(), z.begin() + log_n), z1(z.begin() + log_n, z.end());
+  const auto alpha2 = slice(fp.alpha2, 5);
+  const auto r2 = slice(fp.r2, log_s);
+  const auto r1 = rev(slice(fp.ch_bin, nb));
+  const auto r4 = rev(slice(fp.ch_hash, log_w));
+  const auto r5 = rev(slice(fp.ch_recon, log_w));
+  const auto r3 = rev(slice(fp.ch_table, log_n + 1));
+  const auto r6 = rev(slice(fp.ch_rs, log_n));
+  const auto r_bi = rev(slice(fp.ch_bi, nb));
+  const auto r_a = rev(slice(fp.ch_a, log_n));
+  const auto p_a = cat(r4, alpha2);
+  const auto p_bi_hash = cat(r2, r4);
+  const auto p_bi_recon = cat(r2, r5);
+
+  // ---- parameter block ---------------------------------------------------------------------
+  std::vector<ef2> prm;  // EF section
+  auto put = [&](const std::vector<ef2>& v) {
+    size_t o = prm.size();
+    prm.insert(prm.end(), v.begin(), v.end());
+    return o;
+  };
+  const size_t P_fields = put(slice(0, fp.total));
+  const size_t P_z1 = put(z1), P_z2 = put(z2), P_r3 = put(r3);
+  const size_t P_bipts = put(cat(cat(r1, p_bi_hash), p_bi_recon));
+  const size_t P_apts = put(cat(z2, r6));
+  const size_t P_pa = put(p_a), P_rbi = put(r_bi), P_ra = put(r_a);
+
+  // ---- staging layout ----------------------------------------------------------------------
+  Stage sg;
+  const size_t S_y = sg.take(2), S_y4 = sg.take(2), S_y5 = sg.take(2);
+  const size_t S_coma = sg.take(4), S_comi = sg.take(4);
+  const size_t S_hcols = sg.take(S * DIGEST_ROWS);
+  const std::vector<uint64_t> h_nodes = multiproof_nodes(sorted_idx, two_n);
+  const size_t S_hopen = sg.take(h_nodes.size() * 4);
+  const unsigned sc_k[7] = {nb, log_w, log_w, log_n + 1, log_n, nb, log_n};
+  const unsigned sc_ch[7] = {fp.ch_bin, fp.ch_hash, fp.ch_recon, fp.ch_table, fp.ch_rs, fp.ch_bi, fp.ch_a};
+  size_t S_sc_r[7], S_sc_f[7];
+  for (int i = 0; i < 7; ++i) {
+    S_sc_r[i] = sg.take(sc_k[i] * (SC_D[i] + 1) * 2);
+    S_sc_f[i] = sg.take(SC_D[i] * 2);
+  }
+  const unsigned NCH = 3;
+  const size_t S_msgs = sg.take(NCH * R * 2);
+  const size_t S_roots = sg.take((R ? R - 1 : 0) * 4);
+  const size_t final_len = D >> R;
+  const size_t S_final = sg.take(final_len * 2);
+
+  // ---- device buffers ----------------------------------------------------------------------
+  ef2* d_prm = ar.get<ef2>(prm.size());
+  const ef2* d_fields = d_prm + P_fields;
+  ef2* eqz1 = ar.get<ef2>(m);
+  ef2* a_vec = ar.get<ef2>(n);
+  ef2* ra = ar.get<ef2>(two_n);
+  const unsigned kmax = std::max(nb, log_n + 1);
+  ef2* partials = ar.get<ef2>(std::max<size_t>(eqdot_partials_elems(kmax), 1024));
+  uint64_t* d_idx = ar.get<uint64_t>(S);
+
+  // Basefold states built during prove
+  BasefoldDev a_st, bi_st;
+  const unsigned li_a = s.li(s.naa()), li_bi = s.li(s.nbi()), li_A = s.li(s.na());
+  a_st.codes = ar.get<u64>(D * ((size_t)2 << li_a));
+  a_st.nodes = ar.get<u32>((2 * D - 1) * 8);
+  bi_st.codes = ar.get<u64>(D * ((size_t)1 << li_bi));
+  bi_st.nodes = ar.get<u32>((2 * D - 1) * 8);
+  u64* bi = ar.get<u64>(WS);
+
+  // upload: params, idx
+  h2d(d_prm, prm.data(), prm.size() * sizeof(ef2), st);
+  h2d(d_idx, idx.data(), S * 8, st);
+
+  // Staging is allocated once the layout is final (openings appended below).
+  // -- a-bar, y, commit a-bar, RS(a-bar) (pcs/src/ligesis.rs:365-387)
+  new_eq_dev(d_prm + P_z1, s.log_m, eqz1, st);
+  gemv_eq_rows(cd->f.as<u64>(), eqz1, m, n, a_vec, st);
+
+  std::vector<OpenPlan> opens;  // base_bf(A), base_bf(B_I), base_ef(a), then fold levels
+  SegPlan plan;
+  // The gather plan and the rest of the staging layout are needed before allocation.
+  // Base openings at bpos for the three channels.
+  const BasefoldDev* chan_states[3] = {&pk->a_state, &bi_st, &a_st};
+  const unsigned chan_li[3] = {li_A, li_bi, li_a};
+  const int chan_ef[3] = {0, 0, 1};
+  for (int ch = 0; ch < 3; ++ch) {
+    OpenPlan o;
+    std::vector<uint64_t> nodes = multiproof_nodes(bpos, D);
+    o.nnodes = nodes.size();
+    o.node_off = sg.take(nodes.size() * 4);
+    o.words = ((1u << chan_li[ch]) * (chan_ef[ch] ? 2 : 1));
+    o.val_off = sg.take(bpos.size() * o.words);
+    o.keys = bpos;
+    opens.push_back(o);
+  }
+  std::vector<std::vector<uint64_t>> lvl_pos(R);
+  for (unsigned k = 1; k < R; ++k) {
+    OpenPlan o;
+    lvl_pos[k] = level_positions(base, (D >> k) / 2);
+    std::vector<uint64_t> nodes = multiproof_nodes(lvl_pos[k], D >> k);
+    o.nnodes = nodes.size();
+    o.node_off = sg.take(nodes.size() * 4);
+    o.words = 2;
+    o.val_off = sg.take(lvl_pos[k].size() * 2);
+    o.keys = lvl_pos[k];
+    opens.push_back(o);
+  }
+  u64* stage = ar.get<u64>(sg.total);
+
+  // -- continue the dataflow
+  eq_dot_dev(a_vec, 0, d_prm + P_z2, log_n, (ef2*)(stage + S_y), partials, st);
+  bf_commit(c, (const u64*)a_vec, 1, n, li_a, &a_st);
+  {
+    u64* t1 = ar.get<u64>(2 * n);
+    u64* t2 = ar.get<u64>(2 * two_n);
+    u64* scr = ilog2(two_n) > 12 ? ar.get<u64>(2 * two_n) : nullptr;
+    transpose_u64((const u64*)a_vec, t1, n, 2, 1, st);
+    ntt_batch(t1, n, n, t2, two_n, ilog2(two_n), 2, scr, c->tw.as<u64>(), st);
+    transpose_u64(t2, (u64*)ra, 2, two_n, 1, st);
+  }
+  // -- B_I and its commitment (pcs/src/ligesis.rs:403-416)
+  bits_gather(cd->cw.as<u64>(), two_n, d_idx, S, W, bi, st);
+  bf_commit(c, bi, 0, WS, li_bi, &bi_st);
+
+  // -- binary check (pcs/src/ligesis.rs:419-429)
+  ef2* partials_sc = ar.get<ef2>(sumcheck_partials_elems(kmax, 3));
+  {
+    ef2* p0 = ar.get<ef2>(WS);
+    ef2* p1 = ar.get<ef2>(WS);
+    ef2* p2 = ar.get<ef2>(WS);
+    lift_bf(bi, p0, WS, 0, st);
+    lift_bf(bi, p1, WS, 1, st);
+    new_eq_dev(d_fields + fp.alpha1, nb, p2, st);
+    ef2* ps[3] = {p0, p1, p2};
+    sumcheck_prove_dev(ps, 3, nb, d_fields + fp.ch_bin, (ef2*)(stage + S_sc_r[0]),
+                       (ef2*)(stage + S_sc_f[0]), partials_sc, st);
+  }
+  // -- hash / recon channels (pcs/src/ligesis.rs:432-485)
+  ef2* eq_a2 = ar.get<ef2>(DIGEST_ROWS);
+  ef2* eq_r2 = ar.get<ef2>(S);
+  new_eq_dev(d_fields + fp.alpha2, 5, eq_a2, st);
+  new_eq_dev(d_fields + fp.r2, log_s, eq_r2, st);
+  {
+    ef2* g1 = ar.get<ef2>(W);
+    ef2* g2 = ar.get<ef2>(W);
+    ef2* g2b = ar.get<ef2>(W);
+    ef2* v = ar.get<ef2>(W);
+    g1_build(pk->A.as<u64>(), W, eq_a2, DIGEST_ROWS, g1, st);
+    g2_build(bi, W, S, eq_r2, g2, st);
+    d2d(g2b, g2, W * sizeof(ef2), st);
+    y4_dev(eq_r2, ra, d_idx, S, (ef2*)(stage + S_y4), st);
+    v_build(eqz1, W, v, st);
+    ef2* ph[2] = {g1, g2};
+    sumcheck_prove_dev(ph, 2, log_w, d_fields + fp.ch_hash, (ef2*)(stage + S_sc_r[1]),
+                       (ef2*)(stage + S_sc_f[1]), partials_sc, st);
+    ef2* pr[2] = {v, g2b};
+    sumcheck_prove_dev(pr, 2, log_w, d_fields + fp.ch_recon, (ef2*)(stage + S_sc_r[2]),
+                       (ef2*)(stage + S_sc_f[2]), partials_sc, st);
+  }
+  // -- recon table, y5, RS link (pcs/src/ligesis.rs:487-502)
+  {
+    ef2* sel = ar.get<ef2>(two_n);
+    ef2* rac = ar.get<ef2>(two_n);
+    sel_build(d_idx, eq_r2, S, two_n, sel, st);
+    d2d(rac, ra, two_n * sizeof(ef2), st);
+    ef2* pt[2] = {sel, rac};
+    sumcheck_prove_dev(pt, 2, log_n + 1, d_fields + fp.ch_table, (ef2*)(stage + S_sc_r[3]),
+                       (ef2*)(stage + S_sc_f[3]), partials_sc, st);
+    eq_dot_dev(ra, 0, d_prm + P_r3, log_n + 1, (ef2*)(stage + S_y5), partials, st);
+    ef2* w = ar.get<ef2>(n);
+    ef2* ac = ar.get<ef2>(n);
+    rs_weights_dev(d_prm + P_r3, log_n + 1, n, c->tw.as<u64>(), w, st);
+    d2d(ac, a_vec, n * sizeof(ef2), st);
+    ef2* pw[2] = {ac, w};
+    sumcheck_prove_dev(pw, 2, log_n, d_fields + fp.ch_rs, (ef2*)(stage + S_sc_r[4]),
+                       (ef2*)(stage + S_sc_f[4]), partials_sc, st);
+  }
+  // -- Stage A (pcs/src/ligesis.rs:510-522)
+  {
+    ef2* gbi = ar.get<ef2>(WS);
+    ef2* bie = ar.get<ef2>(WS);
+    combine_eq_dev(d_prm + P_bipts, 3, nb, d_fields + fp.gamma_bi, gbi, st);
+    lift_bf(bi, bie, WS, 0, st);
+    ef2* pb[2] = {bie, gbi};
+    sumcheck_prove_dev(pb, 2, nb, d_fields + fp.ch_bi, (ef2*)(stage + S_sc_r[5]),
+                       (ef2*)(stage + S_sc_f[5]), partials_sc, st);
+    ef2* ga = ar.get<ef2>(n);
+    ef2* ac = ar.get<ef2>(n);
+    combine_eq_dev(d_prm + P_apts, 2, log_n, d_fields + fp.gamma_a, ga, st);
+    d2d(ac, a_vec, n * sizeof(ef2), st);
+    ef2* pa[2] = {ac, ga};
+    sumcheck_prove_dev(pa, 2, log_n, d_fields + fp.ch_a, (ef2*)(stage + S_sc_r[6]),
+                       (ef2*)(stage + S_sc_f[6]), partials_sc, st);
+  }
+  // -- Stage B: shared-domain batched open (pcs/src/basefold.rs:679-856)
+  ef2* levels = ar.get<ef2>(2 * D);
+  {
+    BfChannelDev chs[3];
+    const ef2* pts[3] = {d_prm + P_pa, d_prm + P_rbi, d_prm + P_ra};
+    const u64* polys[3] = {pk->A.as<u64>(), bi, (const u64*)a_vec};
+    for (int ch = 0; ch < 3; ++ch) {
+      chs[ch].codes = chan_states[ch]->codes;
+      chs[ch].poly = polys[ch];
+      chs[ch].is_ef = chan_ef[ch];
+      chs[ch].li = chan_li[ch];
+      chs[ch].point = pts[ch];
+    }
+    BfChannelDev* d_chs = ar.get<BfChannelDev>(3);
+    std::vector<uint8_t>& hs = c->host_stage;  // keep the host copy alive until the sync below
+    hs.assign((const uint8_t*)chs, (const uint8_t*)chs + sizeof(chs));
+    h2d(d_chs, hs.data(), sizeof(chs), st);
+    bf_combine_dev(d_chs, 3, d_fields + fp.coeffs, D, levels, st);
+    ef2* ms[3];
+    ef2* tmps[3];
+    const ef2* zps[3];
+    const size_t mlen = (size_t)1 << R;
+    for (int ch = 0; ch < 3; ++ch) {
+      ms[ch] = ar.get<ef2>(mlen);
+      tmps[ch] = ar.get<ef2>(mlen);
+      bf_fold_poly_dev(polys[ch], chan_ef[ch], chan_li[ch], pts[ch], mlen, ms[ch], st);
+      zps[ch] = pts[ch] + chan_li[ch];
+    }
+    bf_rounds_dev(ms, tmps, zps, 3, R, d_fields + fp.ch_batch, (ef2*)(stage + S_msgs), levels, D,
+                  c->tw.as<u64>(), nullptr, st);
+  }
+  // level trees 1..R-1 (leaf = one serialized EF)
+  std::vector<u32*> lvl_nodes(R, nullptr);
+  {
+    size_t off = D;
+    for (unsigned k = 1; k < R; ++k) {
+      size_t len = D >> k;
+      lvl_nodes[k] = ar.get<u32>((2 * len - 1) * 8);
+      merkle_leaves_contig((const u64*)(levels + off), 2, len, lvl_nodes[k], st);
+      merkle_build_from_leaves(lvl_nodes[k], len, st);
+      off += len;
+    }
+  }
+
+  // ---- gathers into staging ----------------------------------------------------------------
+  {
+    std::vector<uint64_t> hidx;  // H[r][sorted_idx[k]], column by column
+    for (uint64_t j : sorted_idx)
+      for (unsigned r = 0; r < DIGEST_ROWS; ++r) hidx.push_back((uint64_t)r * two_n + j);
+    plan.add(cd->H.as<u64>(), hidx, 1, S_hcols);
+    plan.add((const u64*)cd->nodes.as<u32>(), h_nodes, 4, S_hopen);
+    plan.add((const u64*)a_st.nodes, {2 * D - 2}, 4, S_coma);
+    plan.add((const u64*)bi_st.nodes, {2 * D - 2}, 4, S_comi);
+    for (int ch = 0; ch < 3; ++ch) {
+      const OpenPlan& o = opens[ch];
+      plan.add((const u64*)chan_states[ch]->nodes, multiproof_nodes(bpos, D), 4, o.node_off);
+      plan.add(chan_states[ch]->codes, bpos, o.words, o.val_off);
+    }
+    size_t off = D;
+    for (unsigned k = 1; k < R; ++k) {
+      const OpenPlan& o = opens[2 + k];
+      size_t len = D >> k;
+      plan.add((const u64*)lvl_nodes[k], multiproof_nodes(lvl_pos[k], len), 4, o.node_off);
+      plan.add((const u64*)(levels + off), lvl_pos[k], 2, o.val_off);
+      plan.add((const u64*)lvl_nodes[k], {2 * len - 2}, 4, S_roots + (k - 1) * 4);
+      off += len;
+    }
+    std::vector<uint64_t> fin(final_len);
+    for (size_t i = 0; i < final_len; ++i) fin[i] = i;
+    plan.add((const u64*)(levels + off), fin, 2, S_final);
+  }
+  uint64_t* d_gidx = ar.get<uint64_t>(plan.idx.size());
+  GatherSeg* d_segs = ar.get<GatherSeg>(plan.segs.size());
+  std::vector<GatherSeg> segs = plan.segs;
+  for (auto& g : segs) {
+    g.idx = d_gidx + (uintptr_t)g.idx;
+    g.dst = stage + (uintptr_t)g.dst;
+  }
+  std::vector<uint8_t> seg_bytes((const uint8_t*)segs.data(),
+                                 (const uint8_t*)(segs.data() + segs.size()));
+  h2d(d_gidx, plan.idx.data(), plan.idx.size() * 8, st);
+  h2d(d_segs, seg_bytes.data(), seg_bytes.size(), st);
+  gather_segments(d_segs, (unsigned)segs.size(), st);
+
+  std::vector<u64> hst(sg.total);
+  LGS_CUDA(cudaMemcpyAsync(hst.data(), stage, sg.total * 8, cudaMemcpyDeviceToHost, st));
+  LGS_CUDA(cudaStreamSynchronize(st));
+
+  // ---- assemble ----------------------------------------------------------------------------
+  auto efat = [&](size_t off) { return ef_make(hst[off], hst[off + 1]); };
+  auto h32at = [&](size_t off) {
+    Hash32 h;
+    std::memcpy(h.b, &hst[off], 32);
+    return h;
+  };
+  ProofH p;
+  p.y = efat(S_y);
+  p.y4 = efat(S_y4);
+  p.y5 = efat(S_y5);
+  p.com_a_vec = h32at(S_coma);
+  p.com_i = h32at(S_comi);
+  p.h_cols.assign(S, std::vector<u64>(DIGEST_ROWS));
+  for (size_t k = 0; k < S; ++k)
+    for (unsigned r = 0; r < DIGEST_ROWS; ++r) p.h_cols[k][r] = hst[S_hcols + k * DIGEST_ROWS + r];
+  p.h_open.assign((const uint8_t*)&hst[S_hopen], (const uint8_t*)&hst[S_hopen] + h_nodes.size() * 32);
+  for (int i = 0; i < 7; ++i) {
+    const size_t w = SC_D[i] + 1;
+    p.sc[i].rounds.assign(sc_k[i], std::vector<ef2>(w));
+    for (unsigned t = 0; t < sc_k[i]; ++t)
+      for (size_t q = 0; q < w; ++q) p.sc[i].rounds[t][q] = efat(S_sc_r[i] + (t * w + q) * 2);
+    for (size_t j = 0; j < SC_D[i]; ++j) p.sc[i].finals.push_back(efat(S_sc_f[i] + 2 * j));
+  }
+  (void)sc_ch;
+  BatchProofH& b = p.batch;
+  b.code_rate = CODE_RATE;
+  b.log_len = ilog2(D);
+  b.msgs.assign(NCH, std::vector<ef2>(R));
+  for (unsigned ch = 0; ch < NCH; ++ch)
+    for (unsigned t = 0; t < R; ++t) b.msgs[ch][t] = efat(S_msgs + (ch * R + t) * 2);
+  for (unsigned k = 1; k < R; ++k) b.fold_roots.push_back(h32at(S_roots + (k - 1) * 4));
+  for (size_t i = 0; i < final_len; ++i) b.final_codeword.push_back(efat(S_final + 2 * i));
+  for (size_t oi = 0; oi < opens.size(); ++oi) {
+    const OpenPlan& o = opens[oi];
+    std::vector<uint8_t> pbytes((const uint8_t*)&hst[o.node_off],
+                                (const uint8_t*)&hst[o.node_off] + o.nnodes * 32);
+    if (oi < 2) {
+      OpeningH<u64> op;
+      op.proof = pbytes;
+      for (size_t i = 0; i < o.keys.size(); ++i)
+        op.values.push_back({o.keys[i], std::vector<u64>(&hst[o.val_off + i * o.words],
+                                                          &hst[o.val_off + (i + 1) * o.words])});
+      b.base_bf.push_back(op);
+    } else {
+      OpeningH<ef2> op;
+      op.proof = pbytes;
+      for (size_t i = 0; i < o.keys.size(); ++i) {
+        std::vector<ef2> v(o.words / 2);
+        for (size_t q = 0; q < v.size(); ++q) v[q] = efat(o.val_off + i * o.words + 2 * q);
+        op.values.push_back({o.keys[i], v});
+      }
+      if (oi == 2)
+        b.base_ef.push_back(op);
+      else
+        b.fold_openings.push_back(op);
+    }
+  }
+  *proof_out = encode_proof(p);
+  cursors[0] = f0 + fp.total;
+  cursors[1] = i0 + INTS_PER_PROOF;
+}
+
+}  // namespace lgs

@@ -1,0 +1,115 @@
+// Host-side state of the prover library: device buffers, the per-context arena, the proving
+// key and commitment data (the reference's ProvingKey / CommitData, pcs/src/ligesis.rs:67-97)
+// kept resident on the device.
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "proof.hpp"
+
+namespace lgs {
+
+struct DevMem {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevMem() = default;
+  explicit DevMem(size_t b) { alloc(b); }
+  void alloc(size_t b) {
+    release();
+    if (b) LGS_CUDA(cudaMalloc(&p, b));
+    bytes = b;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  ~DevMem() { release(); }
+  DevMem(const DevMem&) = delete;
+  DevMem& operator=(const DevMem&) = delete;
+  DevMem(DevMem&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr, o.bytes = 0; }
+  DevMem& operator=(DevMem&& o) noexcept {
+    release();
+    p = o.p, bytes = o.bytes;
+    o.p = nullptr, o.bytes = 0;
+    return *this;
+  }
+  template <class T>
+  T* as() const {
+    return (T*)p;
+  }
+};
+
+// Bump allocator for per-call device scratch.  A call that outgrows the buffer takes extra
+// allocations; the next call starts from one buffer of the previous peak size, so steady-state
+// calls of one shape allocate nothing.
+struct Arena {
+  DevMem mem;
+  std::vector<DevMem> overflow;
+  size_t off = 0, peak = 0;
+  void begin() {
+    if (!overflow.empty() || peak > mem.bytes) {
+      overflow.clear();
+      mem.alloc(peak + (peak >> 4));
+    }
+    off = 0;
+    peak = 0;
+  }
+  template <class T>
+  T* get(size_t count) {
+    size_t b = (count * sizeof(T) + 255) & ~(size_t)255;
+    if (b == 0) b = 256;
+    T* r;
+    if (off + b <= mem.bytes) {
+      r = (T*)((char*)mem.p + off);
+    } else {
+      overflow.emplace_back(b);
+      r = overflow.back().as<T>();
+    }
+    off += b;
+    peak = std::max(peak, off);
+    return r;
+  }
+};
+
+struct BasefoldDev {
+  u64* codes = nullptr;  // leaf-major: L x 2^li elements (1 u64 per BF, 2 per EF)
+  u32* nodes = nullptr;  // Merkle tree, layer-major, 8 words per node
+  const u64* poly = nullptr;
+  int is_ef = 0;
+  unsigned li = 0, num_vars = 0;
+  size_t L = 0;
+  unsigned leaf_words() const { return (1u << li) * (is_ef ? 2 : 1); }
+  size_t node_count() const { return 2 * L - 1; }
+};
+
+}  // namespace lgs
+
+struct lgs_ctx {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  lgs::DevMem tw;
+  lgs::Arena arena;
+  std::vector<uint8_t> host_stage;  // host copies that must outlive an async upload
+  std::vector<uint8_t> proof_buf;   // the last proof returned by lgs_prove
+};
+
+struct lgs_pk {
+  lgs::Shape shape;
+  lgs::DevMem A;      // 32 x W canonical u64, row-major (the flat A-bar of subset_sum.rs:73-79)
+  lgs::DevMem alimb;  // 256 x W bytes: byte l of A[r][k] at row 8r + l
+  lgs::DevMem a_codes, a_nodes;
+  lgs::BasefoldDev a_state;
+  lgs::Hash32 com_a;
+};
+
+struct lgs_commit_data {
+  lgs::Shape shape;
+  lgs::DevMem f;      // m x n
+  lgs::DevMem cw;     // m x 2n RS codeword F' (its bits are B)
+  lgs::DevMem H;      // 32 x 2n digest
+  lgs::DevMem nodes;  // column Merkle tree over H
+  lgs::Hash32 root;
+};

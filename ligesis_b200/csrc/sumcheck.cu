@@ -1,0 +1,214 @@
+// Product sumcheck prover (utils/src/sumcheck.rs:37-84) on the device.
+//
+// Round t sends g_t(q) = sum_{i < half} prod_j (lo_j + q (hi_j - lo_j)), q = 0..d, with
+// lo = P[i], hi = P[i + half] (the HIGH variable is bound first), then folds every factor with
+// the round challenge r_t: P[i] = P[i] + r_t (P[i + half] - P[i]).  All challenges come from the
+// pre-drawn oracle (utils/src/oracle.rs:10-64), so no round depends on the host: the fold of
+// round t-1 is fused into the evaluation pass of round t (each thread owns the quadruple
+// i, i + half, i + 2 half, i + 3 half, so the in-place fold has no races), per-CTA partial sums
+// go to a scratch array, and a last kernel reduces them into the round polynomials.  Once the
+// vectors are short, one CTA finishes the remaining rounds on its own.
+#include "kernels.cuh"
+
+namespace lgs {
+
+namespace {
+constexpr unsigned SC_THREADS = 256;
+constexpr unsigned SC_TAIL_LEN = 4096;  // vectors at most this long finish in one CTA
+
+__device__ __forceinline__ ef2 shfl_xor_ef(ef2 v, int m) {
+  ef2 r;
+  r.c0 = __shfl_xor_sync(0xffffffffu, v.c0, m);
+  r.c1 = __shfl_xor_sync(0xffffffffu, v.c1, m);
+  return r;
+}
+
+// Sum D+1 EF values over the CTA; result valid in thread 0.  `red` holds (D+1) * 32 entries.
+template <int D>
+__device__ void block_reduce(ef2 (&s)[D + 1], ef2* red) {
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int q = 0; q <= D; ++q)
+#pragma unroll
+    for (int m = 16; m; m >>= 1) s[q] = ef_add(s[q], shfl_xor_ef(s[q], m));
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q <= D; ++q) red[q * 32 + warp] = s[q];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int q = 0; q <= D; ++q) {
+      ef2 v = lane < nw ? red[q * 32 + lane] : ef_zero();
+#pragma unroll
+      for (int m = 16; m; m >>= 1) v = ef_add(v, shfl_xor_ef(v, m));
+      s[q] = v;
+    }
+  }
+  __syncthreads();
+}
+
+template <int D>
+__device__ __forceinline__ void accumulate_pair(const ef2 (&lo)[D], const ef2 (&hi)[D],
+                                                ef2 (&s)[D + 1]) {
+  ef2 v[D], df[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) v[j] = lo[j], df[j] = ef_sub(hi[j], lo[j]);
+#pragma unroll
+  for (int q = 0; q <= D; ++q) {
+    ef2 p = v[0];
+#pragma unroll
+    for (int j = 1; j < D; ++j) p = ef_mul(p, v[j]);
+    s[q] = ef_add(s[q], p);
+    if (q < D)
+#pragma unroll
+      for (int j = 0; j < D; ++j) v[j] = ef_add(v[j], df[j]);
+  }
+}
+
+template <int D>
+struct Polys {
+  ef2* p[D];
+};
+
+// One round over `half` pairs.  If `fold`, the vectors still hold 4*half entries from the
+// previous round and are folded with r first (results written back to [0, 2*half)).
+template <int D>
+__global__ void __launch_bounds__(SC_THREADS)
+    sc_round_kernel(Polys<D> P, size_t half, int fold, const ef2* __restrict__ rptr,
+                    ef2* __restrict__ partial) {
+  __shared__ ef2 red[(D + 1) * 32];
+  ef2 s[D + 1];
+#pragma unroll
+  for (int q = 0; q <= D; ++q) s[q] = ef_zero();
+  const ef2 r = fold ? *rptr : ef_zero();
+  const size_t len = 2 * half;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < half;
+       i += (size_t)gridDim.x * blockDim.x) {
+    ef2 lo[D], hi[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      ef2* p = P.p[j];
+      if (fold) {
+        lo[j] = ef_lerp(p[i], p[i + len], r);
+        hi[j] = ef_lerp(p[i + half], p[i + half + len], r);
+        p[i] = lo[j];
+        p[i + half] = hi[j];
+      } else {
+        lo[j] = p[i];
+        hi[j] = p[i + half];
+      }
+    }
+    accumulate_pair<D>(lo, hi, s);
+  }
+  block_reduce<D>(s, red);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q <= D; ++q) partial[(size_t)blockIdx.x * (D + 1) + q] = s[q];
+}
+
+// Remaining rounds t0..k-1 in one CTA.  On entry the vectors hold `len` entries; if `fold`,
+// they hold 2*len entries still to be folded with challenge t0-1.
+template <int D>
+__global__ void __launch_bounds__(1024)
+    sc_tail_kernel(Polys<D> P, size_t len, int fold, const ef2* __restrict__ ch, unsigned t0,
+                   unsigned k, ef2* __restrict__ rounds_out, ef2* __restrict__ final_out) {
+  __shared__ ef2 red[(D + 1) * 32];
+  if (fold) {
+    const ef2 r = ch[t0 - 1];
+    for (size_t i = threadIdx.x; i < len; i += blockDim.x)
+#pragma unroll
+      for (int j = 0; j < D; ++j) P.p[j][i] = ef_lerp(P.p[j][i], P.p[j][i + len], r);
+    __syncthreads();
+  }
+  for (unsigned t = t0; t < k; ++t) {
+    const size_t half = len >> 1;
+    ef2 s[D + 1];
+#pragma unroll
+    for (int q = 0; q <= D; ++q) s[q] = ef_zero();
+    for (size_t i = threadIdx.x; i < half; i += blockDim.x) {
+      ef2 lo[D], hi[D];
+#pragma unroll
+      for (int j = 0; j < D; ++j) lo[j] = P.p[j][i], hi[j] = P.p[j][i + half];
+      accumulate_pair<D>(lo, hi, s);
+    }
+    block_reduce<D>(s, red);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int q = 0; q <= D; ++q) rounds_out[(size_t)t * (D + 1) + q] = s[q];
+    const ef2 r = ch[t];
+    for (size_t i = threadIdx.x; i < half; i += blockDim.x)
+#pragma unroll
+      for (int j = 0; j < D; ++j) P.p[j][i] = ef_lerp(P.p[j][i], P.p[j][i + half], r);
+    __syncthreads();
+    len = half;
+  }
+  if (threadIdx.x < D) final_out[threadIdx.x] = P.p[threadIdx.x][0];
+}
+
+// rounds_out[t] = sum of the partials of round t (t < nrounds); round t used
+// min(SC_MAX_BLOCKS, ceil(2^(k-1-t) / SC_THREADS)) CTAs.
+template <int D>
+__global__ void sc_reduce_kernel(const ef2* __restrict__ partials, size_t stride, unsigned k,
+                                 ef2* __restrict__ rounds_out) {
+  __shared__ ef2 red[(D + 1) * 32];
+  const unsigned t = blockIdx.x;
+  const size_t half = (size_t)1 << (k - 1 - t);
+  const unsigned nb = (unsigned)min((size_t)SC_MAX_BLOCKS, (half + SC_THREADS - 1) / SC_THREADS);
+  ef2 s[D + 1];
+#pragma unroll
+  for (int q = 0; q <= D; ++q) s[q] = ef_zero();
+  const ef2* src = partials + (size_t)t * stride;
+  for (unsigned b = threadIdx.x; b < nb; b += blockDim.x)
+#pragma unroll
+    for (int q = 0; q <= D; ++q) s[q] = ef_add(s[q], src[(size_t)b * (D + 1) + q]);
+  block_reduce<D>(s, red);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q <= D; ++q) rounds_out[(size_t)t * (D + 1) + q] = s[q];
+}
+
+template <int D>
+void sumcheck_run(ef2* const* polys, unsigned k, const ef2* ch, ef2* rounds_out, ef2* final_out,
+                  ef2* partials, cudaStream_t st) {
+  Polys<D> P;
+  for (int j = 0; j < D; ++j) P.p[j] = polys[j];
+  const size_t stride = (size_t)SC_MAX_BLOCKS * (D + 1);
+  size_t len = (size_t)1 << k;
+  unsigned t = 0;
+  int fold = 0;
+  while (t < k && len > SC_TAIL_LEN) {
+    size_t half = len >> 1;
+    unsigned blocks = (unsigned)std::min<size_t>(SC_MAX_BLOCKS, cdiv(half, SC_THREADS));
+    sc_round_kernel<D><<<blocks, SC_THREADS, 0, st>>>(P, half, fold, fold ? ch + (t - 1) : ch,
+                                                      partials + (size_t)t * stride);
+    LGS_LAUNCH_CHECK();
+    len = half;
+    fold = 1;
+    ++t;
+  }
+  sc_tail_kernel<D><<<1, 1024, 0, st>>>(P, len, fold, ch, t, k, rounds_out, final_out);
+  LGS_LAUNCH_CHECK();
+  if (t > 0) {
+    sc_reduce_kernel<D><<<t, 256, 0, st>>>(partials, stride, k, rounds_out);
+    LGS_LAUNCH_CHECK();
+  }
+}
+}  // namespace
+
+size_t sumcheck_partials_elems(unsigned k, unsigned d) {
+  return (size_t)(k ? k : 1) * SC_MAX_BLOCKS * (d + 1);
+}
+
+void sumcheck_prove_dev(ef2* const* polys, unsigned d, unsigned k, const ef2* ch, ef2* rounds_out,
+                        ef2* final_out, ef2* partials, cudaStream_t st) {
+  if (k == 0) throw ShapeError("sumcheck: zero variables");
+  if (k > 40) throw ShapeError("sumcheck: too many variables");
+  switch (d) {
+    case 1: sumcheck_run<1>(polys, k, ch, rounds_out, final_out, partials, st); break;
+    case 2: sumcheck_run<2>(polys, k, ch, rounds_out, final_out, partials, st); break;
+    case 3: sumcheck_run<3>(polys, k, ch, rounds_out, final_out, partials, st); break;
+    default: throw ShapeError("sumcheck: 1 to 3 factors supported");
+  }
+}
+
+}  // namespace lgs

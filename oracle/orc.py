@@ -1,0 +1,290 @@
+"""ORACLE (test infrastructure only): ctypes access to the CPU restatement in oracle/*.hpp,
+built into oracle/_build/liborc.so by oracle/Makefile.  Imported only by tests/, the smoke
+check and bench.py's CPU-baseline leg, always as the checker or the timed CPU baseline."""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+import threading
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liborc.so"
+_lib = None
+_lock = threading.Lock()
+
+u64p = C.POINTER(C.c_uint64)
+u8p = C.POINTER(C.c_uint8)
+vp = C.c_void_p
+
+
+def build() -> Path:
+    srcs = list(HERE.glob("*.hpp")) + list(HERE.glob("*.cpp")) + [HERE / "Makefile"]
+    if LIB.exists() and LIB.stat().st_mtime >= max(s.stat().st_mtime for s in srcs):
+        return LIB
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    with _lock:
+        if _lib is None:
+            build()
+            l = C.CDLL(str(LIB))
+            sig = {
+                "orc_last_error": (C.c_char_p, []),
+                "orc_free_buf": (None, [vp]),
+                "orc_two_adic_generator": (C.c_int, [C.c_uint, u64p]),
+                "orc_bf_ops": (C.c_int, [u64p, u64p, C.c_size_t, u64p, u64p, u64p]),
+                "orc_ef_ops": (C.c_int, [u64p, u64p, C.c_size_t, u64p, u64p]),
+                "orc_blake3": (C.c_int, [u8p, C.c_size_t, u8p]),
+                "orc_dft_bf": (C.c_int, [u64p, C.c_size_t]),
+                "orc_dft_ef": (C.c_int, [u64p, C.c_size_t]),
+                "orc_mle_eval": (C.c_int, [u64p, C.c_size_t, u64p, u64p]),
+                "orc_mle_fold": (C.c_int, [u64p, C.c_size_t, u64p, C.c_size_t]),
+                "orc_new_eq": (C.c_int, [u64p, C.c_size_t, u64p]),
+                "orc_hash_columns": (C.c_int, [u64p, C.c_size_t, u64p, C.c_size_t, C.c_size_t, u64p]),
+                "orc_sumcheck_prove": (C.c_int, [u64p, C.c_size_t, C.c_size_t, u64p, C.c_size_t,
+                                                 u64p, u64p, u64p]),
+                "orc_sumcheck_verify": (C.c_int, [u64p, u64p, C.c_size_t, C.c_size_t, u64p, u64p,
+                                                  C.c_size_t]),
+                "orc_merkle_root": (C.c_int, [u8p, C.c_size_t, C.c_size_t, u8p]),
+                "orc_merkle_open": (C.c_int, [u8p, C.c_size_t, C.c_size_t, u64p, C.c_size_t,
+                                              C.POINTER(u8p), C.POINTER(C.c_size_t)]),
+                "orc_merkle_verify": (C.c_int, [u8p, u8p, C.c_size_t, u64p, C.c_size_t, u8p,
+                                                C.c_size_t, C.c_size_t]),
+                "orc_shape_ok": (C.c_int, [C.c_uint, C.c_uint]),
+                "orc_setup": (vp, [C.c_uint, C.c_uint, u64p, u8p]),
+                "orc_key_free": (None, [vp]),
+                "orc_commit": (vp, [vp, u64p, C.c_size_t, u8p]),
+                "orc_commit_free": (None, [vp]),
+                "orc_commit_codeword": (C.c_int, [vp, u64p]),
+                "orc_commit_digest": (C.c_int, [vp, u64p]),
+                "orc_prove": (C.c_int, [vp, vp, u64p, C.c_size_t, u64p, C.c_size_t, u64p,
+                                        C.c_size_t, u64p, C.POINTER(u8p), C.POINTER(C.c_size_t)]),
+                "orc_verify": (C.c_int, [u8p, C.c_uint, C.c_uint, u8p, u64p, C.c_size_t, u8p,
+                                         C.c_size_t, u64p, C.c_size_t, u64p, C.c_size_t, u64p]),
+            }
+            for name, (res, args) in sig.items():
+                fn = getattr(l, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = l
+    return _lib
+
+
+def _p64(a):
+    return a.ctypes.data_as(u64p)
+
+
+def _p8(a):
+    return a.ctypes.data_as(u8p)
+
+
+def _u64(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint64))
+
+
+def _ok(rc):
+    if rc < 0:
+        raise RuntimeError("oracle: " + (lib().orc_last_error() or b"").decode())
+    return rc
+
+
+def two_adic_generator(bits: int) -> int:
+    out = np.zeros(1, np.uint64)
+    _ok(lib().orc_two_adic_generator(bits, _p64(out)))
+    return int(out[0])
+
+
+def bf_ops(a, b):
+    a, b = _u64(a), _u64(b)
+    s, d, p = (np.zeros_like(a) for _ in range(3))
+    _ok(lib().orc_bf_ops(_p64(a), _p64(b), a.size, _p64(s), _p64(d), _p64(p)))
+    return s, d, p
+
+
+def ef_ops(a, b):
+    a, b = _u64(a).reshape(-1, 2), _u64(b).reshape(-1, 2)
+    prod, inv = np.zeros_like(a), np.zeros_like(a)
+    _ok(lib().orc_ef_ops(_p64(a), _p64(b), a.shape[0], _p64(prod), _p64(inv)))
+    return prod, inv
+
+
+def blake3(data: bytes) -> bytes:
+    buf = np.frombuffer(bytes(data) or b"\0", dtype=np.uint8).copy()
+    out = np.zeros(32, np.uint8)
+    _ok(lib().orc_blake3(_p8(buf), len(data), _p8(out)))
+    return out.tobytes()
+
+
+def dft_bf(coeffs, size: int) -> np.ndarray:
+    a = np.zeros(size, np.uint64)
+    c = _u64(coeffs)
+    a[: c.size] = c
+    _ok(lib().orc_dft_bf(_p64(a), size))
+    return a
+
+
+def dft_ef(coeffs, size: int) -> np.ndarray:
+    a = np.zeros((size, 2), np.uint64)
+    c = _u64(coeffs).reshape(-1, 2)
+    a[: c.shape[0]] = c
+    _ok(lib().orc_dft_ef(_p64(a), size))
+    return a
+
+
+def mle_eval(evals, point):
+    e = _u64(evals).reshape(-1, 2).copy()
+    p = _u64(point).reshape(-1, 2).copy()
+    out = np.zeros(2, np.uint64)
+    _ok(lib().orc_mle_eval(_p64(e), p.shape[0], _p64(p), _p64(out)))
+    return (int(out[0]), int(out[1]))
+
+
+def mle_fold(evals, point):
+    e = _u64(evals).reshape(-1, 2).copy()
+    p = _u64(point).reshape(-1, 2).copy()
+    k = e.shape[0].bit_length() - 1
+    _ok(lib().orc_mle_fold(_p64(e), k, _p64(p), p.shape[0]))
+    return e[: e.shape[0] >> p.shape[0]]
+
+
+def new_eq(point):
+    p = _u64(point).reshape(-1, 2).copy()
+    out = np.zeros((1 << p.shape[0], 2), np.uint64)
+    _ok(lib().orc_new_eq(_p64(p), p.shape[0], _p64(out)))
+    return out
+
+
+def hash_columns(A, cw):
+    A, cw = _u64(A), _u64(cw)
+    m, two_n = cw.shape
+    W = A.shape[1]
+    H = np.zeros((32, two_n), np.uint64)
+    _ok(lib().orc_hash_columns(_p64(A), W, _p64(cw), m, two_n, _p64(H)))
+    return H
+
+
+def sumcheck_prove(polys, fields):
+    ps = [_u64(p).reshape(-1, 2) for p in polys]
+    d, k = len(ps), ps[0].shape[0].bit_length() - 1
+    flat = np.ascontiguousarray(np.concatenate(ps))
+    f = _u64(fields).reshape(-1, 2).copy()
+    rounds = np.zeros((k, d + 1, 2), np.uint64)
+    finals = np.zeros((d, 2), np.uint64)
+    ch = np.zeros((k, 2), np.uint64)
+    _ok(lib().orc_sumcheck_prove(_p64(flat), d, k, _p64(f), f.shape[0], _p64(rounds),
+                                 _p64(finals), _p64(ch)))
+    return rounds, finals, ch
+
+
+def sumcheck_verify(claim, rounds, finals, fields) -> bool:
+    c = _u64(claim).reshape(2).copy()
+    r = np.ascontiguousarray(_u64(rounds))
+    f = np.ascontiguousarray(_u64(finals))
+    fl = _u64(fields).reshape(-1, 2).copy()
+    k, w = r.shape[0], r.shape[1]
+    return bool(_ok(lib().orc_sumcheck_verify(_p64(c), _p64(r), k, w - 1, _p64(f), _p64(fl),
+                                              fl.shape[0])))
+
+
+def merkle_root(leaves: np.ndarray) -> bytes:
+    lv = np.ascontiguousarray(leaves).view(np.uint8).reshape(leaves.shape[0], -1)
+    out = np.zeros(32, np.uint8)
+    _ok(lib().orc_merkle_root(_p8(lv), lv.shape[0], lv.shape[1], _p8(out)))
+    return out.tobytes()
+
+
+def merkle_open(leaves: np.ndarray, idx) -> bytes:
+    lv = np.ascontiguousarray(leaves).view(np.uint8).reshape(leaves.shape[0], -1)
+    ix = _u64(idx)
+    p = u8p()
+    n = C.c_size_t()
+    _ok(lib().orc_merkle_open(_p8(lv), lv.shape[0], lv.shape[1], _p64(ix), ix.size, C.byref(p),
+                              C.byref(n)))
+    b = C.string_at(p, n.value)
+    lib().orc_free_buf(p)
+    return b
+
+
+def merkle_verify(root: bytes, proof: bytes, idx, leaves: np.ndarray, total: int) -> bool:
+    lv = np.ascontiguousarray(leaves).view(np.uint8).reshape(len(idx), -1)
+    r = np.frombuffer(root, np.uint8).copy()
+    pb = np.frombuffer(proof or b"\0", np.uint8).copy()
+    ix = _u64(idx)
+    return bool(_ok(lib().orc_merkle_verify(_p8(r), _p8(pb), len(proof), _p64(ix), ix.size, _p8(lv),
+                                            lv.shape[1], total)))
+
+
+class Key:
+    def __init__(self, log_m: int, log_n: int, A):
+        self.A = _u64(A)
+        self.log_m, self.log_n = log_m, log_n
+        com = np.zeros(32, np.uint8)
+        h = lib().orc_setup(log_m, log_n, _p64(self.A), _p8(com))
+        if not h:
+            raise RuntimeError("oracle setup: " + lib().orc_last_error().decode())
+        self.h, self.com_a = h, com.tobytes()
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_key_free(self.h)
+            self.h = None
+
+
+class Commitment:
+    def __init__(self, key: Key, f):
+        f = _u64(f)
+        root = np.zeros(32, np.uint8)
+        h = lib().orc_commit(key.h, _p64(f), f.size, _p8(root))
+        if not h:
+            raise RuntimeError("oracle commit: " + lib().orc_last_error().decode())
+        self.h, self.root, self.key = h, root.tobytes(), key
+
+    def codeword(self):
+        m, two_n = 1 << self.key.log_m, 2 << self.key.log_n
+        out = np.zeros((m, two_n), np.uint64)
+        _ok(lib().orc_commit_codeword(self.h, _p64(out)))
+        return out
+
+    def digest(self):
+        out = np.zeros((32, 2 << self.key.log_n), np.uint64)
+        _ok(lib().orc_commit_digest(self.h, _p64(out)))
+        return out
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_commit_free(self.h)
+            self.h = None
+
+
+def prove(key: Key, cm: Commitment, z, fields, ints, cursors=(0, 0)):
+    z = _u64(z).reshape(-1, 2).copy()
+    f = _u64(fields).reshape(-1, 2).copy()
+    i = _u64(ints).copy()
+    cur = np.array(cursors, dtype=np.uint64)
+    p = u8p()
+    n = C.c_size_t()
+    _ok(lib().orc_prove(key.h, cm.h, _p64(z), z.shape[0], _p64(f), f.shape[0], _p64(i), i.size,
+                        _p64(cur), C.byref(p), C.byref(n)))
+    b = C.string_at(p, n.value)
+    lib().orc_free_buf(p)
+    return b, (int(cur[0]), int(cur[1]))
+
+
+def verify(com_a: bytes, log_m: int, log_n: int, root: bytes, z, proof: bytes, fields, ints,
+           cursors=(0, 0)) -> bool:
+    z = _u64(z).reshape(-1, 2).copy()
+    f = _u64(fields).reshape(-1, 2).copy()
+    i = _u64(ints).copy()
+    cur = np.array(cursors, dtype=np.uint64)
+    ca = np.frombuffer(com_a, np.uint8).copy()
+    rt = np.frombuffer(root, np.uint8).copy()
+    pb = np.frombuffer(proof or b"\0", np.uint8).copy()
+    rc = lib().orc_verify(_p8(ca), log_m, log_n, _p8(rt), _p64(z), z.shape[0], _p8(pb), len(proof),
+                          _p64(f), f.shape[0], _p64(i), i.size, _p64(cur))
+    return bool(_ok(rc))

@@ -1,0 +1,28 @@
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); runs the device code")
+
+
+@pytest.fixture(scope="session")
+def orc():
+    from oracle import orc as _orc
+
+    _orc.lib()
+    return _orc
+
+
+@pytest.fixture(scope="session")
+def lgs():
+    import ligesis_b200
+
+    ligesis_b200.load()
+    return ligesis_b200

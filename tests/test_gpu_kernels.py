@@ -1,0 +1,99 @@
+"""Device operations against the CPU oracle, bit-exact (integer field arithmetic): DFT, subset-sum
+hash, Merkle roots, eq tables, MLE evaluation and the product sumcheck."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import ligesis_b200 as L
+from ligesis_b200 import rng
+from tests.helpers import P
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("log_size,n_in,batch", [(1, 1, 3), (4, 8, 2), (10, 512, 4), (12, 4096, 2),
+                                                 (13, 4096, 3), (15, 16384, 2), (18, 131072, 2),
+                                                 (20, 1 << 19, 1), (14, 5, 2), (17, 1 << 17, 1)])
+def test_dft_matches_oracle(lgs, orc, log_size, n_in, batch):
+    c = rng.field_elements(1000 + log_size, batch * n_in).reshape(batch, n_in)
+    got = L.dft(c, log_size)
+    for b in range(batch):
+        assert np.array_equal(got[b], orc.dft_bf(c[b], 1 << log_size)), b
+
+
+def test_dft_reduces_noncanonical_input(lgs, orc):
+    c = np.array([P, P + 5, (1 << 64) - 1, 3], dtype=np.uint64)
+    got = L.dft(c, 3)[0]
+    want = orc.dft_bf(np.array([0, 5, (1 << 64) - 1 - P, 3], dtype=np.uint64), 8)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("m,cols", [(1, 128), (2, 256), (8, 2048), (16, 384), (128, 1024)])
+def test_subset_sum_hash_matches_oracle(lgs, orc, m, cols):
+    A = rng.field_elements(2000 + m, 32 * 64 * m).reshape(32, 64 * m)
+    cw = rng.field_elements(3000 + m, m * cols).reshape(m, cols)
+    h = L.SubsetSumHash(64 * m, a=A)
+    got = np.zeros((32, cols), dtype=np.uint64)
+    from ligesis_b200._lib import Context, check, load, ptr64
+
+    check(load().lgs_subset_sum_hash(Context.default().handle, ptr64(A), m, ptr64(cw), cols,
+                                     ptr64(got)))
+    assert np.array_equal(got, orc.hash_columns(A, cw))
+    assert h.width == 64 * m
+
+
+def test_subset_sum_hash_extremes(lgs, orc):
+    # every bit set and every limb 0xff-heavy: the largest int32 limb sums the kernel sees
+    m, cols = 128, 256
+    A = np.full((32, 64 * m), P - 1, dtype=np.uint64)
+    cw = np.full((m, cols), P - 1, dtype=np.uint64)
+    cw[:, ::2] = 0
+    from ligesis_b200._lib import Context, check, load, ptr64
+
+    got = np.zeros((32, cols), dtype=np.uint64)
+    check(load().lgs_subset_sum_hash(Context.default().handle, ptr64(A), m, ptr64(cw), cols,
+                                     ptr64(got)))
+    assert np.array_equal(got, orc.hash_columns(A, cw))
+
+
+def test_subset_sum_hash_api_on_bool_columns(lgs, orc):
+    # SubsetSumHash::hash_columns on explicit bit columns (pcs/src/subset_sum.rs:110-124)
+    width = 64
+    A = rng.field_elements(77, 32 * width).reshape(32, width)
+    bits = (rng.ints(78, 10 * width) & np.uint64(1)).astype(bool).reshape(10, width)
+    h = L.SubsetSumHash(width, a=A)
+    got = h.hash_columns(bits)
+    for j in range(10):
+        for r in range(32):
+            assert int(got[r, j]) == sum(int(A[r, i]) for i in range(width) if bits[j, i]) % P
+
+
+@pytest.mark.parametrize("nleaves,words", [(2, 1), (8, 2), (64, 16), (1024, 32), (4096, 64),
+                                           (1 << 15, 2), (256, 128), (1 << 18, 4)])
+def test_merkle_root_matches_oracle(lgs, orc, nleaves, words):
+    leaves = rng.field_elements(4000 + words, nleaves * words).reshape(nleaves, words)
+    assert L.merkle_root(leaves) == orc.merkle_root(leaves)
+
+
+@pytest.mark.parametrize("k", [1, 3, 10, 20])
+def test_new_eq_and_mle_eval_match_oracle(lgs, orc, k):
+    pt = rng.ext_elements(5000 + k, k)
+    eq = L.MlPoly.new_eq(pt).evals
+    assert np.array_equal(eq, orc.new_eq(pt))
+    ev = rng.ext_elements(5100 + k, 1 << k)
+    assert L.MlPoly(ev).eval(pt) == orc.mle_eval(ev, pt)
+    bf = rng.field_elements(5200 + k, 1 << k)
+    lifted = np.stack([bf, np.zeros_like(bf)], axis=1)
+    assert L.MlPoly(bf).eval(pt) == orc.mle_eval(lifted, pt)
+
+
+@pytest.mark.parametrize("d,k", [(1, 4), (2, 1), (2, 12), (2, 13), (3, 12), (3, 14), (2, 18),
+                                 (3, 20)])
+def test_sumcheck_matches_oracle(lgs, orc, d, k):
+    polys = [rng.ext_elements(6000 + 10 * d + j, 1 << k) for j in range(d)]
+    ch = rng.ext_elements(7000 + k, k)
+    rounds, finals = L.sumcheck_prove(polys, ch)
+    r_o, f_o, _ = orc.sumcheck_prove(polys, ch)
+    assert np.array_equal(rounds, r_o)
+    assert np.array_equal(finals, f_o)

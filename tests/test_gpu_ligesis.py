@@ -1,0 +1,149 @@
+"""LigeSIS on the GPU against the CPU oracle: commitments, intermediates and whole proofs
+byte-for-byte, both verifiers accepting, and the reference's tamper tests
+(pcs/src/ligesis.rs:808-868) through the library's verifier."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import ligesis_b200 as L
+from ligesis_b200 import proof as codec
+from ligesis_b200 import rng
+from tests.helpers import P, ligesis_inputs
+
+pytestmark = pytest.mark.gpu
+
+
+def _gpu_run(log_m, log_n, f, A, z, fields, ints):
+    pk, vk = L.Ligesis.setup_with_hash(log_m, log_n, L.SubsetSumHash(64 << log_m, a=A))
+    commit, data = L.Ligesis.commit(pk, L.MlPoly(f))
+    oracle = L.RandomOracle(0, length=8)
+    oracle.fields, oracle.ints = np.ascontiguousarray(fields), np.ascontiguousarray(ints)
+    proof = L.Ligesis.prove(pk, data, z, oracle)
+    return pk, vk, commit, data, oracle, proof
+
+
+@pytest.fixture(scope="module", params=[(3, 10), (5, 13), (6, 14)])
+def pair(request, lgs, orc):
+    log_m, log_n = request.param
+    f, A, z, fields, ints = ligesis_inputs(log_m, log_n, seed=10 * log_m + log_n)
+    pk, vk, commit, data, oracle, proof = _gpu_run(log_m, log_n, f, A, z, fields, ints)
+    key = orc.Key(log_m, log_n, A)
+    cm = orc.Commitment(key, f)
+    oproof, ocur = orc.prove(key, cm, z, fields, ints)
+    return dict(log_m=log_m, log_n=log_n, f=f, A=A, z=z, fields=fields, ints=ints, pk=pk, vk=vk,
+                commit=commit, data=data, oracle=oracle, proof=proof, key=key, cm=cm,
+                oproof=oproof, ocur=ocur)
+
+
+def test_setup_commitment_matches_oracle(pair):
+    assert pair["vk"].com_a == pair["key"].com_a
+
+
+def test_codeword_and_digest_match_oracle(pair):
+    assert np.array_equal(pair["data"].codeword(), pair["cm"].codeword())
+    assert np.array_equal(pair["data"].digest(), pair["cm"].digest())
+
+
+def test_commitment_root_matches_oracle(pair):
+    assert pair["commit"].root == pair["cm"].root
+
+
+def test_proof_bytes_match_oracle(pair):
+    got, want = pair["proof"].data, pair["oproof"]
+    if got != want:  # name the first differing field before failing
+        g, w = codec.decode(got), codec.decode(want)
+        for name in ("y", "com_a_vec", "com_i", "y4", "y5", "h_cols", "h_open"):
+            assert getattr(g, name) == getattr(w, name), name
+        for name in codec.SUMCHECK_NAMES:
+            assert g.sumchecks[name] == w.sumchecks[name], name
+        assert g.batch == w.batch, "batch"
+    assert got == want
+    assert tuple(int(c) for c in pair["oracle"].cursors) == pair["ocur"]
+
+
+def test_both_verifiers_accept(pair, orc):
+    o = pair["oracle"]
+    o.restart()
+    assert L.Ligesis.verify(pair["vk"], pair["commit"], pair["z"], pair["proof"], o)
+    assert tuple(int(c) for c in o.cursors) == pair["ocur"]
+    assert orc.verify(pair["key"].com_a, pair["log_m"], pair["log_n"], pair["commit"].root,
+                      pair["z"], pair["proof"].data, pair["fields"], pair["ints"])
+
+
+def test_claimed_value_is_the_evaluation(pair, orc):
+    lifted = np.stack([pair["f"], np.zeros_like(pair["f"])], axis=1)
+    assert pair["proof"].y == orc.mle_eval(lifted, pair["z"])
+
+
+@pytest.mark.parametrize("what", ["y", "sumcheck", "h_column", "batch_msg", "base_leaf",
+                                  "fold_value", "truncate"])
+def test_tampered_proof_is_rejected(pair, what):
+    pf = codec.decode(pair["proof"].data)
+    if what == "y":
+        pf.y = ((pf.y[0] + 1) % P, pf.y[1])
+    elif what == "sumcheck":
+        rp = pf.sumchecks["sc_hash"].round_polys
+        rp[0][0] = ((rp[0][0][0] + 1) % P, rp[0][0][1])
+    elif what == "h_column":
+        pf.h_cols[0][0] = (pf.h_cols[0][0] + 1) % P
+    elif what == "batch_msg":
+        pf.batch.reduction_msgs[1][0] = ((pf.batch.reduction_msgs[1][0][0] + 1) % P, 0)
+    elif what == "base_leaf":
+        op = pf.batch.base_bf[1]
+        k = max(op.values)
+        op.values[k][3] = (op.values[k][3] + 1) % P
+    elif what == "fold_value":
+        op = pf.batch.fold_openings[0]
+        k = min(op.values)
+        v = op.values[k][0]
+        op.values[k][0] = (v[0], (v[1] + 1) % P)
+    bad = codec.encode(pf) if what != "truncate" else pair["proof"].data[:-3]
+    o = pair["oracle"]
+    o.restart()
+    assert not L.Ligesis.verify(pair["vk"], pair["commit"], pair["z"], bad, o)
+
+
+def test_second_proof_from_advanced_cursors_matches_oracle(pair, orc):
+    """A proof made from a used oracle is identical whether made alone or after others."""
+    o = pair["oracle"]
+    o.cursors[:] = np.array(pair["ocur"], dtype=np.uint64)
+    p2 = L.Ligesis.prove(pair["pk"], pair["data"], pair["z"], o)
+    o2, cur2 = orc.prove(pair["key"], pair["cm"], pair["z"], pair["fields"], pair["ints"],
+                         pair["ocur"])
+    assert p2.data == o2
+    assert tuple(int(c) for c in o.cursors) == cur2
+
+
+def test_public_api_round_trip(lgs):
+    """Ligesis::setup/commit/prove/verify through the reference-shaped API (ligesis.rs:808-822)."""
+    g = L.SeededRng(123)
+    pk, vk = L.Ligesis.setup(3, 10, g)
+    f = L.MlPoly(g.field_elements(1 << 13))
+    z = g.ext_elements(13)
+    commit, data = L.Ligesis.commit(pk, f)
+    oracle = L.RandomOracle(g, length=2048)
+    proof = L.Ligesis.prove(pk, data, z, oracle)
+    assert proof.y == f.eval(z)
+    oracle.restart()
+    assert L.Ligesis.verify(vk, commit, z, proof, oracle)
+    assert 0 < proof.size_bytes() < len(proof.data)
+
+
+def test_oracle_exhaustion_is_reported(lgs):
+    g = L.SeededRng(5)
+    pk, vk = L.Ligesis.setup(3, 10, g)
+    commit, data = L.Ligesis.commit(pk, L.MlPoly(g.field_elements(1 << 13)))
+    oracle = L.RandomOracle(g, length=100)  # fewer than the 612 ints a proof draws
+    with pytest.raises(L.OracleExhausted):
+        L.Ligesis.prove(pk, data, g.ext_elements(13), oracle)
+    assert oracle.drawn() == (0, 0)
+
+
+def test_bad_shapes_and_lengths_are_rejected(lgs):
+    g = L.SeededRng(6)
+    with pytest.raises(L.ShapeError):
+        L.Ligesis.setup(10, 10, g)
+    pk, vk = L.Ligesis.setup(3, 10, g)
+    with pytest.raises(L.LgsError):
+        L.Ligesis.commit(pk, L.MlPoly(g.field_elements(1 << 12)))
