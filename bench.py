@@ -1,0 +1,347 @@
+"""LigeSIS commit + eval at mu = 24 on B200 (the reference's README row
+`LigeSIS 2^7 x 2^17 (mu=24)`, pcs/benches/ligesis.rs:20-60 timing commit and prove).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one `Ligesis::commit` + `Ligesis::prove` of a 2^24-evaluation polynomial arranged as
+2^7 x 2^17 (C = 32, eta = 64, s = 128 opened columns, RS rate 1/2, Basefold batched open with
+100 queries).  Inputs are seeded synthetic data (uniform Goldilocks f and A, uniform F_{p^2}
+point and oracle), the same for every step; f is 128 MiB and the codeword 256 MiB, both larger
+than the 126 MB L2, so no step starts from a warm L2.
+
+`value`   device time per step with f already in HBM (lgs_commit_device + lgs_prove; the prove
+          includes its small parameter upload and the proof read-back), in ms per proof for the
+          whole job (max over ranks / N; N > 1 runs N independent replicas).
+`e2e`     the same through the public API (`Ligesis.commit` on a pinned host f, then
+          `Ligesis.prove`), host->device copy of f and the proof read-back inside the region.
+`--impl reference`: the CPU restatement of the reference prover (single-threaded, as the
+          reference prescribes), timed on a bounded sample (mu = 22, 2^7 x 2^15) scaled to mu = 24.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+LOG_M, LOG_N = 7, 17
+MU = LOG_M + LOG_N
+SAMPLE_SHAPE = (7, 15)  # CPU sample: mu = 22, scaled by 2^(24-22)
+METRIC = "LigeSIS commit+eval ms at mu=24 (2^7 x 2^17)"
+
+
+def _config(n_gpus: int) -> dict:
+    return {
+        "workload": "LigeSIS commit+eval, mu=24 as 2^7 x 2^17, C=32, eta=64, s=128, RS rate 1/2, "
+                    "Basefold batched open (100 queries)",
+        "log_m": LOG_M, "log_n": LOG_N,
+        "l2": "inputs larger than L2 (f 128 MiB, codeword 256 MiB); no flush needed",
+        "parallelism": "replicas" if n_gpus > 1 else "single",
+    }
+
+
+def _dist():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return rank, world, local
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU baseline: the oracle (a single-threaded restatement of the reference prover)
+# ------------------------------------------------------------------------------------------------
+def cpu_sample_ms(shape=SAMPLE_SHAPE, seed: int = 1) -> tuple[float, dict]:
+    from ligesis_b200 import rng
+    from oracle import orc
+
+    lm, ln = shape
+    f = rng.field_elements(seed, 1 << (lm + ln))
+    A = rng.field_elements(seed + 1, 32 * (64 << lm)).reshape(32, 64 << lm)
+    z = rng.ext_elements(seed + 2, lm + ln)
+    g = rng.SeededRng(seed + 3)
+    fields, ints = g.ext_elements(4096), g.ints(4096)
+    key = orc.Key(lm, ln, A)
+    t0 = time.perf_counter()
+    cm = orc.Commitment(key, f)
+    t1 = time.perf_counter()
+    orc.prove(key, cm, z, fields, ints)
+    t2 = time.perf_counter()
+    scale = 2 ** (MU - (lm + ln))
+    info = {"commit_s": round(t1 - t0, 3), "prove_s": round(t2 - t1, 3), "scale": scale}
+    return (t2 - t0) * 1e3 * scale, info
+
+
+def _cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(args) -> None:
+    rank, world, _ = _dist()
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        cpu_sample_ms()
+    times, info = [], {}
+    for _ in range(args.steps):
+        ms, info = cpu_sample_ms()
+        times.append(ms)
+    ms = statistics.mean(times)
+    sample = (f"oracle commit+prove at mu=22 (2^7 x 2^15), {info['commit_s']}+{info['prove_s']} s "
+              f"per sample, scaled x{info['scale']} to mu=24 (the dominant subset-sum hash is "
+              f"linear in 2^mu); 1 thread on {_cpu_model()}")
+    line = {
+        "metric": METRIC, "value": round(ms, 1), "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 1),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (mod p)",
+        "data": "synthetic (seeded uniform Goldilocks)", "config": _config(world),
+        "impl": "reference",
+        "cpu_baseline": {"value": round(ms, 1), "unit": "ms", "cores": 1, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(ms, 1), "unit": "ms", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------------
+# clocks during the timed region
+# ------------------------------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows: list[list[str]] = []
+        self.proc = None
+        self._t = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            if self._t:
+                self._t.join(timeout=2)
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for i, nm in enumerate(names):
+                    if r[5 + i].lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------------
+# GPU arm
+# ------------------------------------------------------------------------------------------------
+def _peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"], "src": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "src": "fallback"}
+
+
+def run_ours(args) -> None:
+    import numpy as np
+    import torch
+
+    import ligesis_b200 as L
+    from ligesis_b200 import rng
+
+    rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    lib = L.load()
+    ctx = L.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=torch.device("cuda", local))
+
+    f = rng.field_elements(1 + rank, 1 << MU)
+    A = rng.field_elements(2, 32 * (64 << LOG_M)).reshape(32, 64 << LOG_M)
+    z = rng.ext_elements(3, MU)
+    g = rng.SeededRng(4)
+    fields, ints = g.ext_elements(4096), g.ints(4096)
+    pk, vk = L.Ligesis.setup_with_hash(LOG_M, LOG_N, L.SubsetSumHash(64 << LOG_M, a=A), ctx)
+    f_dev = torch.from_numpy(f.view(np.int64)).to(f"cuda:{local}")
+    f_pin = torch.from_numpy(f.view(np.int64)).pin_memory()
+    f_pin_np = f_pin.numpy().view(np.uint64)
+    oracle = L.RandomOracle(0, length=8)
+    oracle.fields, oracle.ints = fields, ints
+
+    def step_device():
+        oracle.restart()
+        commit, data = L.Ligesis.commit_device(pk, f_dev.data_ptr(), f.size)
+        proof = L.Ligesis.prove(pk, data, z, oracle)
+        return commit, proof
+
+    def step_e2e():
+        oracle.restart()
+        commit, data = L.Ligesis.commit(pk, L.MlPoly(f_pin_np))
+        proof = L.Ligesis.prove(pk, data, z, oracle)
+        return commit, proof
+
+    # warm-up; the first proof is checked by the library verifier
+    for i in range(args.warmup):
+        commit, proof = step_device()
+        if i == 0:
+            oracle.restart()
+            assert L.Ligesis.verify(vk, commit, z, proof, oracle), "warm-up proof rejected"
+
+    def timed(fn, k):
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        out = None
+        for _ in range(k):
+            out = fn()
+        ev1.record(stream)
+        torch.cuda.synchronize(local)
+        ms = ev0.elapsed_time(ev1) / k
+        if dist:
+            t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, out
+
+    launches0 = lib.lgs_launch_count()
+    L._lib.check(lib.lgs_profile(ctx.handle, 1))
+    with ClockSampler(local) as clk:
+        dev_ms, (commit, proof) = timed(step_device, args.steps)
+    launches = lib.lgs_launch_count() - launches0
+    stages = {}
+    import ctypes as C
+
+    for name in ("commit_upload", "rs_encode", "subset_sum_hash", "merkle_h", "prove_device"):
+        tot, cnt = C.c_double(), C.c_uint64()
+        L._lib.check(lib.lgs_profile_get(ctx.handle, name.encode(), C.byref(tot), C.byref(cnt)))
+        if cnt.value:
+            stages[name] = tot.value / cnt.value
+    L._lib.check(lib.lgs_profile(ctx.handle, 0))
+    e2e_ms, (commit2, proof2) = timed(step_e2e, args.steps)
+    assert commit2.root == commit.root and proof2.data == proof.data, "e2e result differs"
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    peaks = _peaks()
+    # roofline of the dominant kernel stage
+    n, two_n, W = 1 << LOG_N, 2 << LOG_N, 64 << LOG_M
+    m = 1 << LOG_M
+    hash_ops = 2.0 * 256 * W * two_n  # int8 MACs x 2 over 8 limbs x 32 rows
+    ntt_bytes = 8.0 * m * n + 8.0 * m * two_n
+    dom = max(("subset_sum_hash", "rs_encode"), key=lambda s: stages.get(s, 0.0))
+    if dom == "subset_sum_hash":
+        ach = hash_ops / (stages[dom] * 1e-3) / 1e12
+        peak = 2 * peaks["bf16_tflops"]
+        roof = {"kernel": "subset_sum_hash", "bound": "tensor", "achieved": round(ach, 1),
+                "peak": round(peak, 1), "unit": "TOP/s (int8)", "frac": round(ach / peak, 4),
+                "traffic": None,
+                "peak_src": f"2 x {peaks['src']} bf16 dense (no measured int8 peak)",
+                "algorithmic": f"{hash_ops:.3e} int8 ops per launch"}
+    else:
+        ach = ntt_bytes / (stages[dom] * 1e-3) / 1e9
+        peak = peaks["hbm_gbs"]
+        roof = {"kernel": "rs_encode", "bound": "hbm", "achieved": round(ach, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
+                "peak_src": peaks["src"] + " HBM copy",
+                "algorithmic": f"{ntt_bytes:.3e} bytes per launch"}
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        cms, info = cpu_sample_ms()
+        cpu = {"value": round(cms, 1), "unit": "ms", "cores": 1, "kind": "port",
+               "sample": f"oracle commit+prove at mu=22 (2^7 x 2^15), "
+                         f"{info['commit_s']}+{info['prove_s']} s, scaled x{info['scale']} to "
+                         f"mu=24; 1 thread on {_cpu_model()}"}
+
+    value = dev_ms / world
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dev_ms, 3),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (mod p)",
+        "data": "synthetic (seeded uniform Goldilocks)", "config": _config(world),
+        "e2e": {"value": round(e2e_ms / world, 3), "unit": "ms",
+                "h2d_bytes_per_step": int(f.nbytes), "d2h_bytes_per_step": len(proof.data) + 32},
+        "stages_ms": {k: round(v, 4) for k, v in stages.items()},
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "proof_bytes": len(proof.data), "proof_size_bytes_ref_accounting": proof.size_bytes(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

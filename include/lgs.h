@@ -81,6 +81,18 @@ lgs_status lgs_verify(unsigned log_m, unsigned log_n, const uint8_t com_a[32],
                       size_t nfields, const uint64_t* ints, size_t nints, uint64_t cursors[2],
                       int* accept);
 
+/* ---- measurement (no counterpart in the reference, whose benches use wall-clock timers,
+ * pcs/benches/ligesis.rs:27-45) ---- */
+
+/* enable != 0: record CUDA events around each device stage of later calls on this context
+ * (and clear the totals); 0: stop.  Stages: commit_upload, rs_encode, subset_sum_hash,
+ * merkle_h, prove_device. */
+lgs_status lgs_profile(lgs_ctx* ctx, int enable);
+/* Total device milliseconds and number of timed calls of one stage since lgs_profile(ctx, 1). */
+lgs_status lgs_profile_get(lgs_ctx* ctx, const char* stage, double* total_ms, uint64_t* count);
+/* Number of kernels this library has launched in this process. */
+uint64_t lgs_launch_count(void);
+
 /* ---- the individual device operations of the path (host buffers in and out) ---- */
 
 /* Radix2Dit::dft of `batch` vectors (p3-dft 0.5.3; pcs/src/ligesis.rs:231-235): in holds

@@ -1,5 +1,6 @@
 // The extern "C" boundary of liblgs.so (declared in include/lgs.h).  Every entry point catches
 // all C++ exceptions and maps them to an lgs_status; the message is kept per host thread.
+#include <atomic>
 #include <cstring>
 #include <new>
 #include <string>
@@ -21,6 +22,11 @@ int verify_host(unsigned log_m, unsigned log_n, const Hash32& com_a, const Hash3
 }  // namespace lgs
 
 using namespace lgs;
+
+namespace {
+std::atomic<uint64_t> g_launches{0};
+}
+void lgs::count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 namespace {
 thread_local std::string g_err;
@@ -215,6 +221,34 @@ lgs_status lgs_verify(unsigned log_m, unsigned log_n, const uint8_t com_a[32],
                           nints, cursors);
   });
 }
+
+// ---- measurement ----------------------------------------------------------------------------
+
+lgs_status lgs_profile(lgs_ctx* ctx, int enable) {
+  return guarded([&] {
+    need(ctx != nullptr, "lgs_profile: null context");
+    CtxDevice dg(ctx);
+    LGS_CUDA(cudaStreamSynchronize(ctx->st));
+    ctx->prof.flush();
+    ctx->prof.totals.clear();
+    ctx->prof.on = enable != 0;
+  });
+}
+
+lgs_status lgs_profile_get(lgs_ctx* ctx, const char* stage, double* total_ms, uint64_t* count) {
+  return guarded([&] {
+    need(ctx && stage && total_ms && count, "lgs_profile_get: null argument");
+    *total_ms = 0;
+    *count = 0;
+    for (auto& t : ctx->prof.totals)
+      if (t.first == stage) {
+        *total_ms = t.second.first;
+        *count = t.second.second;
+      }
+  });
+}
+
+uint64_t lgs_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 // ---- individual operations ----------------------------------------------------------------
 

@@ -32,7 +32,15 @@ struct OracleError : std::runtime_error {
       throw ::lgs::CudaError(std::string(#call) + ": " + cudaGetErrorString(e_) + " at " +  \
                              __FILE__ + ":" + std::to_string(__LINE__));                    \
   } while (0)
-#define LGS_LAUNCH_CHECK() LGS_CUDA(cudaGetLastError())
+// Every kernel launch of the library is followed by this check, which also counts it.
+#define LGS_LAUNCH_CHECK()                \
+  do {                                    \
+    LGS_CUDA(cudaGetLastError());         \
+    ::lgs::count_launch();                \
+  } while (0)
+
+// Process-wide count of kernels this library has launched (lgs_launch_count()).
+void count_launch();
 
 inline unsigned ilog2(uint64_t x) {
   unsigned k = 0;

@@ -97,18 +97,31 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
   if (cd->cw.bytes != m * two_n * 8) cd->cw.alloc(m * two_n * 8);
   if (cd->H.bytes != DIGEST_ROWS * two_n * 8) cd->H.alloc(DIGEST_ROWS * two_n * 8);
   if (cd->nodes.bytes != (2 * two_n - 1) * 32) cd->nodes.alloc((2 * two_n - 1) * 32);
-  if (f_on_device)
-    d2d(cd->f.p, f, m * n * 8, c->st);
-  else
-    h2d(cd->f.p, f, m * n * 8, c->st);
+  {
+    StageTimer t(c->prof, c->st, "commit_upload");
+    if (f_on_device)
+      d2d(cd->f.p, f, m * n * 8, c->st);
+    else
+      h2d(cd->f.p, f, m * n * 8, c->st);
+  }
   const unsigned logN = ilog2(two_n);
   u64* scr = logN > 12 ? c->arena.get<u64>(m * two_n) : nullptr;
-  ntt_batch(cd->f.as<u64>(), n, n, cd->cw.as<u64>(), two_n, logN, m, scr, c->tw.as<u64>(), c->st);
-  subset_sum_hash(pk->alimb.as<uint8_t>(), cd->cw.as<u64>(), cd->H.as<u64>(), (unsigned)m, two_n,
-                  c->st);
-  merkle_leaves_cols(cd->H.as<u64>(), DIGEST_ROWS, two_n, cd->nodes.as<u32>(), c->st);
-  merkle_build_from_leaves(cd->nodes.as<u32>(), two_n, c->st);
+  {
+    StageTimer t(c->prof, c->st, "rs_encode");
+    ntt_batch(cd->f.as<u64>(), n, n, cd->cw.as<u64>(), two_n, logN, m, scr, c->tw.as<u64>(), c->st);
+  }
+  {
+    StageTimer t(c->prof, c->st, "subset_sum_hash");
+    subset_sum_hash(pk->alimb.as<uint8_t>(), cd->cw.as<u64>(), cd->H.as<u64>(), (unsigned)m,
+                    two_n, c->st);
+  }
+  {
+    StageTimer t(c->prof, c->st, "merkle_h");
+    merkle_leaves_cols(cd->H.as<u64>(), DIGEST_ROWS, two_n, cd->nodes.as<u32>(), c->st);
+    merkle_build_from_leaves(cd->nodes.as<u32>(), two_n, c->st);
+  }
   cd->root = read_root(cd->nodes.as<u32>(), two_n, c->st);
+  c->prof.flush();
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -262,6 +275,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   bi_st.nodes = ar.get<u32>((2 * D - 1) * 8);
   u64* bi = ar.get<u64>(WS);
 
+  StageTimer t_prove(c->prof, st, "prove_device");
   // upload: params, idx
   h2d(d_prm, prm.data(), prm.size() * sizeof(ef2), st);
   h2d(d_idx, idx.data(), S * 8, st);
@@ -473,7 +487,9 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
 
   std::vector<u64> hst(sg.total);
   LGS_CUDA(cudaMemcpyAsync(hst.data(), stage, sg.total * 8, cudaMemcpyDeviceToHost, st));
+  t_prove.stop();
   LGS_CUDA(cudaStreamSynchronize(st));
+  c->prof.flush();
 
   // ---- assemble ----------------------------------------------------------------------------
   auto efat = [&](size_t off) { return ef_make(hst[off], hst[off + 1]); };

@@ -85,6 +85,55 @@ struct BasefoldDev {
   size_t node_count() const { return 2 * L - 1; }
 };
 
+// Optional per-stage device timing: CUDA events recorded on the context stream around each
+// stage, read back after the call's final synchronisation.
+struct Profiler {
+  struct Rec {
+    std::string name;
+    cudaEvent_t a, b;
+  };
+  bool on = false;
+  std::vector<Rec> pending;
+  std::vector<std::pair<std::string, std::pair<double, uint64_t>>> totals;
+  void add(const std::string& name, double ms) {
+    for (auto& t : totals)
+      if (t.first == name) {
+        t.second.first += ms;
+        t.second.second += 1;
+        return;
+      }
+    totals.push_back({name, {ms, 1}});
+  }
+  void flush() {  // call only after the stream has been synchronised
+    for (auto& r : pending) {
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) add(r.name, ms);
+      cudaEventDestroy(r.a);
+      cudaEventDestroy(r.b);
+    }
+    pending.clear();
+  }
+};
+
+struct StageTimer {
+  Profiler* p;
+  cudaStream_t st;
+  Profiler::Rec rec;
+  StageTimer(Profiler& prof, cudaStream_t s, const char* name) : p(prof.on ? &prof : nullptr), st(s) {
+    if (!p) return;
+    rec.name = name;
+    LGS_CUDA(cudaEventCreate(&rec.a));
+    LGS_CUDA(cudaEventCreate(&rec.b));
+    LGS_CUDA(cudaEventRecord(rec.a, st));
+  }
+  void stop() {
+    if (!p) return;
+    if (cudaEventRecord(rec.b, st) == cudaSuccess) p->pending.push_back(rec);
+    p = nullptr;
+  }
+  ~StageTimer() { stop(); }
+};
+
 }  // namespace lgs
 
 struct lgs_ctx {
@@ -92,6 +141,7 @@ struct lgs_ctx {
   cudaStream_t st = nullptr;
   lgs::DevMem tw;
   lgs::Arena arena;
+  lgs::Profiler prof;
   std::vector<uint8_t> host_stage;  // host copies that must outlive an async upload
   std::vector<uint8_t> proof_buf;   // the last proof returned by lgs_prove
 };
