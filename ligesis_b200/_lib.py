@@ -3,6 +3,7 @@ missing or cannot be loaded, every call raises; there is no CPU fallback."""
 from __future__ import annotations
 
 import ctypes as C
+import sys
 import threading
 from pathlib import Path
 
@@ -151,6 +152,7 @@ class Context:
 
     def __del__(self):
         try:
-            self.close()
+            if not sys.is_finalizing():  # at exit the driver tears the context down itself
+                self.close()
         except Exception:
             pass

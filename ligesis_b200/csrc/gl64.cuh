@@ -71,6 +71,18 @@ GL_HD u64 gl_shl(u64 x, unsigned s) {
   if (s == 0) return x;
   return gl_reduce(x << s, x >> (64 - s));
 }
+// x * 2^s mod p for 0 <= s < 192 (2 has order 192: 2^96 = -1).  Roots of unity of order up to
+// 64 are powers of two, so the small DFT butterflies multiply with shifts only.
+GL_HD u64 gl_mul_pow2(u64 x, unsigned s) {
+  if (s >= 96) {
+    x = gl_neg(x);
+    s -= 96;
+  }
+  if (s < 64) return gl_shl(x, s);
+  return gl_shl(gl_shl(x, s - 32), 32);
+}
+// The order-8 root the reference's generator gives: g_3 = 2^120 (checked at context creation).
+constexpr unsigned GL_LOG2_OMEGA8 = 120;
 
 struct ef2 {
   u64 c0, c1;

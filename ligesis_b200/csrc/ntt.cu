@@ -5,9 +5,10 @@
 // (pcs/src/basefold.rs:341-382).  EF ("dft_algebra") vectors are transformed coordinate-wise.
 //
 // Sizes up to 2^12 run as one shared-memory transform per CTA.  Larger sizes use the four-step
-// split N = N1 * N2: pass A does length-N1 column transforms (stride N2) and multiplies by
-// g_N^(j1*k2); pass B does length-N2 row transforms and writes X[j1 + N1*j2].  Zero-padded
-// inputs are never read.
+// split N = N1 * N2 with radix-8 Stockham column transforms (lanes walk adjacent columns, so
+// every global access is coalesced): pass A transforms the length-N1 columns k2 and writes
+// Z[k2][j1] * g_N^(j1*k2) (transposed), pass B transforms the length-N2 columns j1 of Z and
+// writes X[j1 + N1*j2].  Zero-padded inputs are never read.
 #include "kernels.cuh"
 
 namespace lgs {
@@ -51,7 +52,7 @@ __global__ void ntt_small_kernel(const u64* __restrict__ in, size_t in_stride, s
   const unsigned cnt = (unsigned)min((size_t)per_cta, batch - b0);
   for (unsigned idx = threadIdx.x; idx < cnt * N; idx += blockDim.x) {
     unsigned t = idx >> logN, e = idx & (N - 1);
-    u64 v = e < n_in ? in[(b0 + t) * in_stride + e] : 0;
+    u64 v = e < n_in ? gl_canon(in[(b0 + t) * in_stride + e]) : 0;
     sm[t * N + brev(e, logN)] = v;
   }
   __syncthreads();
@@ -62,57 +63,187 @@ __global__ void ntt_small_kernel(const u64* __restrict__ in, size_t in_stride, s
   }
 }
 
-// Pass A: CTA = TC consecutive columns k2 of one vector; transform along k1 (length N1).
-__global__ void ntt_passA_kernel(const u64* __restrict__ in, size_t in_stride, size_t n_in,
-                                 u64* __restrict__ y, unsigned logN, unsigned logN1,
-                                 unsigned logTC, const u64* __restrict__ tw) {
-  extern __shared__ u64 sm[];
-  const unsigned N1 = 1u << logN1, logN2 = logN - logN1, N2 = 1u << logN2, TC = 1u << logTC;
-  const size_t b = blockIdx.y;
-  const unsigned k2_0 = blockIdx.x << logTC;
-  const u64* src = in + b * in_stride;
-  for (unsigned idx = threadIdx.x; idx < (N1 << logTC); idx += blockDim.x) {
-    unsigned k1 = idx >> logTC, c = idx & (TC - 1);
-    size_t e = ((size_t)k1 << logN2) + k2_0 + c;
-    u64 v = e < n_in ? src[e] : 0;
-    sm[(brev(k1, logN1) << logTC) + c] = v;
-  }
-  __syncthreads();
-  smem_dit(sm, logN1, TC, 1, TC, tw);
-  u64* dst = y + b * ((size_t)1 << logN);
-  const unsigned tshift = TW_LOG - logN;
-  for (unsigned idx = threadIdx.x; idx < (N1 << logTC); idx += blockDim.x) {
-    unsigned j1 = idx >> logTC, c = idx & (TC - 1);
-    unsigned k2 = k2_0 + c;
-    u64 v = sm[idx];
-    unsigned ex = (unsigned)(((u64)j1 * k2) & (((u64)1 << logN) - 1));
-    if (ex) v = gl_mul(v, __ldg(tw + ((u64)ex << tshift)));
-    dst[((size_t)j1 << logN2) + k2] = v;
-  }
-  (void)N2;
+// ---- radix-8/4/2 Stockham column transforms ------------------------------------------------
+// Small in-register DFTs v'[q] = sum_r v[r] w_R^(rq) (natural order in and out), radix-2 DIT on
+// the bit-reversed registers.  The order-8 root is 2^120, so every twiddle inside them is a
+// shift (w_4 = 2^48, w_8^3 = 2^168).
+template <int R>
+__device__ __forceinline__ void dft_small(u64* v);
+template <>
+__device__ __forceinline__ void dft_small<2>(u64* v) {
+  u64 t = v[0];
+  v[0] = gl_add(t, v[1]);
+  v[1] = gl_sub(t, v[1]);
+}
+template <>
+__device__ __forceinline__ void dft_small<4>(u64* v) {
+  u64 b0 = gl_add(v[0], v[2]), b1 = gl_sub(v[0], v[2]);
+  u64 b2 = gl_add(v[1], v[3]), b3 = gl_sub(v[1], v[3]);
+  u64 t = gl_mul_pow2(b3, 48);
+  v[0] = gl_add(b0, b2);
+  v[2] = gl_sub(b0, b2);
+  v[1] = gl_add(b1, t);
+  v[3] = gl_sub(b1, t);
+}
+template <>
+__device__ __forceinline__ void dft_small<8>(u64* v) {
+  // bit-reversed order a = v[0,4,2,6,1,5,3,7]
+  u64 a0 = gl_add(v[0], v[4]), a1 = gl_sub(v[0], v[4]);
+  u64 a2 = gl_add(v[2], v[6]), a3 = gl_sub(v[2], v[6]);
+  u64 a4 = gl_add(v[1], v[5]), a5 = gl_sub(v[1], v[5]);
+  u64 a6 = gl_add(v[3], v[7]), a7 = gl_sub(v[3], v[7]);
+  a3 = gl_mul_pow2(a3, 48);
+  a7 = gl_mul_pow2(a7, 48);
+  u64 b0 = gl_add(a0, a2), b2 = gl_sub(a0, a2), b1 = gl_add(a1, a3), b3 = gl_sub(a1, a3);
+  u64 b4 = gl_add(a4, a6), b6 = gl_sub(a4, a6), b5 = gl_add(a5, a7), b7 = gl_sub(a5, a7);
+  b5 = gl_mul_pow2(b5, GL_LOG2_OMEGA8);
+  b6 = gl_mul_pow2(b6, (2 * GL_LOG2_OMEGA8) % 192);
+  b7 = gl_mul_pow2(b7, (3 * GL_LOG2_OMEGA8) % 192);
+  v[0] = gl_add(b0, b4);
+  v[4] = gl_sub(b0, b4);
+  v[1] = gl_add(b1, b5);
+  v[5] = gl_sub(b1, b5);
+  v[2] = gl_add(b2, b6);
+  v[6] = gl_sub(b2, b6);
+  v[3] = gl_add(b3, b7);
+  v[7] = gl_sub(b3, b7);
 }
 
-// Pass B: CTA = TR consecutive rows j1; transform along k2 (length N2, contiguous);
-// write X[j1 + N1 * j2].
-__global__ void ntt_passB_kernel(const u64* __restrict__ y, u64* __restrict__ out,
-                                 size_t out_stride, unsigned logN, unsigned logN1,
-                                 unsigned logTR, const u64* __restrict__ tw) {
-  extern __shared__ u64 sm[];
-  const unsigned logN2 = logN - logN1, N2 = 1u << logN2, TR = 1u << logTR;
-  const unsigned pitch = N2 + 1;
-  const size_t b = blockIdx.y;
-  const unsigned j1_0 = blockIdx.x << logTR;
-  const u64* src = y + b * ((size_t)1 << logN) + ((size_t)j1_0 << logN2);
-  for (unsigned idx = threadIdx.x; idx < (TR << logN2); idx += blockDim.x) {
-    unsigned r = idx >> logN2, k2 = idx & (N2 - 1);
-    sm[r * pitch + brev(k2, logN2)] = src[idx];
+template <int LOGL>
+struct ColCfg {
+  static constexpr int L = 1 << LOGL;
+  static constexpr int C = (4096 >> LOGL) < 1 ? 1 : ((4096 >> LOGL) > 16 ? 16 : (4096 >> LOGL));
+  static constexpr int T = (C * L / 8) < 32 ? 32 : (C * L / 8);
+  static constexpr int R0 = LOGL >= 3 ? 8 : (LOGL == 2 ? 4 : 2);
+  static constexpr size_t SMEM = (size_t)L * (C + 2) * 8;
+};
+
+// One Stockham stage of radix R over C columns of length L in shared memory (pitch C), or from
+// global memory for the first stage.  Each thread owns 8 values (8 / R work items).  The stage
+// reads everything it needs into registers, the CTA synchronises, then it writes: the buffer is
+// updated in place.  Work item w -> column c = w % C, j = w / C; Stockham DIT: inputs at
+// j + r L/R, twiddle w_L^(r (j mod Ns) L/(Ns R)), outputs at (j/Ns) Ns R + j mod Ns + r Ns.
+template <int LOGL, int R>
+__device__ __forceinline__ void col_stage(u64* s, const u64* twL, unsigned Ns, u64 (&v)[8],
+                                          bool from_global, const u64* __restrict__ gsrc,
+                                          size_t ld_in, size_t n_valid, unsigned c0,
+                                          bool last_padded) {
+  constexpr int L = ColCfg<LOGL>::L, C = ColCfg<LOGL>::C, T = ColCfg<LOGL>::T;
+  constexpr int ITEMS = 8 / R;
+  constexpr int NW = C * L / R;
+#pragma unroll
+  for (int it = 0; it < ITEMS; ++it) {
+    const unsigned w = threadIdx.x + it * T;
+    if (w < NW) {
+      const unsigned c = w % C, j = w / C;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const unsigned row = j + r * (L / R);
+        u64 x;
+        if (from_global) {
+          size_t e = (size_t)row * ld_in + c0 + c;
+          x = e < n_valid ? gl_canon(__ldg(gsrc + e)) : 0;
+        } else {
+          x = s[row * C + c];
+        }
+        v[it * R + r] = x;
+      }
+      if (Ns > 1) {
+        const unsigned k = j % Ns, step = k * (L / (Ns * R));
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[it * R + r] = gl_mul(v[it * R + r], twL[r * step]);
+      }
+      dft_small<R>(&v[it * R]);
+    }
   }
   __syncthreads();
-  smem_dit(sm, logN2, TR, pitch, 1, tw);
-  u64* dst = out + b * out_stride;
-  for (unsigned idx = threadIdx.x; idx < (TR << logN2); idx += blockDim.x) {
-    unsigned r = idx & (TR - 1), j2 = idx >> logTR;
-    dst[j1_0 + r + ((size_t)j2 << logN1)] = sm[r * pitch + j2];
+  const unsigned pitch = last_padded ? C + 1 : C;
+#pragma unroll
+  for (int it = 0; it < ITEMS; ++it) {
+    const unsigned w = threadIdx.x + it * T;
+    if (w < NW) {
+      const unsigned c = w % C, j = w / C;
+      const unsigned k = j % Ns, idxD = (j / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) s[(idxD + r * Ns) * pitch + c] = v[it * R + r];
+    }
+  }
+  __syncthreads();
+}
+
+// Transform C consecutive columns (c0 ..) of a row-major matrix (row stride ld_in, L rows,
+// entries at or beyond n_valid read as zero) of vector blockIdx.y.
+// TRANSPOSED: out[b*obs + (c0+c)*L + j] = X_c[j] * w_N^(j (c0+c))   (four-step pass A)
+// otherwise:  out[b*obs + j*ld_out + c0 + c] = X_c[j]                (four-step pass B)
+template <int LOGL, bool TRANSPOSED>
+__global__ void __launch_bounds__(ColCfg<LOGL>::T)
+    ntt_col_kernel(const u64* __restrict__ in, size_t ibs, size_t ld_in, size_t n_valid,
+                   u64* __restrict__ out, size_t obs, size_t ld_out, unsigned logN,
+                   const u64* __restrict__ tw) {
+  constexpr int L = ColCfg<LOGL>::L, C = ColCfg<LOGL>::C, T = ColCfg<LOGL>::T;
+  extern __shared__ u64 sm[];
+  u64* twL = sm;
+  u64* s = sm + L;
+  const size_t b = blockIdx.y;
+  const unsigned c0 = blockIdx.x * C;
+  for (unsigned e = threadIdx.x; e < (unsigned)L; e += T) twL[e] = __ldg(tw + ((size_t)e << (TW_LOG - LOGL)));
+  __syncthreads();
+  const u64* src = in + b * ibs;
+  u64 v[8];
+  constexpr int S8 = LOGL / 3, REM = LOGL % 3;
+  constexpr int NST = S8 + (REM ? 1 : 0);
+  unsigned Ns = 1;
+  int st = 0;
+#pragma unroll
+  for (int q = 0; q < S8; ++q, ++st) {
+    col_stage<LOGL, 8>(s, twL, Ns, v, st == 0, src, ld_in, n_valid, c0, TRANSPOSED && st == NST - 1);
+    Ns *= 8;
+  }
+  if (REM == 2) col_stage<LOGL, 4>(s, twL, Ns, v, st == 0, src, ld_in, n_valid, c0, TRANSPOSED);
+  if (REM == 1) col_stage<LOGL, 2>(s, twL, Ns, v, st == 0, src, ld_in, n_valid, c0, TRANSPOSED);
+  u64* dst = out + b * obs;
+  if (TRANSPOSED) {
+    const unsigned shift = TW_LOG - logN;
+    const size_t mask = ((size_t)1 << logN) - 1;
+    for (unsigned idx = threadIdx.x; idx < (unsigned)(C * L); idx += T) {
+      const unsigned j = idx % L, c = idx / L;
+      u64 x = s[j * (C + 1) + c];
+      const size_t e = ((size_t)j * (c0 + c)) & mask;
+      if (e) x = gl_mul(x, __ldg(tw + (e << shift)));
+      dst[(size_t)(c0 + c) * L + j] = x;
+    }
+  } else {
+    for (unsigned idx = threadIdx.x; idx < (unsigned)(C * L); idx += T) {
+      const unsigned c = idx % C, j = idx / C;
+      dst[(size_t)j * ld_out + c0 + c] = s[j * C + c];
+    }
+  }
+}
+
+template <int LOGL, bool TR>
+void launch_col(const u64* in, size_t ibs, size_t ld_in, size_t n_valid, u64* out, size_t obs,
+                size_t ld_out, unsigned logN, size_t ncols, size_t batch, const u64* tw,
+                cudaStream_t st) {
+  using Cfg = ColCfg<LOGL>;
+  if (ncols % Cfg::C) throw ShapeError("ntt: column count not a multiple of the tile");
+  auto k = ntt_col_kernel<LOGL, TR>;
+  LGS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM));
+  dim3 grid((unsigned)(ncols / Cfg::C), (unsigned)batch);
+  k<<<grid, Cfg::T, Cfg::SMEM, st>>>(in, ibs, ld_in, n_valid, out, obs, ld_out, logN, tw);
+  LGS_LAUNCH_CHECK();
+}
+
+template <bool TR>
+void launch_col_dispatch(unsigned logL, const u64* in, size_t ibs, size_t ld_in, size_t n_valid,
+                         u64* out, size_t obs, size_t ld_out, unsigned logN, size_t ncols,
+                         size_t batch, const u64* tw, cudaStream_t st) {
+  switch (logL) {
+#define LGS_COL_CASE(K) \
+  case K: launch_col<K, TR>(in, ibs, ld_in, n_valid, out, obs, ld_out, logN, ncols, batch, tw, st); break;
+    LGS_COL_CASE(3) LGS_COL_CASE(4) LGS_COL_CASE(5) LGS_COL_CASE(6) LGS_COL_CASE(7)
+    LGS_COL_CASE(8) LGS_COL_CASE(9) LGS_COL_CASE(10) LGS_COL_CASE(11)
+#undef LGS_COL_CASE
+    default: throw ShapeError("ntt: unsupported sub-transform size");
   }
 }
 
@@ -145,18 +276,13 @@ void ntt_batch(const u64* in, size_t in_stride, size_t n_in, u64* out, size_t ou
     return;
   }
   if (!scratch) throw std::runtime_error("ntt_batch: scratch required above 2^12");
-  unsigned logN1 = (logN + 1) / 2, logN2 = logN - logN1;
-  unsigned logTC = logN1 >= 12 ? 0 : std::min(12 - logN1, logN2);
-  unsigned logTR = logN2 >= 12 ? 0 : std::min(12 - logN2, logN1);
-  if (logTR > 5) logTR = 5;
-  size_t smA = ((size_t)1 << (logN1 + logTC)) * 8;
-  size_t smB = ((size_t)(((size_t)1 << logN2) + 1) << logTR) * 8;  // both <= 33 KB
-  dim3 gA((unsigned)(((size_t)1 << logN2) >> logTC), (unsigned)batch);
-  ntt_passA_kernel<<<gA, 256, smA, st>>>(in, in_stride, n_in, scratch, logN, logN1, logTC, tw);
-  LGS_LAUNCH_CHECK();
-  dim3 gB((unsigned)(((size_t)1 << logN1) >> logTR), (unsigned)batch);
-  ntt_passB_kernel<<<gB, 256, smB, st>>>(scratch, out, out_stride, logN, logN1, logTR, tw);
-  LGS_LAUNCH_CHECK();
+  if (logN > 22) throw ShapeError("ntt: transforms above 2^22 are not supported");
+  // four-step: x[k1 N2 + k2]; pass A transforms columns k2 (length N1) into Z[k2][j1] with the
+  // twiddle w_N^(j1 k2); pass B transforms columns j1 of Z (length N2) into X[j1 + N1 j2].
+  const unsigned logN1 = (logN + 1) / 2, logN2 = logN - logN1;
+  const size_t N1 = (size_t)1 << logN1, N2 = (size_t)1 << logN2;
+  launch_col_dispatch<true>(logN1, in, in_stride, N2, n_in, scratch, N, N1, logN, N2, batch, tw, st);
+  launch_col_dispatch<false>(logN2, scratch, N, N1, N, out, out_stride, N1, logN, N1, batch, tw, st);
 }
 
 // out[c][r] = in[r][c] for a rows x cols matrix of u64, `batch` matrices back to back.

@@ -56,7 +56,13 @@ void ctx_init(lgs_ctx* c, int device) {
   c->device = device;
   LGS_CUDA(cudaSetDevice(device));
   LGS_CUDA(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
-  c->tw.alloc(((size_t)1 << TW_LOG) * sizeof(u64));
+  // Keep freed pool memory cached so per-proof buffers are recycled without driver calls.
+  cudaMemPool_t pool;
+  LGS_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+  uint64_t thresh = UINT64_MAX;
+  LGS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thresh));
+  c->arena.st = c->st;
+  c->tw.alloc(((size_t)1 << TW_LOG) * sizeof(u64), c->st);
   build_twiddles(c->tw.as<u64>(), c->st);
   LGS_CUDA(cudaStreamSynchronize(c->st));
 }
@@ -68,16 +74,16 @@ void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lg
   pk->shape = s;
   const size_t W = s.W(), len = (size_t)DIGEST_ROWS * W;
   c->arena.begin();
-  pk->A.alloc(len * 8);
+  pk->A.alloc(len * 8, c->st);
   std::vector<u64> canon(A_host, A_host + len);
   for (auto& x : canon) x = gl_canon(x);
   h2d(pk->A.p, canon.data(), len * 8, c->st);
-  pk->alimb.alloc(len * 8);
+  pk->alimb.alloc(len * 8, c->st);
   alimb_from_a(pk->A.as<u64>(), pk->alimb.as<uint8_t>(), W, c->st);
   const unsigned li = s.li(s.na());
   const size_t L = (len >> li) << CODE_RATE;
-  pk->a_codes.alloc(L * ((size_t)1 << li) * 8);
-  pk->a_nodes.alloc((2 * L - 1) * 32);
+  pk->a_codes.alloc(L * ((size_t)1 << li) * 8, c->st);
+  pk->a_nodes.alloc((2 * L - 1) * 32, c->st);
   pk->a_state.codes = pk->a_codes.as<u64>();
   pk->a_state.nodes = pk->a_nodes.as<u32>();
   bf_commit(c, pk->A.as<u64>(), 0, len, li, &pk->a_state);
@@ -93,10 +99,10 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
   if (two_n % 128) throw ShapeError("commit: 2n must be a multiple of 128");
   cd->shape = s;
   c->arena.begin();
-  if (cd->f.bytes != m * n * 8) cd->f.alloc(m * n * 8);
-  if (cd->cw.bytes != m * two_n * 8) cd->cw.alloc(m * two_n * 8);
-  if (cd->H.bytes != DIGEST_ROWS * two_n * 8) cd->H.alloc(DIGEST_ROWS * two_n * 8);
-  if (cd->nodes.bytes != (2 * two_n - 1) * 32) cd->nodes.alloc((2 * two_n - 1) * 32);
+  if (cd->f.bytes != m * n * 8) cd->f.alloc(m * n * 8, c->st);
+  if (cd->cw.bytes != m * two_n * 8) cd->cw.alloc(m * two_n * 8, c->st);
+  if (cd->H.bytes != DIGEST_ROWS * two_n * 8) cd->H.alloc(DIGEST_ROWS * two_n * 8, c->st);
+  if (cd->nodes.bytes != (2 * two_n - 1) * 32) cd->nodes.alloc((2 * two_n - 1) * 32, c->st);
   {
     StageTimer t(c->prof, c->st, "commit_upload");
     if (f_on_device)

@@ -11,28 +11,33 @@
 
 namespace lgs {
 
+// Device buffer from the device's stream-ordered memory pool (cudaMallocAsync on the owning
+// context's stream).  The pool keeps freed memory cached (the context raises its release
+// threshold), so a commitment allocated and freed per proof costs no cudaMalloc / device sync.
 struct DevMem {
   void* p = nullptr;
   size_t bytes = 0;
+  cudaStream_t st = nullptr;
   DevMem() = default;
-  explicit DevMem(size_t b) { alloc(b); }
-  void alloc(size_t b) {
+  DevMem(size_t b, cudaStream_t s) { alloc(b, s); }
+  void alloc(size_t b, cudaStream_t s) {
     release();
-    if (b) LGS_CUDA(cudaMalloc(&p, b));
+    st = s;
+    if (b) LGS_CUDA(cudaMallocAsync(&p, b, st));
     bytes = b;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, st);
     p = nullptr;
     bytes = 0;
   }
   ~DevMem() { release(); }
   DevMem(const DevMem&) = delete;
   DevMem& operator=(const DevMem&) = delete;
-  DevMem(DevMem&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr, o.bytes = 0; }
+  DevMem(DevMem&& o) noexcept : p(o.p), bytes(o.bytes), st(o.st) { o.p = nullptr, o.bytes = 0; }
   DevMem& operator=(DevMem&& o) noexcept {
     release();
-    p = o.p, bytes = o.bytes;
+    p = o.p, bytes = o.bytes, st = o.st;
     o.p = nullptr, o.bytes = 0;
     return *this;
   }
@@ -43,19 +48,19 @@ struct DevMem {
 };
 
 // Bump allocator for per-call device scratch.  A call that outgrows the buffer takes extra
-// allocations; the next call starts from one buffer of the previous peak size, so steady-state
-// calls of one shape allocate nothing.
+// pool allocations; the next call starts from one buffer of the largest size seen, so
+// steady-state calls allocate nothing.
 struct Arena {
   DevMem mem;
   std::vector<DevMem> overflow;
-  size_t off = 0, peak = 0;
+  size_t off = 0, hwm = 0;
+  cudaStream_t st = nullptr;
   void begin() {
-    if (!overflow.empty() || peak > mem.bytes) {
+    if (!overflow.empty() || hwm > mem.bytes) {
       overflow.clear();
-      mem.alloc(peak + (peak >> 4));
+      mem.alloc(hwm + (hwm >> 4), st);
     }
     off = 0;
-    peak = 0;
   }
   template <class T>
   T* get(size_t count) {
@@ -65,11 +70,11 @@ struct Arena {
     if (off + b <= mem.bytes) {
       r = (T*)((char*)mem.p + off);
     } else {
-      overflow.emplace_back(b);
+      overflow.emplace_back(b, st);
       r = overflow.back().as<T>();
     }
     off += b;
-    peak = std::max(peak, off);
+    hwm = std::max(hwm, off);
     return r;
   }
 };

@@ -11,6 +11,7 @@ pairs or (k, 2) uint64 arrays.  Points are low-bit-first as in the reference.
 from __future__ import annotations
 
 import ctypes as C
+import sys
 from dataclasses import dataclass
 
 import numpy as np
@@ -190,9 +191,9 @@ class ProvingKey:
 
     def __del__(self):
         try:
-            if self.handle:
+            if self.handle and not sys.is_finalizing():
                 load().lgs_pk_free(self.handle)
-                self.handle = None
+            self.handle = None
         except Exception:
             pass
 
@@ -223,9 +224,9 @@ class CommitData:
 
     def __del__(self):
         try:
-            if self.handle:
+            if self.handle and not sys.is_finalizing():
                 load().lgs_commit_data_free(self.handle)
-                self.handle = None
+            self.handle = None
         except Exception:
             pass
 
