@@ -45,6 +45,8 @@ lgs_status guarded(F&& f) {
     return fail(LGS_ERR_BAD_SHAPE, e.what());
   } catch (const OracleError& e) {
     return fail(LGS_ERR_ORACLE_EXHAUSTED, e.what());
+  } catch (const DeviceTimeout& e) {
+    return fail(LGS_ERR_DEVICE_TIMEOUT, e.what());
   } catch (const CudaError& e) {
     std::string m = e.what();
     if (m.find("out of memory") != std::string::npos) return fail(LGS_ERR_OOM, m);
@@ -277,23 +279,35 @@ lgs_status lgs_subset_sum_hash(lgs_ctx* ctx, const uint64_t* A, size_t m, const 
                                size_t cols, uint64_t* H) {
   return guarded([&] {
     need(ctx && A && cw && H, "lgs_subset_sum_hash: null argument");
-    need(m >= 1 && cols >= 1 && cols % 128 == 0, "lgs_subset_sum_hash: cols must be a multiple of 128");
+    need(m >= 1 && m <= 8192 && cols >= 1, "lgs_subset_sum_hash: 1 <= m <= 8192, cols >= 1");
     CtxDevice dg(ctx);
-    const size_t W = 64 * m;
+    const size_t W = 64 * m, cp = (cols + 255) / 256 * 256;  // kernel tile: 256 columns
     ctx->arena.begin();
     u64* dA = ctx->arena.get<u64>(DIGEST_ROWS * W);
     uint8_t* dL = ctx->arena.get<uint8_t>(DIGEST_ROWS * W * 8);
-    u64* dC = ctx->arena.get<u64>(m * cols);
-    u64* dH = ctx->arena.get<u64>(DIGEST_ROWS * cols);
+    u64* dC = ctx->arena.get<u64>(m * cp);
+    u64* dH = ctx->arena.get<u64>(DIGEST_ROWS * cp);
+    u32* dN = ctx->arena.get<u32>(cp * 8);
     std::vector<u64> a(A, A + DIGEST_ROWS * W), c(cw, cw + m * cols);
     for (auto& x : a) x = gl_canon(x);
     for (auto& x : c) x = gl_canon(x);
     LGS_CUDA(cudaMemcpyAsync(dA, a.data(), a.size() * 8, cudaMemcpyHostToDevice, ctx->st));
-    LGS_CUDA(cudaMemcpyAsync(dC, c.data(), c.size() * 8, cudaMemcpyHostToDevice, ctx->st));
+    LGS_CUDA(cudaMemsetAsync(dC, 0, m * cp * 8, ctx->st));
+    LGS_CUDA(cudaMemcpy2DAsync(dC, cp * 8, c.data(), cols * 8, cols * 8, m,
+                               cudaMemcpyHostToDevice, ctx->st));
     alimb_from_a(dA, dL, W, ctx->st);
-    subset_sum_hash(dL, dC, dH, (unsigned)m, cols, ctx->st);
-    LGS_CUDA(cudaMemcpyAsync(H, dH, DIGEST_ROWS * cols * 8, cudaMemcpyDeviceToHost, ctx->st));
+    alignas(64) unsigned char tmap[128];
+    make_alimb_tmap(dL, W, tmap);
+    subset_sum_hash_tc(tmap, dC, dH, dN, (unsigned)m, cp, ctx->err.as<int>(), ctx->st);
+    LGS_CUDA(cudaMemcpy2DAsync(H, cols * 8, dH, cp * 8, cols * 8, DIGEST_ROWS,
+                               cudaMemcpyDeviceToHost, ctx->st));
+    int err = 0;
+    LGS_CUDA(cudaMemcpyAsync(&err, ctx->err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
     LGS_CUDA(cudaStreamSynchronize(ctx->st));
+    if (err) {
+      LGS_CUDA(cudaMemsetAsync(ctx->err.p, 0, sizeof(int), ctx->st));
+      throw DeviceTimeout("subset-sum hash: a bounded device wait gave up");
+    }
   });
 }
 

@@ -24,6 +24,9 @@ struct ShapeError : std::runtime_error {
 struct OracleError : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
+struct DeviceTimeout : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
 
 #define LGS_CUDA(call)                                                                      \
   do {                                                                                      \

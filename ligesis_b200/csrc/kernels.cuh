@@ -18,16 +18,17 @@ void ntt_batch(const u64* in, size_t in_stride, size_t n_in, u64* out, size_t ou
 void transpose_u64(const u64* in, u64* out, size_t rows, size_t cols, size_t batch,
                    cudaStream_t st);
 
-// hash_mma.cu
+// hash_tc.cu (tcgen05): also writes the Merkle leaf hashes of H's columns into `leaves`.
 void alimb_from_a(const u64* A, uint8_t* alimb, size_t W, cudaStream_t st);
-void subset_sum_hash(const uint8_t* alimb, const u64* cw, u64* H, unsigned m, size_t two_n,
-                     cudaStream_t st);
+void make_alimb_tmap(const uint8_t* alimb, size_t W, void* tmap_out);
+size_t tensor_map_bytes();
+void subset_sum_hash_tc(const void* tmap, const u64* cw, u64* H, u32* leaves, unsigned m,
+                        size_t two_n, int* err, cudaStream_t st);
 
 // merkle.cu
 size_t merkle_node_count(size_t nleaves);
 size_t merkle_layer_offset(size_t nleaves, unsigned layer);
 void merkle_build_from_leaves(u32* nodes, size_t nleaves, cudaStream_t st);
-void merkle_leaves_cols(const u64* H, unsigned rows, size_t ncols, u32* nodes, cudaStream_t st);
 void merkle_leaves_contig(const u64* data, unsigned words, size_t nleaves, u32* nodes,
                           cudaStream_t st);
 void gather_u64(const u64* src, const uint64_t* idx, size_t count, unsigned words, u64* dst,

@@ -8,32 +8,6 @@
 
 namespace lgs {
 
-// Leaf j is the C-row column (H[0][j], ..., H[rows-1][j]) of a row-major rows x ncols matrix.
-__global__ void leaf_hash_cols_kernel(const u64* __restrict__ H, unsigned rows, size_t ncols,
-                                      u32* __restrict__ out) {
-  size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= ncols) return;
-  u32 cv[8];
-  b3_init(cv);
-  const unsigned len = rows * 8;
-  const unsigned nblocks = (len + 63) / 64;
-  for (unsigned b = 0; b < nblocks; ++b) {
-    u32 blk[16];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      unsigned r = b * 8 + q;
-      u64 v = r < rows ? H[(size_t)r * ncols + j] : 0;
-      blk[2 * q] = (u32)v;
-      blk[2 * q + 1] = (u32)(v >> 32);
-    }
-    unsigned bl = len - b * 64 < 64 ? len - b * 64 : 64;
-    u32 flags = (b == 0 ? B3_CHUNK_START : 0) | (b + 1 == nblocks ? (B3_CHUNK_END | B3_ROOT) : 0);
-    b3_compress(cv, blk, bl, flags);
-  }
-#pragma unroll
-  for (int q = 0; q < 8; ++q) out[j * 8 + q] = cv[q];
-}
-
 // Leaf p is the `words` consecutive u64 starting at data[p * words] (leaf-major layouts).
 __global__ void leaf_hash_contig_kernel(const u64* __restrict__ data, unsigned words,
                                         size_t nleaves, u32* __restrict__ out) {
@@ -141,10 +115,6 @@ void merkle_build_from_leaves(u32* nodes, size_t nleaves, cudaStream_t st) {
   }
 }
 
-void merkle_leaves_cols(const u64* H, unsigned rows, size_t ncols, u32* nodes, cudaStream_t st) {
-  leaf_hash_cols_kernel<<<cdiv(ncols, 128), 128, 0, st>>>(H, rows, ncols, nodes);
-  LGS_LAUNCH_CHECK();
-}
 void merkle_leaves_contig(const u64* data, unsigned words, size_t nleaves, u32* nodes,
                           cudaStream_t st) {
   if (words * 8 > 1024) throw ShapeError("merkle: leaf larger than one blake3 chunk");

@@ -63,6 +63,10 @@ void ctx_init(lgs_ctx* c, int device) {
   LGS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thresh));
   c->arena.st = c->st;
   c->tw.alloc(((size_t)1 << TW_LOG) * sizeof(u64), c->st);
+  c->err.alloc(sizeof(int), c->st);
+  LGS_CUDA(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->st));
+  if (tensor_map_bytes() > sizeof(((lgs_pk*)nullptr)->tmap))
+    throw std::runtime_error("tensor map larger than its slot");
   build_twiddles(c->tw.as<u64>(), c->st);
   LGS_CUDA(cudaStreamSynchronize(c->st));
 }
@@ -80,6 +84,7 @@ void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lg
   h2d(pk->A.p, canon.data(), len * 8, c->st);
   pk->alimb.alloc(len * 8, c->st);
   alimb_from_a(pk->A.as<u64>(), pk->alimb.as<uint8_t>(), W, c->st);
+  make_alimb_tmap(pk->alimb.as<uint8_t>(), W, pk->tmap);
   const unsigned li = s.li(s.na());
   const size_t L = (len >> li) << CODE_RATE;
   pk->a_codes.alloc(L * ((size_t)1 << li) * 8, c->st);
@@ -117,17 +122,23 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
     ntt_batch(cd->f.as<u64>(), n, n, cd->cw.as<u64>(), two_n, logN, m, scr, c->tw.as<u64>(), c->st);
   }
   {
-    StageTimer t(c->prof, c->st, "subset_sum_hash");
-    subset_sum_hash(pk->alimb.as<uint8_t>(), cd->cw.as<u64>(), cd->H.as<u64>(), (unsigned)m,
-                    two_n, c->st);
+    StageTimer t(c->prof, c->st, "subset_sum_hash");  // H and its Merkle leaf hashes
+    subset_sum_hash_tc(pk->tmap, cd->cw.as<u64>(), cd->H.as<u64>(), cd->nodes.as<u32>(),
+                       (unsigned)m, two_n, c->err.as<int>(), c->st);
   }
   {
     StageTimer t(c->prof, c->st, "merkle_h");
-    merkle_leaves_cols(cd->H.as<u64>(), DIGEST_ROWS, two_n, cd->nodes.as<u32>(), c->st);
     merkle_build_from_leaves(cd->nodes.as<u32>(), two_n, c->st);
   }
+  int err = 0;
+  LGS_CUDA(cudaMemcpyAsync(&err, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   cd->root = read_root(cd->nodes.as<u32>(), two_n, c->st);
   c->prof.flush();
+  if (err) {
+    LGS_CUDA(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->st));
+    throw DeviceTimeout("subset-sum hash: a bounded device wait gave up (code " +
+                        std::to_string(err) + ")");
+  }
 }
 
 // ---------------------------------------------------------------------------------------------

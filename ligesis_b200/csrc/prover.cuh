@@ -147,6 +147,7 @@ struct lgs_ctx {
   lgs::DevMem tw;
   lgs::Arena arena;
   lgs::Profiler prof;
+  lgs::DevMem err;  // device error word of bounded-wait kernels (0 = ok)
   std::vector<uint8_t> host_stage;  // host copies that must outlive an async upload
   std::vector<uint8_t> proof_buf;   // the last proof returned by lgs_prove
 };
@@ -155,6 +156,7 @@ struct lgs_pk {
   lgs::Shape shape;
   lgs::DevMem A;      // 32 x W canonical u64, row-major (the flat A-bar of subset_sum.rs:73-79)
   lgs::DevMem alimb;  // 256 x W bytes: byte l of A[r][k] at row 8r + l
+  alignas(64) unsigned char tmap[128];  // TMA descriptor of alimb (CUtensorMap)
   lgs::DevMem a_codes, a_nodes;
   lgs::BasefoldDev a_state;
   lgs::Hash32 com_a;
