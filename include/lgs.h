@@ -120,6 +120,21 @@ lgs_status lgs_mle_eval(lgs_ctx* ctx, const uint64_t* evals, unsigned k, const u
 /* MlPoly::new_eq (utils/src/poly.rs:44-53): 2^k EF. */
 lgs_status lgs_new_eq(lgs_ctx* ctx, const uint64_t* point, unsigned k, uint64_t* out);
 
+/* ---- allocation-free variant (no counterpart in the reference) ----
+ * The product sumcheck prover (the same computation as lgs_sumcheck_prove) for callers that
+ * must not allocate device memory: processes whose HBM is owned by another allocator, and
+ * serving loops that cannot afford cudaMalloc's device-wide synchronisation.  All pointers are
+ * device pointers on the current device; polys holds d factors of 2^k EF, factor-major,
+ * canonical (< p), and is only read; the work is enqueued on `stream` (a cudaStream_t, NULL for
+ * the legacy default stream) and the call returns without waiting for it.  Limits: 1 <= d <= 3,
+ * 1 <= k <= 16, else LGS_ERR_BAD_SHAPE.  The working storage is a fixed 3.3 MiB device array
+ * that every GPU loading the library holds until exit; the first call on a device looks up its
+ * address (make that call before any stream capture); calls that overlap on the GPU race on it.
+ * It allocates nothing: no cudaMalloc, cudaFree or allocating library call. */
+lgs_status lgs_sumcheck_prove_noalloc(const uint64_t* polys_dev, unsigned d, unsigned k,
+                                      const uint64_t* challenges_dev, uint64_t* rounds_out_dev,
+                                      uint64_t* finals_out_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -71,6 +71,7 @@ _SIGS = {
     "lgs_sumcheck_prove": (C.c_int, [vp, u64p, C.c_uint, C.c_uint, u64p, u64p, u64p]),
     "lgs_mle_eval": (C.c_int, [vp, u64p, C.c_uint, u64p, u64p]),
     "lgs_new_eq": (C.c_int, [vp, u64p, C.c_uint, u64p]),
+    "lgs_sumcheck_prove_noalloc": (C.c_int, [vp, C.c_uint, C.c_uint, vp, vp, vp, vp]),
 }
 
 

@@ -9,6 +9,7 @@
 #include "prover.cuh"
 
 namespace lgs {
+lgs_status set_error(lgs_status s, const std::string& msg);
 void ctx_init(lgs_ctx* c, int device);
 void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lgs_pk* pk);
 void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device, lgs_commit_data* cd);
@@ -62,6 +63,11 @@ lgs_status guarded(F&& f) {
   }
 }
 
+}  // namespace
+
+lgs_status lgs::set_error(lgs_status s, const std::string& msg) { return fail(s, msg); }
+
+namespace {
 void need(bool c, const char* what) {
   if (!c) throw std::invalid_argument(what);
 }
