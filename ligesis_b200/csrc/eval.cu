@@ -29,20 +29,26 @@ __device__ ef2 block_sum(ef2 v, ef2* red) {
   return t;
 }
 
-// tab[j] = prod_{t < b} (bit t of j ? p[t] : 1 - p[t]) for j < 2^b, built by doubling.
+// tab[j] = prod_{t < b} (bit t of j ? p[t] : 1 - p[t]) for j < 2^b (b <= 10): two direct
+// 32-entry half tables (low 5 and high 5 bits) and one product per entry, two barriers.
+// Every thread of the CTA must call it; tab is complete when it returns.
 __device__ void eq_table_smem(const ef2* p, unsigned b, ef2* tab) {
-  if (threadIdx.x == 0) tab[0] = ef_one();
-  __syncthreads();
-  for (unsigned t = 0; t < b; ++t) {
-    const unsigned h = 1u << t;
-    const ef2 pt = p[t], qt = ef_sub(ef_one(), pt);
-    for (unsigned j = threadIdx.x; j < h; j += blockDim.x) {
-      ef2 x = tab[j];
-      tab[j + h] = ef_mul(x, pt);
-      tab[j] = ef_mul(x, qt);
-    }
-    __syncthreads();
+  __shared__ ef2 half_tabs[64];
+  const unsigned b1 = b < 5 ? b : 5, b2 = b - b1;
+  const unsigned n1 = 1u << b1, n2 = 1u << b2;
+  for (unsigned j = threadIdx.x; j < n1 + n2; j += blockDim.x) {
+    const bool hi = j >= n1;
+    const unsigned idx = hi ? j - n1 : j, nb = hi ? b2 : b1;
+    const ef2* pp = hi ? p + b1 : p;
+    ef2 acc = ef_one();
+    for (unsigned t = 0; t < nb; ++t)
+      acc = ef_mul(acc, ((idx >> t) & 1) ? pp[t] : ef_sub(ef_one(), pp[t]));
+    half_tabs[(hi ? 32 : 0) + idx] = acc;
   }
+  __syncthreads();
+  for (unsigned j = threadIdx.x; j < (1u << b); j += blockDim.x)
+    tab[j] = ef_mul(half_tabs[j & (n1 - 1)], half_tabs[32 + (j >> b1)]);
+  __syncthreads();
 }
 // prod_{t in [b, k)} (bit t of idx ? p[t] : 1 - p[t])
 __device__ ef2 eq_high(const ef2* p, unsigned b, unsigned k, size_t idx) {
@@ -178,16 +184,79 @@ void eq_dot_dev(const void* vec, int is_bf, const ef2* point, unsigned k, ef2* o
 }
 
 // ---- a-bar = eq_{z1}^T F (pcs/src/ligesis.rs:372-379) --------------------------------------
+// Two adjacent columns per thread (16-byte loads), four rows in flight with independent sums.
 __global__ void gemv_eq_rows_kernel(const u64* __restrict__ f, const ef2* __restrict__ eq,
                                     size_t m, size_t n, ef2* __restrict__ out) {
-  size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t j = 2 * ((size_t)blockIdx.x * blockDim.x + threadIdx.x);
   if (j >= n) return;
-  ef2 acc = ef_zero();
-  for (size_t i = 0; i < m; ++i) acc = ef_add(acc, ef_scale(eq[i], __ldg(f + i * n + j)));
-  out[j] = acc;
+  ef2 a0[4], a1[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) a0[q] = a1[q] = ef_zero();
+  size_t i = 0;
+  for (; i + 4 <= m; i += 4) {
+    ulonglong2 x[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) x[q] = __ldg((const ulonglong2*)(f + (i + q) * n + j));
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const ef2 e = eq[i + q];
+      a0[q] = ef_add(a0[q], ef_scale(e, x[q].x));
+      a1[q] = ef_add(a1[q], ef_scale(e, x[q].y));
+    }
+  }
+  for (; i < m; ++i) {
+    const ulonglong2 x = __ldg((const ulonglong2*)(f + i * n + j));
+    a0[0] = ef_add(a0[0], ef_scale(eq[i], x.x));
+    a1[0] = ef_add(a1[0], ef_scale(eq[i], x.y));
+  }
+  out[j] = ef_add(ef_add(a0[0], a0[1]), ef_add(a0[2], a0[3]));
+  out[j + 1] = ef_add(ef_add(a1[0], a1[1]), ef_add(a1[2], a1[3]));
 }
 void gemv_eq_rows(const u64* f, const ef2* eq, size_t m, size_t n, ef2* out, cudaStream_t st) {
-  gemv_eq_rows_kernel<<<cdiv(n, 256), 256, 0, st>>>(f, eq, m, n, out);
+  if (n % 2) throw ShapeError("gemv: n must be even");
+  gemv_eq_rows_kernel<<<cdiv(n / 2, 256), 256, 0, st>>>(f, eq, m, n, out);
+  LGS_LAUNCH_CHECK();
+}
+
+// ---- many eq-weighted dots at once: out_t = sum_i vec_t[i] eq_{point_t}(i), all 2^k long ----
+__global__ void eq_dot_multi_kernel(const EqDotTask* __restrict__ tasks, unsigned k,
+                                    ef2* __restrict__ partials) {
+  __shared__ ef2 p[64];
+  __shared__ ef2 tab[1 << EQ_TILE_LOG];
+  __shared__ ef2 red[32];
+  const EqDotTask task = tasks[blockIdx.y];
+  if (threadIdx.x < k) p[threadIdx.x] = task.point[threadIdx.x];
+  __syncthreads();
+  const unsigned b = k < EQ_TILE_LOG ? k : EQ_TILE_LOG;
+  const size_t base = (size_t)blockIdx.x << b;
+  eq_table_smem(p, b, tab);
+  ef2 acc = ef_zero();
+  for (unsigned j = threadIdx.x; j < (1u << b); j += blockDim.x)
+    acc = ef_add(acc, ef_mul(task.vec[base + j], tab[j]));
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0)
+    partials[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = ef_mul(acc, eq_high(p, b, k, base));
+}
+__global__ void eq_dot_multi_reduce(const EqDotTask* __restrict__ tasks,
+                                    const ef2* __restrict__ partials, unsigned ntiles) {
+  __shared__ ef2 red[32];
+  ef2 acc = ef_zero();
+  for (unsigned i = threadIdx.x; i < ntiles; i += blockDim.x)
+    acc = ef_add(acc, partials[(size_t)blockIdx.x * ntiles + i]);
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) *tasks[blockIdx.x].out = acc;
+}
+size_t eq_dot_multi_partials(unsigned k, unsigned ntasks) {
+  return (size_t)ntasks * (k > EQ_TILE_LOG ? ((size_t)1 << (k - EQ_TILE_LOG)) : 1);
+}
+void eq_dot_multi_dev(const EqDotTask* tasks_dev, unsigned ntasks, unsigned k, ef2* partials,
+                      cudaStream_t st) {
+  if (k > 40 || ntasks == 0 || ntasks > 65535) throw ShapeError("eq_dot_multi: bad sizes");
+  const unsigned b = k < EQ_TILE_LOG ? k : EQ_TILE_LOG;
+  const unsigned ntiles = (unsigned)((size_t)1 << (k - b));
+  eq_dot_multi_kernel<<<dim3(ntiles, ntasks), 256, 0, st>>>(tasks_dev, k, partials);
+  LGS_LAUNCH_CHECK();
+  eq_dot_multi_reduce<<<ntasks, 256, 0, st>>>(tasks_dev, partials, ntiles);
   LGS_LAUNCH_CHECK();
 }
 
@@ -381,80 +450,35 @@ void bf_fold_poly_dev(const u64* poly, int is_ef, unsigned li, const ef2* point,
   LGS_LAUNCH_CHECK();
 }
 
-// CTA c < nch: the R evaluation-reduction rounds of channel c (pcs/src/basefold.rs:746-769):
-//   l0 = MLE(m[even])(zp[t+1..]), l1 = MLE(m[odd])(zp[t+1..]); msg = l0; m <- fold(m, r_t).
-// CTA nch: the R codeword folds (eq_fold_codeword, pcs/src/basefold.rs:201-218) on `levels`
-// (level k of length D >> k stored at offset D * (2 - 2^(1-k))).
-struct BfRoundsArgs {
-  ef2* m[4];
-  ef2* tmp[4];
-  const ef2* zp[4];
-};
+// The R codeword folds of the batched open (eq_fold_codeword, pcs/src/basefold.rs:201-218):
+// level t+1[i] = (1 - r_t)(x + nx)/2 + r_t (x - nx) g_len^(-i) / 2, x = level t[i],
+// nx = level t[i + len/2].  Level k (length D >> k) is stored at offset D (2 - 2^(1-k)).
+// One CTA, because every level depends on the previous one and the whole chain is ~2D values.
 __global__ void __launch_bounds__(1024)
-    bf_rounds_kernel(BfRoundsArgs a, unsigned nch, unsigned R, const ef2* __restrict__ ch,
-                     ef2* __restrict__ msgs, ef2* __restrict__ levels, size_t D,
+    bf_levels_kernel(ef2* __restrict__ levels, size_t D, unsigned R, const ef2* __restrict__ ch,
                      const u64* __restrict__ tw) {
-  extern __shared__ ef2 sm[];  // lo table (64) + hi table (2^(R-7))
-  __shared__ ef2 red[32];
-  __shared__ ef2 zp[64];
-  const unsigned c = blockIdx.x;
-  if (c == nch) {
-    const u64 inv2 = 0x7FFFFFFF80000001ULL;  // (p + 1) / 2
-    size_t off = 0, len = D;
-    for (unsigned t = 0; t < R; ++t) {
-      const ef2 r = ch[t];
-      const size_t h = len >> 1;
-      const unsigned lg = 63 - __clzll((long long)len);
-      for (size_t i = threadIdx.x; i < h; i += blockDim.x) {
-        ef2 x = levels[off + i], nx = levels[off + i + h];
-        u64 ginv = i ? __ldg(tw + ((len - i) << (TW_LOG - lg))) : 1;
-        ef2 pe = ef_scale(ef_add(x, nx), inv2);
-        ef2 po = ef_scale(ef_scale(ef_sub(x, nx), ginv), inv2);
-        levels[off + len + i] = ef_add(ef_mul(ef_sub(ef_one(), r), pe), ef_mul(r, po));
-      }
-      __syncthreads();
-      off += len;
-      len = h;
-    }
-    return;
-  }
-  if (threadIdx.x < R) zp[threadIdx.x] = a.zp[c][threadIdx.x];
-  __syncthreads();
-  ef2* m = a.m[c];
-  ef2* tmp = a.tmp[c];
-  ef2* lo_tab = sm;
-  ef2* hi_tab = sm + 64;
+  const u64 inv2 = 0x7FFFFFFF80000001ULL;  // (p + 1) / 2
+  size_t off = 0, len = D;
   for (unsigned t = 0; t < R; ++t) {
-    const unsigned nrest = R - t - 1;  // variables of the rest point
-    const size_t half = (size_t)1 << nrest;
-    const unsigned blo = nrest < 6 ? nrest : 6, bhi = nrest - blo;
-    eq_table_smem(zp + t + 1, blo, lo_tab);
-    eq_table_smem(zp + t + 1 + blo, bhi, hi_tab);
-    ef2 l0 = ef_zero(), l1 = ef_zero();
-    for (size_t i = threadIdx.x; i < half; i += blockDim.x) {
-      ef2 e = ef_mul(lo_tab[i & ((1u << blo) - 1)], hi_tab[i >> blo]);
-      l0 = ef_add(l0, ef_mul(m[2 * i], e));
-      l1 = ef_add(l1, ef_mul(m[2 * i + 1], e));
-    }
-    l0 = block_sum(l0, red);
-    if (threadIdx.x == 0) msgs[(size_t)c * R + t] = l0;
-    (void)l1;
     const ef2 r = ch[t];
-    for (size_t i = threadIdx.x; i < half; i += blockDim.x) tmp[i] = ef_lerp(m[2 * i], m[2 * i + 1], r);
+    const size_t h = len >> 1;
+    const unsigned lg = 63 - __clzll((long long)len);
+    for (size_t i = threadIdx.x; i < h; i += blockDim.x) {
+      const ef2 x = levels[off + i], nx = levels[off + i + h];
+      const u64 ginv = i ? __ldg(tw + ((len - i) << (TW_LOG - lg))) : 1;
+      const ef2 pe = ef_scale(ef_add(x, nx), inv2);
+      const ef2 po = ef_scale(ef_scale(ef_sub(x, nx), ginv), inv2);
+      levels[off + len + i] = ef_add(pe, ef_mul(r, ef_sub(po, pe)));
+    }
     __syncthreads();
-    ef2* sw = m;
-    m = tmp;
-    tmp = sw;
+    off += len;
+    len = h;
   }
 }
-void bf_rounds_dev(ef2* const* ms, ef2* const* tmps, const ef2* const* zps, unsigned nch,
-                   unsigned R, const ef2* ch, ef2* msgs_out, ef2* levels, size_t D,
-                   const u64* tw, void*, cudaStream_t st) {
-  if (nch > 4 || R > 17 || R < 1) throw ShapeError("basefold: unsupported round count");
-  BfRoundsArgs a;
-  for (unsigned c = 0; c < nch; ++c) a.m[c] = ms[c], a.tmp[c] = tmps[c], a.zp[c] = zps[c];
-  size_t smem = (64 + ((size_t)1 << (R > 7 ? R - 7 : 0))) * sizeof(ef2);
-  bf_rounds_kernel<<<nch + 1, 1024, smem, st>>>(a, nch, R, ch, msgs_out, levels, D, tw);
+void bf_levels_dev(ef2* levels, size_t D, unsigned R, const ef2* ch, const u64* tw,
+                   cudaStream_t st) {
+  if (R < 1 || R > 30) throw ShapeError("basefold: unsupported round count");
+  bf_levels_kernel<<<1, 1024, 0, st>>>(levels, D, R, ch, tw);
   LGS_LAUNCH_CHECK();
 }
 

@@ -29,6 +29,13 @@ void subset_sum_hash_tc(const void* tmap, const u64* cw, u64* H, u32* leaves, un
 size_t merkle_node_count(size_t nleaves);
 size_t merkle_layer_offset(size_t nleaves, unsigned layer);
 void merkle_build_from_leaves(u32* nodes, size_t nleaves, cudaStream_t st);
+// Up to 16 independent trees (node buffers with their leaf hashes in place) built together:
+// one launch per 9 layers of the tallest tree.
+void merkle_build_many(u32* const* nodes, const size_t* nleaves, unsigned ntrees, cudaStream_t st);
+// Leaf hashes of up to 16 trees in one launch: tree t's leaves are nleaves[t] runs of `words`
+// u64 starting at data[t], hashed into nodes[t].
+void merkle_leaves_many(const u64* const* data, unsigned words, u32* const* nodes,
+                        const size_t* nleaves, unsigned ntrees, cudaStream_t st);
 void merkle_leaves_contig(const u64* data, unsigned words, size_t nleaves, u32* nodes,
                           cudaStream_t st);
 void gather_u64(const u64* src, const uint64_t* idx, size_t count, unsigned words, u64* dst,
@@ -38,6 +45,9 @@ void gather_u64(const u64* src, const uint64_t* idx, size_t count, unsigned word
 size_t sumcheck_partials_elems(unsigned k, unsigned d);
 void sumcheck_prove_dev(ef2* const* polys, unsigned d, unsigned k, const ef2* ch, ef2* rounds_out,
                         ef2* final_out, ef2* partials, cudaStream_t st);
+// The 3-factor sumcheck of [b, b - 1, eq] storing only b and eq (both folded in place).
+void sumcheck_binary_dev(ef2* b, ef2* eq, unsigned k, const ef2* ch, ef2* rounds_out,
+                         ef2* final_out, ef2* partials, cudaStream_t st);
 
 // eval.cu
 struct GatherSeg {
@@ -80,8 +90,16 @@ void bf_combine_dev(const BfChannelDev* chs_dev, unsigned nch, const ef2* coeffs
                     ef2* combined, cudaStream_t st);
 void bf_fold_poly_dev(const u64* poly, int is_ef, unsigned li, const ef2* point, size_t out_len,
                       ef2* m, cudaStream_t st);
-void bf_rounds_dev(ef2* const* ms, ef2* const* tmps, const ef2* const* zps, unsigned nch,
-                   unsigned R, const ef2* ch, ef2* msgs_out, ef2* levels, size_t D,
-                   const u64* tw, void* scratch_ptrs, cudaStream_t st);
+void bf_levels_dev(ef2* levels, size_t D, unsigned R, const ef2* ch, const u64* tw,
+                   cudaStream_t st);
+// Many MLE evaluations at once: *out = sum_i vec[i] eq_point(i), every vec 2^k EF long.
+struct EqDotTask {
+  const ef2* vec;
+  const ef2* point;
+  ef2* out;
+};
+size_t eq_dot_multi_partials(unsigned k, unsigned ntasks);
+void eq_dot_multi_dev(const EqDotTask* tasks_dev, unsigned ntasks, unsigned k, ef2* partials,
+                      cudaStream_t st);
 
 }  // namespace lgs

@@ -252,6 +252,19 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   const size_t P_bipts = put(cat(cat(r1, p_bi_hash), p_bi_recon));
   const size_t P_apts = put(cat(z2, r6));
   const size_t P_pa = put(p_a), P_rbi = put(r_bi), P_ra = put(r_a);
+  // batched-open evaluation points Q_{c,t} = (r_0 .. r_{t-1}, 0, zp_c[t+1] .. zp_c[R-1])
+  size_t P_q;
+  {
+    const std::vector<ef2>* cpts[3] = {&p_a, &r_bi, &r_a};
+    const unsigned cli[3] = {s.li(s.na()), s.li(s.nbi()), s.li(s.naa())};
+    const auto rb = slice(fp.ch_batch, R);
+    std::vector<ef2> q;
+    for (int ch = 0; ch < 3; ++ch)
+      for (unsigned t = 0; t < R; ++t)
+        for (unsigned u = 0; u < R; ++u)
+          q.push_back(u < t ? rb[u] : (u == t ? ef_zero() : (*cpts[ch])[cli[ch] + u]));
+    P_q = put(q);
+  }
 
   // ---- staging layout ----------------------------------------------------------------------
   Stage sg;
@@ -350,16 +363,13 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
 
   // -- binary check (pcs/src/ligesis.rs:419-429)
   ef2* partials_sc = ar.get<ef2>(sumcheck_partials_elems(kmax, 3));
-  {
+  {  // factors [B_I, B_I - 1, eq_alpha1]; the middle one is derived, not stored
     ef2* p0 = ar.get<ef2>(WS);
-    ef2* p1 = ar.get<ef2>(WS);
     ef2* p2 = ar.get<ef2>(WS);
     lift_bf(bi, p0, WS, 0, st);
-    lift_bf(bi, p1, WS, 1, st);
     new_eq_dev(d_fields + fp.alpha1, nb, p2, st);
-    ef2* ps[3] = {p0, p1, p2};
-    sumcheck_prove_dev(ps, 3, nb, d_fields + fp.ch_bin, (ef2*)(stage + S_sc_r[0]),
-                       (ef2*)(stage + S_sc_f[0]), partials_sc, st);
+    sumcheck_binary_dev(p0, p2, nb, d_fields + fp.ch_bin, (ef2*)(stage + S_sc_r[0]),
+                        (ef2*)(stage + S_sc_f[0]), partials_sc, st);
   }
   // -- hash / recon channels (pcs/src/ligesis.rs:432-485)
   ef2* eq_a2 = ar.get<ef2>(DIGEST_ROWS);
@@ -436,29 +446,47 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     hs.assign((const uint8_t*)chs, (const uint8_t*)chs + sizeof(chs));
     h2d(d_chs, hs.data(), sizeof(chs), st);
     bf_combine_dev(d_chs, 3, d_fields + fp.coeffs, D, levels, st);
-    ef2* ms[3];
-    ef2* tmps[3];
-    const ef2* zps[3];
+    bf_levels_dev(levels, D, R, d_fields + fp.ch_batch, c->tw.as<u64>(), st);
+    // Reduction messages: with m = poly.fold(point[0..li]) (2^R values) and the batch
+    // challenges r_0.., round t's l0 = MLE(m)(r_0, .., r_{t-1}, 0, zp[t+1], .., zp[R-1]): the
+    // sequential fold of pcs/src/basefold.rs:746-769 collapses to R independent evaluations.
     const size_t mlen = (size_t)1 << R;
+    std::vector<EqDotTask> tasks(3 * R);
     for (int ch = 0; ch < 3; ++ch) {
-      ms[ch] = ar.get<ef2>(mlen);
-      tmps[ch] = ar.get<ef2>(mlen);
-      bf_fold_poly_dev(polys[ch], chan_ef[ch], chan_li[ch], pts[ch], mlen, ms[ch], st);
-      zps[ch] = pts[ch] + chan_li[ch];
+      ef2* mch = ar.get<ef2>(mlen);
+      bf_fold_poly_dev(polys[ch], chan_ef[ch], chan_li[ch], pts[ch], mlen, mch, st);
+      for (unsigned t = 0; t < R; ++t) {
+        EqDotTask& tk = tasks[ch * R + t];
+        tk.vec = mch;
+        tk.point = d_prm + P_q + (size_t)(ch * R + t) * R;
+        tk.out = (ef2*)(stage + S_msgs) + ch * R + t;
+      }
     }
-    bf_rounds_dev(ms, tmps, zps, 3, R, d_fields + fp.ch_batch, (ef2*)(stage + S_msgs), levels, D,
-                  c->tw.as<u64>(), nullptr, st);
+    EqDotTask* d_tasks = ar.get<EqDotTask>(tasks.size());
+    ef2* part = ar.get<ef2>(eq_dot_multi_partials(R, (unsigned)tasks.size()));
+    std::vector<uint8_t>& hs2 = c->host_stage2;
+    hs2.assign((const uint8_t*)tasks.data(), (const uint8_t*)(tasks.data() + tasks.size()));
+    h2d(d_tasks, hs2.data(), hs2.size(), st);
+    eq_dot_multi_dev(d_tasks, (unsigned)tasks.size(), R, part, st);
   }
-  // level trees 1..R-1 (leaf = one serialized EF)
+  // level trees 1..R-1 (leaf = one serialized EF), all in two launches per 9 layers
   std::vector<u32*> lvl_nodes(R, nullptr);
   {
+    std::vector<const u64*> ldata;
+    std::vector<u32*> lnodes;
+    std::vector<size_t> lcount;
     size_t off = D;
     for (unsigned k = 1; k < R; ++k) {
-      size_t len = D >> k;
+      const size_t len = D >> k;
       lvl_nodes[k] = ar.get<u32>((2 * len - 1) * 8);
-      merkle_leaves_contig((const u64*)(levels + off), 2, len, lvl_nodes[k], st);
-      merkle_build_from_leaves(lvl_nodes[k], len, st);
+      ldata.push_back((const u64*)(levels + off));
+      lnodes.push_back(lvl_nodes[k]);
+      lcount.push_back(len);
       off += len;
+    }
+    if (!lnodes.empty()) {
+      merkle_leaves_many(ldata.data(), 2, lnodes.data(), lcount.data(), (unsigned)lnodes.size(), st);
+      merkle_build_many(lnodes.data(), lcount.data(), (unsigned)lnodes.size(), st);
     }
   }
 

@@ -149,6 +149,7 @@ struct lgs_ctx {
   lgs::Profiler prof;
   lgs::DevMem err;  // device error word of bounded-wait kernels (0 = ok)
   std::vector<uint8_t> host_stage;  // host copies that must outlive an async upload
+  std::vector<uint8_t> host_stage2;
   std::vector<uint8_t> proof_buf;   // the last proof returned by lgs_prove
 };
 

@@ -7,14 +7,19 @@
 // round t-1 is fused into the evaluation pass of round t (each thread owns the quadruple
 // i, i + half, i + 2 half, i + 3 half, so the in-place fold has no races), per-CTA partial sums
 // go to a scratch array, and a last kernel reduces them into the round polynomials.  Once the
-// vectors are short, one CTA finishes the remaining rounds on its own.
+// vectors are short (1024 entries, 512 for three stored factors), one CTA loads them into shared
+// memory and finishes the remaining rounds there.
+//
+// Binary variant (the B_I check of pcs/src/ligesis.rs:423-428, factors [b, b - 1, eq]): the
+// middle factor is always the first minus one (folding is affine), so only b and eq are stored
+// and folded; the products, round messages and final evaluations are those of the 3-factor run.
 #include "kernels.cuh"
 
 namespace lgs {
 
 namespace {
 constexpr unsigned SC_THREADS = 256;
-constexpr unsigned SC_TAIL_LEN = 4096;  // vectors at most this long finish in one CTA
+constexpr unsigned SC_TAIL_THREADS = 256;
 
 __device__ __forceinline__ ef2 shfl_xor_ef(ef2 v, int m) {
   ef2 r;
@@ -47,35 +52,52 @@ __device__ void block_reduce(ef2 (&s)[D + 1], ef2* red) {
   __syncthreads();
 }
 
-template <int D>
-__device__ __forceinline__ void accumulate_pair(const ef2 (&lo)[D], const ef2 (&hi)[D],
-                                                ef2 (&s)[D + 1]) {
-  ef2 v[D], df[D];
+// Stored factor count: the binary variant keeps [b, eq] for the logical [b, b - 1, eq].
+template <int D, bool BIN>
+struct Fac {
+  static constexpr int S = BIN ? D - 1 : D;
+  // vectors at most this long finish in one CTA (in at most 48 KB of static shared memory)
+  static constexpr unsigned TAIL = S >= 3 ? 512 : 1024;
+};
+
+// Add prod_j (lo_j + q (hi_j - lo_j)) for q = 0..D to s, from the stored factors.
+template <int D, bool BIN>
+__device__ __forceinline__ void accumulate_pair(const ef2* lo, const ef2* hi, ef2 (&s)[D + 1]) {
+  constexpr int S = Fac<D, BIN>::S;
+  ef2 v[S], df[S];
 #pragma unroll
-  for (int j = 0; j < D; ++j) v[j] = lo[j], df[j] = ef_sub(hi[j], lo[j]);
+  for (int j = 0; j < S; ++j) v[j] = lo[j], df[j] = ef_sub(hi[j], lo[j]);
 #pragma unroll
   for (int q = 0; q <= D; ++q) {
-    ef2 p = v[0];
+    ef2 p;
+    if (BIN) {
+      p = ef_mul(v[0], ef_sub(v[0], ef_one()));  // b (b - 1)
 #pragma unroll
-    for (int j = 1; j < D; ++j) p = ef_mul(p, v[j]);
+      for (int j = 1; j < S; ++j) p = ef_mul(p, v[j]);
+    } else {
+      p = v[0];
+#pragma unroll
+      for (int j = 1; j < S; ++j) p = ef_mul(p, v[j]);
+    }
     s[q] = ef_add(s[q], p);
     if (q < D)
 #pragma unroll
-      for (int j = 0; j < D; ++j) v[j] = ef_add(v[j], df[j]);
+      for (int j = 0; j < S; ++j) v[j] = ef_add(v[j], df[j]);
   }
 }
 
-template <int D>
+template <int S>
 struct Polys {
-  ef2* p[D];
+  ef2* p[S];
 };
 
 // One round over `half` pairs.  If `fold`, the vectors still hold 4*half entries from the
 // previous round and are folded with r first (results written back to [0, 2*half)).
-template <int D>
+template <int D, bool BIN>
 __global__ void __launch_bounds__(SC_THREADS)
-    sc_round_kernel(Polys<D> P, size_t half, int fold, const ef2* __restrict__ rptr,
+    sc_round_kernel(Polys<Fac<D, BIN>::S> P, size_t half, int fold, const ef2* __restrict__ rptr,
                     ef2* __restrict__ partial) {
+  constexpr int S = Fac<D, BIN>::S;
   __shared__ ef2 red[(D + 1) * 32];
   ef2 s[D + 1];
 #pragma unroll
@@ -84,9 +106,9 @@ __global__ void __launch_bounds__(SC_THREADS)
   const size_t len = 2 * half;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < half;
        i += (size_t)gridDim.x * blockDim.x) {
-    ef2 lo[D], hi[D];
+    ef2 lo[S], hi[S];
 #pragma unroll
-    for (int j = 0; j < D; ++j) {
+    for (int j = 0; j < S; ++j) {
       ef2* p = P.p[j];
       if (fold) {
         lo[j] = ef_lerp(p[i], p[i + len], r);
@@ -98,7 +120,7 @@ __global__ void __launch_bounds__(SC_THREADS)
         hi[j] = p[i + half];
       }
     }
-    accumulate_pair<D>(lo, hi, s);
+    accumulate_pair<D, BIN>(lo, hi, s);
   }
   block_reduce<D>(s, red);
   if (threadIdx.x == 0)
@@ -106,46 +128,61 @@ __global__ void __launch_bounds__(SC_THREADS)
     for (int q = 0; q <= D; ++q) partial[(size_t)blockIdx.x * (D + 1) + q] = s[q];
 }
 
-// Remaining rounds t0..k-1 in one CTA.  On entry the vectors hold `len` entries; if `fold`,
-// they hold 2*len entries still to be folded with challenge t0-1.
-template <int D>
-__global__ void __launch_bounds__(1024)
-    sc_tail_kernel(Polys<D> P, size_t len, int fold, const ef2* __restrict__ ch, unsigned t0,
-                   unsigned k, ef2* __restrict__ rounds_out, ef2* __restrict__ final_out) {
+// Remaining rounds t0..k-1 in one CTA, in shared memory.  On entry the vectors hold `len`
+// entries (len <= TAIL); if `fold`, they hold 2*len entries still to be folded with
+// challenge t0 - 1.
+template <int D, bool BIN>
+__global__ void __launch_bounds__(SC_TAIL_THREADS)
+    sc_tail_kernel(Polys<Fac<D, BIN>::S> P, unsigned len, int fold, const ef2* __restrict__ ch,
+                   unsigned t0, unsigned k, ef2* __restrict__ rounds_out,
+                   ef2* __restrict__ final_out) {
+  constexpr int S = Fac<D, BIN>::S;
   __shared__ ef2 red[(D + 1) * 32];
-  if (fold) {
-    const ef2 r = ch[t0 - 1];
-    for (size_t i = threadIdx.x; i < len; i += blockDim.x)
+  __shared__ ef2 sv[S][Fac<D, BIN>::TAIL];
+  {
+    const ef2 r = fold ? ch[t0 - 1] : ef_zero();
+    for (unsigned i = threadIdx.x; i < len; i += blockDim.x)
 #pragma unroll
-      for (int j = 0; j < D; ++j) P.p[j][i] = ef_lerp(P.p[j][i], P.p[j][i + len], r);
-    __syncthreads();
+      for (int j = 0; j < S; ++j)
+        sv[j][i] = fold ? ef_lerp(P.p[j][i], P.p[j][i + len], r) : P.p[j][i];
   }
+  __syncthreads();
   for (unsigned t = t0; t < k; ++t) {
-    const size_t half = len >> 1;
+    const unsigned half = len >> 1;
     ef2 s[D + 1];
 #pragma unroll
     for (int q = 0; q <= D; ++q) s[q] = ef_zero();
-    for (size_t i = threadIdx.x; i < half; i += blockDim.x) {
-      ef2 lo[D], hi[D];
+    for (unsigned i = threadIdx.x; i < half; i += blockDim.x) {
+      ef2 lo[S], hi[S];
 #pragma unroll
-      for (int j = 0; j < D; ++j) lo[j] = P.p[j][i], hi[j] = P.p[j][i + half];
-      accumulate_pair<D>(lo, hi, s);
+      for (int j = 0; j < S; ++j) lo[j] = sv[j][i], hi[j] = sv[j][i + half];
+      accumulate_pair<D, BIN>(lo, hi, s);
     }
     block_reduce<D>(s, red);
     if (threadIdx.x == 0)
 #pragma unroll
       for (int q = 0; q <= D; ++q) rounds_out[(size_t)t * (D + 1) + q] = s[q];
     const ef2 r = ch[t];
-    for (size_t i = threadIdx.x; i < half; i += blockDim.x)
+    for (unsigned i = threadIdx.x; i < half; i += blockDim.x)
 #pragma unroll
-      for (int j = 0; j < D; ++j) P.p[j][i] = ef_lerp(P.p[j][i], P.p[j][i + half], r);
+      for (int j = 0; j < S; ++j) sv[j][i] = ef_lerp(sv[j][i], sv[j][i + half], r);
     __syncthreads();
     len = half;
   }
-  if (threadIdx.x < D) final_out[threadIdx.x] = P.p[threadIdx.x][0];
+  if (threadIdx.x == 0) {
+    if (BIN) {
+      final_out[0] = sv[0][0];
+      final_out[1] = ef_sub(sv[0][0], ef_one());
+#pragma unroll
+      for (int j = 1; j < S; ++j) final_out[j + 1] = sv[j][0];
+    } else {
+#pragma unroll
+      for (int j = 0; j < S; ++j) final_out[j] = sv[j][0];
+    }
+  }
 }
 
-// rounds_out[t] = sum of the partials of round t (t < nrounds); round t used
+// rounds_out[t] = sum of the partials of round t; round t used
 // min(SC_MAX_BLOCKS, ceil(2^(k-1-t) / SC_THREADS)) CTAs.
 template <int D>
 __global__ void sc_reduce_kernel(const ef2* __restrict__ partials, size_t stride, unsigned k,
@@ -167,26 +204,28 @@ __global__ void sc_reduce_kernel(const ef2* __restrict__ partials, size_t stride
     for (int q = 0; q <= D; ++q) rounds_out[(size_t)t * (D + 1) + q] = s[q];
 }
 
-template <int D>
+template <int D, bool BIN>
 void sumcheck_run(ef2* const* polys, unsigned k, const ef2* ch, ef2* rounds_out, ef2* final_out,
                   ef2* partials, cudaStream_t st) {
-  Polys<D> P;
-  for (int j = 0; j < D; ++j) P.p[j] = polys[j];
+  constexpr int S = Fac<D, BIN>::S;
+  Polys<S> P;
+  for (int j = 0; j < S; ++j) P.p[j] = polys[j];
   const size_t stride = (size_t)SC_MAX_BLOCKS * (D + 1);
   size_t len = (size_t)1 << k;
   unsigned t = 0;
   int fold = 0;
-  while (t < k && len > SC_TAIL_LEN) {
+  while (t < k && len > Fac<D, BIN>::TAIL) {
     size_t half = len >> 1;
     unsigned blocks = (unsigned)std::min<size_t>(SC_MAX_BLOCKS, cdiv(half, SC_THREADS));
-    sc_round_kernel<D><<<blocks, SC_THREADS, 0, st>>>(P, half, fold, fold ? ch + (t - 1) : ch,
-                                                      partials + (size_t)t * stride);
+    sc_round_kernel<D, BIN><<<blocks, SC_THREADS, 0, st>>>(
+        P, half, fold, fold ? ch + (t - 1) : ch, partials + (size_t)t * stride);
     LGS_LAUNCH_CHECK();
     len = half;
     fold = 1;
     ++t;
   }
-  sc_tail_kernel<D><<<1, 1024, 0, st>>>(P, len, fold, ch, t, k, rounds_out, final_out);
+  sc_tail_kernel<D, BIN><<<1, SC_TAIL_THREADS, 0, st>>>(P, (unsigned)len, fold, ch, t, k,
+                                                        rounds_out, final_out);
   LGS_LAUNCH_CHECK();
   if (t > 0) {
     sc_reduce_kernel<D><<<t, 256, 0, st>>>(partials, stride, k, rounds_out);
@@ -204,11 +243,18 @@ void sumcheck_prove_dev(ef2* const* polys, unsigned d, unsigned k, const ef2* ch
   if (k == 0) throw ShapeError("sumcheck: zero variables");
   if (k > 40) throw ShapeError("sumcheck: too many variables");
   switch (d) {
-    case 1: sumcheck_run<1>(polys, k, ch, rounds_out, final_out, partials, st); break;
-    case 2: sumcheck_run<2>(polys, k, ch, rounds_out, final_out, partials, st); break;
-    case 3: sumcheck_run<3>(polys, k, ch, rounds_out, final_out, partials, st); break;
+    case 1: sumcheck_run<1, false>(polys, k, ch, rounds_out, final_out, partials, st); break;
+    case 2: sumcheck_run<2, false>(polys, k, ch, rounds_out, final_out, partials, st); break;
+    case 3: sumcheck_run<3, false>(polys, k, ch, rounds_out, final_out, partials, st); break;
     default: throw ShapeError("sumcheck: 1 to 3 factors supported");
   }
+}
+
+void sumcheck_binary_dev(ef2* b, ef2* eq, unsigned k, const ef2* ch, ef2* rounds_out,
+                         ef2* final_out, ef2* partials, cudaStream_t st) {
+  if (k == 0 || k > 40) throw ShapeError("sumcheck: variable count out of range");
+  ef2* polys[2] = {b, eq};
+  sumcheck_run<3, true>(polys, k, ch, rounds_out, final_out, partials, st);
 }
 
 }  // namespace lgs
