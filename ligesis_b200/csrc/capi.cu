@@ -111,10 +111,16 @@ lgs_status lgs_ctx_create(int device, unsigned flags, lgs_ctx** out) {
 void lgs_ctx_destroy(lgs_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
-  if (ctx->st) {
-    cudaStreamSynchronize(ctx->st);
-    cudaStreamDestroy(ctx->st);
+  if (ctx->st) cudaStreamSynchronize(ctx->st);
+  for (int i = 0; i < lgs_ctx::NSIDE; ++i) {
+    if (ctx->side[i]) {
+      cudaStreamSynchronize(ctx->side[i]);
+      cudaStreamDestroy(ctx->side[i]);
+    }
+    if (ctx->ev_done[i]) cudaEventDestroy(ctx->ev_done[i]);
   }
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->st) cudaStreamDestroy(ctx->st);
   delete ctx;
 }
 

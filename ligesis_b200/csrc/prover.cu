@@ -22,7 +22,7 @@ void d2d(void* dst, const void* src, size_t bytes, cudaStream_t st) {
 // (MlPoly::split, utils/src/poly.rs:20-31), each zero-padded to 2 len/2^li and DFT'd; leaves are
 // the columns across chunks.  `out` receives codes (leaf-major) and the tree.
 void bf_commit(lgs_ctx* c, const u64* poly, int is_ef, size_t len, unsigned li,
-               BasefoldDev* out) {
+               BasefoldDev* out, cudaStream_t st) {
   Arena& ar = c->arena;
   const size_t rows = len >> li;
   const size_t cols = ((size_t)1 << li) * (is_ef ? 2 : 1);
@@ -31,11 +31,11 @@ void bf_commit(lgs_ctx* c, const u64* poly, int is_ef, size_t len, unsigned li,
   u64* tT = ar.get<u64>(cols * rows);
   u64* cT = ar.get<u64>(cols * L);
   u64* scr = logL > 12 ? ar.get<u64>(cols * L) : nullptr;
-  transpose_u64(poly, tT, rows, cols, 1, c->st);
-  ntt_batch(tT, rows, rows, cT, L, logL, cols, scr, c->tw.as<u64>(), c->st);
-  transpose_u64(cT, out->codes, cols, L, 1, c->st);
-  merkle_leaves_contig(out->codes, (unsigned)cols, L, out->nodes, c->st);
-  merkle_build_from_leaves(out->nodes, L, c->st);
+  transpose_u64(poly, tT, rows, cols, 1, st);
+  ntt_batch(tT, rows, rows, cT, L, logL, cols, scr, c->tw.as<u64>(), st);
+  transpose_u64(cT, out->codes, cols, L, 1, st);
+  merkle_leaves_contig(out->codes, (unsigned)cols, L, out->nodes, st);
+  merkle_build_from_leaves(out->nodes, L, st);
   out->poly = poly;
   out->is_ef = is_ef;
   out->li = li;
@@ -62,6 +62,11 @@ void ctx_init(lgs_ctx* c, int device) {
   uint64_t thresh = UINT64_MAX;
   LGS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thresh));
   c->arena.st = c->st;
+  for (int i = 0; i < lgs_ctx::NSIDE; ++i) {
+    LGS_CUDA(cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking));
+    LGS_CUDA(cudaEventCreateWithFlags(&c->ev_done[i], cudaEventDisableTiming));
+  }
+  LGS_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
   c->tw.alloc(((size_t)1 << TW_LOG) * sizeof(u64), c->st);
   c->err.alloc(sizeof(int), c->st);
   LGS_CUDA(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->st));
@@ -91,7 +96,7 @@ void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lg
   pk->a_nodes.alloc((2 * L - 1) * 32, c->st);
   pk->a_state.codes = pk->a_codes.as<u64>();
   pk->a_state.nodes = pk->a_nodes.as<u32>();
-  bf_commit(c, pk->A.as<u64>(), 0, len, li, &pk->a_state);
+  bf_commit(c, pk->A.as<u64>(), 0, len, li, &pk->a_state, c->st);
   pk->com_a = read_root(pk->a_state.nodes, L, c->st);
 }
 
@@ -292,8 +297,6 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   ef2* eqz1 = ar.get<ef2>(m);
   ef2* a_vec = ar.get<ef2>(n);
   ef2* ra = ar.get<ef2>(two_n);
-  const unsigned kmax = std::max(nb, log_n + 1);
-  ef2* partials = ar.get<ef2>(std::max<size_t>(eqdot_partials_elems(kmax), 1024));
   uint64_t* d_idx = ar.get<uint64_t>(S);
 
   // Basefold states built during prove
@@ -346,115 +349,129 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   }
   u64* stage = ar.get<u64>(sg.total);
 
-  // -- continue the dataflow
-  eq_dot_dev(a_vec, 0, d_prm + P_z2, log_n, (ef2*)(stage + S_y), partials, st);
-  bf_commit(c, (const u64*)a_vec, 1, n, li_a, &a_st);
-  {
-    u64* t1 = ar.get<u64>(2 * n);
-    u64* t2 = ar.get<u64>(2 * two_n);
-    u64* scr = ilog2(two_n) > 12 ? ar.get<u64>(2 * two_n) : nullptr;
-    transpose_u64((const u64*)a_vec, t1, n, 2, 1, st);
-    ntt_batch(t1, n, n, t2, two_n, ilog2(two_n), 2, scr, c->tw.as<u64>(), st);
-    transpose_u64(t2, (u64*)ra, 2, two_n, 1, st);
-  }
-  // -- B_I and its commitment (pcs/src/ligesis.rs:403-416)
+  // -- the rest is a DAG of independent branches (every challenge is pre-drawn): fork them
+  // onto side streams after the shared inputs exist, join before the gather.
   bits_gather(cd->cw.as<u64>(), two_n, d_idx, S, W, bi, st);
-  bf_commit(c, bi, 0, WS, li_bi, &bi_st);
-
-  // -- binary check (pcs/src/ligesis.rs:419-429)
-  ef2* partials_sc = ar.get<ef2>(sumcheck_partials_elems(kmax, 3));
-  {  // factors [B_I, B_I - 1, eq_alpha1]; the middle one is derived, not stored
-    ef2* p0 = ar.get<ef2>(WS);
-    ef2* p2 = ar.get<ef2>(WS);
-    lift_bf(bi, p0, WS, 0, st);
-    new_eq_dev(d_fields + fp.alpha1, nb, p2, st);
-    sumcheck_binary_dev(p0, p2, nb, d_fields + fp.ch_bin, (ef2*)(stage + S_sc_r[0]),
-                        (ef2*)(stage + S_sc_f[0]), partials_sc, st);
-  }
-  // -- hash / recon channels (pcs/src/ligesis.rs:432-485)
   ef2* eq_a2 = ar.get<ef2>(DIGEST_ROWS);
   ef2* eq_r2 = ar.get<ef2>(S);
   new_eq_dev(d_fields + fp.alpha2, 5, eq_a2, st);
   new_eq_dev(d_fields + fp.r2, log_s, eq_r2, st);
+  LGS_CUDA(cudaEventRecord(c->ev_fork, st));
+  unsigned nbr = 0;
+  auto branch = [&]() {
+    if (nbr >= (unsigned)lgs_ctx::NSIDE) throw std::runtime_error("prove: too many branches");
+    cudaStream_t b = c->side[nbr++];
+    LGS_CUDA(cudaStreamWaitEvent(b, c->ev_fork, 0));
+    return b;
+  };
+  auto partials_for = [&](unsigned k, unsigned d) {
+    return ar.get<ef2>(std::max(sumcheck_partials_elems(k, d), eqdot_partials_elems(k) + 1024));
+  };
+  // A1: y = a(z2) and the Basefold commitment to a-bar (pcs/src/ligesis.rs:379-384)
+  const unsigned br_a1 = nbr;
   {
+    cudaStream_t b = branch();
+    eq_dot_dev(a_vec, 0, d_prm + P_z2, log_n, (ef2*)(stage + S_y), partials_for(log_n, 1), b);
+    bf_commit(c, (const u64*)a_vec, 1, n, li_a, &a_st, b);
+  }
+  // A2: RS(a-bar), y4, the recon table sumcheck and y5 (pcs/src/ligesis.rs:387, 458, 487-497)
+  {
+    cudaStream_t b = branch();
+    u64* t1 = ar.get<u64>(2 * n);
+    u64* t2 = ar.get<u64>(2 * two_n);
+    u64* scr = ilog2(two_n) > 12 ? ar.get<u64>(2 * two_n) : nullptr;
+    transpose_u64((const u64*)a_vec, t1, n, 2, 1, b);
+    ntt_batch(t1, n, n, t2, two_n, ilog2(two_n), 2, scr, c->tw.as<u64>(), b);
+    transpose_u64(t2, (u64*)ra, 2, two_n, 1, b);
+    y4_dev(eq_r2, ra, d_idx, S, (ef2*)(stage + S_y4), b);
+    ef2* sel = ar.get<ef2>(two_n);
+    ef2* rac = ar.get<ef2>(two_n);
+    sel_build(d_idx, eq_r2, S, two_n, sel, b);
+    d2d(rac, ra, two_n * sizeof(ef2), b);
+    ef2* pt[2] = {sel, rac};
+    sumcheck_prove_dev(pt, 2, log_n + 1, d_fields + fp.ch_table, (ef2*)(stage + S_sc_r[3]),
+                       (ef2*)(stage + S_sc_f[3]), partials_for(log_n + 1, 2), b);
+    eq_dot_dev(ra, 0, d_prm + P_r3, log_n + 1, (ef2*)(stage + S_y5), partials_for(log_n + 1, 1), b);
+  }
+  // B: the Basefold commitment to B_I (pcs/src/ligesis.rs:411-416)
+  const unsigned br_b = nbr;
+  {
+    cudaStream_t b = branch();
+    bf_commit(c, bi, 0, WS, li_bi, &bi_st, b);
+  }
+  // C: binary check, factors [B_I, B_I - 1, eq_alpha1] (pcs/src/ligesis.rs:419-429)
+  {
+    cudaStream_t b = branch();
+    ef2* p0 = ar.get<ef2>(WS);
+    ef2* p2 = ar.get<ef2>(WS);
+    lift_bf(bi, p0, WS, 0, b);
+    new_eq_dev(d_fields + fp.alpha1, nb, p2, b);
+    sumcheck_binary_dev(p0, p2, nb, d_fields + fp.ch_bin, (ef2*)(stage + S_sc_r[0]),
+                        (ef2*)(stage + S_sc_f[0]), partials_for(nb, 3), b);
+  }
+  // D: hash and recon bilinear sumchecks (pcs/src/ligesis.rs:435-485)
+  {
+    cudaStream_t b = branch();
     ef2* g1 = ar.get<ef2>(W);
     ef2* g2 = ar.get<ef2>(W);
     ef2* g2b = ar.get<ef2>(W);
     ef2* v = ar.get<ef2>(W);
-    g1_build(pk->A.as<u64>(), W, eq_a2, DIGEST_ROWS, g1, st);
-    g2_build(bi, W, S, eq_r2, g2, st);
-    d2d(g2b, g2, W * sizeof(ef2), st);
-    y4_dev(eq_r2, ra, d_idx, S, (ef2*)(stage + S_y4), st);
-    v_build(eqz1, W, v, st);
+    g1_build(pk->A.as<u64>(), W, eq_a2, DIGEST_ROWS, g1, b);
+    g2_build(bi, W, S, eq_r2, g2, b);
+    d2d(g2b, g2, W * sizeof(ef2), b);
+    v_build(eqz1, W, v, b);
     ef2* ph[2] = {g1, g2};
+    ef2* part = partials_for(log_w, 2);
     sumcheck_prove_dev(ph, 2, log_w, d_fields + fp.ch_hash, (ef2*)(stage + S_sc_r[1]),
-                       (ef2*)(stage + S_sc_f[1]), partials_sc, st);
+                       (ef2*)(stage + S_sc_f[1]), part, b);
     ef2* pr[2] = {v, g2b};
     sumcheck_prove_dev(pr, 2, log_w, d_fields + fp.ch_recon, (ef2*)(stage + S_sc_r[2]),
-                       (ef2*)(stage + S_sc_f[2]), partials_sc, st);
+                       (ef2*)(stage + S_sc_f[2]), part, b);
   }
-  // -- recon table, y5, RS link (pcs/src/ligesis.rs:487-502)
+  // E: RS-link sumcheck (pcs/src/ligesis.rs:499-502); r3 is pre-drawn, so w needs no wait
   {
-    ef2* sel = ar.get<ef2>(two_n);
-    ef2* rac = ar.get<ef2>(two_n);
-    sel_build(d_idx, eq_r2, S, two_n, sel, st);
-    d2d(rac, ra, two_n * sizeof(ef2), st);
-    ef2* pt[2] = {sel, rac};
-    sumcheck_prove_dev(pt, 2, log_n + 1, d_fields + fp.ch_table, (ef2*)(stage + S_sc_r[3]),
-                       (ef2*)(stage + S_sc_f[3]), partials_sc, st);
-    eq_dot_dev(ra, 0, d_prm + P_r3, log_n + 1, (ef2*)(stage + S_y5), partials, st);
+    cudaStream_t b = branch();
     ef2* w = ar.get<ef2>(n);
     ef2* ac = ar.get<ef2>(n);
-    rs_weights_dev(d_prm + P_r3, log_n + 1, n, c->tw.as<u64>(), w, st);
-    d2d(ac, a_vec, n * sizeof(ef2), st);
+    rs_weights_dev(d_prm + P_r3, log_n + 1, n, c->tw.as<u64>(), w, b);
+    d2d(ac, a_vec, n * sizeof(ef2), b);
     ef2* pw[2] = {ac, w};
     sumcheck_prove_dev(pw, 2, log_n, d_fields + fp.ch_rs, (ef2*)(stage + S_sc_r[4]),
-                       (ef2*)(stage + S_sc_f[4]), partials_sc, st);
+                       (ef2*)(stage + S_sc_f[4]), partials_for(log_n, 2), b);
   }
-  // -- Stage A (pcs/src/ligesis.rs:510-522)
+  // F, G: Stage A point reductions (pcs/src/ligesis.rs:510-522)
   {
+    cudaStream_t b = branch();
     ef2* gbi = ar.get<ef2>(WS);
     ef2* bie = ar.get<ef2>(WS);
-    combine_eq_dev(d_prm + P_bipts, 3, nb, d_fields + fp.gamma_bi, gbi, st);
-    lift_bf(bi, bie, WS, 0, st);
+    combine_eq_dev(d_prm + P_bipts, 3, nb, d_fields + fp.gamma_bi, gbi, b);
+    lift_bf(bi, bie, WS, 0, b);
     ef2* pb[2] = {bie, gbi};
     sumcheck_prove_dev(pb, 2, nb, d_fields + fp.ch_bi, (ef2*)(stage + S_sc_r[5]),
-                       (ef2*)(stage + S_sc_f[5]), partials_sc, st);
+                       (ef2*)(stage + S_sc_f[5]), partials_for(nb, 2), b);
+  }
+  {
+    cudaStream_t b = branch();
     ef2* ga = ar.get<ef2>(n);
     ef2* ac = ar.get<ef2>(n);
-    combine_eq_dev(d_prm + P_apts, 2, log_n, d_fields + fp.gamma_a, ga, st);
-    d2d(ac, a_vec, n * sizeof(ef2), st);
+    combine_eq_dev(d_prm + P_apts, 2, log_n, d_fields + fp.gamma_a, ga, b);
+    d2d(ac, a_vec, n * sizeof(ef2), b);
     ef2* pa[2] = {ac, ga};
     sumcheck_prove_dev(pa, 2, log_n, d_fields + fp.ch_a, (ef2*)(stage + S_sc_r[6]),
-                       (ef2*)(stage + S_sc_f[6]), partials_sc, st);
+                       (ef2*)(stage + S_sc_f[6]), partials_for(log_n, 2), b);
   }
-  // -- Stage B: shared-domain batched open (pcs/src/basefold.rs:679-856)
-  ef2* levels = ar.get<ef2>(2 * D);
+  // H: Stage B reduction messages (pcs/src/basefold.rs:746-769).  With m = poly.fold(point[0..li])
+  // (2^R values) and the batch challenges r_0.., round t's l0 = MLE(m)(r_0, .., r_{t-1}, 0,
+  // zp[t+1], .., zp[R-1]): the sequential rounds collapse to R independent evaluations.
+  const ef2* pts[3] = {d_prm + P_pa, d_prm + P_rbi, d_prm + P_ra};
+  const u64* polys[3] = {pk->A.as<u64>(), bi, (const u64*)a_vec};
   {
-    BfChannelDev chs[3];
-    const ef2* pts[3] = {d_prm + P_pa, d_prm + P_rbi, d_prm + P_ra};
-    const u64* polys[3] = {pk->A.as<u64>(), bi, (const u64*)a_vec};
-    for (int ch = 0; ch < 3; ++ch) {
-      chs[ch].codes = chan_states[ch]->codes;
-      chs[ch].poly = polys[ch];
-      chs[ch].is_ef = chan_ef[ch];
-      chs[ch].li = chan_li[ch];
-      chs[ch].point = pts[ch];
-    }
-    BfChannelDev* d_chs = ar.get<BfChannelDev>(3);
-    std::vector<uint8_t>& hs = c->host_stage;  // keep the host copy alive until the sync below
-    hs.assign((const uint8_t*)chs, (const uint8_t*)chs + sizeof(chs));
-    h2d(d_chs, hs.data(), sizeof(chs), st);
-    bf_combine_dev(d_chs, 3, d_fields + fp.coeffs, D, levels, st);
-    bf_levels_dev(levels, D, R, d_fields + fp.ch_batch, c->tw.as<u64>(), st);
-    // Reduction messages: with m = poly.fold(point[0..li]) (2^R values) and the batch
-    // challenges r_0.., round t's l0 = MLE(m)(r_0, .., r_{t-1}, 0, zp[t+1], .., zp[R-1]): the
-    // sequential fold of pcs/src/basefold.rs:746-769 collapses to R independent evaluations.
+    cudaStream_t b = branch();
     const size_t mlen = (size_t)1 << R;
     std::vector<EqDotTask> tasks(3 * R);
     for (int ch = 0; ch < 3; ++ch) {
       ef2* mch = ar.get<ef2>(mlen);
-      bf_fold_poly_dev(polys[ch], chan_ef[ch], chan_li[ch], pts[ch], mlen, mch, st);
+      bf_fold_poly_dev(polys[ch], chan_ef[ch], chan_li[ch], pts[ch], mlen, mch, b);
       for (unsigned t = 0; t < R; ++t) {
         EqDotTask& tk = tasks[ch * R + t];
         tk.vec = mch;
@@ -466,10 +483,32 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     ef2* part = ar.get<ef2>(eq_dot_multi_partials(R, (unsigned)tasks.size()));
     std::vector<uint8_t>& hs2 = c->host_stage2;
     hs2.assign((const uint8_t*)tasks.data(), (const uint8_t*)(tasks.data() + tasks.size()));
-    h2d(d_tasks, hs2.data(), hs2.size(), st);
-    eq_dot_multi_dev(d_tasks, (unsigned)tasks.size(), R, part, st);
+    h2d(d_tasks, hs2.data(), hs2.size(), b);
+    eq_dot_multi_dev(d_tasks, (unsigned)tasks.size(), R, part, b);
   }
-  // level trees 1..R-1 (leaf = one serialized EF), all in two launches per 9 layers
+  // join: main waits for every branch
+  for (unsigned i = 0; i < nbr; ++i) LGS_CUDA(cudaEventRecord(c->ev_done[i], c->side[i]));
+  LGS_CUDA(cudaStreamWaitEvent(st, c->ev_done[br_a1], 0));
+  LGS_CUDA(cudaStreamWaitEvent(st, c->ev_done[br_b], 0));
+  // Stage B codeword chain on main (needs both prove-time commitments): combined level 0,
+  // the R folds, and the Merkle trees of levels 1..R-1 (pcs/src/basefold.rs:735-784)
+  ef2* levels = ar.get<ef2>(2 * D);
+  {
+    BfChannelDev chs[3];
+    for (int ch = 0; ch < 3; ++ch) {
+      chs[ch].codes = chan_states[ch]->codes;
+      chs[ch].poly = polys[ch];
+      chs[ch].is_ef = chan_ef[ch];
+      chs[ch].li = chan_li[ch];
+      chs[ch].point = pts[ch];
+    }
+    BfChannelDev* d_chs = ar.get<BfChannelDev>(3);
+    std::vector<uint8_t>& hs = c->host_stage;
+    hs.assign((const uint8_t*)chs, (const uint8_t*)chs + sizeof(chs));
+    h2d(d_chs, hs.data(), sizeof(chs), st);
+    bf_combine_dev(d_chs, 3, d_fields + fp.coeffs, D, levels, st);
+    bf_levels_dev(levels, D, R, d_fields + fp.ch_batch, c->tw.as<u64>(), st);
+  }
   std::vector<u32*> lvl_nodes(R, nullptr);
   {
     std::vector<const u64*> ldata;
@@ -489,6 +528,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
       merkle_build_many(lnodes.data(), lcount.data(), (unsigned)lnodes.size(), st);
     }
   }
+  for (unsigned i = 0; i < nbr; ++i) LGS_CUDA(cudaStreamWaitEvent(st, c->ev_done[i], 0));
 
   // ---- gathers into staging ----------------------------------------------------------------
   {

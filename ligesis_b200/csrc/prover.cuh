@@ -70,7 +70,9 @@ struct Arena {
     if (off + b <= mem.bytes) {
       r = (T*)((char*)mem.p + off);
     } else {
+      // Grown mid-call: make the new block usable from every stream of the context at once.
       overflow.emplace_back(b, st);
+      LGS_CUDA(cudaStreamSynchronize(st));
       r = overflow.back().as<T>();
     }
     off += b;
@@ -142,8 +144,12 @@ struct StageTimer {
 }  // namespace lgs
 
 struct lgs_ctx {
+  static constexpr int NSIDE = 12;  // side streams for the independent branches of prove
   int device = 0;
   cudaStream_t st = nullptr;
+  cudaStream_t side[NSIDE] = {};
+  cudaEvent_t ev_done[NSIDE] = {};
+  cudaEvent_t ev_fork = nullptr;
   lgs::DevMem tw;
   lgs::Arena arena;
   lgs::Profiler prof;
