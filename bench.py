@@ -217,10 +217,18 @@ def run_ours(args) -> None:
     oracle = L.RandomOracle(0, length=8)
     oracle.fields, oracle.ints = fields, ints
 
+    host_ms = {"commit": 0.0, "prove": 0.0, "n": 0}
+
     def step_device():
         oracle.restart()
+        t0 = time.perf_counter()
         commit, data = L.Ligesis.commit_device(pk, f_dev.data_ptr(), f.size)
+        t1 = time.perf_counter()
         proof = L.Ligesis.prove(pk, data, z, oracle)
+        t2 = time.perf_counter()
+        host_ms["commit"] += (t1 - t0) * 1e3
+        host_ms["prove"] += (t2 - t1) * 1e3
+        host_ms["n"] += 1
         return commit, proof
 
     def step_e2e():
@@ -256,6 +264,7 @@ def run_ours(args) -> None:
         return ms, out
 
     launches0 = lib.lgs_launch_count()
+    host_ms.update(commit=0.0, prove=0.0, n=0)
     L._lib.check(lib.lgs_profile(ctx.handle, 1))
     with ClockSampler(local) as clk:
         dev_ms, (commit, proof) = timed(step_device, args.steps)
@@ -318,12 +327,143 @@ def run_ours(args) -> None:
         "e2e": {"value": round(e2e_ms / world, 3), "unit": "ms",
                 "h2d_bytes_per_step": int(f.nbytes), "d2h_bytes_per_step": len(proof.data) + 32},
         "stages_ms": {k: round(v, 4) for k, v in stages.items()},
+        "host_wall_ms": {k: round(host_ms[k] / max(host_ms["n"], 1), 4) for k in ("commit", "prove")},
         "roofline": roof,
         "cpu_baseline": cpu,
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "proof_bytes": len(proof.data), "proof_size_bytes_ref_accounting": proof.size_bytes(),
     }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------------
+# batched and served proving (not part of the default line)
+# ------------------------------------------------------------------------------------------------
+def _keys_for(mus, ctx):
+    import ligesis_b200 as L
+    from ligesis_b200 import rng
+    from ligesis_b200.workloads import shape_for_mu
+
+    keys = {}
+    for mu in sorted(set(mus)):
+        lm, ln = shape_for_mu(mu)
+        A = rng.field_elements(100 + lm, 32 * (64 << lm)).reshape(32, 64 << lm)  # one A per m
+        keys[mu] = L.Ligesis.setup_with_hash(lm, ln, L.SubsetSumHash(64 << lm, a=A), ctx)[0]
+    return keys
+
+
+def run_batch(args) -> None:
+    """96 polynomials of uneven size (mu = floor(14 + 8u)), each committed and opened at its own
+    point: one at a time on one context versus all through the engine's lanes."""
+    import ligesis_b200 as L
+    from ligesis_b200 import rng
+    from ligesis_b200.engine import ProverEngine
+    from ligesis_b200.workloads import batch_mus
+
+    mus = batch_mus(96)
+    ctx = L.Context(0)
+    keys = _keys_for(mus, ctx)
+    jobs = []
+    for i, mu in enumerate(mus):
+        f = rng.field_elements(1000 + i, 1 << mu)
+        z = rng.ext_elements(2000 + i, mu)
+        jobs.append((keys[mu], f, z, 3000 + i))
+
+    def plain():
+        out = []
+        for pk, f, z, os_ in jobs:
+            o = L.RandomOracle(os_, length=1024)
+            c, d = L.Ligesis.commit(pk, L.MlPoly(f))
+            out.append((c.root, L.Ligesis.prove(pk, d, z, o).data))
+        return out
+
+    def batched(eng):
+        res = eng.run([(pk, f, z, L.RandomOracle(os_, length=1024)) for pk, f, z, os_ in jobs])
+        return [(r.commit.root, r.proof.data) for r in res]
+
+    plain()  # warm-up: arenas and pools of every shape
+    t0 = time.perf_counter()
+    ref = plain()
+    t_plain = time.perf_counter() - t0
+    with ProverEngine(0, lanes=args.lanes) as eng:
+        batched(eng)
+        t0 = time.perf_counter()
+        got = batched(eng)
+        t_batch = time.perf_counter() - t0
+    line = {"mode": "batch", "jobs": len(jobs), "mu": [min(mus), max(mus)], "lanes": args.lanes,
+            "plain_proofs_per_s": round(len(jobs) / t_plain, 1),
+            "batched_proofs_per_s": round(len(jobs) / t_batch, 1),
+            "speedup": round(t_plain / t_batch, 2), "identical_proofs": got == ref,
+            "timing": "host wall clock, host f in, proof out (end to end)"}
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args) -> None:
+    """A Poisson stream of commit+eval requests (mean 200/s, mu in [14, 24], 10% GPT-2 layer
+    witnesses): latency percentiles and proofs/s for the one-at-a-time path (1 lane) and the
+    engine (many lanes), plus both when every request is queued at once (peak throughput)."""
+    import threading as th
+
+    import numpy as np
+
+    import ligesis_b200 as L
+    from ligesis_b200 import rng
+    from ligesis_b200.engine import ProverEngine
+    from ligesis_b200.workloads import gpt2_layer_witness, serve_stream
+
+    stream = serve_stream(args.requests, rate_per_s=args.rate)
+    mus = [mu for _, mu, _ in stream]
+    ctx = L.Context(0)
+    keys = _keys_for(mus, ctx)
+    f_by_mu = {mu: rng.field_elements(4000 + mu, 1 << mu) for mu in set(mus)}
+    gpt2 = gpt2_layer_witness()
+    reqs = []
+    for i, (t, mu, kind) in enumerate(stream):
+        f = gpt2 if kind == "gpt2" else f_by_mu[mu]
+        reqs.append((t, keys[mu], f, rng.ext_elements(5000 + i, mu), 6000 + i))
+
+    def drive(lanes: int, paced: bool):
+        with ProverEngine(0, lanes=lanes) as eng:
+            for _, pk, f, z, os_ in reqs[: 2 * lanes]:  # warm every lane
+                eng.wait(eng.submit(pk, f, z, L.RandomOracle(os_, length=1024)))
+            results = [None] * len(reqs)
+            tickets = [None] * len(reqs)
+            ready = th.Semaphore(0)
+
+            def collect():
+                for i in range(len(reqs)):
+                    ready.acquire()
+                    results[i] = eng.wait(tickets[i])
+
+            col = th.Thread(target=collect)
+            col.start()
+            start = time.perf_counter()
+            for i, (t, pk, f, z, os_) in enumerate(reqs):
+                if paced:
+                    delay = start + t - time.perf_counter()
+                    if delay > 0:
+                        time.sleep(delay)
+                tickets[i] = eng.submit(pk, f, z, L.RandomOracle(os_, length=1024))
+                ready.release()
+            col.join()
+            wall = time.perf_counter() - start
+        lat = np.array([r.latency_ms for r in results])
+        return {"proofs_per_s": round(len(reqs) / wall, 1),
+                "p50_ms": round(float(np.percentile(lat, 50)), 2),
+                "p99_ms": round(float(np.percentile(lat, 99)), 2)}, [r.proof.data for r in results]
+
+    plain_paced, ref = drive(1, True)
+    eng_paced, got = drive(args.lanes, True)
+    plain_peak, _ = drive(1, False)
+    eng_peak, got2 = drive(args.lanes, False)
+    line = {"mode": "serve", "requests": len(reqs), "arrival_rate_per_s": args.rate,
+            "mu": [min(mus), max(mus)], "gpt2_requests": sum(1 for r in stream if r[2] == "gpt2"),
+            "lanes": args.lanes, "plain": plain_paced, "served": eng_paced,
+            "plain_saturated": plain_peak, "served_saturated": eng_peak,
+            "throughput_ratio_saturated": round(eng_peak["proofs_per_s"] / plain_peak["proofs_per_s"], 2),
+            "identical_proofs": got == ref and got2 == ref,
+            "timing": "latency = engine clock from submission (arrival) to proof; host f in"}
     print(json.dumps(line), flush=True)
 
 
@@ -334,9 +474,19 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", choices=["line", "batch", "serve"], default="line")
+    ap.add_argument("--lanes", type=int, default=8)
+    ap.add_argument("--requests", type=int, default=600)
+    ap.add_argument("--rate", type=float, default=200.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.mode == "batch":
+        run_batch(args)
+        return
+    if args.mode == "serve":
+        run_serve(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

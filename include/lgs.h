@@ -81,6 +81,45 @@ lgs_status lgs_verify(unsigned log_m, unsigned log_n, const uint8_t com_a[32],
                       size_t nfields, const uint64_t* ints, size_t nints, uint64_t cursors[2],
                       int* accept);
 
+/* ---- batched and served proving (the reference proves one polynomial at a time on one
+ * thread, pcs/benches/ligesis.rs:20-60) ----
+ * An engine owns `lanes` contexts on one device, each driven by its own host thread, so the
+ * commits and proofs of many jobs of uneven sizes run on the GPU together.  A queued job starts
+ * when a lane is free and its device-memory estimate fits the HBM budget (FIFO).  Every job runs
+ * the same lgs_commit + lgs_prove computation, so its root and proof are byte-identical to the
+ * one-at-a-time path.  The job's host buffers and its proving key must stay alive and unchanged
+ * until the job has been waited for. */
+typedef struct lgs_engine lgs_engine;
+typedef struct {
+  const lgs_pk* pk;
+  const uint64_t* f; /* host, 2^(log_m+log_n) BF */
+  size_t len;
+  const uint64_t* z; /* log_m + log_n EF */
+  size_t zlen;
+  const uint64_t* fields; /* RandomOracle arrays and the cursors this proof starts at */
+  size_t nfields;
+  const uint64_t* ints;
+  size_t nints;
+  uint64_t cursors[2];
+} lgs_job;
+typedef struct {
+  lgs_status status;
+  uint8_t root[32];
+  uint8_t* proof; /* owned by the caller after lgs_engine_wait: lgs_engine_free_proof */
+  size_t proof_len;
+  uint64_t cursors[2]; /* advanced cursors */
+  double submit_ms, start_ms, done_ms; /* engine clock (ms since lgs_engine_create) */
+} lgs_result;
+/* hbm_budget 0: 90% of the device memory free at creation. */
+lgs_status lgs_engine_create(int device, unsigned lanes, size_t hbm_budget, lgs_engine** out);
+void lgs_engine_destroy(lgs_engine* e);
+lgs_status lgs_engine_submit(lgs_engine* e, const lgs_job* job, uint64_t* ticket);
+/* Blocks until the job is done (timeout_ms < 0: no limit); the ticket is then released. */
+lgs_status lgs_engine_wait(lgs_engine* e, uint64_t ticket, double timeout_ms, lgs_result* out);
+void lgs_engine_free_proof(uint8_t* proof);
+/* Jobs waiting for a lane, and the device bytes reserved by running jobs. */
+lgs_status lgs_engine_pending(lgs_engine* e, size_t* queued, size_t* running_bytes);
+
 /* ---- measurement (no counterpart in the reference, whose benches use wall-clock timers,
  * pcs/benches/ligesis.rs:27-45) ---- */
 

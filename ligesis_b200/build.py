@@ -21,7 +21,7 @@ INCLUDE = PKG.parent / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
     "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
-    "--expt-relaxed-constexpr", "-I", str(CSRC), "-I", str(INCLUDE),
+    "--expt-relaxed-constexpr", "-Xcompiler", "-pthread", "-I", str(CSRC), "-I", str(INCLUDE),
 ]
 
 
@@ -66,7 +66,8 @@ def build(verbose: bool = False, force: bool = False, extra: list[str] | None = 
         for f in futs:
             f.result()
     if todo or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
-        cmd = [nvcc, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", str(LIB), *map(str, objs)]
+        cmd = [nvcc, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", str(LIB), *map(str, objs),
+               "-lpthread"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")

@@ -10,6 +10,7 @@
 
 namespace lgs {
 lgs_status set_error(lgs_status s, const std::string& msg);
+lgs_status status_of_current_exception();
 void ctx_init(lgs_ctx* c, int device);
 void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lgs_pk* pk);
 void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device, lgs_commit_data* cd);
@@ -37,11 +38,12 @@ lgs_status fail(lgs_status s, const std::string& m) {
   return s;
 }
 
-template <class F>
-lgs_status guarded(F&& f) {
+}  // namespace
+
+// Map the exception being handled to a status and record its message (call inside a catch).
+lgs_status lgs::status_of_current_exception() {
   try {
-    f();
-    return LGS_OK;
+    throw;
   } catch (const ShapeError& e) {
     return fail(LGS_ERR_BAD_SHAPE, e.what());
   } catch (const OracleError& e) {
@@ -60,6 +62,17 @@ lgs_status guarded(F&& f) {
     return fail(LGS_ERR_INTERNAL, e.what());
   } catch (...) {
     return fail(LGS_ERR_INTERNAL, "unknown exception");
+  }
+}
+
+namespace {
+template <class F>
+lgs_status guarded(F&& f) {
+  try {
+    f();
+    return LGS_OK;
+  } catch (...) {
+    return lgs::status_of_current_exception();
   }
 }
 
@@ -111,6 +124,14 @@ lgs_status lgs_ctx_create(int device, unsigned flags, lgs_ctx** out) {
 void lgs_ctx_destroy(lgs_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
+  if (ctx->st) cudaStreamSynchronize(ctx->st);
+  // Release the context's own device memory while its stream still exists (the frees are
+  // ordered on it), then drain and destroy the streams.
+  ctx->prof.flush();
+  ctx->arena.overflow.clear();
+  ctx->arena.mem.release();
+  ctx->tw.release();
+  ctx->err.release();
   if (ctx->st) cudaStreamSynchronize(ctx->st);
   for (int i = 0; i < lgs_ctx::NSIDE; ++i) {
     if (ctx->side[i]) {

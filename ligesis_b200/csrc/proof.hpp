@@ -166,22 +166,33 @@ inline std::vector<uint64_t> multiproof_nodes(std::vector<uint64_t> cur, uint64_
 
 // ---- encoding ----
 struct ByteWriter {
+  // Little-endian hosts only (x86-64, aarch64): integers are copied in memory order.
+  static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "proof encoding assumes little-endian");
   std::vector<uint8_t> b;
-  void u32v(uint32_t v) {
-    for (int i = 0; i < 4; ++i) b.push_back((uint8_t)(v >> (8 * i)));
+  size_t n = 0;
+  void need(size_t k) {
+    if (n + k > b.size()) b.resize(std::max<size_t>(2 * b.size(), n + k + (1 << 16)));
   }
-  void u64v(uint64_t v) {
-    for (int i = 0; i < 8; ++i) b.push_back((uint8_t)(v >> (8 * i)));
+  void raw(const void* p, size_t k) {
+    need(k);
+    std::memcpy(b.data() + n, p, k);
+    n += k;
+  }
+  void u32v(uint32_t v) { raw(&v, 4); }
+  void u64v(uint64_t v) { raw(&v, 8); }
+  std::vector<uint8_t> finish() {
+    b.resize(n);
+    return std::move(b);
   }
   void bf(u64 v) { u64v(gl_canon(v)); }
   void ef(const ef2& e) {
     bf(e.c0);
     bf(e.c1);
   }
-  void h32(const Hash32& h) { b.insert(b.end(), h.b, h.b + 32); }
+  void h32(const Hash32& h) { raw(h.b, 32); }
   void bytes(const std::vector<uint8_t>& v) {
     u32v((uint32_t)v.size());
-    b.insert(b.end(), v.begin(), v.end());
+    raw(v.data(), v.size());
   }
   void val(u64 v) { bf(v); }
   void val(const ef2& v) { ef(v); }
@@ -207,7 +218,7 @@ struct ByteWriter {
 
 inline std::vector<uint8_t> encode_proof(const ProofH& p) {
   ByteWriter w;
-  w.b = {'L', 'G', 'S', 'P'};
+  w.raw("LGSP", 4);
   w.u32v(1);
   w.ef(p.y);
   w.h32(p.com_a_vec);
@@ -238,7 +249,7 @@ inline std::vector<uint8_t> encode_proof(const ProofH& p) {
   for (auto& o : b.base_bf) w.opening(o);
   w.u32v((uint32_t)b.base_ef.size());
   for (auto& o : b.base_ef) w.opening(o);
-  return w.b;
+  return w.finish();
 }
 
 struct ByteReader {

@@ -3,6 +3,7 @@
 // open (pcs/src/basefold.rs:648-856).  Every challenge of the pre-drawn oracle is known before
 // the first kernel runs, so `prove` uploads one parameter block, enqueues the whole dataflow on
 // the context stream, and reads back one staging buffer from which the proof is assembled.
+#include <mutex>
 #include <cstring>
 
 #include "prover.cuh"
@@ -52,6 +53,22 @@ Hash32 read_root(const u32* nodes, size_t nleaves, cudaStream_t st) {
 
 }  // namespace
 
+cudaStream_t release_stream(int device) {
+  static std::mutex mu;
+  static std::vector<cudaStream_t> streams;
+  std::lock_guard<std::mutex> lk(mu);
+  if (device < 0) throw std::runtime_error("release_stream: bad device");
+  if ((size_t)device >= streams.size()) streams.resize(device + 1, nullptr);
+  if (!streams[device]) {
+    int prev = 0;
+    LGS_CUDA(cudaGetDevice(&prev));
+    LGS_CUDA(cudaSetDevice(device));
+    LGS_CUDA(cudaStreamCreateWithFlags(&streams[device], cudaStreamNonBlocking));
+    LGS_CUDA(cudaSetDevice(prev));
+  }
+  return streams[device];
+}
+
 void ctx_init(lgs_ctx* c, int device) {
   c->device = device;
   LGS_CUDA(cudaSetDevice(device));
@@ -84,16 +101,20 @@ void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lg
   const size_t W = s.W(), len = (size_t)DIGEST_ROWS * W;
   c->arena.begin();
   pk->A.alloc(len * 8, c->st);
+  pk->A.detach(release_stream(c->device));
   std::vector<u64> canon(A_host, A_host + len);
   for (auto& x : canon) x = gl_canon(x);
   h2d(pk->A.p, canon.data(), len * 8, c->st);
   pk->alimb.alloc(len * 8, c->st);
+  pk->alimb.detach(release_stream(c->device));
   alimb_from_a(pk->A.as<u64>(), pk->alimb.as<uint8_t>(), W, c->st);
   make_alimb_tmap(pk->alimb.as<uint8_t>(), W, pk->tmap);
   const unsigned li = s.li(s.na());
   const size_t L = (len >> li) << CODE_RATE;
   pk->a_codes.alloc(L * ((size_t)1 << li) * 8, c->st);
+  pk->a_codes.detach(release_stream(c->device));
   pk->a_nodes.alloc((2 * L - 1) * 32, c->st);
+  pk->a_nodes.detach(release_stream(c->device));
   pk->a_state.codes = pk->a_codes.as<u64>();
   pk->a_state.nodes = pk->a_nodes.as<u32>();
   bf_commit(c, pk->A.as<u64>(), 0, len, li, &pk->a_state, c->st);
@@ -109,10 +130,22 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
   if (two_n % 128) throw ShapeError("commit: 2n must be a multiple of 128");
   cd->shape = s;
   c->arena.begin();
-  if (cd->f.bytes != m * n * 8) cd->f.alloc(m * n * 8, c->st);
-  if (cd->cw.bytes != m * two_n * 8) cd->cw.alloc(m * two_n * 8, c->st);
-  if (cd->H.bytes != DIGEST_ROWS * two_n * 8) cd->H.alloc(DIGEST_ROWS * two_n * 8, c->st);
-  if (cd->nodes.bytes != (2 * two_n - 1) * 32) cd->nodes.alloc((2 * two_n - 1) * 32, c->st);
+  if (cd->f.bytes != m * n * 8) {
+    cd->f.alloc(m * n * 8, c->st);
+    cd->f.detach(release_stream(c->device));
+  }
+  if (cd->cw.bytes != m * two_n * 8) {
+    cd->cw.alloc(m * two_n * 8, c->st);
+    cd->cw.detach(release_stream(c->device));
+  }
+  if (cd->H.bytes != DIGEST_ROWS * two_n * 8) {
+    cd->H.alloc(DIGEST_ROWS * two_n * 8, c->st);
+    cd->H.detach(release_stream(c->device));
+  }
+  if (cd->nodes.bytes != (2 * two_n - 1) * 32) {
+    cd->nodes.alloc((2 * two_n - 1) * 32, c->st);
+    cd->nodes.detach(release_stream(c->device));
+  }
   {
     StageTimer t(c->prof, c->st, "commit_upload");
     if (f_on_device)

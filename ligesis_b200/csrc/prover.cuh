@@ -14,6 +14,10 @@ namespace lgs {
 // Device buffer from the device's stream-ordered memory pool (cudaMallocAsync on the owning
 // context's stream).  The pool keeps freed memory cached (the context raises its release
 // threshold), so a commitment allocated and freed per proof costs no cudaMalloc / device sync.
+// A non-blocking stream per device that lives as long as the process: the stream on which
+// buffers that outlive their context are freed.
+cudaStream_t release_stream(int device);
+
 struct DevMem {
   void* p = nullptr;
   size_t bytes = 0;
@@ -31,6 +35,11 @@ struct DevMem {
     p = nullptr;
     bytes = 0;
   }
+  // For buffers that may outlive the context that allocated them (proving keys, commitment
+  // data): free them on `s` (release_stream) instead of the context's stream.  Every API call
+  // synchronises its streams before returning, so no work of the owning context still uses the
+  // buffer when it is freed.
+  void detach(cudaStream_t s) { st = s; }
   ~DevMem() { release(); }
   DevMem(const DevMem&) = delete;
   DevMem& operator=(const DevMem&) = delete;
