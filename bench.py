@@ -23,7 +23,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -121,56 +120,62 @@ def run_reference(args) -> None:
 # clocks during the timed region
 # ------------------------------------------------------------------------------------------------
 class ClockSampler:
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event reasons of one GPU, read through NVML every ~2 ms on a thread
+    while the timed region runs (read-only queries; nothing about the GPU is changed)."""
 
-    def __init__(self, device: int):
-        self.device = device
-        self.rows: list[list[str]] = []
-        self.proc = None
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
+
+    def __init__(self, device: int, period_s: float = 0.002):
+        self.device, self.period = device, period_s
+        self.sm: list[float] = []
+        self.mask = 0
+        self.max_mhz = None
+        self._stop = threading.Event()
         self._t = None
+        self._nv = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self._t = threading.Thread(target=self._read, daemon=True)
+            import pynvml as nv
+
+            nv.nvmlInit()
+            self._nv = nv
+            self._h = nv.nvmlDeviceGetHandleByIndex(self.device)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self._h, nv.NVML_CLOCK_SM))
+            self._t = threading.Thread(target=self._run, daemon=True)
             self._t.start()
-        except OSError:
-            self.proc = None
+        except Exception:
+            self._nv = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.rows.append([c.strip() for c in line.split(",")])
+    def _run(self):
+        nv = self._nv
+        reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self._stop.is_set():
+            try:
+                self.sm.append(float(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM)))
+                self.mask |= int(reasons(self._h))
+            except Exception:
+                return
+            time.sleep(self.period)
 
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=2)
+        if self._nv:
             try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-            if self._t:
-                self._t.join(timeout=2)
+                self._nv.nvmlShutdown()
+            except Exception:
+                pass
 
     def summary(self) -> dict:
-        sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
-            try:
-                sm.append(float(r[1]))
-                mx = max(mx, float(r[2]))
-                for i, nm in enumerate(names):
-                    if r[5 + i].lower().startswith("active"):
-                        reasons.add(nm)
-            except (ValueError, IndexError):
-                continue
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.sm) if self.sm else None,
+                "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(k for k, bit in self.REASONS.items() if self.mask & bit),
+                "samples": len(self.sm)}
 
 
 # ------------------------------------------------------------------------------------------------
@@ -272,11 +277,13 @@ def run_ours(args) -> None:
     stages = {}
     import ctypes as C
 
-    for name in ("commit_upload", "rs_encode", "subset_sum_hash", "merkle_h", "prove_device"):
+    host_phases = {}
+    for name in ("commit_upload", "rs_encode", "subset_sum_hash", "merkle_h", "prove_device",
+                 "host_plan", "host_enqueue", "host_wait", "host_assemble"):
         tot, cnt = C.c_double(), C.c_uint64()
         L._lib.check(lib.lgs_profile_get(ctx.handle, name.encode(), C.byref(tot), C.byref(cnt)))
         if cnt.value:
-            stages[name] = tot.value / cnt.value
+            (host_phases if name.startswith("host_") else stages)[name] = tot.value / cnt.value
     L._lib.check(lib.lgs_profile(ctx.handle, 0))
     e2e_ms, (commit2, proof2) = timed(step_e2e, args.steps)
     assert commit2.root == commit.root and proof2.data == proof.data, "e2e result differs"
@@ -328,6 +335,7 @@ def run_ours(args) -> None:
                 "h2d_bytes_per_step": int(f.nbytes), "d2h_bytes_per_step": len(proof.data) + 32},
         "stages_ms": {k: round(v, 4) for k, v in stages.items()},
         "host_wall_ms": {k: round(host_ms[k] / max(host_ms["n"], 1), 4) for k in ("commit", "prove")},
+        "prove_host_phases_ms": {k[5:]: round(v, 4) for k, v in host_phases.items()},
         "roofline": roof,
         "cpu_baseline": cpu,
         "gpu_launches": int(launches),
@@ -387,6 +395,7 @@ def run_batch(args) -> None:
     ref = plain()
     t_plain = time.perf_counter() - t0
     with ProverEngine(0, lanes=args.lanes) as eng:
+        eng.prepare(keys.values())
         batched(eng)
         t0 = time.perf_counter()
         got = batched(eng)
@@ -425,6 +434,7 @@ def run_serve(args) -> None:
 
     def drive(lanes: int, paced: bool):
         with ProverEngine(0, lanes=lanes) as eng:
+            eng.prepare(keys.values())
             for _, pk, f, z, os_ in reqs[: 2 * lanes]:  # warm every lane
                 eng.wait(eng.submit(pk, f, z, L.RandomOracle(os_, length=1024)))
             results = [None] * len(reqs)
@@ -470,7 +480,7 @@ def run_serve(args) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -117,6 +117,11 @@ lgs_status lgs_engine_submit(lgs_engine* e, const lgs_job* job, uint64_t* ticket
 /* Blocks until the job is done (timeout_ms < 0: no limit); the ticket is then released. */
 lgs_status lgs_engine_wait(lgs_engine* e, uint64_t ticket, double timeout_ms, lgs_result* out);
 void lgs_engine_free_proof(uint8_t* proof);
+/* Warm every lane for the given proving keys' shapes before serving: one eager commit + prove
+ * of each shape sizes the lane's scratch and pinned buffers, a second captures the shape's prove
+ * into a CUDA graph that later jobs of that shape replay.  Synthetic inputs; nothing is returned.
+ * Call with no job queued or running (else LGS_ERR_BAD_ARG).  No reference counterpart. */
+lgs_status lgs_engine_prepare(lgs_engine* e, const lgs_pk* const* pks, size_t npk);
 /* Jobs waiting for a lane, and the device bytes reserved by running jobs. */
 lgs_status lgs_engine_pending(lgs_engine* e, size_t* queued, size_t* running_bytes);
 

@@ -9,14 +9,6 @@
 #include "prover.cuh"
 
 namespace lgs {
-lgs_status set_error(lgs_status s, const std::string& msg);
-lgs_status status_of_current_exception();
-void ctx_init(lgs_ctx* c, int device);
-void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lgs_pk* pk);
-void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device, lgs_commit_data* cd);
-void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u64* z_host,
-               size_t zlen, const u64* fields_host, size_t nfields, const uint64_t* ints_host,
-               size_t nints, uint64_t cursors[2], std::vector<uint8_t>* proof_out);
 int verify_host(unsigned log_m, unsigned log_n, const Hash32& com_a, const Hash32& root,
                 const u64* z_in, size_t zlen, const uint8_t* proof, size_t proof_len,
                 const u64* fields, size_t nfields, const uint64_t* ints, size_t nints,
@@ -28,7 +20,13 @@ using namespace lgs;
 namespace {
 std::atomic<uint64_t> g_launches{0};
 }
-void lgs::count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+thread_local uint64_t t_launches = 0;
+void lgs::count_launch() {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  ++t_launches;
+}
+uint64_t lgs::thread_launches() { return t_launches; }
+void lgs::adjust_launches(int64_t n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
 
 namespace {
 thread_local std::string g_err;
@@ -140,6 +138,11 @@ void lgs_ctx_destroy(lgs_ctx* ctx) {
     }
     if (ctx->ev_done[i]) cudaEventDestroy(ctx->ev_done[i]);
   }
+  for (int i = 0; i < lgs_ctx::RING; ++i)
+    if (ctx->ring_ev[i]) cudaEventDestroy(ctx->ring_ev[i]);
+  for (auto& g : ctx->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  ctx->graphs.clear();
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->st) cudaStreamDestroy(ctx->st);
   delete ctx;

@@ -44,6 +44,8 @@ struct DeviceTimeout : std::runtime_error {
 
 // Process-wide count of kernels this library has launched (lgs_launch_count()).
 void count_launch();
+uint64_t thread_launches();      // launches counted by the calling host thread
+void adjust_launches(int64_t n);  // graph replays add their kernels; captures remove theirs
 
 inline unsigned ilog2(uint64_t x) {
   unsigned k = 0;

@@ -18,16 +18,6 @@
 #include "../../include/lgs.h"
 #include "prover.cuh"
 
-namespace lgs {
-void ctx_init(lgs_ctx* c, int device);
-void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device, lgs_commit_data* cd);
-void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u64* z_host,
-               size_t zlen, const u64* fields_host, size_t nfields, const uint64_t* ints_host,
-               size_t nints, uint64_t cursors[2], std::vector<uint8_t>* proof_out);
-lgs_status set_error(lgs_status s, const std::string& msg);
-lgs_status status_of_current_exception();
-}  // namespace lgs
-
 namespace {
 struct EngineJob {
   lgs_job in;
@@ -49,6 +39,7 @@ struct lgs_engine {
   std::unordered_map<uint64_t, EngineJob*> jobs;
   uint64_t next_ticket = 1;
   bool stop = false;
+  bool preparing = false;  // lgs_engine_prepare owns the lanes
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
   double now_ms() const {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -67,12 +58,14 @@ size_t job_estimate(const lgs_pk* pk) {
 
 void run_job(lgs_ctx* lane, EngineJob* j) {
   lgs_commit_data cd;
-  lgs::commit_dev(lane, j->in.pk, j->in.f, false, &cd);
-  std::memcpy(j->res.root, cd.root.b, 32);
+  // The commit is only enqueued: the prove's single synchronisation completes both.
+  lgs::commit_dev(lane, j->in.pk, j->in.f, false, &cd, false);
   uint64_t cur[2] = {j->in.cursors[0], j->in.cursors[1]};
   std::vector<uint8_t> proof;
   lgs::prove_dev(lane, j->in.pk, &cd, j->in.z, j->in.zlen, j->in.fields, j->in.nfields, j->in.ints,
                  j->in.nints, cur, &proof);
+  lgs::commit_finish(lane, &cd);
+  std::memcpy(j->res.root, cd.root.b, 32);
   j->res.proof = (uint8_t*)std::malloc(proof.size() ? proof.size() : 1);
   if (!j->res.proof) throw std::bad_alloc();
   std::memcpy(j->res.proof, proof.data(), proof.size());
@@ -89,7 +82,7 @@ void worker_main(lgs_engine* e, size_t lane_idx) {
     {
       std::unique_lock<std::mutex> lk(e->mu);
       e->cv_work.wait(lk, [&] {
-        return e->stop || (!e->queue.empty() &&
+        return e->stop || (!e->preparing && !e->queue.empty() &&
                            (e->in_use == 0 || e->in_use + e->queue.front()->est <= e->budget));
       });
       if (e->stop) return;
@@ -137,6 +130,7 @@ lgs_status lgs_engine_create(int device, unsigned lanes, size_t hbm_budget, lgs_
       auto* c = new lgs_ctx;
       e->lanes.push_back(c);
       lgs::ctx_init(c, device);
+      c->copy_pool = false;  // the lanes already copy in parallel
     }
     for (unsigned i = 0; i < lanes; ++i) e->workers.emplace_back(worker_main, e, (size_t)i);
   } catch (...) {
@@ -206,6 +200,69 @@ lgs_status lgs_engine_wait(lgs_engine* e, uint64_t ticket, double timeout_ms, lg
 }
 
 void lgs_engine_free_proof(uint8_t* proof) { std::free(proof); }
+
+lgs_status lgs_engine_prepare(lgs_engine* e, const lgs_pk* const* pks, size_t npk) {
+  if (!e || (npk && !pks)) return lgs::set_error(LGS_ERR_BAD_ARG, "lgs_engine_prepare: null argument");
+  for (size_t i = 0; i < npk; ++i)
+    if (!pks[i]) return lgs::set_error(LGS_ERR_BAD_ARG, "lgs_engine_prepare: null proving key");
+  {
+    std::lock_guard<std::mutex> lk(e->mu);
+    if (!e->queue.empty() || e->in_use != 0 || e->preparing)
+      return lgs::set_error(LGS_ERR_BAD_ARG, "lgs_engine_prepare: jobs are queued or running");
+    e->preparing = true;
+  }
+  lgs_status st = LGS_OK;
+  try {
+    // Synthetic inputs shared by every lane: a zero polynomial of the largest shape, a zero
+    // point, distinct oracle ints (so column sampling succeeds) and nonzero fields.
+    size_t max_len = 0;
+    unsigned max_vars = 0;
+    for (size_t i = 0; i < npk; ++i) {
+      max_len = std::max(max_len, pks[i]->shape.m() * pks[i]->shape.n());
+      max_vars = std::max(max_vars, pks[i]->shape.log_m + pks[i]->shape.log_n);
+    }
+    const std::vector<lgs::u64> f(max_len, 0), z(2 * (size_t)max_vars, 0);
+    size_t nfields = 0;
+    for (size_t i = 0; i < npk; ++i) nfields = std::max<size_t>(nfields, lgs::FieldPlan(pks[i]->shape).total);
+    std::vector<lgs::u64> fields(2 * nfields);
+    for (size_t i = 0; i < fields.size(); ++i) fields[i] = i + 1;
+    std::vector<uint64_t> ints(lgs::INTS_PER_PROOF);
+    for (size_t i = 0; i < ints.size(); ++i) ints[i] = i;
+    std::vector<lgs_status> lane_st(e->lanes.size(), LGS_OK);
+    std::vector<std::thread> th;
+    for (size_t l = 0; l < e->lanes.size(); ++l)
+      th.emplace_back([&, l] {
+        try {
+          LGS_CUDA(cudaSetDevice(e->device));
+          lgs_ctx* lane = e->lanes[l];
+          for (int pass = 0; pass < 2; ++pass)  // sizes everything, then captures
+            for (size_t i = 0; i < npk; ++i) {
+              const lgs::Shape& s = pks[i]->shape;
+              lgs_commit_data cd;
+              lgs::commit_dev(lane, pks[i], f.data(), false, &cd, false);
+              uint64_t cur[2] = {0, 0};
+              std::vector<uint8_t> proof;
+              lgs::prove_dev(lane, pks[i], &cd, z.data(), s.log_m + s.log_n, fields.data(),
+                             nfields, ints.data(), ints.size(), cur, &proof);
+              lgs::commit_finish(lane, &cd);
+            }
+        } catch (...) {
+          lane_st[l] = lgs::status_of_current_exception();
+        }
+      });
+    for (auto& t : th) t.join();
+    for (lgs_status s : lane_st)
+      if (s != LGS_OK) st = s;
+  } catch (...) {
+    st = lgs::status_of_current_exception();
+  }
+  {
+    std::lock_guard<std::mutex> lk(e->mu);
+    e->preparing = false;
+  }
+  e->cv_work.notify_all();
+  return st;
+}
 
 lgs_status lgs_engine_pending(lgs_engine* e, size_t* queued, size_t* running_bytes) {
   if (!e || !queued || !running_bytes) return lgs::set_error(LGS_ERR_BAD_ARG, "null argument");

@@ -185,10 +185,12 @@ void eq_dot_dev(const void* vec, int is_bf, const ef2* point, unsigned k, ef2* o
 
 // ---- a-bar = eq_{z1}^T F (pcs/src/ligesis.rs:372-379) --------------------------------------
 // Two adjacent columns per thread (16-byte loads), four rows in flight with independent sums.
-__global__ void gemv_eq_rows_kernel(const u64* __restrict__ f, const ef2* __restrict__ eq,
-                                    size_t m, size_t n, ef2* __restrict__ out) {
+__global__ void gemv_eq_rows_kernel(const u64* const* __restrict__ fref,
+                                    const ef2* __restrict__ eq, size_t m, size_t n,
+                                    ef2* __restrict__ out) {
   const size_t j = 2 * ((size_t)blockIdx.x * blockDim.x + threadIdx.x);
   if (j >= n) return;
+  const u64* __restrict__ f = *fref;
   ef2 a0[4], a1[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) a0[q] = a1[q] = ef_zero();
@@ -212,9 +214,10 @@ __global__ void gemv_eq_rows_kernel(const u64* __restrict__ f, const ef2* __rest
   out[j] = ef_add(ef_add(a0[0], a0[1]), ef_add(a0[2], a0[3]));
   out[j + 1] = ef_add(ef_add(a1[0], a1[1]), ef_add(a1[2], a1[3]));
 }
-void gemv_eq_rows(const u64* f, const ef2* eq, size_t m, size_t n, ef2* out, cudaStream_t st) {
+void gemv_eq_rows(const u64* const* fref, const ef2* eq, size_t m, size_t n, ef2* out,
+                  cudaStream_t st) {
   if (n % 2) throw ShapeError("gemv: n must be even");
-  gemv_eq_rows_kernel<<<cdiv(n / 2, 256), 256, 0, st>>>(f, eq, m, n, out);
+  gemv_eq_rows_kernel<<<cdiv(n / 2, 256), 256, 0, st>>>(fref, eq, m, n, out);
   LGS_LAUNCH_CHECK();
 }
 
@@ -271,34 +274,37 @@ void lift_bf(const u64* in, ef2* out, size_t n, u64 minus, cudaStream_t st) {
 }
 
 // ---- B_I: bi[i*s + k] = bit (i % 64) of F'[i / 64][idx[k]] (pcs/src/ligesis.rs:403-410) -----
-__global__ void bits_gather_kernel(const u64* __restrict__ cw, size_t two_n,
+__global__ void bits_gather_kernel(const u64* const* __restrict__ cwref, size_t two_n,
                                    const uint64_t* __restrict__ idx, unsigned s, size_t rows,
                                    u64* __restrict__ bi) {
   size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= rows * s) return;
+  const u64* __restrict__ cw = *cwref;
   size_t q = t / s;
   unsigned k = (unsigned)(t % s);
   u64 word = cw[q * two_n + idx[k]];
   for (unsigned b = 0; b < 64; ++b) bi[(q * 64 + b) * s + k] = (word >> b) & 1;
 }
-void bits_gather(const u64* cw, size_t two_n, const uint64_t* idx, unsigned s, size_t W,
-                 u64* bi, cudaStream_t st) {
+void bits_gather(const u64* const* cwref, size_t two_n, const uint64_t* idx, unsigned s,
+                 size_t W, u64* bi, cudaStream_t st) {
   size_t rows = W / 64;
-  bits_gather_kernel<<<cdiv(rows * s, 128), 128, 0, st>>>(cw, two_n, idx, s, rows, bi);
+  bits_gather_kernel<<<cdiv(rows * s, 128), 128, 0, st>>>(cwref, two_n, idx, s, rows, bi);
   LGS_LAUNCH_CHECK();
 }
 
 // g1 = eq_{alpha2}^T A (pcs/src/ligesis.rs:436-444)
-__global__ void g1_kernel(const u64* __restrict__ A, size_t W, const ef2* __restrict__ eq,
-                          unsigned C, ef2* __restrict__ g1) {
+__global__ void g1_kernel(const u64* const* __restrict__ aref, size_t W,
+                          const ef2* __restrict__ eq, unsigned C, ef2* __restrict__ g1) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= W) return;
+  const u64* __restrict__ A = *aref;
   ef2 acc = ef_zero();
   for (unsigned r = 0; r < C; ++r) acc = ef_add(acc, ef_scale(eq[r], A[(size_t)r * W + i]));
   g1[i] = acc;
 }
-void g1_build(const u64* A, size_t W, const ef2* eq_a2, unsigned C, ef2* g1, cudaStream_t st) {
-  g1_kernel<<<cdiv(W, 256), 256, 0, st>>>(A, W, eq_a2, C, g1);
+void g1_build(const u64* const* aref, size_t W, const ef2* eq_a2, unsigned C, ef2* g1,
+              cudaStream_t st) {
+  g1_kernel<<<cdiv(W, 256), 256, 0, st>>>(aref, W, eq_a2, C, g1);
   LGS_LAUNCH_CHECK();
 }
 // g2[i] = sum_k eq_{r2}[k] B[i][idx[k]] (pcs/src/ligesis.rs:445-455); one warp per i.
@@ -422,7 +428,7 @@ void bf_combine_dev(const BfChannelDev* chs_dev, unsigned nch, const ef2* coeffs
 }
 
 // m = poly.fold(point[0..li]) (pcs/src/basefold.rs:667-668): m[t] = sum_j eq4[j] poly[t 2^li + j].
-__global__ void bf_fold_poly_kernel(const u64* __restrict__ poly, int is_ef, unsigned li,
+__global__ void bf_fold_poly_kernel(const u64* const* __restrict__ pref, int is_ef, unsigned li,
                                     const ef2* __restrict__ point, size_t out_len,
                                     ef2* __restrict__ m) {
   __shared__ ef2 pts[8];
@@ -432,6 +438,7 @@ __global__ void bf_fold_poly_kernel(const u64* __restrict__ poly, int is_ef, uns
   eq_table_smem(pts, li, wts);
   size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= out_len) return;
+  const u64* __restrict__ poly = *pref;
   const unsigned L = 1u << li;
   ef2 acc = ef_zero();
   if (is_ef) {
@@ -443,10 +450,10 @@ __global__ void bf_fold_poly_kernel(const u64* __restrict__ poly, int is_ef, uns
   }
   m[t] = acc;
 }
-void bf_fold_poly_dev(const u64* poly, int is_ef, unsigned li, const ef2* point, size_t out_len,
-                      ef2* m, cudaStream_t st) {
+void bf_fold_poly_dev(const u64* const* pref, int is_ef, unsigned li, const ef2* point,
+                      size_t out_len, ef2* m, cudaStream_t st) {
   if (li > 6) throw ShapeError("basefold: log_interleave above 6");
-  bf_fold_poly_kernel<<<cdiv(out_len, 256), 256, 0, st>>>(poly, is_ef, li, point, out_len, m);
+  bf_fold_poly_kernel<<<cdiv(out_len, 256), 256, 0, st>>>(pref, is_ef, li, point, out_len, m);
   LGS_LAUNCH_CHECK();
 }
 

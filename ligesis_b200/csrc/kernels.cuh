@@ -65,11 +65,15 @@ size_t eqdot_partials_elems(unsigned k);
 // out = sum_i vec[i] * eq_point(i); vec is EF (is_bf = 0) or BF (is_bf = 1).
 void eq_dot_dev(const void* vec, int is_bf, const ef2* point, unsigned k, ef2* out,
                 ef2* partials, cudaStream_t st);
-void gemv_eq_rows(const u64* f, const ef2* eq, size_t m, size_t n, ef2* out, cudaStream_t st);
+// The next four read their source address from device memory (`*ref`), so a launch captured in
+// a graph reads whichever buffer the slot names when it runs.
+void gemv_eq_rows(const u64* const* fref, const ef2* eq, size_t m, size_t n, ef2* out,
+                  cudaStream_t st);
 void lift_bf(const u64* in, ef2* out, size_t n, u64 minus, cudaStream_t st);
-void bits_gather(const u64* cw, size_t two_n, const uint64_t* idx, unsigned s, size_t W,
-                 u64* bi, cudaStream_t st);
-void g1_build(const u64* A, size_t W, const ef2* eq_a2, unsigned C, ef2* g1, cudaStream_t st);
+void bits_gather(const u64* const* cwref, size_t two_n, const uint64_t* idx, unsigned s,
+                 size_t W, u64* bi, cudaStream_t st);
+void g1_build(const u64* const* aref, size_t W, const ef2* eq_a2, unsigned C, ef2* g1,
+              cudaStream_t st);
 void g2_build(const u64* bi, size_t W, unsigned s, const ef2* eq_r2, ef2* g2, cudaStream_t st);
 void v_build(const ef2* eqz1, size_t W, ef2* v, cudaStream_t st);
 void y4_dev(const ef2* eq_r2, const ef2* ra, const uint64_t* idx, unsigned s, ef2* out,
@@ -88,8 +92,8 @@ struct BfChannelDev {
 };
 void bf_combine_dev(const BfChannelDev* chs_dev, unsigned nch, const ef2* coeffs, size_t D,
                     ef2* combined, cudaStream_t st);
-void bf_fold_poly_dev(const u64* poly, int is_ef, unsigned li, const ef2* point, size_t out_len,
-                      ef2* m, cudaStream_t st);
+void bf_fold_poly_dev(const u64* const* pref, int is_ef, unsigned li, const ef2* point,
+                      size_t out_len, ef2* m, cudaStream_t st);
 void bf_levels_dev(ef2* levels, size_t D, unsigned R, const ef2* ch, const u64* tw,
                    cudaStream_t st);
 // Many MLE evaluations at once: *out = sum_i vec[i] eq_point(i), every vec 2^k EF long.

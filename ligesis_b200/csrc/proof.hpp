@@ -112,14 +112,27 @@ struct FieldPlan {
 };
 constexpr unsigned INTS_PER_PROOF = 4 * NUM_COLS + QUERIES;
 
-// sample_columns: first s distinct values of ints mod 2n; false if fewer than s.
+// sample_columns: first s distinct values of ints mod 2n; false if fewer than s.  Seen values are
+// kept in a small open-addressed set (at most 4s = 512 draws), not a 2n-entry table.
 inline bool sample_columns(const uint64_t* ints, size_t two_n, std::vector<uint64_t>* idx) {
-  std::vector<uint8_t> seen(two_n, 0);
+  constexpr unsigned SLOTS = 1024, EMPTY = ~0u;
+  static_assert(SLOTS >= 2 * NUM_COLS, "set must stay at most half full");
+  uint32_t slot[SLOTS];
+  std::fill(slot, slot + SLOTS, EMPTY);
   idx->clear();
   for (unsigned t = 0; t < 4 * NUM_COLS; ++t) {
-    uint64_t j = ints[t] % two_n;
-    if (!seen[j]) {
-      seen[j] = 1;
+    const uint64_t j = ints[t] % two_n;
+    unsigned h = (unsigned)((j * 0x9e3779b97f4a7c15ull) >> 54);  // 10-bit multiplicative hash
+    bool fresh = true;
+    while (slot[h] != EMPTY) {
+      if ((*idx)[slot[h]] == j) {
+        fresh = false;
+        break;
+      }
+      h = (h + 1) & (SLOTS - 1);
+    }
+    if (fresh) {
+      slot[h] = (uint32_t)idx->size();
       idx->push_back(j);
       if (idx->size() == NUM_COLS) return true;
     }
@@ -147,21 +160,34 @@ inline std::vector<uint64_t> level_positions(const std::vector<uint64_t>& base, 
 // leaf indices in a power-of-two tree: per layer from the leaves up, the siblings that are not
 // themselves known, ascending.
 inline std::vector<uint64_t> multiproof_nodes(std::vector<uint64_t> cur, uint64_t leaves) {
-  std::vector<uint64_t> out;
+  std::vector<uint64_t> out, par;
   uint64_t off = 0, len = leaves;
   while (len > 1) {
-    for (uint64_t i : cur) {
-      uint64_t s = i ^ 1;
-      if (!std::binary_search(cur.begin(), cur.end(), s)) out.push_back(off + s);
-    }
-    std::vector<uint64_t> par;
-    for (uint64_t i : cur)
+    par.clear();
+    const size_t c = cur.size();
+    for (size_t k = 0; k < c; ++k) {
+      const uint64_t i = cur[k];
+      // cur is sorted and distinct: i's sibling is known iff it is the neighbouring entry
+      const bool known = (i & 1) ? (k > 0 && cur[k - 1] == i - 1) : (k + 1 < c && cur[k + 1] == i + 1);
+      if (!known) out.push_back(off + (i ^ 1));
       if (par.empty() || par.back() != i / 2) par.push_back(i / 2);
+    }
     cur.swap(par);
     off += len;
     len >>= 1;
   }
   return out;
+}
+
+// Upper bound on multiproof_nodes(q distinct leaves of a `leaves`-leaf tree): per layer at most
+// one sibling per touched pair, and no more pairs than the layer has.
+inline size_t multiproof_bound(uint64_t q, uint64_t leaves) {
+  size_t total = 0;
+  for (uint64_t len = leaves; len > 1; len >>= 1) {
+    q = std::min<uint64_t>(q, len / 2);
+    total += q;
+  }
+  return total;
 }
 
 // ---- encoding ----
@@ -185,6 +211,16 @@ struct ByteWriter {
     return std::move(b);
   }
   void bf(u64 v) { u64v(gl_canon(v)); }
+  // `count` field elements from `src`, canonicalised (EF values are 2 consecutive words)
+  void bf_run(const u64* src, size_t count) {
+    need(count * 8);
+    uint8_t* d = b.data() + n;
+    for (size_t i = 0; i < count; ++i) {
+      const u64 v = gl_canon(src[i]);
+      std::memcpy(d + 8 * i, &v, 8);
+    }
+    n += count * 8;
+  }
   void ef(const ef2& e) {
     bf(e.c0);
     bf(e.c1);

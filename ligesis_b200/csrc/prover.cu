@@ -3,8 +3,11 @@
 // open (pcs/src/basefold.rs:648-856).  Every challenge of the pre-drawn oracle is known before
 // the first kernel runs, so `prove` uploads one parameter block, enqueues the whole dataflow on
 // the context stream, and reads back one staging buffer from which the proof is assembled.
-#include <mutex>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
 
 #include "prover.cuh"
 
@@ -42,6 +45,107 @@ void bf_commit(lgs_ctx* c, const u64* poly, int is_ef, size_t len, unsigned li,
   out->li = li;
   out->num_vars = ilog2(len);
   out->L = L;
+}
+
+// Host threads shared by every context of the process for large pageable-to-pinned copies: one
+// thread's memcpy reaches a fraction of the host's memory bandwidth.
+class CopyPool {
+ public:
+  static CopyPool& get() {
+    static CopyPool* pool = new CopyPool;  // never destroyed: its threads wait until exit
+    return *pool;
+  }
+  // memcpy split into parts of at least 1 MiB, run by the pool's threads and the caller.
+  void copy(void* dst, const void* src, size_t bytes) {
+    const size_t parts = std::min<size_t>(threads_.size() + 1, std::max<size_t>(1, bytes >> 20));
+    if (parts <= 1) {
+      std::memcpy(dst, src, bytes);
+      return;
+    }
+    const size_t step = (bytes / parts + 63) & ~(size_t)63;
+    Batch batch;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      for (size_t i = 1; i < parts; ++i) {
+        const size_t off = std::min(bytes, i * step);
+        const size_t len = std::min(bytes, off + step) - off;
+        if (len) {
+          ++batch.left;
+          tasks_.push_back({(char*)dst + off, (const char*)src + off, len, &batch});
+        }
+      }
+    }
+    cv_.notify_all();
+    std::memcpy(dst, src, std::min(bytes, step));
+    std::unique_lock<std::mutex> lk(mu_);
+    batch.cv.wait(lk, [&] { return batch.left == 0; });
+  }
+
+ private:
+  struct Batch {
+    size_t left = 0;
+    std::condition_variable cv;
+  };
+  struct Task {
+    char* dst;
+    const char* src;
+    size_t len;
+    Batch* batch;
+  };
+  CopyPool() {
+    const unsigned hw = std::max(2u, std::thread::hardware_concurrency());
+    for (unsigned i = 0; i < std::min(8u, hw / 2); ++i) {
+      threads_.emplace_back([this] { run(); });
+      threads_.back().detach();  // lives as long as the process
+    }
+  }
+  void run() {
+    std::unique_lock<std::mutex> lk(mu_);
+    while (true) {
+      cv_.wait(lk, [&] { return !tasks_.empty(); });
+      Task t = tasks_.front();
+      tasks_.pop_front();
+      lk.unlock();
+      std::memcpy(t.dst, t.src, t.len);
+      lk.lock();
+      if (--t.batch->left == 0) t.batch->cv.notify_all();
+    }
+  }
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::deque<Task> tasks_;
+  std::vector<std::thread> threads_;
+};
+
+bool host_is_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// Host-to-device copy of a large host array.  Page-locked memory goes straight to the DMA engine;
+// pageable memory goes through the context's ring of pinned chunks (the copy pool fills chunk i
+// while the DMA engine moves chunk i-1).  The caller's array is no longer read when this returns.
+void h2d_staged(lgs_ctx* c, void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (host_is_pinned(src)) {
+    h2d(dst, src, bytes, st);
+    return;
+  }
+  for (size_t off = 0; off < bytes; off += lgs_ctx::RING_CHUNK) {
+    const unsigned slot = c->ring_next++ % lgs_ctx::RING;
+    const size_t len = std::min(lgs_ctx::RING_CHUNK, bytes - off);
+    LGS_CUDA(cudaEventSynchronize(c->ring_ev[slot]));  // the slot's previous copy has landed
+    c->ring[slot].reserve(lgs_ctx::RING_CHUNK);
+    if (c->copy_pool)
+      CopyPool::get().copy(c->ring[slot].p, (const char*)src + off, len);
+    else
+      std::memcpy(c->ring[slot].p, (const char*)src + off, len);
+    LGS_CUDA(cudaMemcpyAsync((char*)dst + off, c->ring[slot].p, len, cudaMemcpyHostToDevice, st));
+    LGS_CUDA(cudaEventRecord(c->ring_ev[slot], st));
+  }
 }
 
 Hash32 read_root(const u32* nodes, size_t nleaves, cudaStream_t st) {
@@ -84,6 +188,9 @@ void ctx_init(lgs_ctx* c, int device) {
     LGS_CUDA(cudaEventCreateWithFlags(&c->ev_done[i], cudaEventDisableTiming));
   }
   LGS_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+  for (int i = 0; i < lgs_ctx::RING; ++i)
+    LGS_CUDA(cudaEventCreateWithFlags(&c->ring_ev[i], cudaEventDisableTiming));
+  c->tail.reserve(64);
   c->tw.alloc(((size_t)1 << TW_LOG) * sizeof(u64), c->st);
   c->err.alloc(sizeof(int), c->st);
   LGS_CUDA(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->st));
@@ -124,7 +231,7 @@ void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lg
 // Ligesis::commit (pcs/src/ligesis.rs:277-325): RS-encode rows, hash B's columns, Merkle the
 // digest columns.  `f` may be a host or a device pointer (f_on_device).
 void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
-                lgs_commit_data* cd) {
+                lgs_commit_data* cd, bool finish) {
   const Shape& s = pk->shape;
   const size_t m = s.m(), n = s.n(), two_n = 2 * n;
   if (two_n % 128) throw ShapeError("commit: 2n must be a multiple of 128");
@@ -151,7 +258,7 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
     if (f_on_device)
       d2d(cd->f.p, f, m * n * 8, c->st);
     else
-      h2d(cd->f.p, f, m * n * 8, c->st);
+      h2d_staged(c, cd->f.p, f, m * n * 8, c->st);
   }
   const unsigned logN = ilog2(two_n);
   u64* scr = logN > 12 ? c->arena.get<u64>(m * two_n) : nullptr;
@@ -168,12 +275,25 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
     StageTimer t(c->prof, c->st, "merkle_h");
     merkle_build_from_leaves(cd->nodes.as<u32>(), two_n, c->st);
   }
-  int err = 0;
-  LGS_CUDA(cudaMemcpyAsync(&err, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
-  cd->root = read_root(cd->nodes.as<u32>(), two_n, c->st);
+  // error word and root into pinned memory; commit_finish reads them after a synchronisation
+  LGS_CUDA(cudaMemcpyAsync(c->tail.as<uint8_t>(), c->err.p, sizeof(int), cudaMemcpyDeviceToHost,
+                           c->st));
+  LGS_CUDA(cudaMemcpyAsync(c->tail.as<uint8_t>() + 32, cd->nodes.as<u32>() + (2 * two_n - 2) * 8,
+                           32, cudaMemcpyDeviceToHost, c->st));
+  if (finish) commit_finish(c, cd);
+}
+
+// Completes commit_dev(finish = false) once the work it enqueued is done: the root, and the error
+// of a bounded device wait if one gave up.  Nothing may overwrite the context's tail in between.
+void commit_finish(lgs_ctx* c, lgs_commit_data* cd) {
+  LGS_CUDA(cudaStreamSynchronize(c->st));
   c->prof.flush();
+  int err = 0;
+  std::memcpy(&err, c->tail.as<uint8_t>(), sizeof(int));
+  std::memcpy(cd->root.b, c->tail.as<uint8_t>() + 32, 32);
   if (err) {
     LGS_CUDA(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->st));
+    LGS_CUDA(cudaStreamSynchronize(c->st));
     throw DeviceTimeout("subset-sum hash: a bounded device wait gave up (code " +
                         std::to_string(err) + ")");
   }
@@ -219,6 +339,64 @@ const size_t SC_D[7] = {3, 2, 2, 2, 2, 2, 2};
 
 }  // namespace
 
+// The captured prove for this shape, capturing it now if the arena is already sized for it (an
+// eager prove of the shape has run); nullptr when this prove must run eagerly.
+template <class F>
+const ProveGraph* prove_graph(lgs_ctx* c, const Shape& s, F&& enqueue) {
+  if (!c->use_graphs) return nullptr;
+  ProveGraph* g = nullptr;
+  for (auto& e : c->graphs)
+    if (e.log_m == s.log_m && e.log_n == s.log_n) g = &e;
+  if (!g) {
+    c->graphs.emplace_back();
+    c->graphs.back().log_m = s.log_m;
+    c->graphs.back().log_n = s.log_n;
+    return nullptr;
+  }
+  const Arena& ar = c->arena;
+  if (g->exec && g->arena == ar.mem.p && g->arena_bytes == ar.mem.bytes && g->up == c->up.p &&
+      g->down == c->down.p)
+    return g;
+  if (g->exec) {
+    LGS_CUDA(cudaGraphExecDestroy(g->exec));
+    g->exec = nullptr;
+  }
+  if (g->need == 0 || g->need > ar.mem.bytes || !ar.overflow.empty()) return nullptr;
+  cudaGraph_t graph = nullptr;
+  LGS_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+  const uint64_t l0 = thread_launches();
+  c->arena.frozen = true;
+  try {
+    enqueue();
+  } catch (...) {
+    c->arena.frozen = false;
+    cudaStreamEndCapture(c->st, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    (void)cudaGetLastError();
+    throw;
+  }
+  c->arena.frozen = false;
+  const uint64_t captured = thread_launches() - l0;
+  adjust_launches(-(int64_t)captured);  // captured, not launched
+  LGS_CUDA(cudaStreamEndCapture(c->st, &graph));
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t err = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  LGS_CUDA(err);
+  g->exec = exec;
+  g->launches = captured;
+  g->arena = ar.mem.p;
+  g->arena_bytes = ar.mem.bytes;
+  g->up = c->up.p;
+  g->down = c->down.p;
+  return g;
+}
+
+void note_prove_need(lgs_ctx* c, const Shape& s, size_t need) {
+  for (auto& e : c->graphs)
+    if (e.log_m == s.log_m && e.log_n == s.log_n) e.need = std::max(e.need, need);
+}
+
 void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u64* z_host,
                size_t zlen, const u64* fields_host, size_t nfields, const uint64_t* ints_host,
                size_t nints, uint64_t cursors[2], std::vector<uint8_t>* proof_out) {
@@ -236,6 +414,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   if (i0 > nints || nints - i0 < INTS_PER_PROOF) throw OracleError("oracle exhausted (ints)");
   cudaStream_t st = c->st;
   Arena& ar = c->arena;
+  HostClock hc(c->prof);
   ar.begin();
 
   // ---- host transcript: indices and points --------------------------------------------------
@@ -305,14 +484,16 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   }
 
   // ---- staging layout ----------------------------------------------------------------------
+  // Every region is sized by its upper bound for the shape, so offsets (and every kernel
+  // argument below) depend on the shape only and a captured graph of the prove replays for any
+  // transcript; the transcript-dependent counts travel in the uploaded gather plan.
   Stage sg;
   const size_t S_y = sg.take(2), S_y4 = sg.take(2), S_y5 = sg.take(2);
   const size_t S_coma = sg.take(4), S_comi = sg.take(4);
   const size_t S_hcols = sg.take(S * DIGEST_ROWS);
   const std::vector<uint64_t> h_nodes = multiproof_nodes(sorted_idx, two_n);
-  const size_t S_hopen = sg.take(h_nodes.size() * 4);
+  const size_t S_hopen = sg.take(multiproof_bound(S, two_n) * 4);
   const unsigned sc_k[7] = {nb, log_w, log_w, log_n + 1, log_n, nb, log_n};
-  const unsigned sc_ch[7] = {fp.ch_bin, fp.ch_hash, fp.ch_recon, fp.ch_table, fp.ch_rs, fp.ch_bi, fp.ch_a};
   size_t S_sc_r[7], S_sc_f[7];
   for (int i = 0; i < 7; ++i) {
     S_sc_r[i] = sg.take(sc_k[i] * (SC_D[i] + 1) * 2);
@@ -323,70 +504,166 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   const size_t S_roots = sg.take((R ? R - 1 : 0) * 4);
   const size_t final_len = D >> R;
   const size_t S_final = sg.take(final_len * 2);
+  // Merkle openings: base positions of the three channels, then one per fold level
+  const unsigned li_a = s.li(s.naa()), li_bi = s.li(s.nbi()), li_A = s.li(s.na());
+  const unsigned chan_li[3] = {li_A, li_bi, li_a};
+  const int chan_ef[3] = {0, 0, 1};
+  const std::vector<uint64_t> b_nodes = multiproof_nodes(bpos, D);
+  size_t idx_bound = S * DIGEST_ROWS + multiproof_bound(S, two_n) + 2 + final_len;
+  std::vector<OpenPlan> opens;  // base_bf(A), base_bf(B_I), base_ef(a), then fold levels
+  {
+    const uint64_t qmax = std::min<uint64_t>(2 * QUERIES, D);  // level_positions(base, D / 2)
+    for (int ch = 0; ch < 3; ++ch) {
+      OpenPlan o;
+      o.nnodes = b_nodes.size();
+      o.node_off = sg.take(multiproof_bound(qmax, D) * 4);
+      o.words = ((1u << chan_li[ch]) * (chan_ef[ch] ? 2 : 1));
+      o.val_off = sg.take(qmax * o.words);
+      o.keys = bpos;
+      opens.push_back(o);
+      idx_bound += multiproof_bound(qmax, D) + qmax;
+    }
+  }
+  std::vector<std::vector<uint64_t>> lvl_pos(R), lvl_mp(R);
+  for (unsigned k = 1; k < R; ++k) {
+    OpenPlan o;
+    const uint64_t len = D >> k, qmax = std::min<uint64_t>(2 * QUERIES, len);
+    lvl_pos[k] = level_positions(base, len / 2);
+    lvl_mp[k] = multiproof_nodes(lvl_pos[k], len);
+    o.nnodes = lvl_mp[k].size();
+    o.node_off = sg.take(multiproof_bound(qmax, len) * 4);
+    o.words = 2;
+    o.val_off = sg.take(qmax * 2);
+    o.keys = lvl_pos[k];
+    opens.push_back(o);
+    idx_bound += multiproof_bound(qmax, len) + qmax + 1;
+  }
 
-  // ---- device buffers ----------------------------------------------------------------------
-  ef2* d_prm = ar.get<ef2>(prm.size());
-  const ef2* d_fields = d_prm + P_fields;
+  // ---- device buffers (arena offsets only: nothing here waits for the device) ----------------
   ef2* eqz1 = ar.get<ef2>(m);
   ef2* a_vec = ar.get<ef2>(n);
   ef2* ra = ar.get<ef2>(two_n);
-  uint64_t* d_idx = ar.get<uint64_t>(S);
-
-  // Basefold states built during prove
-  BasefoldDev a_st, bi_st;
-  const unsigned li_a = s.li(s.naa()), li_bi = s.li(s.nbi()), li_A = s.li(s.na());
+  BasefoldDev a_st, bi_st;  // Basefold states built during prove
   a_st.codes = ar.get<u64>(D * ((size_t)2 << li_a));
   a_st.nodes = ar.get<u32>((2 * D - 1) * 8);
   bi_st.codes = ar.get<u64>(D * ((size_t)1 << li_bi));
   bi_st.nodes = ar.get<u32>((2 * D - 1) * 8);
   u64* bi = ar.get<u64>(WS);
+  u64* stage = ar.get<u64>(sg.total);
+  ef2* eq_a2 = ar.get<ef2>(DIGEST_ROWS);
+  ef2* eq_r2 = ar.get<ef2>(S);
+  ef2* levels = ar.get<ef2>(2 * D);
+  std::vector<u32*> lvl_nodes(R, nullptr);
+  for (unsigned k = 1; k < R; ++k) lvl_nodes[k] = ar.get<u32>((2 * (D >> k) - 1) * 8);
+  const size_t mlen = (size_t)1 << R;
+  ef2* mch[3];
+  for (int ch = 0; ch < 3; ++ch) mch[ch] = ar.get<ef2>(mlen);
+  const BasefoldDev* chan_states[3] = {&pk->a_state, &bi_st, &a_st};
+  const u64* polys[3] = {pk->A.as<u64>(), bi, (const u64*)a_vec};
 
-  StageTimer t_prove(c->prof, st, "prove_device");
-  // upload: params, idx
-  h2d(d_prm, prm.data(), prm.size() * sizeof(ef2), st);
-  h2d(d_idx, idx.data(), S * 8, st);
+  // ---- the gather plan into staging (pcs/src/ligesis.rs:527-549 fields of the proof) --------
+  SegPlan plan;
+  {
+    std::vector<uint64_t> hidx;  // H[r][sorted_idx[k]], column by column
+    hidx.reserve(S * DIGEST_ROWS);
+    for (uint64_t j : sorted_idx)
+      for (unsigned r = 0; r < DIGEST_ROWS; ++r) hidx.push_back((uint64_t)r * two_n + j);
+    plan.add(cd->H.as<u64>(), hidx, 1, S_hcols);
+    plan.add((const u64*)cd->nodes.as<u32>(), h_nodes, 4, S_hopen);
+    plan.add((const u64*)a_st.nodes, {2 * D - 2}, 4, S_coma);
+    plan.add((const u64*)bi_st.nodes, {2 * D - 2}, 4, S_comi);
+    for (int ch = 0; ch < 3; ++ch) {
+      const OpenPlan& o = opens[ch];
+      plan.add((const u64*)chan_states[ch]->nodes, b_nodes, 4, o.node_off);
+      plan.add(chan_states[ch]->codes, bpos, o.words, o.val_off);
+    }
+    size_t off = D;
+    for (unsigned k = 1; k < R; ++k) {
+      const OpenPlan& o = opens[2 + k];
+      const size_t len = D >> k;
+      plan.add((const u64*)lvl_nodes[k], lvl_mp[k], 4, o.node_off);
+      plan.add((const u64*)(levels + off), lvl_pos[k], 2, o.val_off);
+      plan.add((const u64*)lvl_nodes[k], {2 * len - 2}, 4, S_roots + (k - 1) * 4);
+      off += len;
+    }
+    std::vector<uint64_t> fin(final_len);
+    for (size_t i = 0; i < final_len; ++i) fin[i] = i;
+    plan.add((const u64*)(levels + off), fin, 2, S_final);
+  }
 
-  // Staging is allocated once the layout is final (openings appended below).
+  // ---- one upload: parameters, column indices, message tasks, channels, gather plan ---------
+  size_t blob = 0;
+  auto part = [&](size_t bytes) {
+    const size_t o = blob;
+    blob += (bytes + 255) & ~(size_t)255;
+    return o;
+  };
+  const size_t U_prm = part(prm.size() * sizeof(ef2));
+  const size_t U_idx = part(S * 8);
+  const size_t U_tasks = part(3 * R * sizeof(EqDotTask));
+  const size_t U_chs = part(3 * sizeof(BfChannelDev));
+  // source addresses read by kernels through device slots: f, F', A, B_I, a-bar
+  enum { PT_F, PT_CW, PT_A, PT_BI, PT_AVEC, PT_N };
+  const size_t U_ptrs = part(PT_N * sizeof(void*));
+  if (plan.idx.size() > idx_bound) throw std::logic_error("prove: gather plan exceeds its bound");
+  const size_t U_gidx = part(idx_bound * 8);
+  const size_t U_segs = part(plan.segs.size() * sizeof(GatherSeg));
+  uint8_t* d_up = ar.get<uint8_t>(blob);
+  c->up.reserve(blob);
+  uint8_t* h_up = c->up.as<uint8_t>();
+  const ef2* d_prm = (const ef2*)(d_up + U_prm);
+  const ef2* d_fields = d_prm + P_fields;
+  const uint64_t* d_idx = (const uint64_t*)(d_up + U_idx);
+  const ef2* pts[3] = {d_prm + P_pa, d_prm + P_rbi, d_prm + P_ra};
+  std::memcpy(h_up + U_prm, prm.data(), prm.size() * sizeof(ef2));
+  std::memcpy(h_up + U_idx, idx.data(), S * 8);
+  const u64* const* d_ptrs = (const u64* const*)(d_up + U_ptrs);
+  {
+    const u64* pt[PT_N] = {cd->f.as<u64>(), cd->cw.as<u64>(), pk->A.as<u64>(), bi,
+                           (const u64*)a_vec};
+    std::memcpy(h_up + U_ptrs, pt, sizeof(pt));
+  }
+  {
+    EqDotTask* tasks = (EqDotTask*)(h_up + U_tasks);
+    for (int ch = 0; ch < 3; ++ch)
+      for (unsigned t = 0; t < R; ++t) {
+        EqDotTask& tk = tasks[ch * R + t];
+        tk.vec = mch[ch];
+        tk.point = d_prm + P_q + (size_t)(ch * R + t) * R;
+        tk.out = (ef2*)(stage + S_msgs) + ch * R + t;
+      }
+    BfChannelDev* chs = (BfChannelDev*)(h_up + U_chs);
+    for (int ch = 0; ch < 3; ++ch) {
+      chs[ch].codes = chan_states[ch]->codes;
+      chs[ch].poly = polys[ch];
+      chs[ch].is_ef = chan_ef[ch];
+      chs[ch].li = chan_li[ch];
+      chs[ch].point = pts[ch];
+    }
+    std::memcpy(h_up + U_gidx, plan.idx.data(), plan.idx.size() * 8);
+    GatherSeg* segs = (GatherSeg*)(h_up + U_segs);
+    for (size_t i = 0; i < plan.segs.size(); ++i) {
+      segs[i] = plan.segs[i];
+      segs[i].idx = (const uint64_t*)(d_up + U_gidx) + (uintptr_t)plan.segs[i].idx;
+      segs[i].dst = stage + (uintptr_t)plan.segs[i].dst;
+    }
+  }
+  c->down.reserve(sg.total * 8);
+
+  hc.lap("host_plan");
+
+  // Everything from the upload to the read-back depends on the transcript only through the
+  // uploaded blob, so it is captured once per shape into a CUDA graph and replayed.
+  auto enqueue = [&]() {
+  h2d(d_up, h_up, blob, st);
+
   // -- a-bar, y, commit a-bar, RS(a-bar) (pcs/src/ligesis.rs:365-387)
   new_eq_dev(d_prm + P_z1, s.log_m, eqz1, st);
-  gemv_eq_rows(cd->f.as<u64>(), eqz1, m, n, a_vec, st);
-
-  std::vector<OpenPlan> opens;  // base_bf(A), base_bf(B_I), base_ef(a), then fold levels
-  SegPlan plan;
-  // The gather plan and the rest of the staging layout are needed before allocation.
-  // Base openings at bpos for the three channels.
-  const BasefoldDev* chan_states[3] = {&pk->a_state, &bi_st, &a_st};
-  const unsigned chan_li[3] = {li_A, li_bi, li_a};
-  const int chan_ef[3] = {0, 0, 1};
-  for (int ch = 0; ch < 3; ++ch) {
-    OpenPlan o;
-    std::vector<uint64_t> nodes = multiproof_nodes(bpos, D);
-    o.nnodes = nodes.size();
-    o.node_off = sg.take(nodes.size() * 4);
-    o.words = ((1u << chan_li[ch]) * (chan_ef[ch] ? 2 : 1));
-    o.val_off = sg.take(bpos.size() * o.words);
-    o.keys = bpos;
-    opens.push_back(o);
-  }
-  std::vector<std::vector<uint64_t>> lvl_pos(R);
-  for (unsigned k = 1; k < R; ++k) {
-    OpenPlan o;
-    lvl_pos[k] = level_positions(base, (D >> k) / 2);
-    std::vector<uint64_t> nodes = multiproof_nodes(lvl_pos[k], D >> k);
-    o.nnodes = nodes.size();
-    o.node_off = sg.take(nodes.size() * 4);
-    o.words = 2;
-    o.val_off = sg.take(lvl_pos[k].size() * 2);
-    o.keys = lvl_pos[k];
-    opens.push_back(o);
-  }
-  u64* stage = ar.get<u64>(sg.total);
+  gemv_eq_rows(d_ptrs + PT_F, eqz1, m, n, a_vec, st);
 
   // -- the rest is a DAG of independent branches (every challenge is pre-drawn): fork them
   // onto side streams after the shared inputs exist, join before the gather.
-  bits_gather(cd->cw.as<u64>(), two_n, d_idx, S, W, bi, st);
-  ef2* eq_a2 = ar.get<ef2>(DIGEST_ROWS);
-  ef2* eq_r2 = ar.get<ef2>(S);
+  bits_gather(d_ptrs + PT_CW, two_n, d_idx, S, W, bi, st);
   new_eq_dev(d_fields + fp.alpha2, 5, eq_a2, st);
   new_eq_dev(d_fields + fp.r2, log_s, eq_r2, st);
   LGS_CUDA(cudaEventRecord(c->ev_fork, st));
@@ -449,7 +726,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     ef2* g2 = ar.get<ef2>(W);
     ef2* g2b = ar.get<ef2>(W);
     ef2* v = ar.get<ef2>(W);
-    g1_build(pk->A.as<u64>(), W, eq_a2, DIGEST_ROWS, g1, b);
+    g1_build(d_ptrs + PT_A, W, eq_a2, DIGEST_ROWS, g1, b);
     g2_build(bi, W, S, eq_r2, g2, b);
     d2d(g2b, g2, W * sizeof(ef2), b);
     v_build(eqz1, W, v, b);
@@ -496,28 +773,13 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   // H: Stage B reduction messages (pcs/src/basefold.rs:746-769).  With m = poly.fold(point[0..li])
   // (2^R values) and the batch challenges r_0.., round t's l0 = MLE(m)(r_0, .., r_{t-1}, 0,
   // zp[t+1], .., zp[R-1]): the sequential rounds collapse to R independent evaluations.
-  const ef2* pts[3] = {d_prm + P_pa, d_prm + P_rbi, d_prm + P_ra};
-  const u64* polys[3] = {pk->A.as<u64>(), bi, (const u64*)a_vec};
   {
     cudaStream_t b = branch();
-    const size_t mlen = (size_t)1 << R;
-    std::vector<EqDotTask> tasks(3 * R);
-    for (int ch = 0; ch < 3; ++ch) {
-      ef2* mch = ar.get<ef2>(mlen);
-      bf_fold_poly_dev(polys[ch], chan_ef[ch], chan_li[ch], pts[ch], mlen, mch, b);
-      for (unsigned t = 0; t < R; ++t) {
-        EqDotTask& tk = tasks[ch * R + t];
-        tk.vec = mch;
-        tk.point = d_prm + P_q + (size_t)(ch * R + t) * R;
-        tk.out = (ef2*)(stage + S_msgs) + ch * R + t;
-      }
-    }
-    EqDotTask* d_tasks = ar.get<EqDotTask>(tasks.size());
-    ef2* part = ar.get<ef2>(eq_dot_multi_partials(R, (unsigned)tasks.size()));
-    std::vector<uint8_t>& hs2 = c->host_stage2;
-    hs2.assign((const uint8_t*)tasks.data(), (const uint8_t*)(tasks.data() + tasks.size()));
-    h2d(d_tasks, hs2.data(), hs2.size(), b);
-    eq_dot_multi_dev(d_tasks, (unsigned)tasks.size(), R, part, b);
+    const int poly_slot[3] = {PT_A, PT_BI, PT_AVEC};
+    for (int ch = 0; ch < 3; ++ch)
+      bf_fold_poly_dev(d_ptrs + poly_slot[ch], chan_ef[ch], chan_li[ch], pts[ch], mlen, mch[ch], b);
+    ef2* part = ar.get<ef2>(eq_dot_multi_partials(R, 3 * R));
+    eq_dot_multi_dev((const EqDotTask*)(d_up + U_tasks), 3 * R, R, part, b);
   }
   // join: main waits for every branch
   for (unsigned i = 0; i < nbr; ++i) LGS_CUDA(cudaEventRecord(c->ev_done[i], c->side[i]));
@@ -525,149 +787,97 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   LGS_CUDA(cudaStreamWaitEvent(st, c->ev_done[br_b], 0));
   // Stage B codeword chain on main (needs both prove-time commitments): combined level 0,
   // the R folds, and the Merkle trees of levels 1..R-1 (pcs/src/basefold.rs:735-784)
-  ef2* levels = ar.get<ef2>(2 * D);
-  {
-    BfChannelDev chs[3];
-    for (int ch = 0; ch < 3; ++ch) {
-      chs[ch].codes = chan_states[ch]->codes;
-      chs[ch].poly = polys[ch];
-      chs[ch].is_ef = chan_ef[ch];
-      chs[ch].li = chan_li[ch];
-      chs[ch].point = pts[ch];
-    }
-    BfChannelDev* d_chs = ar.get<BfChannelDev>(3);
-    std::vector<uint8_t>& hs = c->host_stage;
-    hs.assign((const uint8_t*)chs, (const uint8_t*)chs + sizeof(chs));
-    h2d(d_chs, hs.data(), sizeof(chs), st);
-    bf_combine_dev(d_chs, 3, d_fields + fp.coeffs, D, levels, st);
-    bf_levels_dev(levels, D, R, d_fields + fp.ch_batch, c->tw.as<u64>(), st);
-  }
-  std::vector<u32*> lvl_nodes(R, nullptr);
-  {
+  bf_combine_dev((const BfChannelDev*)(d_up + U_chs), 3, d_fields + fp.coeffs, D, levels, st);
+  bf_levels_dev(levels, D, R, d_fields + fp.ch_batch, c->tw.as<u64>(), st);
+  if (R > 1) {
     std::vector<const u64*> ldata;
     std::vector<u32*> lnodes;
     std::vector<size_t> lcount;
     size_t off = D;
     for (unsigned k = 1; k < R; ++k) {
       const size_t len = D >> k;
-      lvl_nodes[k] = ar.get<u32>((2 * len - 1) * 8);
       ldata.push_back((const u64*)(levels + off));
       lnodes.push_back(lvl_nodes[k]);
       lcount.push_back(len);
       off += len;
     }
-    if (!lnodes.empty()) {
-      merkle_leaves_many(ldata.data(), 2, lnodes.data(), lcount.data(), (unsigned)lnodes.size(), st);
-      merkle_build_many(lnodes.data(), lcount.data(), (unsigned)lnodes.size(), st);
-    }
+    merkle_leaves_many(ldata.data(), 2, lnodes.data(), lcount.data(), (unsigned)lnodes.size(), st);
+    merkle_build_many(lnodes.data(), lcount.data(), (unsigned)lnodes.size(), st);
   }
   for (unsigned i = 0; i < nbr; ++i) LGS_CUDA(cudaStreamWaitEvent(st, c->ev_done[i], 0));
 
-  // ---- gathers into staging ----------------------------------------------------------------
-  {
-    std::vector<uint64_t> hidx;  // H[r][sorted_idx[k]], column by column
-    for (uint64_t j : sorted_idx)
-      for (unsigned r = 0; r < DIGEST_ROWS; ++r) hidx.push_back((uint64_t)r * two_n + j);
-    plan.add(cd->H.as<u64>(), hidx, 1, S_hcols);
-    plan.add((const u64*)cd->nodes.as<u32>(), h_nodes, 4, S_hopen);
-    plan.add((const u64*)a_st.nodes, {2 * D - 2}, 4, S_coma);
-    plan.add((const u64*)bi_st.nodes, {2 * D - 2}, 4, S_comi);
-    for (int ch = 0; ch < 3; ++ch) {
-      const OpenPlan& o = opens[ch];
-      plan.add((const u64*)chan_states[ch]->nodes, multiproof_nodes(bpos, D), 4, o.node_off);
-      plan.add(chan_states[ch]->codes, bpos, o.words, o.val_off);
-    }
-    size_t off = D;
-    for (unsigned k = 1; k < R; ++k) {
-      const OpenPlan& o = opens[2 + k];
-      size_t len = D >> k;
-      plan.add((const u64*)lvl_nodes[k], multiproof_nodes(lvl_pos[k], len), 4, o.node_off);
-      plan.add((const u64*)(levels + off), lvl_pos[k], 2, o.val_off);
-      plan.add((const u64*)lvl_nodes[k], {2 * len - 2}, 4, S_roots + (k - 1) * 4);
-      off += len;
-    }
-    std::vector<uint64_t> fin(final_len);
-    for (size_t i = 0; i < final_len; ++i) fin[i] = i;
-    plan.add((const u64*)(levels + off), fin, 2, S_final);
+  // ---- gathers into staging, one read-back -------------------------------------------------
+  gather_segments((const GatherSeg*)(d_up + U_segs), (unsigned)plan.segs.size(), st);
+  LGS_CUDA(cudaMemcpyAsync(c->down.p, stage, sg.total * 8, cudaMemcpyDeviceToHost, st));
+  };
+  const ProveGraph* graph = prove_graph(c, s, enqueue);
+  StageTimer t_prove(c->prof, st, "prove_device");
+  if (graph) {
+    LGS_CUDA(cudaGraphLaunch(graph->exec, st));
+    adjust_launches((int64_t)graph->launches);
+  } else {
+    enqueue();
+    note_prove_need(c, s, ar.off);
   }
-  uint64_t* d_gidx = ar.get<uint64_t>(plan.idx.size());
-  GatherSeg* d_segs = ar.get<GatherSeg>(plan.segs.size());
-  std::vector<GatherSeg> segs = plan.segs;
-  for (auto& g : segs) {
-    g.idx = d_gidx + (uintptr_t)g.idx;
-    g.dst = stage + (uintptr_t)g.dst;
-  }
-  std::vector<uint8_t> seg_bytes((const uint8_t*)segs.data(),
-                                 (const uint8_t*)(segs.data() + segs.size()));
-  h2d(d_gidx, plan.idx.data(), plan.idx.size() * 8, st);
-  h2d(d_segs, seg_bytes.data(), seg_bytes.size(), st);
-  gather_segments(d_segs, (unsigned)segs.size(), st);
-
-  std::vector<u64> hst(sg.total);
-  LGS_CUDA(cudaMemcpyAsync(hst.data(), stage, sg.total * 8, cudaMemcpyDeviceToHost, st));
   t_prove.stop();
+  hc.lap("host_enqueue");
+  const u64* hst = c->down.as<u64>();
   LGS_CUDA(cudaStreamSynchronize(st));
+  hc.lap("host_wait");
   c->prof.flush();
 
-  // ---- assemble ----------------------------------------------------------------------------
-  auto efat = [&](size_t off) { return ef_make(hst[off], hst[off + 1]); };
-  auto h32at = [&](size_t off) {
-    Hash32 h;
-    std::memcpy(h.b, &hst[off], 32);
-    return h;
-  };
-  ProofH p;
-  p.y = efat(S_y);
-  p.y4 = efat(S_y4);
-  p.y5 = efat(S_y5);
-  p.com_a_vec = h32at(S_coma);
-  p.com_i = h32at(S_comi);
-  p.h_cols.assign(S, std::vector<u64>(DIGEST_ROWS));
-  for (size_t k = 0; k < S; ++k)
-    for (unsigned r = 0; r < DIGEST_ROWS; ++r) p.h_cols[k][r] = hst[S_hcols + k * DIGEST_ROWS + r];
-  p.h_open.assign((const uint8_t*)&hst[S_hopen], (const uint8_t*)&hst[S_hopen] + h_nodes.size() * 32);
-  for (int i = 0; i < 7; ++i) {
-    const size_t w = SC_D[i] + 1;
-    p.sc[i].rounds.assign(sc_k[i], std::vector<ef2>(w));
-    for (unsigned t = 0; t < sc_k[i]; ++t)
-      for (size_t q = 0; q < w; ++q) p.sc[i].rounds[t][q] = efat(S_sc_r[i] + (t * w + q) * 2);
-    for (size_t j = 0; j < SC_D[i]; ++j) p.sc[i].finals.push_back(efat(S_sc_f[i] + 2 * j));
+  // ---- encode straight from the staging buffer, in the order of encode_proof --------------
+  ByteWriter w;
+  w.need(sg.total * 8 + 4096);
+  w.raw("LGSP", 4);
+  w.u32v(1);
+  w.bf_run(hst + S_y, 2);
+  w.raw(hst + S_coma, 32);
+  w.raw(hst + S_comi, 32);
+  w.bf_run(hst + S_y4, 2);
+  w.bf_run(hst + S_y5, 2);
+  w.u32v((uint32_t)S);
+  w.u32v(DIGEST_ROWS);
+  w.bf_run(hst + S_hcols, S * DIGEST_ROWS);
+  w.u32v((uint32_t)(h_nodes.size() * 32));
+  w.raw(hst + S_hopen, h_nodes.size() * 32);
+  for (int i = 0; i < 7; ++i) {  // ScProof: rounds, width, round values, finals
+    w.u32v(sc_k[i]);
+    w.u32v(sc_k[i] ? (uint32_t)(SC_D[i] + 1) : 0);
+    w.bf_run(hst + S_sc_r[i], (size_t)sc_k[i] * (SC_D[i] + 1) * 2);
+    w.u32v((uint32_t)SC_D[i]);
+    w.bf_run(hst + S_sc_f[i], SC_D[i] * 2);
   }
-  (void)sc_ch;
-  BatchProofH& b = p.batch;
-  b.code_rate = CODE_RATE;
-  b.log_len = ilog2(D);
-  b.msgs.assign(NCH, std::vector<ef2>(R));
-  for (unsigned ch = 0; ch < NCH; ++ch)
-    for (unsigned t = 0; t < R; ++t) b.msgs[ch][t] = efat(S_msgs + (ch * R + t) * 2);
-  for (unsigned k = 1; k < R; ++k) b.fold_roots.push_back(h32at(S_roots + (k - 1) * 4));
-  for (size_t i = 0; i < final_len; ++i) b.final_codeword.push_back(efat(S_final + 2 * i));
-  for (size_t oi = 0; oi < opens.size(); ++oi) {
-    const OpenPlan& o = opens[oi];
-    std::vector<uint8_t> pbytes((const uint8_t*)&hst[o.node_off],
-                                (const uint8_t*)&hst[o.node_off] + o.nnodes * 32);
-    if (oi < 2) {
-      OpeningH<u64> op;
-      op.proof = pbytes;
-      for (size_t i = 0; i < o.keys.size(); ++i)
-        op.values.push_back({o.keys[i], std::vector<u64>(&hst[o.val_off + i * o.words],
-                                                          &hst[o.val_off + (i + 1) * o.words])});
-      b.base_bf.push_back(op);
-    } else {
-      OpeningH<ef2> op;
-      op.proof = pbytes;
-      for (size_t i = 0; i < o.keys.size(); ++i) {
-        std::vector<ef2> v(o.words / 2);
-        for (size_t q = 0; q < v.size(); ++q) v[q] = efat(o.val_off + i * o.words + 2 * q);
-        op.values.push_back({o.keys[i], v});
-      }
-      if (oi == 2)
-        b.base_ef.push_back(op);
-      else
-        b.fold_openings.push_back(op);
+  w.u32v(CODE_RATE);
+  w.u32v(ilog2(D));
+  w.u32v(NCH);
+  for (unsigned ch = 0; ch < NCH; ++ch) {
+    w.u32v(R);
+    w.bf_run(hst + S_msgs + (size_t)ch * R * 2, (size_t)R * 2);
+  }
+  w.u32v(R ? R - 1 : 0);
+  if (R > 1) w.raw(hst + S_roots, (size_t)(R - 1) * 32);
+  w.u32v((uint32_t)final_len);
+  w.bf_run(hst + S_final, final_len * 2);
+  auto opening = [&](const OpenPlan& o, bool ef) {  // Merkle bytes, then (key, values) pairs
+    w.u32v((uint32_t)(o.nnodes * 32));
+    w.raw(hst + o.node_off, o.nnodes * 32);
+    w.u32v((uint32_t)o.keys.size());
+    for (size_t i = 0; i < o.keys.size(); ++i) {
+      w.u64v(o.keys[i]);
+      w.u32v(ef ? o.words / 2 : o.words);
+      w.bf_run(hst + o.val_off + i * o.words, o.words);
     }
-  }
-  *proof_out = encode_proof(p);
+  };
+  w.u32v(R ? R - 1 : 0);  // fold openings
+  for (size_t oi = 3; oi < opens.size(); ++oi) opening(opens[oi], true);
+  w.u32v(2);  // base_bf: A, B_I
+  opening(opens[0], false);
+  opening(opens[1], false);
+  w.u32v(1);  // base_ef: a-bar
+  opening(opens[2], true);
+  *proof_out = w.finish();
+  hc.lap("host_assemble");
   cursors[0] = f0 + fp.total;
   cursors[1] = i0 + INTS_PER_PROOF;
 }

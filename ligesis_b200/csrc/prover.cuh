@@ -2,10 +2,12 @@
 // key and commitment data (the reference's ProvingKey / CommitData, pcs/src/ligesis.rs:67-97)
 // kept resident on the device.
 #pragma once
+#include <chrono>
 #include <memory>
 #include <string>
 #include <vector>
 
+#include "../../include/lgs.h"
 #include "kernels.cuh"
 #include "proof.hpp"
 
@@ -14,6 +16,33 @@ namespace lgs {
 // Device buffer from the device's stream-ordered memory pool (cudaMallocAsync on the owning
 // context's stream).  The pool keeps freed memory cached (the context raises its release
 // threshold), so a commitment allocated and freed per proof costs no cudaMalloc / device sync.
+// Page-locked host buffer that only grows (cudaMallocHost / cudaFreeHost).
+struct PinnedBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  PinnedBuf() = default;
+  PinnedBuf(const PinnedBuf&) = delete;
+  PinnedBuf& operator=(const PinnedBuf&) = delete;
+  void reserve(size_t b) {
+    if (b <= bytes) return;
+    release();
+    size_t want = 4096;
+    while (want < b) want <<= 1;
+    LGS_CUDA(cudaMallocHost(&p, want));
+    bytes = want;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  ~PinnedBuf() { release(); }
+  template <class T>
+  T* as() const {
+    return (T*)p;
+  }
+};
+
 // A non-blocking stream per device that lives as long as the process: the stream on which
 // buffers that outlive their context are freed.
 cudaStream_t release_stream(int device);
@@ -64,6 +93,7 @@ struct Arena {
   std::vector<DevMem> overflow;
   size_t off = 0, hwm = 0;
   cudaStream_t st = nullptr;
+  bool frozen = false;  // set while a graph is captured: growing would need a synchronisation
   void begin() {
     if (!overflow.empty() || hwm > mem.bytes) {
       overflow.clear();
@@ -79,6 +109,7 @@ struct Arena {
     if (off + b <= mem.bytes) {
       r = (T*)((char*)mem.p + off);
     } else {
+      if (frozen) throw std::logic_error("arena: growth while capturing a graph");
       // Grown mid-call: make the new block usable from every stream of the context at once.
       overflow.emplace_back(b, st);
       LGS_CUDA(cudaStreamSynchronize(st));
@@ -150,10 +181,40 @@ struct StageTimer {
   ~StageTimer() { stop(); }
 };
 
+// A prove captured as a CUDA graph for one shape.  Valid while the context's arena block and
+// pinned transfer buffers are the ones it was captured with.
+struct ProveGraph {
+  unsigned log_m = 0, log_n = 0;
+  size_t need = 0;  // arena bytes one prove of this shape uses (measured by an eager prove)
+  const void* arena = nullptr;
+  size_t arena_bytes = 0;
+  const void* up = nullptr;
+  const void* down = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t launches = 0;  // kernels per replay
+};
+
+// Host-side phases of one call (planning, enqueueing, waiting, assembling), recorded in the
+// same profile as the device stages while profiling is on.
+struct HostClock {
+  Profiler* p;
+  std::chrono::steady_clock::time_point t;
+  explicit HostClock(Profiler& prof)
+      : p(prof.on ? &prof : nullptr), t(std::chrono::steady_clock::now()) {}
+  void lap(const char* name) {
+    if (!p) return;
+    const auto now = std::chrono::steady_clock::now();
+    p->add(name, std::chrono::duration<double, std::milli>(now - t).count());
+    t = now;
+  }
+};
+
 }  // namespace lgs
 
 struct lgs_ctx {
   static constexpr int NSIDE = 12;  // side streams for the independent branches of prove
+  static constexpr int RING = 3;    // pinned chunks for staged uploads of host polynomials
+  static constexpr size_t RING_CHUNK = (size_t)8 << 20;
   int device = 0;
   cudaStream_t st = nullptr;
   cudaStream_t side[NSIDE] = {};
@@ -163,8 +224,17 @@ struct lgs_ctx {
   lgs::Arena arena;
   lgs::Profiler prof;
   lgs::DevMem err;  // device error word of bounded-wait kernels (0 = ok)
-  std::vector<uint8_t> host_stage;  // host copies that must outlive an async upload
-  std::vector<uint8_t> host_stage2;
+  // Pinned host memory: every transfer of a call is asynchronous, so the host enqueues a whole
+  // commit or prove without waiting for the device and synchronises once at the end.
+  lgs::PinnedBuf up;    // the parameter blob of one prove (one host-to-device copy)
+  lgs::PinnedBuf down;  // the staging area one prove reads back
+  lgs::PinnedBuf tail;  // error word and root of the last commit
+  lgs::PinnedBuf ring[RING];
+  cudaEvent_t ring_ev[RING] = {};
+  unsigned ring_next = 0;
+  bool copy_pool = true;  // staged uploads use the process's copy threads (engine lanes: no)
+  bool use_graphs = true;
+  std::vector<lgs::ProveGraph> graphs;
   std::vector<uint8_t> proof_buf;   // the last proof returned by lgs_prove
 };
 
@@ -186,3 +256,18 @@ struct lgs_commit_data {
   lgs::DevMem nodes;  // column Merkle tree over H
   lgs::Hash32 root;
 };
+
+namespace lgs {
+// The prover's stages (prover.cu).  commit_dev with finish = false only enqueues: commit_finish
+// (or any later synchronisation of the context followed by commit_finish) completes it.
+void ctx_init(lgs_ctx* c, int device);
+void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lgs_pk* pk);
+void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device, lgs_commit_data* cd,
+                bool finish = true);
+void commit_finish(lgs_ctx* c, lgs_commit_data* cd);
+void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u64* z_host,
+               size_t zlen, const u64* fields_host, size_t nfields, const uint64_t* ints_host,
+               size_t nints, uint64_t cursors[2], std::vector<uint8_t>* proof_out);
+lgs_status set_error(lgs_status s, const std::string& msg);
+lgs_status status_of_current_exception();
+}  // namespace lgs

@@ -37,6 +37,7 @@ _SIGS = {
     "lgs_engine_wait": (C.c_int, [vp, C.c_uint64, C.c_double, C.POINTER(_Result)]),
     "lgs_engine_free_proof": (None, [C.POINTER(C.c_uint8)]),
     "lgs_engine_pending": (C.c_int, [vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "lgs_engine_prepare": (C.c_int, [vp, C.POINTER(vp), C.c_size_t]),
 }
 
 
@@ -112,6 +113,13 @@ class ProverEngine:
         """Batch: submit every (pk, f, z, oracle) job, then collect them in order."""
         tickets = [self.submit(*j) for j in jobs]
         return [self.wait(t) for t in tickets]
+
+    def prepare(self, pks) -> None:
+        """Warm every lane for these proving keys' shapes (sizes scratch buffers and captures
+        each shape's prove as a CUDA graph).  Call before submitting jobs."""
+        pks = list(pks)
+        arr = (vp * max(1, len(pks)))(*[pk.handle for pk in pks])
+        check(self._lib.lgs_engine_prepare(self.handle, arr, len(pks)))
 
     def pending(self) -> tuple[int, int]:
         q, b = C.c_size_t(), C.c_size_t()

@@ -45,6 +45,11 @@ def test_engine_matches_one_at_a_time_path(keyed_jobs):
     with ProverEngine(0, lanes=3) as eng:
         res = eng.run([(keys[s][0], f, z, L.RandomOracle(o, length=1024)) for s, f, z, o in jobs])
     assert [(r.commit.root, r.proof.data) for r in res] == ref
+    with ProverEngine(0, lanes=3) as eng:  # prepared lanes replay captured proves
+        eng.prepare(pk for pk, _ in keys.values())
+        res = eng.run([(keys[s][0], f, z, L.RandomOracle(o, length=1024)) for s, f, z, o in jobs])
+        res += eng.run([(keys[s][0], f, z, L.RandomOracle(o, length=1024)) for s, f, z, o in jobs])
+    assert [(r.commit.root, r.proof.data) for r in res] == ref + ref
     for (shape, _, z, os_), r in zip(jobs, res):
         o = L.RandomOracle(os_, length=1024)
         assert L.Ligesis.verify(keys[shape][1], r.commit, z, r.proof, o)

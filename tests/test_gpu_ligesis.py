@@ -115,6 +115,45 @@ def test_second_proof_from_advanced_cursors_matches_oracle(pair, orc):
     assert tuple(int(c) for c in o.cursors) == cur2
 
 
+def test_captured_and_replayed_proofs_match_oracle(lgs, orc):
+    """On a fresh context the first prove of a shape runs eagerly, the second is captured into a
+    CUDA graph and the rest replay it: every proof, each from its own point and oracle, is the
+    oracle's, whichever path made it."""
+    log_m, log_n = 4, 11
+    f, A, _, _, _ = ligesis_inputs(log_m, log_n, seed=77)
+    ctx = L.Context(0)
+    pk, _ = L.Ligesis.setup_with_hash(log_m, log_n, L.SubsetSumHash(64 << log_m, a=A), ctx)
+    commit, data = L.Ligesis.commit(pk, L.MlPoly(f))
+    key = orc.Key(log_m, log_n, A)
+    cm = orc.Commitment(key, f)
+    assert commit.root == cm.root
+    for i in range(5):
+        z = rng.ext_elements(300 + i, log_m + log_n)
+        g = rng.SeededRng(400 + i)
+        fields, ints = g.ext_elements(2048), g.ints(2048)
+        o = L.RandomOracle(0, length=8)
+        o.fields, o.ints = np.ascontiguousarray(fields), np.ascontiguousarray(ints)
+        got = L.Ligesis.prove(pk, data, z, o)
+        want, cur = orc.prove(key, cm, z, fields, ints)
+        assert got.data == want, f"proof {i}"
+        assert tuple(int(c) for c in o.cursors) == cur
+    # a new commitment (new device buffers) and a new key of the same shape replay the graph too
+    f2 = rng.field_elements(78, 1 << (log_m + log_n))
+    A2 = rng.field_elements(79, 32 * (64 << log_m)).reshape(32, 64 << log_m)
+    for key_a, poly in ((A, f2), (A2, f), (A2, f2)):
+        pk2 = pk if key_a is A else L.Ligesis.setup_with_hash(
+            log_m, log_n, L.SubsetSumHash(64 << log_m, a=key_a), ctx)[0]
+        c2, d2 = L.Ligesis.commit(pk2, L.MlPoly(poly))
+        z = rng.ext_elements(310, log_m + log_n)
+        o = L.RandomOracle(411, length=2048)
+        got = L.Ligesis.prove(pk2, d2, z, o)
+        key2 = orc.Key(log_m, log_n, key_a)
+        cm2 = orc.Commitment(key2, poly)
+        o2 = L.RandomOracle(411, length=2048)
+        want, _ = orc.prove(key2, cm2, z, o2.fields, o2.ints)
+        assert c2.root == cm2.root and got.data == want
+
+
 def test_public_api_round_trip(lgs):
     """Ligesis::setup/commit/prove/verify through the reference-shaped API (ligesis.rs:808-822)."""
     g = L.SeededRng(123)
