@@ -477,6 +477,40 @@ def run_serve(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_commit(args) -> None:
+    """Setup, then `--steps` commits of the mu=24 polynomial already in HBM (no prove): the
+    case the per-kernel ncu captures of the commit kernels run."""
+    import numpy as np
+    import torch
+
+    import ligesis_b200 as L
+    from ligesis_b200 import rng
+
+    lm, ln = args.log_m, args.log_n
+    lib = L.load()
+    ctx = L.Context(0)
+    f = rng.field_elements(1, 1 << (lm + ln))
+    A = rng.field_elements(2, 32 * (64 << lm)).reshape(32, 64 << lm)
+    pk, _ = L.Ligesis.setup_with_hash(lm, ln, L.SubsetSumHash(64 << lm, a=A), ctx)
+    f_dev = torch.from_numpy(f.view(np.int64)).to("cuda:0")
+    import ctypes as C
+
+    L._lib.check(lib.lgs_profile(ctx.handle, 1))
+    roots = set()
+    for _ in range(args.steps):
+        commit, data = L.Ligesis.commit_device(pk, f_dev.data_ptr(), f.size)
+        roots.add(commit.root)
+        del data
+    stages = {}
+    for name in ("rs_encode", "subset_sum_hash", "merkle_h"):
+        tot, cnt = C.c_double(), C.c_uint64()
+        L._lib.check(lib.lgs_profile_get(ctx.handle, name.encode(), C.byref(tot), C.byref(cnt)))
+        if cnt.value:
+            stages[name] = round(tot.value / cnt.value, 4)
+    print(json.dumps({"mode": "commit", "log_m": lm, "log_n": ln, "commits": args.steps,
+                      "stages_ms": stages, "roots_identical": len(roots) == 1}), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -484,7 +518,9 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", choices=["line", "batch", "serve"], default="line")
+    ap.add_argument("--mode", choices=["line", "batch", "serve", "commit"], default="line")
+    ap.add_argument("--log-m", type=int, default=LOG_M)
+    ap.add_argument("--log-n", type=int, default=LOG_N)
     ap.add_argument("--lanes", type=int, default=8)
     ap.add_argument("--requests", type=int, default=600)
     ap.add_argument("--rate", type=float, default=200.0)
@@ -496,6 +532,9 @@ def main() -> None:
         return
     if args.mode == "serve":
         run_serve(args)
+        return
+    if args.mode == "commit":
+        run_commit(args)
         return
     if args.impl == "reference":
         run_reference(args)

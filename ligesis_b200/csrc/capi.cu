@@ -129,6 +129,7 @@ void lgs_ctx_destroy(lgs_ctx* ctx) {
   ctx->arena.overflow.clear();
   ctx->arena.mem.release();
   ctx->tw.release();
+  ctx->rs_tw.release();
   ctx->err.release();
   if (ctx->st) cudaStreamSynchronize(ctx->st);
   for (int i = 0; i < lgs_ctx::NSIDE; ++i) {
@@ -305,7 +306,10 @@ lgs_status lgs_dft(lgs_ctx* ctx, const uint64_t* in, size_t n_in, size_t batch,
     std::vector<u64> canon(in, in + batch * n_in);
     for (auto& x : canon) x = gl_canon(x);
     LGS_CUDA(cudaMemcpyAsync(d_in, canon.data(), canon.size() * 8, cudaMemcpyHostToDevice, ctx->st));
-    ntt_batch(d_in, n_in, n_in, d_out, N, log_size, batch, scr, ctx->tw.as<u64>(), ctx->st);
+    if (rs_dft_supported(log_size, n_in))
+      rs_dft_rows(d_in, n_in, n_in, d_out, N, log_size, batch, scr, ctx->rs_tw.as<u64>(), ctx->st);
+    else
+      ntt_batch(d_in, n_in, n_in, d_out, N, log_size, batch, scr, ctx->tw.as<u64>(), ctx->st);
     LGS_CUDA(cudaMemcpyAsync(out, d_out, batch * N * 8, cudaMemcpyDeviceToHost, ctx->st));
     LGS_CUDA(cudaStreamSynchronize(ctx->st));
   });

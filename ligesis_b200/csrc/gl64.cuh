@@ -42,14 +42,89 @@ GL_HD u64 gl_reduce(u64 lo, u64 hi) {
   if (t2 < t1) t2 += GL_EPS;
   return t2 >= GL_P ? t2 - GL_P : t2;
 }
+#ifdef __CUDA_ARCH__
+// Device versions on 32-bit carry chains.  Operands and results are canonical.
+__device__ __forceinline__ u64 gl_pack(uint32_t lo, uint32_t hi) {
+  return ((u64)hi << 32) | lo;
+}
+// a + b: s = a + b (carry c1), t = s + eps = s - p (carry c2); exactly one of "c1 or c2" says
+// that the canonical result is t (a, b < p, so they are never both set).
+__device__ __forceinline__ u64 gl_add(u64 a, u64 b) {
+  uint32_t s0, s1, t0, t1, c;
+  asm("add.cc.u32 %0, %5, %7;\n\t"
+      "addc.cc.u32 %1, %6, %8;\n\t"
+      "addc.u32 %2, 0, 0;\n\t"
+      "add.cc.u32 %3, %0, 0xffffffff;\n\t"
+      "addc.cc.u32 %4, %1, 0;\n\t"
+      "addc.u32 %2, %2, 0;"
+      : "=&r"(s0), "=&r"(s1), "=&r"(c), "=&r"(t0), "=&r"(t1)
+      : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+  return c ? gl_pack(t0, t1) : gl_pack(s0, s1);
+}
+// a - b: on a borrow, d = a - b + 2^64 and the result is d - eps = a - b + p.
+__device__ __forceinline__ u64 gl_sub(u64 a, u64 b) {
+  uint32_t d0, d1;
+  asm("{\n\t.reg .u32 m;\n\t"
+      "sub.cc.u32 %0, %2, %4;\n\t"
+      "subc.cc.u32 %1, %3, %5;\n\t"
+      "subc.u32 m, 0, 0;\n\t"
+      "sub.cc.u32 %0, %0, m;\n\t"
+      "subc.u32 %1, %1, 0;\n\t}"
+      : "=&r"(d0), "=&r"(d1)
+      : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+  return gl_pack(d0, d1);
+}
+// (r0 + r1 2^32 + r2 2^64 + r3 2^96) mod p = (r0 + r1 2^32) - r3 + r2 (2^32 - 1).
+__device__ __forceinline__ u64 gl_reduce4(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3) {
+  uint32_t w0, w1, t0, t1, c;
+  asm("{\n\t.reg .u32 u0, u1, m, v0, v1;\n\t"
+      "sub.cc.u32 u0, %5, %8;\n\t"       // u = lo - r3
+      "subc.cc.u32 u1, %6, 0;\n\t"
+      "subc.u32 m, 0, 0;\n\t"
+      "sub.cc.u32 u0, u0, m;\n\t"        // borrow: u -= eps
+      "subc.u32 u1, u1, 0;\n\t"
+      "sub.cc.u32 v0, 0, %7;\n\t"        // v = r2 2^32 - r2
+      "subc.u32 v1, %7, 0;\n\t"
+      "add.cc.u32 %0, u0, v0;\n\t"       // w = u + v
+      "addc.cc.u32 %1, u1, v1;\n\t"
+      "addc.u32 m, 0, 0;\n\t"
+      "neg.s32 m, m;\n\t"                 // carry: w += eps (cannot carry again)
+      "add.cc.u32 %0, %0, m;\n\t"
+      "addc.u32 %1, %1, 0;\n\t"
+      "add.cc.u32 %2, %0, 0xffffffff;\n\t" // t = w - p
+      "addc.cc.u32 %3, %1, 0;\n\t"
+      "addc.u32 %4, 0, 0;\n\t}"
+      : "=&r"(w0), "=&r"(w1), "=&r"(t0), "=&r"(t1), "=&r"(c)
+      : "r"(r0), "r"(r1), "r"(r2), "r"(r3));
+  return c ? gl_pack(t0, t1) : gl_pack(w0, w1);
+}
+__device__ __forceinline__ u64 gl_mul(u64 a, u64 b) {
+  const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32);
+  const uint32_t b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+  uint32_t r0, r1, r2, r3;
+  asm("mul.lo.u32 %0, %4, %6;\n\t"
+      "mul.hi.u32 %1, %4, %6;\n\t"
+      "mad.lo.cc.u32 %1, %4, %7, %1;\n\t"
+      "madc.hi.u32 %2, %4, %7, 0;\n\t"
+      "mad.lo.cc.u32 %1, %5, %6, %1;\n\t"
+      "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+      "madc.hi.u32 %3, %5, %7, 0;\n\t"
+      "mad.lo.cc.u32 %2, %5, %7, %2;\n\t"
+      "addc.u32 %3, %3, 0;"
+      : "=&r"(r0), "=&r"(r1), "=&r"(r2), "=&r"(r3)
+      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+  return gl_reduce4(r0, r1, r2, r3);
+}
+#else
 GL_HD u64 gl_add(u64 a, u64 b) {
   u64 s = a + b;
   if (s < a) s += GL_EPS;
   return s >= GL_P ? s - GL_P : s;
 }
 GL_HD u64 gl_sub(u64 a, u64 b) { return a >= b ? a - b : a + (GL_P - b); }
-GL_HD u64 gl_neg(u64 a) { return a ? GL_P - a : 0; }
 GL_HD u64 gl_mul(u64 a, u64 b) { return gl_reduce(a * b, gl_mulhi(a, b)); }
+#endif
+GL_HD u64 gl_neg(u64 a) { return a ? GL_P - a : 0; }
 GL_HD u64 gl_canon(u64 a) { return a >= GL_P ? a - GL_P : a; }
 GL_HD u64 gl_pow(u64 a, u64 e) {
   u64 r = 1;

@@ -18,6 +18,17 @@ void ntt_batch(const u64* in, size_t in_stride, size_t n_in, u64* out, size_t ou
 void transpose_u64(const u64* in, u64* out, size_t rows, size_t cols, size_t batch,
                    cudaStream_t st);
 
+// rs_dft.cu: the commitment rows' RS encoding for 2^RS_LOGN_MIN <= N <= 2^RS_LOGN_MAX, from N/2
+// (zero-padded) or N input values per row.  z: rows x N scratch.  tables: the context's
+// rs_tables_elems() twiddles built by build_rs_tables from the main table.
+constexpr unsigned RS_LOGN_MIN = 14, RS_LOGN_MAX = 18;
+size_t rs_tables_elems();
+size_t rs_table_offset(unsigned logN);
+void build_rs_tables(u64* tables, const u64* tw, cudaStream_t st);
+bool rs_dft_supported(unsigned logN, size_t n_in);
+void rs_dft_rows(const u64* in, size_t ld_in, size_t n_in, u64* out, size_t ld_out,
+                 unsigned logN, size_t rows, u64* z, const u64* tables, cudaStream_t st);
+
 // hash_tc.cu (tcgen05): also writes the Merkle leaf hashes of H's columns into `leaves`.
 void alimb_from_a(const u64* A, uint8_t* alimb, size_t W, cudaStream_t st);
 void make_alimb_tmap(const uint8_t* alimb, size_t W, void* tmap_out);

@@ -197,6 +197,8 @@ void ctx_init(lgs_ctx* c, int device) {
   if (tensor_map_bytes() > sizeof(((lgs_pk*)nullptr)->tmap))
     throw std::runtime_error("tensor map larger than its slot");
   build_twiddles(c->tw.as<u64>(), c->st);
+  c->rs_tw.alloc(rs_tables_elems() * sizeof(u64), c->st);
+  build_rs_tables(c->rs_tw.as<u64>(), c->tw.as<u64>(), c->st);
   LGS_CUDA(cudaStreamSynchronize(c->st));
 }
 
@@ -264,7 +266,12 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
   u64* scr = logN > 12 ? c->arena.get<u64>(m * two_n) : nullptr;
   {
     StageTimer t(c->prof, c->st, "rs_encode");
-    ntt_batch(cd->f.as<u64>(), n, n, cd->cw.as<u64>(), two_n, logN, m, scr, c->tw.as<u64>(), c->st);
+    if (rs_dft_supported(logN, n))
+      rs_dft_rows(cd->f.as<u64>(), n, n, cd->cw.as<u64>(), two_n, logN, m, scr,
+                  c->rs_tw.as<u64>(), c->st);
+    else
+      ntt_batch(cd->f.as<u64>(), n, n, cd->cw.as<u64>(), two_n, logN, m, scr, c->tw.as<u64>(),
+                c->st);
   }
   {
     StageTimer t(c->prof, c->st, "subset_sum_hash");  // H and its Merkle leaf hashes

@@ -221,6 +221,7 @@ struct lgs_ctx {
   cudaEvent_t ev_done[NSIDE] = {};
   cudaEvent_t ev_fork = nullptr;
   lgs::DevMem tw;
+  lgs::DevMem rs_tw;  // twiddles of the row RS encoding (rs_dft.cu)
   lgs::Arena arena;
   lgs::Profiler prof;
   lgs::DevMem err;  // device error word of bounded-wait kernels (0 = ok)

@@ -14,7 +14,9 @@ pytestmark = pytest.mark.gpu
 
 @pytest.mark.parametrize("log_size,n_in,batch", [(1, 1, 3), (4, 8, 2), (10, 512, 4), (12, 4096, 2),
                                                  (13, 4096, 3), (15, 16384, 2), (18, 131072, 2),
-                                                 (20, 1 << 19, 1), (14, 5, 2), (17, 1 << 17, 1)])
+                                                 (20, 1 << 19, 1), (14, 5, 2), (17, 1 << 17, 1),
+                                                 (14, 8192, 3), (14, 16384, 2), (16, 1 << 15, 5),
+                                                 (16, 1 << 16, 1), (18, 1 << 18, 1)])
 def test_dft_matches_oracle(lgs, orc, log_size, n_in, batch):
     c = rng.field_elements(1000 + log_size, batch * n_in).reshape(batch, n_in)
     got = L.dft(c, log_size)
@@ -27,6 +29,19 @@ def test_dft_reduces_noncanonical_input(lgs, orc):
     got = L.dft(c, 3)[0]
     want = orc.dft_bf(np.array([0, 5, (1 << 64) - 1 - P, 3], dtype=np.uint64), 8)
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("log_size", [14, 18])
+def test_dft_large_reduces_noncanonical_input(lgs, orc, log_size):
+    # the four-step row transform (2^14 .. 2^18) canonicalises what it reads, like the small one
+    n_in = 1 << (log_size - 1)
+    c = rng.field_elements(555, 2 * n_in).reshape(2, n_in)
+    c[0, ::7] = np.uint64(P)
+    c[1, 3::11] = np.uint64((1 << 64) - 1)
+    got = L.dft(c, log_size)
+    canon = np.where(c >= np.uint64(P), c - np.uint64(P), c)
+    for b in range(2):
+        assert np.array_equal(got[b], orc.dft_bf(canon[b], 1 << log_size)), b
 
 
 @pytest.mark.parametrize("m,cols", [(1, 128), (2, 256), (8, 2048), (16, 384), (128, 1024)])
