@@ -136,6 +136,10 @@ lgs_status lgs_profile(lgs_ctx* ctx, int enable);
 lgs_status lgs_profile_get(lgs_ctx* ctx, const char* stage, double* total_ms, uint64_t* count);
 /* Number of kernels this library has launched in this process. */
 uint64_t lgs_launch_count(void);
+/* The int8 tensor-core rate the subset-sum hash is measured against: every SM issues `iters` x 4
+ * back-to-back tcgen05.mma.kind::i8 M128 N256 K32 from shared memory (the hash's MMA shape);
+ * *tops receives the best of three timed launches in TOP/s (2 ops per multiply-add). */
+lgs_status lgs_tensor_peak_i8(lgs_ctx* ctx, unsigned iters, double* tops);
 
 /* ---- the individual device operations of the path (host buffers in and out) ---- */
 

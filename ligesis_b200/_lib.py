@@ -65,6 +65,7 @@ _SIGS = {
     "lgs_profile": (C.c_int, [vp, C.c_int]),
     "lgs_profile_get": (C.c_int, [vp, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "lgs_launch_count": (C.c_uint64, []),
+    "lgs_tensor_peak_i8": (C.c_int, [vp, C.c_uint, C.POINTER(C.c_double)]),
     "lgs_dft": (C.c_int, [vp, u64p, C.c_size_t, C.c_size_t, C.c_uint, u64p]),
     "lgs_subset_sum_hash": (C.c_int, [vp, u64p, C.c_size_t, u64p, C.c_size_t, u64p]),
     "lgs_merkle_root": (C.c_int, [vp, u64p, C.c_size_t, C.c_uint, u8p]),

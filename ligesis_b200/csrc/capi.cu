@@ -149,6 +149,20 @@ void lgs_ctx_destroy(lgs_ctx* ctx) {
   delete ctx;
 }
 
+lgs_status lgs_tensor_peak_i8(lgs_ctx* ctx, unsigned iters, double* tops) {
+  return guarded([&] {
+    need(ctx && tops && iters >= 1 && iters <= (1u << 20), "lgs_tensor_peak_i8: bad argument");
+    CtxDevice dg(ctx);
+    *tops = i8_tensor_peak_tops(iters, ctx->err.as<int>(), ctx->st);
+    int err = 0;
+    LGS_CUDA(cudaMemcpy(&err, ctx->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) {
+      LGS_CUDA(cudaMemset(ctx->err.p, 0, sizeof(int)));
+      throw DeviceTimeout("tensor peak: a bounded device wait gave up");
+    }
+  });
+}
+
 lgs_status lgs_ctx_stream(lgs_ctx* ctx, void** stream) {
   return guarded([&] {
     need(ctx && stream, "lgs_ctx_stream: null argument");

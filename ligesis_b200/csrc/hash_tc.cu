@@ -7,17 +7,19 @@
 // exact int32 sum (terms <= 255, at most 64 * 2^13 of them), and H[r][j] = sum_l 2^(8l) S_l mod p
 // is recombined exactly in 128-bit arithmetic.
 //
-// CTA tile: all 256 limb rows (two M = 128 accumulators in TMEM, 2 x 256 columns = the SM's
-// 512 TMEM columns) by 256 codeword columns (N = 256); K advances 128 bytes (two codeword rows)
-// per pipeline stage, 3 stages.
-//   warp 5        TMA producer: the 256 x 128-byte A-limb tile, SWIZZLE_128B, no multicast
-//   warps 0-3     B producers: expand 2 x 256 codeword words into the 256 x 128-byte K-major
-//                 SWIZZLE_128B bit tile; later the epilogue
-//   warp 4        TMEM allocation, and one thread issuing tcgen05.mma.kind::i8 (M128 N256 K32)
-// Epilogue: tcgen05.ld the int32 limb sums, recombine mod p, write H, hash each 256-byte column
-// leaf with BLAKE3 into the Merkle tree's leaf layer.  Every mbarrier wait is bounded by a clock
-// budget; on timeout the CTA records an error code, stops issuing work, waits (bounded) for its
-// issued MMAs, frees its TMEM and exits.
+// Persistent CTAs (one per SM) walk the 256-column tiles.  A tile is all 256 limb rows (two
+// M = 128 accumulators in TMEM, 2 x 256 columns = the SM's 512 TMEM columns) by 256 codeword
+// columns (N = 256); K advances 128 bytes (two codeword rows) per pipeline stage, 3 stages.
+//   warp 0      TMA producer: the 256 x 128-byte A-limb tile, SWIZZLE_128B, no multicast
+//   warp 1      TMEM allocation, and one thread issuing tcgen05.mma.kind::i8 (M128 N256 K32)
+//   warps 2-5   B producers: expand 2 x 256 codeword words (loaded three stages ahead) into the
+//               256 x 128-byte K-major SWIZZLE_128B bit tile
+//   warps 6-9   epilogue: tcgen05.ld the int32 limb sums, recombine mod p, write H, release the
+//               accumulators; then hash each 256-byte column leaf with BLAKE3 (reading H back
+//               from L2) while the MMAs of the next tile run.
+// Every mbarrier wait is bounded by a clock budget and watches a CTA-wide failure flag; on a
+// timeout the CTA records an error code, every role stops issuing work, the MMA thread waits
+// (bounded) for the MMAs it issued, and the TMEM is freed before the CTA exits.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -34,9 +36,14 @@ constexpr int A_TILE = 256 * TC_KB;
 constexpr int B_TILE = TC_N * TC_KB;
 constexpr int STAGE_BYTES = A_TILE + B_TILE;
 constexpr int NPROD = 128;
-constexpr int NTHREADS = 192;
+constexpr int NEPI = 128;
+constexpr int NTHREADS = 320;
 constexpr int TMEM_COLS = 512;
-constexpr int SMEM_BYTES = TC_STAGES * STAGE_BYTES + 1024 /*align*/ + 128 /*barriers*/;
+constexpr int EPI_COLS = 16;     // accumulator columns drained per epilogue step
+constexpr int SS_PITCH = 260;    // u32 per drained column (256 limb rows + pad, 16-byte rows)
+constexpr int SS_BYTES = EPI_COLS * SS_PITCH * 4;
+constexpr int NBARS = 2 * TC_STAGES + 3;
+constexpr int SMEM_BYTES = TC_STAGES * STAGE_BYTES + SS_BYTES + 1024 /*align*/ + 128 /*barriers*/;
 constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s at 1.9 GHz
 // instruction descriptor: D = S32 (2 << 4), A = B = U8 (0), both K-major, N = 256, M = 128
 constexpr uint32_t IDESC = (2u << 4) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
@@ -54,20 +61,36 @@ __device__ __forceinline__ void mbar_arrive_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
                : "memory");
 }
-// Bounded wait for the phase with the given parity to complete; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Bounded wait for the phase with the given parity to complete.  false on timeout, or as soon as
+// another role has flagged a failure (*fail != 0).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* fail) {
   const long long t0 = clock64();
   while (true) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (done) return true;
+    if (mbar_test(bar, parity)) return true;
+    if (*fail) return false;
     if (clock64() - t0 > WAIT_CYCLES) return false;
   }
+}
+// Bounded wait that ignores the failure flag (draining work already issued).
+__device__ __forceinline__ bool mbar_wait_drain(uint32_t bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_test(bar, parity))
+    if (clock64() - t0 > WAIT_CYCLES) return false;
+  return true;
+}
+__device__ __forceinline__ void flag_failure(volatile int* fail, int* err, int code) {
+  *fail = 1;
+  atomicExch(err, code);
 }
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
   uint64_t d = (uint64_t)((addr >> 4) & 0x3FFFu);  // start address
@@ -90,17 +113,30 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
       "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
       : "memory");
 }
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
-      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15}, [%16];\n"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
         "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
-        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
-        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+// Barrier of the 128 epilogue threads that also ANDs their flags, so that they leave a loop
+// together (a lone warp left behind would wait at the next named barrier for good).
+__device__ __forceinline__ bool epi_all(bool ok) {
+  uint32_t r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.and.pred q, 1, 128, p;\n"
+      " selp.u32 %0, 1, 0, q;\n}\n"
+      : "=r"(r)
+      : "r"((uint32_t)ok)
+      : "memory");
+  return r != 0;
 }
 __device__ __forceinline__ uint32_t nib_expand(uint32_t nib) {
   return (nib * 0x00204081u) & 0x01010101u;
@@ -113,13 +149,18 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                    int* __restrict__ err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint64_t* bars = (uint64_t*)(smem + TC_STAGES * STAGE_BYTES);
-  uint32_t* tmem_holder = (uint32_t*)(bars + 8);
-  const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[3]), done = smem_u32(&bars[6]);
+  uint32_t* Ss = (uint32_t*)(smem + TC_STAGES * STAGE_BYTES);
+  uint64_t* bars = (uint64_t*)(smem + TC_STAGES * STAGE_BYTES + SS_BYTES);
+  uint32_t* tmem_holder = (uint32_t*)(bars + NBARS);
+  const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[TC_STAGES]);
+  const uint32_t acc_full = smem_u32(&bars[2 * TC_STAGES]);
+  const uint32_t acc_empty = smem_u32(&bars[2 * TC_STAGES + 1]);
+  const uint32_t drain = smem_u32(&bars[2 * TC_STAGES + 2]);
   const unsigned tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const size_t j0 = (size_t)blockIdx.x * TC_N;
   const unsigned nchunks = (m + 1) / 2;
-  __shared__ int s_fail;
+  const unsigned ntiles = (unsigned)(two_n / TC_N);
+  const unsigned my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  __shared__ volatile int s_fail;
 
   if (tid == 0) {
     s_fail = 0;
@@ -127,10 +168,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       mbar_init(full0 + 8 * s, NPROD + 1);
       mbar_init(empty0 + 8 * s, 1);
     }
-    mbar_init(done, 1);
+    mbar_init(acc_full, 1);
+    mbar_init(acc_empty, NEPI);
+    mbar_init(drain, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 4) {
+  if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_holder)),
                  "r"(TMEM_COLS)
@@ -141,18 +184,17 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_holder;
+  const unsigned nfill = my_tiles * nchunks;
 
-  if (warp == 5) {
+  if (warp == 0) {
     // ---- TMA producer: A-limb tiles ----
     if (lane == 0) {
-      for (unsigned c = 0; c < nchunks; ++c) {
-        const unsigned s = c % TC_STAGES;
-        if (c >= TC_STAGES && !mbar_wait(empty0 + 8 * s, ((c / TC_STAGES) - 1) & 1)) {
-          atomicExch(err, 1);
-          s_fail = 1;
+      for (unsigned f = 0; f < nfill; ++f) {
+        const unsigned s = f % TC_STAGES, c = f % nchunks;
+        if (f >= TC_STAGES && !mbar_wait(empty0 + 8 * s, ((f / TC_STAGES) - 1) & 1, &s_fail)) {
+          if (!s_fail) flag_failure(&s_fail, err, 1);
           break;
         }
-        if (s_fail) break;
         const uint32_t bar = full0 + 8 * s;
         mbar_arrive_tx(bar, A_TILE);
         const uint32_t dst = smem_u32(smem + s * STAGE_BYTES);
@@ -164,48 +206,76 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             : "memory");
       }
     }
-  } else if (warp == 4) {
+  } else if (warp == 1) {
     // ---- MMA issuer ----
     if (lane == 0) {
+      unsigned f = 0;
       bool ok = true;
-      for (unsigned c = 0; c < nchunks && ok; ++c) {
-        const unsigned s = c % TC_STAGES;
-        if (!mbar_wait(full0 + 8 * s, (c / TC_STAGES) & 1)) {
-          atomicExch(err, 2);
-          s_fail = 1;
-          ok = false;
-          break;
+      for (unsigned t = 0; t < my_tiles && ok; ++t) {
+        if (t > 0) {
+          if (!mbar_wait(acc_empty, (t - 1) & 1, &s_fail)) {
+            if (!s_fail) flag_failure(&s_fail, err, 2);
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         }
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t a_base = smem_u32(smem + s * STAGE_BYTES);
-        const uint32_t b_base = a_base + A_TILE;
+        for (unsigned c = 0; c < nchunks; ++c, ++f) {
+          const unsigned s = f % TC_STAGES;
+          if (!mbar_wait(full0 + 8 * s, (f / TC_STAGES) & 1, &s_fail)) {
+            if (!s_fail) flag_failure(&s_fail, err, 3);
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a_base = smem_u32(smem + s * STAGE_BYTES);
+          const uint32_t b_base = a_base + A_TILE;
 #pragma unroll
-        for (int t = 0; t < 2; ++t)
+          for (int h = 0; h < 2; ++h)
 #pragma unroll
-          for (int ks = 0; ks < 4; ++ks)
-            mma_i8(tmem + t * 256, sw128_desc(a_base + t * (128 * TC_KB) + ks * 32),
-                   sw128_desc(b_base + ks * 32), (c > 0 || ks > 0) ? 1u : 0u);
-        mma_commit(empty0 + 8 * s);
+            for (int ks = 0; ks < 4; ++ks)
+              mma_i8(tmem + h * 256, sw128_desc(a_base + h * (128 * TC_KB) + ks * 32),
+                     sw128_desc(b_base + ks * 32), (c > 0 || ks > 0) ? 1u : 0u);
+          mma_commit(empty0 + 8 * s);
+        }
+        if (ok) mma_commit(acc_full);
       }
-      mma_commit(done);  // arrives once every issued MMA has completed
+      // Every MMA issued so far has completed once this arrives; wait for it before the TMEM
+      // is freed (also after a failure).
+      mma_commit(drain);
+      if (!mbar_wait_drain(drain, 0)) atomicExch(err, 7);
     }
-  } else {
-    // ---- B producers (threads 0..127) ----
-    for (unsigned c = 0; c < nchunks; ++c) {
-      const unsigned s = c % TC_STAGES;
-      if (c >= TC_STAGES && !mbar_wait(empty0 + 8 * s, ((c / TC_STAGES) - 1) & 1)) {
-        atomicExch(err, 3);
-        s_fail = 1;
-        break;
+  } else if (warp < 6) {
+    // ---- B producers (128 threads): two columns each, words loaded three fills ahead ----
+    const unsigned pt = tid - 64;
+    auto load_fill = [&](unsigned f, u64 (&w)[4]) {
+      if (f >= nfill) return;
+      const unsigned tl = f / nchunks, c = f % nchunks;
+      const size_t j0 = (size_t)(blockIdx.x + tl * gridDim.x) * TC_N;
+      const bool two = 2 * c + 1 < m;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const size_t j = j0 + pt + h * NPROD;
+        w[2 * h] = __ldg(cw + (size_t)(2 * c) * two_n + j);
+        w[2 * h + 1] = two ? __ldg(cw + (size_t)(2 * c + 1) * two_n + j) : 0;
       }
-      if (s_fail) break;
+    };
+    // one fill: wait for the stage, expand the words of fill f from w, then reuse w for the
+    // loads of fill f + 3 (so each load has three stages of MMA time to arrive)
+    auto fill = [&](unsigned f, u64 (&w)[4]) -> bool {
+      const unsigned s = f % TC_STAGES;
+      if (f >= TC_STAGES && !mbar_wait(empty0 + 8 * s, ((f / TC_STAGES) - 1) & 1, &s_fail)) {
+        if (!s_fail) flag_failure(&s_fail, err, 4);
+        return false;
+      }
       uint8_t* bt = smem + s * STAGE_BYTES + A_TILE;
-      for (unsigned j = tid; j < TC_N; j += NPROD) {
-        const u64 w0 = __ldg(cw + (size_t)(2 * c) * two_n + j0 + j);
-        const u64 w1 = (2 * c + 1 < m) ? __ldg(cw + (size_t)(2 * c + 1) * two_n + j0 + j) : 0;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const unsigned j = pt + h * NPROD;
+        const u64 a = w[2 * h], b = w[2 * h + 1];
 #pragma unroll
         for (int kc = 0; kc < 8; ++kc) {
-          const uint32_t b16 = (uint32_t)((kc < 4 ? (w0 >> (16 * kc)) : (w1 >> (16 * (kc - 4)))) & 0xFFFFu);
+          const uint32_t b16 = (uint32_t)((kc < 4 ? (a >> (16 * kc)) : (b >> (16 * (kc - 4)))) & 0xFFFFu);
           uint4 v;
           v.x = nib_expand(b16 & 15u);
           v.y = nib_expand((b16 >> 4) & 15u);
@@ -216,74 +286,167 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(full0 + 8 * s);
+      load_fill(f + 3, w);
+      return true;
+    };
+    u64 w0[4] = {0, 0, 0, 0}, w1[4] = {0, 0, 0, 0}, w2[4] = {0, 0, 0, 0};
+    load_fill(0, w0);
+    load_fill(1, w1);
+    load_fill(2, w2);
+    for (unsigned f = 0; f < nfill; f += 3) {
+      if (!fill(f, w0)) break;
+      if (f + 1 >= nfill || !fill(f + 1, w1)) break;
+      if (f + 2 >= nfill || !fill(f + 2, w2)) break;
     }
-  }
-
-  // ---- epilogue (warps 0-3) ----
-  if (warp < 4) {
-    const bool got = mbar_wait(done, 0);
-    if (!got) atomicExch(err, 4);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    uint32_t* Ss = (uint32_t*)smem;                    // [32 cols][256 limb rows]
-    u64* Hs = (u64*)(smem + 32 * 256 * 4);             // [256 cols][33] (padded)
-    for (int q = 0; q < TC_N / 32; ++q) {
-      uint32_t r0[32], r1[32];
-      const uint32_t lane_off = (uint32_t)(32 * warp) << 16;
-      tmem_ld32(tmem + lane_off + 32 * q, r0);
-      tmem_ld32(tmem + lane_off + 256 + 32 * q, r1);
-      const unsigned mrow = 32 * warp + lane;
-#pragma unroll
-      for (int cc = 0; cc < 32; ++cc) {
-        Ss[cc * 256 + mrow] = r0[cc];
-        Ss[cc * 256 + 128 + mrow] = r1[cc];
+  } else {
+    // ---- epilogue (128 threads, warps 6-9; TMEM lane quarter = warp % 4) ----
+    const unsigned et = tid - 192, quarter = warp & 3;
+    const uint32_t lane_off = (uint32_t)(32 * quarter) << 16;
+    const unsigned mrow = 32 * quarter + lane;
+    for (unsigned t = 0; t < my_tiles; ++t) {
+      const size_t j0 = (size_t)(blockIdx.x + t * gridDim.x) * TC_N;
+      const bool got = mbar_wait(acc_full, t & 1, &s_fail);
+      if (!epi_all(got)) {
+        if (!s_fail) flag_failure(&s_fail, err, 5);
+        break;
       }
-      asm volatile("bar.sync 1, 128;" ::: "memory");
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      for (int q = 0; q < TC_N / EPI_COLS; ++q) {
+        uint32_t r0[16], r1[16];
+        tmem_ld16(tmem + lane_off + EPI_COLS * q, r0);
+        tmem_ld16(tmem + lane_off + 256 + EPI_COLS * q, r1);
+        tmem_wait_ld();
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const unsigned idx = tid + 128 * i, r = idx & 31, col = idx >> 5;
-        const uint4 lo4 = *(const uint4*)&Ss[col * 256 + 8 * r];
-        const uint4 hi4 = *(const uint4*)&Ss[col * 256 + 8 * r + 4];
-        const u64 a = (u64)lo4.x + ((u64)lo4.y << 8) + ((u64)lo4.z << 16) + ((u64)lo4.w << 24);
-        const u64 b = (u64)hi4.x + ((u64)hi4.y << 8) + ((u64)hi4.z << 16) + ((u64)hi4.w << 24);
-        const u64 lo = a + (b << 32);
-        const u64 hi = (b >> 32) + (lo < a ? 1 : 0);
-        Hs[(32 * q + col) * 33 + r] = gl_reduce(lo, hi);
-      }
-      asm volatile("bar.sync 1, 128;" ::: "memory");
-    }
-    // H to global (row-major 32 x two_n), coalesced along columns
-    for (unsigned r = 0; r < 32; ++r)
-      for (unsigned col = tid; col < (unsigned)TC_N; col += NPROD)
-        H[(size_t)r * two_n + j0 + col] = Hs[col * 33 + r];
-    // leaf hash of each 256-byte column (C = 32 canonical u64, little-endian)
-    for (unsigned col = tid; col < (unsigned)TC_N; col += NPROD) {
-      const u64* hc = Hs + col * 33;
-      u32 cv[8];
-      b3_init(cv);
-#pragma unroll
-      for (int blk = 0; blk < 4; ++blk) {
-        u32 w[16];
-#pragma unroll
-        for (int q2 = 0; q2 < 8; ++q2) {
-          const u64 v = hc[blk * 8 + q2];
-          w[2 * q2] = (u32)v;
-          w[2 * q2 + 1] = (u32)(v >> 32);
+        for (int cc = 0; cc < EPI_COLS; ++cc) {
+          Ss[cc * SS_PITCH + mrow] = r0[cc];
+          Ss[cc * SS_PITCH + 128 + mrow] = r1[cc];
         }
-        const u32 flags = (blk == 0 ? B3_CHUNK_START : 0) | (blk == 3 ? (B3_CHUNK_END | B3_ROOT) : 0);
-        b3_compress(cv, w, 64, flags);
-      }
+        epi_sync();
 #pragma unroll
-      for (int q2 = 0; q2 < 8; ++q2) leaves[(j0 + col) * 8 + q2] = cv[q2];
+        for (int i = 0; i < 4; ++i) {
+          const unsigned idx = et + NEPI * i, col = idx & (EPI_COLS - 1), r = idx >> 4;
+          const uint4 lo4 = *(const uint4*)&Ss[col * SS_PITCH + 8 * r];
+          const uint4 hi4 = *(const uint4*)&Ss[col * SS_PITCH + 8 * r + 4];
+          const u64 a = (u64)lo4.x + ((u64)lo4.y << 8) + ((u64)lo4.z << 16) + ((u64)lo4.w << 24);
+          const u64 b = (u64)hi4.x + ((u64)hi4.y << 8) + ((u64)hi4.z << 16) + ((u64)hi4.w << 24);
+          const u64 lo = a + (b << 32);
+          const u64 hi = (b >> 32) + (lo < a ? 1 : 0);
+          H[(size_t)r * two_n + j0 + EPI_COLS * q + col] = gl_reduce(lo, hi);
+        }
+        epi_sync();
+      }
+      // accumulators drained: the MMAs of the next tile may start
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(acc_empty);
+      __threadfence_block();
+      epi_sync();
+      // leaf hash of each 256-byte column (C = 32 canonical u64, little-endian), from L2
+#pragma unroll 1
+      for (unsigned col = et; col < (unsigned)TC_N; col += NEPI) {
+        const u64* hc = H + j0 + col;
+        u32 cv[8];
+        b3_init(cv);
+#pragma unroll
+        for (int blk = 0; blk < 4; ++blk) {
+          u32 wd[16];
+#pragma unroll
+          for (int q2 = 0; q2 < 8; ++q2) {
+            const u64 v = __ldcg(hc + (size_t)(blk * 8 + q2) * two_n);
+            wd[2 * q2] = (u32)v;
+            wd[2 * q2 + 1] = (u32)(v >> 32);
+          }
+          const u32 flags = (blk == 0 ? B3_CHUNK_START : 0) | (blk == 3 ? (B3_CHUNK_END | B3_ROOT) : 0);
+          b3_compress(cv, wd, 64, flags);
+        }
+        uint4* lp = (uint4*)(leaves + (j0 + col) * 8);
+        lp[0] = make_uint4(cv[0], cv[1], cv[2], cv[3]);
+        lp[1] = make_uint4(cv[4], cv[5], cv[6], cv[7]);
+      }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 4) {
+  if (warp == 1) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(TMEM_COLS)
                  : "memory");
   }
+}
+
+// ---- the int8 tensor-core peak this hash is measured against ----------------------------------
+// One CTA per SM; one thread issues `iters` x 4 back-to-back tcgen05.mma.kind::i8 M128 N256 K32
+// on a fixed 128 x 128-byte A tile and 256 x 128-byte B tile in shared memory (the shape and
+// layout the hash uses), accumulating into TMEM; one commit at the end, waited with a bound.
+constexpr int PK_SMEM = 128 * TC_KB + 256 * TC_KB + 1024 + 64;
+
+__global__ void __launch_bounds__(128, 1) i8_peak_kernel(unsigned iters, int* __restrict__ err) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* bar = (uint64_t*)(smem + 128 * TC_KB + 256 * TC_KB);
+  uint32_t* tmem_holder = (uint32_t*)(bar + 1);
+  const unsigned tid = threadIdx.x, warp = tid >> 5;
+  for (unsigned i = tid; i < (128 + 256) * TC_KB / 16; i += blockDim.x)
+    ((uint4*)smem)[i] = make_uint4(0x01020304u * (i & 7), i, 0x80808080u, 0x7f7f7f7fu);
+  if (tid == 0) {
+    mbar_init(smem_u32(bar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_holder)),
+                 "r"(256)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_holder;
+  if (tid == 0) {
+    const uint32_t a_base = smem_u32(smem), b_base = a_base + 128 * TC_KB;
+    for (unsigned i = 0; i < iters; ++i)
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks)
+        mma_i8(tmem, sw128_desc(a_base + ks * 32), sw128_desc(b_base + ks * 32),
+               (i > 0 || ks > 0) ? 1u : 0u);
+    mma_commit(smem_u32(bar));
+    if (!mbar_wait_drain(smem_u32(bar), 0)) atomicExch(err, 8);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256)
+                 : "memory");
+  }
+}
+
+double i8_tensor_peak_tops(unsigned iters, int* err, cudaStream_t st) {
+  int dev = 0, sms = 0;
+  LGS_CUDA(cudaGetDevice(&dev));
+  LGS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  LGS_CUDA(cudaFuncSetAttribute(i8_peak_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                PK_SMEM));
+  cudaEvent_t e0, e1;
+  LGS_CUDA(cudaEventCreate(&e0));
+  LGS_CUDA(cudaEventCreate(&e1));
+  double best = 0.0;
+  for (int rep = 0; rep < 4; ++rep) {  // the first launch warms up; keep the best
+    LGS_CUDA(cudaEventRecord(e0, st));
+    i8_peak_kernel<<<sms, 128, PK_SMEM, st>>>(iters, err);
+    LGS_LAUNCH_CHECK();
+    LGS_CUDA(cudaEventRecord(e1, st));
+    LGS_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    LGS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    const double ops = 2.0 * 128 * 256 * 32 * 4.0 * iters * sms;
+    if (rep > 0 && ms > 0) best = std::max(best, ops / (ms * 1e-3) / 1e12);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return best;
 }
 
 // Alimb[8r + l][k] = byte l of A[r][k] (the 256 x W limb matrix the TMA descriptor covers).
@@ -340,8 +503,13 @@ void subset_sum_hash_tc(const void* tmap, const u64* cw, u64* H, u32* leaves, un
   if (m == 0 || m > 8192) throw ShapeError("hash: 1 <= m <= 8192");
   LGS_CUDA(cudaFuncSetAttribute(hash_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 SMEM_BYTES));
-  hash_tc_kernel<<<(unsigned)(two_n / TC_N), NTHREADS, SMEM_BYTES, st>>>(
-      *(const CUtensorMap*)tmap, cw, H, leaves, m, two_n, err);
+  int dev = 0, sms = 0;
+  LGS_CUDA(cudaGetDevice(&dev));
+  LGS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const size_t ntiles = two_n / TC_N;
+  const unsigned grid = (unsigned)std::min<size_t>(ntiles, (size_t)std::max(sms, 1));
+  hash_tc_kernel<<<grid, NTHREADS, SMEM_BYTES, st>>>(*(const CUtensorMap*)tmap, cw, H, leaves, m,
+                                                     two_n, err);
   LGS_LAUNCH_CHECK();
 }
 

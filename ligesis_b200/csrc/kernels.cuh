@@ -35,6 +35,8 @@ void make_alimb_tmap(const uint8_t* alimb, size_t W, void* tmap_out);
 size_t tensor_map_bytes();
 void subset_sum_hash_tc(const void* tmap, const u64* cw, u64* H, u32* leaves, unsigned m,
                         size_t two_n, int* err, cudaStream_t st);
+// Dense tcgen05 kind::i8 throughput (TOP/s) of back-to-back M128 N256 K32 MMAs on every SM.
+double i8_tensor_peak_tops(unsigned iters, int* err, cudaStream_t st);
 
 // merkle.cu
 size_t merkle_node_count(size_t nleaves);

@@ -58,6 +58,20 @@ def test_subset_sum_hash_matches_oracle(lgs, orc, m, cols):
     assert h.width == 64 * m
 
 
+@pytest.mark.parametrize("m,cols", [(8, 297 * 256 + 77), (3, 600 * 256)])
+def test_subset_sum_hash_many_tiles_per_cta(lgs, orc, m, cols):
+    # more 256-column tiles than SMs: every persistent CTA walks several tiles, and the pipeline
+    # stages wrap across tile boundaries (m = 3 and 8 give 2 and 4 stages per tile)
+    A = rng.field_elements(2100 + m, 32 * 64 * m).reshape(32, 64 * m)
+    cw = rng.field_elements(3100 + m, m * cols).reshape(m, cols)
+    from ligesis_b200._lib import Context, check, load, ptr64
+
+    got = np.zeros((32, cols), dtype=np.uint64)
+    check(load().lgs_subset_sum_hash(Context.default().handle, ptr64(A), m, ptr64(cw), cols,
+                                     ptr64(got)))
+    assert np.array_equal(got, orc.hash_columns(A, cw))
+
+
 def test_subset_sum_hash_extremes(lgs, orc):
     # every bit set and every limb 0xff-heavy: the largest int32 limb sums the kernel sees
     m, cols = 128, 256
