@@ -184,35 +184,36 @@ void eq_dot_dev(const void* vec, int is_bf, const ef2* point, unsigned k, ef2* o
 }
 
 // ---- a-bar = eq_{z1}^T F (pcs/src/ligesis.rs:372-379) --------------------------------------
-// Two adjacent columns per thread (16-byte loads), four rows in flight with independent sums.
-__global__ void gemv_eq_rows_kernel(const u64* const* __restrict__ fref,
-                                    const ef2* __restrict__ eq, size_t m, size_t n,
-                                    ef2* __restrict__ out) {
+// Two adjacent columns per thread (16-byte loads), eight rows in flight.  The BF x EF products
+// are accumulated unreduced (160-bit sums of 128-bit products) and reduced once per output.
+__global__ void __launch_bounds__(256)
+    gemv_eq_rows_kernel(const u64* const* __restrict__ fref, const ef2* __restrict__ eq,
+                        size_t m, size_t n, ef2* __restrict__ out) {
   const size_t j = 2 * ((size_t)blockIdx.x * blockDim.x + threadIdx.x);
   if (j >= n) return;
   const u64* __restrict__ f = *fref;
-  ef2 a0[4], a1[4];
-#pragma unroll
-  for (int q = 0; q < 4; ++q) a0[q] = a1[q] = ef_zero();
+  Acc160 s00, s01, s10, s11;  // column j / j + 1, coordinate c0 / c1
+  gl_acc_zero(s00), gl_acc_zero(s01), gl_acc_zero(s10), gl_acc_zero(s11);
   size_t i = 0;
-  for (; i + 4 <= m; i += 4) {
-    ulonglong2 x[4];
+  for (; i + 8 <= m; i += 8) {
+    ulonglong2 x[8];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) x[q] = __ldg((const ulonglong2*)(f + (i + q) * n + j));
+    for (int q = 0; q < 8; ++q) x[q] = __ldg((const ulonglong2*)(f + (i + q) * n + j));
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < 8; ++q) {
       const ef2 e = eq[i + q];
-      a0[q] = ef_add(a0[q], ef_scale(e, x[q].x));
-      a1[q] = ef_add(a1[q], ef_scale(e, x[q].y));
+      const u64 a = gl_canon(x[q].x), b = gl_canon(x[q].y);
+      gl_mac(s00, e.c0, a), gl_mac(s01, e.c1, a), gl_mac(s10, e.c0, b), gl_mac(s11, e.c1, b);
     }
   }
   for (; i < m; ++i) {
     const ulonglong2 x = __ldg((const ulonglong2*)(f + i * n + j));
-    a0[0] = ef_add(a0[0], ef_scale(eq[i], x.x));
-    a1[0] = ef_add(a1[0], ef_scale(eq[i], x.y));
+    const ef2 e = eq[i];
+    const u64 a = gl_canon(x.x), b = gl_canon(x.y);
+    gl_mac(s00, e.c0, a), gl_mac(s01, e.c1, a), gl_mac(s10, e.c0, b), gl_mac(s11, e.c1, b);
   }
-  out[j] = ef_add(ef_add(a0[0], a0[1]), ef_add(a0[2], a0[3]));
-  out[j + 1] = ef_add(ef_add(a1[0], a1[1]), ef_add(a1[2], a1[3]));
+  out[j] = ef_make(gl_acc_reduce(s00), gl_acc_reduce(s01));
+  out[j + 1] = ef_make(gl_acc_reduce(s10), gl_acc_reduce(s11));
 }
 void gemv_eq_rows(const u64* const* fref, const ef2* eq, size_t m, size_t n, ef2* out,
                   cudaStream_t st) {
@@ -460,33 +461,67 @@ void bf_fold_poly_dev(const u64* const* pref, int is_ef, unsigned li, const ef2*
 // The R codeword folds of the batched open (eq_fold_codeword, pcs/src/basefold.rs:201-218):
 // level t+1[i] = (1 - r_t)(x + nx)/2 + r_t (x - nx) g_len^(-i) / 2, x = level t[i],
 // nx = level t[i + len/2].  Level k (length D >> k) is stored at offset D (2 - 2^(1-k)).
-// One CTA, because every level depends on the previous one and the whole chain is ~2D values.
-__global__ void __launch_bounds__(1024)
-    bf_levels_kernel(ef2* __restrict__ levels, size_t D, unsigned R, const ef2* __restrict__ ch,
-                     const u64* __restrict__ tw) {
+// Levels longer than BF_TAIL are folded by one grid-wide launch each; the rest of the chain
+// (at most 2 BF_TAIL values) is finished by one CTA in shared memory.
+constexpr unsigned BF_TAIL = 2048;
+
+__device__ __forceinline__ ef2 bf_fold_pair(ef2 x, ef2 nx, ef2 r, size_t i, size_t len,
+                                            const u64* __restrict__ tw) {
   const u64 inv2 = 0x7FFFFFFF80000001ULL;  // (p + 1) / 2
-  size_t off = 0, len = D;
-  for (unsigned t = 0; t < R; ++t) {
+  const unsigned lg = 63 - __clzll((long long)len);
+  const u64 ginv = i ? __ldg(tw + ((len - i) << (TW_LOG - lg))) : 1;
+  const ef2 pe = ef_scale(ef_add(x, nx), inv2);
+  const ef2 po = ef_scale(ef_scale(ef_sub(x, nx), ginv), inv2);
+  return ef_add(pe, ef_mul(r, ef_sub(po, pe)));
+}
+
+__global__ void __launch_bounds__(256)
+    bf_level_kernel(ef2* __restrict__ levels, size_t off, size_t len, const ef2* __restrict__ ch,
+                    unsigned t, const u64* __restrict__ tw) {
+  const size_t h = len >> 1, i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= h) return;
+  levels[off + len + i] = bf_fold_pair(levels[off + i], levels[off + i + h], ch[t], i, len, tw);
+}
+
+__global__ void __launch_bounds__(1024)
+    bf_levels_tail_kernel(ef2* __restrict__ levels, size_t off, unsigned len, unsigned t0,
+                          unsigned R, const ef2* __restrict__ ch, const u64* __restrict__ tw) {
+  extern __shared__ ef2 sl[];  // the chain from level t0 on: < 2 len values
+  for (unsigned i = threadIdx.x; i < len; i += blockDim.x) sl[i] = levels[off + i];
+  __syncthreads();
+  unsigned cur = 0;
+  for (unsigned t = t0; t < R; ++t) {
     const ef2 r = ch[t];
-    const size_t h = len >> 1;
-    const unsigned lg = 63 - __clzll((long long)len);
-    for (size_t i = threadIdx.x; i < h; i += blockDim.x) {
-      const ef2 x = levels[off + i], nx = levels[off + i + h];
-      const u64 ginv = i ? __ldg(tw + ((len - i) << (TW_LOG - lg))) : 1;
-      const ef2 pe = ef_scale(ef_add(x, nx), inv2);
-      const ef2 po = ef_scale(ef_scale(ef_sub(x, nx), ginv), inv2);
-      levels[off + len + i] = ef_add(pe, ef_mul(r, ef_sub(po, pe)));
+    const unsigned h = len >> 1;
+    for (unsigned i = threadIdx.x; i < h; i += blockDim.x) {
+      const ef2 v = bf_fold_pair(sl[cur + i], sl[cur + i + h], r, i, len, tw);
+      sl[cur + len + i] = v;
+      levels[off + cur + len + i] = v;
     }
     __syncthreads();
-    off += len;
+    cur += len;
     len = h;
   }
 }
+
 void bf_levels_dev(ef2* levels, size_t D, unsigned R, const ef2* ch, const u64* tw,
                    cudaStream_t st) {
   if (R < 1 || R > 30) throw ShapeError("basefold: unsupported round count");
-  bf_levels_kernel<<<1, 1024, 0, st>>>(levels, D, R, ch, tw);
-  LGS_LAUNCH_CHECK();
+  size_t off = 0, len = D;
+  unsigned t = 0;
+  for (; t < R && len > BF_TAIL; ++t) {
+    bf_level_kernel<<<cdiv(len / 2, 256), 256, 0, st>>>(levels, off, len, ch, t, tw);
+    LGS_LAUNCH_CHECK();
+    off += len;
+    len >>= 1;
+  }
+  if (t < R) {
+    const size_t smem = 2 * len * sizeof(ef2);
+    LGS_CUDA(cudaFuncSetAttribute(bf_levels_tail_kernel,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    bf_levels_tail_kernel<<<1, 1024, smem, st>>>(levels, off, (unsigned)len, t, R, ch, tw);
+    LGS_LAUNCH_CHECK();
+  }
 }
 
 }  // namespace lgs

@@ -125,6 +125,47 @@ GL_HD u64 gl_sub(u64 a, u64 b) { return a >= b ? a - b : a + (GL_P - b); }
 GL_HD u64 gl_mul(u64 a, u64 b) { return gl_reduce(a * b, gl_mulhi(a, b)); }
 #endif
 GL_HD u64 gl_neg(u64 a) { return a ? GL_P - a : 0; }
+#ifdef __CUDACC__
+// Unreduced multiply-accumulate: acc (five 32-bit words, < 2^160) += a * b as a 128-bit product.
+// Sums of up to 2^32 products are exact; gl_acc_reduce brings the sum back into the field.
+struct Acc160 {
+  uint32_t w[5];
+};
+__device__ __forceinline__ void gl_acc_zero(Acc160& a) {
+  a.w[0] = a.w[1] = a.w[2] = a.w[3] = a.w[4] = 0;
+}
+__device__ __forceinline__ void gl_mac(Acc160& acc, u64 a, u64 b) {
+#ifdef __CUDA_ARCH__
+  const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32);
+  const uint32_t b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+  asm("{\n\t.reg .u32 r0, r1, r2, r3;\n\t"
+      "mul.lo.u32 r0, %5, %7;\n\t"
+      "mul.hi.u32 r1, %5, %7;\n\t"
+      "mad.lo.cc.u32 r1, %5, %8, r1;\n\t"
+      "madc.hi.u32 r2, %5, %8, 0;\n\t"
+      "mad.lo.cc.u32 r1, %6, %7, r1;\n\t"
+      "madc.hi.cc.u32 r2, %6, %7, r2;\n\t"
+      "madc.hi.u32 r3, %6, %8, 0;\n\t"
+      "mad.lo.cc.u32 r2, %6, %8, r2;\n\t"
+      "addc.u32 r3, r3, 0;\n\t"
+      "add.cc.u32 %0, %0, r0;\n\t"
+      "addc.cc.u32 %1, %1, r1;\n\t"
+      "addc.cc.u32 %2, %2, r2;\n\t"
+      "addc.cc.u32 %3, %3, r3;\n\t"
+      "addc.u32 %4, %4, 0;\n\t}"
+      : "+r"(acc.w[0]), "+r"(acc.w[1]), "+r"(acc.w[2]), "+r"(acc.w[3]), "+r"(acc.w[4])
+      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+#endif
+}
+// (w0 + w1 2^32 + w2 2^64 + w3 2^96 + w4 2^128) mod p, with 2^128 = -2^32 mod p.
+__device__ __forceinline__ u64 gl_acc_reduce(const Acc160& a) {
+#ifdef __CUDA_ARCH__
+  return gl_sub(gl_reduce4(a.w[0], a.w[1], a.w[2], a.w[3]), (u64)a.w[4] << 32);
+#else
+  return 0;
+#endif
+}
+#endif
 GL_HD u64 gl_canon(u64 a) { return a >= GL_P ? a - GL_P : a; }
 GL_HD u64 gl_pow(u64 a, u64 e) {
   u64 r = 1;
