@@ -56,6 +56,16 @@ lgs_status lgs_commit(lgs_ctx* ctx, const lgs_pk* pk, const uint64_t* f, size_t 
 /* Same, with f already in device memory of the context's device. */
 lgs_status lgs_commit_device(lgs_ctx* ctx, const lgs_pk* pk, const uint64_t* f_dev, size_t len,
                              uint8_t root[32], lgs_commit_data** out);
+/* Ligesis::commit without waiting for the device: the work is enqueued on the context's stream
+ * and *out is at once usable by lgs_prove on the same context (stream order), so the prove's
+ * host-side planning overlaps the commit's device work.  f is host memory (f_on_device = 0; read
+ * before the call returns) or device memory of the context's device (f_on_device = 1; must stay
+ * unchanged until the commit is done).  lgs_commit_root waits for the commit and returns the
+ * LigesisCommit root (and reports a failed bounded device wait).  The same computation as
+ * lgs_commit, so the root and every later proof are identical. */
+lgs_status lgs_commit_async(lgs_ctx* ctx, const lgs_pk* pk, const uint64_t* f, size_t len,
+                            int f_on_device, lgs_commit_data** out);
+lgs_status lgs_commit_root(lgs_ctx* ctx, lgs_commit_data* cd, uint8_t root[32]);
 void lgs_commit_data_free(lgs_commit_data* cd);
 /* Copy a commitment intermediate to host memory: which = 0 the RS codeword F' (m x 2n),
  * 1 the digest H (32 x 2n).  count must equal the element count. */

@@ -56,6 +56,8 @@ _SIGS = {
     "lgs_commit": (C.c_int, [vp, vp, u64p, C.c_size_t, u8p, C.POINTER(vp)]),
     "lgs_commit_device": (C.c_int, [vp, vp, vp, C.c_size_t, u8p, C.POINTER(vp)]),
     "lgs_commit_data_free": (None, [vp]),
+    "lgs_commit_async": (C.c_int, [vp, vp, vp, C.c_size_t, C.c_int, C.POINTER(vp)]),
+    "lgs_commit_root": (C.c_int, [vp, vp, u8p]),
     "lgs_commit_read": (C.c_int, [vp, vp, C.c_int, u64p, C.c_size_t]),
     "lgs_oracle_need": (C.c_int, [C.c_uint, C.c_uint, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     "lgs_prove": (C.c_int, [vp, vp, vp, u64p, C.c_size_t, u64p, C.c_size_t, u64p, C.c_size_t,

@@ -141,6 +141,8 @@ void lgs_ctx_destroy(lgs_ctx* ctx) {
   }
   for (int i = 0; i < lgs_ctx::RING; ++i)
     if (ctx->ring_ev[i]) cudaEventDestroy(ctx->ring_ev[i]);
+  for (int i = 0; i < lgs_ctx::ROW_BLOCKS; ++i)
+    if (ctx->ev_rows[i]) cudaEventDestroy(ctx->ev_rows[i]);
   for (auto& g : ctx->graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   ctx->graphs.clear();
@@ -214,7 +216,36 @@ lgs_status lgs_commit_device(lgs_ctx* ctx, const lgs_pk* pk, const uint64_t* f_d
                              uint8_t root[32], lgs_commit_data** out) {
   return commit_impl(ctx, pk, f_dev, len, root, out, true);
 }
-void lgs_commit_data_free(lgs_commit_data* cd) { delete cd; }
+lgs_status lgs_commit_async(lgs_ctx* ctx, const lgs_pk* pk, const uint64_t* f, size_t len,
+                            int f_on_device, lgs_commit_data** out) {
+  return guarded([&] {
+    need(ctx && pk && f && out, "lgs_commit_async: null argument");
+    need(len == pk->shape.m() * pk->shape.n(),
+         "lgs_commit_async: f must hold 2^(log_m+log_n) values");
+    CtxDevice dg(ctx);
+    auto* cd = new lgs_commit_data;
+    try {
+      commit_dev(ctx, pk, f, f_on_device != 0, cd, false);
+    } catch (...) {
+      cudaStreamSynchronize(ctx->st);
+      delete cd;
+      throw;
+    }
+    *out = cd;
+  });
+}
+lgs_status lgs_commit_root(lgs_ctx* ctx, lgs_commit_data* cd, uint8_t root[32]) {
+  return guarded([&] {
+    need(ctx && cd && root, "lgs_commit_root: null argument");
+    CtxDevice dg(ctx);
+    commit_root(ctx, cd);
+    std::memcpy(root, cd->root.b, 32);
+  });
+}
+void lgs_commit_data_free(lgs_commit_data* cd) {
+  if (cd && cd->done && !cd->root_ready) cudaEventSynchronize(cd->done);
+  delete cd;
+}
 
 lgs_status lgs_commit_read(lgs_ctx* ctx, const lgs_commit_data* cd, int which, uint64_t* out,
                            size_t count) {

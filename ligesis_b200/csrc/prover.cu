@@ -188,6 +188,8 @@ void ctx_init(lgs_ctx* c, int device) {
     LGS_CUDA(cudaEventCreateWithFlags(&c->ev_done[i], cudaEventDisableTiming));
   }
   LGS_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+  for (int i = 0; i < lgs_ctx::ROW_BLOCKS; ++i)
+    LGS_CUDA(cudaEventCreateWithFlags(&c->ev_rows[i], cudaEventDisableTiming));
   for (int i = 0; i < lgs_ctx::RING; ++i)
     LGS_CUDA(cudaEventCreateWithFlags(&c->ring_ev[i], cudaEventDisableTiming));
   c->tail.reserve(64);
@@ -255,18 +257,44 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
     cd->nodes.alloc((2 * two_n - 1) * 32, c->st);
     cd->nodes.detach(release_stream(c->device));
   }
-  {
-    StageTimer t(c->prof, c->st, "commit_upload");
-    if (f_on_device)
-      d2d(cd->f.p, f, m * n * 8, c->st);
-    else
-      h2d_staged(c, cd->f.p, f, m * n * 8, c->st);
-  }
   const unsigned logN = ilog2(two_n);
   u64* scr = logN > 12 ? c->arena.get<u64>(m * two_n) : nullptr;
-  {
+  const bool rows_path = rs_dft_supported(logN, n);
+  if (!f_on_device && rows_path && m >= 2) {
+    // Host rows: the upload of row block b + 1 overlaps the RS encoding of block b.  Page-locked
+    // f is copied by the DMA engine on a side stream; pageable f goes through the pinned ring on
+    // the context stream, where the host-side staging of the next block is the slower part.
+    StageTimer t(c->prof, c->st, "upload_and_rs_encode");
+    const unsigned nb = (unsigned)std::min<size_t>(lgs_ctx::ROW_BLOCKS, m);
+    const size_t rows = m / nb;  // m and nb are powers of two
+    const bool pinned = host_is_pinned(f);
+    cudaStream_t cp = c->side[0];
+    if (pinned) {
+      LGS_CUDA(cudaEventRecord(c->ev_fork, c->st));  // cd->f exists on the context stream
+      LGS_CUDA(cudaStreamWaitEvent(cp, c->ev_fork, 0));
+    }
+    for (unsigned b = 0; b < nb; ++b) {
+      const size_t off = (size_t)b * rows * n;
+      if (pinned) {
+        h2d(cd->f.as<u64>() + off, f + off, rows * n * 8, cp);
+        LGS_CUDA(cudaEventRecord(c->ev_rows[b], cp));
+        LGS_CUDA(cudaStreamWaitEvent(c->st, c->ev_rows[b], 0));
+      } else {
+        h2d_staged(c, cd->f.as<u64>() + off, f + off, rows * n * 8, c->st);
+      }
+      rs_dft_rows(cd->f.as<u64>() + off, n, n, cd->cw.as<u64>() + (size_t)b * rows * two_n,
+                  two_n, logN, rows, scr + (size_t)b * rows * two_n, c->rs_tw.as<u64>(), c->st);
+    }
+  } else {
+    {
+      StageTimer t(c->prof, c->st, "commit_upload");
+      if (f_on_device)
+        d2d(cd->f.p, f, m * n * 8, c->st);
+      else
+        h2d_staged(c, cd->f.p, f, m * n * 8, c->st);
+    }
     StageTimer t(c->prof, c->st, "rs_encode");
-    if (rs_dft_supported(logN, n))
+    if (rows_path)
       rs_dft_rows(cd->f.as<u64>(), n, n, cd->cw.as<u64>(), two_n, logN, m, scr,
                   c->rs_tw.as<u64>(), c->st);
     else
@@ -287,7 +315,32 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
                            c->st));
   LGS_CUDA(cudaMemcpyAsync(c->tail.as<uint8_t>() + 32, cd->nodes.as<u32>() + (2 * two_n - 2) * 8,
                            32, cudaMemcpyDeviceToHost, c->st));
-  if (finish) commit_finish(c, cd);
+  if (finish) {
+    commit_finish(c, cd);
+  } else {
+    if (!cd->done) LGS_CUDA(cudaEventCreateWithFlags(&cd->done, cudaEventDisableTiming));
+    LGS_CUDA(cudaEventRecord(cd->done, c->st));
+    cd->root_ready = false;
+  }
+}
+
+// The root of an asynchronous commit: waits for its work, then reads the root node and the
+// context's error word directly (the context's pinned tail may already belong to a later call).
+void commit_root(lgs_ctx* c, lgs_commit_data* cd) {
+  if (cd->root_ready) return;
+  if (!cd->done) throw std::logic_error("commit_root: no commit was enqueued");
+  LGS_CUDA(cudaEventSynchronize(cd->done));
+  const size_t two_n = 2 * cd->shape.n();
+  int err = 0;
+  LGS_CUDA(cudaMemcpy(&err, c->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  LGS_CUDA(cudaMemcpy(cd->root.b, cd->nodes.as<u32>() + (2 * two_n - 2) * 8, 32,
+                      cudaMemcpyDeviceToHost));
+  if (err) {
+    LGS_CUDA(cudaMemset(c->err.p, 0, sizeof(int)));
+    throw DeviceTimeout("subset-sum hash: a bounded device wait gave up (code " +
+                        std::to_string(err) + ")");
+  }
+  cd->root_ready = true;
 }
 
 // Completes commit_dev(finish = false) once the work it enqueued is done: the root, and the error
@@ -298,6 +351,7 @@ void commit_finish(lgs_ctx* c, lgs_commit_data* cd) {
   int err = 0;
   std::memcpy(&err, c->tail.as<uint8_t>(), sizeof(int));
   std::memcpy(cd->root.b, c->tail.as<uint8_t>() + 32, 32);
+  cd->root_ready = true;
   if (err) {
     LGS_CUDA(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->st));
     LGS_CUDA(cudaStreamSynchronize(c->st));

@@ -220,6 +220,8 @@ struct lgs_ctx {
   cudaStream_t side[NSIDE] = {};
   cudaEvent_t ev_done[NSIDE] = {};
   cudaEvent_t ev_fork = nullptr;
+  static constexpr int ROW_BLOCKS = 8;  // row blocks of a host upload pipelined with RS encoding
+  cudaEvent_t ev_rows[ROW_BLOCKS] = {};
   lgs::DevMem tw;
   lgs::DevMem rs_tw;  // twiddles of the row RS encoding (rs_dft.cu)
   lgs::Arena arena;
@@ -251,11 +253,16 @@ struct lgs_pk {
 
 struct lgs_commit_data {
   lgs::Shape shape;
+  cudaEvent_t done = nullptr;  // recorded after the commit's last copy (asynchronous commits)
+  bool root_ready = false;
   lgs::DevMem f;      // m x n
   lgs::DevMem cw;     // m x 2n RS codeword F' (its bits are B)
   lgs::DevMem H;      // 32 x 2n digest
   lgs::DevMem nodes;  // column Merkle tree over H
   lgs::Hash32 root;
+  ~lgs_commit_data() {
+    if (done) cudaEventDestroy(done);
+  }
 };
 
 namespace lgs {
@@ -266,6 +273,7 @@ void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lg
 void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device, lgs_commit_data* cd,
                 bool finish = true);
 void commit_finish(lgs_ctx* c, lgs_commit_data* cd);
+void commit_root(lgs_ctx* c, lgs_commit_data* cd);
 void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u64* z_host,
                size_t zlen, const u64* fields_host, size_t nfields, const uint64_t* ints_host,
                size_t nints, uint64_t cursors[2], std::vector<uint8_t>* proof_out);

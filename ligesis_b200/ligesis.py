@@ -198,9 +198,32 @@ class ProvingKey:
             pass
 
 
-@dataclass(frozen=True)
 class LigesisCommit:
-    root: bytes
+    """The commitment (pcs/src/ligesis.rs:85-86): the 32-byte Merkle root of H's columns.  A
+    commitment returned by `Ligesis.commit` is resolved on first use of `root`, which waits for
+    the commit's device work; until then the device runs the commit while the host goes on."""
+
+    def __init__(self, root: bytes | None = None, *, data: "CommitData | None" = None):
+        if root is None and data is None:
+            raise ValueError("a commitment needs its root or its pending commit data")
+        self._root, self._data = root, data
+
+    @property
+    def root(self) -> bytes:
+        if self._root is None:
+            r = np.zeros(32, dtype=np.uint8)
+            check(load().lgs_commit_root(self._data.pk.ctx.handle, self._data.handle, ptr8(r)))
+            self._root, self._data = r.tobytes(), None
+        return self._root
+
+    def __eq__(self, other):
+        return isinstance(other, LigesisCommit) and self.root == other.root
+
+    def __hash__(self):
+        return hash(self.root)
+
+    def __repr__(self):
+        return f"LigesisCommit({self.root.hex()})"
 
 
 class CommitData:
@@ -296,23 +319,26 @@ class Ligesis:
 
     @staticmethod
     def commit(pk: ProvingKey, f: MlPoly) -> tuple[LigesisCommit, CommitData]:
+        """Enqueues the commit (lgs_commit_async) and returns at once: the root is read when
+        first used, and a prove on the same context runs after the commit on the device."""
         if f.is_ext:
             raise ValueError("LigeSIS commits base-field polynomials")
         ev = f.evals
-        root = np.zeros(32, dtype=np.uint8)
         h = vp()
-        check(load().lgs_commit(pk.ctx.handle, pk.handle, ptr64(ev), ev.size, ptr8(root),
-                                C.byref(h)))
-        return LigesisCommit(root.tobytes()), CommitData(h, pk)
+        check(load().lgs_commit_async(pk.ctx.handle, pk.handle, ptr64(ev), ev.size, 0,
+                                      C.byref(h)))
+        data = CommitData(h, pk)
+        return LigesisCommit(data=data), data
 
     @staticmethod
     def commit_device(pk: ProvingKey, f_dev_ptr: int, length: int):
-        """commit with f already in device memory (e.g. a torch uint64/int64 CUDA tensor)."""
-        root = np.zeros(32, dtype=np.uint8)
+        """commit with f already in device memory (e.g. a torch uint64/int64 CUDA tensor); f must
+        stay unchanged until the commitment's root has been read or a prove has returned."""
         h = vp()
-        check(load().lgs_commit_device(pk.ctx.handle, pk.handle, vp(f_dev_ptr), length,
-                                       ptr8(root), C.byref(h)))
-        return LigesisCommit(root.tobytes()), CommitData(h, pk)
+        check(load().lgs_commit_async(pk.ctx.handle, pk.handle, vp(f_dev_ptr), length, 1,
+                                      C.byref(h)))
+        data = CommitData(h, pk)
+        return LigesisCommit(data=data), data
 
     @staticmethod
     def prove(pk: ProvingKey, data: CommitData, z, oracle: RandomOracle) -> LigesisProof:

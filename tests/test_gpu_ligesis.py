@@ -154,6 +154,28 @@ def test_captured_and_replayed_proofs_match_oracle(lgs, orc):
         assert c2.root == cm2.root and got.data == want
 
 
+def test_async_commits_overlap_and_match_oracle(lgs, orc):
+    # two commits enqueued back to back on one context, a prove of the first while the second is
+    # still in flight, roots read afterwards in reverse order: all equal the oracle's
+    log_m, log_n = 3, 10
+    f1, A, z, fields, ints = ligesis_inputs(log_m, log_n, seed=71)
+    f2 = rng.field_elements(72, f1.size)
+    pk, vk = L.Ligesis.setup_with_hash(log_m, log_n, L.SubsetSumHash(64 << log_m, a=A))
+    c1, d1 = L.Ligesis.commit(pk, L.MlPoly(f1))
+    c2, d2 = L.Ligesis.commit(pk, L.MlPoly(f2))
+    oracle = L.RandomOracle(0, length=8)
+    oracle.fields, oracle.ints = np.ascontiguousarray(fields), np.ascontiguousarray(ints)
+    proof = L.Ligesis.prove(pk, d1, z, oracle)
+    key = orc.Key(log_m, log_n, A)
+    cm1, cm2 = orc.Commitment(key, f1), orc.Commitment(key, f2)
+    assert c2.root == cm2.root
+    assert c1.root == cm1.root
+    want, _ = orc.prove(key, cm1, z, fields, ints)
+    assert proof.data == want
+    oracle.restart()
+    assert L.Ligesis.verify(vk, c1, z, proof, oracle)
+
+
 def test_public_api_round_trip(lgs):
     """Ligesis::setup/commit/prove/verify through the reference-shaped API (ligesis.rs:808-822)."""
     g = L.SeededRng(123)
