@@ -20,6 +20,7 @@ than the 126 MB L2, so no step starts from a warm L2.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -248,14 +249,23 @@ def run_ours(args) -> None:
         proof = L.Ligesis.prove(pk, data, z, oracle)
         return commit, proof
 
-    # warm-up; the first proof is checked by the library verifier
+    # warm-up; the first proof is checked by the library verifier.  Like the timed loop, it keeps
+    # only the previous step's commitment alive while the next one is made, and drops it before
+    # the timed region, so the timed steps reuse the buffers the warm-up created.
+    prev = None
     for i in range(args.warmup):
-        commit, proof = step_device()
+        prev = step_device()
         if i == 0:
             oracle.restart()
-            assert L.Ligesis.verify(vk, commit, z, proof, oracle), "warm-up proof rejected"
+            assert L.Ligesis.verify(vk, prev[0], z, prev[1], oracle), "warm-up proof rejected"
+    del prev
 
     def timed(fn, k):
+        # no cyclic-GC pass of the interpreter inside the timed region (a full collection over
+        # torch's object graph takes up to hundreds of ms and lands on whichever step triggers it)
+        gc.collect()
+        gc.freeze()
+        gc.disable()
         if dist:
             dist.barrier()
         torch.cuda.synchronize(local)
@@ -267,6 +277,7 @@ def run_ours(args) -> None:
             out = fn()
         ev1.record(stream)
         torch.cuda.synchronize(local)
+        gc.enable()
         ms = ev0.elapsed_time(ev1) / k
         if dist:
             t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
@@ -291,8 +302,11 @@ def run_ours(args) -> None:
         if cnt.value:
             (host_phases if name.startswith("host_") else stages)[name] = tot.value / cnt.value
     L._lib.check(lib.lgs_profile(ctx.handle, 0))
+    root_dev, proof_dev = commit.root, proof.data
+    del commit, proof  # the e2e loop reuses these buffers, like the device loop reused the warm-up's
     e2e_ms, (commit2, proof2) = timed(step_e2e, args.steps)
-    assert commit2.root == commit.root and proof2.data == proof.data, "e2e result differs"
+    assert commit2.root == root_dev and proof2.data == proof_dev, "e2e result differs"
+    proof = proof2
 
     if dist:
         dist.barrier()
@@ -421,6 +435,9 @@ def run_batch(args) -> None:
         return [(r.commit.root, r.proof.data) for r in res]
 
     plain()  # warm-up: arenas and pools of every shape
+    gc.collect()
+    gc.freeze()
+    gc.disable()
     t0 = time.perf_counter()
     ref = plain()
     t_plain = time.perf_counter() - t0
@@ -430,6 +447,7 @@ def run_batch(args) -> None:
         t0 = time.perf_counter()
         got = batched(eng)
         t_batch = time.perf_counter() - t0
+    gc.enable()
     line = {"mode": "batch", "jobs": len(jobs), "mu": [min(mus), max(mus)], "lanes": args.lanes,
             "plain_proofs_per_s": round(len(jobs) / t_plain, 1),
             "batched_proofs_per_s": round(len(jobs) / t_batch, 1),
@@ -482,6 +500,9 @@ def run_serve(args) -> None:
                     results[i] = eng.wait(tickets[i])
 
             col = th.Thread(target=collect)
+            gc.collect()
+            gc.freeze()
+            gc.disable()
             col.start()
             start = time.perf_counter()
             for i, (t, pk, f, z, o) in enumerate(reqs):
@@ -493,6 +514,7 @@ def run_serve(args) -> None:
                 ready.release()
             col.join()
             wall = time.perf_counter() - start
+            gc.enable()
         lat = np.array([r.latency_ms for r in results])
         return {"proofs_per_s": round(len(reqs) / wall, 1),
                 "p50_ms": round(float(np.percentile(lat, 50)), 2),
@@ -546,6 +568,51 @@ def run_commit(args) -> None:
                       "stages_ms": stages, "roots_identical": len(roots) == 1}), flush=True)
 
 
+def run_timeline(args) -> None:
+    """The prove's replayed graph with timeline event nodes (profile level 2): for each branch
+    boundary, ms from the prove's start, averaged over `--steps` proves of one commitment."""
+    import numpy as np
+    import torch
+
+    import ligesis_b200 as L
+    from ligesis_b200 import rng
+
+    lm, ln = args.log_m, args.log_n
+    lib = L.load()
+    ctx = L.Context(0)
+    f = rng.field_elements(1, 1 << (lm + ln))
+    A = rng.field_elements(2, 32 * (64 << lm)).reshape(32, 64 << lm)
+    z = rng.ext_elements(3, lm + ln)
+    g = rng.SeededRng(4)
+    oracle = L.RandomOracle(0, length=8)
+    oracle.fields, oracle.ints = g.ext_elements(4096), g.ints(4096)
+    pk, _ = L.Ligesis.setup_with_hash(lm, ln, L.SubsetSumHash(64 << lm, a=A), ctx)
+    f_dev = torch.from_numpy(f.view(np.int64)).to("cuda:0")
+    commit, data = L.Ligesis.commit_device(pk, f_dev.data_ptr(), f.size)
+    import ctypes as C
+
+    L._lib.check(lib.lgs_profile(ctx.handle, 2))
+    for _ in range(3):  # eager, capture, first replay
+        oracle.restart()
+        L.Ligesis.prove(pk, data, z, oracle)
+    L._lib.check(lib.lgs_profile(ctx.handle, 2))
+    for _ in range(args.steps):
+        oracle.restart()
+        L.Ligesis.prove(pk, data, z, oracle)
+    marks = ["prefix_end", "abar_end", "A1_abar_commit_end", "A2_rs_abar_table_sc_end", "B_bi_commit_end",
+             "C_binary_sc_end", "D_hash_recon_sc_end", "E_rslink_sc_end", "F_bi_batch_sc_end",
+             "G_a_batch_sc_end", "H_basefold_msgs_end", "main_suffix_start", "main_levels_end",
+             "main_level_trees_end", "join", "end"]
+    out = {}
+    for name in ["prove_device"] + ["tl:" + m for m in marks]:
+        tot, cnt = C.c_double(), C.c_uint64()
+        L._lib.check(lib.lgs_profile_get(ctx.handle, name.encode(), C.byref(tot), C.byref(cnt)))
+        if cnt.value:
+            out[name] = round(tot.value / cnt.value, 4)
+    print(json.dumps({"mode": "timeline", "log_m": lm, "log_n": ln, "proves": args.steps,
+                      "ms_from_prove_start": out, "root": commit.root.hex()[:16]}), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -553,7 +620,8 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", choices=["line", "batch", "serve", "commit"], default="line")
+    ap.add_argument("--mode", choices=["line", "batch", "serve", "commit", "timeline"],
+                    default="line")
     ap.add_argument("--log-m", type=int, default=LOG_M)
     ap.add_argument("--log-n", type=int, default=LOG_N)
     ap.add_argument("--lanes", type=int, default=12)
@@ -570,6 +638,9 @@ def main() -> None:
         return
     if args.mode == "commit":
         run_commit(args)
+        return
+    if args.mode == "timeline":
+        run_timeline(args)
         return
     if args.impl == "reference":
         run_reference(args)

@@ -140,7 +140,10 @@ lgs_status lgs_engine_pending(lgs_engine* e, size_t* queued, size_t* running_byt
 
 /* enable != 0: record CUDA events around each device stage of later calls on this context
  * (and clear the totals); 0: stop.  Stages: commit_upload, rs_encode, subset_sum_hash,
- * merkle_h, prove_device. */
+ * merkle_h, upload_and_rs_encode (host f), prove_device, and the host phases host_plan,
+ * host_enqueue, host_wait, host_assemble.  enable = 2 also records the prove's timeline: event
+ * nodes at its branch boundaries, captured into its graph, reported as "tl:<mark>" = ms from the
+ * prove's start to that point (marks: prefix_end, A1_abar_commit_end, ..., join, end). */
 lgs_status lgs_profile(lgs_ctx* ctx, int enable);
 /* Total device milliseconds and number of timed calls of one stage since lgs_profile(ctx, 1). */
 lgs_status lgs_profile_get(lgs_ctx* ctx, const char* stage, double* total_ms, uint64_t* count);

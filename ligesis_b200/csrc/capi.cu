@@ -143,10 +143,18 @@ void lgs_ctx_destroy(lgs_ctx* ctx) {
     if (ctx->ring_ev[i]) cudaEventDestroy(ctx->ring_ev[i]);
   for (int i = 0; i < lgs_ctx::ROW_BLOCKS; ++i)
     if (ctx->ev_rows[i]) cudaEventDestroy(ctx->ev_rows[i]);
+  for (int i = 0; i < lgs_ctx::TL_MAX; ++i)
+    if (ctx->tl_ev[i]) cudaEventDestroy(ctx->tl_ev[i]);
   for (auto& g : ctx->graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   ctx->graphs.clear();
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_fork2) cudaEventDestroy(ctx->ev_fork2);
+  for (int i = 0; i < lgs_ctx::NSIDE_HI; ++i)
+    if (ctx->side_hi[i]) {
+      cudaStreamSynchronize(ctx->side_hi[i]);
+      cudaStreamDestroy(ctx->side_hi[i]);
+    }
   if (ctx->st) cudaStreamDestroy(ctx->st);
   delete ctx;
 }
@@ -251,7 +259,7 @@ lgs_status lgs_commit_read(lgs_ctx* ctx, const lgs_commit_data* cd, int which, u
                            size_t count) {
   return guarded([&] {
     need(ctx && cd && out, "lgs_commit_read: null argument");
-    const DevMem& src = which == 0 ? cd->cw : cd->H;
+    const RecycledBuf& src = which == 0 ? cd->cw : cd->H;
     need(which == 0 || which == 1, "lgs_commit_read: which must be 0 or 1");
     need(count * 8 == src.bytes, "lgs_commit_read: wrong element count");
     CtxDevice dg(ctx);
@@ -316,6 +324,7 @@ lgs_status lgs_profile(lgs_ctx* ctx, int enable) {
     ctx->prof.flush();
     ctx->prof.totals.clear();
     ctx->prof.on = enable != 0;
+    ctx->prof_level = enable;
   });
 }
 

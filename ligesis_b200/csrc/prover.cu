@@ -173,10 +173,87 @@ cudaStream_t release_stream(int device) {
   return streams[device];
 }
 
+namespace {
+constexpr size_t CACHE_BYTES = (size_t)8 << 30;
+struct Cached {
+  int device;
+  size_t bytes;
+  void* p;
+};
+std::mutex g_cache_mu;
+std::vector<Cached> g_cache;
+std::vector<cudaEvent_t> g_events;
+size_t g_cached_bytes = 0;
+}  // namespace
+
+void RecycledBuf::acquire(size_t b, int dev, cudaStream_t s) {
+  if (p && bytes == b && device == dev) return;
+  release();
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    for (size_t i = 0; i < g_cache.size(); ++i)
+      if (g_cache[i].device == dev && g_cache[i].bytes == b) {
+        p = g_cache[i].p;
+        g_cache.erase(g_cache.begin() + i);
+        g_cached_bytes -= b;
+        bytes = b;
+        device = dev;
+        return;
+      }
+  }
+  if (b) LGS_CUDA(cudaMallocAsync(&p, b, s));
+  bytes = b;
+  device = dev;
+}
+
+void RecycledBuf::release() {
+  if (!p) return;
+  bool keep = false;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    if (g_cached_bytes + bytes <= CACHE_BYTES) {
+      g_cache.push_back({device, bytes, p});
+      g_cached_bytes += bytes;
+      keep = true;
+    }
+  }
+  if (!keep) cudaFreeAsync(p, release_stream(device));
+  p = nullptr;
+  bytes = 0;
+}
+
+cudaEvent_t recycled_event() {
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    if (!g_events.empty()) {
+      cudaEvent_t e = g_events.back();
+      g_events.pop_back();
+      return e;
+    }
+  }
+  cudaEvent_t e = nullptr;
+  LGS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  return e;
+}
+
+void recycle_event(cudaEvent_t e) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  if (g_events.size() < 256)
+    g_events.push_back(e);
+  else
+    cudaEventDestroy(e);
+}
+
 void ctx_init(lgs_ctx* c, int device) {
   c->device = device;
   LGS_CUDA(cudaSetDevice(device));
-  LGS_CUDA(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+  int prio_lo = 0, prio_hi = 0;
+  LGS_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+  // the main stream and the prove's critical branches outrank the other branches
+  LGS_CUDA(cudaStreamCreateWithPriority(&c->st, cudaStreamNonBlocking, prio_hi));
+  for (int i = 0; i < lgs_ctx::NSIDE_HI; ++i)
+    LGS_CUDA(cudaStreamCreateWithPriority(&c->side_hi[i], cudaStreamNonBlocking, prio_hi));
+  LGS_CUDA(cudaEventCreateWithFlags(&c->ev_fork2, cudaEventDisableTiming));
   // Keep freed pool memory cached so per-proof buffers are recycled without driver calls.
   cudaMemPool_t pool;
   LGS_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
@@ -239,27 +316,17 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
   const Shape& s = pk->shape;
   const size_t m = s.m(), n = s.n(), two_n = 2 * n;
   if (two_n % 128) throw ShapeError("commit: 2n must be a multiple of 128");
+  HostClock hc(c->prof);
   cd->shape = s;
   c->arena.begin();
-  if (cd->f.bytes != m * n * 8) {
-    cd->f.alloc(m * n * 8, c->st);
-    cd->f.detach(release_stream(c->device));
-  }
-  if (cd->cw.bytes != m * two_n * 8) {
-    cd->cw.alloc(m * two_n * 8, c->st);
-    cd->cw.detach(release_stream(c->device));
-  }
-  if (cd->H.bytes != DIGEST_ROWS * two_n * 8) {
-    cd->H.alloc(DIGEST_ROWS * two_n * 8, c->st);
-    cd->H.detach(release_stream(c->device));
-  }
-  if (cd->nodes.bytes != (2 * two_n - 1) * 32) {
-    cd->nodes.alloc((2 * two_n - 1) * 32, c->st);
-    cd->nodes.detach(release_stream(c->device));
-  }
+  cd->f.acquire(m * n * 8, c->device, c->st);
+  cd->cw.acquire(m * two_n * 8, c->device, c->st);
+  cd->H.acquire(DIGEST_ROWS * two_n * 8, c->device, c->st);
+  cd->nodes.acquire((2 * two_n - 1) * 32, c->device, c->st);
   const unsigned logN = ilog2(two_n);
   u64* scr = logN > 12 ? c->arena.get<u64>(m * two_n) : nullptr;
   const bool rows_path = rs_dft_supported(logN, n);
+  hc.lap("host_commit_alloc");
   if (!f_on_device && rows_path && m >= 2) {
     // Host rows: the upload of row block b + 1 overlaps the RS encoding of block b.  Page-locked
     // f is copied by the DMA engine on a side stream; pageable f goes through the pinned ring on
@@ -301,6 +368,7 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
       ntt_batch(cd->f.as<u64>(), n, n, cd->cw.as<u64>(), two_n, logN, m, scr, c->tw.as<u64>(),
                 c->st);
   }
+  hc.lap("host_commit_rs");
   {
     StageTimer t(c->prof, c->st, "subset_sum_hash");  // H and its Merkle leaf hashes
     subset_sum_hash_tc(pk->tmap, cd->cw.as<u64>(), cd->H.as<u64>(), cd->nodes.as<u32>(),
@@ -315,13 +383,15 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
                            c->st));
   LGS_CUDA(cudaMemcpyAsync(c->tail.as<uint8_t>() + 32, cd->nodes.as<u32>() + (2 * two_n - 2) * 8,
                            32, cudaMemcpyDeviceToHost, c->st));
+  hc.lap("host_commit_hash_merkle");
   if (finish) {
     commit_finish(c, cd);
   } else {
-    if (!cd->done) LGS_CUDA(cudaEventCreateWithFlags(&cd->done, cudaEventDisableTiming));
+    if (!cd->done) cd->done = recycled_event();
     LGS_CUDA(cudaEventRecord(cd->done, c->st));
     cd->root_ready = false;
   }
+  hc.lap("host_commit_tail");
 }
 
 // The root of an asynchronous commit: waits for its work, then reads the root node and the
@@ -415,8 +485,9 @@ const ProveGraph* prove_graph(lgs_ctx* c, const Shape& s, F&& enqueue) {
     return nullptr;
   }
   const Arena& ar = c->arena;
+  const bool tl = c->prof_level >= 2;
   if (g->exec && g->arena == ar.mem.p && g->arena_bytes == ar.mem.bytes && g->up == c->up.p &&
-      g->down == c->down.p)
+      g->down == c->down.p && g->timeline == tl)
     return g;
   if (g->exec) {
     LGS_CUDA(cudaGraphExecDestroy(g->exec));
@@ -441,10 +512,13 @@ const ProveGraph* prove_graph(lgs_ctx* c, const Shape& s, F&& enqueue) {
   adjust_launches(-(int64_t)captured);  // captured, not launched
   LGS_CUDA(cudaStreamEndCapture(c->st, &graph));
   cudaGraphExec_t exec = nullptr;
-  const cudaError_t err = cudaGraphInstantiate(&exec, graph, 0);
+  // kernel nodes keep the priority of the stream they were captured from
+  const cudaError_t err =
+      cudaGraphInstantiateWithFlags(&exec, graph, cudaGraphInstantiateFlagUseNodePriority);
   cudaGraphDestroy(graph);
   LGS_CUDA(err);
   g->exec = exec;
+  g->timeline = tl;
   g->launches = captured;
   g->arena = ar.mem.p;
   g->arena_bytes = ar.mem.bytes;
@@ -715,60 +789,62 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
 
   // Everything from the upload to the read-back depends on the transcript only through the
   // uploaded blob, so it is captured once per shape into a CUDA graph and replayed.
+  const bool tl = c->prof_level >= 2;
+  unsigned ntl = 0;
+  if (tl)
+    for (int i = 0; i < lgs_ctx::TL_MAX; ++i)
+      if (!c->tl_ev[i]) LGS_CUDA(cudaEventCreate(&c->tl_ev[i]));
+  auto mark = [&](const char* name, cudaStream_t where) {
+    if (!tl || ntl >= (unsigned)lgs_ctx::TL_MAX) return;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    LGS_CUDA(cudaStreamIsCapturing(where, &cs));
+    if (cs == cudaStreamCaptureStatusActive)
+      LGS_CUDA(cudaEventRecordWithFlags(c->tl_ev[ntl], where, cudaEventRecordExternal));
+    else
+      LGS_CUDA(cudaEventRecord(c->tl_ev[ntl], where));
+    if (c->tl_names.size() <= ntl) c->tl_names.resize(ntl + 1);
+    c->tl_names[ntl++] = name;
+  };
   auto enqueue = [&]() {
+  ntl = 0;
+  mark("start", st);
   h2d(d_up, h_up, blob, st);
 
-  // -- a-bar, y, commit a-bar, RS(a-bar) (pcs/src/ligesis.rs:365-387)
+  // -- the transcript is a DAG of independent branches (every challenge is pre-drawn): fork them
+  // onto side streams as soon as their inputs exist, join before the gather.  The branches that
+  // need only B_I fork before the a-bar GEMV; the two Basefold commitments (A1, B) gate the
+  // Stage B codeword chain on the main stream and run on high-priority streams.
   new_eq_dev(d_prm + P_z1, s.log_m, eqz1, st);
-  gemv_eq_rows(d_ptrs + PT_F, eqz1, m, n, a_vec, st);
-
-  // -- the rest is a DAG of independent branches (every challenge is pre-drawn): fork them
-  // onto side streams after the shared inputs exist, join before the gather.
   bits_gather(d_ptrs + PT_CW, two_n, d_idx, S, W, bi, st);
   new_eq_dev(d_fields + fp.alpha2, 5, eq_a2, st);
   new_eq_dev(d_fields + fp.r2, log_s, eq_r2, st);
+  mark("prefix_end", st);
   LGS_CUDA(cudaEventRecord(c->ev_fork, st));
-  unsigned nbr = 0;
-  auto branch = [&]() {
-    if (nbr >= (unsigned)lgs_ctx::NSIDE) throw std::runtime_error("prove: too many branches");
-    cudaStream_t b = c->side[nbr++];
-    LGS_CUDA(cudaStreamWaitEvent(b, c->ev_fork, 0));
+  std::vector<cudaStream_t> brs;
+  unsigned n_hi = 0;
+  cudaEvent_t fork_ev = c->ev_fork;
+  auto branch = [&](bool hi = false) {
+    if (brs.size() >= (size_t)lgs_ctx::NSIDE) throw std::runtime_error("prove: too many branches");
+    cudaStream_t b;
+    if (hi) {
+      if (n_hi >= (unsigned)lgs_ctx::NSIDE_HI) throw std::runtime_error("prove: too many branches");
+      b = c->side_hi[n_hi++];
+    } else {
+      b = c->side[brs.size() - n_hi];
+    }
+    brs.push_back(b);
+    LGS_CUDA(cudaStreamWaitEvent(b, fork_ev, 0));
     return b;
   };
   auto partials_for = [&](unsigned k, unsigned d) {
     return ar.get<ef2>(std::max(sumcheck_partials_elems(k, d), eqdot_partials_elems(k) + 1024));
   };
-  // A1: y = a(z2) and the Basefold commitment to a-bar (pcs/src/ligesis.rs:379-384)
-  const unsigned br_a1 = nbr;
-  {
-    cudaStream_t b = branch();
-    eq_dot_dev(a_vec, 0, d_prm + P_z2, log_n, (ef2*)(stage + S_y), partials_for(log_n, 1), b);
-    bf_commit(c, (const u64*)a_vec, 1, n, li_a, &a_st, b);
-  }
-  // A2: RS(a-bar), y4, the recon table sumcheck and y5 (pcs/src/ligesis.rs:387, 458, 487-497)
-  {
-    cudaStream_t b = branch();
-    u64* t1 = ar.get<u64>(2 * n);
-    u64* t2 = ar.get<u64>(2 * two_n);
-    u64* scr = ilog2(two_n) > 12 ? ar.get<u64>(2 * two_n) : nullptr;
-    transpose_u64((const u64*)a_vec, t1, n, 2, 1, b);
-    ntt_batch(t1, n, n, t2, two_n, ilog2(two_n), 2, scr, c->tw.as<u64>(), b);
-    transpose_u64(t2, (u64*)ra, 2, two_n, 1, b);
-    y4_dev(eq_r2, ra, d_idx, S, (ef2*)(stage + S_y4), b);
-    ef2* sel = ar.get<ef2>(two_n);
-    ef2* rac = ar.get<ef2>(two_n);
-    sel_build(d_idx, eq_r2, S, two_n, sel, b);
-    d2d(rac, ra, two_n * sizeof(ef2), b);
-    ef2* pt[2] = {sel, rac};
-    sumcheck_prove_dev(pt, 2, log_n + 1, d_fields + fp.ch_table, (ef2*)(stage + S_sc_r[3]),
-                       (ef2*)(stage + S_sc_f[3]), partials_for(log_n + 1, 2), b);
-    eq_dot_dev(ra, 0, d_prm + P_r3, log_n + 1, (ef2*)(stage + S_y5), partials_for(log_n + 1, 1), b);
-  }
+  const unsigned br_b = (unsigned)brs.size();
   // B: the Basefold commitment to B_I (pcs/src/ligesis.rs:411-416)
-  const unsigned br_b = nbr;
   {
-    cudaStream_t b = branch();
+    cudaStream_t b = branch(true);
     bf_commit(c, bi, 0, WS, li_bi, &bi_st, b);
+    mark("B_bi_commit_end", b);
   }
   // C: binary check, factors [B_I, B_I - 1, eq_alpha1] (pcs/src/ligesis.rs:419-429)
   {
@@ -779,6 +855,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     new_eq_dev(d_fields + fp.alpha1, nb, p2, b);
     sumcheck_binary_dev(p0, p2, nb, d_fields + fp.ch_bin, (ef2*)(stage + S_sc_r[0]),
                         (ef2*)(stage + S_sc_f[0]), partials_for(nb, 3), b);
+    mark("C_binary_sc_end", b);
   }
   // D: hash and recon bilinear sumchecks (pcs/src/ligesis.rs:435-485)
   {
@@ -798,6 +875,52 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     ef2* pr[2] = {v, g2b};
     sumcheck_prove_dev(pr, 2, log_w, d_fields + fp.ch_recon, (ef2*)(stage + S_sc_r[2]),
                        (ef2*)(stage + S_sc_f[2]), part, b);
+    mark("D_hash_recon_sc_end", b);
+  }
+  // F: Stage A point reduction of B_I (pcs/src/ligesis.rs:510-516)
+  {
+    cudaStream_t b = branch();
+    ef2* gbi = ar.get<ef2>(WS);
+    ef2* bie = ar.get<ef2>(WS);
+    combine_eq_dev(d_prm + P_bipts, 3, nb, d_fields + fp.gamma_bi, gbi, b);
+    lift_bf(bi, bie, WS, 0, b);
+    ef2* pb[2] = {bie, gbi};
+    sumcheck_prove_dev(pb, 2, nb, d_fields + fp.ch_bi, (ef2*)(stage + S_sc_r[5]),
+                       (ef2*)(stage + S_sc_f[5]), partials_for(nb, 2), b);
+    mark("F_bi_batch_sc_end", b);
+  }
+  // -- a-bar = eq_{z1}^T F and everything that needs it (pcs/src/ligesis.rs:365-387)
+  gemv_eq_rows(d_ptrs + PT_F, eqz1, m, n, a_vec, st);
+  mark("abar_end", st);
+  LGS_CUDA(cudaEventRecord(c->ev_fork2, st));
+  fork_ev = c->ev_fork2;
+  const unsigned br_a1 = (unsigned)brs.size();
+  // A1: y = a(z2) and the Basefold commitment to a-bar (pcs/src/ligesis.rs:379-384)
+  {
+    cudaStream_t b = branch(true);
+    eq_dot_dev(a_vec, 0, d_prm + P_z2, log_n, (ef2*)(stage + S_y), partials_for(log_n, 1), b);
+    bf_commit(c, (const u64*)a_vec, 1, n, li_a, &a_st, b);
+    mark("A1_abar_commit_end", b);
+  }
+  // A2: RS(a-bar), y4, the recon table sumcheck and y5 (pcs/src/ligesis.rs:387, 458, 487-497)
+  {
+    cudaStream_t b = branch();
+    u64* t1 = ar.get<u64>(2 * n);
+    u64* t2 = ar.get<u64>(2 * two_n);
+    u64* scr = ilog2(two_n) > 12 ? ar.get<u64>(2 * two_n) : nullptr;
+    transpose_u64((const u64*)a_vec, t1, n, 2, 1, b);
+    ntt_batch(t1, n, n, t2, two_n, ilog2(two_n), 2, scr, c->tw.as<u64>(), b);
+    transpose_u64(t2, (u64*)ra, 2, two_n, 1, b);
+    y4_dev(eq_r2, ra, d_idx, S, (ef2*)(stage + S_y4), b);
+    ef2* sel = ar.get<ef2>(two_n);
+    ef2* rac = ar.get<ef2>(two_n);
+    sel_build(d_idx, eq_r2, S, two_n, sel, b);
+    d2d(rac, ra, two_n * sizeof(ef2), b);
+    ef2* pt[2] = {sel, rac};
+    sumcheck_prove_dev(pt, 2, log_n + 1, d_fields + fp.ch_table, (ef2*)(stage + S_sc_r[3]),
+                       (ef2*)(stage + S_sc_f[3]), partials_for(log_n + 1, 2), b);
+    eq_dot_dev(ra, 0, d_prm + P_r3, log_n + 1, (ef2*)(stage + S_y5), partials_for(log_n + 1, 1), b);
+    mark("A2_rs_abar_table_sc_end", b);
   }
   // E: RS-link sumcheck (pcs/src/ligesis.rs:499-502); r3 is pre-drawn, so w needs no wait
   {
@@ -809,18 +932,9 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     ef2* pw[2] = {ac, w};
     sumcheck_prove_dev(pw, 2, log_n, d_fields + fp.ch_rs, (ef2*)(stage + S_sc_r[4]),
                        (ef2*)(stage + S_sc_f[4]), partials_for(log_n, 2), b);
+    mark("E_rslink_sc_end", b);
   }
-  // F, G: Stage A point reductions (pcs/src/ligesis.rs:510-522)
-  {
-    cudaStream_t b = branch();
-    ef2* gbi = ar.get<ef2>(WS);
-    ef2* bie = ar.get<ef2>(WS);
-    combine_eq_dev(d_prm + P_bipts, 3, nb, d_fields + fp.gamma_bi, gbi, b);
-    lift_bf(bi, bie, WS, 0, b);
-    ef2* pb[2] = {bie, gbi};
-    sumcheck_prove_dev(pb, 2, nb, d_fields + fp.ch_bi, (ef2*)(stage + S_sc_r[5]),
-                       (ef2*)(stage + S_sc_f[5]), partials_for(nb, 2), b);
-  }
+  // G: Stage A point reduction of a-bar (pcs/src/ligesis.rs:518-522)
   {
     cudaStream_t b = branch();
     ef2* ga = ar.get<ef2>(n);
@@ -830,6 +944,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     ef2* pa[2] = {ac, ga};
     sumcheck_prove_dev(pa, 2, log_n, d_fields + fp.ch_a, (ef2*)(stage + S_sc_r[6]),
                        (ef2*)(stage + S_sc_f[6]), partials_for(log_n, 2), b);
+    mark("G_a_batch_sc_end", b);
   }
   // H: Stage B reduction messages (pcs/src/basefold.rs:746-769).  With m = poly.fold(point[0..li])
   // (2^R values) and the batch challenges r_0.., round t's l0 = MLE(m)(r_0, .., r_{t-1}, 0,
@@ -841,15 +956,18 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
       bf_fold_poly_dev(d_ptrs + poly_slot[ch], chan_ef[ch], chan_li[ch], pts[ch], mlen, mch[ch], b);
     ef2* part = ar.get<ef2>(eq_dot_multi_partials(R, 3 * R));
     eq_dot_multi_dev((const EqDotTask*)(d_up + U_tasks), 3 * R, R, part, b);
+    mark("H_basefold_msgs_end", b);
   }
   // join: main waits for every branch
-  for (unsigned i = 0; i < nbr; ++i) LGS_CUDA(cudaEventRecord(c->ev_done[i], c->side[i]));
+  for (size_t i = 0; i < brs.size(); ++i) LGS_CUDA(cudaEventRecord(c->ev_done[i], brs[i]));
   LGS_CUDA(cudaStreamWaitEvent(st, c->ev_done[br_a1], 0));
   LGS_CUDA(cudaStreamWaitEvent(st, c->ev_done[br_b], 0));
+  mark("main_suffix_start", st);
   // Stage B codeword chain on main (needs both prove-time commitments): combined level 0,
   // the R folds, and the Merkle trees of levels 1..R-1 (pcs/src/basefold.rs:735-784)
   bf_combine_dev((const BfChannelDev*)(d_up + U_chs), 3, d_fields + fp.coeffs, D, levels, st);
   bf_levels_dev(levels, D, R, d_fields + fp.ch_batch, c->tw.as<u64>(), st);
+  mark("main_levels_end", st);
   if (R > 1) {
     std::vector<const u64*> ldata;
     std::vector<u32*> lnodes;
@@ -865,11 +983,14 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     merkle_leaves_many(ldata.data(), 2, lnodes.data(), lcount.data(), (unsigned)lnodes.size(), st);
     merkle_build_many(lnodes.data(), lcount.data(), (unsigned)lnodes.size(), st);
   }
-  for (unsigned i = 0; i < nbr; ++i) LGS_CUDA(cudaStreamWaitEvent(st, c->ev_done[i], 0));
+  mark("main_level_trees_end", st);
+  for (size_t i = 0; i < brs.size(); ++i) LGS_CUDA(cudaStreamWaitEvent(st, c->ev_done[i], 0));
+  mark("join", st);
 
   // ---- gathers into staging, one read-back -------------------------------------------------
   gather_segments((const GatherSeg*)(d_up + U_segs), (unsigned)plan.segs.size(), st);
   LGS_CUDA(cudaMemcpyAsync(c->down.p, stage, sg.total * 8, cudaMemcpyDeviceToHost, st));
+  mark("end", st);
   };
   const ProveGraph* graph = prove_graph(c, s, enqueue);
   StageTimer t_prove(c->prof, st, "prove_device");
@@ -886,6 +1007,13 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   LGS_CUDA(cudaStreamSynchronize(st));
   hc.lap("host_wait");
   c->prof.flush();
+  if (tl && c->tl_ev[0]) {
+    for (unsigned i = 1; i < c->tl_names.size() && i < (unsigned)lgs_ctx::TL_MAX; ++i) {
+      float ms = 0;
+      if (c->tl_ev[i] && cudaEventElapsedTime(&ms, c->tl_ev[0], c->tl_ev[i]) == cudaSuccess)
+        c->prof.add("tl:" + c->tl_names[i], ms);
+    }
+  }
 
   // ---- encode straight from the staging buffer, in the order of encode_proof --------------
   ByteWriter w;

@@ -85,6 +85,31 @@ struct DevMem {
   }
 };
 
+// Device buffers and events of commitment data, recycled per device: a commitment is created and
+// freed once per proof, and returning its buffers to the stream-ordered pool (and allocating them
+// again) put driver calls that can stall for milliseconds on that path.  A buffer is handed back
+// only when no work uses it any more, so a later commitment may take it on any stream.  At most
+// CACHE_BYTES stay cached per device; beyond that buffers go back to the pool.
+struct RecycledBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  int device = -1;
+  RecycledBuf() = default;
+  RecycledBuf(const RecycledBuf&) = delete;
+  RecycledBuf& operator=(const RecycledBuf&) = delete;
+  // A buffer of exactly `b` bytes on `device` (reused if one is cached), stream-ordered on `s`
+  // when newly allocated.
+  void acquire(size_t b, int dev, cudaStream_t s);
+  void release();
+  ~RecycledBuf() { release(); }
+  template <class T>
+  T* as() const {
+    return (T*)p;
+  }
+};
+cudaEvent_t recycled_event();
+void recycle_event(cudaEvent_t e);
+
 // Bump allocator for per-call device scratch.  A call that outgrows the buffer takes extra
 // pool allocations; the next call starts from one buffer of the largest size seen, so
 // steady-state calls allocate nothing.
@@ -192,6 +217,7 @@ struct ProveGraph {
   const void* down = nullptr;
   cudaGraphExec_t exec = nullptr;
   uint64_t launches = 0;  // kernels per replay
+  bool timeline = false;  // captured with the timeline event nodes of profile level 2
 };
 
 // Host-side phases of one call (planning, enqueueing, waiting, assembling), recorded in the
@@ -218,6 +244,9 @@ struct lgs_ctx {
   int device = 0;
   cudaStream_t st = nullptr;
   cudaStream_t side[NSIDE] = {};
+  static constexpr int NSIDE_HI = 2;  // high-priority side streams for the critical branches
+  cudaStream_t side_hi[NSIDE_HI] = {};
+  cudaEvent_t ev_fork2 = nullptr;
   cudaEvent_t ev_done[NSIDE] = {};
   cudaEvent_t ev_fork = nullptr;
   static constexpr int ROW_BLOCKS = 8;  // row blocks of a host upload pipelined with RS encoding
@@ -226,6 +255,12 @@ struct lgs_ctx {
   lgs::DevMem rs_tw;  // twiddles of the row RS encoding (rs_dft.cu)
   lgs::Arena arena;
   lgs::Profiler prof;
+  // Profile level 2: event-record nodes at the prove's branch boundaries (captured into its
+  // graph), read back as "tl:<mark>" = ms since the prove's start.
+  int prof_level = 0;
+  static constexpr int TL_MAX = 32;
+  cudaEvent_t tl_ev[TL_MAX] = {};
+  std::vector<std::string> tl_names;
   lgs::DevMem err;  // device error word of bounded-wait kernels (0 = ok)
   // Pinned host memory: every transfer of a call is asynchronous, so the host enqueues a whole
   // commit or prove without waiting for the device and synchronises once at the end.
@@ -255,13 +290,13 @@ struct lgs_commit_data {
   lgs::Shape shape;
   cudaEvent_t done = nullptr;  // recorded after the commit's last copy (asynchronous commits)
   bool root_ready = false;
-  lgs::DevMem f;      // m x n
-  lgs::DevMem cw;     // m x 2n RS codeword F' (its bits are B)
-  lgs::DevMem H;      // 32 x 2n digest
-  lgs::DevMem nodes;  // column Merkle tree over H
+  lgs::RecycledBuf f;      // m x n
+  lgs::RecycledBuf cw;     // m x 2n RS codeword F' (its bits are B)
+  lgs::RecycledBuf H;      // 32 x 2n digest
+  lgs::RecycledBuf nodes;  // column Merkle tree over H
   lgs::Hash32 root;
   ~lgs_commit_data() {
-    if (done) cudaEventDestroy(done);
+    if (done) lgs::recycle_event(done);
   }
 };
 

@@ -60,30 +60,56 @@ struct Fac {
   static constexpr unsigned TAIL = S >= 3 ? 512 : 1024;
 };
 
-// Add prod_j (lo_j + q (hi_j - lo_j)) for q = 0..D to s, from the stored factors.
+// Add prod_j (lo_j + q (hi_j - lo_j)) for q = 0..D to s, from the stored factors.  skip1: leave
+// out q = 1 (the round's g(1) is then recovered from the running claim, g(1) = claim - g(0)).
 template <int D, bool BIN>
-__device__ __forceinline__ void accumulate_pair(const ef2* lo, const ef2* hi, ef2 (&s)[D + 1]) {
+__device__ __forceinline__ void accumulate_pair(const ef2* lo, const ef2* hi, ef2 (&s)[D + 1],
+                                                bool skip1) {
   constexpr int S = Fac<D, BIN>::S;
   ef2 v[S], df[S];
 #pragma unroll
   for (int j = 0; j < S; ++j) v[j] = lo[j], df[j] = ef_sub(hi[j], lo[j]);
 #pragma unroll
   for (int q = 0; q <= D; ++q) {
-    ef2 p;
-    if (BIN) {
-      p = ef_mul(v[0], ef_sub(v[0], ef_one()));  // b (b - 1)
+    if (q != 1 || !skip1) {
+      ef2 p;
+      if (BIN) {
+        p = ef_mul(v[0], ef_sub(v[0], ef_one()));  // b (b - 1)
 #pragma unroll
-      for (int j = 1; j < S; ++j) p = ef_mul(p, v[j]);
-    } else {
-      p = v[0];
+        for (int j = 1; j < S; ++j) p = ef_mul(p, v[j]);
+      } else {
+        p = v[0];
 #pragma unroll
-      for (int j = 1; j < S; ++j) p = ef_mul(p, v[j]);
+        for (int j = 1; j < S; ++j) p = ef_mul(p, v[j]);
+      }
+      s[q] = ef_add(s[q], p);
     }
-    s[q] = ef_add(s[q], p);
     if (q < D)
 #pragma unroll
-      for (int j = 0; j < S; ++j) v[j] = ef_add(v[j], df[j]);
+      for (int j = 0; j < S; ++j) v[j] = (q == 0) ? hi[j] : ef_add(v[j], df[j]);
   }
+}
+
+// g(r) for the degree-D round polynomial given by its values g(0..D) (Lagrange on 0..D).
+template <int D>
+__device__ ef2 interp_at(const ef2* g, ef2 r) {
+  const u64 inv2 = 0x7FFFFFFF80000001ULL, inv6 = 0xD555555480000001ULL;
+  const ef2 r1 = ef_sub(r, ef_from(1)), r2 = ef_sub(r, ef_from(2));
+  if (D == 1) return ef_add(g[0], ef_mul(r, ef_sub(g[1], g[0])));
+  if (D == 2) {
+    const ef2 l0 = ef_scale(ef_mul(r1, r2), inv2);
+    const ef2 l1 = ef_sub(ef_zero(), ef_mul(r, r2));
+    const ef2 l2 = ef_scale(ef_mul(r, r1), inv2);
+    return ef_add(ef_add(ef_mul(g[0], l0), ef_mul(g[1], l1)), ef_mul(g[2], l2));
+  }
+  const ef2 r3 = ef_sub(r, ef_from(3));
+  const ef2 r12 = ef_mul(r1, r2), rr1 = ef_mul(r, r1);
+  const ef2 l0 = ef_sub(ef_zero(), ef_scale(ef_mul(r12, r3), inv6));
+  const ef2 l1 = ef_scale(ef_mul(ef_mul(r, r2), r3), inv2);
+  const ef2 l2 = ef_sub(ef_zero(), ef_scale(ef_mul(rr1, r3), inv2));
+  const ef2 l3 = ef_scale(ef_mul(rr1, r2), inv6);
+  return ef_add(ef_add(ef_mul(g[0], l0), ef_mul(g[1], l1)),
+                ef_add(ef_mul(g[2], l2), ef_mul(g[3], l3)));
 }
 
 template <int S>
@@ -97,6 +123,7 @@ template <int D, bool BIN>
 __global__ void __launch_bounds__(SC_THREADS)
     sc_round_kernel(Polys<Fac<D, BIN>::S> P, size_t half, int fold, const ef2* __restrict__ rptr,
                     ef2* __restrict__ partial) {
+  const bool skip1 = fold != 0;  // every round but the first: g(1) comes from the claim
   constexpr int S = Fac<D, BIN>::S;
   __shared__ ef2 red[(D + 1) * 32];
   ef2 s[D + 1];
@@ -120,12 +147,39 @@ __global__ void __launch_bounds__(SC_THREADS)
         hi[j] = p[i + half];
       }
     }
-    accumulate_pair<D, BIN>(lo, hi, s);
+    accumulate_pair<D, BIN>(lo, hi, s, skip1);
   }
   block_reduce<D>(s, red);
   if (threadIdx.x == 0)
 #pragma unroll
     for (int q = 0; q <= D; ++q) partial[(size_t)blockIdx.x * (D + 1) + q] = s[q];
+}
+
+// Round 0 of the binary check [b, b - 1, eq] with b in {0, 1}: over a pair, b(q) (b(q) - 1) is 0
+// at q = 0, 1, and 2 resp. 6 at q = 2, 3 exactly when lo != hi (b(q) = q or 1 - q), so the round
+// is g(0) = g(1) = 0, g(2) = 2 sum eq(2), g(3) = 6 sum eq(3) over the pairs with lo != hi.
+__global__ void __launch_bounds__(SC_THREADS)
+    sc_bin_round0_kernel(const ef2* __restrict__ b, const ef2* __restrict__ eq, size_t half,
+                         ef2* __restrict__ partial) {
+  __shared__ ef2 red[4 * 32];
+  ef2 s[4] = {ef_zero(), ef_zero(), ef_zero(), ef_zero()};
+  const u64* bc = (const u64*)b;  // c0 of b[i] at bc[2 i]
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < half;
+       i += (size_t)gridDim.x * blockDim.x) {
+    if (bc[2 * i] != bc[2 * (i + half)]) {
+      const ef2 lo = eq[i], hi = eq[i + half];
+      const ef2 d = ef_sub(hi, lo), e2 = ef_add(hi, d);
+      s[2] = ef_add(s[2], e2);
+      s[3] = ef_add(s[3], ef_add(e2, d));
+    }
+  }
+  block_reduce<3>(s, red);
+  if (threadIdx.x == 0) {
+    partial[(size_t)blockIdx.x * 4 + 0] = ef_zero();
+    partial[(size_t)blockIdx.x * 4 + 1] = ef_zero();
+    partial[(size_t)blockIdx.x * 4 + 2] = ef_scale(s[2], 2);
+    partial[(size_t)blockIdx.x * 4 + 3] = ef_scale(s[3], 6);
+  }
 }
 
 // Remaining rounds t0..k-1 in one CTA, in shared memory.  On entry the vectors hold `len`
@@ -139,6 +193,15 @@ __global__ void __launch_bounds__(SC_TAIL_THREADS)
   constexpr int S = Fac<D, BIN>::S;
   __shared__ ef2 red[(D + 1) * 32];
   __shared__ ef2 sv[S][Fac<D, BIN>::TAIL];
+  // Rounds 0 .. t0-1 were summed without g(1) (except round 0): fill it in along the claim
+  // chain, g_t(1) = g_{t-1}(r_{t-1}) - g_t(0), and carry the claim into this kernel's rounds.
+  ef2 claim = ef_zero();
+  if (threadIdx.x == 0)
+    for (unsigned t = 0; t < t0; ++t) {
+      ef2* g = rounds_out + (size_t)t * (D + 1);
+      if (t > 0) g[1] = ef_sub(claim, g[0]);
+      claim = interp_at<D>(g, ch[t]);
+    }
   {
     const ef2 r = fold ? ch[t0 - 1] : ef_zero();
     for (unsigned i = threadIdx.x; i < len; i += blockDim.x)
@@ -152,16 +215,20 @@ __global__ void __launch_bounds__(SC_TAIL_THREADS)
     ef2 s[D + 1];
 #pragma unroll
     for (int q = 0; q <= D; ++q) s[q] = ef_zero();
+    const bool skip1 = t > 0;
     for (unsigned i = threadIdx.x; i < half; i += blockDim.x) {
       ef2 lo[S], hi[S];
 #pragma unroll
       for (int j = 0; j < S; ++j) lo[j] = sv[j][i], hi[j] = sv[j][i + half];
-      accumulate_pair<D, BIN>(lo, hi, s);
+      accumulate_pair<D, BIN>(lo, hi, s, skip1);
     }
     block_reduce<D>(s, red);
-    if (threadIdx.x == 0)
+    if (threadIdx.x == 0) {
+      if (skip1) s[1] = ef_sub(claim, s[0]);
 #pragma unroll
       for (int q = 0; q <= D; ++q) rounds_out[(size_t)t * (D + 1) + q] = s[q];
+      claim = interp_at<D>(s, ch[t]);
+    }
     const ef2 r = ch[t];
     for (unsigned i = threadIdx.x; i < half; i += blockDim.x)
 #pragma unroll
@@ -217,20 +284,24 @@ void sumcheck_run(ef2* const* polys, unsigned k, const ef2* ch, ef2* rounds_out,
   while (t < k && len > Fac<D, BIN>::TAIL) {
     size_t half = len >> 1;
     unsigned blocks = (unsigned)std::min<size_t>(SC_MAX_BLOCKS, cdiv(half, SC_THREADS));
-    sc_round_kernel<D, BIN><<<blocks, SC_THREADS, 0, st>>>(
-        P, half, fold, fold ? ch + (t - 1) : ch, partials + (size_t)t * stride);
+    if (BIN && t == 0)
+      sc_bin_round0_kernel<<<blocks, SC_THREADS, 0, st>>>(P.p[0], P.p[S - 1], half, partials);
+    else
+      sc_round_kernel<D, BIN><<<blocks, SC_THREADS, 0, st>>>(
+          P, half, fold, fold ? ch + (t - 1) : ch, partials + (size_t)t * stride);
     LGS_LAUNCH_CHECK();
     len = half;
     fold = 1;
     ++t;
   }
-  sc_tail_kernel<D, BIN><<<1, SC_TAIL_THREADS, 0, st>>>(P, (unsigned)len, fold, ch, t, k,
-                                                        rounds_out, final_out);
-  LGS_LAUNCH_CHECK();
+  // the multi-CTA rounds' sums first: the tail completes their g(1) along the claim chain
   if (t > 0) {
     sc_reduce_kernel<D><<<t, 256, 0, st>>>(partials, stride, k, rounds_out);
     LGS_LAUNCH_CHECK();
   }
+  sc_tail_kernel<D, BIN><<<1, SC_TAIL_THREADS, 0, st>>>(P, (unsigned)len, fold, ch, t, k,
+                                                        rounds_out, final_out);
+  LGS_LAUNCH_CHECK();
 }
 }  // namespace
 
