@@ -846,9 +846,10 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     bf_commit(c, bi, 0, WS, li_bi, &bi_st, b);
     mark("B_bi_commit_end", b);
   }
-  // C: binary check, factors [B_I, B_I - 1, eq_alpha1] (pcs/src/ligesis.rs:419-429)
+  // C: binary check, factors [B_I, B_I - 1, eq_alpha1] (pcs/src/ligesis.rs:419-429); the
+  // longest branch, so it is the third high-priority one
   {
-    cudaStream_t b = branch();
+    cudaStream_t b = branch(true);
     ef2* p0 = ar.get<ef2>(WS);
     ef2* p2 = ar.get<ef2>(WS);
     lift_bf(bi, p0, WS, 0, b);

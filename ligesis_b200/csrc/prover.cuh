@@ -244,7 +244,7 @@ struct lgs_ctx {
   int device = 0;
   cudaStream_t st = nullptr;
   cudaStream_t side[NSIDE] = {};
-  static constexpr int NSIDE_HI = 2;  // high-priority side streams for the critical branches
+  static constexpr int NSIDE_HI = 3;  // high-priority side streams for the critical branches
   cudaStream_t side_hi[NSIDE_HI] = {};
   cudaEvent_t ev_fork2 = nullptr;
   cudaEvent_t ev_done[NSIDE] = {};
