@@ -15,7 +15,8 @@ than the 126 MB L2, so no step starts from a warm L2.
 `e2e`     the same through the public API (`Ligesis.commit` on a pinned host f, then
           `Ligesis.prove`), host->device copy of f and the proof read-back inside the region.
 `--impl reference`: the CPU restatement of the reference prover (single-threaded, as the
-          reference prescribes), timed on a bounded sample (mu = 22, 2^7 x 2^15) scaled to mu = 24.
+          reference prescribes), timed on a bounded sample (mu = 20, 2^6 x 2^14) scaled x16 to
+          mu = 24 (the dominant subset-sum hash is linear in 2^mu).
 """
 from __future__ import annotations
 
@@ -34,7 +35,7 @@ sys.path.insert(0, str(ROOT))
 
 LOG_M, LOG_N = 7, 17
 MU = LOG_M + LOG_N
-SAMPLE_SHAPE = (7, 15)  # CPU sample: mu = 22, scaled by 2^(24-22)
+SAMPLE_SHAPE = (6, 14)  # CPU sample: mu = 20, scaled by 2^(24-20)
 METRIC = "LigeSIS commit+eval ms at mu=24 (2^7 x 2^17)"
 
 
@@ -100,7 +101,7 @@ def run_reference(args) -> None:
         ms, info = cpu_sample_ms()
         times.append(ms)
     ms = statistics.mean(times)
-    sample = (f"oracle commit+prove at mu=22 (2^7 x 2^15), {info['commit_s']}+{info['prove_s']} s "
+    sample = (f"oracle commit+prove at mu=20 (2^6 x 2^14), {info['commit_s']}+{info['prove_s']} s "
               f"per sample, scaled x{info['scale']} to mu=24 (the dominant subset-sum hash is "
               f"linear in 2^mu); 1 thread on {_cpu_model()}")
     line = {
@@ -359,7 +360,7 @@ def run_ours(args) -> None:
     if not args.no_cpu_baseline:
         cms, info = cpu_sample_ms()
         cpu = {"value": round(cms, 1), "unit": "ms", "cores": 1, "kind": "port",
-               "sample": f"oracle commit+prove at mu=22 (2^7 x 2^15), "
+               "sample": f"oracle commit+prove at mu=20 (2^6 x 2^14), "
                          f"{info['commit_s']}+{info['prove_s']} s, scaled x{info['scale']} to "
                          f"mu=24; 1 thread on {_cpu_model()}"}
 
