@@ -603,7 +603,7 @@ def run_timeline(args) -> None:
     marks = ["prefix_end", "abar_end", "A1_abar_commit_end", "A2_rs_abar_table_sc_end", "B_bi_commit_end",
              "C_binary_sc_end", "D_hash_recon_sc_end", "E_rslink_sc_end", "F_bi_batch_sc_end",
              "G_a_batch_sc_end", "H_basefold_msgs_end", "main_suffix_start", "main_levels_end",
-             "main_level_trees_end", "join", "end"]
+             "main_level_trees_end", "join", "tree_ready", "end"]
     out = {}
     for name in ["prove_device"] + ["tl:" + m for m in marks]:
         tot, cnt = C.c_double(), C.c_uint64()

@@ -123,6 +123,7 @@ void lgs_ctx_destroy(lgs_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->st) cudaStreamSynchronize(ctx->st);
+  if (ctx->hs) cudaStreamSynchronize(ctx->hs);
   // Release the context's own device memory while its stream still exists (the frees are
   // ordered on it), then drain and destroy the streams.
   ctx->prof.flush();
@@ -150,6 +151,11 @@ void lgs_ctx_destroy(lgs_ctx* ctx) {
   ctx->graphs.clear();
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_fork2) cudaEventDestroy(ctx->ev_fork2);
+  if (ctx->ev_cw) cudaEventDestroy(ctx->ev_cw);
+  if (ctx->hs) {
+    cudaStreamSynchronize(ctx->hs);
+    cudaStreamDestroy(ctx->hs);
+  }
   for (int i = 0; i < lgs_ctx::NSIDE_HI; ++i)
     if (ctx->side_hi[i]) {
       cudaStreamSynchronize(ctx->side_hi[i]);
@@ -263,6 +269,7 @@ lgs_status lgs_commit_read(lgs_ctx* ctx, const lgs_commit_data* cd, int which, u
     need(which == 0 || which == 1, "lgs_commit_read: which must be 0 or 1");
     need(count * 8 == src.bytes, "lgs_commit_read: wrong element count");
     CtxDevice dg(ctx);
+    if (cd->done) LGS_CUDA(cudaStreamWaitEvent(ctx->st, cd->done, 0));  // H is the hash stream's
     LGS_CUDA(cudaMemcpyAsync(out, src.p, src.bytes, cudaMemcpyDeviceToHost, ctx->st));
     LGS_CUDA(cudaStreamSynchronize(ctx->st));
   });
@@ -287,10 +294,8 @@ lgs_status lgs_prove(lgs_ctx* ctx, const lgs_pk* pk, const lgs_commit_data* cd,
          "lgs_prove: null argument");
     CtxDevice dg(ctx);
     uint64_t cur[2] = {cursors[0], cursors[1]};
-    std::vector<uint8_t>& buf = ctx->proof_buf;
-    std::vector<uint8_t> out;
-    prove_dev(ctx, pk, cd, z, zlen, fields, nfields, ints, nints, cur, &out);
-    buf.swap(out);
+    std::vector<uint8_t>& buf = ctx->proof_buf;  // reused: written in place by the prove
+    prove_dev(ctx, pk, cd, z, zlen, fields, nfields, ints, nints, cur, &buf);
     *proof = buf.data();
     *proof_len = buf.size();
     cursors[0] = cur[0];

@@ -47,19 +47,24 @@ GL_HD u64 gl_reduce(u64 lo, u64 hi) {
 __device__ __forceinline__ u64 gl_pack(uint32_t lo, uint32_t hi) {
   return ((u64)hi << 32) | lo;
 }
-// a + b: s = a + b (carry c1), t = s + eps = s - p (carry c2); exactly one of "c1 or c2" says
-// that the canonical result is t (a, b < p, so they are never both set).
+// a + b: s = a + b (carry c1), and c2 = the carry of s + eps (that is, s >= p); exactly one of
+// them set means the canonical result is s + eps = s - p (mod 2^64) (a, b < p, so never both).
+// The correction s + (c1 + c2) eps is one wide multiply-add, which runs on the FMA pipe instead
+// of selects on the integer ALU pipe.
 __device__ __forceinline__ u64 gl_add(u64 a, u64 b) {
-  uint32_t s0, s1, t0, t1, c;
-  asm("add.cc.u32 %0, %5, %7;\n\t"
-      "addc.cc.u32 %1, %6, %8;\n\t"
-      "addc.u32 %2, 0, 0;\n\t"
-      "add.cc.u32 %3, %0, 0xffffffff;\n\t"
-      "addc.cc.u32 %4, %1, 0;\n\t"
-      "addc.u32 %2, %2, 0;"
-      : "=&r"(s0), "=&r"(s1), "=&r"(c), "=&r"(t0), "=&r"(t1)
+  u64 r;
+  asm("{\n\t.reg .u32 s0, s1, d, c;\n\t.reg .u64 s;\n\t"
+      "add.cc.u32 s0, %1, %3;\n\t"
+      "addc.cc.u32 s1, %2, %4;\n\t"
+      "addc.u32 c, 0, 0;\n\t"
+      "add.cc.u32 d, s0, 0xffffffff;\n\t"
+      "addc.cc.u32 d, s1, 0;\n\t"
+      "addc.u32 c, c, 0;\n\t"
+      "mov.b64 s, {s0, s1};\n\t"
+      "mad.wide.u32 %0, c, 0xffffffff, s;\n\t}"
+      : "=l"(r)
       : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
-  return c ? gl_pack(t0, t1) : gl_pack(s0, s1);
+  return r;
 }
 // a - b: on a borrow, d = a - b + 2^64 and the result is d - eps = a - b + p.
 __device__ __forceinline__ u64 gl_sub(u64 a, u64 b) {
@@ -75,28 +80,32 @@ __device__ __forceinline__ u64 gl_sub(u64 a, u64 b) {
   return gl_pack(d0, d1);
 }
 // (r0 + r1 2^32 + r2 2^64 + r3 2^96) mod p = (r0 + r1 2^32) - r3 + r2 (2^32 - 1).
+// u = lo - r3 (minus eps on a borrow), w = u + r2 eps (plus eps on a carry, which cannot carry
+// again), then the canonical w - p if w >= p.  The products and both conditional corrections
+// are wide multiplies/multiply-adds (FMA pipe).
 __device__ __forceinline__ u64 gl_reduce4(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3) {
-  uint32_t w0, w1, t0, t1, c;
-  asm("{\n\t.reg .u32 u0, u1, m, v0, v1;\n\t"
-      "sub.cc.u32 u0, %5, %8;\n\t"       // u = lo - r3
-      "subc.cc.u32 u1, %6, 0;\n\t"
+  u64 r;
+  asm("{\n\t.reg .u32 u0, u1, m, v0, v1, w0, w1, d, c;\n\t.reg .u64 v, w;\n\t"
+      "sub.cc.u32 u0, %1, %4;\n\t"
+      "subc.cc.u32 u1, %2, 0;\n\t"
       "subc.u32 m, 0, 0;\n\t"
-      "sub.cc.u32 u0, u0, m;\n\t"        // borrow: u -= eps
+      "sub.cc.u32 u0, u0, m;\n\t"
       "subc.u32 u1, u1, 0;\n\t"
-      "sub.cc.u32 v0, 0, %7;\n\t"        // v = r2 2^32 - r2
-      "subc.u32 v1, %7, 0;\n\t"
-      "add.cc.u32 %0, u0, v0;\n\t"       // w = u + v
-      "addc.cc.u32 %1, u1, v1;\n\t"
-      "addc.u32 m, 0, 0;\n\t"
-      "neg.s32 m, m;\n\t"                 // carry: w += eps (cannot carry again)
-      "add.cc.u32 %0, %0, m;\n\t"
-      "addc.u32 %1, %1, 0;\n\t"
-      "add.cc.u32 %2, %0, 0xffffffff;\n\t" // t = w - p
-      "addc.cc.u32 %3, %1, 0;\n\t"
-      "addc.u32 %4, 0, 0;\n\t}"
-      : "=&r"(w0), "=&r"(w1), "=&r"(t0), "=&r"(t1), "=&r"(c)
+      "mul.wide.u32 v, %3, 0xffffffff;\n\t"
+      "mov.b64 {v0, v1}, v;\n\t"
+      "add.cc.u32 w0, u0, v0;\n\t"
+      "addc.cc.u32 w1, u1, v1;\n\t"
+      "addc.u32 c, 0, 0;\n\t"
+      "mov.b64 w, {w0, w1};\n\t"
+      "mad.wide.u32 w, c, 0xffffffff, w;\n\t"
+      "mov.b64 {w0, w1}, w;\n\t"
+      "add.cc.u32 d, w0, 0xffffffff;\n\t"
+      "addc.cc.u32 d, w1, 0;\n\t"
+      "addc.u32 c, 0, 0;\n\t"
+      "mad.wide.u32 %0, c, 0xffffffff, w;\n\t}"
+      : "=l"(r)
       : "r"(r0), "r"(r1), "r"(r2), "r"(r3));
-  return c ? gl_pack(t0, t1) : gl_pack(w0, w1);
+  return r;
 }
 __device__ __forceinline__ u64 gl_mul(u64 a, u64 b) {
   const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32);

@@ -194,8 +194,13 @@ inline size_t multiproof_bound(uint64_t q, uint64_t leaves) {
 struct ByteWriter {
   // Little-endian hosts only (x86-64, aarch64): integers are copied in memory order.
   static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "proof encoding assumes little-endian");
-  std::vector<uint8_t> b;
+  // Writes into `b`, which only grows: a buffer reused across proofs is neither reallocated nor
+  // cleared again once it is large enough.
+  std::vector<uint8_t> own;
+  std::vector<uint8_t>& b;
   size_t n = 0;
+  ByteWriter() : b(own) {}
+  explicit ByteWriter(std::vector<uint8_t>& into) : b(into) {}
   void need(size_t k) {
     if (n + k > b.size()) b.resize(std::max<size_t>(2 * b.size(), n + k + (1 << 16)));
   }
@@ -206,18 +211,30 @@ struct ByteWriter {
   }
   void u32v(uint32_t v) { raw(&v, 4); }
   void u64v(uint64_t v) { raw(&v, 8); }
+  // Shrinks the buffer to the bytes written and returns it (moved out of a writer that owns it).
   std::vector<uint8_t> finish() {
     b.resize(n);
     return std::move(b);
   }
+  size_t finish_in_place() {
+    b.resize(n);
+    return n;
+  }
   void bf(u64 v) { u64v(gl_canon(v)); }
-  // `count` field elements from `src`, canonicalised (EF values are 2 consecutive words)
+  // `count` field elements from `src`, canonicalised (EF values are 2 consecutive words): one
+  // bulk copy when every value is already canonical (a vectorisable check), else word by word.
   void bf_run(const u64* src, size_t count) {
     need(count * 8);
     uint8_t* d = b.data() + n;
-    for (size_t i = 0; i < count; ++i) {
-      const u64 v = gl_canon(src[i]);
-      std::memcpy(d + 8 * i, &v, 8);
+    bool canon = true;
+    for (size_t i = 0; i < count; ++i) canon &= src[i] < GL_P;
+    if (canon) {
+      std::memcpy(d, src, count * 8);
+    } else {
+      for (size_t i = 0; i < count; ++i) {
+        const u64 v = gl_canon(src[i]);
+        std::memcpy(d + 8 * i, &v, 8);
+      }
     }
     n += count * 8;
   }

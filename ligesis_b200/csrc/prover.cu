@@ -254,6 +254,8 @@ void ctx_init(lgs_ctx* c, int device) {
   for (int i = 0; i < lgs_ctx::NSIDE_HI; ++i)
     LGS_CUDA(cudaStreamCreateWithPriority(&c->side_hi[i], cudaStreamNonBlocking, prio_hi));
   LGS_CUDA(cudaEventCreateWithFlags(&c->ev_fork2, cudaEventDisableTiming));
+  LGS_CUDA(cudaStreamCreateWithPriority(&c->hs, cudaStreamNonBlocking, prio_lo));
+  LGS_CUDA(cudaEventCreateWithFlags(&c->ev_cw, cudaEventDisableTiming));
   // Keep freed pool memory cached so per-proof buffers are recycled without driver calls.
   cudaMemPool_t pool;
   LGS_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
@@ -369,28 +371,29 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
                 c->st);
   }
   hc.lap("host_commit_rs");
+  // The hash and the tree need only the codeword: they run on the hash stream, and a prove
+  // enqueued next on the context stream runs beside them (its gather waits for cd->done).
+  LGS_CUDA(cudaEventRecord(c->ev_cw, c->st));
+  LGS_CUDA(cudaStreamWaitEvent(c->hs, c->ev_cw, 0));
   {
-    StageTimer t(c->prof, c->st, "subset_sum_hash");  // H and its Merkle leaf hashes
+    StageTimer t(c->prof, c->hs, "subset_sum_hash");  // H and its Merkle leaf hashes
     subset_sum_hash_tc(pk->tmap, cd->cw.as<u64>(), cd->H.as<u64>(), cd->nodes.as<u32>(),
-                       (unsigned)m, two_n, c->err.as<int>(), c->st);
+                       (unsigned)m, two_n, c->err.as<int>(), c->hs);
   }
   {
-    StageTimer t(c->prof, c->st, "merkle_h");
-    merkle_build_from_leaves(cd->nodes.as<u32>(), two_n, c->st);
+    StageTimer t(c->prof, c->hs, "merkle_h");
+    merkle_build_from_leaves(cd->nodes.as<u32>(), two_n, c->hs);
   }
   // error word and root into pinned memory; commit_finish reads them after a synchronisation
   LGS_CUDA(cudaMemcpyAsync(c->tail.as<uint8_t>(), c->err.p, sizeof(int), cudaMemcpyDeviceToHost,
-                           c->st));
+                           c->hs));
   LGS_CUDA(cudaMemcpyAsync(c->tail.as<uint8_t>() + 32, cd->nodes.as<u32>() + (2 * two_n - 2) * 8,
-                           32, cudaMemcpyDeviceToHost, c->st));
+                           32, cudaMemcpyDeviceToHost, c->hs));
+  if (!cd->done) cd->done = recycled_event();
+  LGS_CUDA(cudaEventRecord(cd->done, c->hs));
   hc.lap("host_commit_hash_merkle");
-  if (finish) {
-    commit_finish(c, cd);
-  } else {
-    if (!cd->done) cd->done = recycled_event();
-    LGS_CUDA(cudaEventRecord(cd->done, c->st));
-    cd->root_ready = false;
-  }
+  cd->root_ready = false;
+  if (finish) commit_finish(c, cd);
   hc.lap("host_commit_tail");
 }
 
@@ -417,6 +420,7 @@ void commit_root(lgs_ctx* c, lgs_commit_data* cd) {
 // of a bounded device wait if one gave up.  Nothing may overwrite the context's tail in between.
 void commit_finish(lgs_ctx* c, lgs_commit_data* cd) {
   LGS_CUDA(cudaStreamSynchronize(c->st));
+  LGS_CUDA(cudaStreamSynchronize(c->hs));
   c->prof.flush();
   int err = 0;
   std::memcpy(&err, c->tail.as<uint8_t>(), sizeof(int));
@@ -987,11 +991,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   mark("main_level_trees_end", st);
   for (size_t i = 0; i < brs.size(); ++i) LGS_CUDA(cudaStreamWaitEvent(st, c->ev_done[i], 0));
   mark("join", st);
-
-  // ---- gathers into staging, one read-back -------------------------------------------------
-  gather_segments((const GatherSeg*)(d_up + U_segs), (unsigned)plan.segs.size(), st);
-  LGS_CUDA(cudaMemcpyAsync(c->down.p, stage, sg.total * 8, cudaMemcpyDeviceToHost, st));
-  mark("end", st);
+  c->tl_count = ntl;
   };
   const ProveGraph* graph = prove_graph(c, s, enqueue);
   StageTimer t_prove(c->prof, st, "prove_device");
@@ -1002,6 +1002,14 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     enqueue();
     note_prove_need(c, s, ar.off);
   }
+  ntl = c->tl_count;
+  // ---- gathers into staging, one read-back: after the commitment's tree (the only thing the
+  // prove reads from the commit's hash stream: H columns and their Merkle nodes) -------------
+  if (cd->done) LGS_CUDA(cudaStreamWaitEvent(st, cd->done, 0));
+  mark("tree_ready", st);
+  gather_segments((const GatherSeg*)(d_up + U_segs), (unsigned)plan.segs.size(), st);
+  LGS_CUDA(cudaMemcpyAsync(c->down.p, stage, sg.total * 8, cudaMemcpyDeviceToHost, st));
+  mark("end", st);
   t_prove.stop();
   hc.lap("host_enqueue");
   const u64* hst = c->down.as<u64>();
@@ -1017,7 +1025,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   }
 
   // ---- encode straight from the staging buffer, in the order of encode_proof --------------
-  ByteWriter w;
+  ByteWriter w(*proof_out);
   w.need(sg.total * 8 + 4096);
   w.raw("LGSP", 4);
   w.u32v(1);
@@ -1066,7 +1074,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   opening(opens[1], false);
   w.u32v(1);  // base_ef: a-bar
   opening(opens[2], true);
-  *proof_out = w.finish();
+  w.finish_in_place();
   hc.lap("host_assemble");
   cursors[0] = f0 + fp.total;
   cursors[1] = i0 + INTS_PER_PROOF;

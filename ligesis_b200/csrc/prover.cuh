@@ -247,6 +247,10 @@ struct lgs_ctx {
   static constexpr int NSIDE_HI = 3;  // high-priority side streams for the critical branches
   cudaStream_t side_hi[NSIDE_HI] = {};
   cudaEvent_t ev_fork2 = nullptr;
+  // The commit's hash and Merkle tree run on hs after the codeword is ready (ev_cw), so a prove
+  // that follows overlaps them; only its final gather waits for the commitment's tree.
+  cudaStream_t hs = nullptr;
+  cudaEvent_t ev_cw = nullptr;
   cudaEvent_t ev_done[NSIDE] = {};
   cudaEvent_t ev_fork = nullptr;
   static constexpr int ROW_BLOCKS = 8;  // row blocks of a host upload pipelined with RS encoding
@@ -261,6 +265,7 @@ struct lgs_ctx {
   static constexpr int TL_MAX = 32;
   cudaEvent_t tl_ev[TL_MAX] = {};
   std::vector<std::string> tl_names;
+  unsigned tl_count = 0;  // marks recorded inside the prove's graph
   lgs::DevMem err;  // device error word of bounded-wait kernels (0 = ok)
   // Pinned host memory: every transfer of a call is asynchronous, so the host enqueues a whole
   // commit or prove without waiting for the device and synchronises once at the end.
