@@ -614,6 +614,69 @@ def run_timeline(args) -> None:
                       "ms_from_prove_start": out, "root": commit.root.hex()[:16]}), flush=True)
 
 
+def run_basefold(args) -> None:
+    """Standalone Basefold (pcs/benches/basefold.rs:144-150: mu in {22, 24}, code_rate 1, BF,
+    log_interleave 6): device commit (host polynomial in, root out), prove (host point and oracle
+    in, proof bytes out) and host verify, each the mean of `--steps` runs after warm-up; the CPU
+    oracle's commit and prove at mu = 22 beside it, and the README's single-thread numbers
+    (README.md:172,174) for context."""
+    import numpy as np
+
+    import ligesis_b200 as L
+    from ligesis_b200 import rng
+
+    ctx = L.Context(0)
+    readme = {22: {"commit_s": 1.0, "eval_s": 0.85, "verify_s": 0.007, "proof_kb": 391},
+              24: {"commit_s": 5.0, "eval_s": 3.5, "verify_s": 0.009, "proof_kb": 527}}
+    out = {}
+    for mu in (22, 24):
+        poly = L.MlPoly(rng.field_elements(10 + mu, 1 << mu))
+        pt = rng.ext_elements(20 + mu, mu)
+        oracle = L.RandomOracle(30 + mu, length=1024)
+        for _ in range(args.warmup):
+            state, commit = L.Basefold.commit_base(poly, 1, ctx)
+            oracle.restart()
+            proof = L.Basefold.prove(state, pt, oracle)
+        gc.collect()
+        gc.disable()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            del state
+            state, commit = L.Basefold.commit_base(poly, 1, ctx)
+        t1 = time.perf_counter()
+        for _ in range(args.steps):
+            oracle.restart()
+            proof = L.Basefold.prove(state, pt, oracle)
+        t2 = time.perf_counter()
+        for _ in range(args.steps):
+            oracle.restart()
+            ok = L.Basefold.verify(commit, pt, proof, oracle)
+        t3 = time.perf_counter()
+        gc.enable()
+        assert ok, "Basefold proof rejected"
+        k = args.steps
+        out[mu] = {"commit_ms": round((t1 - t0) / k * 1e3, 3), "prove_ms": round((t2 - t1) / k * 1e3, 3),
+                   "verify_ms": round((t3 - t2) / k * 1e3, 3), "proof_bytes": len(proof),
+                   "readme_cpu_1thread": readme[mu]}
+        del state
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import orc
+
+        poly = rng.field_elements(32, 1 << 22)
+        t0 = time.perf_counter()
+        cm = orc.BasefoldCommitment(poly, False, 1, 6)
+        t1 = time.perf_counter()
+        g = rng.SeededRng(52)
+        orc.basefold_prove(cm, rng.ext_elements(42, 22), g.ext_elements(1024), g.ints(1024))
+        t2 = time.perf_counter()
+        cpu = {"mu": 22, "commit_ms": round((t1 - t0) * 1e3, 1), "prove_ms": round((t2 - t1) * 1e3, 1),
+               "cores": 1, "kind": "port", "cpu": _cpu_model()}
+    print(json.dumps({"mode": "basefold", "code_rate": 1, "log_interleave": 6, "steps": args.steps,
+                      "timing": "host wall clock per call: host polynomial / point in, root / "
+                                "proof bytes out", "gpu": out, "cpu_oracle": cpu}), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -621,7 +684,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", choices=["line", "batch", "serve", "commit", "timeline"],
+    ap.add_argument("--mode", choices=["line", "batch", "serve", "commit", "timeline", "basefold"],
                     default="line")
     ap.add_argument("--log-m", type=int, default=LOG_M)
     ap.add_argument("--log-n", type=int, default=LOG_N)
@@ -642,6 +705,9 @@ def main() -> None:
         return
     if args.mode == "timeline":
         run_timeline(args)
+        return
+    if args.mode == "basefold":
+        run_basefold(args)
         return
     if args.impl == "reference":
         run_reference(args)

@@ -91,6 +91,32 @@ lgs_status lgs_verify(unsigned log_m, unsigned log_n, const uint8_t com_a[32],
                       size_t nfields, const uint64_t* ints, size_t nints, uint64_t cursors[2],
                       int* accept);
 
+/* ---- standalone Basefold PCS (pcs/src/basefold.rs) ----
+ * Basefold::commit_{base,ext}_on_domain (:341-382; commit_base/commit_ext are log_interleave 6,
+ * :309-339): poly holds 2^n values, BF (is_ef = 0, one u64 each) or EF (is_ef = 1, c0 c1),
+ * split into 2^log_interleave interleaved chunks (MlPoly::split), each RS-encoded at rate
+ * 2^-code_rate; root receives the BasefoldCommit.  The handle keeps the prover state
+ * (BasefoldProverState, :46-58) on the device until lgs_basefold_free.
+ * Limits: 1 <= log_interleave + 1 <= n, log_interleave <= 6, n - log_interleave + code_rate
+ * <= 22. */
+typedef struct lgs_basefold lgs_basefold;
+lgs_status lgs_basefold_commit(lgs_ctx* ctx, const uint64_t* poly, size_t len, int is_ef,
+                               unsigned code_rate, unsigned log_interleave, uint8_t root[32],
+                               lgs_basefold** out);
+void lgs_basefold_free(lgs_basefold* b);
+/* Basefold::prove (:384-516) at an n-coordinate EF point; the RandomOracle arrays and cursors as
+ * for lgs_prove (it draws n - log_interleave fields, then ceil(100 / code_rate) ints).  *proof is
+ * the encoded BasefoldProof ("LGSB", proof.hpp), owned by the context until its next prove. */
+lgs_status lgs_basefold_prove(lgs_ctx* ctx, const lgs_basefold* b, const uint64_t* point,
+                              size_t plen, const uint64_t* fields, size_t nfields,
+                              const uint64_t* ints, size_t nints, uint64_t cursors[2],
+                              const uint8_t** proof, size_t* proof_len);
+/* Basefold::verify (:518-642), on the host.  *accept = 1 or 0. */
+lgs_status lgs_basefold_verify(const uint8_t root[32], const uint64_t* point, size_t plen,
+                               const uint8_t* proof, size_t proof_len, const uint64_t* fields,
+                               size_t nfields, const uint64_t* ints, size_t nints,
+                               uint64_t cursors[2], int* accept);
+
 /* ---- batched and served proving (the reference proves one polynomial at a time on one
  * thread, pcs/benches/ligesis.rs:20-60) ----
  * An engine owns `lanes` contexts on one device, each driven by its own host thread, so the

@@ -25,10 +25,11 @@ from .ligesis import (
     shape_ok,
     sumcheck_prove,
 )
+from .basefold import Basefold, BasefoldCommit, BasefoldProof, BasefoldProverState
 from .rng import SeededRng
 
 __all__ = [
-    "CODE_RATE", "C_ROWS", "ETA", "NUM_COLS_OPENED", "CommitData", "Context", "LgsError",
+    "Basefold", "BasefoldCommit", "BasefoldProof", "BasefoldProverState", "CODE_RATE", "C_ROWS", "ETA", "NUM_COLS_OPENED", "CommitData", "Context", "LgsError",
     "Ligesis", "LigesisCommit", "LigesisProof", "MlPoly", "OracleExhausted", "ProvingKey",
     "RandomOracle", "SeededRng", "ShapeError", "SubsetSumHash", "VerifyingKey", "dft", "load",
     "merkle_root", "oracle_need", "shape_ok", "sumcheck_prove",

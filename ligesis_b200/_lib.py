@@ -67,6 +67,13 @@ _SIGS = {
     "lgs_profile": (C.c_int, [vp, C.c_int]),
     "lgs_profile_get": (C.c_int, [vp, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "lgs_launch_count": (C.c_uint64, []),
+    "lgs_basefold_commit": (C.c_int, [vp, u64p, C.c_size_t, C.c_int, C.c_uint, C.c_uint, u8p,
+                                      C.POINTER(vp)]),
+    "lgs_basefold_free": (None, [vp]),
+    "lgs_basefold_prove": (C.c_int, [vp, vp, u64p, C.c_size_t, u64p, C.c_size_t, u64p,
+                                     C.c_size_t, u64p, C.POINTER(u8p), C.POINTER(C.c_size_t)]),
+    "lgs_basefold_verify": (C.c_int, [u8p, u64p, C.c_size_t, u8p, C.c_size_t, u64p, C.c_size_t,
+                                      u64p, C.c_size_t, u64p, C.POINTER(C.c_int)]),
     "lgs_tensor_peak_i8": (C.c_int, [vp, C.c_uint, C.POINTER(C.c_double)]),
     "lgs_dft": (C.c_int, [vp, u64p, C.c_size_t, C.c_size_t, C.c_uint, u64p]),
     "lgs_subset_sum_hash": (C.c_int, [vp, u64p, C.c_size_t, u64p, C.c_size_t, u64p]),

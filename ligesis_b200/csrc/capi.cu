@@ -319,6 +319,61 @@ lgs_status lgs_verify(unsigned log_m, unsigned log_n, const uint8_t com_a[32],
   });
 }
 
+// ---- standalone Basefold ---------------------------------------------------------------------
+
+lgs_status lgs_basefold_commit(lgs_ctx* ctx, const uint64_t* poly, size_t len, int is_ef,
+                               unsigned code_rate, unsigned log_interleave, uint8_t root[32],
+                               lgs_basefold** out) {
+  return guarded([&] {
+    need(ctx && poly && root && out, "lgs_basefold_commit: null argument");
+    CtxDevice dg(ctx);
+    auto* b = new lgs_basefold;
+    try {
+      basefold_commit_dev(ctx, poly, len, is_ef != 0, code_rate, log_interleave, b);
+    } catch (...) {
+      cudaStreamSynchronize(ctx->st);
+      delete b;
+      throw;
+    }
+    std::memcpy(root, b->root.b, 32);
+    *out = b;
+  });
+}
+void lgs_basefold_free(lgs_basefold* b) { delete b; }
+
+lgs_status lgs_basefold_prove(lgs_ctx* ctx, const lgs_basefold* b, const uint64_t* point,
+                              size_t plen, const uint64_t* fields, size_t nfields,
+                              const uint64_t* ints, size_t nints, uint64_t cursors[2],
+                              const uint8_t** proof, size_t* proof_len) {
+  return guarded([&] {
+    need(ctx && b && point && fields && ints && cursors && proof && proof_len,
+         "lgs_basefold_prove: null argument");
+    need(b->device == ctx->device, "lgs_basefold_prove: commitment of another device");
+    CtxDevice dg(ctx);
+    uint64_t cur[2] = {cursors[0], cursors[1]};
+    std::vector<uint8_t>& buf = ctx->proof_buf;
+    basefold_prove_dev(ctx, b, point, plen, fields, nfields, ints, nints, cur, &buf);
+    *proof = buf.data();
+    *proof_len = buf.size();
+    cursors[0] = cur[0];
+    cursors[1] = cur[1];
+  });
+}
+
+lgs_status lgs_basefold_verify(const uint8_t root[32], const uint64_t* point, size_t plen,
+                               const uint8_t* proof, size_t proof_len, const uint64_t* fields,
+                               size_t nfields, const uint64_t* ints, size_t nints,
+                               uint64_t cursors[2], int* accept) {
+  return guarded([&] {
+    need(root && point && proof && fields && ints && cursors && accept,
+         "lgs_basefold_verify: null argument");
+    Hash32 rt;
+    std::memcpy(rt.b, root, 32);
+    *accept = basefold_verify_host(rt, point, plen, proof, proof_len, fields, nfields, ints, nints,
+                                   cursors);
+  });
+}
+
 // ---- measurement ----------------------------------------------------------------------------
 
 lgs_status lgs_profile(lgs_ctx* ctx, int enable) {

@@ -183,6 +183,17 @@ void eq_dot_dev(const void* vec, int is_bf, const ef2* point, unsigned k, ef2* o
   LGS_LAUNCH_CHECK();
 }
 
+__global__ void canon_kernel(u64* __restrict__ p, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    p[i] = gl_canon(p[i]);
+}
+void canon_u64(u64* p, size_t n, cudaStream_t st) {
+  if (!n) return;
+  canon_kernel<<<(unsigned)std::min<size_t>(cdiv(n, 256), 148 * 8), 256, 0, st>>>(p, n);
+  LGS_LAUNCH_CHECK();
+}
+
 // ---- a-bar = eq_{z1}^T F (pcs/src/ligesis.rs:372-379) --------------------------------------
 // Two adjacent columns per thread (16-byte loads), eight rows in flight.  The BF x EF products
 // are accumulated unreduced (160-bit sums of 128-bit products) and reduced once per output.

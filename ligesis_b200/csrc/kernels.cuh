@@ -63,6 +63,7 @@ void sumcheck_binary_dev(ef2* b, ef2* eq, unsigned k, const ef2* ch, ef2* rounds
                          ef2* final_out, ef2* partials, cudaStream_t st);
 
 // eval.cu
+void canon_u64(u64* p, size_t n, cudaStream_t st);  // p[i] = p[i] mod p, in place
 struct GatherSeg {
   const u64* src;
   const uint64_t* idx;  // item indices into src (units of `words`)

@@ -393,6 +393,52 @@ struct ByteReader {
   }
 };
 
+// Standalone Basefold proof ("LGSB", pcs/src/basefold.rs:84-103):
+//   "LGSB" u32:version=1, u32 num_vars, u32 code_rate, u32 log_interleave, u32 leaf_ef,
+//   claimed_eval:EF, u32 rounds, rounds x (l0:EF, l1:EF), u32 nroots, nroots*H32,
+//   u32 nfinal, nfinal EF, base opening<BF or EF>, u32 nfold, nfold*opening<EF>
+struct BasefoldProofH {
+  uint32_t num_vars = 0, code_rate = 0, log_interleave = 0, leaf_ef = 0;
+  ef2 claimed{};
+  std::vector<std::pair<ef2, ef2>> msgs;
+  std::vector<Hash32> roots;
+  std::vector<ef2> final_codeword;
+  OpeningH<u64> base_bf;
+  OpeningH<ef2> base_ef;
+  std::vector<OpeningH<ef2>> folds;
+};
+
+inline bool decode_basefold_proof(const uint8_t* d, size_t len, BasefoldProofH* p) {
+  ByteReader r(d, len);
+  if (!r.need(4) || std::memcmp(d, "LGSB", 4) != 0) return false;
+  r.pos = 4;
+  if (r.u32v() != 1) return false;
+  p->num_vars = r.u32v();
+  p->code_rate = r.u32v();
+  p->log_interleave = r.u32v();
+  p->leaf_ef = r.u32v();
+  if (!r.ok || p->num_vars > 40 || p->code_rate < 1 || p->code_rate > 8 ||
+      p->log_interleave > 6 || p->log_interleave >= p->num_vars || p->leaf_ef > 1)
+    return false;
+  p->claimed = r.ef();
+  size_t rounds = r.count(32);
+  for (size_t i = 0; i < rounds && r.ok; ++i) {
+    ef2 a = r.ef(), b = r.ef();
+    p->msgs.push_back({a, b});
+  }
+  size_t nroots = r.count(32);
+  for (size_t i = 0; i < nroots && r.ok; ++i) p->roots.push_back(r.h32());
+  size_t nf = r.count(16);
+  for (size_t i = 0; i < nf && r.ok; ++i) p->final_codeword.push_back(r.ef());
+  if (p->leaf_ef)
+    p->base_ef = r.opening<ef2>(16);
+  else
+    p->base_bf = r.opening<u64>(8);
+  size_t nfo = r.count(8);
+  for (size_t i = 0; i < nfo && r.ok; ++i) p->folds.push_back(r.opening<ef2>(16));
+  return r.ok && r.pos == len;
+}
+
 inline bool decode_proof(const uint8_t* d, size_t len, ProofH* p) {
   ByteReader r(d, len);
   if (!r.need(4) || std::memcmp(d, "LGSP", 4) != 0) return false;

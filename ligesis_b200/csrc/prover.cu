@@ -23,20 +23,25 @@ void d2d(void* dst, const void* src, size_t bytes, cudaStream_t st) {
 }
 
 // Basefold commit of `poly` (len elements, BF or EF) split into 2^li interleaved chunks
-// (MlPoly::split, utils/src/poly.rs:20-31), each zero-padded to 2 len/2^li and DFT'd; leaves are
-// the columns across chunks.  `out` receives codes (leaf-major) and the tree.
+// (MlPoly::split, utils/src/poly.rs:20-31), each zero-padded to len/2^li << code_rate and
+// DFT'd; leaves are the columns across chunks.  `out` receives codes (leaf-major) and the tree.
 void bf_commit(lgs_ctx* c, const u64* poly, int is_ef, size_t len, unsigned li,
-               BasefoldDev* out, cudaStream_t st) {
+               unsigned code_rate, BasefoldDev* out, cudaStream_t st) {
   Arena& ar = c->arena;
   const size_t rows = len >> li;
   const size_t cols = ((size_t)1 << li) * (is_ef ? 2 : 1);
-  const size_t L = rows << CODE_RATE;
+  const size_t L = rows << code_rate;
   const unsigned logL = ilog2(L);
   u64* tT = ar.get<u64>(cols * rows);
   u64* cT = ar.get<u64>(cols * L);
   u64* scr = logL > 12 ? ar.get<u64>(cols * L) : nullptr;
   transpose_u64(poly, tT, rows, cols, 1, st);
-  ntt_batch(tT, rows, rows, cT, L, logL, cols, scr, c->tw.as<u64>(), st);
+  // large transforms use the row kernels (one CTA per four columns of a row, which fills the
+  // GPU only with many rows); the prove's small Basefold commits keep the Stockham kernels
+  if (rs_dft_supported(logL, rows) && cols * L >= ((size_t)1 << 22) && cols <= 65535)
+    rs_dft_rows(tT, rows, rows, cT, L, logL, cols, scr, c->rs_tw.as<u64>(), st);
+  else
+    ntt_batch(tT, rows, rows, cT, L, logL, cols, scr, c->tw.as<u64>(), st);
   transpose_u64(cT, out->codes, cols, L, 1, st);
   merkle_leaves_contig(out->codes, (unsigned)cols, L, out->nodes, st);
   merkle_build_from_leaves(out->nodes, L, st);
@@ -307,7 +312,7 @@ void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lg
   pk->a_nodes.detach(release_stream(c->device));
   pk->a_state.codes = pk->a_codes.as<u64>();
   pk->a_state.nodes = pk->a_nodes.as<u32>();
-  bf_commit(c, pk->A.as<u64>(), 0, len, li, &pk->a_state, c->st);
+  bf_commit(c, pk->A.as<u64>(), 0, len, li, CODE_RATE, &pk->a_state, c->st);
   pk->com_a = read_root(pk->a_state.nodes, L, c->st);
 }
 
@@ -847,7 +852,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   // B: the Basefold commitment to B_I (pcs/src/ligesis.rs:411-416)
   {
     cudaStream_t b = branch(true);
-    bf_commit(c, bi, 0, WS, li_bi, &bi_st, b);
+    bf_commit(c, bi, 0, WS, li_bi, CODE_RATE, &bi_st, b);
     mark("B_bi_commit_end", b);
   }
   // C: binary check, factors [B_I, B_I - 1, eq_alpha1] (pcs/src/ligesis.rs:419-429); the
@@ -904,7 +909,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   {
     cudaStream_t b = branch(true);
     eq_dot_dev(a_vec, 0, d_prm + P_z2, log_n, (ef2*)(stage + S_y), partials_for(log_n, 1), b);
-    bf_commit(c, (const u64*)a_vec, 1, n, li_a, &a_st, b);
+    bf_commit(c, (const u64*)a_vec, 1, n, li_a, CODE_RATE, &a_st, b);
     mark("A1_abar_commit_end", b);
   }
   // A2: RS(a-bar), y4, the recon table sumcheck and y5 (pcs/src/ligesis.rs:387, 458, 487-497)
@@ -1078,6 +1083,226 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   hc.lap("host_assemble");
   cursors[0] = f0 + fp.total;
   cursors[1] = i0 + INTS_PER_PROOF;
+}
+
+// ---------------------------------------------------------------------------------------------
+// standalone Basefold (pcs/src/basefold.rs:309-516)
+// ---------------------------------------------------------------------------------------------
+void basefold_commit_dev(lgs_ctx* c, const u64* poly, size_t len, int is_ef, unsigned code_rate,
+                         unsigned li, lgs_basefold* out) {
+  if (len < 2 || (len & (len - 1))) throw ShapeError("basefold: 2^n values, n >= 1");
+  const unsigned n = ilog2(len);
+  if (li > LOG_INTERLEAVE || li >= n) throw ShapeError("basefold: 0 <= log_interleave < n, <= 6");
+  if (code_rate < 1 || n - li + code_rate > TW_LOG)
+    throw ShapeError("basefold: code_rate >= 1 and a code length up to 2^22");
+  const size_t words = len * (is_ef ? 2 : 1);
+  const size_t L = (len >> li) << code_rate;
+  const size_t cols = ((size_t)1 << li) * (is_ef ? 2 : 1);
+  out->device = c->device;
+  out->code_rate = code_rate;
+  c->arena.begin();
+  out->poly.alloc(words * 8, c->st);
+  out->codes.alloc(L * cols * 8, c->st);
+  out->nodes.alloc((2 * L - 1) * 32, c->st);
+  for (DevMem* d : {&out->poly, &out->codes, &out->nodes}) d->detach(release_stream(c->device));
+  h2d_staged(c, out->poly.p, poly, words * 8, c->st);
+  canon_u64(out->poly.as<u64>(), words, c->st);
+  out->st.codes = out->codes.as<u64>();
+  out->st.nodes = out->nodes.as<u32>();
+  bf_commit(c, out->poly.as<u64>(), is_ef, len, li, code_rate, &out->st, c->st);
+  LGS_CUDA(cudaMemcpyAsync(out->root.b, out->nodes.as<u32>() + (2 * L - 2) * 8, 32,
+                           cudaMemcpyDeviceToHost, c->st));
+  LGS_CUDA(cudaStreamSynchronize(c->st));
+}
+
+void basefold_prove_dev(lgs_ctx* c, const lgs_basefold* bf, const u64* point_host, size_t plen,
+                        const u64* fields_host, size_t nfields, const uint64_t* ints_host,
+                        size_t nints, uint64_t cursors[2], std::vector<uint8_t>* proof_out) {
+  const BasefoldDev& B = bf->st;
+  const unsigned n = B.num_vars, li = B.li, R = n - li, cr = bf->code_rate;
+  const size_t L = B.L, final_len = L >> R, q = (100 + cr - 1) / cr;  // query_num, :107-109
+  const unsigned words = B.leaf_words();
+  if (plen != n) throw ShapeError("basefold prove: the point must have num_vars coordinates");
+  const uint64_t f0 = cursors[0], i0 = cursors[1];
+  if (f0 > nfields || nfields - f0 < R) throw OracleError("oracle exhausted (fields)");
+  if (i0 > nints || nints - i0 < q) throw OracleError("oracle exhausted (ints)");
+  cudaStream_t st = c->st;
+  Arena& ar = c->arena;
+  ar.begin();
+
+  // ---- host transcript ------------------------------------------------------------------
+  std::vector<ef2> pt(n), rch(R);
+  for (unsigned i = 0; i < n; ++i)
+    pt[i] = ef_make(gl_canon(point_host[2 * i]), gl_canon(point_host[2 * i + 1]));
+  for (unsigned t = 0; t < R; ++t)
+    rch[t] = ef_make(fields_host[2 * (f0 + t)], fields_host[2 * (f0 + t) + 1]);
+  std::vector<uint64_t> base;  // q ints mod L/2, sorted and deduplicated (:787-795)
+  for (size_t t = 0; t < q; ++t) base.push_back(ints_host[i0 + t] % (L / 2));
+  std::sort(base.begin(), base.end());
+  base.erase(std::unique(base.begin(), base.end()), base.end());
+  const std::vector<uint64_t> bpos = level_positions(base, L / 2);
+  const std::vector<uint64_t> b_nodes = multiproof_nodes(bpos, L);
+  std::vector<std::vector<uint64_t>> lvl_pos(R), lvl_mp(R);
+  for (unsigned k = 1; k < R; ++k) {
+    lvl_pos[k] = level_positions(base, (L >> k) / 2);
+    lvl_mp[k] = multiproof_nodes(lvl_pos[k], L >> k);
+  }
+  // round t's messages are MLE(m) at (r_0 .. r_{t-1}, b, zp[t+1] .. zp[R-1]), b = 0, 1, with
+  // m = poly.fold(point[0..li]) (the reference folds m round by round, :419-443)
+  std::vector<ef2> qpts;
+  for (unsigned t = 0; t < R; ++t)
+    for (unsigned bit = 0; bit < 2; ++bit)
+      for (unsigned u = 0; u < R; ++u)
+        qpts.push_back(u < t ? rch[u] : (u == t ? (bit ? ef_one() : ef_zero()) : pt[li + u]));
+
+  // ---- staging layout (exact: this prove runs eagerly) --------------------------------------
+  Stage sg;
+  const size_t S_y = sg.take(2), S_msgs = sg.take((size_t)R * 4);
+  const size_t S_roots = sg.take((size_t)(R - 1) * 4), S_final = sg.take(final_len * 2);
+  const size_t S_bnodes = sg.take(b_nodes.size() * 4), S_bvals = sg.take(bpos.size() * words);
+  std::vector<size_t> S_lnodes(R), S_lvals(R);
+  for (unsigned k = 1; k < R; ++k) {
+    S_lnodes[k] = sg.take(lvl_mp[k].size() * 4);
+    S_lvals[k] = sg.take(lvl_pos[k].size() * 2);
+  }
+
+  // ---- device buffers --------------------------------------------------------------------
+  ef2* levels = ar.get<ef2>(2 * L);
+  std::vector<u32*> lvl_nodes(R, nullptr);
+  for (unsigned k = 1; k < R; ++k) lvl_nodes[k] = ar.get<u32>((2 * (L >> k) - 1) * 8);
+  const size_t mlen = (size_t)1 << R;
+  ef2* mv = ar.get<ef2>(mlen);
+  ef2* part1 = ar.get<ef2>(eqdot_partials_elems(n) + 1024);
+  ef2* part2 = ar.get<ef2>(eq_dot_multi_partials(R, 2 * R));
+  u64* stage = ar.get<u64>(sg.total);
+
+  SegPlan plan;
+  plan.add((const u64*)B.nodes, b_nodes, 4, S_bnodes);
+  plan.add(B.codes, bpos, words, S_bvals);
+  {
+    size_t off = L;
+    for (unsigned k = 1; k < R; ++k) {
+      const size_t len = L >> k;
+      plan.add((const u64*)lvl_nodes[k], lvl_mp[k], 4, S_lnodes[k]);
+      plan.add((const u64*)(levels + off), lvl_pos[k], 2, S_lvals[k]);
+      plan.add((const u64*)lvl_nodes[k], {2 * len - 2}, 4, S_roots + (k - 1) * 4);
+      off += len;
+    }
+    std::vector<uint64_t> fin(final_len);
+    for (size_t i = 0; i < final_len; ++i) fin[i] = i;
+    plan.add((const u64*)(levels + off), fin, 2, S_final);
+  }
+
+  // ---- one upload: point, challenges, message points, one-channel table, pointer, plan -------
+  size_t blob = 0;
+  auto part = [&](size_t bytes) {
+    const size_t o = blob;
+    blob += (bytes + 255) & ~(size_t)255;
+    return o;
+  };
+  const size_t U_pt = part(n * sizeof(ef2)), U_ch = part(R * sizeof(ef2));
+  const size_t U_q = part(qpts.size() * sizeof(ef2)), U_one = part(sizeof(ef2));
+  const size_t U_tasks = part(2 * R * sizeof(EqDotTask)), U_chs = part(sizeof(BfChannelDev));
+  const size_t U_ptr = part(sizeof(void*)), U_gidx = part(plan.idx.size() * 8);
+  const size_t U_segs = part(plan.segs.size() * sizeof(GatherSeg));
+  uint8_t* d_up = ar.get<uint8_t>(blob);
+  c->up.reserve(blob);
+  uint8_t* h_up = c->up.as<uint8_t>();
+  std::memcpy(h_up + U_pt, pt.data(), n * sizeof(ef2));
+  std::memcpy(h_up + U_ch, rch.data(), R * sizeof(ef2));
+  std::memcpy(h_up + U_q, qpts.data(), qpts.size() * sizeof(ef2));
+  const ef2 one = ef_one();
+  std::memcpy(h_up + U_one, &one, sizeof(ef2));
+  const ef2* d_pt = (const ef2*)(d_up + U_pt);
+  {
+    EqDotTask* tasks = (EqDotTask*)(h_up + U_tasks);
+    for (unsigned i = 0; i < 2 * R; ++i) {
+      tasks[i].vec = mv;
+      tasks[i].point = (const ef2*)(d_up + U_q) + (size_t)i * R;
+      tasks[i].out = (ef2*)(stage + S_msgs) + i;
+    }
+    BfChannelDev* ch = (BfChannelDev*)(h_up + U_chs);
+    ch->codes = B.codes;
+    ch->poly = bf->poly.as<u64>();
+    ch->is_ef = B.is_ef;
+    ch->li = li;
+    ch->point = d_pt;
+    const u64* pp = bf->poly.as<u64>();
+    std::memcpy(h_up + U_ptr, &pp, sizeof(pp));
+    std::memcpy(h_up + U_gidx, plan.idx.data(), plan.idx.size() * 8);
+    GatherSeg* segs = (GatherSeg*)(h_up + U_segs);
+    for (size_t i = 0; i < plan.segs.size(); ++i) {
+      segs[i] = plan.segs[i];
+      segs[i].idx = (const uint64_t*)(d_up + U_gidx) + (uintptr_t)plan.segs[i].idx;
+      segs[i].dst = stage + (uintptr_t)plan.segs[i].dst;
+    }
+  }
+  c->down.reserve(sg.total * 8);
+
+  // ---- device dataflow (pcs/src/basefold.rs:398-476) ----------------------------------------
+  h2d(d_up, h_up, blob, st);
+  eq_dot_dev(bf->poly.as<u64>(), B.is_ef ? 0 : 1, d_pt, n, (ef2*)(stage + S_y), part1, st);
+  bf_combine_dev((const BfChannelDev*)(d_up + U_chs), 1, (const ef2*)(d_up + U_one), L, levels,
+                 st);
+  bf_fold_poly_dev((const u64* const*)(d_up + U_ptr), B.is_ef, li, d_pt, mlen, mv, st);
+  eq_dot_multi_dev((const EqDotTask*)(d_up + U_tasks), 2 * R, R, part2, st);
+  bf_levels_dev(levels, L, R, (const ef2*)(d_up + U_ch), c->tw.as<u64>(), st);
+  {
+    std::vector<const u64*> ldata;
+    std::vector<u32*> lnodes;
+    std::vector<size_t> lcount;
+    size_t off = L;
+    for (unsigned k = 1; k < R; ++k) {
+      ldata.push_back((const u64*)(levels + off));
+      lnodes.push_back(lvl_nodes[k]);
+      lcount.push_back(L >> k);
+      off += L >> k;
+    }
+    for (size_t i = 0; i < lnodes.size(); i += 16) {  // the batched tree kernels take 16 trees
+      const unsigned cnt = (unsigned)std::min<size_t>(16, lnodes.size() - i);
+      merkle_leaves_many(ldata.data() + i, 2, lnodes.data() + i, lcount.data() + i, cnt, st);
+      merkle_build_many(lnodes.data() + i, lcount.data() + i, cnt, st);
+    }
+  }
+  gather_segments((const GatherSeg*)(d_up + U_segs), (unsigned)plan.segs.size(), st);
+  LGS_CUDA(cudaMemcpyAsync(c->down.p, stage, sg.total * 8, cudaMemcpyDeviceToHost, st));
+  LGS_CUDA(cudaStreamSynchronize(st));
+  const u64* hst = c->down.as<u64>();
+
+  // ---- encode ("LGSB", proof.hpp) ----------------------------------------------------------
+  ByteWriter w(*proof_out);
+  w.need(sg.total * 8 + 4096);
+  w.raw("LGSB", 4);
+  w.u32v(1);
+  w.u32v(n);
+  w.u32v(cr);
+  w.u32v(li);
+  w.u32v(B.is_ef ? 1 : 0);
+  w.bf_run(hst + S_y, 2);
+  w.u32v(R);
+  w.bf_run(hst + S_msgs, (size_t)R * 4);
+  w.u32v(R - 1);
+  w.raw(hst + S_roots, (size_t)(R - 1) * 32);
+  w.u32v((uint32_t)final_len);
+  w.bf_run(hst + S_final, final_len * 2);
+  auto opening = [&](size_t node_off, size_t nnodes, const std::vector<uint64_t>& keys,
+                     size_t val_off, unsigned vwords, unsigned nvals) {
+    w.u32v((uint32_t)(nnodes * 32));
+    w.raw(hst + node_off, nnodes * 32);
+    w.u32v((uint32_t)keys.size());
+    for (size_t i = 0; i < keys.size(); ++i) {
+      w.u64v(keys[i]);
+      w.u32v(nvals);
+      w.bf_run(hst + val_off + i * vwords, vwords);
+    }
+  };
+  opening(S_bnodes, b_nodes.size(), bpos, S_bvals, words, 1u << li);
+  w.u32v(R - 1);
+  for (unsigned k = 1; k < R; ++k)
+    opening(S_lnodes[k], lvl_mp[k].size(), lvl_pos[k], S_lvals[k], 2, 1);
+  w.finish_in_place();
+  cursors[0] = f0 + R;
+  cursors[1] = i0 + q;
 }
 
 }  // namespace lgs

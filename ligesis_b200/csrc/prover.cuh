@@ -305,6 +305,18 @@ struct lgs_commit_data {
   }
 };
 
+// A standalone Basefold commitment (pcs/src/basefold.rs:46-58 BasefoldProverState) resident on
+// the device: the polynomial, its interleaved codewords (leaf-major) and their Merkle tree.
+struct lgs_basefold {
+  int device = 0;
+  lgs::DevMem poly;   // 2^n values: BF (1 u64) or EF (2 u64), canonical
+  lgs::DevMem codes;  // L x 2^li values, leaf-major
+  lgs::DevMem nodes;  // Merkle tree over the L leaves
+  lgs::BasefoldDev st;
+  unsigned code_rate = 0;
+  lgs::Hash32 root;
+};
+
 namespace lgs {
 // The prover's stages (prover.cu).  commit_dev with finish = false only enqueues: commit_finish
 // (or any later synchronisation of the context followed by commit_finish) completes it.
@@ -314,6 +326,16 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device, lg
                 bool finish = true);
 void commit_finish(lgs_ctx* c, lgs_commit_data* cd);
 void commit_root(lgs_ctx* c, lgs_commit_data* cd);
+// Standalone Basefold (pcs/src/basefold.rs:309-516): commit_{base,ext}_on_domain of a host
+// polynomial and Basefold::prove at a point, the proof encoded as in proof.hpp ("LGSB").
+void basefold_commit_dev(lgs_ctx* c, const u64* poly, size_t len, int is_ef, unsigned code_rate,
+                         unsigned li, lgs_basefold* out);
+void basefold_prove_dev(lgs_ctx* c, const lgs_basefold* b, const u64* point, size_t plen,
+                        const u64* fields, size_t nfields, const uint64_t* ints, size_t nints,
+                        uint64_t cursors[2], std::vector<uint8_t>* proof_out);
+int basefold_verify_host(const Hash32& root, const u64* point, size_t plen, const uint8_t* proof,
+                         size_t proof_len, const u64* fields, size_t nfields, const uint64_t* ints,
+                         size_t nints, uint64_t cursors[2]);
 void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u64* z_host,
                size_t zlen, const u64* fields_host, size_t nfields, const uint64_t* ints_host,
                size_t nints, uint64_t cursors[2], std::vector<uint8_t>* proof_out);

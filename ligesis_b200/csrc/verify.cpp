@@ -15,6 +15,8 @@ namespace {
 using EFv = std::vector<ef2>;
 
 ef2 E(u64 a) { return ef_make(a, 0); }
+ef2 lift_value(u64 a) { return ef_make(a, 0); }
+ef2 lift_value(const ef2& a) { return a; }
 
 EFv new_eq(const EFv& p) {
   EFv ev{ef_one()};
@@ -293,7 +295,100 @@ bool batch_verify(const std::vector<Claim>& bfc, const std::vector<Claim>& efc,
   return ef_eq(comb, pf.final_codeword[0]);
 }
 
+// The level-0 value at leaf p of a standalone Basefold proof: sum_j eq4[j] leaf[j].
+template <class F>
+bool base_value(const OpeningH<F>& op, uint64_t p, const EFv& eq4, ef2* out) {
+  auto it = std::lower_bound(op.values.begin(), op.values.end(), p,
+                             [](const std::pair<uint64_t, std::vector<F>>& kv, uint64_t k) {
+                               return kv.first < k;
+                             });
+  if (it == op.values.end() || it->first != p || it->second.size() != eq4.size()) return false;
+  ef2 acc = ef_zero();
+  for (size_t j = 0; j < eq4.size(); ++j) acc = ef_add(acc, ef_mul(eq4[j], lift_value(it->second[j])));
+  *out = acc;
+  return true;
+}
+
 }  // namespace
+
+// Basefold::verify (pcs/src/basefold.rs:518-642): 1 accept, 0 reject.
+int basefold_verify_host(const Hash32& root, const u64* point, size_t plen, const uint8_t* proof,
+                         size_t proof_len, const u64* fields, size_t nfields,
+                         const uint64_t* ints, size_t nints, uint64_t cursors[2]) {
+  BasefoldProofH pf;
+  if (!decode_basefold_proof(proof, proof_len, &pf)) return 0;
+  const unsigned n = pf.num_vars, li = pf.log_interleave;
+  if (plen != n || n <= li || n - li + pf.code_rate > 40) return 0;
+  const unsigned rounds = n - li;
+  const uint64_t l = ((uint64_t)1 << (n - li)) << pf.code_rate;
+  if (pf.msgs.size() != rounds || pf.roots.size() + 1 != rounds || pf.folds.size() + 1 != rounds ||
+      pf.final_codeword.size() != (l >> rounds))
+    return 0;
+  Oracle o{fields, nfields, (size_t)cursors[0], ints, nints, (size_t)cursors[1]};
+  EFv pt(n);
+  for (unsigned i = 0; i < n; ++i) pt[i] = ef_make(gl_canon(point[2 * i]), gl_canon(point[2 * i + 1]));
+  auto run = [&]() -> bool {
+    const EFv eq4 = new_eq(EFv(pt.begin(), pt.begin() + li));
+    // evaluation-reduction claim chain
+    ef2 y = pf.claimed;
+    EFv ch;
+    for (unsigned t = 0; t < rounds; ++t) {
+      const ef2 l0 = pf.msgs[t].first, l1 = pf.msgs[t].second, zi = pt[li + t];
+      if (!ef_eq(ef_add(ef_mul(ef_sub(ef_one(), zi), l0), ef_mul(zi, l1)), y)) return false;
+      const ef2 r = o.field();
+      ch.push_back(r);
+      y = ef_add(ef_mul(ef_sub(ef_one(), r), l0), ef_mul(r, l1));
+    }
+    const size_t q = (100 + pf.code_rate - 1) / pf.code_rate;
+    const uint64_t* qi = o.take_ints(q);
+    std::vector<uint64_t> base;
+    for (size_t t = 0; t < q; ++t) base.push_back(qi[t] % (l / 2));
+    std::sort(base.begin(), base.end());
+    base.erase(std::unique(base.begin(), base.end()), base.end());
+    // Merkle openings: level 0 in the leaf field, folded levels in EF
+    if (pf.leaf_ef ? !opening_check(pf.base_ef, root, l) : !opening_check(pf.base_bf, root, l))
+      return false;
+    for (unsigned k = 1; k < rounds; ++k)
+      if (!opening_check(pf.folds[k - 1], pf.roots[k - 1], l >> k)) return false;
+    auto val_at = [&](unsigned k, uint64_t p, ef2* v) -> bool {
+      if (k == 0) return pf.leaf_ef ? base_value(pf.base_ef, p, eq4, v) : base_value(pf.base_bf, p, eq4, v);
+      const auto& vals = pf.folds[k - 1].values;
+      auto it = std::lower_bound(vals.begin(), vals.end(), p,
+                                 [](const std::pair<uint64_t, std::vector<ef2>>& kv, uint64_t key) {
+                                   return kv.first < key;
+                                 });
+      if (it == vals.end() || it->first != p || it->second.size() != 1) return false;
+      *v = it->second[0];
+      return true;
+    };
+    // fold consistency of every query down to the final codeword
+    const uint64_t final_len = l >> rounds;
+    for (uint64_t idx : base) {
+      ef2 derived{};
+      for (unsigned k = 0; k < rounds; ++k) {
+        const uint64_t cur = l >> k, half = cur / 2, pos = idx % half, sib = pos + half;
+        ef2 a, b;
+        if (!val_at(k, pos, &a) || !val_at(k, sib, &b)) return false;
+        if (k > 0 && !ef_eq(derived, (idx % cur == pos) ? a : b)) return false;
+        derived = eq_fold_at(a, b, ch[k], cur, pos);
+      }
+      if (!ef_eq(derived, pf.final_codeword[idx % final_len])) return false;
+    }
+    // the final codeword is constant and equals the reduced claim
+    for (const ef2& v : pf.final_codeword)
+      if (!ef_eq(v, pf.final_codeword[0])) return false;
+    return ef_eq(y, pf.final_codeword[0]);
+  };
+  bool ok;
+  try {
+    ok = run();
+  } catch (const std::runtime_error&) {
+    ok = false;  // oracle exhausted
+  }
+  cursors[0] = o.fi;
+  cursors[1] = o.ii;
+  return ok ? 1 : 0;
+}
 
 // Returns 1 accept, 0 reject.  Throws only on invalid arguments.
 int verify_host(unsigned log_m, unsigned log_n, const Hash32& com_a, const Hash32& root,

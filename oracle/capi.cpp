@@ -267,4 +267,88 @@ int orc_verify(const uint8_t* com_a, unsigned log_m, unsigned log_n, const uint8
   });
 }
 
+// ---- standalone Basefold (pcs/src/basefold.rs:309-642) ----
+struct OrcBasefold {
+  int is_ef = 0;
+  BasefoldState<u64> bf;
+  BasefoldState<EF> ef;
+};
+void* orc_basefold_commit(const u64* poly, size_t len, int is_ef, unsigned code_rate, unsigned li,
+                          uint8_t* root) {
+  try {
+    auto* h = new OrcBasefold;
+    h->is_ef = is_ef;
+    Hash r;
+    if (is_ef) {
+      h->ef = commit_on_domain(load_ef(poly, len), code_rate, li, &r);
+    } else {
+      std::vector<u64> v(poly, poly + len);
+      for (auto& x : v) x = canon(x);
+      h->bf = commit_on_domain(v, code_rate, li, &r);
+    }
+    std::memcpy(root, r.data(), 32);
+    return h;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return nullptr;
+  }
+}
+void orc_basefold_free(void* h) { delete (OrcBasefold*)h; }
+int orc_basefold_prove(void* h, const u64* point, size_t plen, const u64* fields, size_t nf,
+                       const u64* ints, size_t ni, uint64_t* cursors, uint8_t** proof,
+                       size_t* proof_len) {
+  ORC_TRY({
+    auto fv = load_ef(fields, nf);
+    Oracle o;
+    o.fields = fv.data();
+    o.nfields = fv.size();
+    o.ints = ints;
+    o.nints = ni;
+    o.fi = cursors[0];
+    o.ii = cursors[1];
+    auto* b = (OrcBasefold*)h;
+    const auto pt = load_ef(point, plen);
+    std::vector<uint8_t> bytes = b->is_ef ? encode_basefold_proof(basefold_prove(b->ef, pt, o))
+                                          : encode_basefold_proof(basefold_prove(b->bf, pt, o));
+    cursors[0] = o.fi;
+    cursors[1] = o.ii;
+    *proof = dup_bytes(bytes, proof_len);
+  });
+  return 0;
+}
+int orc_basefold_verify(const uint8_t* root, const u64* point, size_t plen, const uint8_t* proof,
+                        size_t proof_len, const u64* fields, size_t nf, const u64* ints,
+                        size_t ni, uint64_t* cursors) {
+  ORC_TRY({
+    const int leaf_ef = basefold_proof_leaf_ef(proof, proof_len);
+    if (leaf_ef < 0) return 0;
+    Hash r;
+    std::memcpy(r.data(), root, 32);
+    auto fv = load_ef(fields, nf);
+    Oracle o;
+    o.fields = fv.data();
+    o.nfields = fv.size();
+    o.ints = ints;
+    o.nints = ni;
+    o.fi = cursors[0];
+    o.ii = cursors[1];
+    const auto pt = load_ef(point, plen);
+    bool okv = false;
+    try {
+      if (leaf_ef) {
+        BasefoldProof<EF> pf;
+        okv = decode_basefold_proof(proof, proof_len, &pf) && basefold_verify(r, pt, pf, o);
+      } else {
+        BasefoldProof<u64> pf;
+        okv = decode_basefold_proof(proof, proof_len, &pf) && basefold_verify(r, pt, pf, o);
+      }
+    } catch (const std::exception&) {
+      okv = false;
+    }
+    cursors[0] = o.fi;
+    cursors[1] = o.ii;
+    return okv ? 1 : 0;
+  });
+}
+
 }  // extern "C"

@@ -67,6 +67,13 @@ def lib():
                                         C.c_size_t, u64p, C.POINTER(u8p), C.POINTER(C.c_size_t)]),
                 "orc_verify": (C.c_int, [u8p, C.c_uint, C.c_uint, u8p, u64p, C.c_size_t, u8p,
                                          C.c_size_t, u64p, C.c_size_t, u64p, C.c_size_t, u64p]),
+                "orc_basefold_commit": (vp, [u64p, C.c_size_t, C.c_int, C.c_uint, C.c_uint, u8p]),
+                "orc_basefold_free": (None, [vp]),
+                "orc_basefold_prove": (C.c_int, [vp, u64p, C.c_size_t, u64p, C.c_size_t, u64p,
+                                                 C.c_size_t, u64p, C.POINTER(u8p),
+                                                 C.POINTER(C.c_size_t)]),
+                "orc_basefold_verify": (C.c_int, [u8p, u64p, C.c_size_t, u8p, C.c_size_t, u64p,
+                                                  C.c_size_t, u64p, C.c_size_t, u64p]),
             }
             for name, (res, args) in sig.items():
                 fn = getattr(l, name)
@@ -287,4 +294,49 @@ def verify(com_a: bytes, log_m: int, log_n: int, root: bytes, z, proof: bytes, f
     pb = np.frombuffer(proof or b"\0", np.uint8).copy()
     rc = lib().orc_verify(_p8(ca), log_m, log_n, _p8(rt), _p64(z), z.shape[0], _p8(pb), len(proof),
                           _p64(f), f.shape[0], _p64(i), i.size, _p64(cur))
+    return bool(_ok(rc))
+
+
+# ---- standalone Basefold (pcs/src/basefold.rs:309-642) ----
+class BasefoldCommitment:
+    """Basefold::commit_{base,ext}_on_domain of `poly` (2^n BF, or 2^n x 2 EF)."""
+
+    def __init__(self, poly, is_ef: bool, code_rate: int, log_interleave: int = 6):
+        p = _u64(poly).reshape(-1)
+        n = p.size // 2 if is_ef else p.size
+        root = np.zeros(32, np.uint8)
+        h = lib().orc_basefold_commit(_p64(p), n, int(is_ef), code_rate, log_interleave, _p8(root))
+        if not h:
+            raise RuntimeError("oracle basefold commit: " + lib().orc_last_error().decode())
+        self.h, self.root, self.is_ef = h, root.tobytes(), is_ef
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_basefold_free(self.h)
+            self.h = None
+
+
+def basefold_prove(cm: BasefoldCommitment, point, fields, ints, cursors=(0, 0)):
+    pt = _u64(point).reshape(-1, 2).copy()
+    f = _u64(fields).reshape(-1, 2).copy()
+    i = _u64(ints).copy()
+    cur = np.array(cursors, dtype=np.uint64)
+    p = u8p()
+    n = C.c_size_t()
+    _ok(lib().orc_basefold_prove(cm.h, _p64(pt), pt.shape[0], _p64(f), f.shape[0], _p64(i), i.size,
+                                 _p64(cur), C.byref(p), C.byref(n)))
+    b = C.string_at(p, n.value)
+    lib().orc_free_buf(p)
+    return b, (int(cur[0]), int(cur[1]))
+
+
+def basefold_verify(root: bytes, point, proof: bytes, fields, ints, cursors=(0, 0)) -> bool:
+    pt = _u64(point).reshape(-1, 2).copy()
+    f = _u64(fields).reshape(-1, 2).copy()
+    i = _u64(ints).copy()
+    cur = np.array(cursors, dtype=np.uint64)
+    rt = np.frombuffer(root, np.uint8).copy()
+    pb = np.frombuffer(proof or b"\0", np.uint8).copy()
+    rc = lib().orc_basefold_verify(_p8(rt), _p64(pt), pt.shape[0], _p8(pb), len(proof), _p64(f),
+                                   f.shape[0], _p64(i), i.size, _p64(cur))
     return bool(_ok(rc))

@@ -15,6 +15,13 @@
 //          u32 nfold, nfold*opening<EF>, u32 nbf, nbf*opening<BF>, u32 nef, nef*opening<EF>
 //   opening<F>: u32 nbytes, bytes, u32 nvals, per value (u64 key, u32 len, len F), keys ascending
 // Integers are little-endian; BF is a canonical u64; EF is c0 then c1.
+//
+// Standalone BasefoldProof (pcs/src/basefold.rs:84-103), the same conventions:
+//   "LGSB" u32:version=1
+//   u32 num_vars, u32 code_rate, u32 log_interleave, u32 leaf_ef (0: BF leaves, 1: EF leaves)
+//   claimed_eval:EF, u32 rounds, rounds x (l0:EF, l1:EF)
+//   u32 nroots, nroots*H32, u32 nfinal, nfinal EF
+//   base:opening<LF>, u32 nfold, nfold*opening<EF>
 #pragma once
 #include <cstring>
 #include <vector>
@@ -229,6 +236,68 @@ inline bool decode_proof(const uint8_t* data, size_t len, LigesisProof* p) {
   for (size_t i = 0; i < nbf && r.ok; ++i) b.base_bf.push_back(r.opening<u64>(8));
   size_t nef = r.count(8);
   for (size_t i = 0; i < nef && r.ok; ++i) b.base_ef.push_back(r.opening<EF>(16));
+  return r.ok && r.pos == len;
+}
+
+// ---- standalone Basefold proofs ----
+template <class LF>
+inline std::vector<uint8_t> encode_basefold_proof(const BasefoldProof<LF>& p) {
+  Writer w;
+  w.b.insert(w.b.end(), {'L', 'G', 'S', 'B'});
+  w.u32(1);
+  w.u32(p.num_vars);
+  w.u32(p.code_rate);
+  w.u32(p.log_interleave);
+  w.u32(std::is_same<LF, EF>::value ? 1 : 0);
+  w.ef(p.claimed_eval);
+  w.u32((uint32_t)p.reduction_msgs.size());
+  for (auto& m : p.reduction_msgs) {
+    w.ef(m.first);
+    w.ef(m.second);
+  }
+  w.u32((uint32_t)p.fold_roots.size());
+  for (auto& h : p.fold_roots) w.hash(h);
+  w.u32((uint32_t)p.final_codeword.size());
+  for (auto& e : p.final_codeword) w.ef(e);
+  w.opening(p.base_opening);
+  w.u32((uint32_t)p.fold_openings.size());
+  for (auto& o : p.fold_openings) w.opening(o);
+  return w.b;
+}
+
+// The leaf field of an encoded standalone Basefold proof: 0 BF, 1 EF, -1 not such a proof.
+inline int basefold_proof_leaf_ef(const uint8_t* d, size_t len) {
+  if (len < 24 || std::memcmp(d, "LGSB", 4) != 0) return -1;
+  uint32_t v = 0;
+  std::memcpy(&v, d + 20, 4);
+  return v <= 1 ? (int)v : -1;
+}
+
+template <class LF>
+inline bool decode_basefold_proof(const uint8_t* d, size_t len, BasefoldProof<LF>* p) {
+  Reader r(d, len);
+  if (!r.need(4) || std::memcmp(d, "LGSB", 4) != 0) return false;
+  r.pos = 4;
+  if (r.u32() != 1) return false;
+  p->num_vars = r.u32();
+  p->code_rate = r.u32();
+  p->log_interleave = r.u32();
+  if (r.u32() != (std::is_same<LF, EF>::value ? 1u : 0u)) return false;
+  if (!r.ok || p->num_vars > 40 || p->code_rate > 8 || p->log_interleave > p->num_vars)
+    return false;
+  p->claimed_eval = r.ef();
+  size_t rounds = r.count(32);
+  for (size_t i = 0; i < rounds && r.ok; ++i) {
+    EF a = r.ef(), b = r.ef();
+    p->reduction_msgs.push_back({a, b});
+  }
+  size_t nroots = r.count(32);
+  for (size_t i = 0; i < nroots && r.ok; ++i) p->fold_roots.push_back(r.hash());
+  size_t nf = r.count(16);
+  for (size_t i = 0; i < nf && r.ok; ++i) p->final_codeword.push_back(r.ef());
+  p->base_opening = r.opening<LF>(sizeof(LF) == 8 ? 8 : 16);
+  size_t nfo = r.count(8);
+  for (size_t i = 0; i < nfo && r.ok; ++i) p->fold_openings.push_back(r.opening<EF>(16));
   return r.ok && r.pos == len;
 }
 

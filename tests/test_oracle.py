@@ -237,3 +237,40 @@ def test_setup_rejects_shapes_outside_window(orc):
     assert orc.lib().orc_shape_ok(7, 17) == 1
     assert orc.lib().orc_shape_ok(10, 10) == 0  # counts [21, 23, 10]
     assert orc.lib().orc_shape_ok(3, 10) == 1
+
+
+# ---- standalone Basefold (pcs/src/basefold.rs:1055-1146, restated on the oracle) ----
+def _basefold_case(orc, is_ef, n=12, code_rate=2, li=6, seed=90):
+    poly = rng.ext_elements(seed, 1 << n) if is_ef else rng.field_elements(seed, 1 << n)
+    cm = orc.BasefoldCommitment(poly, is_ef, code_rate, li)
+    pt = rng.ext_elements(seed + 1, n)
+    g = rng.SeededRng(seed + 2)
+    fields, ints = g.ext_elements(512), g.ints(512)
+    pf, cur = orc.basefold_prove(cm, pt, fields, ints)
+    return poly, cm, pt, fields, ints, pf, cur
+
+
+@pytest.mark.parametrize("is_ef", [False, True])
+def test_basefold_round_trip(orc, is_ef):
+    # commit_prove_verify_round_trip / commit_ext_round_trip: claimed_eval is the MLE value and
+    # verify accepts from the restarted oracle
+    poly, cm, pt, fields, ints, pf, cur = _basefold_case(orc, is_ef)
+    ev = poly if is_ef else np.stack([poly, np.zeros_like(poly)], axis=1)
+    want = orc.mle_eval(ev, pt)
+    got = np.frombuffer(pf[24:40], dtype=np.uint64)
+    assert [int(x) for x in got] == [int(x) for x in want]
+    assert cur == (12 - 6, 50)  # n - log_interleave fields, ceil(100 / code_rate) ints
+    assert orc.basefold_verify(cm.root, pt, pf, fields, ints)
+
+
+def test_basefold_tampered_message_is_rejected(orc):
+    # tampered_proof_is_rejected: reduction_msgs[0].0 += 1
+    _, cm, pt, fields, ints, pf, _ = _basefold_case(orc, False)
+    b = bytearray(pf)
+    c0 = int.from_bytes(b[44:52], "little")
+    b[44:52] = ((c0 + 1) % P).to_bytes(8, "little")
+    assert not orc.basefold_verify(cm.root, pt, bytes(b), fields, ints)
+    assert not orc.basefold_verify(cm.root, pt, pf[:-1], fields, ints)
+    wrong_pt = np.array(pt, dtype=np.uint64).copy()
+    wrong_pt[0, 0] ^= np.uint64(1)
+    assert not orc.basefold_verify(cm.root, wrong_pt, pf, fields, ints)
