@@ -26,10 +26,12 @@ from .ligesis import (
     sumcheck_prove,
 )
 from .basefold import Basefold, BasefoldCommit, BasefoldProof, BasefoldProverState
+from .pcs import BasefoldPcs, NoopCommit, NoopPcs
 from .rng import SeededRng
 
 __all__ = [
-    "Basefold", "BasefoldCommit", "BasefoldProof", "BasefoldProverState", "CODE_RATE", "C_ROWS", "ETA", "NUM_COLS_OPENED", "CommitData", "Context", "LgsError",
+    "Basefold", "BasefoldCommit", "BasefoldPcs", "BasefoldProof", "BasefoldProverState",
+    "CODE_RATE", "NoopCommit", "NoopPcs", "C_ROWS", "ETA", "NUM_COLS_OPENED", "CommitData", "Context", "LgsError",
     "Ligesis", "LigesisCommit", "LigesisProof", "MlPoly", "OracleExhausted", "ProvingKey",
     "RandomOracle", "SeededRng", "ShapeError", "SubsetSumHash", "VerifyingKey", "dft", "load",
     "merkle_root", "oracle_need", "shape_ok", "sumcheck_prove",

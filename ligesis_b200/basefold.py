@@ -64,6 +64,10 @@ class BasefoldProof:
     def num_vars(self) -> int:
         return struct.unpack_from("<I", self.data, 8)[0]
 
+    @property
+    def leaf_ef(self) -> bool:
+        return struct.unpack_from("<I", self.data, 20)[0] != 0
+
     def __len__(self) -> int:
         return len(self.data)
 

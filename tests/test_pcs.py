@@ -1,0 +1,34 @@
+"""The PolyCommitmentScheme mirror on the CPU: the reference's NoopPcs test (pcs/src/noop.rs:80-108)
+and BasefoldPcs's host-side rejections, which decide before any device call."""
+from __future__ import annotations
+
+import numpy as np
+
+import ligesis_b200 as L
+from ligesis_b200.pcs import BasefoldPcsCommitment, BasefoldPcsProof
+from tests.helpers import P
+
+
+def test_noop_commit_is_empty_and_verify_always_accepts(orc):
+    poly = L.MlPoly(np.arange(1, 9, dtype=np.uint64))
+    point = [5, 9, 2]
+    oracle = L.RandomOracle(3, length=16)
+    data, commit = L.NoopPcs.commit(poly)
+    assert data is poly and np.array_equal(data.evals, poly.evals)
+    assert commit == L.NoopCommit()
+    proof = L.NoopPcs.batch_prove([(data, point)], oracle)
+    ev = np.stack([poly.evals, np.zeros_like(poly.evals)], axis=1)
+    v = orc.mle_eval(ev, np.array([[x, 0] for x in point], dtype=np.uint64))
+    bogus = ((v[0] + 1) % P, v[1])
+    assert L.NoopPcs.batch_verify([(commit, point, bogus)], proof, oracle)
+
+
+def test_basefold_pcs_rejects_shape_mismatch_without_device():
+    pcs = L.BasefoldPcs()
+    oracle = L.RandomOracle(1, length=16)
+    com = BasefoldPcsCommitment(bytes(32), 4, True)
+    assert not pcs.batch_verify([(com, [1, 2, 3, 4], 0)], None, oracle)
+    assert not pcs.batch_verify([(com, [1, 2, 3, 4], 0)], BasefoldPcsProof([]), oracle)
+    assert not pcs.batch_verify([(com, [1, 2, 3], 0)], BasefoldPcsProof([b"LGSB" + bytes(60)]),
+                                oracle)
+    assert not pcs.batch_verify([(com, [1, 2, 3, 4], 0)], BasefoldPcsProof([b"junk"]), oracle)
