@@ -95,3 +95,45 @@ def test_basefold_pcs_small_polys(lgs, orc):
         assert proof.openings[0] == want
         oracle.restart()
         assert pcs.batch_verify([(com, pt, orc.mle_eval(raw, pt))], proof, oracle)
+
+
+def test_ligesis_pcs_batch_matches_oracle(lgs, orc):
+    """LigesisPcs: lifted integer witnesses of 10, 14 and 16 variables (the first zero-padded to
+    14) committed and opened in one batch; every root and proof equals the oracle's LigeSIS run on
+    the padded polynomial at the zero-extended point, cursors carried from task to task."""
+    pcs = L.LigesisPcs(seed=5)
+    raws = [rng.field_elements(60 + n, 1 << n) for n in (10, 14, 16)]
+    polys = [L.MlPoly(np.stack([r, np.zeros_like(r)], axis=1)) for r in raws]
+    commits = [pcs.commit(p) for p in polys]
+    points = [rng.ext_elements(70 + i, p.num_vars) for i, p in enumerate(polys)]
+    oracle = L.RandomOracle(9, length=4096)
+    fields, ints = oracle.fields.copy(), oracle.ints.copy()
+    proof = pcs.batch_prove([(d, pt) for (d, _), pt in zip(commits, points)], oracle)
+    cur = (0, 0)
+    values = []
+    for (d, com), raw, pt, pb in zip(commits, raws, points, proof.proofs):
+        mu = com.log_m + com.log_n
+        f = np.concatenate([raw, np.zeros((1 << mu) - raw.size, dtype=np.uint64)])
+        z = L.LigesisPcs._pad_point(pt, com.num_vars, mu)
+        key = orc.Key(com.log_m, com.log_n, d.pk.hash.a)
+        cm = orc.Commitment(key, f)
+        assert com.root == cm.root
+        want, cur = orc.prove(key, cm, z, fields, ints, cur)
+        assert pb == want
+        v = orc.mle_eval(np.stack([raw, np.zeros_like(raw)], axis=1), pt)
+        assert L.LigesisProof(pb).y == v
+        values.append(v)
+    assert tuple(int(x) for x in oracle.cursors) == cur
+
+    claims = [(com, pt, v) for (_, com), pt, v in zip(commits, points, values)]
+    oracle.restart()
+    assert pcs.batch_verify(claims, proof, oracle)
+    bogus = list(claims)
+    bogus[0] = (claims[0][0], claims[0][1], ((values[0][0] + 1) % P, values[0][1]))
+    oracle.restart()
+    assert not pcs.batch_verify(bogus, proof, oracle)
+    oracle.restart()
+    assert not pcs.batch_verify(claims[:2], proof, oracle)
+    other = [(claims[2][0], claims[1][1], claims[1][2])] + claims[2:]
+    oracle.restart()
+    assert not pcs.batch_verify([claims[0]] + other, proof, oracle)

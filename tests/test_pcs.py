@@ -32,3 +32,24 @@ def test_basefold_pcs_rejects_shape_mismatch_without_device():
     assert not pcs.batch_verify([(com, [1, 2, 3], 0)], BasefoldPcsProof([b"LGSB" + bytes(60)]),
                                 oracle)
     assert not pcs.batch_verify([(com, [1, 2, 3, 4], 0)], BasefoldPcsProof([b"junk"]), oracle)
+
+
+def test_ligesis_pcs_shapes_and_padding():
+    from ligesis_b200.workloads import shape_for_mu
+
+    for n in range(1, 29):
+        mu = L.LigesisPcs.padded_vars(n)
+        assert mu == max(n, 14)
+        log_m, log_n = shape_for_mu(mu)
+        assert log_m + log_n == mu and L.shape_ok(log_m, log_n)
+    pt = L.LigesisPcs._pad_point([3, 4, 5], 3, 14)
+    assert pt.shape == (14, 2) and list(pt[:3, 0]) == [3, 4, 5] and not pt[3:].any()
+
+
+def test_ligesis_pcs_refuses_extension_values():
+    import pytest
+
+    ev = np.zeros((1 << 4, 2), dtype=np.uint64)
+    ev[5, 1] = 1
+    with pytest.raises(ValueError):
+        L.LigesisPcs().commit(L.MlPoly(ev))
