@@ -9,6 +9,7 @@
 #include <cstring>
 #include <string>
 
+#include "frac_sum.hpp"
 #include "proof_io.hpp"
 
 using namespace orc;
@@ -351,4 +352,110 @@ int orc_basefold_verify(const uint8_t* root, const u64* point, size_t plen, cons
   });
 }
 
+}  // extern "C"
+
+// ---- GKR fraction sum and GKR-LogUp lookup (logup/src/frac_sum.rs, logup/src/lookup.rs) -----
+static Oracle make_oracle(const std::vector<EF>& fv, const u64* ints, size_t ni,
+                          const uint64_t* cursors) {
+  Oracle o;
+  o.fields = fv.data();
+  o.nfields = fv.size();
+  o.ints = ints;
+  o.nints = ni;
+  o.fi = cursors[0];
+  o.ii = cursors[1];
+  return o;
+}
+static void store_claim(const FsClaim& c, u64* point, u64* pq) {
+  for (size_t i = 0; i < c.point.size(); ++i) store_ef(c.point[i], point + 2 * i);
+  store_ef(c.p, pq);
+  store_ef(c.q, pq + 2);
+}
+
+extern "C" {
+// p == NULL: the numerators are all one.  point receives log2(n) EF, pq receives p_in(point) and
+// q_in(point).
+int orc_frac_sum_prove(const u64* p, const u64* q, size_t n, const u64* fields, size_t nf,
+                       uint64_t* cursors, uint8_t** proof, size_t* proof_len, u64* point,
+                       u64* pq) {
+  ORC_TRY({
+    auto fv = load_ef(fields, nf);
+    Oracle o = make_oracle(fv, nullptr, 0, cursors);
+    std::vector<EF> pv = p ? load_ef(p, n) : std::vector<EF>(n, ef_one());
+    FsClaim c;
+    auto pf = frac_sum_prove(pv, load_ef(q, n), o, &c);
+    cursors[0] = o.fi;
+    store_claim(c, point, pq);
+    *proof = dup_bytes(encode_frac_sum_proof(pf), proof_len);
+  });
+  return 0;
+}
+// 1 accept, 0 reject; point receives nlayers EF.
+int orc_frac_sum_verify(const uint8_t* proof, size_t len, const u64* fields, size_t nf,
+                        uint64_t* cursors, u64* point, size_t point_cap, u64* pq) {
+  ORC_TRY({
+    FracSumProof pf;
+    if (!decode_frac_sum_proof(proof, len, &pf) || pf.layers.size() > point_cap) return 0;
+    auto fv = load_ef(fields, nf);
+    Oracle o = make_oracle(fv, nullptr, 0, cursors);
+    FsClaim c;
+    bool okv = false;
+    try {
+      okv = frac_sum_verify(pf, o, &c);
+    } catch (const std::exception&) {
+      okv = false;
+    }
+    cursors[0] = o.fi;
+    if (!okv) return 0;
+    store_claim(c, point, pq);
+  });
+  return 1;
+}
+// e == NULL: the multiplicities are counted from a and t (lookup.rs:85-88).
+int orc_lookup_prove(const u64* a, size_t m, const u64* t, size_t n, const u64* e,
+                     const u64* fields, size_t nf, uint64_t* cursors, uint8_t** proof,
+                     size_t* proof_len, u64* zq, u64* zt) {
+  ORC_TRY({
+    auto fv = load_ef(fields, nf);
+    Oracle o = make_oracle(fv, nullptr, 0, cursors);
+    auto av = load_ef(a, m), tv = load_ef(t, n);
+    auto ev = e ? load_ef(e, n) : lookup_multiplicities(av, tv);
+    std::vector<EF> pq, pt;
+    auto pf = lookup_prove(av, tv, ev, o, &pq, &pt);
+    cursors[0] = o.fi;
+    for (size_t i = 0; i < pq.size(); ++i) store_ef(pq[i], zq + 2 * i);
+    for (size_t i = 0; i < pt.size(); ++i) store_ef(pt[i], zt + 2 * i);
+    *proof = dup_bytes(encode_lookup_proof(pf), proof_len);
+  });
+  return 0;
+}
+// 1 accept, 0 reject.  vals receives a(zq), e(zt), t(zt); zq / zt receive the points (their
+// lengths are the proof's layer counts, at most the given capacities).
+int orc_lookup_verify(const uint8_t* proof, size_t len, const u64* fields, size_t nf,
+                      uint64_t* cursors, u64* zq, size_t zq_cap, u64* zt, size_t zt_cap,
+                      u64* vals) {
+  ORC_TRY({
+    LookupProof pf;
+    if (!decode_lookup_proof(proof, len, &pf) || pf.query.layers.size() > zq_cap ||
+        pf.table.layers.size() > zt_cap)
+      return 0;
+    auto fv = load_ef(fields, nf);
+    Oracle o = make_oracle(fv, nullptr, 0, cursors);
+    LookupClaims c;
+    bool okv = false;
+    try {
+      okv = lookup_verify(pf, o, &c);
+    } catch (const std::exception&) {
+      okv = false;
+    }
+    cursors[0] = o.fi;
+    if (!okv) return 0;
+    for (size_t i = 0; i < c.zq.size(); ++i) store_ef(c.zq[i], zq + 2 * i);
+    for (size_t i = 0; i < c.zt.size(); ++i) store_ef(c.zt[i], zt + 2 * i);
+    store_ef(c.a, vals);
+    store_ef(c.e, vals + 2);
+    store_ef(c.t, vals + 4);
+  });
+  return 1;
+}
 }  // extern "C"

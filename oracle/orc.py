@@ -4,6 +4,7 @@ check and bench.py's CPU-baseline leg, always as the checker or the timed CPU ba
 from __future__ import annotations
 
 import ctypes as C
+import struct
 import subprocess
 import threading
 from pathlib import Path
@@ -74,6 +75,16 @@ def lib():
                                                  C.POINTER(C.c_size_t)]),
                 "orc_basefold_verify": (C.c_int, [u8p, u64p, C.c_size_t, u8p, C.c_size_t, u64p,
                                                   C.c_size_t, u64p, C.c_size_t, u64p]),
+                "orc_frac_sum_prove": (C.c_int, [u64p, u64p, C.c_size_t, u64p, C.c_size_t, u64p,
+                                                 C.POINTER(u8p), C.POINTER(C.c_size_t), u64p,
+                                                 u64p]),
+                "orc_frac_sum_verify": (C.c_int, [u8p, C.c_size_t, u64p, C.c_size_t, u64p, u64p,
+                                                  C.c_size_t, u64p]),
+                "orc_lookup_prove": (C.c_int, [u64p, C.c_size_t, u64p, C.c_size_t, u64p, u64p,
+                                               C.c_size_t, u64p, C.POINTER(u8p),
+                                               C.POINTER(C.c_size_t), u64p, u64p]),
+                "orc_lookup_verify": (C.c_int, [u8p, C.c_size_t, u64p, C.c_size_t, u64p, u64p,
+                                                C.c_size_t, u64p, C.c_size_t, u64p]),
             }
             for name, (res, args) in sig.items():
                 fn = getattr(l, name)
@@ -340,3 +351,97 @@ def basefold_verify(root: bytes, point, proof: bytes, fields, ints, cursors=(0, 
     rc = lib().orc_basefold_verify(_p8(rt), _p64(pt), pt.shape[0], _p8(pb), len(proof), _p64(f),
                                    f.shape[0], _p64(i), i.size, _p64(cur))
     return bool(_ok(rc))
+
+
+# ---- GKR fraction sum / GKR-LogUp lookup (logup/src/frac_sum.rs, logup/src/lookup.rs) ---------
+def _ef2(a):
+    return _u64(a).reshape(-1, 2).copy()
+
+
+def _take(p, n):
+    b = C.string_at(p, n.value)
+    lib().orc_free_buf(p)
+    return b
+
+
+def frac_sum_prove(p, q, fields, cursor: int = 0):
+    """frac_sum::prove over EF arrays p, q (p None: all ones).  Returns (proof bytes, point,
+    p_in(point), q_in(point), fields cursor after)."""
+    qq = _ef2(q)
+    n = qq.shape[0]
+    pp = None if p is None else _ef2(p)
+    f = _ef2(fields)
+    cur = np.array([cursor, 0], dtype=np.uint64)
+    k = n.bit_length() - 1
+    point = np.zeros((max(k, 1), 2), np.uint64)
+    pq = np.zeros(4, np.uint64)
+    b, ln = u8p(), C.c_size_t()
+    _ok(lib().orc_frac_sum_prove(None if pp is None else _p64(pp), _p64(qq), n, _p64(f),
+                                 f.shape[0], _p64(cur), C.byref(b), C.byref(ln), _p64(point),
+                                 _p64(pq)))
+    return (_take(b, ln), point[:k], (int(pq[0]), int(pq[1])), (int(pq[2]), int(pq[3])),
+            int(cur[0]))
+
+
+def frac_sum_verify(proof: bytes, fields, cursor: int = 0):
+    """frac_sum::verify: None on reject, else (point, p_in, q_in, fields cursor after)."""
+    f = _ef2(fields)
+    cur = np.array([cursor, 0], dtype=np.uint64)
+    point = np.zeros((64, 2), np.uint64)
+    pq = np.zeros(4, np.uint64)
+    pb = np.frombuffer(proof or b"\0", np.uint8).copy()
+    rc = _ok(lib().orc_frac_sum_verify(_p8(pb), len(proof), _p64(f), f.shape[0], _p64(cur),
+                                       _p64(point), 64, _p64(pq)))
+    if rc != 1:
+        return None
+    k = struct.unpack_from("<I", proof, 40)[0]
+    return point[:k], (int(pq[0]), int(pq[1])), (int(pq[2]), int(pq[3])), int(cur[0])
+
+
+def lookup_prove(a, t, e, fields, cursor: int = 0):
+    """lookup::prove_with_opening_points (e None: multiplicities counted as lookup::prove does).
+    Returns (proof bytes, zq, zt, fields cursor after)."""
+    aa, tt = _ef2(a), _ef2(t)
+    ee = None if e is None else _ef2(e)
+    f = _ef2(fields)
+    cur = np.array([cursor, 0], dtype=np.uint64)
+    mu, nu = aa.shape[0].bit_length() - 1, tt.shape[0].bit_length() - 1
+    zq = np.zeros((max(mu, 1), 2), np.uint64)
+    zt = np.zeros((max(nu, 1), 2), np.uint64)
+    b, ln = u8p(), C.c_size_t()
+    _ok(lib().orc_lookup_prove(_p64(aa), aa.shape[0], _p64(tt), tt.shape[0],
+                               None if ee is None else _p64(ee), _p64(f), f.shape[0], _p64(cur),
+                               C.byref(b), C.byref(ln), _p64(zq), _p64(zt)))
+    return _take(b, ln), zq[:mu], zt[:nu], int(cur[0])
+
+
+def lookup_verify(proof: bytes, fields, cursor: int = 0):
+    """lookup::verify: None on reject, else (zq, zt, a(zq), e(zt), t(zt), fields cursor after)."""
+    f = _ef2(fields)
+    cur = np.array([cursor, 0], dtype=np.uint64)
+    zq = np.zeros((64, 2), np.uint64)
+    zt = np.zeros((64, 2), np.uint64)
+    vals = np.zeros(6, np.uint64)
+    pb = np.frombuffer(proof or b"\0", np.uint8).copy()
+    rc = _ok(lib().orc_lookup_verify(_p8(pb), len(proof), _p64(f), f.shape[0], _p64(cur),
+                                     _p64(zq), 64, _p64(zt), 64, _p64(vals)))
+    if rc != 1:
+        return None
+    kq = struct.unpack_from("<I", proof, 48)[0]
+    kt = _frac_sum_layers(proof, 8 + _frac_sum_len(proof, 8))
+    v = [(int(vals[2 * i]), int(vals[2 * i + 1])) for i in range(3)]
+    return zq[:kq], zt[:kt], v[0], v[1], v[2], int(cur[0])
+
+
+def _frac_sum_layers(proof: bytes, off: int) -> int:
+    return struct.unpack_from("<I", proof, off + 40)[0]
+
+
+def _frac_sum_len(proof: bytes, off: int) -> int:
+    """Byte length of the FracSumProof encoded at off."""
+    nl = _frac_sum_layers(proof, off)
+    pos = off + 44
+    for _ in range(nl):
+        r = struct.unpack_from("<I", proof, pos)[0]
+        pos += 4 + (4 * r + 4) * 16
+    return pos - off
