@@ -117,6 +117,40 @@ lgs_status lgs_basefold_verify(const uint8_t root[32], const uint64_t* point, si
                                size_t nfields, const uint64_t* ints, size_t nints,
                                uint64_t cursors[2], int* accept);
 
+/* ---- GKR fraction sum and GKR-LogUp lookup (logup/src/frac_sum.rs, logup/src/lookup.rs) ----
+ * EF arrays hold 2 u64 per value (c0, c1), canonical.  With on_device = 1 the input pointers are
+ * device pointers on the context's device (16-byte aligned) and are only read; otherwise host
+ * memory.  `cursor` is the RandomOracle's fields cursor (in/out); these provers draw no ints.
+ * Proofs are owned by the context until its next prove.
+ *
+ * frac_sum::prove (:110-161): proves sum_i p_i / q_i = num / den over n = 2^k fractions (p NULL:
+ * every numerator is one), drawing k (k + 3) / 2 fields.  point receives the reduced input point
+ * (k EF, low-bit-first) and claim p_in(point), q_in(point) (2 EF).  The proof is "LGSF"
+ * (num, den, then per layer r its r round polynomials g(0..3) and the leaves A0 A1 B0 B1).
+ * Limit: k <= 28. */
+lgs_status lgs_frac_sum_prove(lgs_ctx* ctx, const uint64_t* p, const uint64_t* q, size_t n,
+                              int on_device, const uint64_t* fields, size_t nfields,
+                              uint64_t* cursor, const uint8_t** proof, size_t* proof_len,
+                              uint64_t* point, uint64_t claim[4]);
+/* frac_sum::verify (:221-258), on the host: *accept = 1 with point (point_cap EF at most) and
+ * claim filled, or 0 (the reference's None). */
+lgs_status lgs_frac_sum_verify(const uint8_t* proof, size_t proof_len, const uint64_t* fields,
+                               size_t nfields, uint64_t* cursor, uint64_t* point,
+                               size_t point_cap, uint64_t claim[4], int* accept);
+/* lookup::prove_with_opening_points (lookup.rs:119-143): every query a_i (m = 2^mu) lies in the
+ * table t (n = 2^nu distinct values) with multiplicities e (n values).  Draws alpha, then the
+ * query circuit's and the table circuit's fields.  zq / zt receive the opening points (mu / nu
+ * EF).  The proof is "LGSL" followed by the two "LGSF" proofs. */
+lgs_status lgs_lookup_prove(lgs_ctx* ctx, const uint64_t* a, size_t m, const uint64_t* t,
+                            const uint64_t* e, size_t n, int on_device, const uint64_t* fields,
+                            size_t nfields, uint64_t* cursor, const uint8_t** proof,
+                            size_t* proof_len, uint64_t* zq, uint64_t* zt);
+/* lookup::verify (:191-229), on the host: *accept = 1 with the opening claims a(zq), e(zt), t(zt)
+ * in vals (3 EF) and the points in zq / zt, or 0. */
+lgs_status lgs_lookup_verify(const uint8_t* proof, size_t proof_len, const uint64_t* fields,
+                             size_t nfields, uint64_t* cursor, uint64_t* zq, size_t zq_cap,
+                             uint64_t* zt, size_t zt_cap, uint64_t vals[6], int* accept);
+
 /* ---- batched and served proving (the reference proves one polynomial at a time on one
  * thread, pcs/benches/ligesis.rs:20-60) ----
  * An engine owns `lanes` contexts on one device, each driven by its own host thread, so the

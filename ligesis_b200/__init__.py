@@ -26,12 +26,15 @@ from .ligesis import (
     sumcheck_prove,
 )
 from .basefold import Basefold, BasefoldCommit, BasefoldProof, BasefoldProverState
+from .logup import (FracSum, FracSumProof, Lookup, LookupProof, OpeningClaim, Poly,
+                    multiplicity_vector)
 from .pcs import BasefoldPcs, LigesisPcs, NoopCommit, NoopPcs
 from .rng import SeededRng
 
 __all__ = [
     "Basefold", "BasefoldCommit", "BasefoldPcs", "BasefoldProof", "BasefoldProverState",
-    "CODE_RATE", "LigesisPcs", "NoopCommit", "NoopPcs", "C_ROWS", "ETA", "NUM_COLS_OPENED", "CommitData", "Context", "LgsError",
+    "CODE_RATE", "FracSum", "FracSumProof", "Lookup", "LookupProof", "OpeningClaim", "Poly",
+    "multiplicity_vector", "LigesisPcs", "NoopCommit", "NoopPcs", "C_ROWS", "ETA", "NUM_COLS_OPENED", "CommitData", "Context", "LgsError",
     "Ligesis", "LigesisCommit", "LigesisProof", "MlPoly", "OracleExhausted", "ProvingKey",
     "RandomOracle", "SeededRng", "ShapeError", "SubsetSumHash", "VerifyingKey", "dft", "load",
     "merkle_root", "oracle_need", "shape_ok", "sumcheck_prove",

@@ -74,6 +74,16 @@ _SIGS = {
                                      C.c_size_t, u64p, C.POINTER(u8p), C.POINTER(C.c_size_t)]),
     "lgs_basefold_verify": (C.c_int, [u8p, u64p, C.c_size_t, u8p, C.c_size_t, u64p, C.c_size_t,
                                       u64p, C.c_size_t, u64p, C.POINTER(C.c_int)]),
+    "lgs_frac_sum_prove": (C.c_int, [vp, u64p, u64p, C.c_size_t, C.c_int, u64p, C.c_size_t,
+                                     C.POINTER(C.c_uint64), C.POINTER(u8p), C.POINTER(C.c_size_t),
+                                     u64p, u64p]),
+    "lgs_frac_sum_verify": (C.c_int, [u8p, C.c_size_t, u64p, C.c_size_t, C.POINTER(C.c_uint64),
+                                      u64p, C.c_size_t, u64p, C.POINTER(C.c_int)]),
+    "lgs_lookup_prove": (C.c_int, [vp, u64p, C.c_size_t, u64p, u64p, C.c_size_t, C.c_int, u64p,
+                                   C.c_size_t, C.POINTER(C.c_uint64), C.POINTER(u8p),
+                                   C.POINTER(C.c_size_t), u64p, u64p]),
+    "lgs_lookup_verify": (C.c_int, [u8p, C.c_size_t, u64p, C.c_size_t, C.POINTER(C.c_uint64),
+                                    u64p, C.c_size_t, u64p, C.c_size_t, u64p, C.POINTER(C.c_int)]),
     "lgs_tensor_peak_i8": (C.c_int, [vp, C.c_uint, C.POINTER(C.c_double)]),
     "lgs_dft": (C.c_int, [vp, u64p, C.c_size_t, C.c_size_t, C.c_uint, u64p]),
     "lgs_subset_sum_hash": (C.c_int, [vp, u64p, C.c_size_t, u64p, C.c_size_t, u64p]),

@@ -360,6 +360,62 @@ lgs_status lgs_basefold_prove(lgs_ctx* ctx, const lgs_basefold* b, const uint64_
   });
 }
 
+lgs_status lgs_frac_sum_prove(lgs_ctx* ctx, const uint64_t* p, const uint64_t* q, size_t n,
+                              int on_device, const uint64_t* fields, size_t nfields,
+                              uint64_t* cursor, const uint8_t** proof, size_t* proof_len,
+                              uint64_t* point, uint64_t claim[4]) {
+  return guarded([&] {
+    need(ctx && q && fields && cursor && proof && proof_len && point && claim,
+         "lgs_frac_sum_prove: null argument");
+    CtxDevice dg(ctx);
+    uint64_t cur = *cursor;
+    std::vector<uint8_t>& buf = ctx->proof_buf;
+    frac_sum_prove_dev(ctx, p, q, n, on_device != 0, fields, nfields, &cur, &buf, point, claim);
+    *proof = buf.data();
+    *proof_len = buf.size();
+    *cursor = cur;
+  });
+}
+
+lgs_status lgs_frac_sum_verify(const uint8_t* proof, size_t proof_len, const uint64_t* fields,
+                               size_t nfields, uint64_t* cursor, uint64_t* point,
+                               size_t point_cap, uint64_t claim[4], int* accept) {
+  return guarded([&] {
+    need(proof && fields && cursor && point && claim && accept,
+         "lgs_frac_sum_verify: null argument");
+    *accept = frac_sum_verify_host(proof, proof_len, fields, nfields, cursor, point, point_cap,
+                                   claim);
+  });
+}
+
+lgs_status lgs_lookup_prove(lgs_ctx* ctx, const uint64_t* a, size_t m, const uint64_t* t,
+                            const uint64_t* e, size_t n, int on_device, const uint64_t* fields,
+                            size_t nfields, uint64_t* cursor, const uint8_t** proof,
+                            size_t* proof_len, uint64_t* zq, uint64_t* zt) {
+  return guarded([&] {
+    need(ctx && a && t && e && fields && cursor && proof && proof_len && zq && zt,
+         "lgs_lookup_prove: null argument");
+    CtxDevice dg(ctx);
+    uint64_t cur = *cursor;
+    std::vector<uint8_t>& buf = ctx->proof_buf;
+    lookup_prove_dev(ctx, a, m, t, e, n, on_device != 0, fields, nfields, &cur, &buf, zq, zt);
+    *proof = buf.data();
+    *proof_len = buf.size();
+    *cursor = cur;
+  });
+}
+
+lgs_status lgs_lookup_verify(const uint8_t* proof, size_t proof_len, const uint64_t* fields,
+                             size_t nfields, uint64_t* cursor, uint64_t* zq, size_t zq_cap,
+                             uint64_t* zt, size_t zt_cap, uint64_t vals[6], int* accept) {
+  return guarded([&] {
+    need(proof && fields && cursor && zq && zt && vals && accept,
+         "lgs_lookup_verify: null argument");
+    *accept = lookup_verify_host(proof, proof_len, fields, nfields, cursor, zq, zq_cap, zt,
+                                 zt_cap, vals);
+  });
+}
+
 lgs_status lgs_basefold_verify(const uint8_t root[32], const uint64_t* point, size_t plen,
                                const uint8_t* proof, size_t proof_len, const uint64_t* fields,
                                size_t nfields, const uint64_t* ints, size_t nints,

@@ -131,6 +131,8 @@ bool host_is_pinned(const void* p) {
   return a.type == cudaMemoryTypeHost;
 }
 
+}  // namespace
+
 // Host-to-device copy of a large host array.  Page-locked memory goes straight to the DMA engine;
 // pageable memory goes through the context's ring of pinned chunks (the copy pool fills chunk i
 // while the DMA engine moves chunk i-1).  The caller's array is no longer read when this returns.
@@ -152,6 +154,8 @@ void h2d_staged(lgs_ctx* c, void* dst, const void* src, size_t bytes, cudaStream
     LGS_CUDA(cudaEventRecord(c->ring_ev[slot], st));
   }
 }
+
+namespace {
 
 Hash32 read_root(const u32* nodes, size_t nleaves, cudaStream_t st) {
   Hash32 h;

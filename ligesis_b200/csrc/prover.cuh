@@ -339,6 +339,23 @@ int basefold_verify_host(const Hash32& root, const u64* point, size_t plen, cons
 void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u64* z_host,
                size_t zlen, const u64* fields_host, size_t nfields, const uint64_t* ints_host,
                size_t nints, uint64_t cursors[2], std::vector<uint8_t>* proof_out);
+// Host-to-device copy of a (pageable) host buffer through the context's pinned ring.
+void h2d_staged(lgs_ctx* c, void* dst, const void* src, size_t bytes, cudaStream_t st);
+// GKR fraction sum (logup/src/frac_sum.rs:110-161) and GKR-LogUp lookup
+// (logup/src/lookup.rs:119-143) on the device (frac_sum.cu), proofs encoded "LGSF" / "LGSL"; and
+// their host verifiers (logup_verify.cpp).  Inputs are EF arrays (2 u64 per value) on the host,
+// or on the device when on_device; `cursor` is the oracle's fields cursor.
+void frac_sum_prove_dev(lgs_ctx* c, const u64* p, const u64* q, size_t n, bool on_device,
+                        const u64* fields, size_t nfields, uint64_t* cursor,
+                        std::vector<uint8_t>* proof_out, u64* point_out, u64* claim_out);
+void lookup_prove_dev(lgs_ctx* c, const u64* a, size_t m, const u64* t, const u64* e, size_t n,
+                      bool on_device, const u64* fields, size_t nfields, uint64_t* cursor,
+                      std::vector<uint8_t>* proof_out, u64* zq_out, u64* zt_out);
+int frac_sum_verify_host(const uint8_t* proof, size_t len, const u64* fields, size_t nfields,
+                         uint64_t* cursor, u64* point, size_t point_cap, u64* claim);
+int lookup_verify_host(const uint8_t* proof, size_t len, const u64* fields, size_t nfields,
+                       uint64_t* cursor, u64* zq, size_t zq_cap, u64* zt, size_t zt_cap,
+                       u64* vals);
 lgs_status set_error(lgs_status s, const std::string& msg);
 lgs_status status_of_current_exception();
 }  // namespace lgs
