@@ -677,6 +677,99 @@ def run_basefold(args) -> None:
                                 "proof bytes out", "gpu": out, "cpu_oracle": cpu}), flush=True)
 
 
+def _field_sub(x, a):
+    """x - a mod p elementwise (x a canonical scalar, a canonical uint64 array)."""
+    import numpy as np
+
+    p = np.uint64(0xFFFFFFFF00000001)
+    d = p - a  # in (0, p]
+    s = np.uint64(x) + d
+    s = np.where(s < d, s + np.uint64(0xFFFFFFFF), s)  # wrapped: add 2^64 mod p
+    return np.where(s >= p, s - p, s)
+
+
+def run_logup(args) -> None:
+    """GKR-LogUp lookup (logup/benches/logup.rs:33-79: m = 2^mu queries into an n = 2^nu table,
+    multiplicities precomputed, (mu, nu) in {(20, 14), (22, 16)}): lookup prove from host arrays
+    (copies in the timed call), from device-resident tensors, and the query-side fraction sum
+    alone (the m-sized pass that dominates), each the mean of `--steps` calls after warm-up; host
+    verify; the CPU oracle's lookup prove at (20, 14) beside it."""
+    import numpy as np
+    import torch
+
+    import ligesis_b200 as L
+    from ligesis_b200 import rng
+
+    ctx = L.Context(0)
+    out = {}
+    shapes = ((20, 14), (22, 16)) if args.mu is None else ((args.mu, args.nu),)
+    for mu, nu in shapes:
+        t = rng.ext_elements(70 + nu, 1 << nu)
+        idx = (rng.ints(71 + mu, 1 << mu) % np.uint64(1 << nu)).astype(np.int64)
+        a = t[idx]
+        e = L.multiplicity_vector(a, t)
+        fields = rng.ext_elements(72 + mu, 1024)
+        oracle = L.RandomOracle(0, length=4)
+        oracle.fields = np.ascontiguousarray(fields)
+        dev = [torch.from_numpy(x.view(np.int64)).cuda() for x in (a, t, e)]
+        qq = np.stack([_field_sub(fields[0][c], a[:, c]) for c in (0, 1)], 1)
+        qq_dev = torch.from_numpy(np.ascontiguousarray(qq).view(np.int64)).cuda()
+        torch.cuda.synchronize()
+
+        def host_call():
+            oracle.restart()
+            return L.Lookup.prove_with_mults(a, t, e, oracle, ctx)
+
+        def dev_call():
+            oracle.restart()
+            return L.Lookup.prove_with_mults(*dev, oracle, ctx)
+
+        def query_call():
+            oracle.restart()
+            return L.FracSum.prove(None, qq_dev, oracle, ctx)
+
+        res = {}
+        for name, fn in (("prove_host_inputs_ms", host_call), ("prove_device_inputs_ms", dev_call),
+                         ("query_frac_sum_device_ms", query_call)):
+            for _ in range(args.warmup):
+                r = fn()
+            gc.collect()
+            gc.disable()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                r = fn()
+            t1 = time.perf_counter()
+            gc.enable()
+            res[name] = round((t1 - t0) / args.steps * 1e3, 3)
+        proof = host_call()
+        oracle.restart()
+        t0 = time.perf_counter()
+        claims = L.Lookup.verify(proof, oracle)
+        res["verify_ms"] = round((time.perf_counter() - t0) * 1e3, 3)
+        assert claims is not None, "lookup proof rejected"
+        res["proof_bytes"] = proof.size_bytes()
+        res["h2d_bytes"] = int(a.nbytes + t.nbytes + e.nbytes)
+        out[f"mu{mu}_nu{nu}"] = res
+        del dev, qq_dev
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import orc
+
+        mu, nu = 20, 14
+        t = rng.ext_elements(70 + nu, 1 << nu)
+        idx = (rng.ints(71 + mu, 1 << mu) % np.uint64(1 << nu)).astype(np.int64)
+        a = t[idx]
+        e = L.multiplicity_vector(a, t)
+        fields = rng.ext_elements(72 + mu, 1024)
+        t0 = time.perf_counter()
+        orc.lookup_prove(a, t, e, fields)
+        cpu = {"mu": mu, "nu": nu, "prove_ms": round((time.perf_counter() - t0) * 1e3, 1),
+               "cores": 1, "kind": "port", "cpu": _cpu_model()}
+    print(json.dumps({"mode": "logup", "steps": args.steps,
+                      "timing": "host wall clock per call, proof bytes out", "gpu": out,
+                      "cpu_oracle": cpu}), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -684,11 +777,13 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", choices=["line", "batch", "serve", "commit", "timeline", "basefold"],
-                    default="line")
+    ap.add_argument("--mode", choices=["line", "batch", "serve", "commit", "timeline", "basefold",
+                                       "logup"], default="line")
     ap.add_argument("--log-m", type=int, default=LOG_M)
     ap.add_argument("--log-n", type=int, default=LOG_N)
     ap.add_argument("--lanes", type=int, default=12)
+    ap.add_argument("--mu", type=int, default=None, help="logup mode: one shape, 2^mu queries")
+    ap.add_argument("--nu", type=int, default=16, help="logup mode: 2^nu table entries")
     ap.add_argument("--requests", type=int, default=600)
     ap.add_argument("--rate", type=float, default=200.0)
     args = ap.parse_args()
@@ -708,6 +803,9 @@ def main() -> None:
         return
     if args.mode == "basefold":
         run_basefold(args)
+        return
+    if args.mode == "logup":
+        run_logup(args)
         return
     if args.impl == "reference":
         run_reference(args)

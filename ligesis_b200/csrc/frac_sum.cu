@@ -20,10 +20,12 @@
 //    A1 (folding is affine), so the stored arrays are A0, U, B0, B1: 6 products for H at 0, 1 and
 //    its leading coefficient, 3 for the weights, 4 for the folds.  With all numerators one (the
 //    query side of a lookup) A0 stays 1 and that drops to 3 + 3 + 3.
-// A pass folds FS_B rounds: each CTA takes 2^FS_B consecutive elements of the four arrays, the
-// first round straight from the level (or the previous pass's output), the rest in shared memory,
-// and leaves one element per array; per-CTA sums of every round go to a scratch array that
-// fs_rounds_kernel reduces into the round polynomials.  Round polynomials hold the same field
+// While a layer's arrays hold more than 2^FS_TAIL_LOG values, wide passes fold them two rounds at a
+// time, four values per thread with no block barrier: a pair's weight is lo[j mod 2^10] from a
+// small table of the round, and the factor hi[j >> 10], common to a warp, multiplies the warp's
+// sums, which go to a scratch array.  All layers share each wide launch.  The last rounds of
+// every layer then run in one CTA per layer (fs_tail_kernel) in shared memory, and
+// fs_rounds_kernel reduces the sums into the round polynomials.  Round polynomials hold the same field
 // values as the reference's (the identities are exact), so the proofs are byte-identical.
 #include <algorithm>
 #include <array>
@@ -36,7 +38,6 @@ namespace lgs {
 namespace {
 
 constexpr unsigned FS_THREADS = 256;
-constexpr unsigned FS_B = 10;        // rounds per sumcheck pass (2^FS_B elements per CTA)
 constexpr unsigned FS_BUILD_T = 10;  // tree levels per build launch
 constexpr unsigned FS_MAX_K = 28;
 
@@ -118,21 +119,49 @@ __global__ void __launch_bounds__(FS_THREADS)
 
 }  // namespace
 
-// One pass of one layer: rounds t0 .. t0+nb-1 of the layer-r sumcheck.
-struct FsJob {
-  FsSrc src;          // the first pass reads level r+1 (entries 2i, 2i+1 are element i)
-  const ef2* fin;     // later passes: the previous pass's arrays A0 | U | B0 | B1 (n each)
-  ef2* fout;          // this pass's arrays (ncta each); on the layer's last pass, the leaves
-  ef2* part;          // per-round, per-CTA sums: [tau][cta][S(0), S(1), leading coefficient]
-  const ef2* z;       // the layer's point z_r (r coordinates)
-  const ef2* ch;      // the layer's fold challenges (r)
+// The four arrays of a layer's sumcheck between kernels: A0 | U | B0 | B1, n values each (A0 is
+// neither written nor read when the numerators are all one: it stays 1).
+struct FsArrays {
+  FsSrc src;       // before the first fold: level r+1, entries 2i, 2i+1 are element i
+  const ef2* fin;  // after: the arrays (null while reading the level)
+  size_t n;
   ef2 lambda;
-  size_t n;           // elements per array at round t0 (2^(r - t0))
-  unsigned r, t0, nb, ncta, first_cta;
-  int ones;           // A0 == 1 throughout (numerators all one)
+  int ones;
 };
 
-// Reduction of one round: the CTA sums of the pass that ran it, times K_t(0..3).
+// Rounds t (and t+1) of one layer over its whole arrays, two (or one) folds per thread.  Round t's
+// pair j has weight E_{t+1}(j) = lo[j mod 2^10] hi[j >> 10]; hi is the same for a CTA's pairs, so
+// it multiplies the CTA's sums.
+struct FsWide {
+  FsArrays in;
+  ef2* fout;           // the folded arrays, (n >> rounds) values each
+  ef2* part;           // [round][cta][S(0), S(1), leading coefficient]
+  const ef2* lo[2];
+  const ef2* hi[2];
+  ef2 c[2];
+  unsigned rounds, first_cta;
+};
+
+// The eq tables of one wide round: lo[i] = prod_{b<10} eq(z_{t+1+b}, bit b of i) (1024 entries)
+// and hi[i] = prod_b eq(z_{t+11+b}, bit b of i) (2^(r-t-11) entries).
+struct FsTable {
+  const ef2* z;  // the layer's point
+  ef2* lo;
+  ef2* hi;
+  unsigned t, r;
+};
+
+// The last rounds t0 .. r-1 of one layer in one CTA (at most 2^FS_TAIL_LOG values per array).
+struct FsTail {
+  FsArrays in;
+  ef2* leaves;  // A0, U, B0, B1 after the last fold
+  ef2* part;    // [round][S(0), S(1), leading coefficient]
+  const ef2* z;
+  const ef2* ch;
+  unsigned r, t0;
+};
+
+// Reduction of one round: the partial sums of the kernel that ran it, times K_t(0..3).
 struct FsRound {
   const ef2* part;  // ncta x 3
   ef2* out;         // g(0), g(1), g(2), g(3)
@@ -141,6 +170,9 @@ struct FsRound {
 };
 
 namespace {
+
+constexpr unsigned FS_TAIL_LOG = 11;
+constexpr unsigned FS_EQ_LO = 10;
 
 struct Q4 {
   ef2 a0, u, b0, b1;
@@ -174,25 +206,31 @@ __device__ __forceinline__ Q4 fs_pair(const Q4& lo, const Q4& hi, ef2 w, ef2 c, 
   return o;
 }
 
-__device__ __forceinline__ Q4 job_load(const FsJob& jb, size_t e) {
+__device__ __forceinline__ Q4 arr_load(const FsArrays& a, size_t e) {
   Q4 x;
-  if (jb.fin) {
-    x.a0 = ld_ef(jb.fin + e);
-    x.u = ld_ef(jb.fin + jb.n + e);
-    x.b0 = ld_ef(jb.fin + 2 * jb.n + e);
-    x.b1 = ld_ef(jb.fin + 3 * jb.n + e);
+  if (a.fin) {
+    x.a0 = a.ones ? ef_one() : ld_ef(a.fin + e);
+    x.u = ld_ef(a.fin + a.n + e);
+    x.b0 = ld_ef(a.fin + 2 * a.n + e);
+    x.b1 = ld_ef(a.fin + 3 * a.n + e);
   } else {
-    x.b0 = src_q(jb.src, 2 * e);
-    x.b1 = src_q(jb.src, 2 * e + 1);
-    if (jb.ones) {
+    x.b0 = src_q(a.src, 2 * e);
+    x.b1 = src_q(a.src, 2 * e + 1);
+    if (a.ones) {
       x.a0 = ef_one();
-      x.u = ef_add(ef_one(), ef_mul(jb.lambda, x.b1));
+      x.u = ef_add(ef_one(), ef_mul(a.lambda, x.b1));
     } else {
-      x.a0 = src_p(jb.src, 2 * e);
-      x.u = ef_add(src_p(jb.src, 2 * e + 1), ef_mul(jb.lambda, x.b1));
+      x.a0 = src_p(a.src, 2 * e);
+      x.u = ef_add(src_p(a.src, 2 * e + 1), ef_mul(a.lambda, x.b1));
     }
   }
   return x;
+}
+__device__ __forceinline__ void arr_store(ef2* out, size_t n, size_t e, const Q4& x, bool ones) {
+  if (!ones) st_ef(out + e, x.a0);
+  st_ef(out + n + e, x.u);
+  st_ef(out + 2 * n + e, x.b0);
+  st_ef(out + 3 * n + e, x.b1);
 }
 
 __device__ __forceinline__ void warp_sum3(ef2 (&s)[3]) {
@@ -202,57 +240,127 @@ __device__ __forceinline__ void warp_sum3(ef2 (&s)[3]) {
     for (int m = 16; m; m >>= 1) s[q] = ef_add(s[q], shfl_xor_ef(s[q], m));
 }
 
-// Sum s over the CTA and store it at dst (3 EF).  Every thread must call it.
-__device__ void block_store3(ef2 (&s)[3], ef2* red, ef2* dst) {
-  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  warp_sum3(s);
-  if (lane == 0)
+__global__ void __launch_bounds__(FS_THREADS)
+    fs_tables_kernel(const FsTable* __restrict__ tabs) {
+  __shared__ ef2 zs[64];
+  __shared__ ef2 lo[1u << FS_EQ_LO];
+  const FsTable& tb = tabs[blockIdx.x];
+  const unsigned t = tb.t, r = tb.r;
+  for (unsigned i = threadIdx.x; i < r; i += blockDim.x) zs[i] = ld_ef(tb.z + i);
+  // lo by doubling from the high bit down: after step b, lo[i] (i < 2^(b+1)) is the product over
+  // coordinates t+nlo-1-b .. t+nlo of bit order low -> high
+  const unsigned nlo = r - t - 1 < FS_EQ_LO ? r - t - 1 : FS_EQ_LO;
+  if (threadIdx.x == 0) lo[0] = ef_one();
+  for (unsigned b = 0; b < nlo; ++b) {
+    __syncthreads();
+    const unsigned sz = 1u << b;
+    const ef2 z = zs[t + nlo - b], nz = ef_sub(ef_one(), z);  // the new lowest coordinate
+    // lo'[2m + bit] = lo[m] eq(z, bit): read all, then write (in place, top down)
+    ef2 v[2][2];  // sz <= 2^(FS_EQ_LO-1) = 2 x FS_THREADS entries
 #pragma unroll
-    for (int q = 0; q < 3; ++q) red[q * 32 + warp] = s[q];
-  __syncthreads();
-  if (warp == 0) {
-    ef2 v[3];
+    for (unsigned q = 0; q < 2; ++q) {
+      const unsigned m = threadIdx.x + q * FS_THREADS;
+      if (m < sz) {
+        const ef2 w = lo[m];
+        v[q][0] = ef_mul(w, nz);
+        v[q][1] = ef_mul(w, z);
+      }
+    }
+    __syncthreads();
 #pragma unroll
-    for (int q = 0; q < 3; ++q) v[q] = lane < nw ? red[q * 32 + lane] : ef_zero();
-    warp_sum3(v);
-    if (lane == 0)
-#pragma unroll
-      for (int q = 0; q < 3; ++q) st_ef(dst + q, v[q]);
+    for (unsigned q = 0; q < 2; ++q) {
+      const unsigned m = threadIdx.x + q * FS_THREADS;
+      if (m < sz) {
+        lo[2 * m] = v[q][0];
+        lo[2 * m + 1] = v[q][1];
+      }
+    }
   }
   __syncthreads();
+  for (unsigned i = threadIdx.x; i < (1u << nlo); i += blockDim.x) st_ef(tb.lo + i, lo[i]);
+  const unsigned nhi = r - t - 1 - nlo;
+  for (size_t i = threadIdx.x; i < ((size_t)1 << nhi); i += blockDim.x) {
+    ef2 w = ef_one();
+    for (unsigned b = 0; b < nhi; ++b) {
+      const ef2 z = zs[t + 1 + FS_EQ_LO + b];
+      w = ef_mul(w, ((i >> b) & 1) ? z : ef_sub(ef_one(), z));
+    }
+    st_ef(tb.hi + i, w);
+  }
 }
 
-// Shared memory of a pass: the weight tables (2^FS_B entries), the folded elements after the
-// first round (2^(FS_B-1) x 4) and the reduction scratch (3 x 32).
-constexpr size_t FS_PASS_SMEM =
-    ((size_t)1 << FS_B) * sizeof(ef2) + ((size_t)1 << (FS_B - 1)) * sizeof(Q4) + 96 * sizeof(ef2);
-
 __global__ void __launch_bounds__(FS_THREADS)
-    fs_pass_kernel(const FsJob* __restrict__ jobs, unsigned njobs) {
-  extern __shared__ ef2 fs_sm[];
-  ef2* wt = fs_sm;                                     // W_tau at offset 2^(nb - tau - 1) - 1
-  Q4* xs = reinterpret_cast<Q4*>(fs_sm + (1u << FS_B));
-  ef2* red = fs_sm + (1u << FS_B) + 4 * (1u << (FS_B - 1));
+    fs_wide_kernel(const FsWide* __restrict__ jobs, unsigned njobs) {
   unsigned ji = 0;
   while (ji + 1 < njobs && blockIdx.x >= jobs[ji + 1].first_cta) ++ji;
-  const FsJob& jb = jobs[ji];
-  const unsigned cta = blockIdx.x - jb.first_cta, nb = jb.nb, t0 = jb.t0, r = jb.r;
-  const bool ones = jb.ones != 0;
-
-  // W_{nb-1} = [prod over k in [t0+nb, r) of eq(z_k, bit k-t0-nb of cta)]; then
-  // W_tau[2m + b] = W_{tau+1}[m] eq(z_{t0+tau+1}, b): the weight of local pair jl in round
-  // t0+tau is W_tau[jl] = E_{t+1}(cta 2^(nb-tau-1) + jl).
-  if (threadIdx.x < 32) {
-    ef2 f = ef_one();
-    const unsigned k = t0 + nb + threadIdx.x;
-    if (k < r) {
-      const ef2 zk = ld_ef(jb.z + k);
-      f = ((cta >> threadIdx.x) & 1) ? zk : ef_sub(ef_one(), zk);
-    }
-#pragma unroll
-    for (int m = 16; m; m >>= 1) f = ef_mul(f, shfl_xor_ef(f, m));
-    if (threadIdx.x == 0) wt[0] = f;
+  const FsWide& jb = jobs[ji];
+  const bool ones = jb.in.ones != 0;
+  const size_t g = (size_t)(blockIdx.x - jb.first_cta) * blockDim.x + threadIdx.x;
+  const size_t nthr = jb.in.n >> jb.rounds;
+  ef2 s0[3] = {ef_zero(), ef_zero(), ef_zero()};
+  ef2 s1[3] = {ef_zero(), ef_zero(), ef_zero()};
+  Q4 y;
+  if (jb.rounds == 2) {
+    const size_t e = g << 2;
+    const Q4 x0 = arr_load(jb.in, e), x1 = arr_load(jb.in, e + 1);
+    const Q4 x2 = arr_load(jb.in, e + 2), x3 = arr_load(jb.in, e + 3);
+    const unsigned j0 = (unsigned)(2 * g) & ((1u << FS_EQ_LO) - 1);
+    const Q4 f0 = fs_pair(x0, x1, ld_ef(jb.lo[0] + j0), jb.c[0], ones, s0);
+    const Q4 f1 = fs_pair(x2, x3, ld_ef(jb.lo[0] + j0 + 1), jb.c[0], ones, s0);
+    y = fs_pair(f0, f1, ld_ef(jb.lo[1] + (g & ((1u << FS_EQ_LO) - 1))), jb.c[1], ones, s1);
+  } else {
+    const size_t e = g << 1;
+    const Q4 x0 = arr_load(jb.in, e), x1 = arr_load(jb.in, e + 1);
+    y = fs_pair(x0, x1, ld_ef(jb.lo[0] + (g & ((1u << FS_EQ_LO) - 1))), jb.c[0], ones, s0);
   }
+  arr_store(jb.fout, nthr, g, y, ones);
+  // CTA sums of each round; round t's factor hi[j >> 10] is common to the CTA (256 threads cover
+  // 512 or 256 consecutive pairs of an aligned block of 1024)
+  __shared__ ef2 red[2][3][8];
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  warp_sum3(s0);
+  if (jb.rounds == 2) warp_sum3(s1);
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      red[0][q][warp] = s0[q];
+      red[1][q][warp] = s1[q];
+    }
+  __syncthreads();
+  const size_t cta = blockIdx.x - jb.first_cta, ncta = nthr / FS_THREADS;
+  if (threadIdx.x < 3 * jb.rounds) {
+    const unsigned rd = threadIdx.x / 3, q = threadIdx.x % 3;
+    ef2 v = ef_zero();
+#pragma unroll
+    for (int w = 0; w < 8; ++w) v = ef_add(v, red[rd][q][w]);
+    const size_t g0 = cta * FS_THREADS;  // first thread of the CTA
+    const size_t hj = rd == 0 ? (jb.rounds == 2 ? (g0 >> (FS_EQ_LO - 1)) : (g0 >> FS_EQ_LO))
+                              : (g0 >> FS_EQ_LO);
+    const ef2 h = ld_ef(jb.hi[rd] + hj);
+    st_ef(jb.part + (rd * ncta + cta) * 3 + q, ef_mul(h, v));
+  }
+}
+
+// Shared memory of a tail: weight tables (2^FS_TAIL_LOG entries), the folded elements after the
+// first round (2^(FS_TAIL_LOG-1)), per-warp round sums (FS_TAIL_LOG x 16 warps x 3).
+constexpr size_t FS_TAIL_SMEM = ((size_t)1 << FS_TAIL_LOG) * sizeof(ef2) +
+                                ((size_t)1 << (FS_TAIL_LOG - 1)) * sizeof(Q4) +
+                                (size_t)FS_TAIL_LOG * 16 * 3 * sizeof(ef2);
+constexpr unsigned FS_TAIL_THREADS = 512;  // latency-bound: as many warps as the registers allow
+
+__global__ void __launch_bounds__(FS_TAIL_THREADS) fs_tail_kernel(const FsTail* __restrict__ jobs) {
+  extern __shared__ ef2 fs_sm[];
+  ef2* wt = fs_sm;  // W_tau at offset 2^(nb - tau - 1) - 1
+  Q4* xs = reinterpret_cast<Q4*>(fs_sm + (1u << FS_TAIL_LOG));
+  ef2* acc = fs_sm + (1u << FS_TAIL_LOG) + 4 * (1u << (FS_TAIL_LOG - 1));  // [tau][warp][3]
+  const FsTail& jb = jobs[blockIdx.x];
+  const unsigned t0 = jb.t0, nb = jb.r - t0;
+  const bool ones = jb.in.ones != 0;
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+
+  // W_{nb-1} = [1]; W_tau[2m + b] = W_{tau+1}[m] eq(z_{t0+tau+1}, b): the weight of pair jl in
+  // round t0+tau is E_{t0+tau+1}(jl).
+  if (threadIdx.x == 0) wt[0] = ef_one();
   for (int tau = (int)nb - 2; tau >= 0; --tau) {
     __syncthreads();
     const unsigned sz = 1u << (nb - tau - 1), prev = (sz >> 1) - 1, off = sz - 1;
@@ -262,37 +370,71 @@ __global__ void __launch_bounds__(FS_THREADS)
   }
   __syncthreads();
 
-  // round t0: straight from global memory
-  {
+  auto warp_acc = [&](ef2 (&s)[3], unsigned tau) {  // per-warp sums, no block barrier
+    warp_sum3(s);
+    if (lane == 0)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) acc[(tau * nw + warp) * 3 + q] = s[q];
+  };
+  {  // round t0 from global memory
     const unsigned np = 1u << (nb - 1);
     const ef2 c = ld_ef(jb.ch + t0);
     ef2 s[3] = {ef_zero(), ef_zero(), ef_zero()};
     for (unsigned jl = threadIdx.x; jl < np; jl += blockDim.x) {
-      const size_t e = ((size_t)cta << nb) + 2 * jl;
-      const Q4 lo = job_load(jb, e), hi = job_load(jb, e + 1);
+      const Q4 lo = arr_load(jb.in, 2 * jl), hi = arr_load(jb.in, 2 * jl + 1);
       xs[jl] = fs_pair(lo, hi, wt[np - 1 + jl], c, ones, s);
     }
-    block_store3(s, red, jb.part + (size_t)cta * 3);
+    warp_acc(s, 0);
   }
-  // rounds t0+1 .. t0+nb-1 in shared memory (at most 2^(FS_B-2) = blockDim pairs)
-  for (unsigned tau = 1; tau < nb; ++tau) {
+  // rounds with more pairs than one warp: exchange through shared memory with barriers
+  unsigned tau = 1;
+  for (; tau < nb && (1u << (nb - tau - 1)) > 32; ++tau) {
     const unsigned np = 1u << (nb - tau - 1);
     const ef2 c = ld_ef(jb.ch + t0 + tau);
     ef2 s[3] = {ef_zero(), ef_zero(), ef_zero()};
-    Q4 o;
-    const bool act = threadIdx.x < np;
-    if (act) o = fs_pair(xs[2 * threadIdx.x], xs[2 * threadIdx.x + 1], wt[np - 1 + threadIdx.x], c,
-                         ones, s);
+    Q4 o[2];
     __syncthreads();
-    if (act) xs[threadIdx.x] = o;
-    block_store3(s, red, jb.part + ((size_t)tau * jb.ncta + cta) * 3);
+#pragma unroll
+    for (unsigned q = 0; q < 2; ++q) {
+      const unsigned jl = threadIdx.x + q * blockDim.x;
+      if (jl < np) o[q] = fs_pair(xs[2 * jl], xs[2 * jl + 1], wt[np - 1 + jl], c, ones, s);
+    }
+    __syncthreads();
+#pragma unroll
+    for (unsigned q = 0; q < 2; ++q) {
+      const unsigned jl = threadIdx.x + q * blockDim.x;
+      if (jl < np) xs[jl] = o[q];
+    }
+    warp_acc(s, tau);
+  }
+  __syncthreads();
+  // the rest in warp 0 (the other warps' sums of these rounds are zero)
+  for (; tau < nb; ++tau) {
+    const unsigned np = 1u << (nb - tau - 1);
+    ef2 s[3] = {ef_zero(), ef_zero(), ef_zero()};
+    if (warp == 0) {
+      const ef2 c = ld_ef(jb.ch + t0 + tau);
+      Q4 o;
+      if (lane < np) o = fs_pair(xs[2 * lane], xs[2 * lane + 1], wt[np - 1 + lane], c, ones, s);
+      __syncwarp();
+      if (lane < np) xs[lane] = o;
+      __syncwarp();
+    }
+    warp_acc(s, tau);
+  }
+  __syncthreads();
+  for (unsigned i = threadIdx.x; i < nb * 3; i += blockDim.x) {
+    const unsigned tt = i / 3, q = i % 3;
+    ef2 v = ef_zero();
+    for (unsigned w = 0; w < nw; ++w) v = ef_add(v, acc[(tt * nw + w) * 3 + q]);
+    st_ef(jb.part + i, v);
   }
   if (threadIdx.x == 0) {
     const Q4 x = xs[0];
-    st_ef(jb.fout + cta, x.a0);
-    st_ef(jb.fout + jb.ncta + cta, x.u);
-    st_ef(jb.fout + 2 * jb.ncta + cta, x.b0);
-    st_ef(jb.fout + 3 * jb.ncta + cta, x.b1);
+    st_ef(jb.leaves + 0, x.a0);
+    st_ef(jb.leaves + 1, x.u);
+    st_ef(jb.leaves + 2, x.b0);
+    st_ef(jb.leaves + 3, x.b1);
   }
 }
 
@@ -353,7 +495,8 @@ size_t ceil256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 }  // namespace
 
-// The device plan of one fraction-sum proof: what fs_enqueue launched, what the host reads back.
+// The device plan of one fraction-sum proof: its challenges, device buffers, the parameter blob
+// its kernels read, and where its values land in the staging area.
 struct FsPlan {
   unsigned k = 0;
   uint64_t f0 = 0;              // fields cursor at the start
@@ -362,23 +505,38 @@ struct FsPlan {
   size_t stage_off = 0;         // EF offset of this proof's values in the staging area
   size_t round_off = 0;         // EF offset of the round polynomials (within the staging)
   size_t stage_elems = 0;
+  FsSrc in{};
+  ef2* stage = nullptr;
+  ef2* P = nullptr;
+  ef2* Q = nullptr;
+  uint8_t* d_up = nullptr;
+  std::vector<uint8_t> blob;    // z / challenges, tables, wide jobs (launch by launch), tails,
+                                // rounds
+  size_t up_tables = 0, up_wide = 0, up_tails = 0, up_rounds = 0, nrounds = 0;
+  unsigned ntables = 0, ntails = 0;
+  std::vector<unsigned> pass_jobs, pass_ctas;
 };
 
 static size_t fs_fields_needed(unsigned k) { return (size_t)k * (k + 3) / 2; }
 
-// Enqueues one fraction-sum proof of 2^k inputs on st.  Its values land in `stage` (device) at
-// plan->stage_off: num, den, level-1 entries (6 EF), then per layer r >= 1 the leaves
-// (A0, U, B0, B1), then the round polynomials layer by layer.
-static void fs_enqueue(lgs_ctx* c, const FsSrc& in, unsigned k, const u64* fields, size_t nfields,
-                       uint64_t f0, ef2* stage, size_t stage_off, FsPlan* plan, cudaStream_t st) {
+// Plans one fraction-sum proof of 2^k inputs: challenges, device buffers (from the arena) and the
+// parameter blob.  Its values land in `stage` (device) at stage_off: num, den, level-1 entries
+// (6 EF), then per layer r >= 1 the leaves (A0, U, B0, B1), then the round polynomials layer by
+// layer.
+static void fs_plan(lgs_ctx* c, const FsSrc& in, unsigned k, const u64* fields, size_t nfields,
+                    uint64_t f0, ef2* stage, size_t stage_off, FsPlan* plan) {
   Arena& ar = c->arena;
   if (k > FS_MAX_K) throw ShapeError("frac_sum: at most 2^28 fractions");
   const size_t need = fs_fields_needed(k);
   if (f0 > nfields || nfields - f0 < need) throw OracleError("oracle exhausted (fields)");
   plan->k = k;
   plan->f0 = f0;
+  plan->in = in;
+  plan->stage = stage;
   plan->stage_off = stage_off;
-  auto F = [&](size_t i) { return ef_make(gl_canon(fields[2 * (f0 + i)]), gl_canon(fields[2 * (f0 + i) + 1])); };
+  auto F = [&](size_t i) {
+    return ef_make(gl_canon(fields[2 * (f0 + i)]), gl_canon(fields[2 * (f0 + i) + 1]));
+  };
   plan->lambda.assign(k, ef_zero());
   plan->beta.assign(k, ef_zero());
   plan->z.assign(k, {});
@@ -395,39 +553,22 @@ static void fs_enqueue(lgs_ctx* c, const FsSrc& in, unsigned k, const u64* field
   }
   size_t nrounds = 0;
   for (unsigned r = 1; r < k; ++r) nrounds += r;
+  plan->nrounds = nrounds;
   plan->round_off = stage_off + 6 + 4 * (k ? k - 1 : 0);
-  plan->stage_elems = 6 + 4 * (k ? k - 1 : 0) + 4 * nrounds;
-  if (k == 0) {
-    fs_single_kernel<<<1, 32, 0, st>>>(in, stage + stage_off);
-    LGS_LAUNCH_CHECK();
-    plan->stage_elems = 2;
-    return;
-  }
+  plan->stage_elems = k ? 6 + 4 * (k - 1) + 4 * nrounds : 2;
+  if (k == 0) return;
 
-  // ---- levels ---------------------------------------------------------------------------
   const size_t nlev = ((size_t)1 << k) - 1;  // levels 0 .. k-1
-  ef2* P = ar.get<ef2>(nlev);
-  ef2* Q = ar.get<ef2>(nlev);
-  {
-    unsigned S = k;
-    FsSrc src = in;
-    while (S > 0) {
-      const unsigned T = std::min(S, FS_BUILD_T);
-      const size_t smem = 2 * ((size_t)1 << T) * sizeof(ef2);
-      fs_build_kernel<<<(unsigned)((size_t)1 << (S - T)), FS_THREADS, smem, st>>>(src, S, T, P, Q);
-      LGS_LAUNCH_CHECK();
-      S -= T;
-      src = FsSrc{P + ((size_t)1 << S) - 1, Q + ((size_t)1 << S) - 1, ef_zero(), 0};
-    }
-  }
+  ef2* P = plan->P = ar.get<ef2>(nlev);
+  ef2* Q = plan->Q = ar.get<ef2>(nlev);
   auto level = [&](unsigned s) -> FsSrc {
     if (s == k) return in;
     return FsSrc{P + ((size_t)1 << s) - 1, Q + ((size_t)1 << s) - 1, ef_zero(), 0};
   };
 
-  // ---- parameter blob: per layer z and challenges; jobs per pass; rounds ------------------
-  const unsigned npass = k > 1 ? (k - 2) / FS_B + 1 : 0;  // layer k-1 has k-1 rounds
-  std::vector<std::vector<FsJob>> jobs(npass);
+  std::vector<std::vector<FsWide>> wide;  // per wide launch
+  std::vector<FsTable> tables;
+  std::vector<FsTail> tails;
   std::vector<FsRound> rounds;
   std::vector<ef2> zc;  // z_r then ch_r for every layer r >= 1
   std::vector<size_t> zoff(k, 0);
@@ -436,15 +577,27 @@ static void fs_enqueue(lgs_ctx* c, const FsSrc& in, unsigned k, const u64* field
     zc.insert(zc.end(), plan->z[r].begin(), plan->z[r].end());
     zc.insert(zc.end(), plan->ch[r].begin(), plan->ch[r].end());
   }
+  // device pointers into the blob are fixed once its layout is: count the records first
+  size_t n_wide = 0, n_tab = 0;
+  for (unsigned r = 1; r < k; ++r)
+    for (size_t n = (size_t)1 << r; n > ((size_t)1 << FS_TAIL_LOG);) {
+      const unsigned rr = n >= ((size_t)4 << FS_TAIL_LOG) ? 2 : 1;
+      ++n_wide;
+      n_tab += rr;
+      n >>= rr;
+    }
   size_t up_bytes = ceil256(zc.size() * sizeof(ef2));
-  const size_t up_jobs = up_bytes;
-  size_t total_jobs = 0;
-  for (unsigned r = 1; r < k; ++r) total_jobs += (r - 1) / FS_B + 1;
-  up_bytes += ceil256(total_jobs * sizeof(FsJob));
-  const size_t up_rounds = up_bytes;
+  plan->up_tables = up_bytes;
+  up_bytes += ceil256(n_tab * sizeof(FsTable));
+  plan->up_wide = up_bytes;
+  up_bytes += ceil256(n_wide * sizeof(FsWide));
+  plan->up_tails = up_bytes;
+  up_bytes += ceil256((k - 1) * sizeof(FsTail));
+  plan->up_rounds = up_bytes;
   up_bytes += ceil256(nrounds * sizeof(FsRound));
-  uint8_t* d_up = ar.get<uint8_t>(up_bytes);
-  std::vector<uint8_t> h_up(up_bytes, 0);
+  uint8_t* d_up = plan->d_up = ar.get<uint8_t>(up_bytes);
+  std::vector<uint8_t>& h_up = plan->blob;
+  h_up.assign(up_bytes, 0);
   std::memcpy(h_up.data(), zc.data(), zc.size() * sizeof(ef2));
   const ef2* d_zc = (const ef2*)d_up;
 
@@ -465,76 +618,128 @@ static void fs_enqueue(lgs_ctx* c, const FsSrc& in, unsigned k, const u64* field
       }
       C = ef_mul(C, h_eq1(zt, plan->ch[r][t]));
     }
-    const ef2* fin = nullptr;
-    for (unsigned t0 = 0, pi = 0; t0 < r; t0 += FS_B, ++pi) {
-      const unsigned nb = std::min(FS_B, r - t0);
-      FsJob jb{};
-      jb.src = level(r + 1);
-      jb.fin = fin;
-      jb.n = (size_t)1 << (r - t0);
-      jb.ncta = 1u << (r - t0 - nb);
-      jb.fout = t0 + nb == r ? stage + stage_off + 6 + 4 * (r - 1) : ar.get<ef2>(4 * (size_t)jb.ncta);
-      jb.part = ar.get<ef2>((size_t)nb * jb.ncta * 3);
-      jb.z = z;
-      jb.ch = chp;
-      jb.lambda = plan->lambda[r];
-      jb.r = r;
-      jb.t0 = t0;
-      jb.nb = nb;
-      jb.ones = (r + 1 == k && in.p == nullptr) ? 1 : 0;
-      jobs[pi].push_back(jb);
-      for (unsigned tau = 0; tau < nb; ++tau) {
-        FsRound rd{};
-        rd.part = jb.part + (size_t)tau * jb.ncta * 3;
-        rd.out = stage + round_pos + 4 * (t0 + tau);
-        for (int x = 0; x < 4; ++x) rd.K[x] = K[t0 + tau][x];
-        rd.ncta = jb.ncta;
-        rounds.push_back(rd);
+    auto add_round = [&](unsigned t, const ef2* part, unsigned nparts) {
+      FsRound rd{};
+      rd.part = part;
+      rd.out = stage + round_pos + 4 * t;
+      for (int x = 0; x < 4; ++x) rd.K[x] = K[t][x];
+      rd.ncta = nparts;
+      rounds.push_back(rd);
+    };
+    FsArrays cur{level(r + 1), nullptr, (size_t)1 << r, plan->lambda[r],
+                 (r + 1 == k && in.p == nullptr) ? 1 : 0};
+    unsigned t = 0, pass = 0;
+    while (cur.n > ((size_t)1 << FS_TAIL_LOG)) {
+      FsWide w{};
+      w.in = cur;
+      w.rounds = cur.n >= ((size_t)4 << FS_TAIL_LOG) ? 2 : 1;
+      const size_t nout = cur.n >> w.rounds, nctas = nout / FS_THREADS;
+      w.fout = ar.get<ef2>(4 * nout);
+      w.part = ar.get<ef2>(w.rounds * nctas * 3);
+      for (unsigned q = 0; q < w.rounds; ++q) {
+        FsTable tb{};
+        tb.z = z;
+        tb.t = t + q;
+        tb.r = r;
+        tb.lo = ar.get<ef2>((size_t)1 << FS_EQ_LO);
+        tb.hi = ar.get<ef2>((size_t)1 << (r - (t + q) - 1 - FS_EQ_LO));
+        tables.push_back(tb);
+        w.lo[q] = tb.lo;
+        w.hi[q] = tb.hi;
+        w.c[q] = plan->ch[r][t + q];
+        add_round(t + q, w.part + q * nctas * 3, (unsigned)nctas);
       }
-      fin = jb.fout;
+      if (wide.size() <= pass) wide.resize(pass + 1);
+      wide[pass].push_back(w);
+      cur.fin = w.fout;
+      cur.n = nout;
+      t += w.rounds;
+      ++pass;
     }
+    FsTail tl{};
+    tl.in = cur;
+    tl.leaves = stage + stage_off + 6 + 4 * (r - 1);
+    tl.part = ar.get<ef2>((size_t)(r - t) * 3);
+    tl.z = z;
+    tl.ch = chp;
+    tl.r = r;
+    tl.t0 = t;
+    tails.push_back(tl);
+    for (unsigned q = t; q < r; ++q) add_round(q, tl.part + (size_t)(q - t) * 3, 1);
     round_pos += 4 * (size_t)r;
   }
-  {
-    size_t o = up_jobs;
-    for (auto& pj : jobs) {
-      unsigned first = 0;
-      for (auto& jb : pj) {
-        jb.first_cta = first;
-        first += jb.ncta;
-      }
-      std::memcpy(h_up.data() + o, pj.data(), pj.size() * sizeof(FsJob));
-      o += pj.size() * sizeof(FsJob);
+  std::memcpy(h_up.data() + plan->up_tables, tables.data(), tables.size() * sizeof(FsTable));
+  plan->ntables = (unsigned)tables.size();
+  size_t o = plan->up_wide;
+  for (auto& pj : wide) {
+    unsigned first = 0;
+    for (auto& w : pj) {
+      w.first_cta = first;
+      first += (unsigned)((w.in.n >> w.rounds) / FS_THREADS);
     }
-    std::memcpy(h_up.data() + up_rounds, rounds.data(), rounds.size() * sizeof(FsRound));
+    std::memcpy(h_up.data() + o, pj.data(), pj.size() * sizeof(FsWide));
+    o += pj.size() * sizeof(FsWide);
+    plan->pass_jobs.push_back((unsigned)pj.size());
+    plan->pass_ctas.push_back(first);
   }
-  LGS_CUDA(cudaMemcpyAsync(d_up, h_up.data(), up_bytes, cudaMemcpyHostToDevice, st));
-  // the blob is pageable host memory: the copy is complete (staged) when the call returns
+  std::memcpy(h_up.data() + plan->up_tails, tails.data(), tails.size() * sizeof(FsTail));
+  plan->ntails = (unsigned)tails.size();
+  std::memcpy(h_up.data() + plan->up_rounds, rounds.data(), rounds.size() * sizeof(FsRound));
+}
 
-  // ---- passes, rounds, root --------------------------------------------------------------
-  static bool attr_set = false;
-  if (!attr_set) {
-    LGS_CUDA(cudaFuncSetAttribute(fs_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)FS_PASS_SMEM));
-    attr_set = true;
+// Enqueues a planned proof on st; `pinned` is page-locked host memory holding nothing else for
+// plan->blob.size() bytes until the stream has passed the copy.
+static void fs_launch(const FsPlan& pl, uint8_t* pinned, cudaStream_t st) {
+  const unsigned k = pl.k;
+  if (k == 0) {
+    fs_single_kernel<<<1, 32, 0, st>>>(pl.in, pl.stage + pl.stage_off);
+    LGS_LAUNCH_CHECK();
+    return;
   }
-  {
-    const FsJob* dj = (const FsJob*)(d_up + up_jobs);
-    for (auto& pj : jobs) {
-      unsigned ctas = 0;
-      for (auto& jb : pj) ctas += jb.ncta;
-      fs_pass_kernel<<<ctas, FS_THREADS, FS_PASS_SMEM, st>>>(dj, (unsigned)pj.size());
-      LGS_LAUNCH_CHECK();
-      dj += pj.size();
-    }
-  }
-  if (!rounds.empty()) {
-    fs_rounds_kernel<<<(unsigned)rounds.size(), FS_THREADS, 0, st>>>(
-        (const FsRound*)(d_up + up_rounds));
+  std::memcpy(pinned, pl.blob.data(), pl.blob.size());
+  LGS_CUDA(cudaMemcpyAsync(pl.d_up, pinned, pl.blob.size(), cudaMemcpyHostToDevice, st));
+  ef2* P = pl.P;
+  ef2* Q = pl.Q;
+  if (pl.ntables) {
+    fs_tables_kernel<<<pl.ntables, FS_THREADS, 0, st>>>((const FsTable*)(pl.d_up + pl.up_tables));
     LGS_LAUNCH_CHECK();
   }
-  fs_root_kernel<<<1, 32, 0, st>>>(level(1), P, Q, stage + stage_off);
+  {
+    unsigned S = k;
+    FsSrc src = pl.in;
+    while (S > 0) {
+      const unsigned T = std::min(S, FS_BUILD_T);
+      const size_t smem = 2 * ((size_t)1 << T) * sizeof(ef2);
+      fs_build_kernel<<<(unsigned)((size_t)1 << (S - T)), FS_THREADS, smem, st>>>(src, S, T, P, Q);
+      LGS_LAUNCH_CHECK();
+      S -= T;
+      src = FsSrc{P + ((size_t)1 << S) - 1, Q + ((size_t)1 << S) - 1, ef_zero(), 0};
+    }
+  }
+  const FsWide* dw = (const FsWide*)(pl.d_up + pl.up_wide);
+  for (size_t pi = 0; pi < pl.pass_jobs.size(); ++pi) {
+    fs_wide_kernel<<<pl.pass_ctas[pi], FS_THREADS, 0, st>>>(dw, pl.pass_jobs[pi]);
+    LGS_LAUNCH_CHECK();
+    dw += pl.pass_jobs[pi];
+  }
+  if (pl.ntails) {
+    fs_tail_kernel<<<pl.ntails, FS_TAIL_THREADS, FS_TAIL_SMEM, st>>>(
+        (const FsTail*)(pl.d_up + pl.up_tails));
+    LGS_LAUNCH_CHECK();
+  }
+  if (pl.nrounds) {
+    fs_rounds_kernel<<<(unsigned)pl.nrounds, FS_THREADS, 0, st>>>(
+        (const FsRound*)(pl.d_up + pl.up_rounds));
+    LGS_LAUNCH_CHECK();
+  }
+  const FsSrc l1 = k == 1 ? pl.in : FsSrc{P + 1, Q + 1, ef_zero(), 0};
+  fs_root_kernel<<<1, 32, 0, st>>>(l1, P, Q, pl.stage + pl.stage_off);
   LGS_LAUNCH_CHECK();
+}
+
+static void fs_kernel_attrs() {
+  LGS_CUDA(cudaFuncSetAttribute(fs_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)FS_TAIL_SMEM));
 }
 
 // Assembles the "LGSF" encoding of one proof from the staged values and returns the reduced
@@ -613,7 +818,10 @@ void frac_sum_prove_dev(lgs_ctx* c, const u64* p, const u64* q, size_t n, bool o
   const size_t elems = 6 + 4 * (size_t)k + 4 * nrounds;
   ef2* stage = c->arena.get<ef2>(elems);
   FsPlan pl;
-  fs_enqueue(c, in, k, fields, nfields, *cursor, stage, 0, &pl, st);
+  fs_plan(c, in, k, fields, nfields, *cursor, stage, 0, &pl);
+  fs_kernel_attrs();
+  c->up.reserve(pl.blob.size());
+  fs_launch(pl, c->up.as<uint8_t>(), st);
   c->down.reserve(elems * sizeof(ef2));
   ef2* hst = c->down.as<ef2>();
   LGS_CUDA(cudaMemcpyAsync(hst, stage, pl.stage_elems * sizeof(ef2), cudaMemcpyDeviceToHost, st));
@@ -658,9 +866,14 @@ void lookup_prove_dev(lgs_ctx* c, const u64* a, size_t m, const u64* t, const u6
   LGS_CUDA(cudaEventRecord(c->ev_fork, st));
   LGS_CUDA(cudaStreamWaitEvent(sd, c->ev_fork, 0));
   FsPlan pq, ptab;
-  fs_enqueue(c, FsSrc{nullptr, da, alpha, 1}, kq, fields, nfields, f0 + 1, stage, 0, &pq, st);
-  fs_enqueue(c, FsSrc{de, dt, alpha, 1}, kt, fields, nfields, f0 + 1 + fs_fields_needed(kq), stage,
-             eq_n, &ptab, sd);
+  fs_plan(c, FsSrc{nullptr, da, alpha, 1}, kq, fields, nfields, f0 + 1, stage, 0, &pq);
+  fs_plan(c, FsSrc{de, dt, alpha, 1}, kt, fields, nfields, f0 + 1 + fs_fields_needed(kq), stage,
+          eq_n, &ptab);
+  fs_kernel_attrs();
+  const size_t qb = ceil256(pq.blob.size());
+  c->up.reserve(qb + ptab.blob.size());
+  fs_launch(pq, c->up.as<uint8_t>(), st);
+  fs_launch(ptab, c->up.as<uint8_t>() + qb, sd);
   LGS_CUDA(cudaEventRecord(c->ev_done[0], sd));
   LGS_CUDA(cudaStreamWaitEvent(st, c->ev_done[0], 0));
   c->down.reserve((eq_n + et_n) * sizeof(ef2));
