@@ -179,24 +179,17 @@ struct Q4 {
 };
 
 // One pair (lo = element 2j, hi = element 2j+1) of round t: adds w H(0), w H(1) and w times the
-// leading coefficient of H to s, and returns the element folded with c.
-__device__ __forceinline__ Q4 fs_pair(const Q4& lo, const Q4& hi, ef2 w, ef2 c, bool ones,
-                                      ef2 (&s)[3]) {
-  const ef2 du = ef_sub(hi.u, lo.u), db0 = ef_sub(hi.b0, lo.b0), db1 = ef_sub(hi.b1, lo.b1);
-  ef2 h0, h1, h2;
+// leading coefficient of H to s, and writes the element folded with c to o.  Not inlined: a
+// kernel calls it three times or more, and inlined copies of its 13 extension-field products
+// overflowed the instruction cache (ncu: "no instruction" was the top stall).
+__device__ __noinline__ Q4 fs_pair_gen(const Q4 lo, const Q4 hi, ef2 w, ef2 c, ef2 (&s)[3]) {
   Q4 o;
-  if (ones) {
-    h0 = ef_add(lo.b1, ef_mul(lo.b0, lo.u));
-    h1 = ef_add(hi.b1, ef_mul(hi.b0, hi.u));
-    h2 = ef_mul(db0, du);
-    o.a0 = ef_one();
-  } else {
-    const ef2 da0 = ef_sub(hi.a0, lo.a0);
-    h0 = ef_add(ef_mul(lo.a0, lo.b1), ef_mul(lo.b0, lo.u));
-    h1 = ef_add(ef_mul(hi.a0, hi.b1), ef_mul(hi.b0, hi.u));
-    h2 = ef_add(ef_mul(da0, db1), ef_mul(db0, du));
-    o.a0 = ef_add(lo.a0, ef_mul(c, da0));
-  }
+  const ef2 du = ef_sub(hi.u, lo.u), db0 = ef_sub(hi.b0, lo.b0), db1 = ef_sub(hi.b1, lo.b1);
+  const ef2 da0 = ef_sub(hi.a0, lo.a0);
+  const ef2 h0 = ef_add(ef_mul(lo.a0, lo.b1), ef_mul(lo.b0, lo.u));
+  const ef2 h1 = ef_add(ef_mul(hi.a0, hi.b1), ef_mul(hi.b0, hi.u));
+  const ef2 h2 = ef_add(ef_mul(da0, db1), ef_mul(db0, du));
+  o.a0 = ef_add(lo.a0, ef_mul(c, da0));
   s[0] = ef_add(s[0], ef_mul(w, h0));
   s[1] = ef_add(s[1], ef_mul(w, h1));
   s[2] = ef_add(s[2], ef_mul(w, h2));
@@ -204,6 +197,26 @@ __device__ __forceinline__ Q4 fs_pair(const Q4& lo, const Q4& hi, ef2 w, ef2 c, 
   o.b0 = ef_add(lo.b0, ef_mul(c, db0));
   o.b1 = ef_add(lo.b1, ef_mul(c, db1));
   return o;
+}
+// The same with A0 == 1 (numerators all one): H = B1 + B0 U.
+__device__ __noinline__ Q4 fs_pair_ones(const Q4 lo, const Q4 hi, ef2 w, ef2 c, ef2 (&s)[3]) {
+  Q4 o;
+  const ef2 du = ef_sub(hi.u, lo.u), db0 = ef_sub(hi.b0, lo.b0), db1 = ef_sub(hi.b1, lo.b1);
+  const ef2 h0 = ef_add(lo.b1, ef_mul(lo.b0, lo.u));
+  const ef2 h1 = ef_add(hi.b1, ef_mul(hi.b0, hi.u));
+  const ef2 h2 = ef_mul(db0, du);
+  o.a0 = ef_one();
+  s[0] = ef_add(s[0], ef_mul(w, h0));
+  s[1] = ef_add(s[1], ef_mul(w, h1));
+  s[2] = ef_add(s[2], ef_mul(w, h2));
+  o.u = ef_add(lo.u, ef_mul(c, du));
+  o.b0 = ef_add(lo.b0, ef_mul(c, db0));
+  o.b1 = ef_add(lo.b1, ef_mul(c, db1));
+  return o;
+}
+__device__ __forceinline__ Q4 fs_pair(const Q4& lo, const Q4& hi, ef2 w, ef2 c, bool ones,
+                                      ef2 (&s)[3]) {
+  return ones ? fs_pair_ones(lo, hi, w, c, s) : fs_pair_gen(lo, hi, w, c, s);
 }
 
 __device__ __forceinline__ Q4 arr_load(const FsArrays& a, size_t e) {
@@ -289,7 +302,7 @@ __global__ void __launch_bounds__(FS_THREADS)
   }
 }
 
-__global__ void __launch_bounds__(FS_THREADS)
+__global__ void __launch_bounds__(FS_THREADS, 2)
     fs_wide_kernel(const FsWide* __restrict__ jobs, unsigned njobs) {
   unsigned ji = 0;
   while (ji + 1 < njobs && blockIdx.x >= jobs[ji + 1].first_cta) ++ji;
