@@ -17,15 +17,19 @@
 //    sum_j E_{t+1}(j) H_j(x) is quadratic: S_t at 0, 1 and its leading coefficient give
 //    g_t(0..3) (the host supplies K_t(x) = C_t l_t(x)).  Nothing of size 2^r is built for eq.
 //  * H = A0 B1 + A1 B0 + lambda B0 B1 = A0 B1 + B0 U with U = A1 + lambda B1, and U folds like
-//    A1 (folding is affine), so the stored arrays are A0, U, B0, B1: 6 products for H at 0, 1 and
-//    its leading coefficient, 3 for the weights, 4 for the folds.  With all numerators one (the
-//    query side of a lookup) A0 stays 1 and that drops to 3 + 3 + 3.
+//    A1 (folding is affine), so the stored arrays are A0, U, B0, B1.
+//  * S_t(1) follows from the claim: (1 - z_t) S_t(0) + z_t S_t(1) = sigma_t, with sigma_0 the
+//    layer's claim and sigma_{t+1} = S_t(c_t).  So a pair costs 4 products for H at 0 and its
+//    leading coefficient, 2 for the weights and 4 for the folds; with all numerators one (the
+//    query side of a lookup) A0 stays 1: 2 + 2 + 3.  A layer with a zero coordinate in its point
+//    sums S(1) as well.
 // While a layer's arrays hold more than 2^FS_TAIL_LOG values, wide passes fold them two rounds at a
 // time, four values per thread with no block barrier: a pair's weight is lo[j mod 2^10] from a
-// small table of the round, and the factor hi[j >> 10], common to a warp, multiplies the warp's
+// small table of the round, and the factor hi[j >> 10], common to a CTA, multiplies the CTA's
 // sums, which go to a scratch array.  All layers share each wide launch.  The last rounds of
 // every layer then run in one CTA per layer (fs_tail_kernel) in shared memory, and
-// fs_rounds_kernel reduces the sums into the round polynomials.  Round polynomials hold the same field
+// fs_sums_kernel reduces the sums; fs_chain_kernel recovers each round's S(1) along the claim
+// chain and writes the round polynomials.  Round polynomials hold the same field
 // values as the reference's (the identities are exact), so the proofs are byte-identical.
 #include <algorithm>
 #include <array>
@@ -127,6 +131,7 @@ struct FsArrays {
   size_t n;
   ef2 lambda;
   int ones;
+  int s1;  // sum S(1) too (a layer with a zero point coordinate: the claim chain cannot divide)
 };
 
 // Rounds t (and t+1) of one layer over its whole arrays, two (or one) folds per thread.  Round t's
@@ -161,12 +166,29 @@ struct FsTail {
   unsigned r, t0;
 };
 
-// Reduction of one round: the partial sums of the kernel that ran it, times K_t(0..3).
+// Reduction of one round: the partial sums of the kernel that ran it, into S(0), S(1), L.
 struct FsRound {
   const ef2* part;  // ncta x 3
-  ef2* out;         // g(0), g(1), g(2), g(3)
-  ef2 K[4];
+  ef2* out;         // S(0), S(1) (zero when not summed), L
   unsigned ncta;
+};
+
+// The claim chain of one layer r >= 1 (one warp, r <= 27 rounds): sigma_0 = P_r + lambda Q_r from layer r-1's
+// leaves and beta_{r-1}; per round S(1) = (sigma_t - (1 - z_t) S(0)) / z_t unless it was summed,
+// g(x) = K_t(x) S(x) for x = 0..3, and sigma_{t+1} = S(c_t).  (1 - z_t) S(0) + z_t S(1) = sigma_t
+// is the sumcheck identity divided by C_t, so g(1) equals the reference's g(1) exactly.
+struct FsChainRound {
+  ef2 K[4];
+  ef2 omz, invz, c, c2;  // 1 - z_t, 1 / z_t (unused when summed), c_t, c_t^2
+};
+struct FsChain {
+  const ef2* sums;            // r x (S(0), S(1), L)
+  ef2* out;                   // r x g(0..3)
+  const ef2* prev;            // layer r-1's leaves: A0 A1 B0 B1 (r = 1) or A0 U B0 B1
+  const FsChainRound* rounds;
+  ef2 lambda, lambda_prev, beta_prev;
+  unsigned r;
+  int prev_direct, s1;
 };
 
 namespace {
@@ -178,36 +200,31 @@ struct Q4 {
   ef2 a0, u, b0, b1;
 };
 
-// One pair (lo = element 2j, hi = element 2j+1) of round t: adds w H(0), w H(1) and w times the
-// leading coefficient of H to s, and writes the element folded with c to o.  Not inlined: a
-// kernel calls it three times or more, and inlined copies of its 13 extension-field products
-// overflowed the instruction cache (ncu: "no instruction" was the top stall).
-__device__ __noinline__ Q4 fs_pair_gen(const Q4 lo, const Q4 hi, ef2 w, ef2 c, ef2 (&s)[3]) {
+// One pair (lo = element 2j, hi = element 2j+1) of round t: adds w H(0), w H(1) (when S1) and w
+// times the leading coefficient of H to s, and returns the element folded with c.  ONES: A0 == 1
+// (numerators all one), H = B1 + B0 U.  Without S1 the round's S(1) is recovered from the claim
+// chain (fs_chain_kernel), which saves three of the thirteen products.  Not inlined: a kernel
+// calls it three times or more, and inlined copies of its extension-field products overflowed
+// the instruction cache (ncu: "no instruction" was the top stall).
+template <bool ONES, bool S1>
+__device__ __noinline__ Q4 fs_pair_t(const Q4 lo, const Q4 hi, ef2 w, ef2 c, ef2 (&s)[3]) {
   Q4 o;
   const ef2 du = ef_sub(hi.u, lo.u), db0 = ef_sub(hi.b0, lo.b0), db1 = ef_sub(hi.b1, lo.b1);
-  const ef2 da0 = ef_sub(hi.a0, lo.a0);
-  const ef2 h0 = ef_add(ef_mul(lo.a0, lo.b1), ef_mul(lo.b0, lo.u));
-  const ef2 h1 = ef_add(ef_mul(hi.a0, hi.b1), ef_mul(hi.b0, hi.u));
-  const ef2 h2 = ef_add(ef_mul(da0, db1), ef_mul(db0, du));
-  o.a0 = ef_add(lo.a0, ef_mul(c, da0));
+  ef2 h0, h2;
+  if (ONES) {
+    h0 = ef_add(lo.b1, ef_mul(lo.b0, lo.u));
+    h2 = ef_mul(db0, du);
+    if (S1) s[1] = ef_add(s[1], ef_mul(w, ef_add(hi.b1, ef_mul(hi.b0, hi.u))));
+    o.a0 = ef_one();
+  } else {
+    const ef2 da0 = ef_sub(hi.a0, lo.a0);
+    h0 = ef_add(ef_mul(lo.a0, lo.b1), ef_mul(lo.b0, lo.u));
+    h2 = ef_add(ef_mul(da0, db1), ef_mul(db0, du));
+    if (S1)
+      s[1] = ef_add(s[1], ef_mul(w, ef_add(ef_mul(hi.a0, hi.b1), ef_mul(hi.b0, hi.u))));
+    o.a0 = ef_add(lo.a0, ef_mul(c, da0));
+  }
   s[0] = ef_add(s[0], ef_mul(w, h0));
-  s[1] = ef_add(s[1], ef_mul(w, h1));
-  s[2] = ef_add(s[2], ef_mul(w, h2));
-  o.u = ef_add(lo.u, ef_mul(c, du));
-  o.b0 = ef_add(lo.b0, ef_mul(c, db0));
-  o.b1 = ef_add(lo.b1, ef_mul(c, db1));
-  return o;
-}
-// The same with A0 == 1 (numerators all one): H = B1 + B0 U.
-__device__ __noinline__ Q4 fs_pair_ones(const Q4 lo, const Q4 hi, ef2 w, ef2 c, ef2 (&s)[3]) {
-  Q4 o;
-  const ef2 du = ef_sub(hi.u, lo.u), db0 = ef_sub(hi.b0, lo.b0), db1 = ef_sub(hi.b1, lo.b1);
-  const ef2 h0 = ef_add(lo.b1, ef_mul(lo.b0, lo.u));
-  const ef2 h1 = ef_add(hi.b1, ef_mul(hi.b0, hi.u));
-  const ef2 h2 = ef_mul(db0, du);
-  o.a0 = ef_one();
-  s[0] = ef_add(s[0], ef_mul(w, h0));
-  s[1] = ef_add(s[1], ef_mul(w, h1));
   s[2] = ef_add(s[2], ef_mul(w, h2));
   o.u = ef_add(lo.u, ef_mul(c, du));
   o.b0 = ef_add(lo.b0, ef_mul(c, db0));
@@ -215,8 +232,10 @@ __device__ __noinline__ Q4 fs_pair_ones(const Q4 lo, const Q4 hi, ef2 w, ef2 c, 
   return o;
 }
 __device__ __forceinline__ Q4 fs_pair(const Q4& lo, const Q4& hi, ef2 w, ef2 c, bool ones,
-                                      ef2 (&s)[3]) {
-  return ones ? fs_pair_ones(lo, hi, w, c, s) : fs_pair_gen(lo, hi, w, c, s);
+                                      bool s1, ef2 (&s)[3]) {
+  if (ones)
+    return s1 ? fs_pair_t<true, true>(lo, hi, w, c, s) : fs_pair_t<true, false>(lo, hi, w, c, s);
+  return s1 ? fs_pair_t<false, true>(lo, hi, w, c, s) : fs_pair_t<false, false>(lo, hi, w, c, s);
 }
 
 __device__ __forceinline__ Q4 arr_load(const FsArrays& a, size_t e) {
@@ -307,7 +326,7 @@ __global__ void __launch_bounds__(FS_THREADS, 2)
   unsigned ji = 0;
   while (ji + 1 < njobs && blockIdx.x >= jobs[ji + 1].first_cta) ++ji;
   const FsWide& jb = jobs[ji];
-  const bool ones = jb.in.ones != 0;
+  const bool ones = jb.in.ones != 0, s1f = jb.in.s1 != 0;
   const size_t g = (size_t)(blockIdx.x - jb.first_cta) * blockDim.x + threadIdx.x;
   const size_t nthr = jb.in.n >> jb.rounds;
   ef2 s0[3] = {ef_zero(), ef_zero(), ef_zero()};
@@ -318,13 +337,15 @@ __global__ void __launch_bounds__(FS_THREADS, 2)
     const Q4 x0 = arr_load(jb.in, e), x1 = arr_load(jb.in, e + 1);
     const Q4 x2 = arr_load(jb.in, e + 2), x3 = arr_load(jb.in, e + 3);
     const unsigned j0 = (unsigned)(2 * g) & ((1u << FS_EQ_LO) - 1);
-    const Q4 f0 = fs_pair(x0, x1, ld_ef(jb.lo[0] + j0), jb.c[0], ones, s0);
-    const Q4 f1 = fs_pair(x2, x3, ld_ef(jb.lo[0] + j0 + 1), jb.c[0], ones, s0);
-    y = fs_pair(f0, f1, ld_ef(jb.lo[1] + (g & ((1u << FS_EQ_LO) - 1))), jb.c[1], ones, s1);
+    const Q4 f0 = fs_pair(x0, x1, ld_ef(jb.lo[0] + j0), jb.c[0], ones, s1f, s0);
+    const Q4 f1 = fs_pair(x2, x3, ld_ef(jb.lo[0] + j0 + 1), jb.c[0], ones, s1f, s0);
+    y = fs_pair(f0, f1, ld_ef(jb.lo[1] + (g & ((1u << FS_EQ_LO) - 1))), jb.c[1], ones, s1f,
+                s1);
   } else {
     const size_t e = g << 1;
     const Q4 x0 = arr_load(jb.in, e), x1 = arr_load(jb.in, e + 1);
-    y = fs_pair(x0, x1, ld_ef(jb.lo[0] + (g & ((1u << FS_EQ_LO) - 1))), jb.c[0], ones, s0);
+    y = fs_pair(x0, x1, ld_ef(jb.lo[0] + (g & ((1u << FS_EQ_LO) - 1))), jb.c[0], ones, s1f,
+                s0);
   }
   arr_store(jb.fout, nthr, g, y, ones);
   // CTA sums of each round; round t's factor hi[j >> 10] is common to the CTA (256 threads cover
@@ -368,7 +389,7 @@ __global__ void __launch_bounds__(FS_TAIL_THREADS) fs_tail_kernel(const FsTail* 
   ef2* acc = fs_sm + (1u << FS_TAIL_LOG) + 4 * (1u << (FS_TAIL_LOG - 1));  // [tau][warp][3]
   const FsTail& jb = jobs[blockIdx.x];
   const unsigned t0 = jb.t0, nb = jb.r - t0;
-  const bool ones = jb.in.ones != 0;
+  const bool ones = jb.in.ones != 0, s1f = jb.in.s1 != 0;
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 
   // W_{nb-1} = [1]; W_tau[2m + b] = W_{tau+1}[m] eq(z_{t0+tau+1}, b): the weight of pair jl in
@@ -395,7 +416,7 @@ __global__ void __launch_bounds__(FS_TAIL_THREADS) fs_tail_kernel(const FsTail* 
     ef2 s[3] = {ef_zero(), ef_zero(), ef_zero()};
     for (unsigned jl = threadIdx.x; jl < np; jl += blockDim.x) {
       const Q4 lo = arr_load(jb.in, 2 * jl), hi = arr_load(jb.in, 2 * jl + 1);
-      xs[jl] = fs_pair(lo, hi, wt[np - 1 + jl], c, ones, s);
+      xs[jl] = fs_pair(lo, hi, wt[np - 1 + jl], c, ones, s1f, s);
     }
     warp_acc(s, 0);
   }
@@ -410,7 +431,8 @@ __global__ void __launch_bounds__(FS_TAIL_THREADS) fs_tail_kernel(const FsTail* 
 #pragma unroll
     for (unsigned q = 0; q < 2; ++q) {
       const unsigned jl = threadIdx.x + q * blockDim.x;
-      if (jl < np) o[q] = fs_pair(xs[2 * jl], xs[2 * jl + 1], wt[np - 1 + jl], c, ones, s);
+      if (jl < np)
+        o[q] = fs_pair(xs[2 * jl], xs[2 * jl + 1], wt[np - 1 + jl], c, ones, s1f, s);
     }
     __syncthreads();
 #pragma unroll
@@ -428,7 +450,8 @@ __global__ void __launch_bounds__(FS_TAIL_THREADS) fs_tail_kernel(const FsTail* 
     if (warp == 0) {
       const ef2 c = ld_ef(jb.ch + t0 + tau);
       Q4 o;
-      if (lane < np) o = fs_pair(xs[2 * lane], xs[2 * lane + 1], wt[np - 1 + lane], c, ones, s);
+      if (lane < np)
+        o = fs_pair(xs[2 * lane], xs[2 * lane + 1], wt[np - 1 + lane], c, ones, s1f, s);
       __syncwarp();
       if (lane < np) xs[lane] = o;
       __syncwarp();
@@ -451,9 +474,8 @@ __global__ void __launch_bounds__(FS_TAIL_THREADS) fs_tail_kernel(const FsTail* 
   }
 }
 
-// g(x) = K(x) S(x) with S quadratic: S(2) = -S(0) + 2 S(1) + 2 L, S(3) = -2 S(0) + 3 S(1) + 6 L
-// (L the leading coefficient).
-__global__ void __launch_bounds__(FS_THREADS) fs_rounds_kernel(const FsRound* __restrict__ rounds) {
+// Sums the partial sums of each round: one CTA per round.
+__global__ void __launch_bounds__(FS_THREADS) fs_sums_kernel(const FsRound* __restrict__ rounds) {
   __shared__ ef2 red[96];
   const FsRound& rd = rounds[blockIdx.x];
   ef2 s[3] = {ef_zero(), ef_zero(), ef_zero()};
@@ -470,16 +492,66 @@ __global__ void __launch_bounds__(FS_THREADS) fs_rounds_kernel(const FsRound* __
 #pragma unroll
   for (int q = 0; q < 3; ++q) s[q] = lane < nw ? red[q * 32 + lane] : ef_zero();
   warp_sum3(s);
-  if (lane != 0) return;
-  const ef2 s0 = s[0], s1 = s[1], l = s[2];
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) st_ef(rd.out + q, s[q]);
+}
+
+// g(x) = K(x) S(x) with S quadratic: S(2) = -S(0) + 2 S(1) + 2 L, S(3) = -2 S(0) + 3 S(1) + 6 L
+// (L the leading coefficient).  One warp per layer (see FsChain): lane t holds round t's sums and
+// constants (loaded at once), the chain passes sigma from lane to lane, and every lane then writes
+// its own round polynomial.
+__global__ void __launch_bounds__(32) fs_chain_kernel(const FsChain* __restrict__ chains) {
+  const FsChain& ch = chains[blockIdx.x];
+  const unsigned lane = threadIdx.x, r = ch.r;
+  const bool act = lane < r;
+  FsChainRound rd{};
+  ef2 s0 = ef_zero(), s1 = ef_zero(), l = ef_zero();
+  if (act) {
+    rd = ch.rounds[lane];
+    s0 = ld_ef(ch.sums + 3 * lane);
+    s1 = ld_ef(ch.sums + 3 * lane + 1);
+    l = ld_ef(ch.sums + 3 * lane + 2);
+  }
+  ef2 sigma = ef_zero();
+  if (lane == 0) {
+    const ef2 a0 = ld_ef(ch.prev), b0 = ld_ef(ch.prev + 2), b1 = ld_ef(ch.prev + 3);
+    const ef2 a1 = ch.prev_direct ? ld_ef(ch.prev + 1)
+                                  : ef_sub(ld_ef(ch.prev + 1), ef_mul(ch.lambda_prev, b1));
+    const ef2 P = ef_add(a0, ef_mul(ch.beta_prev, ef_sub(a1, a0)));
+    const ef2 Q = ef_add(b0, ef_mul(ch.beta_prev, ef_sub(b1, b0)));
+    sigma = ef_add(P, ef_mul(ch.lambda, Q));
+  }
+  // sigma_{t+1} = S(c) = S(0) + (S(1) - S(0) - L) c + L c^2 is affine in sigma_t: with
+  // S(1) = (sigma_t - (1 - z) S(0)) / z it is beta_t + gamma_t sigma_t, gamma_t = c / z; with S(1)
+  // summed, gamma_t = 0.  Only the one product gamma_t sigma_t per round is sequential.
+  const ef2 base = ef_add(ef_sub(s0, ef_mul(ef_add(s0, l), rd.c)), ef_mul(l, rd.c2));
+  ef2 gamma = ef_zero(), beta;
+  if (ch.s1) {
+    beta = ef_add(base, ef_mul(s1, rd.c));
+  } else {
+    gamma = ef_mul(rd.invz, rd.c);
+    beta = ef_sub(base, ef_mul(gamma, ef_mul(rd.omz, s0)));
+  }
+  ef2 mine = ef_zero();  // sigma_lane
+  for (unsigned t = 0; t < r; ++t) {
+    ef2 next = ef_zero();
+    if (lane == t) {
+      mine = sigma;
+      next = ef_add(beta, ef_mul(gamma, sigma));
+    }
+    sigma = ef_make(__shfl_sync(0xffffffffu, next.c0, t), __shfl_sync(0xffffffffu, next.c1, t));
+  }
+  if (act && !ch.s1) s1 = ef_mul(ef_sub(mine, ef_mul(rd.omz, s0)), rd.invz);
+  if (!act) return;
   const ef2 two_s1 = ef_add(s1, s1), two_l = ef_add(l, l);
   const ef2 s2 = ef_sub(ef_add(two_s1, two_l), s0);
   const ef2 s3 = ef_sub(ef_add(ef_add(two_s1, s1), ef_add(ef_add(two_l, two_l), two_l)),
                         ef_add(s0, s0));
-  st_ef(rd.out + 0, ef_mul(rd.K[0], s0));
-  st_ef(rd.out + 1, ef_mul(rd.K[1], s1));
-  st_ef(rd.out + 2, ef_mul(rd.K[2], s2));
-  st_ef(rd.out + 3, ef_mul(rd.K[3], s3));
+  st_ef(ch.out + 4 * lane + 0, ef_mul(rd.K[0], s0));
+  st_ef(ch.out + 4 * lane + 1, ef_mul(rd.K[1], s1));
+  st_ef(ch.out + 4 * lane + 2, ef_mul(rd.K[2], s2));
+  st_ef(ch.out + 4 * lane + 3, ef_mul(rd.K[3], s3));
 }
 
 // num, den (level 0) and level 1's four entries (layer 0's leaves).
@@ -525,8 +597,9 @@ struct FsPlan {
   uint8_t* d_up = nullptr;
   std::vector<uint8_t> blob;    // z / challenges, tables, wide jobs (launch by launch), tails,
                                 // rounds
-  size_t up_tables = 0, up_wide = 0, up_tails = 0, up_rounds = 0, nrounds = 0;
-  unsigned ntables = 0, ntails = 0;
+  size_t up_tables = 0, up_wide = 0, up_tails = 0, up_rounds = 0, up_chains = 0, up_crounds = 0;
+  size_t nrounds = 0;
+  unsigned ntables = 0, ntails = 0, nchains = 0;
   std::vector<unsigned> pass_jobs, pass_ctas;
 };
 
@@ -583,6 +656,8 @@ static void fs_plan(lgs_ctx* c, const FsSrc& in, unsigned k, const u64* fields, 
   std::vector<FsTable> tables;
   std::vector<FsTail> tails;
   std::vector<FsRound> rounds;
+  std::vector<FsChain> chains;
+  std::vector<FsChainRound> crounds;
   std::vector<ef2> zc;  // z_r then ch_r for every layer r >= 1
   std::vector<size_t> zoff(k, 0);
   for (unsigned r = 1; r < k; ++r) {
@@ -608,13 +683,44 @@ static void fs_plan(lgs_ctx* c, const FsSrc& in, unsigned k, const u64* fields, 
   up_bytes += ceil256((k - 1) * sizeof(FsTail));
   plan->up_rounds = up_bytes;
   up_bytes += ceil256(nrounds * sizeof(FsRound));
+  plan->up_chains = up_bytes;
+  up_bytes += ceil256((k - 1) * sizeof(FsChain));
+  plan->up_crounds = up_bytes;
+  up_bytes += ceil256(nrounds * sizeof(FsChainRound));
   uint8_t* d_up = plan->d_up = ar.get<uint8_t>(up_bytes);
   std::vector<uint8_t>& h_up = plan->blob;
   h_up.assign(up_bytes, 0);
   std::memcpy(h_up.data(), zc.data(), zc.size() * sizeof(ef2));
   const ef2* d_zc = (const ef2*)d_up;
 
-  size_t round_pos = plan->round_off;
+  // 1 / z_t for every round (one inversion, Montgomery's batch trick); a layer with a zero
+  // coordinate sums S(1) instead (its chain cannot divide)
+  std::vector<int> layer_s1(k, 0);
+  std::vector<ef2> invz;
+  {
+    std::vector<ef2> pre;
+    ef2 acc = ef_one();
+    for (unsigned r = 1; r < k; ++r)
+      for (const ef2& zt : plan->z[r]) {
+        if (ef_eq(zt, ef_zero())) layer_s1[r] = 1;
+        pre.push_back(acc);
+        if (!ef_eq(zt, ef_zero())) acc = ef_mul(acc, zt);
+      }
+    invz.assign(pre.size(), ef_zero());
+    ef2 inv = ef_inv(acc);  // acc is a product of nonzero values
+    size_t i = pre.size();
+    for (unsigned r = k - 1; r >= 1; --r)
+      for (unsigned t = r; t-- > 0;) {
+        const ef2 zt = plan->z[r][t];
+        --i;
+        if (ef_eq(zt, ef_zero())) continue;
+        invz[i] = ef_mul(inv, pre[i]);
+        inv = ef_mul(inv, zt);
+      }
+  }
+  ef2* sums = ar.get<ef2>(3 * nrounds);
+  const FsChainRound* d_crounds = (const FsChainRound*)(d_up + plan->up_crounds);
+  size_t round_pos = plan->round_off, round_idx = 0;
   for (unsigned r = 1; r < k; ++r) {
     const ef2* z = d_zc + zoff[r];
     const ef2* chp = z + r;
@@ -634,13 +740,33 @@ static void fs_plan(lgs_ctx* c, const FsSrc& in, unsigned k, const u64* fields, 
     auto add_round = [&](unsigned t, const ef2* part, unsigned nparts) {
       FsRound rd{};
       rd.part = part;
-      rd.out = stage + round_pos + 4 * t;
-      for (int x = 0; x < 4; ++x) rd.K[x] = K[t][x];
+      rd.out = sums + 3 * (round_idx + t);
       rd.ncta = nparts;
       rounds.push_back(rd);
     };
+    FsChain chn{};
+    chn.sums = sums + 3 * round_idx;
+    chn.out = stage + round_pos;
+    chn.prev = r == 1 ? stage + stage_off + 2 : stage + stage_off + 6 + 4 * (r - 2);
+    chn.rounds = d_crounds + round_idx;
+    chn.lambda = plan->lambda[r];
+    chn.lambda_prev = plan->lambda[r - 1];
+    chn.beta_prev = plan->beta[r - 1];
+    chn.r = r;
+    chn.prev_direct = r == 1 ? 1 : 0;
+    chn.s1 = layer_s1[r];
+    chains.push_back(chn);
+    for (unsigned t = 0; t < r; ++t) {
+      FsChainRound cr{};
+      for (int x = 0; x < 4; ++x) cr.K[x] = K[t][x];
+      cr.omz = ef_sub(ef_one(), plan->z[r][t]);
+      cr.invz = invz[round_idx + t];
+      cr.c = plan->ch[r][t];
+      cr.c2 = ef_mul(cr.c, cr.c);
+      crounds.push_back(cr);
+    }
     FsArrays cur{level(r + 1), nullptr, (size_t)1 << r, plan->lambda[r],
-                 (r + 1 == k && in.p == nullptr) ? 1 : 0};
+                 (r + 1 == k && in.p == nullptr) ? 1 : 0, layer_s1[r]};
     unsigned t = 0, pass = 0;
     while (cur.n > ((size_t)1 << FS_TAIL_LOG)) {
       FsWide w{};
@@ -680,6 +806,7 @@ static void fs_plan(lgs_ctx* c, const FsSrc& in, unsigned k, const u64* fields, 
     tails.push_back(tl);
     for (unsigned q = t; q < r; ++q) add_round(q, tl.part + (size_t)(q - t) * 3, 1);
     round_pos += 4 * (size_t)r;
+    round_idx += r;
   }
   std::memcpy(h_up.data() + plan->up_tables, tables.data(), tables.size() * sizeof(FsTable));
   plan->ntables = (unsigned)tables.size();
@@ -698,6 +825,10 @@ static void fs_plan(lgs_ctx* c, const FsSrc& in, unsigned k, const u64* fields, 
   std::memcpy(h_up.data() + plan->up_tails, tails.data(), tails.size() * sizeof(FsTail));
   plan->ntails = (unsigned)tails.size();
   std::memcpy(h_up.data() + plan->up_rounds, rounds.data(), rounds.size() * sizeof(FsRound));
+  std::memcpy(h_up.data() + plan->up_chains, chains.data(), chains.size() * sizeof(FsChain));
+  std::memcpy(h_up.data() + plan->up_crounds, crounds.data(),
+              crounds.size() * sizeof(FsChainRound));
+  plan->nchains = (unsigned)chains.size();
 }
 
 // Enqueues a planned proof on st; `pinned` is page-locked host memory holding nothing else for
@@ -741,13 +872,17 @@ static void fs_launch(const FsPlan& pl, uint8_t* pinned, cudaStream_t st) {
     LGS_LAUNCH_CHECK();
   }
   if (pl.nrounds) {
-    fs_rounds_kernel<<<(unsigned)pl.nrounds, FS_THREADS, 0, st>>>(
+    fs_sums_kernel<<<(unsigned)pl.nrounds, FS_THREADS, 0, st>>>(
         (const FsRound*)(pl.d_up + pl.up_rounds));
     LGS_LAUNCH_CHECK();
   }
   const FsSrc l1 = k == 1 ? pl.in : FsSrc{P + 1, Q + 1, ef_zero(), 0};
   fs_root_kernel<<<1, 32, 0, st>>>(l1, P, Q, pl.stage + pl.stage_off);
   LGS_LAUNCH_CHECK();
+  if (pl.nchains) {  // after the root kernel: layer 1's chain starts from level 1's entries
+    fs_chain_kernel<<<pl.nchains, 32, 0, st>>>((const FsChain*)(pl.d_up + pl.up_chains));
+    LGS_LAUNCH_CHECK();
+  }
 }
 
 static void fs_kernel_attrs() {

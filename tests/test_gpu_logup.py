@@ -106,3 +106,20 @@ def test_device_inputs_same_bytes(lgs):
     qd = torch.from_numpy(q.view(np.int64)).cuda()
     torch.cuda.synchronize()
     assert L.FracSum.prove(None, qd, _oracle(fields))[0].data == hp.data
+
+
+def test_frac_sum_zero_coordinates(lgs, orc):
+    """Challenges equal to zero or one (a lambda, a beta, fold challenges): layers whose point has
+    a zero coordinate sum S(1) instead of taking it from the claim chain, and eq(z, c) factors can
+    vanish; the bytes still equal the oracle's."""
+    k = 14
+    p, q = rng.ext_elements(31, 1 << k), rng.ext_elements(32, 1 << k)
+    fields = rng.ext_elements(33, 512).copy()
+    # offset o = r (r + 3) / 2 of layer r: lambda at o, ch[r][t] at o + 1 + t, beta at o + 1 + r
+    for r, t in ((5, 1), (12, 3), (12, 12), (12, 13), (13, 0)):
+        fields[r * (r + 3) // 2 + t] = 0
+    fields[9 * 12 // 2 + 2] = (1, 0)
+    proof, point, pe, qe = L.FracSum.prove(p, q, _oracle(fields))
+    want, wpoint, wpe, wqe, _ = orc.frac_sum_prove(p, q, fields)
+    assert proof.data == want and (pe, qe) == (wpe, wqe)
+    assert L.FracSum.verify(proof, _oracle(fields)) is not None
