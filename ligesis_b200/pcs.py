@@ -1,10 +1,10 @@
-"""The `PolyCommitmentScheme` trait of the reference (pcs/src/noop.rs:23-48) and two backends.
+"""The `PolyCommitmentScheme` trait of the reference (pcs/src/noop.rs:23-48) and three backends.
 
 `NoopPcs` mirrors the reference's measurement fake (pcs/src/noop.rs:53-78): an empty commitment,
 no proof, and a `batch_verify` that accepts anything.  It is not sound; it exists so that callers
 written against the trait run unchanged.
 
-`LigesisPcs` is the other sound backend: the adapter that puts LigeSIS (pcs/src/ligesis.rs:239-575)
+`LigesisPcs` is a sound backend: the adapter that puts LigeSIS (pcs/src/ligesis.rs:239-575)
 behind the trait.  LigeSIS commits base-field polynomials, so `commit` projects the F_{p^2} values
 onto F_p, which is exact for integer witnesses and refused for any value with c1 != 0.  A
 polynomial of mu variables is committed as a 2^log_m x 2^log_n matrix of the reference-valid
@@ -12,7 +12,7 @@ shape (log_m = min(7, (mu - 7) / 2)); one of fewer than 14 variables is zero-pad
 high variables and opened at its point with zeros appended, at which the padded polynomial takes
 the same value.  Each proof's `y` is the opened value.
 
-`BasefoldPcs` is a sound backend over F_{p^2} (the field proofsys instantiates the trait over,
+`BasefoldPcs` is the other sound backend, over F_{p^2} (the field proofsys instantiates the trait over,
 proofsys/src/commit.rs:24) built on the GPU Basefold of this package.  `commit` commits the
 polynomial with Basefold.  When every value lies in the base field (proofsys witnesses are
 integers lifted with encode_i64, proofsys/src/witness.rs:102-108), it uses base-field leaves,
