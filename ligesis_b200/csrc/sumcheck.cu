@@ -182,26 +182,46 @@ __global__ void __launch_bounds__(SC_THREADS)
   }
 }
 
+// Lagrange weights of the nodes 0..D at r: g(r) = sum_q L[q] g(q) (the same values as
+// interp_at<D>, so the claims are the same field elements).
+template <int D>
+__device__ void interp_weights(ef2 r, ef2 (&L)[D + 1]) {
+  const u64 inv2 = 0x7FFFFFFF80000001ULL, inv6 = 0xD555555480000001ULL;
+  const ef2 r1 = ef_sub(r, ef_from(1)), r2 = ef_sub(r, ef_from(2));
+  if (D == 1) {
+    L[0] = ef_sub(ef_one(), r);
+    L[1] = r;
+  } else if (D == 2) {
+    L[0] = ef_scale(ef_mul(r1, r2), inv2);
+    L[1] = ef_sub(ef_zero(), ef_mul(r, r2));
+    L[D] = ef_scale(ef_mul(r, r1), inv2);
+  } else {
+    const ef2 r3 = ef_sub(r, ef_from(3));
+    const ef2 r12 = ef_mul(r1, r2), rr1 = ef_mul(r, r1);
+    L[0] = ef_sub(ef_zero(), ef_scale(ef_mul(r12, r3), inv6));
+    L[1] = ef_scale(ef_mul(ef_mul(r, r2), r3), inv2);
+    L[D - 1] = ef_sub(ef_zero(), ef_scale(ef_mul(rr1, r3), inv2));
+    L[D] = ef_scale(ef_mul(rr1, r2), inv6);
+  }
+}
+
 // Remaining rounds t0..k-1 in one CTA, in shared memory.  On entry the vectors hold `len`
 // entries (len <= TAIL); if `fold`, they hold 2*len entries still to be folded with
-// challenge t0 - 1.
+// challenge t0 - 1.  A round's sums go per warp to shared memory (no block reduction per round);
+// the accumulation and the fold of an index are done by the same thread, so one barrier per
+// round suffices, and none once a single warp holds all pairs.  g(1) of every round after the
+// first is filled in at the end along the claim chain (see the chain below).
 template <int D, bool BIN>
 __global__ void __launch_bounds__(SC_TAIL_THREADS)
     sc_tail_kernel(Polys<Fac<D, BIN>::S> P, unsigned len, int fold, const ef2* __restrict__ ch,
                    unsigned t0, unsigned k, ef2* __restrict__ rounds_out,
                    ef2* __restrict__ final_out) {
   constexpr int S = Fac<D, BIN>::S;
-  __shared__ ef2 red[(D + 1) * 32];
+  constexpr unsigned NW = SC_TAIL_THREADS / 32;
+  constexpr unsigned MAXR = 11;  // log2(TAIL) + 1 rounds at most
   __shared__ ef2 sv[S][Fac<D, BIN>::TAIL];
-  // Rounds 0 .. t0-1 were summed without g(1) (except round 0): fill it in along the claim
-  // chain, g_t(1) = g_{t-1}(r_{t-1}) - g_t(0), and carry the claim into this kernel's rounds.
-  ef2 claim = ef_zero();
-  if (threadIdx.x == 0)
-    for (unsigned t = 0; t < t0; ++t) {
-      ef2* g = rounds_out + (size_t)t * (D + 1);
-      if (t > 0) g[1] = ef_sub(claim, g[0]);
-      claim = interp_at<D>(g, ch[t]);
-    }
+  __shared__ ef2 acc[MAXR][NW][D + 1];
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   {
     const ef2 r = fold ? ch[t0 - 1] : ef_zero();
     for (unsigned i = threadIdx.x; i < len; i += blockDim.x)
@@ -210,8 +230,8 @@ __global__ void __launch_bounds__(SC_TAIL_THREADS)
         sv[j][i] = fold ? ef_lerp(P.p[j][i], P.p[j][i + len], r) : P.p[j][i];
   }
   __syncthreads();
-  for (unsigned t = t0; t < k; ++t) {
-    const unsigned half = len >> 1;
+  // one round over `half` pairs: sums of the thread's pairs, then the fold of the same indices
+  auto round = [&](unsigned t, unsigned half) {
     ef2 s[D + 1];
 #pragma unroll
     for (int q = 0; q <= D; ++q) s[q] = ef_zero();
@@ -222,19 +242,43 @@ __global__ void __launch_bounds__(SC_TAIL_THREADS)
       for (int j = 0; j < S; ++j) lo[j] = sv[j][i], hi[j] = sv[j][i + half];
       accumulate_pair<D, BIN>(lo, hi, s, skip1);
     }
-    block_reduce<D>(s, red);
-    if (threadIdx.x == 0) {
-      if (skip1) s[1] = ef_sub(claim, s[0]);
 #pragma unroll
-      for (int q = 0; q <= D; ++q) rounds_out[(size_t)t * (D + 1) + q] = s[q];
-      claim = interp_at<D>(s, ch[t]);
-    }
+    for (int q = 0; q <= D; ++q)
+#pragma unroll
+      for (int m = 16; m; m >>= 1) s[q] = ef_add(s[q], shfl_xor_ef(s[q], m));
+    if (lane == 0)
+#pragma unroll
+      for (int q = 0; q <= D; ++q) acc[t - t0][warp][q] = s[q];
     const ef2 r = ch[t];
     for (unsigned i = threadIdx.x; i < half; i += blockDim.x)
 #pragma unroll
       for (int j = 0; j < S; ++j) sv[j][i] = ef_lerp(sv[j][i], sv[j][i + half], r);
+  };
+  unsigned t = t0;
+  for (; t < k && (len >> 1) > 32; ++t, len >>= 1) {
+    round(t, len >> 1);
     __syncthreads();
-    len = half;
+  }
+  if (warp == 0) {
+    for (unsigned tt = t, l = len; tt < k; ++tt, l >>= 1) {
+      round(tt, l >> 1);
+      __syncwarp();
+    }
+  } else {
+    for (unsigned tt = t; tt < k; ++tt)
+      if (lane == 0)
+#pragma unroll
+        for (int q = 0; q <= D; ++q) acc[tt - t0][warp][q] = ef_zero();
+  }
+  __syncthreads();
+  // this kernel's rounds: sums over the warps (g(1) only for round 0)
+  for (unsigned i = threadIdx.x; i < (k - t0) * (D + 1); i += blockDim.x) {
+    const unsigned tt = i / (D + 1), q = i % (D + 1);
+    if (q == 1 && t0 + tt > 0) continue;
+    ef2 v = ef_zero();
+#pragma unroll
+    for (unsigned w = 0; w < NW; ++w) v = ef_add(v, acc[tt][w][q]);
+    rounds_out[(size_t)(t0 + tt) * (D + 1) + q] = v;
   }
   if (threadIdx.x == 0) {
     if (BIN) {
@@ -246,6 +290,41 @@ __global__ void __launch_bounds__(SC_TAIL_THREADS)
 #pragma unroll
       for (int j = 0; j < S; ++j) final_out[j] = sv[j][0];
     }
+  }
+  __syncthreads();
+  // The claim chain: g_t(1) = claim_t - g_t(0) for t >= 1, claim_{t+1} = g_t(r_t).  With
+  // g_t(r) = sum_q L_q(r) g_t(q), claim_{t+1} = A_t + L_1(r_t) claim_t, A_t collecting the other
+  // terms (and A_0 = g_0(r_0), whose g(1) is summed), so lane t prepares its round's A_t and
+  // L_1(r_t) in parallel and the claim moves from lane to lane with one product per round.
+  if (warp != 0) return;
+  ef2 claim = ef_zero();
+  for (unsigned c0 = 0; c0 < k; c0 += 32) {
+    const unsigned tt = c0 + lane;
+    ef2 g[D + 1], L[D + 1], a = ef_zero(), w1 = ef_zero();
+    if (tt < k) {
+#pragma unroll
+      for (int q = 0; q <= D; ++q) g[q] = rounds_out[(size_t)tt * (D + 1) + q];
+      interp_weights<D>(ch[tt], L);
+#pragma unroll
+      for (int q = 0; q <= D; ++q)
+        if (q != 1) a = ef_add(a, ef_mul(L[q], g[q]));
+      if (tt == 0) {
+        a = ef_add(a, ef_mul(L[1], g[1]));
+      } else {
+        w1 = L[1];
+        a = ef_sub(a, ef_mul(L[1], g[0]));
+      }
+    }
+    ef2 mine = ef_zero();  // claim_tt
+    for (unsigned j = 0; j < 32 && c0 + j < k; ++j) {
+      ef2 next = ef_zero();
+      if (lane == j) {
+        mine = claim;
+        next = ef_add(a, ef_mul(w1, claim));
+      }
+      claim = ef_make(__shfl_sync(0xffffffffu, next.c0, j), __shfl_sync(0xffffffffu, next.c1, j));
+    }
+    if (tt < k && tt > 0) rounds_out[(size_t)tt * (D + 1) + 1] = ef_sub(mine, g[0]);
   }
 }
 
