@@ -60,17 +60,37 @@ __device__ ef2 eq_high(const ef2* p, unsigned b, unsigned k, size_t idx) {
 }  // namespace
 
 // ---- gather ------------------------------------------------------------------------------
+// GATHER_SPLIT CTAs per segment (blockIdx.y picks a contiguous share of its items), 32-bit index
+// math, and eight loads in flight per thread before their stores: a segment of thousands of words
+// in one CTA was a long serial chain of dependent loads.
+constexpr unsigned GATHER_SPLIT = 8;
 __global__ void gather_segments_kernel(const GatherSeg* __restrict__ segs) {
   const GatherSeg s = segs[blockIdx.x];
-  const size_t total = s.count * s.words;
-  for (size_t t = threadIdx.x; t < total; t += blockDim.x) {
-    size_t i = t / s.words, w = t % s.words;
-    s.dst[t] = s.src[s.idx[i] * s.words + w];
+  const unsigned words = s.words, count = (unsigned)s.count;
+  const unsigned per = (count + GATHER_SPLIT - 1) / GATHER_SPLIT;
+  const unsigned i0 = min(count, blockIdx.y * per), i1 = min(count, i0 + per);
+  const unsigned t_end = i1 * words;
+  constexpr unsigned U = 8;
+  for (unsigned t0 = i0 * words + threadIdx.x; t0 < t_end; t0 += U * blockDim.x) {
+    u64 v[U];
+#pragma unroll
+    for (unsigned u = 0; u < U; ++u) {
+      const unsigned t = t0 + u * blockDim.x;
+      if (t < t_end) {
+        const unsigned i = t / words, w = t - i * words;
+        v[u] = s.src[s.idx[i] * words + w];
+      }
+    }
+#pragma unroll
+    for (unsigned u = 0; u < U; ++u) {
+      const unsigned t = t0 + u * blockDim.x;
+      if (t < t_end) s.dst[t] = v[u];
+    }
   }
 }
 void gather_segments(const GatherSeg* segs_dev, unsigned nseg, cudaStream_t st) {
   if (!nseg) return;
-  gather_segments_kernel<<<nseg, 256, 0, st>>>(segs_dev);
+  gather_segments_kernel<<<dim3(nseg, GATHER_SPLIT), 256, 0, st>>>(segs_dev);
   LGS_LAUNCH_CHECK();
 }
 
