@@ -56,6 +56,18 @@ def _dist():
     return rank, world, local
 
 
+def _max_over_ranks(ms: float, dist, device) -> float:
+    """The slowest rank's time (replicas run in parallel, so the job takes the longest one);
+    `dist` is torch.distributed after init_process_group, or None for one process."""
+    if dist is None:
+        return ms
+    import torch
+
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ------------------------------------------------------------------------------------------------
 # CPU baseline: the oracle (a single-threaded restatement of the reference prover)
 # ------------------------------------------------------------------------------------------------
@@ -279,11 +291,7 @@ def run_ours(args) -> None:
         ev1.record(stream)
         torch.cuda.synchronize(local)
         gc.enable()
-        ms = ev0.elapsed_time(ev1) / k
-        if dist:
-            t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = _max_over_ranks(ev0.elapsed_time(ev1) / k, dist, f"cuda:{local}")
         return ms, out
 
     launches0 = lib.lgs_launch_count()
