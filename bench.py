@@ -778,6 +778,64 @@ def run_logup(args) -> None:
                       "cpu_oracle": cpu}), flush=True)
 
 
+def run_witness(args) -> None:
+    """proofsys' rescaled linear layers of the integer GPT-2 (Config::gpt2_31: 31 positions,
+    d_model 768, MLP 3072, vocabulary 50257, scale 2^12; model.rs:360-374, :225-228) on the GPU:
+    each layer shape from host arrays (copies in the timed call) and from device tensors, the
+    whole forward's linear work (12 blocks x (qkv, attention projection, fc, fproj) + the
+    vocabulary head), and the oracle's time for one MLP fc layer.  Seeded synthetic values:
+    activations within +-max_v * scale, weights within +-2^15 (no exported model here)."""
+    import numpy as np
+    import torch
+
+    import ligesis_b200 as L
+    from ligesis_b200 import proofsys as ps
+
+    ctx = L.Context(0)
+    cfg = ps.GPT2_31
+    n, d, h, v, sc = cfg["n_seq"], cfg["d_model"], cfg["mlp_hidden"], cfg["vocab"], cfg["scale"]
+    g = np.random.default_rng(8)
+    act = cfg["max_v"] * sc
+    shapes = {"qkv": (d, 3 * d, False), "attn_proj": (d, d, False), "fc": (d, h, False),
+              "fproj": (h, d, False), "vocab_head": (d, v, True)}
+    out = {}
+    for name, (inner, cols, wt) in shapes.items():
+        x = g.integers(-act, act, size=(n, inner), dtype=np.int64)
+        w = g.integers(-(1 << 15), 1 << 15, size=(cols, inner) if wt else (inner, cols),
+                       dtype=np.int64)
+        b = g.integers(-act, act, size=cols, dtype=np.int64)
+        xd, wd, bd = (torch.from_numpy(a).cuda() for a in (x, w, b))
+        res = {}
+        for label, fn in (("host_ms", lambda: ps.linear_witness(x, w, b, sc, wt, ctx)),
+                          ("device_ms", lambda: ps.linear_witness(xd, wd, bd, sc, wt, ctx))):
+            for _ in range(args.warmup):
+                fn()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                fn()
+            torch.cuda.synchronize()
+            res[label] = round((time.perf_counter() - t0) / args.steps * 1e3, 3)
+        res["products"] = n * inner * cols
+        out[name] = res
+    forward = 12 * sum(out[k]["device_ms"] for k in ("qkv", "attn_proj", "fc", "fproj")) \
+        + out["vocab_head"]["device_ms"]
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import orc
+
+        x = g.integers(-act, act, size=(n, d), dtype=np.int64)
+        w = g.integers(-(1 << 15), 1 << 15, size=(d, h), dtype=np.int64)
+        t0 = time.perf_counter()
+        orc.linear_witness(x, w, None, sc)
+        cpu = {"layer": "fc", "ms": round((time.perf_counter() - t0) * 1e3, 1), "cores": 1,
+               "kind": "port", "cpu": _cpu_model()}
+    print(json.dumps({"mode": "witness", "config": "gpt2_31", "steps": args.steps,
+                      "timing": "host wall clock per call", "layers": out,
+                      "forward_linear_device_ms": round(forward, 3), "cpu_oracle": cpu}),
+          flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -786,7 +844,7 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", choices=["line", "batch", "serve", "commit", "timeline", "basefold",
-                                       "logup"], default="line")
+                                       "logup", "witness"], default="line")
     ap.add_argument("--log-m", type=int, default=LOG_M)
     ap.add_argument("--log-n", type=int, default=LOG_N)
     ap.add_argument("--lanes", type=int, default=12)
@@ -814,6 +872,9 @@ def main() -> None:
         return
     if args.mode == "logup":
         run_logup(args)
+        return
+    if args.mode == "witness":
+        run_witness(args)
         return
     if args.impl == "reference":
         run_reference(args)

@@ -151,6 +151,19 @@ lgs_status lgs_lookup_verify(const uint8_t* proof, size_t proof_len, const uint6
                              size_t nfields, uint64_t* cursor, uint64_t* zq, size_t zq_cap,
                              uint64_t* zt, size_t zt_cap, uint64_t vals[6], int* accept);
 
+/* ---- proofsys' integer witness (proofsys/src/tensor.rs, proofsys/src/model.rs) ----
+ * The rescaled linear layer of the integer GPT-2 (model.rs:360-361): Q, REM =
+ * floor_div_const_with_rem(X.matmul(W), divisor) (tensor.rs:76-89, :121-133) and Y = Q + bias
+ * (add_row_vector, :51-60); with w_transposed, X.matmul_transposed_rhs(W) (:91-104) and W is
+ * cols x inner.  X is rows x inner, all row-major int64; REM lies in [0, divisor); bias (cols) and
+ * y_field (rows x cols, encode_i64(Y) as canonical Goldilocks, witness.rs:102-108) may be NULL.
+ * on_device = 1: every array is a device pointer on the context's device.  A product or a Q + bias
+ * outside the int64 range (where the reference panics) gives LGS_ERR_BAD_SHAPE. */
+lgs_status lgs_linear_witness(lgs_ctx* ctx, const int64_t* x, size_t rows, size_t inner,
+                              const int64_t* w, size_t cols, int w_transposed,
+                              const int64_t* bias, int64_t divisor, int on_device, int64_t* q,
+                              int64_t* rem, int64_t* y, uint64_t* y_field);
+
 /* ---- batched and served proving (the reference proves one polynomial at a time on one
  * thread, pcs/benches/ligesis.rs:20-60) ----
  * An engine owns `lanes` contexts on one device, each driven by its own host thread, so the

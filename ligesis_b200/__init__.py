@@ -28,6 +28,7 @@ from .ligesis import (
 from .basefold import Basefold, BasefoldCommit, BasefoldProof, BasefoldProverState
 from .logup import (FracSum, FracSumProof, Lookup, LookupProof, OpeningClaim, Poly,
                     multiplicity_vector)
+from . import proofsys
 from .pcs import BasefoldPcs, LigesisPcs, NoopCommit, NoopPcs
 from .rng import SeededRng
 

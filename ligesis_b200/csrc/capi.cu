@@ -416,6 +416,18 @@ lgs_status lgs_lookup_verify(const uint8_t* proof, size_t proof_len, const uint6
   });
 }
 
+lgs_status lgs_linear_witness(lgs_ctx* ctx, const int64_t* x, size_t rows, size_t inner,
+                              const int64_t* w, size_t cols, int w_transposed,
+                              const int64_t* bias, int64_t divisor, int on_device, int64_t* q,
+                              int64_t* rem, int64_t* y, uint64_t* y_field) {
+  return guarded([&] {
+    need(ctx && x && w && q && rem && y, "lgs_linear_witness: null argument");
+    CtxDevice dg(ctx);
+    linear_witness_dev(ctx, x, rows, inner, w, cols, w_transposed != 0, bias, divisor,
+                       on_device != 0, q, rem, y, y_field);
+  });
+}
+
 lgs_status lgs_basefold_verify(const uint8_t root[32], const uint64_t* point, size_t plen,
                                const uint8_t* proof, size_t proof_len, const uint64_t* fields,
                                size_t nfields, const uint64_t* ints, size_t nints,

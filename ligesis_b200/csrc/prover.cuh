@@ -356,6 +356,11 @@ int frac_sum_verify_host(const uint8_t* proof, size_t len, const u64* fields, si
 int lookup_verify_host(const uint8_t* proof, size_t len, const u64* fields, size_t nfields,
                        uint64_t* cursor, u64* zq, size_t zq_cap, u64* zt, size_t zt_cap,
                        u64* vals);
+// proofsys' rescaled linear-layer witness (witness.cu): Q, REM = floor_div(X W, divisor),
+// Y = Q + bias, Y_field = encode_i64(Y); row-major i64 arrays, on the host or (on_device) the device.
+void linear_witness_dev(lgs_ctx* c, const int64_t* x, size_t rows, size_t inner, const int64_t* w,
+                        size_t cols, bool w_transposed, const int64_t* bias, int64_t divisor,
+                        bool on_device, int64_t* q, int64_t* rem, int64_t* y, uint64_t* y_field);
 lgs_status set_error(lgs_status s, const std::string& msg);
 lgs_status status_of_current_exception();
 }  // namespace lgs

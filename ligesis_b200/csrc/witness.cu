@@ -1,0 +1,234 @@
+// proofsys' rescaled linear-layer witness on the device (proofsys/src/model.rs:360-361 and the
+// integer kernels of proofsys/src/tensor.rs): Q, REM = floor_div(X W, divisor) with REM in
+// [0, divisor), Y = Q + bias, and Y lifted to Goldilocks like encode_i64
+// (proofsys/src/witness.rs:102-108).  The reference multiplies i64 matrices with i128
+// accumulators and panics when a result leaves the i64 range; this kernel does the same products
+// exactly (128-bit accumulators) and reports such a result as an error instead.
+//
+// The values are fixed-point integers (scale 2^12, activations up to about 2^20), not int8, so the
+// product runs on the integer pipes: a 32 x 64 output tile per CTA, 16 x 16 threads with a 2 x 4
+// block each, the K dimension staged through shared memory 32 at a time, exact 128-bit sums as
+// (hi, lo) words.  GPT-2's layers have 31 rows, so K is split over CTAs to fill the GPU and the
+// exact partial sums are added by a second kernel.  The largest layer, the vocabulary head
+// (31 x 768 x 50257), is 1.2 G products.
+#include <algorithm>
+#include <cstring>
+
+#include "prover.cuh"
+
+namespace lgs {
+
+namespace {
+
+constexpr int LW_TM = 32, LW_TN = 64, LW_K = 32;  // output tile rows x cols, K per stage
+
+// 128-bit accumulator as (hi:lo); a product of two i64 is added exactly.
+// (two's complement in two words, added modulo 2^128 like the reference's i128)
+struct Acc128 {
+  uint64_t lo, hi;
+};
+__device__ __forceinline__ void mac128(Acc128& a, int64_t x, int64_t y) {
+  const uint64_t pl = (uint64_t)x * (uint64_t)y;
+  const uint64_t ph = (uint64_t)__mul64hi(x, y);
+  a.lo += pl;
+  a.hi += ph + (a.lo < pl ? 1 : 0);
+}
+__device__ __forceinline__ void add128(Acc128& a, const Acc128& b) {
+  a.lo += b.lo;
+  a.hi += b.hi + (a.lo < b.lo ? 1 : 0);
+}
+__device__ __forceinline__ bool fits_i64(uint64_t hi, uint64_t lo) {
+  return (int64_t)hi == ((int64_t)lo >> 63);  // the high word extends the low word's sign
+}
+
+// Q, REM, Y, Y_field of one output from its exact sum; false when a value leaves the i64 range.
+__device__ __forceinline__ bool lw_finish(const Acc128& s, const int64_t* bias, size_t c,
+                                          int64_t d, size_t o, int64_t* q_out, int64_t* rem_out,
+                                          int64_t* y_out, uint64_t* yf_out) {
+  if (!fits_i64(s.hi, s.lo)) return false;  // checked_i128_to_i64 of the product
+  const int64_t v = (int64_t)s.lo;
+  int64_t q = v / d, rm = v % d;  // floor division: a negative remainder moves q down
+  if (rm < 0) {
+    q -= 1;
+    rm += d;
+  }
+  const int64_t b = bias ? bias[c] : 0;
+  const int64_t yy = (int64_t)((uint64_t)q + (uint64_t)b);
+  if (((q ^ yy) & (b ^ yy)) < 0) return false;  // signed overflow of q + bias
+  q_out[o] = q;
+  rem_out[o] = rm;
+  y_out[o] = yy;
+  if (yf_out) {  // encode_i64: y mod p, or -(|y| mod p)
+    uint64_t e;
+    if (yy >= 0) {
+      e = (uint64_t)yy % GL_P;
+    } else {
+      const uint64_t m = ((uint64_t)(-(yy + 1)) + 1) % GL_P;
+      e = m ? GL_P - m : 0;
+    }
+    yf_out[o] = e;
+  }
+  return true;
+}
+
+struct LwArgs {
+  const int64_t* x;
+  const int64_t* w;
+  const int64_t* bias;
+  size_t rows, inner, cols, kchunk;
+  int64_t d;
+  int wt;
+  Acc128* part;  // [split][rows][cols] when split over K
+  int64_t *q, *rem, *y;
+  uint64_t* yf;
+  int* err;
+};
+
+// A 32 x 64 output tile over the K range of blockIdx.z; 16 x 16 threads, 2 x 4 outputs each.
+// FINAL (one K split): finish the outputs here; else store the exact partial sums.
+template <bool FINAL>
+__global__ void __launch_bounds__(256) linear_witness_kernel(const LwArgs a) {
+  __shared__ int64_t xs[LW_K][LW_TM + 1];
+  __shared__ int64_t ws[LW_K][LW_TN + 1];
+  const unsigned tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const size_t r0 = (size_t)blockIdx.y * LW_TM, c0 = (size_t)blockIdx.x * LW_TN;
+  const size_t kb = (size_t)blockIdx.z * a.kchunk, ke = min(a.inner, kb + a.kchunk);
+  Acc128 acc[2][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = Acc128{0, 0};
+  for (size_t k0 = kb; k0 < ke; k0 += LW_K) {
+    for (unsigned e = threadIdx.x; e < LW_TM * LW_K; e += blockDim.x) {
+      const unsigned rr = e / LW_K, kk = e % LW_K;
+      const size_t gr = r0 + rr, gk = k0 + kk;
+      xs[kk][rr] = (gr < a.rows && gk < ke) ? a.x[gr * a.inner + gk] : 0;
+    }
+    for (unsigned e = threadIdx.x; e < LW_TN * LW_K; e += blockDim.x) {
+      unsigned cc, kk;
+      if (a.wt) {  // w is cols x inner: consecutive threads read consecutive k
+        cc = e / LW_K;
+        kk = e % LW_K;
+      } else {  // w is inner x cols: consecutive threads read consecutive columns
+        kk = e / LW_TN;
+        cc = e % LW_TN;
+      }
+      const size_t gc = c0 + cc, gk = k0 + kk;
+      int64_t v = 0;
+      if (gc < a.cols && gk < ke) v = a.wt ? a.w[gc * a.inner + gk] : a.w[gk * a.cols + gc];
+      ws[kk][cc] = v;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int kk = 0; kk < LW_K; ++kk) {
+      const int64_t x0 = xs[kk][2 * ty], x1 = xs[kk][2 * ty + 1];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int64_t b = ws[kk][4 * tx + j];
+        mac128(acc[0][j], x0, b);
+        mac128(acc[1][j], x1, b);
+      }
+    }
+    __syncthreads();
+  }
+  bool bad = false;
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const size_t r = r0 + 2 * ty + i, c = c0 + 4 * tx + j;
+      if (r >= a.rows || c >= a.cols) continue;
+      const size_t o = r * a.cols + c;
+      if (FINAL)
+        bad |= !lw_finish(acc[i][j], a.bias, c, a.d, o, a.q, a.rem, a.y, a.yf);
+      else
+        a.part[(size_t)blockIdx.z * a.rows * a.cols + o] = acc[i][j];
+    }
+  if (bad) atomicOr(a.err, 1);
+}
+
+// Sums the K splits of every output (exactly) and finishes it.
+__global__ void linear_witness_finish_kernel(const LwArgs a, unsigned nsplit) {
+  const size_t n = a.rows * a.cols;
+  bool bad = false;
+  for (size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x; o < n;
+       o += (size_t)gridDim.x * blockDim.x) {
+    Acc128 s{0, 0};
+    for (unsigned z = 0; z < nsplit; ++z) add128(s, a.part[(size_t)z * n + o]);
+    bad |= !lw_finish(s, a.bias, o % a.cols, a.d, o, a.q, a.rem, a.y, a.yf);
+  }
+  if (bad) atomicOr(a.err, 1);
+}
+
+}  // namespace
+
+void linear_witness_dev(lgs_ctx* c, const int64_t* x, size_t rows, size_t inner, const int64_t* w,
+                        size_t cols, bool w_transposed, const int64_t* bias, int64_t divisor,
+                        bool on_device, int64_t* q, int64_t* rem, int64_t* y, uint64_t* y_field) {
+  if (divisor <= 0) throw ShapeError("linear witness: the divisor must be positive");
+  if (rows == 0 || inner == 0 || cols == 0) throw ShapeError("linear witness: empty matrix");
+  if (rows > ((size_t)1 << 20) || cols > ((size_t)1 << 24) || inner > ((size_t)1 << 24))
+    throw ShapeError("linear witness: matrix too large");
+  cudaStream_t st = c->st;
+  Arena& ar = c->arena;
+  ar.begin();
+  const size_t nx = rows * inner, nw = inner * cols, no = rows * cols;
+  auto in = [&](const int64_t* h, size_t n) -> const int64_t* {
+    if (!h) return nullptr;
+    if (on_device) return h;
+    int64_t* d = ar.get<int64_t>(n);
+    h2d_staged(c, d, h, n * 8, st);
+    return d;
+  };
+  const int64_t* dx = in(x, nx);
+  const int64_t* dw = in(w, nw);
+  const int64_t* db = in(bias, cols);
+  int64_t *dq = q, *dr = rem, *dy = y;
+  uint64_t* df = y_field;
+  if (!on_device) {
+    dq = ar.get<int64_t>(no);
+    dr = ar.get<int64_t>(no);
+    dy = ar.get<int64_t>(no);
+    df = y_field ? ar.get<uint64_t>(no) : nullptr;
+  }
+  int* derr = ar.get<int>(1);
+  LGS_CUDA(cudaMemsetAsync(derr, 0, sizeof(int), st));
+  // Few rows (GPT-2 runs 31 positions) leave most SMs idle: split K until there are about two
+  // CTAs per SM, each with at least 128 values of K, and sum the exact partials afterwards.
+  const size_t tiles = ((cols + LW_TN - 1) / LW_TN) * ((rows + LW_TM - 1) / LW_TM);
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  size_t split = std::max<size_t>(1, (2 * (size_t)nsm + tiles - 1) / tiles);
+  split = std::min<size_t>(split, std::max<size_t>(1, inner / 128));
+  split = std::min<size_t>(split, 64);
+  size_t kchunk = (inner + split - 1) / split;
+  kchunk = (kchunk + LW_K - 1) / LW_K * LW_K;
+  split = (inner + kchunk - 1) / kchunk;
+  LwArgs a{dx, dw, db, rows, inner, cols, kchunk, divisor, w_transposed ? 1 : 0, nullptr,
+           dq, dr, dy, df, derr};
+  const dim3 grid((unsigned)((cols + LW_TN - 1) / LW_TN), (unsigned)((rows + LW_TM - 1) / LW_TM),
+                  (unsigned)split);
+  if (split == 1) {
+    linear_witness_kernel<true><<<grid, 256, 0, st>>>(a);
+    LGS_LAUNCH_CHECK();
+  } else {
+    a.part = ar.get<Acc128>(split * no);
+    linear_witness_kernel<false><<<grid, 256, 0, st>>>(a);
+    LGS_LAUNCH_CHECK();
+    const unsigned blocks = (unsigned)std::min<size_t>((no + 255) / 256, 148 * 8);
+    linear_witness_finish_kernel<<<blocks, 256, 0, st>>>(a, (unsigned)split);
+    LGS_LAUNCH_CHECK();
+  }
+  int herr = 0;
+  LGS_CUDA(cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (!on_device) {
+    LGS_CUDA(cudaMemcpyAsync(q, dq, no * 8, cudaMemcpyDeviceToHost, st));
+    LGS_CUDA(cudaMemcpyAsync(rem, dr, no * 8, cudaMemcpyDeviceToHost, st));
+    LGS_CUDA(cudaMemcpyAsync(y, dy, no * 8, cudaMemcpyDeviceToHost, st));
+    if (y_field) LGS_CUDA(cudaMemcpyAsync(y_field, df, no * 8, cudaMemcpyDeviceToHost, st));
+  }
+  LGS_CUDA(cudaStreamSynchronize(st));
+  if (herr) throw ShapeError("linear witness: a product or Q + bias leaves the i64 range");
+}
+
+}  // namespace lgs

@@ -10,6 +10,7 @@
 #include <string>
 
 #include "frac_sum.hpp"
+#include "proofsys.hpp"
 #include "proof_io.hpp"
 
 using namespace orc;
@@ -457,5 +458,25 @@ int orc_lookup_verify(const uint8_t* proof, size_t len, const u64* fields, size_
     store_ef(c.t, vals + 4);
   });
   return 1;
+}
+
+// proofsys' rescaled linear-layer witness (proofsys/src/tensor.rs, model.rs:360-361); bias may be
+// NULL, y_field (encode_i64 of y) may be NULL.
+int orc_linear_witness(const int64_t* x, size_t rows, size_t inner, const int64_t* w, size_t cols,
+                       int w_transposed, const int64_t* bias, int64_t divisor, int64_t* q,
+                       int64_t* rem, int64_t* y, uint64_t* y_field) {
+  ORC_TRY({
+    std::vector<i64> xv(x, x + rows * inner), wv(w, w + inner * cols), bv;
+    if (bias) bv.assign(bias, bias + cols);
+    const LinearWitness lw =
+        linear_witness(xv, rows, inner, wv, cols, w_transposed != 0, bias ? &bv : nullptr, divisor);
+    for (size_t i = 0; i < rows * cols; ++i) {
+      q[i] = lw.q[i];
+      rem[i] = lw.rem[i];
+      y[i] = lw.y[i];
+      if (y_field) y_field[i] = encode_i64(lw.y[i]);
+    }
+  });
+  return 0;
 }
 }  // extern "C"

@@ -83,6 +83,9 @@ def lib():
                 "orc_lookup_prove": (C.c_int, [u64p, C.c_size_t, u64p, C.c_size_t, u64p, u64p,
                                                C.c_size_t, u64p, C.POINTER(u8p),
                                                C.POINTER(C.c_size_t), u64p, u64p]),
+                "orc_linear_witness": (C.c_int, [i64p, C.c_size_t, C.c_size_t, i64p, C.c_size_t,
+                                                 C.c_int, i64p, C.c_int64, i64p, i64p, i64p,
+                                                 u64p]),
                 "orc_lookup_verify": (C.c_int, [u8p, C.c_size_t, u64p, C.c_size_t, u64p, u64p,
                                                 C.c_size_t, u64p, C.c_size_t, u64p]),
             }
@@ -354,6 +357,28 @@ def basefold_verify(root: bytes, point, proof: bytes, fields, ints, cursors=(0, 
 
 
 # ---- GKR fraction sum / GKR-LogUp lookup (logup/src/frac_sum.rs, logup/src/lookup.rs) ---------
+i64p = C.POINTER(C.c_int64)
+
+
+def linear_witness(x, w, bias, divisor: int, w_transposed: bool = False):
+    """proofsys' rescaled linear layer: (q, rem, y, encode_i64(y)) of x.matmul(w) (or
+    x.matmul_transposed_rhs(w)), floor-divided by divisor, plus the bias row."""
+    xa = np.ascontiguousarray(x, dtype=np.int64)
+    wa = np.ascontiguousarray(w, dtype=np.int64)
+    rows, inner = xa.shape
+    cols = wa.shape[0] if w_transposed else wa.shape[1]
+    ba = None if bias is None else np.ascontiguousarray(bias, dtype=np.int64)
+    q = np.zeros((rows, cols), np.int64)
+    rem = np.zeros_like(q)
+    y = np.zeros_like(q)
+    yf = np.zeros((rows, cols), np.uint64)
+    p64 = lambda a: a.ctypes.data_as(i64p)
+    _ok(lib().orc_linear_witness(p64(xa), rows, inner, p64(wa), cols, int(w_transposed),
+                                 None if ba is None else p64(ba), int(divisor), p64(q), p64(rem),
+                                 p64(y), _p64(yf)))
+    return q, rem, y, yf
+
+
 def _ef2(a):
     return _u64(a).reshape(-1, 2).copy()
 

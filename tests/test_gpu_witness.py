@@ -1,0 +1,49 @@
+"""proofsys' rescaled linear-layer witness on the GPU against the oracle (proofsys/src/tensor.rs,
+model.rs:360-361): q, rem, y and encode_i64(y) equal element for element at GPT-2's layer shapes
+and ragged ones, both operand layouts, host and device arrays, and the overflow error."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import ligesis_b200 as L
+from ligesis_b200 import proofsys as ps
+
+pytestmark = pytest.mark.gpu
+
+
+def _rand(seed, shape, bits):
+    g = np.random.default_rng(seed)
+    return g.integers(-(1 << bits), 1 << bits, size=shape, dtype=np.int64)
+
+
+@pytest.mark.parametrize("rows,inner,cols,wt", [(31, 768, 3072, False), (31, 3072, 768, False),
+                                                (31, 768, 2304, False), (5, 70, 33, False),
+                                                (31, 768, 4099, True), (1, 1, 1, True),
+                                                (67, 129, 65, True)])
+def test_linear_witness_matches_oracle(lgs, orc, rows, inner, cols, wt):
+    x = _rand(rows + inner, (rows, inner), 20)
+    w = _rand(cols + 1, (cols, inner) if wt else (inner, cols), 15)
+    b = _rand(cols + 2, cols, 30)
+    got = ps.linear_witness(x, w, b, 1 << 12, wt)
+    want = orc.linear_witness(x, w, b, 1 << 12, wt)
+    for g_, w_ in zip(got, want):
+        assert np.array_equal(g_, w_)
+    assert np.array_equal(got[3], ps.encode_i64(got[2]))
+
+
+def test_linear_witness_device_and_odd_divisor(lgs, orc):
+    torch = pytest.importorskip("torch")
+    x, w = _rand(1, (31, 768), 20), _rand(2, (768, 3072), 15)
+    want = orc.linear_witness(x, w, None, 4097)
+    got = ps.linear_witness(torch.from_numpy(x).cuda(), torch.from_numpy(w).cuda(), None, 4097)
+    for g_, w_ in zip(got, want):
+        assert np.array_equal(g_.cpu().numpy().view(w_.dtype), w_)
+
+
+def test_linear_witness_overflow_is_an_error(lgs):
+    big = np.full((2, 4), 1 << 40, dtype=np.int64)
+    with pytest.raises(L.ShapeError):
+        ps.linear_witness(big, big.T.copy(), None, 1)
+    with pytest.raises(L.ShapeError):
+        ps.linear_witness(big[:, :1], big[:1, :], None, 0)

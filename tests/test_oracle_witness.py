@@ -1,0 +1,58 @@
+"""The oracle's proofsys linear-layer witness (proofsys/src/tensor.rs:51-133, :194-216;
+witness.rs:102-108) against Python integers: i128-exact products, floor division with a
+non-negative remainder for negative values, the bias row, encode_i64, and the overflow check."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from ligesis_b200 import field as fld
+
+
+def _py(x, w, bias, d, wt):
+    rows, inner = x.shape
+    cols = w.shape[0] if wt else w.shape[1]
+    q = np.zeros((rows, cols), dtype=object)
+    r = np.zeros_like(q)
+    y = np.zeros_like(q)
+    for i in range(rows):
+        for j in range(cols):
+            acc = sum(int(x[i, k]) * int(w[j, k] if wt else w[k, j]) for k in range(inner))
+            qq = acc // d  # Python floors
+            q[i, j], r[i, j] = qq, acc - qq * d
+            y[i, j] = qq + (0 if bias is None else int(bias[j]))
+    return q, r, y
+
+
+@pytest.mark.parametrize("wt", [False, True])
+def test_linear_witness_matches_python(orc, wt):
+    g = np.random.default_rng(3)
+    x = g.integers(-(1 << 20), 1 << 20, size=(7, 33), dtype=np.int64)
+    w = g.integers(-(1 << 15), 1 << 15, size=(5, 33) if wt else (33, 5), dtype=np.int64)
+    b = g.integers(-(1 << 30), 1 << 30, size=5, dtype=np.int64)
+    q, r, y, yf = orc.linear_witness(x, w, b, 4096, wt)
+    wq, wr, wy = _py(x, w, b, 4096, wt)
+    assert (q == wq.astype(np.int64)).all() and (r == wr.astype(np.int64)).all()
+    assert (y == wy.astype(np.int64)).all()
+    assert (r >= 0).all() and (r < 4096).all() and (q < 0).any()
+    assert all(int(yf.flat[i]) == int(y.flat[i]) % fld.P for i in range(y.size))
+
+
+def test_linear_witness_edges(orc):
+    x = np.array([[-1, 0], [1 << 62, 1]], dtype=np.int64)
+    w = np.array([[1], [1]], dtype=np.int64)
+    q, r, y, yf = orc.linear_witness(x, w, None, 3)
+    assert q.ravel().tolist() == [-1, (1 << 62) // 3] and r.ravel().tolist() == [2, ((1 << 62) + 1) % 3]
+    assert int(yf[0, 0]) == fld.P - 1
+    big = np.array([[1 << 40]], dtype=np.int64)
+    with pytest.raises(Exception):
+        orc.linear_witness(big, big, None, 1)  # 2^80 does not fit an i64
+
+
+def test_encode_i64_mirror():
+    from ligesis_b200.proofsys import encode_i64
+
+    xs = np.array([0, 1, -1, 5, -5, (1 << 63) - 1, -(1 << 63), fld.P - 1 - (1 << 63)], dtype=object)
+    a = np.array([int(v) for v in xs], dtype=np.int64)
+    want = [int(v) % fld.P for v in a.tolist()]
+    assert encode_i64(a).tolist() == want
