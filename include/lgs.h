@@ -163,6 +163,16 @@ lgs_status lgs_linear_witness(lgs_ctx* ctx, const int64_t* x, size_t rows, size_
                               const int64_t* w, size_t cols, int w_transposed,
                               const int64_t* bias, int64_t divisor, int on_device, int64_t* q,
                               int64_t* rem, int64_t* y, uint64_t* y_field);
+/* layer_norm of the integer GPT-2 (model.rs:241-279): for each of `rows` rows of X (d columns),
+ * sum_x, sum_x2, var_sum = d sum_x2 - sum_x^2 and std = round_sqrt(var_sum + 1) (tensor.rs:
+ * 218-222); for each entry dividend = gain (d x - sum_x), quotient = floor(dividend / std),
+ * output = quotient + bias.  Per-row outputs hold rows values, per-entry ones rows x d.  A sum or
+ * a dividend outside the int64 range gives LGS_ERR_BAD_SHAPE. */
+lgs_status lgs_layer_norm_witness(lgs_ctx* ctx, const int64_t* x, size_t rows, size_t d,
+                                  const int64_t* gain, const int64_t* bias, int on_device,
+                                  int64_t* sum_x, int64_t* sum_x2, int64_t* var_sum,
+                                  int64_t* stdv, int64_t* dividend, int64_t* quotient,
+                                  int64_t* output);
 
 /* ---- batched and served proving (the reference proves one polynomial at a time on one
  * thread, pcs/benches/ligesis.rs:20-60) ----

@@ -428,6 +428,22 @@ lgs_status lgs_linear_witness(lgs_ctx* ctx, const int64_t* x, size_t rows, size_
   });
 }
 
+lgs_status lgs_layer_norm_witness(lgs_ctx* ctx, const int64_t* x, size_t rows, size_t d,
+                                  const int64_t* gain, const int64_t* bias, int on_device,
+                                  int64_t* sum_x, int64_t* sum_x2, int64_t* var_sum,
+                                  int64_t* stdv, int64_t* dividend, int64_t* quotient,
+                                  int64_t* output) {
+  return guarded([&] {
+    need(ctx && x && gain && bias && sum_x && sum_x2 && var_sum && stdv && dividend && quotient &&
+             output,
+         "lgs_layer_norm_witness: null argument");
+    CtxDevice dg(ctx);
+    int64_t* const rows_out[4] = {sum_x, sum_x2, var_sum, stdv};
+    int64_t* const ent_out[3] = {dividend, quotient, output};
+    layer_norm_witness_dev(ctx, x, rows, d, gain, bias, on_device != 0, rows_out, ent_out);
+  });
+}
+
 lgs_status lgs_basefold_verify(const uint8_t root[32], const uint64_t* point, size_t plen,
                                const uint8_t* proof, size_t proof_len, const uint64_t* fields,
                                size_t nfields, const uint64_t* ints, size_t nints,

@@ -361,6 +361,11 @@ int lookup_verify_host(const uint8_t* proof, size_t len, const u64* fields, size
 void linear_witness_dev(lgs_ctx* c, const int64_t* x, size_t rows, size_t inner, const int64_t* w,
                         size_t cols, bool w_transposed, const int64_t* bias, int64_t divisor,
                         bool on_device, int64_t* q, int64_t* rem, int64_t* y, uint64_t* y_field);
+// proofsys' layer-norm witness (witness.cu): per row sum_x, sum_x2, var_sum, std; per entry
+// dividend, quotient, output.
+void layer_norm_witness_dev(lgs_ctx* c, const int64_t* x, size_t rows, size_t d,
+                            const int64_t* gain, const int64_t* bias, bool on_device,
+                            int64_t* const per_row[4], int64_t* const per_entry[3]);
 lgs_status set_error(lgs_status s, const std::string& msg);
 lgs_status status_of_current_exception();
 }  // namespace lgs

@@ -160,6 +160,85 @@ __global__ void linear_witness_finish_kernel(const LwArgs a, unsigned nsplit) {
   if (bad) atomicOr(a.err, 1);
 }
 
+// layer_norm (proofsys/src/model.rs:241-279), one CTA per row: exact 128-bit sums of x and x^2,
+// vs = d sx2 - sx^2, std = round_sqrt(vs + 1) (the double square root rounded half away from zero,
+// tensor.rs:218-222; sqrt is correctly rounded on both sides), then per entry dividend =
+// gain (d x - sx), quotient = floor(dividend / std), output = quotient + bias.
+struct LnArgs {
+  const int64_t *x, *gain, *bias;
+  size_t rows, d;
+  int64_t *sum_x, *sum_x2, *var_sum, *stdv, *dividend, *quotient, *output;
+  int* err;
+};
+__device__ __forceinline__ __int128 as128(const Acc128& a) {
+  return (__int128)(((unsigned __int128)a.hi << 64) | a.lo);
+}
+__device__ __forceinline__ bool fits64(__int128 v) {
+  return v >= (__int128)INT64_MIN && v <= (__int128)INT64_MAX;
+}
+__global__ void __launch_bounds__(256) layer_norm_witness_kernel(const LnArgs a) {
+  __shared__ Acc128 red[2][256];
+  __shared__ int64_t s_sx, s_st;
+  __shared__ int s_ok;
+  const size_t r = blockIdx.x, d = a.d;
+  const int64_t* xr = a.x + r * d;
+  Acc128 s1{0, 0}, s2{0, 0};
+  for (size_t c = threadIdx.x; c < d; c += blockDim.x) {
+    const int64_t v = xr[c];
+    add128(s1, Acc128{(uint64_t)v, (uint64_t)(v >> 63)});
+    mac128(s2, v, v);
+  }
+  red[0][threadIdx.x] = s1;
+  red[1][threadIdx.x] = s2;
+  __syncthreads();
+  for (unsigned h = blockDim.x / 2; h; h >>= 1) {
+    if (threadIdx.x < h) {
+      add128(red[0][threadIdx.x], red[0][threadIdx.x + h]);
+      add128(red[1][threadIdx.x], red[1][threadIdx.x + h]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const __int128 sx = as128(red[0][0]), sx2 = as128(red[1][0]);
+    const __int128 vs = sx2 * (__int128)d - sx * sx;
+    int ok = fits64(sx) && fits64(sx2) && fits64(vs) && vs >= 0;
+    int64_t st = 1;
+    if (ok) {
+      const double root = sqrt((double)(unsigned long long)((uint64_t)(int64_t)vs + 1));
+      st = (int64_t)llround(root);
+      a.sum_x[r] = (int64_t)sx;
+      a.sum_x2[r] = (int64_t)sx2;
+      a.var_sum[r] = (int64_t)vs;
+      a.stdv[r] = st;
+    }
+    s_sx = ok ? (int64_t)sx : 0;
+    s_st = st;
+    s_ok = ok;
+  }
+  __syncthreads();
+  if (!s_ok) {
+    if (threadIdx.x == 0) atomicOr(a.err, 1);
+    return;
+  }
+  const int64_t sx = s_sx, st = s_st;
+  bool bad = false;
+  for (size_t c = threadIdx.x; c < d; c += blockDim.x) {
+    const __int128 av = (__int128)a.gain[c] * ((__int128)d * (__int128)xr[c] - (__int128)sx);
+    if (!fits64(av)) {  // the reference's checked dividend
+      bad = true;
+      continue;
+    }
+    const int64_t v = (int64_t)av;
+    int64_t q = v / st;
+    if (v % st < 0) q -= 1;
+    const size_t o = r * d + c;
+    a.dividend[o] = v;
+    a.quotient[o] = q;
+    a.output[o] = (int64_t)((uint64_t)q + (uint64_t)a.bias[c]);
+  }
+  if (bad) atomicOr(a.err, 1);
+}
+
 }  // namespace
 
 void linear_witness_dev(lgs_ctx* c, const int64_t* x, size_t rows, size_t inner, const int64_t* w,
@@ -229,6 +308,47 @@ void linear_witness_dev(lgs_ctx* c, const int64_t* x, size_t rows, size_t inner,
   }
   LGS_CUDA(cudaStreamSynchronize(st));
   if (herr) throw ShapeError("linear witness: a product or Q + bias leaves the i64 range");
+}
+
+}  // namespace lgs
+
+namespace lgs {
+
+void layer_norm_witness_dev(lgs_ctx* c, const int64_t* x, size_t rows, size_t d,
+                            const int64_t* gain, const int64_t* bias, bool on_device,
+                            int64_t* const per_row[4], int64_t* const per_entry[3]) {
+  if (rows == 0 || d == 0) throw ShapeError("layer norm witness: empty matrix");
+  if (rows > ((size_t)1 << 24) || d > ((size_t)1 << 24))
+    throw ShapeError("layer norm witness: matrix too large");
+  cudaStream_t st = c->st;
+  Arena& ar = c->arena;
+  ar.begin();
+  auto in = [&](const int64_t* h, size_t n) -> const int64_t* {
+    if (on_device) return h;
+    int64_t* dv = ar.get<int64_t>(n);
+    h2d_staged(c, dv, h, n * 8, st);
+    return dv;
+  };
+  int64_t* dr[4];
+  int64_t* de[3];
+  for (int i = 0; i < 4; ++i) dr[i] = on_device ? per_row[i] : ar.get<int64_t>(rows);
+  for (int i = 0; i < 3; ++i) de[i] = on_device ? per_entry[i] : ar.get<int64_t>(rows * d);
+  int* derr = ar.get<int>(1);
+  LGS_CUDA(cudaMemsetAsync(derr, 0, sizeof(int), st));
+  LnArgs a{in(x, rows * d), in(gain, d), in(bias, d), rows, d, dr[0], dr[1], dr[2], dr[3],
+           de[0], de[1], de[2], derr};
+  layer_norm_witness_kernel<<<(unsigned)rows, 256, 0, st>>>(a);
+  LGS_LAUNCH_CHECK();
+  int herr = 0;
+  LGS_CUDA(cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (!on_device) {
+    for (int i = 0; i < 4; ++i)
+      LGS_CUDA(cudaMemcpyAsync(per_row[i], dr[i], rows * 8, cudaMemcpyDeviceToHost, st));
+    for (int i = 0; i < 3; ++i)
+      LGS_CUDA(cudaMemcpyAsync(per_entry[i], de[i], rows * d * 8, cudaMemcpyDeviceToHost, st));
+  }
+  LGS_CUDA(cudaStreamSynchronize(st));
+  if (herr) throw ShapeError("layer norm witness: a sum, the variance or a dividend leaves the i64 range");
 }
 
 }  // namespace lgs

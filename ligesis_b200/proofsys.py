@@ -1,12 +1,14 @@
-"""proofsys' integer witness on the GPU: the rescaled linear layer of the integer GPT-2
-(proofsys/src/model.rs:360-361 with the Matrix kernels of proofsys/src/tensor.rs) over liblgs.so
-(`lgs_linear_witness` in include/lgs.h), and `encode_i64` (proofsys/src/witness.rs:102-108).
+"""proofsys' integer witness on the GPU, over liblgs.so (include/lgs.h):
 
-`linear_witness(x, w, bias, divisor)` returns (q, rem, y, y_field): q, rem =
-x.matmul(w).floor_div_const_with_rem(divisor), y = q.add_row_vector(bias), y_field =
-encode_i64(y) as canonical Goldilocks.  With w_transposed, x.matmul_transposed_rhs(w) (the
-vocabulary head, model.rs:225-228).  Arrays are int64 numpy arrays, or CUDA int64 tensors (then
-the outputs are CUDA tensors too).
+* `linear_witness(x, w, bias, divisor)`: the rescaled linear layer of the integer GPT-2
+  (proofsys/src/model.rs:360-374 with the Matrix kernels of proofsys/src/tensor.rs) ->
+  (q, rem, y, y_field): q, rem = x.matmul(w).floor_div_const_with_rem(divisor),
+  y = q.add_row_vector(bias), y_field = encode_i64(y) as canonical Goldilocks.  With
+  w_transposed, x.matmul_transposed_rhs(w) (the vocabulary head, model.rs:225-228).  int64 numpy
+  arrays, or CUDA int64 tensors (then the outputs are CUDA tensors too).
+* `layer_norm_witness(x, gain, bias)`: layer_norm (model.rs:241-279) -> (sum_x, sum_x2, var_sum,
+  std, dividend, quotient, output).
+* `encode_i64` (proofsys/src/witness.rs:102-108).
 """
 from __future__ import annotations
 
@@ -71,3 +73,21 @@ def linear_witness(x, w, bias, divisor: int, w_transposed: bool = False,
                                     int(w_transposed), None if ba is None else p(ba),
                                     int(divisor), 0, p(q), p(rem), p(y), ptr64(yf)))
     return q, rem, y, yf
+
+
+def layer_norm_witness(x, gain, bias, ctx: Context | None = None):
+    """layer_norm (proofsys/src/model.rs:241-279) on the GPU: (sum_x, sum_x2, var_sum, std,
+    dividend, quotient, output), the first four per row, the rest per entry.  Host int64 arrays."""
+    ctx = ctx or Context.default()
+    xa = np.ascontiguousarray(x, dtype=np.int64)
+    rows, d = xa.shape
+    ga = np.ascontiguousarray(gain, dtype=np.int64)
+    ba = np.ascontiguousarray(bias, dtype=np.int64)
+    if ga.shape != (d,) or ba.shape != (d,):
+        raise ValueError("layer norm witness: gain and bias hold one value per column")
+    per_row = [np.empty(rows, np.int64) for _ in range(4)]
+    per_ent = [np.empty((rows, d), np.int64) for _ in range(3)]
+    p = lambda a: a.ctypes.data_as(i64p)
+    check(load().lgs_layer_norm_witness(ctx.handle, p(xa), rows, d, p(ga), p(ba), 0,
+                                        *[p(a) for a in per_row + per_ent]))
+    return tuple(per_row + per_ent)

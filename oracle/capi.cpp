@@ -4,6 +4,7 @@
 //
 // Buffers: BF = u64, EF = two u64 (c0, c1).  Status: 0 = ok, negative = error (message in
 // orc_last_error()).
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -476,6 +477,26 @@ int orc_linear_witness(const int64_t* x, size_t rows, size_t inner, const int64_
       y[i] = lw.y[i];
       if (y_field) y_field[i] = encode_i64(lw.y[i]);
     }
+  });
+  return 0;
+}
+
+// proofsys' layer-norm witness (proofsys/src/model.rs:241-279); per-row outputs hold rows values,
+// per-entry outputs rows x d.
+int orc_layer_norm_witness(const int64_t* x, size_t rows, size_t d, const int64_t* gain,
+                           const int64_t* bias, int64_t* sum_x, int64_t* sum_x2, int64_t* var_sum,
+                           int64_t* stdv, int64_t* dividend, int64_t* quotient, int64_t* output) {
+  ORC_TRY({
+    const LayerNormWitness w = layer_norm_witness(std::vector<i64>(x, x + rows * d), rows, d,
+                                                  std::vector<i64>(gain, gain + d),
+                                                  std::vector<i64>(bias, bias + d));
+    std::copy(w.sum_x.begin(), w.sum_x.end(), sum_x);
+    std::copy(w.sum_x2.begin(), w.sum_x2.end(), sum_x2);
+    std::copy(w.var_sum.begin(), w.var_sum.end(), var_sum);
+    std::copy(w.stdv.begin(), w.stdv.end(), stdv);
+    std::copy(w.dividend.begin(), w.dividend.end(), dividend);
+    std::copy(w.quotient.begin(), w.quotient.end(), quotient);
+    std::copy(w.output.begin(), w.output.end(), output);
   });
   return 0;
 }

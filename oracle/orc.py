@@ -86,6 +86,8 @@ def lib():
                 "orc_linear_witness": (C.c_int, [i64p, C.c_size_t, C.c_size_t, i64p, C.c_size_t,
                                                  C.c_int, i64p, C.c_int64, i64p, i64p, i64p,
                                                  u64p]),
+                "orc_layer_norm_witness": (C.c_int, [i64p, C.c_size_t, C.c_size_t, i64p, i64p,
+                                                     i64p, i64p, i64p, i64p, i64p, i64p, i64p]),
                 "orc_lookup_verify": (C.c_int, [u8p, C.c_size_t, u64p, C.c_size_t, u64p, u64p,
                                                 C.c_size_t, u64p, C.c_size_t, u64p]),
             }
@@ -377,6 +379,20 @@ def linear_witness(x, w, bias, divisor: int, w_transposed: bool = False):
                                  None if ba is None else p64(ba), int(divisor), p64(q), p64(rem),
                                  p64(y), _p64(yf)))
     return q, rem, y, yf
+
+
+def layer_norm_witness(x, gain, bias):
+    """proofsys' layer_norm: (sum_x, sum_x2, var_sum, std, dividend, quotient, output)."""
+    xa = np.ascontiguousarray(x, dtype=np.int64)
+    rows, d = xa.shape
+    ga = np.ascontiguousarray(gain, dtype=np.int64)
+    ba = np.ascontiguousarray(bias, dtype=np.int64)
+    per_row = [np.zeros(rows, np.int64) for _ in range(4)]
+    per_ent = [np.zeros((rows, d), np.int64) for _ in range(3)]
+    p64 = lambda a: a.ctypes.data_as(i64p)
+    _ok(lib().orc_layer_norm_witness(p64(xa), rows, d, p64(ga), p64(ba),
+                                     *[p64(a) for a in per_row + per_ent]))
+    return tuple(per_row + per_ent)
 
 
 def _ef2(a):

@@ -1,9 +1,10 @@
 // ORACLE (test infrastructure only): a single-threaded CPU restatement of proofsys' integer
-// linear-layer witness (proofsys/src/tensor.rs, proofsys/src/witness.rs): the i128-accumulated
-// matrix products, floor division with remainder by a positive constant, the bias row and the
-// lift of an i64 into Goldilocks.  Only tests/, the smoke check and bench.py's CPU-baseline leg
+// linear-layer and layer-norm witnesses (proofsys/src/tensor.rs, model.rs, witness.rs): the
+// i128-accumulated matrix products, floor division with remainder by a positive constant, the
+// bias row, the rounded square root of the layer norm and the lift of an i64 into Goldilocks.  Only tests/, the smoke check and bench.py's CPU-baseline leg
 // load this code, and only as the checker; the product library never links it.
 #pragma once
+#include <cmath>
 #include <cstdint>
 #include <stdexcept>
 #include <vector>
@@ -67,6 +68,51 @@ inline LinearWitness linear_witness(const std::vector<i64>& x, size_t rows, size
       out.y[i * cols + j] = checked_i64(y);
     }
   return out;
+}
+
+// round_sqrt (tensor.rs:218-222): the f64 square root rounded half away from zero.
+inline i64 round_sqrt(i128 n) {
+  if (n < 0) throw std::runtime_error("round_sqrt: negative");
+  return checked_i64((i128)std::llround(std::sqrt((double)n)));
+}
+
+// layer_norm (proofsys/src/model.rs:241-279): per row sx, sx2, vs = d sx2 - sx^2, std =
+// round_sqrt(vs + 1); per entry dividend = gain (d x - sx), quotient = floor(dividend / std),
+// output = quotient + bias.
+struct LayerNormWitness {
+  std::vector<i64> sum_x, sum_x2, var_sum, stdv, dividend, quotient, output;
+};
+inline LayerNormWitness layer_norm_witness(const std::vector<i64>& x, size_t rows, size_t d,
+                                           const std::vector<i64>& gain,
+                                           const std::vector<i64>& bias) {
+  if (x.size() != rows * d || gain.size() != d || bias.size() != d)
+    throw std::runtime_error("layer_norm_witness: shapes");
+  LayerNormWitness w;
+  for (auto* v : {&w.sum_x, &w.sum_x2, &w.var_sum, &w.stdv}) v->resize(rows);
+  for (auto* v : {&w.dividend, &w.quotient, &w.output}) v->resize(rows * d);
+  const i128 dd = (i128)d;
+  for (size_t r = 0; r < rows; ++r) {
+    i128 sx = 0, sx2 = 0;
+    for (size_t c = 0; c < d; ++c) {
+      const i128 v = x[r * d + c];
+      sx += v;
+      sx2 += v * v;
+    }
+    const i128 vs = sx2 * dd - sx * sx;
+    const i64 st = round_sqrt(vs + 1);
+    w.sum_x[r] = checked_i64(sx);
+    w.sum_x2[r] = checked_i64(sx2);
+    w.var_sum[r] = checked_i64(vs);
+    w.stdv[r] = st;
+    for (size_t c = 0; c < d; ++c) {
+      const i128 a = (i128)gain[c] * (dd * (i128)x[r * d + c] - sx);
+      const i64 q = floor_div(a, (i128)st);
+      w.dividend[r * d + c] = checked_i64(a);
+      w.quotient[r * d + c] = q;
+      w.output[r * d + c] = q + bias[c];
+    }
+  }
+  return w;
 }
 
 }  // namespace orc

@@ -47,3 +47,22 @@ def test_linear_witness_overflow_is_an_error(lgs):
         ps.linear_witness(big, big.T.copy(), None, 1)
     with pytest.raises(L.ShapeError):
         ps.linear_witness(big[:, :1], big[:1, :], None, 0)
+
+
+@pytest.mark.parametrize("rows,d", [(31, 768), (1, 1), (3, 257), (64, 3072)])
+def test_layer_norm_witness_matches_oracle(lgs, orc, rows, d):
+    x = _rand(rows * 7 + d, (rows, d), 20)
+    gain = _rand(d + 3, d, 13)
+    bias = _rand(d + 4, d, 13)
+    got = ps.layer_norm_witness(x, gain, bias)
+    want = orc.layer_norm_witness(x, gain, bias)
+    for g_, w_ in zip(got, want):
+        assert np.array_equal(g_, w_)
+
+
+def test_layer_norm_witness_constant_row(lgs, orc):
+    x = np.full((2, 16), -12345, dtype=np.int64)  # zero variance: std = round_sqrt(1) = 1
+    got = ps.layer_norm_witness(x, np.ones(16, np.int64), np.zeros(16, np.int64))
+    assert got[3].tolist() == [1, 1] and not got[4].any()
+    for g_, w_ in zip(got, orc.layer_norm_witness(x, np.ones(16, np.int64), np.zeros(16, np.int64))):
+        assert np.array_equal(g_, w_)

@@ -56,3 +56,25 @@ def test_encode_i64_mirror():
     a = np.array([int(v) for v in xs], dtype=np.int64)
     want = [int(v) % fld.P for v in a.tolist()]
     assert encode_i64(a).tolist() == want
+
+
+def test_layer_norm_witness_matches_python(orc):
+    import math
+
+    g = np.random.default_rng(5)
+    x = g.integers(-(1 << 20), 1 << 20, size=(4, 48), dtype=np.int64)
+    gain = g.integers(-(1 << 13), 1 << 13, size=48, dtype=np.int64)
+    bias = g.integers(-(1 << 13), 1 << 13, size=48, dtype=np.int64)
+    sx, sx2, vs, st, dv, qu, out = orc.layer_norm_witness(x, gain, bias)
+    d = 48
+    for r in range(4):
+        row = [int(v) for v in x[r]]
+        s1, s2 = sum(row), sum(v * v for v in row)
+        v = s2 * d - s1 * s1
+        root = math.sqrt(float(v + 1))
+        rs = math.floor(root + 0.5)  # half away from zero for a non-negative value
+        assert (int(sx[r]), int(sx2[r]), int(vs[r]), int(st[r])) == (s1, s2, v, rs)
+        for c in range(d):
+            a = int(gain[c]) * (d * row[c] - s1)
+            assert int(dv[r, c]) == a and int(qu[r, c]) == a // rs
+            assert int(out[r, c]) == a // rs + int(bias[c])
