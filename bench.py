@@ -820,6 +820,16 @@ def run_witness(args) -> None:
         out[name] = res
     forward = 12 * sum(out[k]["device_ms"] for k in ("qkv", "attn_proj", "fc", "fproj")) \
         + out["vocab_head"]["device_ms"]
+    # one whole block's witness (layer norms, attention with 12 heads, softmax, MLP, GELU
+    # lookup), host arrays in and out, every step on the GPU
+    bcfg = dict(cfg, n_head=12)
+    bx, bw, bel, bgl = ps.synthetic_block(12, bcfg)
+    for _ in range(args.warmup):
+        ps.block_witness(bx, bw, bel, bgl, bcfg, ctx)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ps.block_witness(bx, bw, bel, bgl, bcfg, ctx)
+    block_ms = round((time.perf_counter() - t0) / args.steps * 1e3, 3)
     cpu = None
     if not args.no_cpu_baseline:
         from oracle import orc
@@ -828,11 +838,15 @@ def run_witness(args) -> None:
         w = g.integers(-(1 << 15), 1 << 15, size=(d, h), dtype=np.int64)
         t0 = time.perf_counter()
         orc.linear_witness(x, w, None, sc)
-        cpu = {"layer": "fc", "ms": round((time.perf_counter() - t0) * 1e3, 1), "cores": 1,
-               "kind": "port", "cpu": _cpu_model()}
+        t1 = time.perf_counter()
+        orc.block_witness(bx, bw, bel, bgl, bcfg)
+        t2 = time.perf_counter()
+        cpu = {"fc_ms": round((t1 - t0) * 1e3, 1), "block_ms": round((t2 - t1) * 1e3, 1),
+               "cores": 1, "kind": "port", "cpu": _cpu_model()}
     print(json.dumps({"mode": "witness", "config": "gpt2_31", "steps": args.steps,
                       "timing": "host wall clock per call", "layers": out,
-                      "forward_linear_device_ms": round(forward, 3), "cpu_oracle": cpu}),
+                      "forward_linear_device_ms": round(forward, 3),
+                      "block_witness_host_arrays_ms": block_ms, "cpu_oracle": cpu}),
           flush=True)
 
 

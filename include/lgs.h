@@ -173,6 +173,19 @@ lgs_status lgs_layer_norm_witness(lgs_ctx* ctx, const int64_t* x, size_t rows, s
                                   int64_t* sum_x, int64_t* sum_x2, int64_t* var_sum,
                                   int64_t* stdv, int64_t* dividend, int64_t* quotient,
                                   int64_t* output);
+/* softmax of the integer GPT-2 attention (model.rs:409-443), causal, for `heads` score matrices
+ * of n x n (heads x n x n, row-major): x_max[h][i] = max_{j <= i} s, exp[h][i][j] =
+ * exp_lut[s - x_max + offset] and prob[h][i][j] = floor(exp scale / sum_exp) for j <= i (zero
+ * above the diagonal), sum_exp[h][i] = sum_j exp.  An index outside the table or a zero sum gives
+ * LGS_ERR_BAD_SHAPE (the reference asserts). */
+lgs_status lgs_softmax_witness(lgs_ctx* ctx, const int64_t* scores, unsigned heads, unsigned n,
+                               const int64_t* exp_lut, size_t lut_len, int64_t offset,
+                               int64_t scale, int on_device, int64_t* x_max, int64_t* exp,
+                               int64_t* sum_exp, int64_t* prob);
+/* out[i] = lut[v[i] + offset], the GELU activation of the MLP (model.rs:362-373); an index
+ * outside the table gives LGS_ERR_BAD_SHAPE. */
+lgs_status lgs_lut_gather(lgs_ctx* ctx, const int64_t* v, size_t count, const int64_t* lut,
+                          size_t lut_len, int64_t offset, int on_device, int64_t* out);
 
 /* ---- batched and served proving (the reference proves one polynomial at a time on one
  * thread, pcs/benches/ligesis.rs:20-60) ----

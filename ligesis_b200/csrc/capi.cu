@@ -444,6 +444,28 @@ lgs_status lgs_layer_norm_witness(lgs_ctx* ctx, const int64_t* x, size_t rows, s
   });
 }
 
+lgs_status lgs_softmax_witness(lgs_ctx* ctx, const int64_t* scores, unsigned heads, unsigned n,
+                               const int64_t* exp_lut, size_t lut_len, int64_t offset,
+                               int64_t scale, int on_device, int64_t* x_max, int64_t* exp,
+                               int64_t* sum_exp, int64_t* prob) {
+  return guarded([&] {
+    need(ctx && scores && exp_lut && x_max && exp && sum_exp && prob,
+         "lgs_softmax_witness: null argument");
+    CtxDevice dg(ctx);
+    softmax_witness_dev(ctx, scores, heads, n, exp_lut, lut_len, offset, scale, on_device != 0,
+                        x_max, exp, sum_exp, prob);
+  });
+}
+
+lgs_status lgs_lut_gather(lgs_ctx* ctx, const int64_t* v, size_t count, const int64_t* lut,
+                          size_t lut_len, int64_t offset, int on_device, int64_t* out) {
+  return guarded([&] {
+    need(ctx && v && lut && out, "lgs_lut_gather: null argument");
+    CtxDevice dg(ctx);
+    lut_gather_dev(ctx, v, count, lut, lut_len, offset, on_device != 0, out);
+  });
+}
+
 lgs_status lgs_basefold_verify(const uint8_t root[32], const uint64_t* point, size_t plen,
                                const uint8_t* proof, size_t proof_len, const uint64_t* fields,
                                size_t nfields, const uint64_t* ints, size_t nints,

@@ -366,6 +366,13 @@ void linear_witness_dev(lgs_ctx* c, const int64_t* x, size_t rows, size_t inner,
 void layer_norm_witness_dev(lgs_ctx* c, const int64_t* x, size_t rows, size_t d,
                             const int64_t* gain, const int64_t* bias, bool on_device,
                             int64_t* const per_row[4], int64_t* const per_entry[3]);
+// proofsys' causal softmax witness and lookup gather (witness.cu).
+void softmax_witness_dev(lgs_ctx* c, const int64_t* scores, unsigned heads, unsigned n,
+                         const int64_t* lut, size_t lut_len, int64_t offset, int64_t scale,
+                         bool on_device, int64_t* x_max, int64_t* ex, int64_t* sum_exp,
+                         int64_t* prob);
+void lut_gather_dev(lgs_ctx* c, const int64_t* v, size_t count, const int64_t* lut,
+                    size_t lut_len, int64_t offset, bool on_device, int64_t* out);
 lgs_status set_error(lgs_status s, const std::string& msg);
 lgs_status status_of_current_exception();
 }  // namespace lgs

@@ -352,3 +352,142 @@ void layer_norm_witness_dev(lgs_ctx* c, const int64_t* x, size_t rows, size_t d,
 }
 
 }  // namespace lgs
+
+// ---- softmax and lookup gathers of the integer GPT-2 (proofsys/src/model.rs:362-373, 409-443) ----
+namespace lgs {
+
+namespace {
+
+// softmax (model.rs:409-443), causal: for head h and row i, x_max = max_{j <= i} s[i][j],
+// exp[i][j] = exp_lut[s[i][j] - x_max + offset] and prob[i][j] = floor(exp[i][j] scale / sum)
+// for j <= i (zero above the diagonal), sum_exp = sum_j exp[i][j].  One thread per (head, row).
+__global__ void softmax_witness_kernel(const int64_t* __restrict__ s, unsigned heads, unsigned n,
+                                       const int64_t* __restrict__ lut, size_t lut_len,
+                                       int64_t offset, int64_t scale, int64_t* __restrict__ x_max,
+                                       int64_t* __restrict__ ex, int64_t* __restrict__ sum_exp,
+                                       int64_t* __restrict__ prob, int* __restrict__ err) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)heads * n) return;
+  const size_t i = t % n, base = t * n;  // row i of head t / n: s[base + j]
+  int64_t mx = s[base];
+  for (size_t j = 1; j <= i; ++j) mx = max(mx, s[base + j]);
+  x_max[t] = mx;
+  int64_t sum = 0;
+  bool bad = false;
+  for (size_t j = 0; j < n; ++j) {
+    int64_t e = 0;
+    if (j <= i) {
+      const int64_t idx = s[base + j] - mx + offset;
+      if (idx < 0 || (uint64_t)idx >= lut_len) {
+        bad = true;
+      } else {
+        e = lut[idx];
+        sum += e;
+      }
+    }
+    ex[base + j] = e;
+  }
+  sum_exp[t] = sum;
+  if (sum <= 0) bad = true;  // the reference's floor_div_i128 asserts a positive divisor
+  for (size_t j = 0; j < n; ++j) {
+    int64_t p = 0;
+    if (j <= i && !bad) {
+      const __int128 a = (__int128)ex[base + j] * scale;
+      __int128 q = a / sum;
+      if (a % sum < 0) q -= 1;
+      if (q < (__int128)INT64_MIN || q > (__int128)INT64_MAX) bad = true;
+      p = (int64_t)q;
+    }
+    prob[base + j] = p;
+  }
+  if (bad) atomicOr(err, 1);
+}
+
+// out[i] = lut[v[i] + offset] (the GELU activation, model.rs:362-373).
+__global__ void lut_gather_kernel(const int64_t* __restrict__ v, size_t count,
+                                  const int64_t* __restrict__ lut, size_t lut_len, int64_t offset,
+                                  int64_t* __restrict__ out, int* __restrict__ err) {
+  bool bad = false;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int64_t idx = v[i] + offset;
+    if (idx < 0 || (uint64_t)idx >= lut_len) {
+      bad = true;
+      out[i] = 0;
+    } else {
+      out[i] = lut[idx];
+    }
+  }
+  if (bad) atomicOr(err, 1);
+}
+
+// Uploads host arrays (or passes device ones), runs `launch`, reads the outputs back.
+template <class F>
+void run_small(lgs_ctx* c, bool on_device, std::initializer_list<std::pair<const int64_t*, size_t>> ins,
+               std::initializer_list<std::pair<int64_t*, size_t>> outs, const char* what,
+               F&& launch) {
+  cudaStream_t st = c->st;
+  Arena& ar = c->arena;
+  ar.begin();
+  std::vector<const int64_t*> din;
+  for (auto& p : ins) {
+    if (on_device) {
+      din.push_back(p.first);
+    } else {
+      int64_t* d = ar.get<int64_t>(p.second);
+      h2d_staged(c, d, p.first, p.second * 8, st);
+      din.push_back(d);
+    }
+  }
+  std::vector<int64_t*> dout;
+  for (auto& p : outs) dout.push_back(on_device ? p.first : ar.get<int64_t>(p.second));
+  int* derr = ar.get<int>(1);
+  LGS_CUDA(cudaMemsetAsync(derr, 0, sizeof(int), st));
+  launch(din, dout, derr);
+  int herr = 0;
+  LGS_CUDA(cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (!on_device) {
+    size_t k = 0;
+    for (auto& p : outs) {
+      LGS_CUDA(cudaMemcpyAsync(p.first, dout[k], p.second * 8, cudaMemcpyDeviceToHost, st));
+      ++k;
+    }
+  }
+  LGS_CUDA(cudaStreamSynchronize(st));
+  if (herr) throw ShapeError(what);
+}
+
+}  // namespace
+
+void softmax_witness_dev(lgs_ctx* c, const int64_t* scores, unsigned heads, unsigned n,
+                         const int64_t* lut, size_t lut_len, int64_t offset, int64_t scale,
+                         bool on_device, int64_t* x_max, int64_t* ex, int64_t* sum_exp,
+                         int64_t* prob) {
+  if (heads == 0 || n == 0 || lut_len == 0) throw ShapeError("softmax witness: empty input");
+  if ((size_t)heads * n > ((size_t)1 << 24) || n > 65536) throw ShapeError("softmax witness: too large");
+  const size_t hn = (size_t)heads * n, hnn = hn * n;
+  run_small(c, on_device, {{scores, hnn}, {lut, lut_len}},
+            {{x_max, hn}, {ex, hnn}, {sum_exp, hn}, {prob, hnn}},
+            "softmax witness: an exp index outside the table, or a zero sum",
+            [&](const std::vector<const int64_t*>& in, const std::vector<int64_t*>& out, int* err) {
+              softmax_witness_kernel<<<(unsigned)((hn + 127) / 128), 128, 0, c->st>>>(
+                  in[0], heads, n, in[1], lut_len, offset, scale, out[0], out[1], out[2], out[3],
+                  err);
+              LGS_LAUNCH_CHECK();
+            });
+}
+
+void lut_gather_dev(lgs_ctx* c, const int64_t* v, size_t count, const int64_t* lut,
+                    size_t lut_len, int64_t offset, bool on_device, int64_t* out) {
+  if (count == 0 || lut_len == 0) throw ShapeError("lookup gather: empty input");
+  run_small(c, on_device, {{v, count}, {lut, lut_len}}, {{out, count}},
+            "lookup gather: an index outside the table",
+            [&](const std::vector<const int64_t*>& in, const std::vector<int64_t*>& o, int* err) {
+              const unsigned blocks = (unsigned)std::min<size_t>((count + 255) / 256, 148 * 8);
+              lut_gather_kernel<<<blocks, 256, 0, c->st>>>(in[0], count, in[1], lut_len, offset,
+                                                           o[0], err);
+              LGS_LAUNCH_CHECK();
+            });
+}
+
+}  // namespace lgs

@@ -8,6 +8,10 @@
   arrays, or CUDA int64 tensors (then the outputs are CUDA tensors too).
 * `layer_norm_witness(x, gain, bias)`: layer_norm (model.rs:241-279) -> (sum_x, sum_x2, var_sum,
   std, dividend, quotient, output).
+* `softmax_witness`, `lut_gather`: the attention's causal softmax with its exp table and the
+  MLP's GELU table (model.rs:409-443, :362-373).
+* `block_witness`, `forward_witness`: one block's and the whole forward's witness
+  (model.rs:208-237), every step on the GPU.
 * `encode_i64` (proofsys/src/witness.rs:102-108).
 """
 from __future__ import annotations
@@ -91,3 +95,136 @@ def layer_norm_witness(x, gain, bias, ctx: Context | None = None):
     check(load().lgs_layer_norm_witness(ctx.handle, p(xa), rows, d, p(ga), p(ba), 0,
                                         *[p(a) for a in per_row + per_ent]))
     return tuple(per_row + per_ent)
+
+
+def _call_small(fn, *args):
+    check(fn(*args))
+
+
+def softmax_witness(scores, exp_lut, offset: int, scale: int, ctx: Context | None = None):
+    """The causal softmax of the integer GPT-2 (model.rs:409-443) over heads x n x n scores:
+    (x_max (heads, n), exp (heads, n, n), sum_exp (heads, n), prob (heads, n, n))."""
+    ctx = ctx or Context.default()
+    s = np.ascontiguousarray(scores, dtype=np.int64)
+    if s.ndim == 2:
+        s = s[None]
+    heads, n, n2 = s.shape
+    if n != n2:
+        raise ValueError("softmax witness: square score matrices")
+    lut = np.ascontiguousarray(exp_lut, dtype=np.int64)
+    xm, se = np.empty((heads, n), np.int64), np.empty((heads, n), np.int64)
+    ex, pr = np.empty((heads, n, n), np.int64), np.empty((heads, n, n), np.int64)
+    p = lambda a: a.ctypes.data_as(i64p)
+    check(load().lgs_softmax_witness(ctx.handle, p(s), heads, n, p(lut), lut.size, int(offset),
+                                     int(scale), 0, p(xm), p(ex), p(se), p(pr)))
+    return xm, ex, se, pr
+
+
+def lut_gather(v, lut, offset: int, ctx: Context | None = None):
+    """lut[v + offset] elementwise (the GELU activation, model.rs:362-373)."""
+    ctx = ctx or Context.default()
+    va = np.ascontiguousarray(v, dtype=np.int64)
+    la = np.ascontiguousarray(lut, dtype=np.int64)
+    out = np.empty_like(va)
+    p = lambda a: a.ctypes.data_as(i64p)
+    check(load().lgs_lut_gather(ctx.handle, p(va), va.size, p(la), la.size, int(offset), 0,
+                                p(out)))
+    return out
+
+
+# The fields of one block's witness (BlockWitness of proofsys/src/witness.rs: ln1, attention, ln2,
+# mlp), in the order block_witness returns them.
+LN_FIELDS = ("sum_x", "sum_x2", "var_sum", "std", "dividend", "quotient", "output")
+ATTN_FIELDS = ("q_qkv", "qkv", "scores", "x_max", "exp", "sum_exp", "q_prob", "q_ao_heads",
+               "q_ao", "q_apr", "x_out", "rem_qkv", "rem_sc", "rem_ao_heads", "rem_apr")
+MLP_FIELDS = ("q_fc", "fc", "act", "q_fpr", "x_out", "rem_fc", "rem_fpr")
+BLOCK_FIELDS = (tuple("ln1." + f for f in LN_FIELDS) + tuple("attn." + f for f in ATTN_FIELDS)
+                + tuple("ln2." + f for f in LN_FIELDS) + tuple("mlp." + f for f in MLP_FIELDS))
+WEIGHT_NAMES = ("ln_1_g", "ln_1_b", "attn_w", "attn_b", "attn_proj_w", "attn_proj_b", "ln_2_g",
+                "ln_2_b", "fc_w", "fc_b", "fproj_w", "fproj_b")
+
+
+def block_witness(x, w: dict, exp_lut, gelu_lut, cfg: dict = GPT2_31,
+                  ctx: Context | None = None) -> dict:
+    """One block of the integer GPT-2 forward (model.rs:213-221): ln1, attention (qkv, per-head
+    scores, softmax, weighted values, projection, residual), ln2 and the MLP (fc, GELU lookup,
+    projection, residual), every step on the GPU.  `w` holds WEIGHT_NAMES (matrices row-major:
+    attn_w d x 3d, attn_proj_w d x d, fc_w d x hidden, fproj_w hidden x d).  Returns the witness
+    keyed by BLOCK_FIELDS."""
+    n, d = cfg["n_seq"], cfg["d_model"]
+    H = cfg.get("n_head", 12)
+    dh = d // H
+    sc = cfg["scale"]
+    sqrt_d_scale = sc * int(round(dh ** 0.5))  # Config::sqrt_d_scale (witness.rs:33-35)
+    offset = cfg["max_v"] * sc
+    x = np.ascontiguousarray(x, dtype=np.int64)
+    out = {}
+    ln1 = layer_norm_witness(x, w["ln_1_g"], w["ln_1_b"], ctx)
+    out.update({"ln1." + f: v for f, v in zip(LN_FIELDS, ln1)})
+    q_qkv, rem_qkv, qkv, _ = linear_witness(ln1[6], w["attn_w"], w["attn_b"], sc, False, ctx)
+    qh = qkv[:, :d].reshape(n, H, dh).transpose(1, 0, 2)
+    kh = qkv[:, d:2 * d].reshape(n, H, dh).transpose(1, 0, 2)
+    vh = qkv[:, 2 * d:].reshape(n, H, dh).transpose(1, 0, 2)
+    scores = np.empty((H, n, n), np.int64)
+    rem_sc = np.empty_like(scores)
+    for h in range(H):
+        scores[h], rem_sc[h], _, _ = linear_witness(qh[h], kh[h], None, sqrt_d_scale, True, ctx)
+    xm, ex, se, prob = softmax_witness(scores, exp_lut, offset, sc, ctx)
+    aoh = np.empty((H, n, dh), np.int64)
+    rao = np.empty_like(aoh)
+    for h in range(H):
+        aoh[h], rao[h], _, _ = linear_witness(prob[h], vh[h], None, sc, False, ctx)
+    merged = np.ascontiguousarray(aoh.transpose(1, 0, 2).reshape(n, d))
+    q_apr, rem_apr, proj, _ = linear_witness(merged, w["attn_proj_w"], w["attn_proj_b"], sc,
+                                             False, ctx)
+    attn_out = x + proj
+    vals = (q_qkv, qkv, scores, xm, ex, se, prob, aoh, merged, q_apr, attn_out, rem_qkv, rem_sc,
+            rao, rem_apr)
+    out.update({"attn." + f: v for f, v in zip(ATTN_FIELDS, vals)})
+    ln2 = layer_norm_witness(attn_out, w["ln_2_g"], w["ln_2_b"], ctx)
+    out.update({"ln2." + f: v for f, v in zip(LN_FIELDS, ln2)})
+    q_fc, rem_fc, fc, _ = linear_witness(ln2[6], w["fc_w"], w["fc_b"], sc, False, ctx)
+    act = lut_gather(fc, gelu_lut, offset, ctx)
+    q_fpr, rem_fpr, fpr, _ = linear_witness(act, w["fproj_w"], w["fproj_b"], sc, False, ctx)
+    vals = (q_fc, fc, act, q_fpr, attn_out + fpr, rem_fc, rem_fpr)
+    out.update({"mlp." + f: v for f, v in zip(MLP_FIELDS, vals)})
+    return out
+
+
+def synthetic_block(seed: int, cfg: dict = GPT2_31):
+    """Seeded weights, lookup tables and input for one block, sized so that every lookup index
+    stays inside its table (no exported model here): x ~ +-2^18, gains ~ scale / 32, matrix entries
+    ~ +-2^6, biases ~ +-2^10; exp table positive and decreasing toward small indices, GELU table
+    increasing."""
+    g = np.random.default_rng(seed)
+    n, d, hid, sc = cfg["n_seq"], cfg["d_model"], cfg["mlp_hidden"], cfg["scale"]
+    r = lambda shape, b: g.integers(-(1 << b), 1 << b, size=shape, dtype=np.int64)
+    w = {"ln_1_g": g.integers(sc // 48, sc // 24, size=d, dtype=np.int64), "ln_1_b": r(d, 10),
+         "attn_w": r((d, 3 * d), 6), "attn_b": r(3 * d, 10), "attn_proj_w": r((d, d), 6),
+         "attn_proj_b": r(d, 10), "ln_2_g": g.integers(sc // 48, sc // 24, size=d, dtype=np.int64),
+         "ln_2_b": r(d, 10), "fc_w": r((d, hid), 6), "fc_b": r(hid, 10), "fproj_w": r((hid, d), 6),
+         "fproj_b": r(d, 10)}
+    off = cfg["max_v"] * sc
+    idx = np.arange(off + 1, dtype=np.float64)
+    exp_lut = np.maximum(1, np.round(sc * np.exp((idx - off) / sc))).astype(np.int64)
+    gidx = np.arange(2 * off + 1, dtype=np.float64) - off
+    gelu_lut = np.round(np.maximum(gidx, 0) + gidx / 64).astype(np.int64)
+    return r((n, d), 18), w, exp_lut, gelu_lut
+
+
+def forward_witness(x0, blocks, ln_f_g, ln_f_b, wte, exp_lut, gelu_lut, cfg: dict = GPT2_31,
+                    ctx: Context | None = None) -> dict:
+    """The integer GPT-2 forward's witness (proofsys/src/model.rs:208-237) on the GPU: every
+    block's witness (`block_witness`, each block's input the previous mlp.x_out), the final
+    layer norm, and the vocabulary head q_log, rem_log = floor_div(lnf.output wteᵀ, scale).
+    Returns {"blocks": [block dicts], "lnf": 7 layer-norm arrays, "q_log", "rem_log"}."""
+    x = np.ascontiguousarray(x0, dtype=np.int64)
+    out = {"blocks": []}
+    for w in blocks:
+        b = block_witness(x, w, exp_lut, gelu_lut, cfg, ctx)
+        out["blocks"].append(b)
+        x = b["mlp.x_out"]
+    out["lnf"] = layer_norm_witness(x, ln_f_g, ln_f_b, ctx)
+    q, rem, _, _ = linear_witness(out["lnf"][6], wte, None, cfg["scale"], True, ctx)
+    out["q_log"], out["rem_log"] = q, rem
+    return out

@@ -500,4 +500,26 @@ int orc_layer_norm_witness(const int64_t* x, size_t rows, size_t d, const int64_
   });
   return 0;
 }
+
+// One GPT-2 block's witness (see block_witness): dims = n, d, heads, d_head, hidden; consts =
+// scale, sqrt_d_scale, offset; weights in BlockWeights order; out receives the 36 arrays.
+int orc_block_witness(const int64_t* x, const uint64_t* dims, const int64_t* consts,
+                      const int64_t* const* weights, const int64_t* exp_lut, size_t exp_len,
+                      const int64_t* gelu_lut, size_t gelu_len, int64_t* const* out) {
+  ORC_TRY({
+    GptDims g{dims[0], dims[1], dims[2], dims[3], dims[4], consts[0], consts[1], consts[2]};
+    const size_t n = g.n, d = g.d, hid = g.hidden;
+    const size_t sizes[12] = {d, d, d * 3 * d, 3 * d, d * d, d, d, d, d * hid, hid, hid * d, d};
+    BlockWeights w;
+    std::vector<i64>* fields[12] = {&w.ln1_g, &w.ln1_b, &w.attn_w, &w.attn_b, &w.proj_w,
+                                    &w.proj_b, &w.ln2_g, &w.ln2_b, &w.fc_w, &w.fc_b, &w.fproj_w,
+                                    &w.fproj_b};
+    for (int i = 0; i < 12; ++i) fields[i]->assign(weights[i], weights[i] + sizes[i]);
+    const auto res = block_witness(std::vector<i64>(x, x + n * d), g, w,
+                                   std::vector<i64>(exp_lut, exp_lut + exp_len),
+                                   std::vector<i64>(gelu_lut, gelu_lut + gelu_len));
+    for (size_t i = 0; i < res.size(); ++i) std::copy(res[i].begin(), res[i].end(), out[i]);
+  });
+  return 0;
+}
 }  // extern "C"

@@ -88,6 +88,8 @@ def lib():
                                                  u64p]),
                 "orc_layer_norm_witness": (C.c_int, [i64p, C.c_size_t, C.c_size_t, i64p, i64p,
                                                      i64p, i64p, i64p, i64p, i64p, i64p, i64p]),
+                "orc_block_witness": (C.c_int, [i64p, u64p, i64p, C.POINTER(i64p), i64p,
+                                                C.c_size_t, i64p, C.c_size_t, C.POINTER(i64p)]),
                 "orc_lookup_verify": (C.c_int, [u8p, C.c_size_t, u64p, C.c_size_t, u64p, u64p,
                                                 C.c_size_t, u64p, C.c_size_t, u64p]),
             }
@@ -393,6 +395,53 @@ def layer_norm_witness(x, gain, bias):
     _ok(lib().orc_layer_norm_witness(p64(xa), rows, d, p64(ga), p64(ba),
                                      *[p64(a) for a in per_row + per_ent]))
     return tuple(per_row + per_ent)
+
+
+def block_witness(x, w: dict, exp_lut, gelu_lut, cfg: dict) -> dict:
+    """One GPT-2 block's witness (proofsys/src/model.rs:213-443) on the CPU, keyed like
+    ligesis_b200.proofsys.block_witness."""
+    from ligesis_b200 import proofsys as ps
+
+    n, d, hid = cfg["n_seq"], cfg["d_model"], cfg["mlp_hidden"]
+    H = cfg.get("n_head", 12)
+    dh = d // H
+    sc = cfg["scale"]
+    dims = np.array([n, d, H, dh, hid], dtype=np.uint64)
+    consts = np.array([sc, sc * int(round(dh ** 0.5)), cfg["max_v"] * sc], dtype=np.int64)
+    ws = [np.ascontiguousarray(w[k], dtype=np.int64).ravel() for k in ps.WEIGHT_NAMES]
+    shapes = {"ln": [(n,)] * 4 + [(n, d)] * 3,
+              "attn": [(n, 3 * d), (n, 3 * d), (H, n, n), (H, n), (H, n, n), (H, n), (H, n, n),
+                       (H, n, dh), (n, d), (n, d), (n, d), (n, 3 * d), (H, n, n), (H, n, dh),
+                       (n, d)],
+              "mlp": [(n, hid), (n, hid), (n, hid), (n, d), (n, d), (n, hid), (n, d)]}
+    outs = ([np.zeros(s, np.int64) for s in shapes["ln"]] +
+            [np.zeros(s, np.int64) for s in shapes["attn"]] +
+            [np.zeros(s, np.int64) for s in shapes["ln"]] +
+            [np.zeros(s, np.int64) for s in shapes["mlp"]])
+    xa = np.ascontiguousarray(x, dtype=np.int64)
+    el = np.ascontiguousarray(exp_lut, dtype=np.int64)
+    gl = np.ascontiguousarray(gelu_lut, dtype=np.int64)
+    p64 = lambda a: a.ctypes.data_as(i64p)
+    wptr = (i64p * 12)(*[p64(a) for a in ws])
+    optr = (i64p * len(outs))(*[p64(a) for a in outs])
+    _ok(lib().orc_block_witness(p64(xa), _p64(dims), p64(consts), wptr, p64(el), el.size,
+                                p64(gl), gl.size, optr))
+    return dict(zip(ps.BLOCK_FIELDS, outs))
+
+
+def forward_witness(x0, blocks, ln_f_g, ln_f_b, wte, exp_lut, gelu_lut, cfg: dict) -> dict:
+    """The integer GPT-2 forward's witness (proofsys/src/model.rs:208-237) from the oracle's
+    blocks, layer norm and linear layer, keyed like ligesis_b200.proofsys.forward_witness."""
+    x = np.ascontiguousarray(x0, dtype=np.int64)
+    out = {"blocks": []}
+    for w in blocks:
+        b = block_witness(x, w, exp_lut, gelu_lut, cfg)
+        out["blocks"].append(b)
+        x = b["mlp.x_out"]
+    out["lnf"] = layer_norm_witness(x, ln_f_g, ln_f_b)
+    q, rem, _, _ = linear_witness(out["lnf"][6], wte, None, cfg["scale"], True)
+    out["q_log"], out["rem_log"] = q, rem
+    return out
 
 
 def _ef2(a):

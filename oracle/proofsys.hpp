@@ -4,8 +4,10 @@
 // bias row, the rounded square root of the layer norm and the lift of an i64 into Goldilocks.  Only tests/, the smoke check and bench.py's CPU-baseline leg
 // load this code, and only as the checker; the product library never links it.
 #pragma once
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <initializer_list>
 #include <stdexcept>
 #include <vector>
 
@@ -113,6 +115,105 @@ inline LayerNormWitness layer_norm_witness(const std::vector<i64>& x, size_t row
     }
   }
   return w;
+}
+
+// softmax (proofsys/src/model.rs:409-443) of one n x n score matrix, causal.
+inline void softmax_witness(const std::vector<i64>& sc, size_t n, const std::vector<i64>& lut,
+                            i64 offset, i64 scale, i64* xm, i64* ex, i64* se, i64* pr) {
+  for (size_t i = 0; i < n; ++i) {
+    i64 mx = sc[i * n];
+    for (size_t j = 1; j <= i; ++j) mx = std::max(mx, sc[i * n + j]);
+    xm[i] = mx;
+    i64 sum = 0;
+    for (size_t j = 0; j < n; ++j) ex[i * n + j] = 0;
+    for (size_t j = 0; j <= i; ++j) {
+      const i64 idx = sc[i * n + j] - mx + offset;
+      if (idx < 0 || (size_t)idx >= lut.size()) throw std::runtime_error("EXP index out of range");
+      ex[i * n + j] = lut[idx];
+      sum += lut[idx];
+    }
+    se[i] = sum;
+    for (size_t j = 0; j < n; ++j)
+      pr[i * n + j] = j <= i ? floor_div((i128)ex[i * n + j] * (i128)scale, (i128)sum) : 0;
+  }
+}
+
+// One GPT-2 block's witness (model.rs:213-221 with layer_norm :241-279, attention :281-351, the
+// softmax above and mlp :353-386).  Weight matrices are row-major: attn_w d x 3d, attn_proj_w
+// d x d, fc_w d x hidden, fproj_w hidden x d.
+struct BlockWeights {
+  std::vector<i64> ln1_g, ln1_b, attn_w, attn_b, proj_w, proj_b, ln2_g, ln2_b, fc_w, fc_b,
+      fproj_w, fproj_b;
+};
+struct GptDims {
+  size_t n, d, heads, dh, hidden;
+  i64 scale, sqrt_d_scale, offset;  // offset = max_v * scale
+};
+// The 36 output arrays in the order of the library's block witness (see ligesis_b200/proofsys.py).
+inline std::vector<std::vector<i64>> block_witness(const std::vector<i64>& x, const GptDims& g,
+                                                   const BlockWeights& w,
+                                                   const std::vector<i64>& exp_lut,
+                                                   const std::vector<i64>& gelu_lut) {
+  const size_t n = g.n, d = g.d, H = g.heads, dh = g.dh, hid = g.hidden;
+  std::vector<std::vector<i64>> out;
+  auto push_ln = [&](const LayerNormWitness& l) {
+    for (const std::vector<i64>* v :
+         {&l.sum_x, &l.sum_x2, &l.var_sum, &l.stdv, &l.dividend, &l.quotient, &l.output})
+      out.push_back(*v);
+  };
+  auto add = [](std::vector<i64> a, const std::vector<i64>& b) {
+    for (size_t i = 0; i < a.size(); ++i) a[i] += b[i];
+    return a;
+  };
+  // ln1, attention
+  const LayerNormWitness ln1 = layer_norm_witness(x, n, d, w.ln1_g, w.ln1_b);
+  push_ln(ln1);
+  const LinearWitness qkv = linear_witness(ln1.output, n, d, w.attn_w, 3 * d, false, &w.attn_b,
+                                           g.scale);
+  std::vector<i64> scores(H * n * n), xmax(H * n), ex(H * n * n), se(H * n), prob(H * n * n),
+      aoh(H * n * dh), rsc(H * n * n), raoh(H * n * dh), merged(n * d);
+  for (size_t h = 0; h < H; ++h) {
+    std::vector<i64> q(n * dh), k(n * dh), v(n * dh);
+    for (size_t s2 = 0; s2 < n; ++s2)
+      for (size_t e = 0; e < dh; ++e) {
+        q[s2 * dh + e] = qkv.y[s2 * 3 * d + h * dh + e];
+        k[s2 * dh + e] = qkv.y[s2 * 3 * d + d + h * dh + e];
+        v[s2 * dh + e] = qkv.y[s2 * 3 * d + 2 * d + h * dh + e];
+      }
+    const LinearWitness sc = linear_witness(q, n, dh, k, n, true, nullptr, g.sqrt_d_scale);
+    std::copy(sc.q.begin(), sc.q.end(), scores.begin() + h * n * n);
+    std::copy(sc.rem.begin(), sc.rem.end(), rsc.begin() + h * n * n);
+    softmax_witness(sc.q, n, exp_lut, g.offset, g.scale, &xmax[h * n], &ex[h * n * n], &se[h * n],
+                    &prob[h * n * n]);
+    const std::vector<i64> ph(prob.begin() + h * n * n, prob.begin() + (h + 1) * n * n);
+    const LinearWitness ao = linear_witness(ph, n, n, v, dh, false, nullptr, g.scale);
+    std::copy(ao.q.begin(), ao.q.end(), aoh.begin() + h * n * dh);
+    std::copy(ao.rem.begin(), ao.rem.end(), raoh.begin() + h * n * dh);
+    for (size_t i = 0; i < n; ++i)
+      for (size_t e = 0; e < dh; ++e) merged[i * d + h * dh + e] = ao.q[i * dh + e];
+  }
+  const LinearWitness apr = linear_witness(merged, n, d, w.proj_w, d, false, &w.proj_b, g.scale);
+  const std::vector<i64> attn_out = add(x, apr.y);
+  using CV = const std::vector<i64>*;
+  for (CV v : std::initializer_list<CV>{&qkv.q, &qkv.y, &scores, &xmax, &ex, &se, &prob, &aoh,
+                                        &merged, &apr.q, &attn_out, &qkv.rem, &rsc, &raoh,
+                                        &apr.rem})
+    out.push_back(*v);
+  // ln2, mlp
+  const LayerNormWitness ln2 = layer_norm_witness(attn_out, n, d, w.ln2_g, w.ln2_b);
+  push_ln(ln2);
+  const LinearWitness fc = linear_witness(ln2.output, n, d, w.fc_w, hid, false, &w.fc_b, g.scale);
+  std::vector<i64> act(n * hid);
+  for (size_t i = 0; i < n * hid; ++i) {
+    const i64 idx = fc.y[i] + g.offset;
+    if (idx < 0 || (size_t)idx >= gelu_lut.size()) throw std::runtime_error("GELU index out of range");
+    act[i] = gelu_lut[idx];
+  }
+  const LinearWitness fpr = linear_witness(act, n, hid, w.fproj_w, d, false, &w.fproj_b, g.scale);
+  const std::vector<i64> mlp_out = add(attn_out, fpr.y);
+  for (CV v : std::initializer_list<CV>{&fc.q, &fc.y, &act, &fpr.q, &mlp_out, &fc.rem, &fpr.rem})
+    out.push_back(*v);
+  return out;
 }
 
 }  // namespace orc

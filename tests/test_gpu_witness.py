@@ -66,3 +66,49 @@ def test_layer_norm_witness_constant_row(lgs, orc):
     assert got[3].tolist() == [1, 1] and not got[4].any()
     for g_, w_ in zip(got, orc.layer_norm_witness(x, np.ones(16, np.int64), np.zeros(16, np.int64))):
         assert np.array_equal(g_, w_)
+
+
+@pytest.mark.parametrize("cfg_over", [{}, {"n_seq": 5, "d_model": 64, "mlp_hidden": 128,
+                                           "n_head": 4}])
+def test_block_witness_matches_oracle(lgs, orc, cfg_over):
+    """One GPT-2 block's whole witness (36 arrays: ln1, attention with per-head scores, softmax
+    and weighted values, ln2, MLP with the GELU lookup) equals the oracle's element for element."""
+    cfg = {**ps.GPT2_31, "n_head": 12, **cfg_over}
+    x, w, el, gl = ps.synthetic_block(11, cfg)
+    got = ps.block_witness(x, w, el, gl, cfg)
+    want = orc.block_witness(x, w, el, gl, cfg)
+    assert set(got) == set(want) == set(ps.BLOCK_FIELDS)
+    for k in ps.BLOCK_FIELDS:
+        assert np.array_equal(got[k], want[k]), k
+
+
+def test_softmax_and_gather_reject_out_of_table(lgs):
+    s = np.zeros((1, 3, 3), dtype=np.int64)
+    s[0, 2, 0] = -1000  # index -1000 + offset 10 < 0
+    with pytest.raises(L.ShapeError):
+        ps.softmax_witness(s, np.ones(11, np.int64), 10, 4)
+    with pytest.raises(L.ShapeError):
+        ps.lut_gather(np.array([5, 6], np.int64), np.ones(11, np.int64), 5)  # 6 + 5 = 11
+    xm, ex, se, pr = ps.softmax_witness(np.zeros((1, 3, 3), np.int64), np.ones(11, np.int64), 10, 4)
+    assert se.tolist() == [[1, 2, 3]] and pr[0].tolist() == [[4, 0, 0], [2, 2, 0], [1, 1, 1]]
+
+
+def test_forward_witness_matches_oracle(lgs, orc):
+    """A three-block forward with the final layer norm and a 4099-token vocabulary head (the
+    block shape of GPT-2 small, fewer blocks and tokens to keep the oracle quick)."""
+    cfg = {**ps.GPT2_31, "n_head": 12}
+    x0, _, el, gl = ps.synthetic_block(20, cfg)
+    blocks = [ps.synthetic_block(21 + i, cfg)[1] for i in range(3)]
+    g = np.random.default_rng(30)
+    ln_g = g.integers(cfg["scale"] // 48, cfg["scale"] // 24, size=768, dtype=np.int64)
+    ln_b = g.integers(-1024, 1024, size=768, dtype=np.int64)
+    wte = g.integers(-64, 64, size=(4099, 768), dtype=np.int64)
+    got = ps.forward_witness(x0, blocks, ln_g, ln_b, wte, el, gl, cfg)
+    want = orc.forward_witness(x0, blocks, ln_g, ln_b, wte, el, gl, cfg)
+    for gb, wb in zip(got["blocks"], want["blocks"]):
+        for k in ps.BLOCK_FIELDS:
+            assert np.array_equal(gb[k], wb[k]), k
+    for a, b in zip(got["lnf"], want["lnf"]):
+        assert np.array_equal(a, b)
+    assert np.array_equal(got["q_log"], want["q_log"])
+    assert np.array_equal(got["rem_log"], want["rem_log"])

@@ -78,3 +78,26 @@ def test_layer_norm_witness_matches_python(orc):
             a = int(gain[c]) * (d * row[c] - s1)
             assert int(dv[r, c]) == a and int(qu[r, c]) == a // rs
             assert int(out[r, c]) == a // rs + int(bias[c])
+
+
+def test_block_witness_structure(orc):
+    """The oracle's GPT-2 block (proofsys/src/model.rs:213-443) on a small config: causal softmax
+    (zeros above the diagonal, row maxima over the causal part, probabilities summing to at most
+    scale), residuals, and the GELU lookup."""
+    from ligesis_b200 import proofsys as ps
+
+    cfg = dict(ps.GPT2_31, n_seq=5, d_model=64, mlp_hidden=128, n_head=4)
+    x, w, el, gl = ps.synthetic_block(9, cfg)
+    o = orc.block_witness(x, w, el, gl, cfg)
+    n, sc, off = 5, cfg["scale"], cfg["max_v"] * cfg["scale"]
+    ex, pr, sco = o["attn.exp"], o["attn.q_prob"], o["attn.scores"]
+    for h in range(4):
+        for i in range(n):
+            assert o["attn.x_max"][h, i] == sco[h, i, :i + 1].max()
+            assert not ex[h, i, i + 1:].any() and not pr[h, i, i + 1:].any()
+            assert 0 < pr[h, i, :i + 1].sum() <= sc
+            assert ex[h, i, :i + 1].tolist() == [int(el[v - sco[h, i, :i + 1].max() + off])
+                                                 for v in sco[h, i, :i + 1]]
+    assert np.array_equal(o["attn.x_out"], x + o["attn.q_apr"] + w["attn_proj_b"])
+    assert np.array_equal(o["mlp.act"], gl[o["mlp.fc"] + off])
+    assert np.array_equal(o["mlp.x_out"], o["attn.x_out"] + o["mlp.q_fpr"] + w["fproj_b"])
