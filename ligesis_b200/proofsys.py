@@ -12,6 +12,9 @@
   MLP's GELU table (model.rs:409-443, :362-373).
 * `block_witness`, `forward_witness`: one block's and the whole forward's witness
   (model.rs:208-237), every step on the GPU.
+* `canonical_online`: the merged polynomials of the witness types in the canonical commitment
+  layout (proofsys/src/canonical.rs:249-331), ready for a PolyCommitmentScheme backend
+  (ligesis_b200.pcs).
 * `encode_i64` (proofsys/src/witness.rs:102-108).
 """
 from __future__ import annotations
@@ -30,10 +33,12 @@ GPT2_31 = {"n_seq": 31, "d_model": 768, "mlp_hidden": 3072, "vocab": 50257, "sca
 def encode_i64(x) -> np.ndarray:
     """encode_i64 (proofsys/src/witness.rs:102-108): x >= 0 -> x mod p, else -(|x| mod p)."""
     a = np.asarray(x, dtype=np.int64)
-    mag = np.where(a >= 0, a.astype(np.uint64),
-                   (-(a + 1)).astype(np.uint64) + np.uint64(1)) % np.uint64(fld.P)
-    neg = (a < 0) & (mag != 0)
-    return np.where(neg, np.uint64(fld.P) - mag, mag)
+    flat = np.atleast_1d(a)
+    u = flat.view(np.uint64)
+    neg = flat < 0
+    p = np.uint64(fld.P)
+    mag = np.where(neg, (~u) + np.uint64(1), u) % p  # |x|, two's complement (exact at -2^63)
+    return np.where(neg & (mag != 0), p - mag, mag).reshape(a.shape)
 
 
 def _ptr(t):
@@ -228,3 +233,76 @@ def forward_witness(x0, blocks, ln_f_g, ln_f_b, wte, exp_lut, gelu_lut, cfg: dic
     q, rem, _, _ = linear_witness(out["lnf"][6], wte, None, cfg["scale"], True, ctx)
     out["q_log"], out["rem_log"] = q, rem
     return out
+
+
+# ---- the canonical online commitment layout (proofsys/src/canonical.rs:75-331) ----------------
+def _np2(x: int) -> int:
+    return 1 << max(0, (int(x) - 1).bit_length())
+
+
+def _stack_matrices(mats, pad: int = 0) -> np.ndarray:
+    """commit_matrices (canonical.rs:135-158) with stack_instances (commit.rs:32-41): each matrix
+    padded to row_pow x col_pow (column on the low variables), instances on the high variables,
+    values encode_i64'd."""
+    m0 = np.asarray(mats[0])
+    rows, cols = (m0.shape[0], 1) if m0.ndim == 1 else m0.shape
+    rp, cp = _np2(rows), _np2(cols)
+    k = _np2(len(mats))
+    out = np.full((k, rp, cp), encode_i64(np.int64(pad)), dtype=np.uint64)
+    if pad == 0:
+        out[:] = 0
+    for i, m in enumerate(mats):
+        a = np.asarray(m, dtype=np.int64)
+        a = a.reshape(-1, 1) if a.ndim == 1 else a
+        out[i, :a.shape[0], :a.shape[1]] = encode_i64(a)
+    return out.reshape(-1)
+
+
+def _stack_vectors_padded(vecs, pad: int) -> np.ndarray:
+    """commit_vectors_padded (canonical.rs:164-181): padding rows and instances hold pad."""
+    rp, k = _np2(len(vecs[0])), _np2(len(vecs))
+    out = np.full((k, rp), int(encode_i64(np.int64(pad))), dtype=np.uint64)
+    for i, v in enumerate(vecs):
+        out[i, :len(v)] = encode_i64(np.asarray(v, dtype=np.int64))
+    return out.reshape(-1)
+
+
+CANONICAL_TYPES = ("q_ln", "a_ln", "std", "var", "q_sc", "exp", "q_prob", "x_max", "sum_exp",
+                   "q_qkv", "q_ao", "q_apr", "q_fc", "act", "q_fpr", "x_out", "q_log")
+
+
+def canonical_online(fw: dict) -> dict:
+    """build_online (canonical.rs:249-331): the merged polynomial of every witness type of a
+    `forward_witness`, as Goldilocks values (uint64) of 2^(instance + row + column variables)
+    entries, keyed by CANONICAL_TYPES.  Layer norms in the order [ln1_0, ln2_0, ..., lnf], heads
+    12 l + h, x_out [attn_0, mlp_0, ...]; `std` and `sum_exp` pad with 1, everything else with 0."""
+    blocks = fw["blocks"]
+    lns = []
+    for b in blocks:
+        lns.append([b["ln1." + f] for f in LN_FIELDS])
+        lns.append([b["ln2." + f] for f in LN_FIELDS])
+    lns.append(list(fw["lnf"]))
+    heads = lambda key: [b[key][h] for b in blocks for h in range(b[key].shape[0])]
+    per_layer = lambda key: [b[key] for b in blocks]
+    x_out = []
+    for b in blocks:
+        x_out += [b["attn.x_out"], b["mlp.x_out"]]
+    return {
+        "q_ln": _stack_matrices([ln[5] for ln in lns]),
+        "a_ln": _stack_matrices([ln[4] for ln in lns]),
+        "std": _stack_vectors_padded([ln[3] for ln in lns], 1),
+        "var": _stack_vectors_padded([ln[2] for ln in lns], 0),
+        "q_sc": _stack_matrices(heads("attn.scores")),
+        "exp": _stack_matrices(heads("attn.exp")),
+        "q_prob": _stack_matrices(heads("attn.q_prob")),
+        "x_max": _stack_matrices(heads("attn.x_max")),
+        "sum_exp": _stack_vectors_padded(heads("attn.sum_exp"), 1),
+        "q_qkv": _stack_matrices(per_layer("attn.q_qkv")),
+        "q_ao": _stack_matrices(per_layer("attn.q_ao")),
+        "q_apr": _stack_matrices(per_layer("attn.q_apr")),
+        "q_fc": _stack_matrices(per_layer("mlp.q_fc")),
+        "act": _stack_matrices(per_layer("mlp.act")),
+        "q_fpr": _stack_matrices(per_layer("mlp.q_fpr")),
+        "x_out": _stack_matrices(x_out),
+        "q_log": _stack_matrices([fw["q_log"]]),
+    }

@@ -444,6 +444,56 @@ def forward_witness(x0, blocks, ln_f_g, ln_f_b, wte, exp_lut, gelu_lut, cfg: dic
     return out
 
 
+def canonical_online(fw: dict) -> dict:
+    """build_online (proofsys/src/canonical.rs:249-331) restated with plain Python integers:
+    {type: list of Goldilocks values}, for checking the library's layout."""
+    P_ = 0xFFFFFFFF00000001
+    enc = lambda v: int(v) % P_
+    np2 = lambda x: 1 if x <= 1 else 1 << (int(x) - 1).bit_length()
+
+    def mats(ms, pad=0):
+        rows = len(ms[0])
+        a0 = np.asarray(ms[0])
+        cols = 1 if a0.ndim == 1 else a0.shape[1]
+        rp, cp, k = np2(rows), np2(cols), np2(len(ms))
+        out = [enc(pad)] * (k * rp * cp) if pad else [0] * (k * rp * cp)
+        for i, m in enumerate(ms):
+            a = np.asarray(m)
+            for r in range(a.shape[0]):
+                for c in range(1 if a.ndim == 1 else a.shape[1]):
+                    out[(i * rp + r) * cp + c] = enc(a[r] if a.ndim == 1 else a[r, c])
+        return out
+
+    def vecs(vs, pad):
+        rp, k = np2(len(vs[0])), np2(len(vs))
+        out = [enc(pad)] * (k * rp)
+        for i, v in enumerate(vs):
+            for r, x in enumerate(v):
+                out[i * rp + r] = enc(x)
+        return out
+
+    bl = fw["blocks"]
+    lns = []
+    for b in bl:
+        for which in ("ln1.", "ln2."):
+            lns.append({f: b[which + f] for f in ("var_sum", "std", "dividend", "quotient")})
+    lf = fw["lnf"]
+    lns.append({"var_sum": lf[2], "std": lf[3], "dividend": lf[4], "quotient": lf[5]})
+    heads = lambda key: [b[key][h] for b in bl for h in range(len(b[key]))]
+    xo = []
+    for b in bl:
+        xo += [b["attn.x_out"], b["mlp.x_out"]]
+    return {"q_ln": mats([l["quotient"] for l in lns]), "a_ln": mats([l["dividend"] for l in lns]),
+            "std": vecs([l["std"] for l in lns], 1), "var": vecs([l["var_sum"] for l in lns], 0),
+            "q_sc": mats(heads("attn.scores")), "exp": mats(heads("attn.exp")),
+            "q_prob": mats(heads("attn.q_prob")), "x_max": mats(heads("attn.x_max")),
+            "sum_exp": vecs(heads("attn.sum_exp"), 1),
+            "q_qkv": mats([b["attn.q_qkv"] for b in bl]), "q_ao": mats([b["attn.q_ao"] for b in bl]),
+            "q_apr": mats([b["attn.q_apr"] for b in bl]), "q_fc": mats([b["mlp.q_fc"] for b in bl]),
+            "act": mats([b["mlp.act"] for b in bl]), "q_fpr": mats([b["mlp.q_fpr"] for b in bl]),
+            "x_out": mats(xo), "q_log": mats([fw["q_log"]])}
+
+
 def _ef2(a):
     return _u64(a).reshape(-1, 2).copy()
 

@@ -8,6 +8,7 @@ import pytest
 
 import ligesis_b200 as L
 from ligesis_b200 import proofsys as ps
+from tests.helpers import tiny_gpt
 
 pytestmark = pytest.mark.gpu
 
@@ -112,3 +113,41 @@ def test_forward_witness_matches_oracle(lgs, orc):
         assert np.array_equal(a, b)
     assert np.array_equal(got["q_log"], want["q_log"])
     assert np.array_equal(got["rem_log"], want["rem_log"])
+
+
+def test_canonical_commitment_of_the_reference_tiny_model(lgs, orc):
+    """The reference's tiny model through the GPU forward witness equals the oracle's; its
+    canonical merged polynomials equal an independent restatement of build_online; the
+    reference's check (canonical.rs:363-385): q_ln's instance 1 (ln2 of layer 0) at row 1,
+    column 0 reads ln2's quotient there; and every merged polynomial commits and opens with the
+    Basefold backend of the PolyCommitmentScheme."""
+    cfg, x0, w, lg, lb, wte, el, gl = tiny_gpt()
+    fw = ps.forward_witness(x0, [w], lg, lb, wte, el, gl, cfg)
+    ofw = orc.forward_witness(x0, [w], lg, lb, wte, el, gl, cfg)
+    for k in ps.BLOCK_FIELDS:
+        assert np.array_equal(fw["blocks"][0][k], ofw["blocks"][0][k]), k
+    assert np.array_equal(fw["q_log"], ofw["q_log"])
+    canon = ps.canonical_online(fw)
+    want = orc.canonical_online(ofw)
+    assert list(canon) == list(ps.CANONICAL_TYPES)
+    for k in ps.CANONICAL_TYPES:
+        assert canon[k].tolist() == want[k], k
+    # q_ln: 3 instances -> 2 instance vars, rows 2 -> 1 var, cols 2 -> 1 var
+    point = np.array([[0, 0], [1, 0], [1, 0], [0, 0]], dtype=np.uint64)  # col 0, row 1, inst 1
+    ev = np.stack([canon["q_ln"], np.zeros_like(canon["q_ln"])], axis=1)
+    want_v = int(ps.encode_i64(fw["blocks"][0]["ln2.quotient"][1, 0]))
+    assert orc.mle_eval(ev, point) == (want_v, 0)
+    pcs = L.BasefoldPcs(code_rate=1)
+    from ligesis_b200 import rng
+
+    oracle = L.RandomOracle(4, length=4096)
+    tasks, claims = [], []
+    for i, k in enumerate(ps.CANONICAL_TYPES):
+        poly = L.MlPoly(canon[k])
+        data, com = pcs.commit(poly)
+        pt = rng.ext_elements(500 + i, poly.num_vars)
+        tasks.append((data, pt))
+        claims.append((com, pt, orc.mle_eval(np.stack([canon[k], np.zeros_like(canon[k])], 1), pt)))
+    proof = pcs.batch_prove(tasks, oracle)
+    oracle.restart()
+    assert pcs.batch_verify(claims, proof, oracle)

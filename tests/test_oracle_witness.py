@@ -101,3 +101,18 @@ def test_block_witness_structure(orc):
     assert np.array_equal(o["attn.x_out"], x + o["attn.q_apr"] + w["attn_proj_b"])
     assert np.array_equal(o["mlp.act"], gl[o["mlp.fc"] + off])
     assert np.array_equal(o["mlp.x_out"], o["attn.x_out"] + o["mlp.q_fpr"] + w["fproj_b"])
+
+
+def test_canonical_layout_of_the_reference_tiny_model(orc):
+    """The library's canonical layout (numpy) against the independent restatement of build_online
+    (proofsys/src/canonical.rs:249-331) on the oracle's witness of the reference's tiny model."""
+    from ligesis_b200 import proofsys as ps
+    from tests.helpers import tiny_gpt
+
+    cfg, x0, w, lg, lb, wte, el, gl = tiny_gpt()
+    fw = orc.forward_witness(x0, [w], lg, lb, wte, el, gl, cfg)
+    got, want = ps.canonical_online(fw), orc.canonical_online(fw)
+    assert list(got) == list(ps.CANONICAL_TYPES) == list(want)
+    for k in ps.CANONICAL_TYPES:
+        assert got[k].tolist() == want[k], k
+    assert len(got["q_ln"]) == 16 and got["std"].tolist()[-2:] == [1, 1]
