@@ -151,3 +151,15 @@ def test_canonical_commitment_of_the_reference_tiny_model(lgs, orc):
     proof = pcs.batch_prove(tasks, oracle)
     oracle.restart()
     assert pcs.batch_verify(claims, proof, oracle)
+
+
+@pytest.mark.parametrize("xb,wb,inner", [(40, 8, 64), (40, 21, 1), (31, 30, 2), (20, 15, 3072)])
+def test_linear_witness_arithmetic_paths(lgs, orc, xb, wb, inner):
+    """Operand sizes that select each exact path: 32-bit products, 64-bit products with 64-bit
+    sums, and 128-bit sums (wide operands whose results still fit an i64)."""
+    x = _rand(xb + inner, (7, inner), xb)
+    w = _rand(wb + inner, (inner, 9), wb)
+    got = ps.linear_witness(x, w, None, 3)
+    want = orc.linear_witness(x, w, None, 3)
+    for g_, w_ in zip(got, want):
+        assert np.array_equal(g_, w_)
