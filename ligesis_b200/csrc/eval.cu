@@ -215,41 +215,64 @@ void canon_u64(u64* p, size_t n, cudaStream_t st) {
 }
 
 // ---- a-bar = eq_{z1}^T F (pcs/src/ligesis.rs:372-379) --------------------------------------
-// Two adjacent columns per thread (16-byte loads), eight rows in flight.  The BF x EF products
-// are accumulated unreduced (160-bit sums of 128-bit products) and reduced once per output.
-__global__ void __launch_bounds__(256)
+// A CTA owns 64 column pairs (16-byte loads, 512 contiguous bytes per warp and row); its four
+// groups of two warps each sum a quarter of the rows, eight rows in flight.  The BF x EF products
+// are accumulated unreduced (160-bit sums of 128-bit products) and reduced once per group; the
+// groups' field values are added through shared memory.  Four groups give the SM enough warps to
+// overlap one group's loads with another's multiply-adds.
+constexpr unsigned GEMV_GROUPS = 4;
+constexpr unsigned GEMV_PAIRS = 64;  // column pairs per CTA
+__global__ void __launch_bounds__(GEMV_GROUPS * GEMV_PAIRS)
     gemv_eq_rows_kernel(const u64* const* __restrict__ fref, const ef2* __restrict__ eq,
                         size_t m, size_t n, ef2* __restrict__ out) {
-  const size_t j = 2 * ((size_t)blockIdx.x * blockDim.x + threadIdx.x);
-  if (j >= n) return;
+  __shared__ u64 part[GEMV_GROUPS - 1][GEMV_PAIRS][4];
+  const unsigned c = threadIdx.x % GEMV_PAIRS, g = threadIdx.x / GEMV_PAIRS;
+  const size_t j = 2 * ((size_t)blockIdx.x * GEMV_PAIRS + c);
+  const bool live = j < n;
+  const size_t per = (m + GEMV_GROUPS - 1) / GEMV_GROUPS;
+  const size_t i0 = min(m, (size_t)g * per), i1 = min(m, i0 + per);
   const u64* __restrict__ f = *fref;
   Acc160 s00, s01, s10, s11;  // column j / j + 1, coordinate c0 / c1
   gl_acc_zero(s00), gl_acc_zero(s01), gl_acc_zero(s10), gl_acc_zero(s11);
-  size_t i = 0;
-  for (; i + 8 <= m; i += 8) {
-    ulonglong2 x[8];
+  if (live) {
+    size_t i = i0;
+    for (; i + 8 <= i1; i += 8) {
+      ulonglong2 x[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) x[q] = __ldg((const ulonglong2*)(f + (i + q) * n + j));
+      for (int q = 0; q < 8; ++q) x[q] = __ldg((const ulonglong2*)(f + (i + q) * n + j));
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const ef2 e = eq[i + q];
-      const u64 a = gl_canon(x[q].x), b = gl_canon(x[q].y);
+      for (int q = 0; q < 8; ++q) {
+        const ef2 e = eq[i + q];
+        const u64 a = gl_canon(x[q].x), b = gl_canon(x[q].y);
+        gl_mac(s00, e.c0, a), gl_mac(s01, e.c1, a), gl_mac(s10, e.c0, b), gl_mac(s11, e.c1, b);
+      }
+    }
+    for (; i < i1; ++i) {
+      const ulonglong2 x = __ldg((const ulonglong2*)(f + i * n + j));
+      const ef2 e = eq[i];
+      const u64 a = gl_canon(x.x), b = gl_canon(x.y);
       gl_mac(s00, e.c0, a), gl_mac(s01, e.c1, a), gl_mac(s10, e.c0, b), gl_mac(s11, e.c1, b);
     }
   }
-  for (; i < m; ++i) {
-    const ulonglong2 x = __ldg((const ulonglong2*)(f + i * n + j));
-    const ef2 e = eq[i];
-    const u64 a = gl_canon(x.x), b = gl_canon(x.y);
-    gl_mac(s00, e.c0, a), gl_mac(s01, e.c1, a), gl_mac(s10, e.c0, b), gl_mac(s11, e.c1, b);
+  u64 r[4] = {gl_acc_reduce(s00), gl_acc_reduce(s01), gl_acc_reduce(s10), gl_acc_reduce(s11)};
+  if (g > 0)
+#pragma unroll
+    for (int t = 0; t < 4; ++t) part[g - 1][c][t] = r[t];
+  __syncthreads();
+  if (g == 0 && live) {
+#pragma unroll
+    for (unsigned h = 0; h + 1 < GEMV_GROUPS; ++h)
+#pragma unroll
+      for (int t = 0; t < 4; ++t) r[t] = gl_add(r[t], part[h][c][t]);
+    out[j] = ef_make(r[0], r[1]);
+    out[j + 1] = ef_make(r[2], r[3]);
   }
-  out[j] = ef_make(gl_acc_reduce(s00), gl_acc_reduce(s01));
-  out[j + 1] = ef_make(gl_acc_reduce(s10), gl_acc_reduce(s11));
 }
 void gemv_eq_rows(const u64* const* fref, const ef2* eq, size_t m, size_t n, ef2* out,
                   cudaStream_t st) {
   if (n % 2) throw ShapeError("gemv: n must be even");
-  gemv_eq_rows_kernel<<<cdiv(n / 2, 256), 256, 0, st>>>(fref, eq, m, n, out);
+  gemv_eq_rows_kernel<<<cdiv(n / 2, GEMV_PAIRS), GEMV_GROUPS * GEMV_PAIRS, 0, st>>>(fref, eq, m,
+                                                                                    n, out);
   LGS_LAUNCH_CHECK();
 }
 
