@@ -82,45 +82,34 @@ struct LwArgs {
   int64_t *q, *rem, *y;
   uint64_t* yf;
   int* err;
-  const int* bits;  // bit lengths of max |x| and max |w| (lw_bits_kernel)
 };
 
-// Bit lengths of the largest |x| and |w| (atomicMax into bits[0], bits[1]): they decide whether
-// the sums of a K chunk fit 64 bits (and the operands 32), so the GEMM may skip the 128-bit
-// arithmetic and stay exact.
-__global__ void lw_bits_kernel(const int64_t* __restrict__ x, size_t nx,
-                               const int64_t* __restrict__ w, size_t nw, int* __restrict__ bits) {
-  int bx = 0, bw = 0;
-  const size_t stride = (size_t)gridDim.x * blockDim.x;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nx + nw; i += stride) {
-    const int64_t v = i < nx ? x[i] : w[i - nx];
-    const uint64_t m = v < 0 ? ~(uint64_t)v + 1 : (uint64_t)v;  // |v| (2^63 at INT64_MIN)
-    const int b = 64 - __clzll((long long)m);
-    if (i < nx) bx = max(bx, b); else bw = max(bw, b);
-  }
-  for (int o = 16; o; o >>= 1) {
-    bx = max(bx, __shfl_xor_sync(0xffffffffu, bx, o));
-    bw = max(bw, __shfl_xor_sync(0xffffffffu, bw, o));
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomicMax(bits, bx);
-    atomicMax(bits + 1, bw);
-  }
+__device__ __forceinline__ uint64_t mag64(int64_t v) {
+  return v < 0 ? ~(uint64_t)v + 1 : (uint64_t)v;  // |v| (2^63 at INT64_MIN)
 }
+__device__ __forceinline__ int bitlen64(uint64_t v) { return 64 - __clzll((long long)v); }
 
-// The K loop of a tile: MODE 2 = 128-bit sums of 64-bit products; 1 = 64-bit sums of 64-bit
-// products; 0 = 64-bit sums of 32-bit products (mode chosen so that every sum is exact).
-template <int MODE>
+// The K loop of a tile.  Each stage of LW_K values picks its own exact arithmetic from the
+// largest |x| and |w| it has just staged (an OR of their magnitudes, gathered in shared memory),
+// so no separate pass over the operands is needed:
+//   bx + bw + log2 LW_K <= 62 and both <= 31 bits: 32-bit products summed in 64 bits;
+//   bx + bw + log2 LW_K <= 62: 64-bit products summed in 64 bits;
+//   otherwise: 128-bit sums of the 64-bit products.
+// A stage's 64-bit sum is exact and is added to the 128-bit accumulator.
 __device__ __forceinline__ void lw_tile_loop(const LwArgs& a, int64_t (*xs)[LW_TM + 1],
-                                             int64_t (*ws)[LW_TN + 1], size_t r0, size_t c0,
+                                             int64_t (*ws)[LW_TN + 1],
+                                             unsigned long long (*mags)[2], size_t r0, size_t c0,
                                              size_t kb, size_t ke, Acc128 (&acc)[2][4]) {
-  const unsigned tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  int64_t s64[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-  for (size_t k0 = kb; k0 < ke; k0 += LW_K) {
+  const unsigned tx = threadIdx.x & 15, ty = threadIdx.x >> 4, lane = threadIdx.x & 31;
+  unsigned par = 0;
+  for (size_t k0 = kb; k0 < ke; k0 += LW_K, par ^= 1) {
+    uint64_t ox = 0, ow = 0;
     for (unsigned e = threadIdx.x; e < LW_TM * LW_K; e += blockDim.x) {
       const unsigned rr = e / LW_K, kk = e % LW_K;
       const size_t gr = r0 + rr, gk = k0 + kk;
-      xs[kk][rr] = (gr < a.rows && gk < ke) ? a.x[gr * a.inner + gk] : 0;
+      const int64_t v = (gr < a.rows && gk < ke) ? a.x[gr * a.inner + gk] : 0;
+      xs[kk][rr] = v;
+      ox |= mag64(v);
     }
     for (unsigned e = threadIdx.x; e < LW_TN * LW_K; e += blockDim.x) {
       unsigned cc, kk;
@@ -135,34 +124,65 @@ __device__ __forceinline__ void lw_tile_loop(const LwArgs& a, int64_t (*xs)[LW_T
       int64_t v = 0;
       if (gc < a.cols && gk < ke) v = a.wt ? a.w[gc * a.inner + gk] : a.w[gk * a.cols + gc];
       ws[kk][cc] = v;
+      ow |= mag64(v);
+    }
+    // OR over the warp (two 32-bit halves), then over the CTA into this stage's slot
+    const unsigned xl = __reduce_or_sync(0xffffffffu, (unsigned)ox);
+    const unsigned xh = __reduce_or_sync(0xffffffffu, (unsigned)(ox >> 32));
+    const unsigned wl = __reduce_or_sync(0xffffffffu, (unsigned)ow);
+    const unsigned wh = __reduce_or_sync(0xffffffffu, (unsigned)(ow >> 32));
+    if (lane == 0) {
+      atomicOr(&mags[par][0], ((unsigned long long)xh << 32) | xl);
+      atomicOr(&mags[par][1], ((unsigned long long)wh << 32) | wl);
     }
     __syncthreads();
+    const int bx = bitlen64(mags[par][0]), bw = bitlen64(mags[par][1]);
+    // the other slot was last read before this barrier and is next written after the next one
+    if (threadIdx.x == 0) mags[par ^ 1][0] = mags[par ^ 1][1] = 0;
+    if (bx + bw + 5 <= 62) {  // 2^5 = LW_K products per sum
+      int64_t s64[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+      if (bx <= 31 && bw <= 31) {
 #pragma unroll 8
-    for (int kk = 0; kk < LW_K; ++kk) {
-      const int64_t x0 = xs[kk][2 * ty], x1 = xs[kk][2 * ty + 1];
+        for (int kk = 0; kk < LW_K; ++kk) {
+          const int32_t x0 = (int32_t)xs[kk][2 * ty], x1 = (int32_t)xs[kk][2 * ty + 1];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int64_t b = ws[kk][4 * tx + j];
-        if (MODE == 2) {
+          for (int j = 0; j < 4; ++j) {
+            const int32_t b = (int32_t)ws[kk][4 * tx + j];
+            s64[0][j] += (int64_t)x0 * b;
+            s64[1][j] += (int64_t)x1 * b;
+          }
+        }
+      } else {
+#pragma unroll 8
+        for (int kk = 0; kk < LW_K; ++kk) {
+          const int64_t x0 = xs[kk][2 * ty], x1 = xs[kk][2 * ty + 1];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int64_t b = ws[kk][4 * tx + j];
+            s64[0][j] += x0 * b;
+            s64[1][j] += x1 * b;
+          }
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          add128(acc[i][j], Acc128{(uint64_t)s64[i][j], (uint64_t)(s64[i][j] >> 63)});
+    } else {
+#pragma unroll 8
+      for (int kk = 0; kk < LW_K; ++kk) {
+        const int64_t x0 = xs[kk][2 * ty], x1 = xs[kk][2 * ty + 1];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int64_t b = ws[kk][4 * tx + j];
           mac128(acc[0][j], x0, b);
           mac128(acc[1][j], x1, b);
-        } else if (MODE == 1) {
-          s64[0][j] += x0 * b;
-          s64[1][j] += x1 * b;
-        } else {
-          s64[0][j] += (int64_t)(int32_t)x0 * (int32_t)b;
-          s64[1][j] += (int64_t)(int32_t)x1 * (int32_t)b;
         }
       }
     }
     __syncthreads();
   }
-  if (MODE != 2)
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        acc[i][j] = Acc128{(uint64_t)s64[i][j], (uint64_t)(s64[i][j] >> 63)};
 }
 
 // A 32 x 64 output tile over the K range of blockIdx.z; 16 x 16 threads, 2 x 4 outputs each.
@@ -171,6 +191,7 @@ template <bool FINAL>
 __global__ void __launch_bounds__(256) linear_witness_kernel(const LwArgs a) {
   __shared__ int64_t xs[LW_K][LW_TM + 1];
   __shared__ int64_t ws[LW_K][LW_TN + 1];
+  __shared__ unsigned long long mags[2][2];  // per stage parity: OR of |x|, OR of |w|
   const unsigned tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const size_t r0 = (size_t)blockIdx.y * LW_TM, c0 = (size_t)blockIdx.x * LW_TN;
   const size_t kb = (size_t)blockIdx.z * a.kchunk, ke = min(a.inner, kb + a.kchunk);
@@ -179,17 +200,9 @@ __global__ void __launch_bounds__(256) linear_witness_kernel(const LwArgs a) {
   for (int i = 0; i < 2; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = Acc128{0, 0};
-  // |a sum| < 2^(bx + bw + log2 kchunk) must stay below 2^63 for the 64-bit modes
-  const int bx = a.bits[0], bw = a.bits[1];
-  int lk = 0;
-  while (((size_t)1 << lk) < a.kchunk) ++lk;
-  if (bx + bw + lk <= 62)
-    if (bx <= 31 && bw <= 31)
-      lw_tile_loop<0>(a, xs, ws, r0, c0, kb, ke, acc);
-    else
-      lw_tile_loop<1>(a, xs, ws, r0, c0, kb, ke, acc);
-  else
-    lw_tile_loop<2>(a, xs, ws, r0, c0, kb, ke, acc);
+  if (threadIdx.x == 0) mags[0][0] = mags[0][1] = mags[1][0] = mags[1][1] = 0;
+  __syncthreads();
+  lw_tile_loop(a, xs, ws, mags, r0, c0, kb, ke, acc);
   bool bad = false;
 #pragma unroll
   for (int i = 0; i < 2; ++i)
@@ -329,13 +342,8 @@ void linear_witness_dev(lgs_ctx* c, const int64_t* x, size_t rows, size_t inner,
     dy = ar.get<int64_t>(no);
     df = y_field ? ar.get<uint64_t>(no) : nullptr;
   }
-  int* derr = ar.get<int>(3);  // error word, bit lengths of max |x| and max |w|
-  LGS_CUDA(cudaMemsetAsync(derr, 0, 3 * sizeof(int), st));
-  {
-    const unsigned blocks = (unsigned)std::min<size_t>((nx + nw + 255) / 256, 148 * 4);
-    lw_bits_kernel<<<blocks, 256, 0, st>>>(dx, nx, dw, nw, derr + 1);
-    LGS_LAUNCH_CHECK();
-  }
+  int* derr = ar.get<int>(1);  // error word
+  LGS_CUDA(cudaMemsetAsync(derr, 0, sizeof(int), st));
   // Few rows (GPT-2 runs 31 positions) leave most SMs idle: split K until there are about two
   // CTAs per SM, each with at least 128 values of K, and sum the exact partials afterwards.
   const size_t tiles = ((cols + LW_TN - 1) / LW_TN) * ((rows + LW_TM - 1) / LW_TM);
@@ -348,7 +356,7 @@ void linear_witness_dev(lgs_ctx* c, const int64_t* x, size_t rows, size_t inner,
   kchunk = (kchunk + LW_K - 1) / LW_K * LW_K;
   split = (inner + kchunk - 1) / kchunk;
   LwArgs a{dx, dw, db, rows, inner, cols, kchunk, divisor, w_transposed ? 1 : 0, nullptr,
-           dq, dr, dy, df, derr, derr + 1};
+           dq, dr, dy, df, derr};
   const dim3 grid((unsigned)((cols + LW_TN - 1) / LW_TN), (unsigned)((rows + LW_TM - 1) / LW_TM),
                   (unsigned)split);
   if (split == 1) {

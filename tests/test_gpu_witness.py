@@ -163,3 +163,24 @@ def test_linear_witness_arithmetic_paths(lgs, orc, xb, wb, inner):
     want = orc.linear_witness(x, w, None, 3)
     for g_, w_ in zip(got, want):
         assert np.array_equal(g_, w_)
+
+
+@pytest.mark.parametrize("wt", [False, True])
+def test_linear_witness_mixed_widths_across_k(lgs, orc, wt):
+    """Each K stage of 32 picks its own exact arithmetic from the operands it stages: here the
+    first stage needs 128-bit sums (38-bit x, 20-bit w), the second 64-bit products (36-bit x,
+    8-bit w) and the rest 32-bit products (12-bit operands), in one product and with K split
+    over CTAs."""
+    rows, inner, cols = 7, 4096, 9
+    x = _rand(5, (rows, inner), 12)
+    x[:, :32] = _rand(6, (rows, 32), 38)
+    x[:, 32:64] = _rand(7, (rows, 32), 36)
+    w = _rand(8, (inner, cols), 12)
+    w[:32] = _rand(9, (32, cols), 20)
+    w[32:64] = _rand(10, (32, cols), 8)
+    if wt:
+        w = np.ascontiguousarray(w.T)
+    got = ps.linear_witness(x, w, None, 1 << 12, wt)
+    want = orc.linear_witness(x, w, None, 1 << 12, wt)
+    for g_, w_ in zip(got, want):
+        assert np.array_equal(g_, w_)
