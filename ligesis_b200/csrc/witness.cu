@@ -88,6 +88,10 @@ __device__ __forceinline__ uint64_t mag64(int64_t v) {
   return v < 0 ? ~(uint64_t)v + 1 : (uint64_t)v;  // |v| (2^63 at INT64_MIN)
 }
 __device__ __forceinline__ int bitlen64(uint64_t v) { return 64 - __clzll((long long)v); }
+// s += x * y for 32-bit signed x, y: one wide multiply-add into the 64-bit sum.
+__device__ __forceinline__ void mad_wide(int64_t& s, int32_t x, int32_t y) {
+  asm("mad.wide.s32 %0, %1, %2, %0;" : "+l"(s) : "r"(x), "r"(y));
+}
 
 // The K loop of a tile.  Each stage of LW_K values picks its own exact arithmetic from the
 // largest |x| and |w| it has just staged (an OR of their magnitudes, gathered in shared memory),
@@ -147,9 +151,9 @@ __device__ __forceinline__ void lw_tile_loop(const LwArgs& a, int64_t (*xs)[LW_T
           const int32_t x0 = (int32_t)xs[kk][2 * ty], x1 = (int32_t)xs[kk][2 * ty + 1];
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
-            const int32_t b = (int32_t)ws[kk][4 * tx + j];
-            s64[0][j] += (int64_t)x0 * b;
-            s64[1][j] += (int64_t)x1 * b;
+            const int32_t b = (int32_t)ws[kk][tx + 16 * j];
+            mad_wide(s64[0][j], x0, b);
+            mad_wide(s64[1][j], x1, b);
           }
         }
       } else {
@@ -158,7 +162,7 @@ __device__ __forceinline__ void lw_tile_loop(const LwArgs& a, int64_t (*xs)[LW_T
           const int64_t x0 = xs[kk][2 * ty], x1 = xs[kk][2 * ty + 1];
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
-            const int64_t b = ws[kk][4 * tx + j];
+            const int64_t b = ws[kk][tx + 16 * j];
             s64[0][j] += x0 * b;
             s64[1][j] += x1 * b;
           }
@@ -175,7 +179,7 @@ __device__ __forceinline__ void lw_tile_loop(const LwArgs& a, int64_t (*xs)[LW_T
         const int64_t x0 = xs[kk][2 * ty], x1 = xs[kk][2 * ty + 1];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          const int64_t b = ws[kk][4 * tx + j];
+          const int64_t b = ws[kk][tx + 16 * j];
           mac128(acc[0][j], x0, b);
           mac128(acc[1][j], x1, b);
         }
@@ -185,7 +189,9 @@ __device__ __forceinline__ void lw_tile_loop(const LwArgs& a, int64_t (*xs)[LW_T
   }
 }
 
-// A 32 x 64 output tile over the K range of blockIdx.z; 16 x 16 threads, 2 x 4 outputs each.
+// A 32 x 64 output tile over the K range of blockIdx.z; 16 x 16 threads, 2 x 4 outputs each:
+// rows 2 ty, 2 ty + 1 and columns tx + 16 j, so that 16 threads read 16 consecutive staged
+// weights (no shared-memory bank conflicts) and write 16 consecutive outputs.
 // FINAL (one K split): finish the outputs here; else store the exact partial sums.
 template <bool FINAL>
 __global__ void __launch_bounds__(256) linear_witness_kernel(const LwArgs a) {
@@ -208,7 +214,7 @@ __global__ void __launch_bounds__(256) linear_witness_kernel(const LwArgs a) {
   for (int i = 0; i < 2; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const size_t r = r0 + 2 * ty + i, c = c0 + 4 * tx + j;
+      const size_t r = r0 + 2 * ty + i, c = c0 + tx + 16 * j;
       if (r >= a.rows || c >= a.cols) continue;
       const size_t o = r * a.cols + c;
       if (FINAL)
