@@ -798,6 +798,8 @@ def run_witness(args) -> None:
     act = cfg["max_v"] * sc
     shapes = {"qkv": (d, 3 * d, False), "attn_proj": (d, d, False), "fc": (d, h, False),
               "fproj": (h, d, False), "vocab_head": (d, v, True)}
+    if args.layer:
+        shapes = {args.layer: shapes[args.layer]}
     out = {}
     for name, (inner, cols, wt) in shapes.items():
         x = g.integers(-act, act, size=(n, inner), dtype=np.int64)
@@ -818,6 +820,10 @@ def run_witness(args) -> None:
             res[label] = round((time.perf_counter() - t0) / args.steps * 1e3, 3)
         res["products"] = n * inner * cols
         out[name] = res
+    if args.layer:
+        print(json.dumps({"mode": "witness", "config": "gpt2_31", "steps": args.steps,
+                          "timing": "host wall clock per call", "layers": out}), flush=True)
+        return
     forward = 12 * sum(out[k]["device_ms"] for k in ("qkv", "attn_proj", "fc", "fproj")) \
         + out["vocab_head"]["device_ms"]
     # one whole block's witness (layer norms, attention with 12 heads, softmax, MLP, GELU
@@ -866,6 +872,9 @@ def main() -> None:
     ap.add_argument("--nu", type=int, default=16, help="logup mode: 2^nu table entries")
     ap.add_argument("--requests", type=int, default=600)
     ap.add_argument("--rate", type=float, default=200.0)
+    ap.add_argument("--layer", default=None,
+                    choices=["qkv", "attn_proj", "fc", "fproj", "vocab_head"],
+                    help="witness mode: time this linear layer only (no block, no oracle)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
