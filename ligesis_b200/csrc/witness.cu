@@ -21,6 +21,9 @@ namespace lgs {
 namespace {
 
 constexpr int LW_TM = 32, LW_TN = 64, LW_K = 32;  // output tile rows x cols, K per stage
+constexpr size_t LW_XS_BYTES = (size_t)LW_K * (LW_TM + 1) * 8;
+constexpr size_t LW_WS_BYTES = (size_t)LW_K * (LW_TN + 1) * 8;
+constexpr size_t LW_SMEM = 2 * (LW_XS_BYTES + LW_WS_BYTES) + 4 * 8;
 
 // 128-bit accumulator as (hi:lo); a product of two i64 is added exactly.
 // (two's complement in two words, added modulo 2^128 like the reference's i128)
@@ -96,40 +99,77 @@ __device__ __forceinline__ void mad_wide(int64_t& s, int32_t x, int32_t y) {
 // The K loop of a tile.  Each stage of LW_K values picks its own exact arithmetic from the
 // largest |x| and |w| it has just staged (an OR of their magnitudes, gathered in shared memory),
 // so no separate pass over the operands is needed:
+//   bx + bw + log2 LW_K <= 53: fused multiply-adds of doubles (exact: every intermediate is an
+//     integer below 2^53), one instruction per product;
 //   bx + bw + log2 LW_K <= 62 and both <= 31 bits: 32-bit products summed in 64 bits;
 //   bx + bw + log2 LW_K <= 62: 64-bit products summed in 64 bits;
 //   otherwise: 128-bit sums of the 64-bit products.
-// A stage's 64-bit sum is exact and is added to the 128-bit accumulator.
+// A stage's sum is exact and is added to the 128-bit accumulator.
 __device__ __forceinline__ void lw_tile_loop(const LwArgs& a, int64_t (*xs)[LW_TM + 1],
-                                             int64_t (*ws)[LW_TN + 1],
+                                             int64_t (*ws)[LW_TN + 1], double (*xd)[LW_TM + 1],
+                                             double (*wd)[LW_TN + 1],
                                              unsigned long long (*mags)[2], size_t r0, size_t c0,
                                              size_t kb, size_t ke, Acc128 (&acc)[2][4]) {
   const unsigned tx = threadIdx.x & 15, ty = threadIdx.x >> 4, lane = threadIdx.x & 31;
-  unsigned par = 0;
-  for (size_t k0 = kb; k0 < ke; k0 += LW_K, par ^= 1) {
-    uint64_t ox = 0, ow = 0;
-    for (unsigned e = threadIdx.x; e < LW_TM * LW_K; e += blockDim.x) {
-      const unsigned rr = e / LW_K, kk = e % LW_K;
-      const size_t gr = r0 + rr, gk = k0 + kk;
-      const int64_t v = (gr < a.rows && gk < ke) ? a.x[gr * a.inner + gk] : 0;
-      xs[kk][rr] = v;
-      ox |= mag64(v);
+  // Each of the 256 threads stages 4 values of x and 8 of w per stage (LW_TM x LW_K and
+  // LW_TN x LW_K).  The next stage's values are loaded into registers before this stage's
+  // arithmetic, so their global-memory latency is hidden behind it.
+  constexpr int NX = LW_TM * LW_K / 256, NW = LW_TN * LW_K / 256;
+  int64_t vx[NX], vw[NW];
+  auto x_slot = [&](int i, unsigned& rr, unsigned& kk) {
+    const unsigned e = threadIdx.x + 256 * i;
+    rr = e / LW_K;
+    kk = e % LW_K;
+  };
+  auto w_slot = [&](int i, unsigned& cc, unsigned& kk) {
+    const unsigned e = threadIdx.x + 256 * i;
+    if (a.wt) {  // w is cols x inner: consecutive threads read consecutive k
+      cc = e / LW_K;
+      kk = e % LW_K;
+    } else {  // w is inner x cols: consecutive threads read consecutive columns
+      kk = e / LW_TN;
+      cc = e % LW_TN;
     }
-    for (unsigned e = threadIdx.x; e < LW_TN * LW_K; e += blockDim.x) {
+  };
+  auto fetch = [&](size_t k0) {
+#pragma unroll
+    for (int i = 0; i < NX; ++i) {
+      unsigned rr, kk;
+      x_slot(i, rr, kk);
+      const size_t gr = r0 + rr, gk = k0 + kk;
+      vx[i] = (gr < a.rows && gk < ke) ? a.x[gr * a.inner + gk] : 0;
+    }
+#pragma unroll
+    for (int i = 0; i < NW; ++i) {
       unsigned cc, kk;
-      if (a.wt) {  // w is cols x inner: consecutive threads read consecutive k
-        cc = e / LW_K;
-        kk = e % LW_K;
-      } else {  // w is inner x cols: consecutive threads read consecutive columns
-        kk = e / LW_TN;
-        cc = e % LW_TN;
-      }
+      w_slot(i, cc, kk);
       const size_t gc = c0 + cc, gk = k0 + kk;
       int64_t v = 0;
       if (gc < a.cols && gk < ke) v = a.wt ? a.w[gc * a.inner + gk] : a.w[gk * a.cols + gc];
-      ws[kk][cc] = v;
-      ow |= mag64(v);
+      vw[i] = v;
     }
+  };
+  fetch(kb);
+  unsigned par = 0;
+  for (size_t k0 = kb; k0 < ke; k0 += LW_K, par ^= 1) {
+    uint64_t ox = 0, ow = 0;
+#pragma unroll
+    for (int i = 0; i < NX; ++i) {
+      unsigned rr, kk;
+      x_slot(i, rr, kk);
+      xs[kk][rr] = vx[i];
+      xd[kk][rr] = (double)vx[i];
+      ox |= mag64(vx[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < NW; ++i) {
+      unsigned cc, kk;
+      w_slot(i, cc, kk);
+      ws[kk][cc] = vw[i];
+      wd[kk][cc] = (double)vw[i];
+      ow |= mag64(vw[i]);
+    }
+    if (k0 + LW_K < ke) fetch(k0 + LW_K);
     // OR over the warp (two 32-bit halves), then over the CTA into this stage's slot
     const unsigned xl = __reduce_or_sync(0xffffffffu, (unsigned)ox);
     const unsigned xh = __reduce_or_sync(0xffffffffu, (unsigned)(ox >> 32));
@@ -143,7 +183,28 @@ __device__ __forceinline__ void lw_tile_loop(const LwArgs& a, int64_t (*xs)[LW_T
     const int bx = bitlen64(mags[par][0]), bw = bitlen64(mags[par][1]);
     // the other slot was last read before this barrier and is next written after the next one
     if (threadIdx.x == 0) mags[par ^ 1][0] = mags[par ^ 1][1] = 0;
-    if (bx + bw + 5 <= 62) {  // 2^5 = LW_K products per sum
+    if (bx + bw + 5 <= 53) {  // 2^5 = LW_K products per sum
+      // every product and partial sum is an integer below 2^53 in magnitude, so each fused
+      // multiply-add of doubles is exact (no rounding ever happens)
+      double d[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+#pragma unroll 8
+      for (int kk = 0; kk < LW_K; ++kk) {
+        const double x0 = xd[kk][2 * ty], x1 = xd[kk][2 * ty + 1];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const double b = wd[kk][tx + 16 * j];
+          d[0][j] = __fma_rn(x0, b, d[0][j]);
+          d[1][j] = __fma_rn(x1, b, d[1][j]);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int64_t v = __double2ll_rn(d[i][j]);
+          add128(acc[i][j], Acc128{(uint64_t)v, (uint64_t)(v >> 63)});
+        }
+    } else if (bx + bw + 5 <= 62) {
       int64_t s64[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
       if (bx <= 31 && bw <= 31) {
 #pragma unroll 8
@@ -194,10 +255,15 @@ __device__ __forceinline__ void lw_tile_loop(const LwArgs& a, int64_t (*xs)[LW_T
 // weights (no shared-memory bank conflicts) and write 16 consecutive outputs.
 // FINAL (one K split): finish the outputs here; else store the exact partial sums.
 template <bool FINAL>
-__global__ void __launch_bounds__(256) linear_witness_kernel(const LwArgs a) {
-  __shared__ int64_t xs[LW_K][LW_TM + 1];
-  __shared__ int64_t ws[LW_K][LW_TN + 1];
-  __shared__ unsigned long long mags[2][2];  // per stage parity: OR of |x|, OR of |w|
+__global__ void __launch_bounds__(256, 2) linear_witness_kernel(const LwArgs a) {
+  // staged operands as int64 and as doubles (exact below 2^53), and per stage parity the ORs of
+  // |x| and |w|: LW_SMEM bytes of dynamic shared memory
+  extern __shared__ __align__(16) unsigned char lw_smem[];
+  auto xs = (int64_t(*)[LW_TM + 1])lw_smem;
+  auto ws = (int64_t(*)[LW_TN + 1])(lw_smem + LW_XS_BYTES);
+  auto xd = (double(*)[LW_TM + 1])(lw_smem + LW_XS_BYTES + LW_WS_BYTES);
+  auto wd = (double(*)[LW_TN + 1])(lw_smem + 2 * LW_XS_BYTES + LW_WS_BYTES);
+  auto mags = (unsigned long long(*)[2])(lw_smem + 2 * (LW_XS_BYTES + LW_WS_BYTES));
   const unsigned tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const size_t r0 = (size_t)blockIdx.y * LW_TM, c0 = (size_t)blockIdx.x * LW_TN;
   const size_t kb = (size_t)blockIdx.z * a.kchunk, ke = min(a.inner, kb + a.kchunk);
@@ -208,7 +274,7 @@ __global__ void __launch_bounds__(256) linear_witness_kernel(const LwArgs a) {
     for (int j = 0; j < 4; ++j) acc[i][j] = Acc128{0, 0};
   if (threadIdx.x == 0) mags[0][0] = mags[0][1] = mags[1][0] = mags[1][1] = 0;
   __syncthreads();
-  lw_tile_loop(a, xs, ws, mags, r0, c0, kb, ke, acc);
+  lw_tile_loop(a, xs, ws, xd, wd, mags, r0, c0, kb, ke, acc);
   bool bad = false;
 #pragma unroll
   for (int i = 0; i < 2; ++i)
@@ -365,12 +431,16 @@ void linear_witness_dev(lgs_ctx* c, const int64_t* x, size_t rows, size_t inner,
            dq, dr, dy, df, derr};
   const dim3 grid((unsigned)((cols + LW_TN - 1) / LW_TN), (unsigned)((rows + LW_TM - 1) / LW_TM),
                   (unsigned)split);
+  LGS_CUDA(cudaFuncSetAttribute(linear_witness_kernel<true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LW_SMEM));
+  LGS_CUDA(cudaFuncSetAttribute(linear_witness_kernel<false>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LW_SMEM));
   if (split == 1) {
-    linear_witness_kernel<true><<<grid, 256, 0, st>>>(a);
+    linear_witness_kernel<true><<<grid, 256, LW_SMEM, st>>>(a);
     LGS_LAUNCH_CHECK();
   } else {
     a.part = ar.get<Acc128>(split * no);
-    linear_witness_kernel<false><<<grid, 256, 0, st>>>(a);
+    linear_witness_kernel<false><<<grid, 256, LW_SMEM, st>>>(a);
     LGS_LAUNCH_CHECK();
     const unsigned blocks = (unsigned)std::min<size_t>((no + 255) / 256, 148 * 8);
     linear_witness_finish_kernel<<<blocks, 256, 0, st>>>(a, (unsigned)split);

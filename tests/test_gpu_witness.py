@@ -153,10 +153,12 @@ def test_canonical_commitment_of_the_reference_tiny_model(lgs, orc):
     assert pcs.batch_verify(claims, proof, oracle)
 
 
-@pytest.mark.parametrize("xb,wb,inner", [(40, 8, 64), (40, 21, 1), (31, 30, 2), (20, 15, 3072)])
+@pytest.mark.parametrize("xb,wb,inner", [(20, 15, 3072), (40, 8, 64), (28, 28, 64), (40, 15, 64),
+                                         (40, 21, 1), (31, 30, 2)])
 def test_linear_witness_arithmetic_paths(lgs, orc, xb, wb, inner):
-    """Operand sizes that select each exact path: 32-bit products, 64-bit products with 64-bit
-    sums, and 128-bit sums (wide operands whose results still fit an i64)."""
+    """Operand sizes that select each exact path: fused multiply-adds of doubles (GPT-2's
+    sizes), 64-bit products with 64-bit sums (40 + 8 and 40 + 15 bits), 32-bit products
+    (28 + 28 bits), and 128-bit sums (wide operands whose results still fit an i64)."""
     x = _rand(xb + inner, (7, inner), xb)
     w = _rand(wb + inner, (inner, 9), wb)
     got = ps.linear_witness(x, w, None, 3)
@@ -169,18 +171,33 @@ def test_linear_witness_arithmetic_paths(lgs, orc, xb, wb, inner):
 def test_linear_witness_mixed_widths_across_k(lgs, orc, wt):
     """Each K stage of 32 picks its own exact arithmetic from the operands it stages: here the
     first stage needs 128-bit sums (38-bit x, 20-bit w), the second 64-bit products (36-bit x,
-    8-bit w) and the rest 32-bit products (12-bit operands), in one product and with K split
-    over CTAs."""
+    18-bit w), the third 32-bit products (26-bit operands) and the rest doubles (12-bit
+    operands), in one product and with K split over CTAs."""
     rows, inner, cols = 7, 4096, 9
     x = _rand(5, (rows, inner), 12)
     x[:, :32] = _rand(6, (rows, 32), 38)
     x[:, 32:64] = _rand(7, (rows, 32), 36)
+    x[:, 64:96] = _rand(11, (rows, 32), 26)
     w = _rand(8, (inner, cols), 12)
     w[:32] = _rand(9, (32, cols), 20)
-    w[32:64] = _rand(10, (32, cols), 8)
+    w[32:64] = _rand(10, (32, cols), 18)
+    w[64:96] = _rand(12, (32, cols), 26)
     if wt:
         w = np.ascontiguousarray(w.T)
     got = ps.linear_witness(x, w, None, 1 << 12, wt)
     want = orc.linear_witness(x, w, None, 1 << 12, wt)
+    for g_, w_ in zip(got, want):
+        assert np.array_equal(g_, w_)
+
+
+@pytest.mark.parametrize("sign", [1, -1])
+def test_linear_witness_double_path_at_its_bound(lgs, orc, sign):
+    """Stages whose sums come closest to 2^53 still take the double path (40-bit by 8-bit
+    operands, 32 products per stage: 32 (2^40 - 1) 255 < 2^53) and stay exact."""
+    x = np.full((3, 96), sign * ((1 << 40) - 1), dtype=np.int64)
+    w = np.full((96, 5), 255, dtype=np.int64)
+    x[1, ::7] = -x[1, ::7]
+    got = ps.linear_witness(x, w, None, 1 << 12)
+    want = orc.linear_witness(x, w, None, 1 << 12)
     for g_, w_ in zip(got, want):
         assert np.array_equal(g_, w_)
