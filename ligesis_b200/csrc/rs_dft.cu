@@ -42,7 +42,13 @@ __device__ __forceinline__ u64 rot(u64 x) {
   } else if constexpr (s < 64) {
     return gl_reduce(x << s, x >> (64 - s));
   } else {
-    return rot<32>(rot<s - 32>(x));
+    // x = xl + 2^32 xh; 2^64 = 2^32 - 1 and 2^96 = -1 give
+    // x 2^s = xl 2^(s-32) - (xl + xh) 2^(s-64): one 96-bit reduction and a subtraction.
+    const u64 xl = x & GL_EPS, xh = x >> 32;
+    const u64 a = reduce_hi32(xl << (s - 32), xl >> (96 - s));
+    u64 b = (xl + xh) << (s - 64);  // < 2^64
+    if (b >= GL_P) b -= GL_P;
+    return gl_sub(a, b);
   }
 }
 
