@@ -204,7 +204,13 @@ GL_HD u64 gl_mul_pow2(u64 x, unsigned s) {
     s -= 96;
   }
   if (s < 64) return gl_shl(x, s);
-  return gl_shl(gl_shl(x, s - 32), 32);
+  // 64 <= s < 96: x = xl + 2^32 xh, 2^64 = 2^32 - 1 and 2^96 = -1 give
+  // x 2^s = xl 2^(s-32) - (xl + xh) 2^(s-64): one reduction and a subtraction.
+  const u64 xl = x & GL_EPS, xh = x >> 32;
+  const u64 a = gl_reduce(xl << (s - 32), xl >> (96 - s));
+  u64 b = (xl + xh) << (s - 64);  // < 2^64
+  if (b >= GL_P) b -= GL_P;
+  return gl_sub(a, b);
 }
 // The order-8 root the reference's generator gives: g_3 = 2^120 (checked at context creation).
 constexpr unsigned GL_LOG2_OMEGA8 = 120;
