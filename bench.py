@@ -198,7 +198,7 @@ class ClockSampler:
 # DRAM bytes (read + write) per launch of the two commit stages at mu = 24, from one ncu capture
 # each (`bench.py --mode commit --steps 3` under ncu --set full; profiles/rs_encode_mu24.md and
 # profiles/hash_tc_mu24.md): rs_encode = rs_pass_a + rs_pass_b.
-NCU_TRAFFIC = {"rs_encode": 842.7e6, "subset_sum_hash": 328.9e6}
+NCU_TRAFFIC = {"rs_encode": 842.0e6, "subset_sum_hash": 328.9e6}
 
 
 def _peaks() -> dict:
@@ -349,7 +349,9 @@ def run_ours(args) -> None:
         roof = {"kernel": "rs_encode (rs_pass_a + rs_pass_b)", "bound": "hbm",
                 "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(ach / peak, 4), "traffic": NCU_TRAFFIC["rs_encode"],
-                "peak_src": peaks["src"] + " HBM copy (MEASURED_PEAKS.json)",
+                "peak_src": ("measured HBM copy (MEASURED_PEAKS.json)" if peaks["src"] == "measured"
+                             else "fallback: 6.65 TB/s, an earlier copy measurement on this pool "
+                                  "(MEASURED_PEAKS.json absent)"),
                 "algorithmic": f"{ntt_bytes:.3e} bytes per launch"}
     others = {}
     if "rs_encode" in stages:
