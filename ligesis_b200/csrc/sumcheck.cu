@@ -19,7 +19,7 @@ namespace lgs {
 
 namespace {
 constexpr unsigned SC_THREADS = 256;
-constexpr unsigned SC_TAIL_THREADS = 256;
+constexpr unsigned SC_TAIL_THREADS = 512;
 
 __device__ __forceinline__ ef2 shfl_xor_ef(ef2 v, int m) {
   ef2 r;
