@@ -90,6 +90,39 @@ __device__ __forceinline__ void accumulate_pair(const ef2* lo, const ef2* hi, ef
   }
 }
 
+// One pair's contributions, out of line: inlined, the pair arithmetic appears three times in a
+// two-round pass (and in the one-round and tail kernels), and those copies overflowed the
+// instruction cache (warps stalled on instruction fetch).  Small structs by value keep the
+// operands in registers across the call.
+template <int S>
+struct FacVals {
+  ef2 v[S];
+};
+template <int D>
+struct PairSums {
+  ef2 s[D + 1];
+};
+template <int D, bool BIN>
+__device__ __noinline__ PairSums<D> pair_sums(FacVals<Fac<D, BIN>::S> lo,
+                                              FacVals<Fac<D, BIN>::S> hi, bool skip1) {
+  PairSums<D> r;
+#pragma unroll
+  for (int q = 0; q <= D; ++q) r.s[q] = ef_zero();
+  accumulate_pair<D, BIN>(lo.v, hi.v, r.s, skip1);
+  return r;
+}
+template <int D, bool BIN>
+__device__ __forceinline__ void add_pair(const ef2* lo, const ef2* hi, ef2 (&s)[D + 1],
+                                         bool skip1) {
+  constexpr int S = Fac<D, BIN>::S;
+  FacVals<S> a, b;
+#pragma unroll
+  for (int j = 0; j < S; ++j) a.v[j] = lo[j], b.v[j] = hi[j];
+  const PairSums<D> r = pair_sums<D, BIN>(a, b, skip1);
+#pragma unroll
+  for (int q = 0; q <= D; ++q) s[q] = ef_add(s[q], r.s[q]);
+}
+
 // g(r) for the degree-D round polynomial given by its values g(0..D) (Lagrange on 0..D).
 template <int D>
 __device__ ef2 interp_at(const ef2* g, ef2 r) {
@@ -147,7 +180,7 @@ __global__ void __launch_bounds__(SC_THREADS)
         hi[j] = p[i + half];
       }
     }
-    accumulate_pair<D, BIN>(lo, hi, s, skip1);
+    add_pair<D, BIN>(lo, hi, s, skip1);
   }
   block_reduce<D>(s, red);
   if (threadIdx.x == 0)
@@ -189,8 +222,8 @@ __global__ void __launch_bounds__(SC_THREADS, 2)
         e[m][j] = fold ? ef_lerp(p[x], p[x + len], ra) : p[x];
       }
     }
-    accumulate_pair<D, BIN>(e[0], e[2], s0, skip1);
-    accumulate_pair<D, BIN>(e[1], e[3], s0, skip1);
+    add_pair<D, BIN>(e[0], e[2], s0, skip1);
+    add_pair<D, BIN>(e[1], e[3], s0, skip1);
     ef2 y0[S], y1[S];
 #pragma unroll
     for (int j = 0; j < S; ++j) {
@@ -199,7 +232,7 @@ __global__ void __launch_bounds__(SC_THREADS, 2)
       P.p[j][i] = y0[j];
       P.p[j][i + qlen] = y1[j];
     }
-    accumulate_pair<D, BIN>(y0, y1, s1, true);
+    add_pair<D, BIN>(y0, y1, s1, true);
   }
   block_reduce<D>(s0, red);
   if (threadIdx.x == 0)
@@ -301,7 +334,7 @@ __global__ void __launch_bounds__(SC_TAIL_THREADS)
       ef2 lo[S], hi[S];
 #pragma unroll
       for (int j = 0; j < S; ++j) lo[j] = sv[j][i], hi[j] = sv[j][i + half];
-      accumulate_pair<D, BIN>(lo, hi, s, skip1);
+      add_pair<D, BIN>(lo, hi, s, skip1);
     }
 #pragma unroll
     for (int q = 0; q <= D; ++q)
