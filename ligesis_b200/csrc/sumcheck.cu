@@ -309,13 +309,35 @@ template <int D, bool BIN>
 __global__ void __launch_bounds__(SC_TAIL_THREADS)
     sc_tail_kernel(Polys<Fac<D, BIN>::S> P, unsigned len, int fold, const ef2* __restrict__ ch,
                    unsigned t0, unsigned k, ef2* __restrict__ rounds_out,
-                   ef2* __restrict__ final_out) {
+                   ef2* __restrict__ final_out, const ef2* __restrict__ partials,
+                   size_t stride) {
   constexpr int S = Fac<D, BIN>::S;
   constexpr unsigned NW = SC_TAIL_THREADS / 32;
   constexpr unsigned MAXR = 11;  // log2(TAIL) + 1 rounds at most
   __shared__ ef2 sv[S][Fac<D, BIN>::TAIL];
   __shared__ ef2 acc[MAXR][NW][D + 1];
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // The multi-CTA rounds 0..t0-1: round t's sums over the CTAs that ran it (one warp per round);
+  // the claim chain at the end reads them, after the barriers below.
+  for (unsigned t = warp; t < t0; t += NW) {
+    const size_t half = (size_t)1 << (k - 1 - t);
+    const unsigned nb =
+        (unsigned)min((size_t)SC_MAX_BLOCKS, (half + SC_THREADS - 1) / SC_THREADS);
+    ef2 s[D + 1];
+#pragma unroll
+    for (int q = 0; q <= D; ++q) s[q] = ef_zero();
+    const ef2* src = partials + (size_t)t * stride;
+    for (unsigned b = lane; b < nb; b += 32)
+#pragma unroll
+      for (int q = 0; q <= D; ++q) s[q] = ef_add(s[q], src[(size_t)b * (D + 1) + q]);
+#pragma unroll
+    for (int q = 0; q <= D; ++q)
+#pragma unroll
+      for (int m = 16; m; m >>= 1) s[q] = ef_add(s[q], shfl_xor_ef(s[q], m));
+    if (lane == 0)
+#pragma unroll
+      for (int q = 0; q <= D; ++q) rounds_out[(size_t)t * (D + 1) + q] = s[q];
+  }
   {
     const ef2 r = fold ? ch[t0 - 1] : ef_zero();
     for (unsigned i = threadIdx.x; i < len; i += blockDim.x)
@@ -422,28 +444,6 @@ __global__ void __launch_bounds__(SC_TAIL_THREADS)
   }
 }
 
-// rounds_out[t] = sum of the partials of round t; round t used
-// min(SC_MAX_BLOCKS, ceil(2^(k-1-t) / SC_THREADS)) CTAs.
-template <int D>
-__global__ void sc_reduce_kernel(const ef2* __restrict__ partials, size_t stride, unsigned k,
-                                 ef2* __restrict__ rounds_out) {
-  __shared__ ef2 red[(D + 1) * 32];
-  const unsigned t = blockIdx.x;
-  const size_t half = (size_t)1 << (k - 1 - t);
-  const unsigned nb = (unsigned)min((size_t)SC_MAX_BLOCKS, (half + SC_THREADS - 1) / SC_THREADS);
-  ef2 s[D + 1];
-#pragma unroll
-  for (int q = 0; q <= D; ++q) s[q] = ef_zero();
-  const ef2* src = partials + (size_t)t * stride;
-  for (unsigned b = threadIdx.x; b < nb; b += blockDim.x)
-#pragma unroll
-    for (int q = 0; q <= D; ++q) s[q] = ef_add(s[q], src[(size_t)b * (D + 1) + q]);
-  block_reduce<D>(s, red);
-  if (threadIdx.x == 0)
-#pragma unroll
-    for (int q = 0; q <= D; ++q) rounds_out[(size_t)t * (D + 1) + q] = s[q];
-}
-
 template <int D, bool BIN>
 void sumcheck_run(ef2* const* polys, unsigned k, const ef2* ch, ef2* rounds_out, ef2* final_out,
                   ef2* partials, cudaStream_t st) {
@@ -479,13 +479,10 @@ void sumcheck_run(ef2* const* polys, unsigned k, const ef2* ch, ef2* rounds_out,
     fold = 1;
     ++t;
   }
-  // the multi-CTA rounds' sums first: the tail completes their g(1) along the claim chain
-  if (t > 0) {
-    sc_reduce_kernel<D><<<t, 256, 0, st>>>(partials, stride, k, rounds_out);
-    LGS_LAUNCH_CHECK();
-  }
+  // the tail also sums the multi-CTA rounds' partials, and completes their g(1) along the
+  // claim chain
   sc_tail_kernel<D, BIN><<<1, SC_TAIL_THREADS, 0, st>>>(P, (unsigned)len, fold, ch, t, k,
-                                                        rounds_out, final_out);
+                                                        rounds_out, final_out, partials, stride);
   LGS_LAUNCH_CHECK();
 }
 }  // namespace
