@@ -5,12 +5,14 @@
 // accumulators and panics when a result leaves the i64 range; this kernel does the same products
 // exactly (128-bit accumulators) and reports such a result as an error instead.
 //
-// The values are fixed-point integers (scale 2^12, activations up to about 2^20), not int8, so the
-// product runs on the integer pipes: a 32 x 64 output tile per CTA, 16 x 16 threads with a 2 x 4
-// block each, the K dimension staged through shared memory 32 at a time, exact 128-bit sums as
-// (hi, lo) words.  GPT-2's layers have 31 rows, so K is split over CTAs to fill the GPU and the
-// exact partial sums are added by a second kernel.  The largest layer, the vocabulary head
-// (31 x 768 x 50257), is 1.2 G products.
+// The values are fixed-point integers (scale 2^12, activations up to about 2^20), not int8: a
+// 32 x 64 output tile per CTA, 16 x 16 threads with a 2 x 4 block each, the K dimension staged
+// through shared memory 32 at a time.  Each stage sums in the cheapest exact arithmetic its
+// operands allow (fused multiply-adds of doubles while every partial sum stays below 2^53, else
+// 64-bit or 128-bit integer sums) and adds the stage sum to exact 128-bit (hi, lo) accumulators.
+// GPT-2's layers have 31 rows, so K is split over CTAs to fill the GPU and the exact partial sums
+// are added by a second kernel.  The largest layer, the vocabulary head (31 x 768 x 50257), is
+// 1.2 G products.
 #include <algorithm>
 #include <cstring>
 
