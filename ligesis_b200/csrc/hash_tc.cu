@@ -41,7 +41,8 @@ constexpr int NTHREADS = 320;
 constexpr int TMEM_COLS = 512;
 constexpr int EPI_COLS = 16;     // accumulator columns drained per epilogue step
 constexpr int SS_PITCH = 260;    // u32 per drained column (256 limb rows + pad, 16-byte rows)
-constexpr int SS_BYTES = EPI_COLS * SS_PITCH * 4;
+constexpr int SS_WORDS = EPI_COLS * SS_PITCH;  // one staging buffer; two alternate
+constexpr int SS_BYTES = 2 * SS_WORDS * 4;
 constexpr int NBARS = 2 * TC_STAGES + 3;
 constexpr int SMEM_BYTES = TC_STAGES * STAGE_BYTES + SS_BYTES + 1024 /*align*/ + 128 /*barriers*/;
 constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s at 1.9 GHz
@@ -311,29 +312,31 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      // Step q stages its columns in buffer q & 1: the step before last read that buffer before
+      // the previous step's barrier, so one barrier per step suffices.
       for (int q = 0; q < TC_N / EPI_COLS; ++q) {
+        uint32_t* Sb = Ss + (q & 1) * SS_WORDS;
         uint32_t r0[16], r1[16];
         tmem_ld16(tmem + lane_off + EPI_COLS * q, r0);
         tmem_ld16(tmem + lane_off + 256 + EPI_COLS * q, r1);
         tmem_wait_ld();
 #pragma unroll
         for (int cc = 0; cc < EPI_COLS; ++cc) {
-          Ss[cc * SS_PITCH + mrow] = r0[cc];
-          Ss[cc * SS_PITCH + 128 + mrow] = r1[cc];
+          Sb[cc * SS_PITCH + mrow] = r0[cc];
+          Sb[cc * SS_PITCH + 128 + mrow] = r1[cc];
         }
         epi_sync();
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
           const unsigned idx = et + NEPI * i, col = idx & (EPI_COLS - 1), r = idx >> 4;
-          const uint4 lo4 = *(const uint4*)&Ss[col * SS_PITCH + 8 * r];
-          const uint4 hi4 = *(const uint4*)&Ss[col * SS_PITCH + 8 * r + 4];
+          const uint4 lo4 = *(const uint4*)&Sb[col * SS_PITCH + 8 * r];
+          const uint4 hi4 = *(const uint4*)&Sb[col * SS_PITCH + 8 * r + 4];
           const u64 a = (u64)lo4.x + ((u64)lo4.y << 8) + ((u64)lo4.z << 16) + ((u64)lo4.w << 24);
           const u64 b = (u64)hi4.x + ((u64)hi4.y << 8) + ((u64)hi4.z << 16) + ((u64)hi4.w << 24);
           const u64 lo = a + (b << 32);
           const u64 hi = (b >> 32) + (lo < a ? 1 : 0);
           H[(size_t)r * two_n + j0 + EPI_COLS * q + col] = gl_reduce(lo, hi);
         }
-        epi_sync();
       }
       // accumulators drained: the MMAs of the next tile may start
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
