@@ -50,11 +50,21 @@ __device__ void eq_table_smem(const ef2* p, unsigned b, ef2* tab) {
     tab[j] = ef_mul(half_tabs[j & (n1 - 1)], half_tabs[32 + (j >> b1)]);
   __syncthreads();
 }
-// prod_{t in [b, k)} (bit t of idx ? p[t] : 1 - p[t])
-__device__ ef2 eq_high(const ef2* p, unsigned b, unsigned k, size_t idx) {
+// prod_{t in [b, k)} (bit t of idx ? p[t] : 1 - p[t]), by a whole warp: lane l multiplies the
+// terms t = b + l, b + l + 32, and a shuffle tree multiplies the lanes' products (the field
+// product does not depend on the order, so every lane gets the same element).  One thread alone
+// took a chain of k - b dependent products while the rest of its CTA waited.
+__device__ ef2 eq_high_warp(const ef2* p, unsigned b, unsigned k, size_t idx) {
   ef2 acc = ef_one();
-  for (unsigned t = b; t < k; ++t)
+  if (k <= b + 6) {  // a short chain: every lane alone, no tree
+    for (unsigned t = b; t < k; ++t)
+      acc = ef_mul(acc, ((idx >> t) & 1) ? p[t] : ef_sub(ef_one(), p[t]));
+    return acc;
+  }
+  for (unsigned t = b + (threadIdx.x & 31); t < k; t += 32)
     acc = ef_mul(acc, ((idx >> t) & 1) ? p[t] : ef_sub(ef_one(), p[t]));
+#pragma unroll
+  for (int m = 16; m; m >>= 1) acc = ef_mul(acc, shfl_xor_ef(acc, m));
   return acc;
 }
 }  // namespace
@@ -104,8 +114,11 @@ __global__ void new_eq_kernel(const ef2* __restrict__ point, unsigned k, ef2* __
   __syncthreads();
   const unsigned b = k < EQ_TILE_LOG ? k : EQ_TILE_LOG;
   const size_t base = (size_t)blockIdx.x << b;
-  if (threadIdx.x == 0) hi = eq_high(p, b, k, base);
-  eq_table_smem(p, b, tab);
+  if (threadIdx.x < 32) {
+    const ef2 h = eq_high_warp(p, b, k, base);
+    if (threadIdx.x == 0) hi = h;
+  }
+  eq_table_smem(p, b, tab);  // ends with a barrier, so hi is visible
   for (unsigned j = threadIdx.x; j < (1u << b); j += blockDim.x) out[base + j] = ef_mul(hi, tab[j]);
 }
 void new_eq_dev(const ef2* point, unsigned k, ef2* out, cudaStream_t st) {
@@ -131,7 +144,10 @@ __global__ void combine_eq_kernel(const ef2* __restrict__ points, unsigned npts,
   for (unsigned q = 0; q < PER; ++q) acc[q] = ef_zero();
   ef2 g = ef_one();
   for (unsigned j = 0; j < npts; ++j) {
-    if (threadIdx.x == 0) coef = ef_mul(g, eq_high(p + j * k, b, k, base));
+    if (threadIdx.x < 32) {
+      const ef2 h = eq_high_warp(p + j * k, b, k, base);
+      if (threadIdx.x == 0) coef = ef_mul(g, h);
+    }
     eq_table_smem(p + j * k, b, tab);  // ends with a barrier, so coef is visible
 #pragma unroll
     for (unsigned q = 0; q < PER; ++q) {
@@ -177,7 +193,10 @@ __global__ void eq_dot_kernel(const void* __restrict__ vec, const ef2* __restric
     }
   }
   acc = block_sum(acc, red);
-  if (threadIdx.x == 0) partials[blockIdx.x] = ef_mul(acc, eq_high(p, b, k, base));
+  if (threadIdx.x < 32) {
+    const ef2 h = eq_high_warp(p, b, k, base);
+    if (threadIdx.x == 0) partials[blockIdx.x] = ef_mul(acc, h);
+  }
 }
 __global__ void sum_partials_kernel(const ef2* __restrict__ partials, size_t n, ef2* out) {
   __shared__ ef2 red[32];
@@ -292,8 +311,10 @@ __global__ void eq_dot_multi_kernel(const EqDotTask* __restrict__ tasks, unsigne
   for (unsigned j = threadIdx.x; j < (1u << b); j += blockDim.x)
     acc = ef_add(acc, ef_mul(task.vec[base + j], tab[j]));
   acc = block_sum(acc, red);
-  if (threadIdx.x == 0)
-    partials[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = ef_mul(acc, eq_high(p, b, k, base));
+  if (threadIdx.x < 32) {
+    const ef2 h = eq_high_warp(p, b, k, base);
+    if (threadIdx.x == 0) partials[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = ef_mul(acc, h);
+  }
 }
 __global__ void eq_dot_multi_reduce(const EqDotTask* __restrict__ tasks,
                                     const ef2* __restrict__ partials, unsigned ntiles) {
