@@ -14,9 +14,10 @@ than the 126 MB L2, so no step starts from a warm L2.
           whole job (max over ranks / N; N > 1 runs N independent replicas).
 `e2e`     the same through the public API (`Ligesis.commit` on a pinned host f, then
           `Ligesis.prove`), host->device copy of f and the proof read-back inside the region.
-`--impl reference`: the CPU restatement of the reference prover (single-threaded, as the
-          reference prescribes), timed on a bounded sample (mu = 20, 2^6 x 2^14) scaled x16 to
-          mu = 24 (the dominant subset-sum hash is linear in 2^mu).
+`--impl reference`: the CPU restatement of the reference prover (oracle/), timed on the same
+          mu = 24 workload and inputs, commit and prove separately as
+          pcs/benches/ligesis.rs:31-38 times them; its independent loops (rows, columns,
+          sumcheck pairs) split over every host core this process may use.
 """
 from __future__ import annotations
 
@@ -33,18 +34,30 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+# The line's shape: mu = 24 as 2^7 x 2^17 by default; `--log-m/--log-n` select another
+# reference-valid shape (mu = 26 is 2^7 x 2^19).
 LOG_M, LOG_N = 7, 17
 MU = LOG_M + LOG_N
-SAMPLE_SHAPE = (6, 14)  # CPU sample: mu = 20, scaled by 2^(24-20)
-METRIC = "LigeSIS commit+eval ms at mu=24 (2^7 x 2^17)"
+L2_BYTES = 126 << 20
+
+
+def metric_for(log_m: int, log_n: int) -> str:
+    return f"LigeSIS commit+eval ms at mu={log_m + log_n} (2^{log_m} x 2^{log_n})"
+
+
+METRIC = metric_for(LOG_M, LOG_N)
 
 
 def _config(n_gpus: int) -> dict:
+    f_mib, cw_mib = (8 << MU) >> 20, (16 << MU) >> 20
+    l2 = (f"inputs larger than L2 (f {f_mib} MiB, codeword {cw_mib} MiB); no flush needed"
+          if (8 << MU) > L2_BYTES else
+          f"inputs smaller than L2 (f {(8 << MU) >> 10} KiB): a test shape, not a bench line")
     return {
-        "workload": "LigeSIS commit+eval, mu=24 as 2^7 x 2^17, C=32, eta=64, s=128, RS rate 1/2, "
-                    "Basefold batched open (100 queries)",
+        "workload": f"LigeSIS commit+eval, mu={MU} as 2^{LOG_M} x 2^{LOG_N}, C=32, eta=64, s=128, "
+                    "RS rate 1/2, Basefold batched open (100 queries)",
         "log_m": LOG_M, "log_n": LOG_N,
-        "l2": "inputs larger than L2 (f 128 MiB, codeword 256 MiB); no flush needed",
+        "l2": l2,
         "parallelism": "replicas" if n_gpus > 1 else "single",
     }
 
@@ -69,27 +82,46 @@ def _max_over_ranks(ms: float, dist, device) -> float:
 
 
 # ------------------------------------------------------------------------------------------------
-# CPU baseline: the oracle (a single-threaded restatement of the reference prover)
+# CPU baseline: the oracle (the C++ restatement of the reference prover)
 # ------------------------------------------------------------------------------------------------
-def cpu_sample_ms(shape=SAMPLE_SHAPE, seed: int = 1) -> tuple[float, dict]:
+def bench_inputs(rank: int = 0):
+    """The workload's inputs: f (seed 1 + rank), A (seed 2), z (seed 3), oracle arrays (seed 4)."""
     from ligesis_b200 import rng
-    from oracle import orc
 
-    lm, ln = shape
-    f = rng.field_elements(seed, 1 << (lm + ln))
-    A = rng.field_elements(seed + 1, 32 * (64 << lm)).reshape(32, 64 << lm)
-    z = rng.ext_elements(seed + 2, lm + ln)
-    g = rng.SeededRng(seed + 3)
-    fields, ints = g.ext_elements(4096), g.ints(4096)
-    key = orc.Key(lm, ln, A)
-    t0 = time.perf_counter()
-    cm = orc.Commitment(key, f)
-    t1 = time.perf_counter()
-    orc.prove(key, cm, z, fields, ints)
-    t2 = time.perf_counter()
-    scale = 2 ** (MU - (lm + ln))
-    info = {"commit_s": round(t1 - t0, 3), "prove_s": round(t2 - t1, 3), "scale": scale}
-    return (t2 - t0) * 1e3 * scale, info
+    f = rng.field_elements(1 + rank, 1 << MU)
+    A = rng.field_elements(2, 32 * (64 << LOG_M)).reshape(32, 64 << LOG_M)
+    z = rng.ext_elements(3, MU)
+    g = rng.SeededRng(4)
+    return f, A, z, g.ext_elements(4096), g.ints(4096)
+
+
+class CpuProver:
+    """The oracle's setup, commit and prove on the bench workload.  Setup (the key and its
+    Basefold commitment of A) is made once, outside any timing, as pcs/benches/ligesis.rs:28
+    times it apart from commit and eval."""
+
+    def __init__(self, threads: int | None = None, rank: int = 0):
+        from oracle import orc
+
+        self.orc = orc
+        self.threads = orc.set_threads(threads)
+        self.f, A, self.z, self.fields, self.ints = bench_inputs(rank)
+        self.key = orc.Key(LOG_M, LOG_N, A)
+
+    def step(self) -> tuple[float, float, bytes, bytes]:
+        """One commit + prove: (commit s, prove s, root, proof bytes)."""
+        t0 = time.perf_counter()
+        cm = self.orc.Commitment(self.key, self.f)
+        t1 = time.perf_counter()
+        proof, _ = self.orc.prove(self.key, cm, self.z, self.fields, self.ints)
+        t2 = time.perf_counter()
+        return t1 - t0, t2 - t1, cm.root, proof
+
+    def sample_text(self, commit_s: float, prove_s: float, steps: int) -> str:
+        return (f"oracle commit+prove on the full mu={MU} workload (2^{LOG_M} x 2^{LOG_N}, same "
+                f"inputs as the GPU arm), "
+                f"{steps} step(s), mean commit {commit_s:.2f} s + prove {prove_s:.2f} s; "
+                f"{self.threads} threads on {_cpu_model()}")
 
 
 def _cpu_model() -> str:
@@ -106,24 +138,25 @@ def run_reference(args) -> None:
     rank, world, _ = _dist()
     if rank != 0:
         return
+    cpu = CpuProver()
     for _ in range(args.warmup):
-        cpu_sample_ms()
-    times, info = [], {}
+        cpu.step()
+    commit_s, prove_s = [], []
     for _ in range(args.steps):
-        ms, info = cpu_sample_ms()
-        times.append(ms)
-    ms = statistics.mean(times)
-    sample = (f"oracle commit+prove at mu=20 (2^6 x 2^14), {info['commit_s']}+{info['prove_s']} s "
-              f"per sample, scaled x{info['scale']} to mu=24 (the dominant subset-sum hash is "
-              f"linear in 2^mu); 1 thread on {_cpu_model()}")
+        c, p, _, _ = cpu.step()
+        commit_s.append(c)
+        prove_s.append(p)
+    c_ms, p_ms = statistics.mean(commit_s) * 1e3, statistics.mean(prove_s) * 1e3
+    ms = c_ms + p_ms
     line = {
-        "metric": METRIC, "value": round(ms, 1), "unit": "ms", "n_gpus": world,
+        "metric": metric_for(LOG_M, LOG_N), "value": round(ms, 1), "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 1),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (mod p)",
         "data": "synthetic (seeded uniform Goldilocks)", "config": _config(world),
         "impl": "reference",
-        "cpu_baseline": {"value": round(ms, 1), "unit": "ms", "cores": 1, "kind": "port",
-                         "sample": sample},
+        "stages_ms": {"commit": round(c_ms, 1), "prove": round(p_ms, 1)},
+        "cpu_baseline": {"value": round(ms, 1), "unit": "ms", "cores": cpu.threads, "kind": "port",
+                         "sample": cpu.sample_text(c_ms / 1e3, p_ms / 1e3, args.steps)},
         "e2e": {"value": round(ms, 1), "unit": "ms", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -198,7 +231,49 @@ class ClockSampler:
 # DRAM bytes (read + write) per launch of the two commit stages at mu = 24, from one ncu capture
 # each (`bench.py --mode commit --steps 3` under ncu --set full; profiles/rs_encode_mu24.md and
 # profiles/hash_tc_mu24.md): rs_encode = rs_pass_a + rs_pass_b.
-NCU_TRAFFIC = {"rs_encode": 842.0e6, "subset_sum_hash": 326.6e6}
+NCU_TRAFFIC_MU24 = {"rs_encode": 842.0e6, "subset_sum_hash": 326.6e6}
+
+
+def ncu_traffic(stage: str) -> float:
+    """Per-launch DRAM bytes of a stage at the line's mu: the mu = 24 capture scaled by 2^(mu-24)
+    (both stages stream arrays proportional to 2^mu)."""
+    return NCU_TRAFFIC_MU24[stage] * 2.0 ** (MU - 24)
+
+
+def prove_work(log_m: int, log_n: int) -> dict:
+    """Algorithmic HBM bytes and F_{p^2} multiplications of one prove (pcs/src/ligesis.rs:347-549)
+    at this shape, item by item: each array is counted once per pass that must touch it.  A
+    sumcheck over 2^k entries of S stored factors reads its vectors once per round and writes the
+    folded halves: 48 S 2^k bytes; per pair and round it multiplies d + S times (products at the
+    evaluation points and the folds).  Kernel-launch latency, partial sums and the proof gather
+    are not counted."""
+    m, n = 1 << log_m, 1 << log_n
+    two_n, W, S = 2 * n, 64 * m, 128
+    WS = W * S
+    R = max(11 + log_m, log_m + 13, log_n) - 6  # Basefold fold rounds (shared domain)
+    D = 2 << R  # Basefold codeword length (rate 1/2)
+
+    def sc(k_len, s_fac, d):
+        return 48.0 * s_fac * k_len, (d + s_fac) * k_len  # bytes, EF muls (pairs x 2 rounds)
+
+    items = {
+        "abar_gemv": (8.0 * m * n + 16.0 * n, 1.0 * m * n / 2),  # BF x EF = half an EF mul
+        "bi_gather_lift": (32.0 * m * S + 8.0 * WS + 2 * (8.0 + 16.0) * WS, 0.0),
+        "eq_tables": (16.0 * (WS + WS + n + W), 2.0 * WS + n),
+        "sc_binary": sc(WS, 2, 3),
+        "sc_bi_batch": sc(WS, 2, 2),
+        "sc_hash_recon": tuple(2 * v for v in sc(W, 2, 2)),
+        "sc_table": sc(two_n, 2, 2),
+        "sc_rslink_a_batch": tuple(2 * v for v in sc(n, 2, 2)),
+        "g1_g2_v": (8.0 * 32 * W + 8.0 * WS + 3 * 16.0 * W, 32.0 * W),
+        "rs_abar": (16.0 * n + 32.0 * two_n + 2 * 32.0 * two_n, 0.0),
+        "basefold_commit_bi": (8.0 * WS * 2 + 16.0 * WS * 3 + 32.0 * D, 0.0),
+        "basefold_commit_abar": (16.0 * n * 2 + 32.0 * n * 3 + 32.0 * D, 0.0),
+        "batch_open": (8.0 * (32 * W + WS) + 16.0 * n + 16.0 * D * 4, 4.0 * D),
+    }
+    return {"bytes": sum(v[0] for v in items.values()),
+            "ef_muls": sum(v[1] for v in items.values()),
+            "items_mb": {k: round(v[0] / 1e6, 2) for k, v in items.items()}}
 
 
 def _peaks() -> dict:
@@ -230,11 +305,7 @@ def run_ours(args) -> None:
     ctx = L.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=torch.device("cuda", local))
 
-    f = rng.field_elements(1 + rank, 1 << MU)
-    A = rng.field_elements(2, 32 * (64 << LOG_M)).reshape(32, 64 << LOG_M)
-    z = rng.ext_elements(3, MU)
-    g = rng.SeededRng(4)
-    fields, ints = g.ext_elements(4096), g.ints(4096)
+    f, A, z, fields, ints = bench_inputs(rank)
     pk, vk = L.Ligesis.setup_with_hash(LOG_M, LOG_N, L.SubsetSumHash(64 << LOG_M, a=A), ctx)
     f_dev = torch.from_numpy(f.view(np.int64)).to(f"cuda:{local}")
     f_pin = torch.from_numpy(f.view(np.int64)).pin_memory()
@@ -339,7 +410,7 @@ def run_ours(args) -> None:
         peak = i8.value
         roof = {"kernel": "subset_sum_hash (hash_tc_kernel)", "bound": "tensor",
                 "achieved": round(ach, 1), "peak": round(peak, 1), "unit": "TOP/s (int8)",
-                "frac": round(ach / peak, 4), "traffic": NCU_TRAFFIC["subset_sum_hash"],
+                "frac": round(ach / peak, 4), "traffic": ncu_traffic("subset_sum_hash"),
                 "peak_src": "measured: tcgen05.mma kind::i8 M128N256K32 from shared memory on "
                             "every SM (lgs_tensor_peak_i8)",
                 "algorithmic": f"{hash_ops:.3e} int8 ops per launch"}
@@ -348,7 +419,7 @@ def run_ours(args) -> None:
         peak = peaks["hbm_gbs"]
         roof = {"kernel": "rs_encode (rs_pass_a + rs_pass_b)", "bound": "hbm",
                 "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(ach / peak, 4), "traffic": NCU_TRAFFIC["rs_encode"],
+                "frac": round(ach / peak, 4), "traffic": ncu_traffic("rs_encode"),
                 "peak_src": ("measured HBM copy (MEASURED_PEAKS.json)" if peaks["src"] == "measured"
                              else "fallback: 6.65 TB/s, an earlier copy measurement on this pool "
                                   "(MEASURED_PEAKS.json absent)"),
@@ -358,25 +429,37 @@ def run_ours(args) -> None:
         a = ntt_bytes / (stages["rs_encode"] * 1e-3) / 1e9
         others["rs_encode"] = {"bound": "hbm", "achieved": round(a, 1), "unit": "GB/s",
                                "peak": peaks["hbm_gbs"], "frac": round(a / peaks["hbm_gbs"], 4),
-                               "traffic": NCU_TRAFFIC["rs_encode"]}
+                               "traffic": ncu_traffic("rs_encode")}
     if "subset_sum_hash" in stages:
         a = hash_ops / (stages["subset_sum_hash"] * 1e-3) / 1e12
         others["subset_sum_hash"] = {"bound": "tensor", "achieved": round(a, 1),
                                      "unit": "TOP/s (int8)", "peak": round(i8.value, 1),
                                      "frac": round(a / i8.value, 4),
-                                     "traffic": NCU_TRAFFIC["subset_sum_hash"]}
+                                     "traffic": ncu_traffic("subset_sum_hash")}
+
+    if "prove_device" in stages:
+        pw = prove_work(LOG_M, LOG_N)
+        t = stages["prove_device"] * 1e-3
+        a = pw["bytes"] / t / 1e9
+        others["prove_device"] = {
+            "bound": "hbm", "achieved": round(a, 1), "unit": "GB/s", "peak": peaks["hbm_gbs"],
+            "frac": round(a / peaks["hbm_gbs"], 4), "traffic": None,
+            "algorithmic": f"{pw['bytes']:.3e} bytes, {pw['ef_muls']:.3e} F_p2 muls per prove",
+            "ef_muls_per_s": round(pw["ef_muls"] / t / 1e9, 2), "items_mb": pw["items_mb"],
+            "note": "the prove's time inside the step (beside the commit's hash and tree)"}
 
     cpu = None
-    if not args.no_cpu_baseline:
-        cms, info = cpu_sample_ms()
-        cpu = {"value": round(cms, 1), "unit": "ms", "cores": 1, "kind": "port",
-               "sample": f"oracle commit+prove at mu=20 (2^6 x 2^14), "
-                         f"{info['commit_s']}+{info['prove_s']} s, scaled x{info['scale']} to "
-                         f"mu=24; 1 thread on {_cpu_model()}"}
+    if not args.no_cpu_baseline and world == 1:
+        # one full step of the same workload (not scaled); its root and proof must equal ours
+        cp = CpuProver(rank=rank)
+        c_s, p_s, c_root, c_proof = cp.step()
+        assert c_root == root_dev and c_proof == proof_dev, "oracle and GPU proofs differ"
+        cpu = {"value": round((c_s + p_s) * 1e3, 1), "unit": "ms", "cores": cp.threads,
+               "kind": "port", "sample": cp.sample_text(c_s, p_s, 1)}
 
     value = dev_ms / world
     line = {
-        "metric": METRIC, "value": round(value, 3), "unit": "ms", "n_gpus": world,
+        "metric": metric_for(LOG_M, LOG_N), "value": round(value, 3), "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dev_ms, 3),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (mod p)",
         "data": "synthetic (seeded uniform Goldilocks)", "config": _config(world),
@@ -546,37 +629,160 @@ def run_serve(args) -> None:
 
 
 def run_commit(args) -> None:
-    """Setup, then `--steps` commits of the mu=24 polynomial already in HBM (no prove): the
-    case the per-kernel ncu captures of the commit kernels run."""
+    """Commit only (RS encode, subset-sum hash with its leaf hashes, Merkle tree) of a polynomial
+    already in HBM, `--steps` times after warm-up, per shape: the square shapes 2^10 x 2^10,
+    2^12 x 2^12 and 2^13 x 2^13 (mu = 20, 24, 26) that setup's shared-domain window rejects run
+    through the commit-only key.  Also the case the per-kernel ncu captures of the commit
+    kernels run (--shapes 7x17)."""
+    import ctypes as C
+
     import numpy as np
     import torch
 
     import ligesis_b200 as L
     from ligesis_b200 import rng
 
-    lm, ln = args.log_m, args.log_n
+    shapes = [tuple(int(v) for v in sh.split("x")) for sh in args.shapes.split(",")]
     lib = L.load()
     ctx = L.Context(0)
-    f = rng.field_elements(1, 1 << (lm + ln))
-    A = rng.field_elements(2, 32 * (64 << lm)).reshape(32, 64 << lm)
-    pk, _ = L.Ligesis.setup_with_hash(lm, ln, L.SubsetSumHash(64 << lm, a=A), ctx)
-    f_dev = torch.from_numpy(f.view(np.int64)).to("cuda:0")
-    import ctypes as C
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=torch.device("cuda", 0))
+    peaks = _peaks()
+    i8 = C.c_double()
+    L._lib.check(lib.lgs_tensor_peak_i8(ctx.handle, 32768, C.byref(i8)))
+    for lm, ln in shapes:
+        f = rng.field_elements(1, 1 << (lm + ln))
+        A = rng.field_elements(2, 32 * (64 << lm)).reshape(32, 64 << lm)
+        hsh = L.SubsetSumHash(64 << lm, a=A)
+        full = L.shape_ok(lm, ln)
+        pk = (L.Ligesis.setup_with_hash(lm, ln, hsh, ctx)[0] if full
+              else L.Ligesis.setup_commit_only(lm, ln, hsh, ctx))
+        f_dev = torch.from_numpy(f.view(np.int64)).to("cuda:0")
+        roots = set()
+        for _ in range(args.warmup):
+            commit, data = L.Ligesis.commit_device(pk, f_dev.data_ptr(), f.size)
+            roots.add(commit.root)
+            del data
+        L._lib.check(lib.lgs_profile(ctx.handle, 1))
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            commit, data = L.Ligesis.commit_device(pk, f_dev.data_ptr(), f.size)
+            roots.add(commit.root)  # waits for the commit's hash stream too
+            del data
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        stages = {}
+        for name in ("rs_encode", "subset_sum_hash", "merkle_h"):
+            tot, cnt = C.c_double(), C.c_uint64()
+            L._lib.check(lib.lgs_profile_get(ctx.handle, name.encode(), C.byref(tot), C.byref(cnt)))
+            if cnt.value:
+                stages[name] = round(tot.value / cnt.value, 4)
+        L._lib.check(lib.lgs_profile(ctx.handle, 0))
+        m, n = 1 << lm, 1 << ln
+        W, two_n = 64 * m, 2 * n
+        ntt_gbs = (8.0 * m * n + 8.0 * m * two_n) / (stages["rs_encode"] * 1e-3) / 1e9
+        hash_tops = 2.0 * 256 * W * two_n / (stages["subset_sum_hash"] * 1e-3) / 1e12
+        merkle_gbs = (256.0 * two_n + 64.0 * (two_n - 1)) / (stages["merkle_h"] * 1e-3) / 1e9
+        print(json.dumps({
+            "mode": "commit", "metric": f"LigeSIS commit ms at mu={lm + ln} (2^{lm} x 2^{ln})",
+            "value": round(ms, 4), "unit": "ms", "log_m": lm, "log_n": ln,
+            "key": "setup" if full else "commit-only (outside setup's shared-domain window)",
+            "steps": args.steps, "warmup": args.warmup, "stages_ms": stages,
+            "ntt_gbs": round(ntt_gbs, 1), "ntt_frac_hbm": round(ntt_gbs / peaks["hbm_gbs"], 4),
+            "hash_int8_tops": round(hash_tops, 1),
+            "hash_frac_int8": round(hash_tops / i8.value, 4),
+            "merkle_input_gbs": round(merkle_gbs, 1), "roots_identical": len(roots) == 1,
+            "timing": "CUDA events on the library stream; f resident in HBM"}), flush=True)
+        del pk, f_dev, commit
 
-    L._lib.check(lib.lgs_profile(ctx.handle, 1))
-    roots = set()
-    for _ in range(args.steps):
-        commit, data = L.Ligesis.commit_device(pk, f_dev.data_ptr(), f.size)
-        roots.add(commit.root)
-        del data
-    stages = {}
-    for name in ("rs_encode", "subset_sum_hash", "merkle_h"):
-        tot, cnt = C.c_double(), C.c_uint64()
-        L._lib.check(lib.lgs_profile_get(ctx.handle, name.encode(), C.byref(tot), C.byref(cnt)))
-        if cnt.value:
-            stages[name] = round(tot.value / cnt.value, 4)
-    print(json.dumps({"mode": "commit", "log_m": lm, "log_n": ln, "commits": args.steps,
-                      "stages_ms": stages, "roots_identical": len(roots) == 1}), flush=True)
+
+def run_sumcheck(args) -> None:
+    """The reference's sumcheck microbenchmark (pcs/benches/sumcheck.rs:64-68: a product of 3
+    multilinears) over F_{p^2} at mu = 20, 22, 24, device-resident factors; the eq-product
+    variant [eq_z, f, g] (eq_z built on the device first, inside the timing); and an MlPoly
+    new_eq / fold (one variable) / eval sweep.  Each timed call gets fresh inputs: the factors
+    are folded in place, so they are restored from a pristine copy between calls, outside the
+    CUDA events.  Bytes are algorithmic: the sumcheck reads its 3 x 16 B factors once per round
+    and writes the folded half (144 B per element over all rounds); new_eq writes 16 B per
+    entry, fold reads 16 B and writes 8 B per input entry, eval reads 16 B per entry."""
+    import numpy as np
+    import torch
+
+    import ligesis_b200 as L
+    from ligesis_b200 import rng
+
+    lib = L.load()
+    ctx = L.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=torch.device("cuda", 0))
+    peaks = _peaks()
+    mus = [int(v) for v in args.mus.split(",")]
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a).view(np.int64).reshape(-1)).to("cuda:0")
+
+    def timed(fn, prep=None):
+        tot = 0.0
+        for i in range(args.warmup + args.steps):
+            if prep:
+                prep()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if i >= args.warmup:
+                tot += e0.elapsed_time(e1)
+        return tot / args.steps
+
+    def line(op, mu, ms, nbytes, **kw):
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        print(json.dumps({"mode": "sumcheck", "op": op, "mu": mu, "value": round(ms, 4),
+                          "unit": "ms", "gbs": round(gbs, 1),
+                          "frac_hbm": round(gbs / peaks["hbm_gbs"], 4), "steps": args.steps,
+                          "warmup": args.warmup, **kw}), flush=True)
+
+    for mu in mus:
+        n = 1 << mu
+        pristine = dev(np.concatenate([rng.ext_elements(9000 + j, n) for j in range(3)]))
+        work = torch.empty_like(pristine)
+        ch = dev(rng.ext_elements(9100 + mu, mu))
+        z = dev(rng.ext_elements(9200 + mu, mu))
+        rounds = torch.zeros(mu * 4 * 2, dtype=torch.int64, device="cuda:0")
+        finals = torch.zeros(3 * 2, dtype=torch.int64, device="cuda:0")
+
+        def restore():
+            work.copy_(pristine)
+
+        def sc():
+            L._lib.check(lib.lgs_sumcheck_prove_dev(ctx.handle, work.data_ptr(), 3, mu,
+                                                    ch.data_ptr(), rounds.data_ptr(),
+                                                    finals.data_ptr()))
+
+        ms = timed(sc, restore)
+        line("sumcheck_3", mu, ms, 144.0 * n, ef_muls_per_s=round(11.0 * n / (ms * 1e-3) / 1e9, 2))
+
+        def eq_variant():
+            L._lib.check(lib.lgs_new_eq_dev(ctx.handle, z.data_ptr(), mu, work.data_ptr()))
+            sc()
+
+        ms = timed(eq_variant, restore)
+        line("sumcheck_eq_f_g", mu, ms, 144.0 * n + 16.0 * n)
+
+        out = torch.empty(2 * n, dtype=torch.int64, device="cuda:0")
+        ms = timed(lambda: L._lib.check(lib.lgs_new_eq_dev(ctx.handle, z.data_ptr(), mu,
+                                                           out.data_ptr())))
+        line("new_eq", mu, ms, 16.0 * n)
+        ms = timed(lambda: L._lib.check(lib.lgs_mle_fold_dev(ctx.handle, pristine.data_ptr(), mu,
+                                                             z.data_ptr(), 1, out.data_ptr())))
+        line("fold_1", mu, ms, 24.0 * n)
+        val = torch.zeros(2, dtype=torch.int64, device="cuda:0")
+        ms = timed(lambda: L._lib.check(lib.lgs_mle_eval_dev(ctx.handle, pristine.data_ptr(), mu,
+                                                             z.data_ptr(), val.data_ptr())))
+        line("eval", mu, ms, 16.0 * n)
+        del pristine, work, out
 
 
 def run_timeline(args) -> None:
@@ -610,16 +816,18 @@ def run_timeline(args) -> None:
     for _ in range(args.steps):
         oracle.restart()
         L.Ligesis.prove(pk, data, z, oracle)
-    marks = ["prefix_end", "abar_end", "A1_abar_commit_end", "A2_rs_abar_table_sc_end", "B_bi_commit_end",
-             "C_binary_sc_end", "D_hash_recon_sc_end", "E_rslink_sc_end", "F_bi_batch_sc_end",
-             "G_a_batch_sc_end", "H_basefold_msgs_end", "main_suffix_start", "main_levels_end",
-             "main_level_trees_end", "join", "tree_ready", "end"]
+    need = C.c_size_t()
+    L._lib.check(lib.lgs_profile_names(ctx.handle, None, 0, C.byref(need)))
+    buf = C.create_string_buffer(need.value)
+    L._lib.check(lib.lgs_profile_names(ctx.handle, buf, need.value, C.byref(need)))
+    names = [nm for nm in buf.value.decode().split("\n") if nm.startswith("tl:")]
     out = {}
-    for name in ["prove_device"] + ["tl:" + m for m in marks]:
+    for name in ["prove_device"] + names:
         tot, cnt = C.c_double(), C.c_uint64()
         L._lib.check(lib.lgs_profile_get(ctx.handle, name.encode(), C.byref(tot), C.byref(cnt)))
         if cnt.value:
             out[name] = round(tot.value / cnt.value, 4)
+    out = dict(sorted(out.items(), key=lambda kv: kv[1]))
     print(json.dumps({"mode": "timeline", "log_m": lm, "log_n": ln, "proves": args.steps,
                       "ms_from_prove_start": out, "root": commit.root.hex()[:16]}), flush=True)
 
@@ -859,6 +1067,7 @@ def run_witness(args) -> None:
 
 
 def main() -> None:
+    global LOG_M, LOG_N, MU
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
@@ -866,10 +1075,13 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", choices=["line", "batch", "serve", "commit", "timeline", "basefold",
-                                       "logup", "witness"], default="line")
+                                       "logup", "witness", "sumcheck"], default="line")
     ap.add_argument("--log-m", type=int, default=LOG_M)
     ap.add_argument("--log-n", type=int, default=LOG_N)
     ap.add_argument("--lanes", type=int, default=12)
+    ap.add_argument("--mus", default="20,22,24", help="sumcheck mode: polynomial sizes")
+    ap.add_argument("--shapes", default="10x10,12x12,13x13",
+                    help="commit mode: comma-separated log_m x log_n shapes")
     ap.add_argument("--mu", type=int, default=None, help="logup mode: one shape, 2^mu queries")
     ap.add_argument("--nu", type=int, default=16, help="logup mode: 2^nu table entries")
     ap.add_argument("--requests", type=int, default=600)
@@ -880,6 +1092,7 @@ def main() -> None:
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    LOG_M, LOG_N, MU = args.log_m, args.log_n, args.log_m + args.log_n
     if args.mode == "batch":
         run_batch(args)
         return
@@ -900,6 +1113,9 @@ def main() -> None:
         return
     if args.mode == "witness":
         run_witness(args)
+        return
+    if args.mode == "sumcheck":
+        run_sumcheck(args)
         return
     if args.impl == "reference":
         run_reference(args)

@@ -38,19 +38,22 @@ inline BasefoldState<LF> commit_on_domain(const std::vector<LF>& poly, unsigned 
   BasefoldState<LF> st;
   auto chunks = mle_split(poly, poly.size() >> li);
   size_t code_len = chunks[0].size() << code_rate;
-  for (auto& c : chunks) {
-    c.resize(code_len, zero_of<LF>());
-    dft_any(c);
-    st.codes.push_back(std::move(c));
-  }
-  std::vector<Hash> lh;
-  lh.reserve(code_len);
-  std::vector<LF> col(st.codes.size());
-  for (size_t p = 0; p < code_len; ++p) {
-    for (size_t j = 0; j < st.codes.size(); ++j) col[j] = st.codes[j][p];
-    auto bytes = ser_leaf(col);
-    lh.push_back(hash_bytes(bytes.data(), bytes.size()));
-  }
+  parallel_ranges(chunks.size(), [&](size_t lo, size_t hi) {
+    for (size_t j = lo; j < hi; ++j) {
+      chunks[j].resize(code_len, zero_of<LF>());
+      dft_any(chunks[j]);
+    }
+  });
+  for (auto& c : chunks) st.codes.push_back(std::move(c));
+  std::vector<Hash> lh(code_len);
+  parallel_ranges(code_len, [&](size_t lo, size_t hi) {
+    std::vector<LF> col(st.codes.size());
+    for (size_t p = lo; p < hi; ++p) {
+      for (size_t j = 0; j < st.codes.size(); ++j) col[j] = st.codes[j][p];
+      auto bytes = ser_leaf(col);
+      lh[p] = hash_bytes(bytes.data(), bytes.size());
+    }
+  }, size_t(1) << 10);
   st.tree = MerkleTree::from_leaf_hashes(std::move(lh));
   *root = st.tree.root();
   st.poly.reserve(poly.size());
@@ -309,8 +312,10 @@ inline Channel make_channel(const BasefoldState<LF>& st, const std::vector<EF>& 
   unsigned li = st.log_interleave;
   auto eq4 = new_eq(std::vector<EF>(pt.begin(), pt.begin() + li));
   c.oracle0.assign(d, ef_zero());
-  for (size_t j = 0; j < st.codes.size(); ++j)
-    for (size_t i = 0; i < d; ++i) c.oracle0[i] += eq4[j] * lift(st.codes[j][i]);
+  parallel_ranges(d, [&](size_t lo, size_t hi) {
+    for (size_t j = 0; j < st.codes.size(); ++j)
+      for (size_t i = lo; i < hi; ++i) c.oracle0[i] += eq4[j] * lift(st.codes[j][i]);
+  }, size_t(1) << 12);
   c.m = st.poly;
   mle_fold(c.m, std::vector<EF>(pt.begin(), pt.begin() + li));
   c.y = mle_eval(st.poly, pt);

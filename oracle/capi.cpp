@@ -51,6 +51,9 @@ struct OrcKey {
 extern "C" {
 
 const char* orc_last_error() { return g_err.c_str(); }
+// Threads for the oracle's independent bulk loops (par.hpp); outputs do not depend on it.
+void orc_set_threads(unsigned n) { oracle_threads() = n ? n : 1; }
+unsigned orc_get_threads() { return oracle_threads(); }
 void orc_free_buf(void* p) { std::free(p); }
 
 // ---- field / primitive checks ----
@@ -188,6 +191,16 @@ void* orc_setup(unsigned log_m, unsigned log_n, const u64* A, uint8_t* com_a) {
     auto* k = new OrcKey;
     setup(log_m, log_n, A, &k->pk, &k->vk);
     std::memcpy(com_a, k->pk.com_a.data(), 32);
+    return k;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return nullptr;
+  }
+}
+void* orc_setup_commit_only(unsigned log_m, unsigned log_n, const u64* A) {
+  try {
+    auto* k = new OrcKey;
+    setup_commit_only(log_m, log_n, A, &k->pk);
     return k;
   } catch (const std::exception& e) {
     g_err = e.what();

@@ -74,17 +74,19 @@ struct LigesisProof {
 inline std::vector<u64> hash_columns(const std::vector<u64>& A, size_t W,
                                      const std::vector<u64>& cw, size_t m, size_t two_n) {
   std::vector<u64> H(C * two_n, 0);
-  std::vector<u64> acc(C);
-  for (size_t j = 0; j < two_n; ++j) {
-    std::fill(acc.begin(), acc.end(), 0);
-    for (size_t i = 0; i < m; ++i) {
-      u64 v = cw[i * two_n + j];
-      for (unsigned k = 0; k < ETA; ++k)
-        if ((v >> k) & 1)
-          for (unsigned r = 0; r < C; ++r) acc[r] = add(acc[r], A[r * W + ETA * i + k]);
+  parallel_ranges(two_n, [&](size_t lo, size_t hi) {  // columns are independent
+    std::vector<u64> acc(C);
+    for (size_t j = lo; j < hi; ++j) {
+      std::fill(acc.begin(), acc.end(), 0);
+      for (size_t i = 0; i < m; ++i) {
+        u64 v = cw[i * two_n + j];
+        for (unsigned k = 0; k < ETA; ++k)
+          if ((v >> k) & 1)
+            for (unsigned r = 0; r < C; ++r) acc[r] = add(acc[r], A[r * W + ETA * i + k]);
+      }
+      for (unsigned r = 0; r < C; ++r) H[r * two_n + j] = acc[r];
     }
-    for (unsigned r = 0; r < C; ++r) H[r * two_n + j] = acc[r];
-  }
+  }, 64);
   return H;
 }
 
@@ -107,27 +109,42 @@ inline void setup(unsigned log_m, unsigned log_n, const u64* A_in, ProvingKey* p
   vk->width = W;
 }
 
+// A key for commit alone: Ligesis::commit (ligesis.rs:277-325) takes any m x n; only setup's
+// Basefold commitment of A (and prove) need the shared-domain window.
+inline void setup_commit_only(unsigned log_m, unsigned log_n, const u64* A_in, ProvingKey* pk) {
+  size_t m = size_t(1) << log_m, W = ETA * m;
+  pk->A.assign(A_in, A_in + C * W);
+  for (auto& x : pk->A) x = canon(x);
+  pk->width = W;
+  pk->log_m = log_m;
+  pk->log_n = log_n;
+}
+
 inline void commit(const ProvingKey& pk, const u64* f, size_t len, CommitData* cd, Hash* root) {
   size_t m = size_t(1) << pk.log_m, n = size_t(1) << pk.log_n, two_n = 2 * n;
   if (len != m * n) throw std::runtime_error("commit: f length");
   cd->f.assign(f, f + len);
   for (auto& x : cd->f) x = canon(x);
   cd->cw.assign(m * two_n, 0);
-  std::vector<u64> row(two_n);
-  for (size_t i = 0; i < m; ++i) {  // ligesis.rs:288-300
-    std::fill(row.begin(), row.end(), 0);
-    std::copy(cd->f.begin() + i * n, cd->f.begin() + (i + 1) * n, row.begin());
-    dft_bf(row);
-    std::copy(row.begin(), row.end(), cd->cw.begin() + i * two_n);
-  }
+  parallel_ranges(m, [&](size_t lo, size_t hi) {  // ligesis.rs:288-300, rows are independent
+    std::vector<u64> row(two_n);
+    for (size_t i = lo; i < hi; ++i) {
+      std::fill(row.begin(), row.end(), 0);
+      std::copy(cd->f.begin() + i * n, cd->f.begin() + (i + 1) * n, row.begin());
+      dft_bf(row);
+      std::copy(row.begin(), row.end(), cd->cw.begin() + i * two_n);
+    }
+  });
   cd->H = hash_columns(pk.A, pk.width, cd->cw, m, two_n);
   std::vector<Hash> lh(two_n);  // ligesis.rs:306-313
-  std::vector<u64> col(C);
-  for (size_t j = 0; j < two_n; ++j) {
-    for (unsigned r = 0; r < C; ++r) col[r] = cd->H[r * two_n + j];
-    auto b = serialize_bf(col);
-    lh[j] = hash_bytes(b.data(), b.size());
-  }
+  parallel_ranges(two_n, [&](size_t lo, size_t hi) {
+    std::vector<u64> col(C);
+    for (size_t j = lo; j < hi; ++j) {
+      for (unsigned r = 0; r < C; ++r) col[r] = cd->H[r * two_n + j];
+      auto b = serialize_bf(col);
+      lh[j] = hash_bytes(b.data(), b.size());
+    }
+  }, size_t(1) << 10);
   cd->h_tree = MerkleTree::from_leaf_hashes(std::move(lh));
   *root = cd->h_tree.root();
 }
@@ -154,7 +171,9 @@ inline std::vector<EF> combine_eq(const std::vector<std::vector<EF>>& pts, EF ga
   EF g = ef_one();
   for (auto& p : pts) {
     auto e = new_eq(p);
-    for (size_t i = 0; i < len; ++i) out[i] += g * e[i];
+    parallel_ranges(len, [&](size_t lo, size_t hi) {
+      for (size_t i = lo; i < hi; ++i) out[i] += g * e[i];
+    }, size_t(1) << 15);
     g *= gamma;
   }
   return out;
@@ -177,14 +196,16 @@ inline std::vector<EF> rs_weights(const std::vector<EF>& r3, size_t n, size_t tw
   unsigned lg = lg2(two_n);  // ligesis.rs:553-567
   u64 g = two_adic_generator(lg);
   std::vector<EF> w(n);
-  for (size_t k = 0; k < n; ++k) {
-    EF prod = ef_one();
-    for (unsigned t = 0; t < lg; ++t) {
-      u64 e = (u64)((((u128)1 << t) * k) % two_n);
-      prod *= ef_one() - r3[t] + r3[t] * lift(pow(g, e));
+  parallel_ranges(n, [&](size_t lo, size_t hi) {
+    for (size_t k = lo; k < hi; ++k) {
+      EF prod = ef_one();
+      for (unsigned t = 0; t < lg; ++t) {
+        u64 e = (u64)((((u128)1 << t) * k) % two_n);
+        prod *= ef_one() - r3[t] + r3[t] * lift(pow(g, e));
+      }
+      w[k] = prod;
     }
-    w[k] = prod;
-  }
+  }, size_t(1) << 10);
   return w;
 }
 
@@ -201,9 +222,11 @@ inline LigesisProof prove(const ProvingKey& pk, const CommitData& cd, const std:
   std::vector<EF> z2(z.begin(), z.begin() + log_n), z1(z.begin() + log_n, z.end());
   auto eqz1 = new_eq(z1);
   LigesisProof pf;
-  std::vector<EF> a_vec(n, ef_zero());  // ligesis.rs:372-379
-  for (size_t i = 0; i < m; ++i)
-    for (size_t j = 0; j < n; ++j) a_vec[j] += eqz1[i] * cd.f[i * n + j];
+  std::vector<EF> a_vec(n, ef_zero());  // ligesis.rs:372-379 (columns are independent)
+  parallel_ranges(n, [&](size_t lo, size_t hi) {
+    for (size_t i = 0; i < m; ++i)
+      for (size_t j = lo; j < hi; ++j) a_vec[j] += eqz1[i] * cd.f[i * n + j];
+  }, size_t(1) << 12);
   pf.y = mle_eval(a_vec, z2);
   auto a_vec_state = commit_on_domain<EF>(a_vec, CODE_RATE, shared_li(log_n, log_m, log_n),
                                           &pf.com_a_vec);
@@ -224,8 +247,10 @@ inline LigesisProof prove(const ProvingKey& pk, const CommitData& cd, const std:
     return (cd.cw[(i / ETA) * two_n + j] >> (i % ETA)) & 1;
   };
   std::vector<u64> bi_flat(W * s);  // ligesis.rs:403-410
-  for (size_t i = 0; i < W; ++i)
-    for (size_t k = 0; k < s; ++k) bi_flat[i * s + k] = bit(i, idx[k]);
+  parallel_ranges(W, [&](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; ++i)
+      for (size_t k = 0; k < s; ++k) bi_flat[i * s + k] = bit(i, idx[k]);
+  }, 256);
   unsigned bi_vars = lg2(W * s);
   auto bi_state = commit_on_domain<u64>(bi_flat, CODE_RATE, shared_li(bi_vars, log_m, log_n),
                                         &pf.com_i);
@@ -235,7 +260,9 @@ inline LigesisProof prove(const ProvingKey& pk, const CommitData& cd, const std:
   auto eq_alpha2 = new_eq(alpha2);
 
   std::vector<EF> bi_ef(W * s), bi_m1(W * s);
-  for (size_t i = 0; i < W * s; ++i) bi_ef[i] = lift(bi_flat[i]), bi_m1[i] = bi_ef[i] - ef_one();
+  parallel_ranges(W * s, [&](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; ++i) bi_ef[i] = lift(bi_flat[i]), bi_m1[i] = bi_ef[i] - ef_one();
+  }, size_t(1) << 15);
   std::vector<EF> ch_bin;
   pf.sc_binary = sumcheck_prove({bi_ef, bi_m1, new_eq(alpha1)}, o, &ch_bin);
   auto r1 = rev(ch_bin);

@@ -20,6 +20,7 @@
 
 #include "blake3_ref.hpp"
 #include "gl.hpp"
+#include "par.hpp"
 
 namespace orc {
 
@@ -74,9 +75,13 @@ struct MerkleTree {
     t.layers.push_back(std::move(lh));
     while (t.layers.back().size() > 1) {
       const auto& cur = t.layers.back();
-      std::vector<Hash> next;
-      for (size_t i = 0; i < cur.size(); i += 2)
-        next.push_back(i + 1 < cur.size() ? hash_pair(cur[i], cur[i + 1]) : cur[i]);
+      std::vector<Hash> next((cur.size() + 1) / 2);
+      parallel_ranges(next.size(), [&](size_t lo, size_t hi) {
+        for (size_t k = lo; k < hi; ++k) {
+          size_t i = 2 * k;
+          next[k] = i + 1 < cur.size() ? hash_pair(cur[i], cur[i + 1]) : cur[i];
+        }
+      }, size_t(1) << 12);
       t.layers.push_back(std::move(next));
     }
     return t;

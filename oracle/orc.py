@@ -38,6 +38,8 @@ def lib():
             sig = {
                 "orc_last_error": (C.c_char_p, []),
                 "orc_free_buf": (None, [vp]),
+                "orc_set_threads": (None, [C.c_uint]),
+                "orc_get_threads": (C.c_uint, []),
                 "orc_two_adic_generator": (C.c_int, [C.c_uint, u64p]),
                 "orc_bf_ops": (C.c_int, [u64p, u64p, C.c_size_t, u64p, u64p, u64p]),
                 "orc_ef_ops": (C.c_int, [u64p, u64p, C.c_size_t, u64p, u64p]),
@@ -59,6 +61,7 @@ def lib():
                                                 C.c_size_t, C.c_size_t]),
                 "orc_shape_ok": (C.c_int, [C.c_uint, C.c_uint]),
                 "orc_setup": (vp, [C.c_uint, C.c_uint, u64p, u8p]),
+                "orc_setup_commit_only": (vp, [C.c_uint, C.c_uint, u64p]),
                 "orc_key_free": (None, [vp]),
                 "orc_commit": (vp, [vp, u64p, C.c_size_t, u8p]),
                 "orc_commit_free": (None, [vp]),
@@ -99,6 +102,17 @@ def lib():
                 fn.argtypes = args
             _lib = l
     return _lib
+
+
+def set_threads(n: int | None = None) -> int:
+    """Threads for the oracle's independent bulk loops; None = every core this process may use.
+    The outputs do not depend on the count (exact residues mod p)."""
+    import os
+
+    if n is None:
+        n = len(os.sched_getaffinity(0))
+    lib().orc_set_threads(int(n))
+    return int(lib().orc_get_threads())
 
 
 def _p64(a):
@@ -246,14 +260,19 @@ def merkle_verify(root: bytes, proof: bytes, idx, leaves: np.ndarray, total: int
 
 
 class Key:
-    def __init__(self, log_m: int, log_n: int, A):
+    """setup (commit_only=False) or a key for commit alone, at any shape (commit_only=True)."""
+
+    def __init__(self, log_m: int, log_n: int, A, commit_only: bool = False):
         self.A = _u64(A)
         self.log_m, self.log_n = log_m, log_n
         com = np.zeros(32, np.uint8)
-        h = lib().orc_setup(log_m, log_n, _p64(self.A), _p8(com))
+        if commit_only:
+            h = lib().orc_setup_commit_only(log_m, log_n, _p64(self.A))
+        else:
+            h = lib().orc_setup(log_m, log_n, _p64(self.A), _p8(com))
         if not h:
             raise RuntimeError("oracle setup: " + lib().orc_last_error().decode())
-        self.h, self.com_a = h, com.tobytes()
+        self.h, self.com_a = h, (None if commit_only else com.tobytes())
 
     def __del__(self):
         if getattr(self, "h", None):

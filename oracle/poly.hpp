@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "gl.hpp"
+#include "par.hpp"
 
 namespace orc {
 
@@ -16,8 +17,12 @@ namespace orc {
 inline EF mle_eval(std::vector<EF> s, const std::vector<EF>& point) {
   if ((size_t(1) << point.size()) != s.size()) throw std::runtime_error("mle_eval size");
   size_t cur = s.size() >> 1;
+  std::vector<EF> nx(cur);
   for (const EF& r : point) {
-    for (size_t i = 0; i < cur; ++i) s[i] = s[2 * i] + (s[2 * i + 1] - s[2 * i]) * r;
+    parallel_ranges(cur, [&](size_t lo, size_t hi) {
+      for (size_t i = lo; i < hi; ++i) nx[i] = s[2 * i] + (s[2 * i + 1] - s[2 * i]) * r;
+    }, size_t(1) << 15);
+    std::copy(nx.begin(), nx.begin() + cur, s.begin());
     cur >>= 1;
   }
   return s[0];
@@ -36,12 +41,13 @@ inline std::vector<EF> new_eq(const std::vector<EF>& point) {
   std::vector<EF> ev{ef_one()};
   for (size_t t = point.size(); t-- > 0;) {
     const EF& p = point[t];
-    std::vector<EF> nx;
-    nx.reserve(ev.size() * 2);
-    for (const EF& x : ev) {
-      nx.push_back((ef_one() - p) * x);
-      nx.push_back(p * x);
-    }
+    std::vector<EF> nx(ev.size() * 2);
+    parallel_ranges(ev.size(), [&](size_t lo, size_t hi) {
+      for (size_t j = lo; j < hi; ++j) {
+        nx[2 * j] = (ef_one() - p) * ev[j];
+        nx[2 * j + 1] = p * ev[j];
+      }
+    }, size_t(1) << 15);
     ev.swap(nx);
   }
   return ev;
@@ -80,12 +86,14 @@ inline void dft_bf(std::vector<u64>& a) {
     std::vector<u64> tw(half);
     tw[0] = 1;
     for (size_t k = 1; k < half; ++k) tw[k] = mul(tw[k - 1], w_len);
-    for (size_t i = 0; i < n; i += len)
-      for (size_t k = 0; k < half; ++k) {
+    parallel_ranges(n / 2, [&](size_t lo, size_t hi) {
+      for (size_t t = lo; t < hi; ++t) {
+        size_t i = (t >> (s - 1)) << s, k = t & (half - 1);
         u64 u = a[i + k], v = mul(a[i + k + half], tw[k]);
         a[i + k] = add(u, v);
         a[i + k + half] = sub(u, v);
       }
+    }, size_t(1) << 15);
   }
 }
 // dft_algebra over EF: the base-field DFT applied coordinate-wise.
@@ -143,20 +151,31 @@ inline SumcheckProof sumcheck_prove(std::vector<std::vector<EF>> polys, Oracle& 
   challenges->clear();
   for (unsigned round = 0; round < n; ++round) {
     size_t half = polys[0].size() / 2;
-    std::vector<EF> evals(d + 1, ef_zero());
-    for (size_t i = 0; i < half; ++i) {
-      for (size_t k = 0; k <= d; ++k) {
-        EF t = EF::from(k);
-        EF prod = ef_one();
-        for (auto& p : polys) prod *= p[i] + t * (p[i + half] - p[i]);
-        evals[k] += prod;
+    // Per-range partial sums, added afterwards: the residues are exact, so the split
+    // does not change the round polynomial.
+    const size_t grain = size_t(1) << 14;
+    std::vector<std::vector<EF>> part(parallel_parts(half, grain), std::vector<EF>(d + 1, ef_zero()));
+    parallel_chunks(half, grain, [&](size_t pi, size_t lo, size_t hi) {
+      auto& ev = part[pi];
+      for (size_t i = lo; i < hi; ++i) {
+        for (size_t k = 0; k <= d; ++k) {
+          EF t = EF::from(k);
+          EF prod = ef_one();
+          for (auto& p : polys) prod *= p[i] + t * (p[i + half] - p[i]);
+          ev[k] += prod;
+        }
       }
-    }
+    });
+    std::vector<EF> evals(d + 1, ef_zero());
+    for (auto& ev : part)
+      for (size_t k = 0; k <= d; ++k) evals[k] += ev[k];
     pf.round_polys.push_back(evals);
     EF r = o.next_field();
     challenges->push_back(r);
     for (auto& p : polys) {
-      for (size_t i = 0; i < half; ++i) p[i] = p[i] + r * (p[i + half] - p[i]);
+      parallel_ranges(half, [&](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; ++i) p[i] = p[i] + r * (p[i + half] - p[i]);
+      }, grain);
       p.resize(half);
     }
   }
