@@ -11,12 +11,14 @@
 // 4 = 215,552 values of 16 bytes, about 3.3 MiB) that every GPU loading the library holds until
 // the process exits.  It holds the working copies of the d
 // factors (the sumcheck folds them in place) and the per-round partial sums.  Host code only has
-// a host-side stand-in for the array's name, so its device address is looked up once per device
-// with cudaGetSymbolAddress, on that device's first call; make that first call before any stream
-// capture.  Every call shares the array and it keeps the last call's contents: the copies of the
+// a host-side stand-in for the array's name, so its device address is looked up with
+// cudaGetSymbolAddress on the first call in each CUDA context (normally a device's primary
+// context) and cached for that context; make that first call before any stream capture.
+// Every call shares the array and it keeps the last call's contents: the copies of the
 // factors are rewritten and every partial sum a call reads is written by that same call first,
 // so nothing needs clearing.  Calls that overlap on the GPU (other streams, other host threads)
 // race on the array.
+#include <cuda.h>
 #include <mutex>
 #include <string>
 
@@ -34,21 +36,53 @@ constexpr size_t NA_ELEMS = NA_POLY_ELEMS + NA_PART_ELEMS;
 
 __device__ __align__(256) ef2 g_noalloc_scratch[NA_ELEMS];
 
-constexpr int NA_MAX_DEVICES = 64;
+// The address of a __device__ symbol belongs to a CUDA context, not to a device index: after
+// cudaDeviceReset, or under a driver-API context the caller made current, a device's old
+// address is not mapped.  So the cache is keyed on the current context.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+constexpr int NA_MAX_CONTEXTS = 64;
 std::mutex g_na_mu;
-ef2* g_na_addr[NA_MAX_DEVICES] = {};
+CUcontext g_na_ctx[NA_MAX_CONTEXTS] = {};
+ef2* g_na_addr[NA_MAX_CONTEXTS] = {};
+int g_na_used = 0;
 
-// Device address of the scratch on the current device (looked up on its first use there).
-ef2* scratch_address(int dev) {
-  std::lock_guard<std::mutex> lk(g_na_mu);
-  if (!g_na_addr[dev]) {
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = nullptr;
+  if (!fn) {
     void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      throw CudaError(std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-    g_na_addr[dev] = (ef2*)p;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q);
+    if (e != cudaSuccess || !p || q != cudaDriverEntryPointSuccess)
+      throw CudaError("cuCtxGetCurrent is not available from the driver");
+    fn = (CtxGetCurrentFn)p;
   }
-  return g_na_addr[dev];
+  return fn;
+}
+
+// Device address of the scratch in the current context (looked up on its first use there).
+ef2* scratch_address() {
+  std::lock_guard<std::mutex> lk(g_na_mu);
+  CUcontext ctx = nullptr;
+  if (ctx_get_current()(&ctx) != CUDA_SUCCESS || !ctx)
+    throw CudaError("lgs_sumcheck_prove_noalloc: no current CUDA context");
+  for (int i = 0; i < g_na_used; ++i)
+    if (g_na_ctx[i] == ctx) return g_na_addr[i];
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    throw CudaError(std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+  // A full table (64 contexts seen) drops its oldest entry; that context is likely gone.
+  if (g_na_used == NA_MAX_CONTEXTS) {
+    for (int i = 1; i < NA_MAX_CONTEXTS; ++i) {
+      g_na_ctx[i - 1] = g_na_ctx[i];
+      g_na_addr[i - 1] = g_na_addr[i];
+    }
+    --g_na_used;
+  }
+  int slot = g_na_used++;
+  g_na_ctx[slot] = ctx;
+  g_na_addr[slot] = (ef2*)p;
+  return (ef2*)p;
 }
 
 }  // namespace
@@ -71,10 +105,8 @@ extern "C" lgs_status lgs_sumcheck_prove_noalloc(const uint64_t* polys_dev, unsi
     if (sumcheck_partials_elems(k, d) > NA_PART_ELEMS)
       return set_error(LGS_ERR_INTERNAL, "lgs_sumcheck_prove_noalloc: partials exceed scratch");
     int dev = 0;
-    LGS_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= NA_MAX_DEVICES)
-      return set_error(LGS_ERR_BAD_ARG, "lgs_sumcheck_prove_noalloc: device index too large");
-    ef2* scratch = scratch_address(dev);
+    LGS_CUDA(cudaGetDevice(&dev));  // makes the device's primary context current if none is
+    ef2* scratch = scratch_address();
     cudaStream_t st = (cudaStream_t)stream;
     const size_t len = (size_t)1 << k;
     ef2* polys[NA_MAX_D];

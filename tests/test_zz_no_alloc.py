@@ -4,7 +4,8 @@ It exists for callers that cannot allocate device memory themselves or through t
 process whose HBM belongs to another allocator, or a serving loop that must not pay for
 cudaMalloc's device-wide synchronisation.  They pass device buffers for inputs and outputs and
 the library works in a fixed device array.  This test drives it through the C ABI with device
-buffers and requires the same round polynomials and final evaluations, bit for bit, as the
+buffers and requires the same round polynomials and final evaluations, bit for bit, as the CPU
+oracle's sumcheck prover (an independent restatement of utils/src/sumcheck.rs:37-84) and as the
 allocating entry point lgs_sumcheck_prove, on two calls in a row (different shapes and inputs,
 so the second call also shows that the shared array carries nothing over)."""
 from __future__ import annotations
@@ -29,14 +30,18 @@ def _host(t) -> np.ndarray:
     return t.cpu().numpy().view(np.uint64)
 
 
-def test_noalloc_sumcheck_matches_allocating_entry_point():
+def test_noalloc_sumcheck_matches_oracle(orc):
     import torch
 
     lib = load()
     for call, (d, k) in enumerate([(3, 14), (2, 16)]):
         polys = [rng.ext_elements(900 + 10 * call + j, 1 << k) for j in range(d)]
         ch = rng.ext_elements(950 + call, k)
-        want_rounds, want_finals = L.sumcheck_prove(polys, ch)
+        want_rounds, want_finals, used = orc.sumcheck_prove(polys, ch)
+        assert np.array_equal(used, ch), call
+        alloc_rounds, alloc_finals = L.sumcheck_prove(polys, ch)
+        assert np.array_equal(alloc_rounds, want_rounds), call
+        assert np.array_equal(alloc_finals, want_finals), call
 
         d_polys = _dev(np.concatenate(polys))
         d_ch = _dev(ch)
