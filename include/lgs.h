@@ -47,6 +47,13 @@ lgs_status lgs_ctx_stream(lgs_ctx* ctx, void** stream);
  * com_a receives the Basefold commitment to the flattened A. */
 lgs_status lgs_setup(lgs_ctx* ctx, unsigned log_m, unsigned log_n, const uint64_t* A,
                      lgs_pk** pk, uint8_t com_a[32]);
+/* A key for Ligesis::commit alone (pcs/src/ligesis.rs:277-325, whose RS encoding, hash and
+ * Merkle tree take any m x n): the reference's setup (:239-273) asserts the shared-domain window
+ * log_m + 7 <= log_n <= log_m + 17 that only the prove needs, so square shapes such as
+ * 2^12 x 2^12 can be committed only through this key.  It holds A and its limbs, no Basefold
+ * commitment of A; lgs_prove rejects it (LGS_ERR_BAD_SHAPE).  Needs log_m <= 13, 7 <= log_n. */
+lgs_status lgs_setup_commit_only(lgs_ctx* ctx, unsigned log_m, unsigned log_n, const uint64_t* A,
+                                 lgs_pk** pk);
 void lgs_pk_free(lgs_pk* pk);
 
 /* Ligesis::commit (pcs/src/ligesis.rs:277-325).  f: 2^(log_m+log_n) BF evaluations in host
@@ -243,6 +250,17 @@ lgs_status lgs_engine_pending(lgs_engine* e, size_t* queued, size_t* running_byt
 lgs_status lgs_profile(lgs_ctx* ctx, int enable);
 /* Total device milliseconds and number of timed calls of one stage since lgs_profile(ctx, 1). */
 lgs_status lgs_profile_get(lgs_ctx* ctx, const char* stage, double* total_ms, uint64_t* count);
+/* Names of the stages with totals since lgs_profile(ctx, 1|2), one per line ("tl:<mark>" for
+ * timeline marks); *needed receives the buffer size that holds them all (with the NUL). */
+lgs_status lgs_profile_names(lgs_ctx* ctx, char* buf, size_t cap, size_t* needed);
+/* Clock-cycle budget of the bounded device waits in the kernels this context launches (the
+ * subset-sum hash's pipeline waits; no counterpart in the reference, whose code has no device
+ * waits).  0 restores the default of about 2 s.  A budget shorter than the awaited event makes
+ * the wait give up: the kernel stops its roles, waits for the tensor-core work and the copies it
+ * has in flight (those two drains keep the default budget), frees its tensor memory and returns,
+ * and the call reports LGS_ERR_DEVICE_TIMEOUT; the context stays usable.  For tests of that
+ * path. */
+lgs_status lgs_set_wait_budget(lgs_ctx* ctx, uint64_t cycles);
 /* Number of kernels this library has launched in this process. */
 uint64_t lgs_launch_count(void);
 /* The int8 tensor-core rate the subset-sum hash is measured against: every SM issues `iters` x 4
@@ -277,16 +295,37 @@ lgs_status lgs_mle_eval(lgs_ctx* ctx, const uint64_t* evals, unsigned k, const u
 /* MlPoly::new_eq (utils/src/poly.rs:44-53): 2^k EF. */
 lgs_status lgs_new_eq(lgs_ctx* ctx, const uint64_t* point, unsigned k, uint64_t* out);
 
+/* ---- device-resident forms of the same operations (inputs already in HBM of the context's
+ * device, all canonical; the work is enqueued on the context's stream, lgs_ctx_stream, and the
+ * call returns without waiting for it) ---- */
+/* sumcheck::prove (utils/src/sumcheck.rs:37-84) on d factors of 2^k EF stored factor-major at
+ * polys_dev.  Like the reference's prove, which takes its polys by value, it consumes them:
+ * the factors are folded in place.  rounds_out_dev: k x (d+1) EF; finals_out_dev: d EF. */
+lgs_status lgs_sumcheck_prove_dev(lgs_ctx* ctx, uint64_t* polys_dev, unsigned d, unsigned k,
+                                  const uint64_t* challenges_dev, uint64_t* rounds_out_dev,
+                                  uint64_t* finals_out_dev);
+/* MlPoly::new_eq (utils/src/poly.rs:44-53): 2^k EF written to out_dev. */
+lgs_status lgs_new_eq_dev(lgs_ctx* ctx, const uint64_t* point_dev, unsigned k, uint64_t* out_dev);
+/* MlPoly::fold (utils/src/poly.rs:33-42) of the np lowest variables (1 <= np <= 8) at
+ * point_dev[0 .. np): 2^k EF in, 2^(k-np) EF out. */
+lgs_status lgs_mle_fold_dev(lgs_ctx* ctx, const uint64_t* evals_dev, unsigned k,
+                            const uint64_t* point_dev, unsigned np, uint64_t* out_dev);
+/* MlPoly::eval (utils/src/poly.rs:7-18): one EF written to out_dev. */
+lgs_status lgs_mle_eval_dev(lgs_ctx* ctx, const uint64_t* evals_dev, unsigned k,
+                            const uint64_t* point_dev, uint64_t* out_dev);
+
 /* ---- allocation-free variant (no counterpart in the reference) ----
  * The product sumcheck prover (the same computation as lgs_sumcheck_prove) for callers that
  * must not allocate device memory: processes whose HBM is owned by another allocator, and
  * serving loops that cannot afford cudaMalloc's device-wide synchronisation.  All pointers are
- * device pointers on the current device; polys holds d factors of 2^k EF, factor-major,
- * canonical (< p), and is only read; the work is enqueued on `stream` (a cudaStream_t, NULL for
+ * device pointers on the current device; polys holds d factors of 2^k EF, factor-major, and
+ * challenges_dev k EF, all canonical (< p: unlike lgs_sumcheck_prove, this call does not reduce
+ * its inputs); polys is only read; the work is enqueued on `stream` (a cudaStream_t, NULL for
  * the legacy default stream) and the call returns without waiting for it.  Limits: 1 <= d <= 3,
  * 1 <= k <= 16, else LGS_ERR_BAD_SHAPE.  The working storage is a fixed 3.3 MiB device array
- * that every GPU loading the library holds until exit; the first call on a device looks up its
- * address (make that call before any stream capture); calls that overlap on the GPU race on it.
+ * that every GPU loading the library holds until exit; the first call in a CUDA context (a
+ * device's primary context, normally) looks up the array's address there and caches it for that
+ * context (make that call before any stream capture); calls that overlap on the GPU race on it.
  * It allocates nothing: no cudaMalloc, cudaFree or allocating library call. */
 lgs_status lgs_sumcheck_prove_noalloc(const uint64_t* polys_dev, unsigned d, unsigned k,
                                       const uint64_t* challenges_dev, uint64_t* rounds_out_dev,

@@ -4,7 +4,7 @@ The compute path is liblgs.so (hand-written CUDA, C ABI in include/lgs.h); this 
 Python host mirror of the reference's API for the path (paulguoyanpei/ligesis:
 pcs/src/ligesis.rs, pcs/src/subset_sum.rs, utils/src/poly.rs, utils/src/oracle.rs).
 """
-from ._lib import Context, LgsError, OracleExhausted, ShapeError, load
+from ._lib import Context, DeviceTimeout, LgsError, OracleExhausted, ShapeError, load
 from .ligesis import (
     CODE_RATE,
     C_ROWS,
@@ -35,7 +35,7 @@ from .rng import SeededRng
 __all__ = [
     "Basefold", "BasefoldCommit", "BasefoldPcs", "BasefoldProof", "BasefoldProverState",
     "CODE_RATE", "FracSum", "FracSumProof", "Lookup", "LookupProof", "OpeningClaim", "Poly",
-    "multiplicity_vector", "LigesisPcs", "NoopCommit", "NoopPcs", "C_ROWS", "ETA", "NUM_COLS_OPENED", "CommitData", "Context", "LgsError",
+    "multiplicity_vector", "LigesisPcs", "NoopCommit", "NoopPcs", "C_ROWS", "ETA", "NUM_COLS_OPENED", "CommitData", "Context", "DeviceTimeout", "LgsError",
     "Ligesis", "LigesisCommit", "LigesisProof", "MlPoly", "OracleExhausted", "ProvingKey",
     "RandomOracle", "SeededRng", "ShapeError", "SubsetSumHash", "VerifyingKey", "dft", "load",
     "merkle_root", "oracle_need", "shape_ok", "sumcheck_prove",

@@ -38,6 +38,10 @@ class OracleExhausted(LgsError):
     pass
 
 
+class DeviceTimeout(LgsError):
+    """A bounded device wait gave up (LGS_ERR_DEVICE_TIMEOUT); the context stays usable."""
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -53,6 +57,7 @@ _SIGS = {
     "lgs_ctx_destroy": (None, [vp]),
     "lgs_ctx_stream": (C.c_int, [vp, C.POINTER(vp)]),
     "lgs_setup": (C.c_int, [vp, C.c_uint, C.c_uint, u64p, C.POINTER(vp), u8p]),
+    "lgs_setup_commit_only": (C.c_int, [vp, C.c_uint, C.c_uint, u64p, C.POINTER(vp)]),
     "lgs_pk_free": (None, [vp]),
     "lgs_commit": (C.c_int, [vp, vp, u64p, C.c_size_t, u8p, C.POINTER(vp)]),
     "lgs_commit_device": (C.c_int, [vp, vp, vp, C.c_size_t, u8p, C.POINTER(vp)]),
@@ -68,6 +73,12 @@ _SIGS = {
     "lgs_profile": (C.c_int, [vp, C.c_int]),
     "lgs_profile_get": (C.c_int, [vp, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "lgs_launch_count": (C.c_uint64, []),
+    "lgs_set_wait_budget": (C.c_int, [vp, C.c_uint64]),
+    "lgs_profile_names": (C.c_int, [vp, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "lgs_sumcheck_prove_dev": (C.c_int, [vp, vp, C.c_uint, C.c_uint, vp, vp, vp]),
+    "lgs_new_eq_dev": (C.c_int, [vp, vp, C.c_uint, vp]),
+    "lgs_mle_fold_dev": (C.c_int, [vp, vp, C.c_uint, vp, C.c_uint, vp]),
+    "lgs_mle_eval_dev": (C.c_int, [vp, vp, C.c_uint, vp, vp]),
     "lgs_basefold_commit": (C.c_int, [vp, u64p, C.c_size_t, C.c_int, C.c_uint, C.c_uint, u8p,
                                       C.POINTER(vp)]),
     "lgs_basefold_free": (None, [vp]),
@@ -132,6 +143,8 @@ def check(status: int) -> None:
         raise ShapeError(status, msg)
     if status == 3:
         raise OracleExhausted(status, msg)
+    if status == 4:
+        raise DeviceTimeout(status, msg)
     raise LgsError(status, msg)
 
 
@@ -174,6 +187,11 @@ class Context:
         s = vp()
         check(self._lib.lgs_ctx_stream(self.handle, C.byref(s)))
         return int(s.value or 0)
+
+    def set_wait_budget(self, cycles: int) -> None:
+        """Clock-cycle budget of the bounded device waits of this context's kernels (0 = the
+        default of about 2 s); a short budget makes them give up (DeviceTimeout)."""
+        check(self._lib.lgs_set_wait_budget(self.handle, int(cycles)))
 
     def close(self):
         if getattr(self, "handle", None):

@@ -203,6 +203,23 @@ lgs_status lgs_setup(lgs_ctx* ctx, unsigned log_m, unsigned log_n, const uint64_
     *pk = k;
   });
 }
+lgs_status lgs_setup_commit_only(lgs_ctx* ctx, unsigned log_m, unsigned log_n,
+                                 const uint64_t* A, lgs_pk** pk) {
+  return guarded([&] {
+    need(ctx && A && pk, "lgs_setup_commit_only: null argument");
+    need(log_m <= 13 && log_n >= 7 && log_n <= 21,
+         "lgs_setup_commit_only: needs log_m <= 13 and 7 <= log_n <= 21");
+    CtxDevice dg(ctx);
+    auto* k = new lgs_pk;
+    try {
+      setup_dev(ctx, log_m, log_n, A, k, true);
+    } catch (...) {
+      delete k;
+      throw;
+    }
+    *pk = k;
+  });
+}
 void lgs_pk_free(lgs_pk* pk) { delete pk; }
 
 static lgs_status commit_impl(lgs_ctx* ctx, const lgs_pk* pk, const uint64_t* f, size_t len,
@@ -292,6 +309,7 @@ lgs_status lgs_prove(lgs_ctx* ctx, const lgs_pk* pk, const lgs_commit_data* cd,
   return guarded([&] {
     need(ctx && pk && cd && z && fields && ints && cursors && proof && proof_len,
          "lgs_prove: null argument");
+    if (pk->commit_only) throw ShapeError("lgs_prove: a commit-only key cannot prove");
     CtxDevice dg(ctx);
     uint64_t cur[2] = {cursors[0], cursors[1]};
     std::vector<uint8_t>& buf = ctx->proof_buf;  // reused: written in place by the prove
@@ -494,6 +512,27 @@ lgs_status lgs_profile(lgs_ctx* ctx, int enable) {
   });
 }
 
+lgs_status lgs_profile_names(lgs_ctx* ctx, char* buf, size_t cap, size_t* needed) {
+  return guarded([&] {
+    need(ctx && needed, "lgs_profile_names: null argument");
+    std::string all;
+    for (auto& t : ctx->prof.totals) all += t.first + "\n";
+    *needed = all.size() + 1;
+    if (buf && cap) {
+      const size_t nb = std::min(cap - 1, all.size());
+      std::memcpy(buf, all.data(), nb);
+      buf[nb] = 0;
+    }
+  });
+}
+
+lgs_status lgs_set_wait_budget(lgs_ctx* ctx, uint64_t cycles) {
+  return guarded([&] {
+    need(ctx != nullptr, "lgs_set_wait_budget: null context");
+    ctx->wait_cycles = cycles;
+  });
+}
+
 lgs_status lgs_profile_get(lgs_ctx* ctx, const char* stage, double* total_ms, uint64_t* count) {
   return guarded([&] {
     need(ctx && stage && total_ms && count, "lgs_profile_get: null argument");
@@ -558,7 +597,8 @@ lgs_status lgs_subset_sum_hash(lgs_ctx* ctx, const uint64_t* A, size_t m, const 
     alimb_from_a(dA, dL, W, ctx->st);
     alignas(64) unsigned char tmap[128];
     make_alimb_tmap(dL, W, tmap);
-    subset_sum_hash_tc(tmap, dC, dH, dN, (unsigned)m, cp, ctx->err.as<int>(), ctx->st);
+    subset_sum_hash_tc(tmap, dC, dH, dN, (unsigned)m, cp, ctx->err.as<int>(), ctx->st,
+                       ctx->wait_cycles);
     LGS_CUDA(cudaMemcpy2DAsync(H, cols * 8, dH, cp * 8, cols * 8, DIGEST_ROWS,
                                cudaMemcpyDeviceToHost, ctx->st));
     int err = 0;
@@ -614,6 +654,56 @@ lgs_status lgs_sumcheck_prove(lgs_ctx* ctx, const uint64_t* polys, unsigned d, u
     LGS_CUDA(cudaMemcpyAsync(rounds_out, ro, (size_t)k * (d + 1) * 16, cudaMemcpyDeviceToHost, ctx->st));
     LGS_CUDA(cudaMemcpyAsync(finals_out, fo, d * 16, cudaMemcpyDeviceToHost, ctx->st));
     LGS_CUDA(cudaStreamSynchronize(ctx->st));
+  });
+}
+
+// ---- device-resident forms (inputs already in HBM; enqueued on the context's stream) ----------
+lgs_status lgs_sumcheck_prove_dev(lgs_ctx* ctx, uint64_t* polys_dev, unsigned d, unsigned k,
+                                  const uint64_t* challenges_dev, uint64_t* rounds_out_dev,
+                                  uint64_t* finals_out_dev) {
+  return guarded([&] {
+    need(ctx && polys_dev && challenges_dev && rounds_out_dev && finals_out_dev,
+         "lgs_sumcheck_prove_dev: null argument");
+    need(d >= 1 && d <= 3 && k >= 1 && k <= 30, "lgs_sumcheck_prove_dev: 1..3 factors, 1..30 variables");
+    CtxDevice dg(ctx);
+    const size_t len = (size_t)1 << k;
+    ctx->arena.begin();
+    ef2* part = ctx->arena.get<ef2>(sumcheck_partials_elems(k, d));
+    ef2* p[3];
+    for (unsigned j = 0; j < d; ++j) p[j] = (ef2*)polys_dev + j * len;
+    sumcheck_prove_dev(p, d, k, (const ef2*)challenges_dev, (ef2*)rounds_out_dev,
+                       (ef2*)finals_out_dev, part, ctx->st);
+  });
+}
+
+lgs_status lgs_new_eq_dev(lgs_ctx* ctx, const uint64_t* point_dev, unsigned k, uint64_t* out_dev) {
+  return guarded([&] {
+    need(ctx && point_dev && out_dev, "lgs_new_eq_dev: null argument");
+    need(k >= 1 && k <= 30, "lgs_new_eq_dev: 1..30 variables");
+    CtxDevice dg(ctx);
+    new_eq_dev((const ef2*)point_dev, k, (ef2*)out_dev, ctx->st);
+  });
+}
+
+lgs_status lgs_mle_fold_dev(lgs_ctx* ctx, const uint64_t* evals_dev, unsigned k,
+                            const uint64_t* point_dev, unsigned np, uint64_t* out_dev) {
+  return guarded([&] {
+    need(ctx && evals_dev && point_dev && out_dev, "lgs_mle_fold_dev: null argument");
+    need(k >= 1 && k <= 30, "lgs_mle_fold_dev: 1..30 variables");
+    CtxDevice dg(ctx);
+    mle_fold_dev((const ef2*)evals_dev, k, (const ef2*)point_dev, np, (ef2*)out_dev, ctx->st);
+  });
+}
+
+lgs_status lgs_mle_eval_dev(lgs_ctx* ctx, const uint64_t* evals_dev, unsigned k,
+                            const uint64_t* point_dev, uint64_t* out_dev) {
+  return guarded([&] {
+    need(ctx && evals_dev && point_dev && out_dev, "lgs_mle_eval_dev: null argument");
+    need(k >= 1 && k <= 30, "lgs_mle_eval_dev: 1..30 variables");
+    CtxDevice dg(ctx);
+    ctx->arena.begin();
+    ef2* part = ctx->arena.get<ef2>(eqdot_partials_elems(k));
+    eq_dot_dev(evals_dev, 0, (const ef2*)point_dev, k, (ef2*)out_dev, part, ctx->st);
   });
 }
 

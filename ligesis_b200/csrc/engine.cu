@@ -166,6 +166,8 @@ lgs_status lgs_engine_submit(lgs_engine* e, const lgs_job* job, uint64_t* ticket
     return lgs::set_error(LGS_ERR_BAD_ARG, "lgs_engine_submit: null argument");
   if (job->len != job->pk->shape.m() * job->pk->shape.n())
     return lgs::set_error(LGS_ERR_BAD_ARG, "lgs_engine_submit: f must hold 2^(log_m+log_n) values");
+  if (job->pk->commit_only)
+    return lgs::set_error(LGS_ERR_BAD_SHAPE, "lgs_engine_submit: a commit-only key cannot prove");
   auto* j = new EngineJob;
   j->in = *job;
   j->est = job_estimate(job->pk);
@@ -203,8 +205,11 @@ void lgs_engine_free_proof(uint8_t* proof) { std::free(proof); }
 
 lgs_status lgs_engine_prepare(lgs_engine* e, const lgs_pk* const* pks, size_t npk) {
   if (!e || (npk && !pks)) return lgs::set_error(LGS_ERR_BAD_ARG, "lgs_engine_prepare: null argument");
-  for (size_t i = 0; i < npk; ++i)
+  for (size_t i = 0; i < npk; ++i) {
     if (!pks[i]) return lgs::set_error(LGS_ERR_BAD_ARG, "lgs_engine_prepare: null proving key");
+    if (pks[i]->commit_only)
+      return lgs::set_error(LGS_ERR_BAD_SHAPE, "lgs_engine_prepare: a commit-only key cannot prove");
+  }
   {
     std::lock_guard<std::mutex> lk(e->mu);
     if (!e->queue.empty() || e->in_use != 0 || e->preparing)

@@ -128,6 +128,39 @@ void new_eq_dev(const ef2* point, unsigned k, ef2* out, cudaStream_t st) {
   LGS_LAUNCH_CHECK();
 }
 
+// MlPoly::fold (utils/src/poly.rs:33-42): binds the np lowest variables to point[0 .. np):
+// out[i] = sum_{y < 2^np} eq(point, y) in[i 2^np + y], which for np = 1 is the reference's
+// s[2i] + (s[2i+1] - s[2i]) r (the same field element).
+__global__ void mle_fold_kernel(const ef2* __restrict__ in, size_t nout, unsigned np,
+                                const ef2* __restrict__ point, ef2* __restrict__ out) {
+  __shared__ ef2 p[8];
+  __shared__ ef2 tab[256];
+  if (threadIdx.x < np) p[threadIdx.x] = point[threadIdx.x];
+  __syncthreads();
+  if (np > 1) eq_table_smem(p, np, tab);
+  const ef2 r = p[0];
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nout;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const ef2* s = in + (i << np);
+    if (np == 1) {
+      const ef2 a = s[0], b = s[1];
+      out[i] = ef_add(a, ef_mul(r, ef_sub(b, a)));
+    } else {
+      ef2 acc = ef_mul(tab[0], s[0]);
+      for (unsigned y = 1; y < (1u << np); ++y) acc = ef_add(acc, ef_mul(tab[y], s[y]));
+      out[i] = acc;
+    }
+  }
+}
+void mle_fold_dev(const ef2* in, unsigned k, const ef2* point, unsigned np, ef2* out,
+                  cudaStream_t st) {
+  if (np < 1 || np > 8 || np > k) throw ShapeError("mle_fold: 1 <= np <= min(8, k)");
+  const size_t nout = (size_t)1 << (k - np);
+  const unsigned grid = (unsigned)std::min<size_t>(cdiv(nout, 256), 148 * 16);
+  mle_fold_kernel<<<grid, 256, 0, st>>>(in, nout, np, point, out);
+  LGS_LAUNCH_CHECK();
+}
+
 // combine_eq (pcs/src/ligesis.rs:159-171): out = sum_j gamma^j eq_{points[j]}.
 __global__ void combine_eq_kernel(const ef2* __restrict__ points, unsigned npts, unsigned k,
                                   const ef2* __restrict__ gamma, ef2* __restrict__ out) {

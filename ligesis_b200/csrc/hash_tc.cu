@@ -19,7 +19,11 @@
 //               from L2) while the MMAs of the next tile run.
 // Every mbarrier wait is bounded by a clock budget and watches a CTA-wide failure flag; on a
 // timeout the CTA records an error code, every role stops issuing work, the MMA thread waits
-// (bounded) for the MMAs it issued, and the TMEM is freed before the CTA exits.
+// (bounded) for the MMAs it issued, the TMA thread waits (bounded) for the A-limb copies it
+// issued (each stage's copy completes on its own barrier, so this wait does not depend on the
+// other roles), and the TMEM is freed before the CTA exits.  The budget of the role waits is a
+// kernel argument (lgs_set_wait_budget shortens it to test this path); the two drain waits
+// always keep the long default.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -43,9 +47,9 @@ constexpr int EPI_COLS = 16;     // accumulator columns drained per epilogue ste
 constexpr int SS_PITCH = 260;    // u32 per drained column (256 limb rows + pad, 16-byte rows)
 constexpr int SS_WORDS = EPI_COLS * SS_PITCH;  // one staging buffer; two alternate
 constexpr int SS_BYTES = 2 * SS_WORDS * 4;
-constexpr int NBARS = 2 * TC_STAGES + 3;
+constexpr int NBARS = 3 * TC_STAGES + 3;  // full, empty, acc_full/acc_empty/drain, tma
 constexpr int SMEM_BYTES = TC_STAGES * STAGE_BYTES + SS_BYTES + 1024 /*align*/ + 128 /*barriers*/;
-constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s at 1.9 GHz
+constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s at 1.9 GHz (default budget)
 // instruction descriptor: D = S32 (2 << 4), A = B = U8 (0), both K-major, N = 256, M = 128
 constexpr uint32_t IDESC = (2u << 4) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
 
@@ -72,14 +76,15 @@ __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
       : "memory");
   return done != 0;
 }
-// Bounded wait for the phase with the given parity to complete.  false on timeout, or as soon as
-// another role has flagged a failure (*fail != 0).
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* fail) {
+// Bounded wait for the phase with the given parity to complete.  false after `budget` clock
+// cycles, or as soon as another role has flagged a failure (*fail != 0).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* fail,
+                                          long long budget) {
   const long long t0 = clock64();
   while (true) {
     if (mbar_test(bar, parity)) return true;
     if (*fail) return false;
-    if (clock64() - t0 > WAIT_CYCLES) return false;
+    if (clock64() - t0 > budget) return false;
   }
 }
 // Bounded wait that ignores the failure flag (draining work already issued).
@@ -147,7 +152,7 @@ __device__ __forceinline__ uint32_t nib_expand(uint32_t nib) {
 __global__ void __launch_bounds__(NTHREADS, 1)
     hash_tc_kernel(const __grid_constant__ CUtensorMap tmap_a, const u64* __restrict__ cw,
                    u64* __restrict__ H, u32* __restrict__ leaves, unsigned m, size_t two_n,
-                   int* __restrict__ err) {
+                   int* __restrict__ err, long long budget) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint32_t* Ss = (uint32_t*)(smem + TC_STAGES * STAGE_BYTES);
@@ -157,6 +162,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   const uint32_t acc_full = smem_u32(&bars[2 * TC_STAGES]);
   const uint32_t acc_empty = smem_u32(&bars[2 * TC_STAGES + 1]);
   const uint32_t drain = smem_u32(&bars[2 * TC_STAGES + 2]);
+  const uint32_t tma0 = smem_u32(&bars[2 * TC_STAGES + 3]);
   const unsigned tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const unsigned nchunks = (m + 1) / 2;
   const unsigned ntiles = (unsigned)(two_n / TC_N);
@@ -166,8 +172,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   if (tid == 0) {
     s_fail = 0;
     for (int s = 0; s < TC_STAGES; ++s) {
-      mbar_init(full0 + 8 * s, NPROD + 1);
+      mbar_init(full0 + 8 * s, NPROD);
       mbar_init(empty0 + 8 * s, 1);
+      mbar_init(tma0 + 8 * s, 1);
     }
     mbar_init(acc_full, 1);
     mbar_init(acc_empty, NEPI);
@@ -190,13 +197,15 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   if (warp == 0) {
     // ---- TMA producer: A-limb tiles ----
     if (lane == 0) {
+      unsigned issued = 0;
       for (unsigned f = 0; f < nfill; ++f) {
         const unsigned s = f % TC_STAGES, c = f % nchunks;
-        if (f >= TC_STAGES && !mbar_wait(empty0 + 8 * s, ((f / TC_STAGES) - 1) & 1, &s_fail)) {
+        if (f >= TC_STAGES &&
+            !mbar_wait(empty0 + 8 * s, ((f / TC_STAGES) - 1) & 1, &s_fail, budget)) {
           if (!s_fail) flag_failure(&s_fail, err, 1);
           break;
         }
-        const uint32_t bar = full0 + 8 * s;
+        const uint32_t bar = tma0 + 8 * s;
         mbar_arrive_tx(bar, A_TILE);
         const uint32_t dst = smem_u32(smem + s * STAGE_BYTES);
         const int x = (int)(c * TC_KB), y = 0;
@@ -205,7 +214,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             "[%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
             "l"((uint64_t)&tmap_a), "r"(x), "r"(y), "r"(bar)
             : "memory");
+        issued = f + 1;
       }
+      // Only the newest copy of each stage can still be in flight (an older one was consumed
+      // before its stage was refilled): wait for those before the CTA may exit.
+      for (unsigned g = issued > TC_STAGES ? issued - TC_STAGES : 0; g < issued; ++g)
+        if (!mbar_wait_drain(tma0 + 8 * (g % TC_STAGES), (g / TC_STAGES) & 1)) atomicExch(err, 6);
     }
   } else if (warp == 1) {
     // ---- MMA issuer ----
@@ -214,7 +228,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       bool ok = true;
       for (unsigned t = 0; t < my_tiles && ok; ++t) {
         if (t > 0) {
-          if (!mbar_wait(acc_empty, (t - 1) & 1, &s_fail)) {
+          if (!mbar_wait(acc_empty, (t - 1) & 1, &s_fail, budget)) {
             if (!s_fail) flag_failure(&s_fail, err, 2);
             ok = false;
             break;
@@ -223,7 +237,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
         for (unsigned c = 0; c < nchunks; ++c, ++f) {
           const unsigned s = f % TC_STAGES;
-          if (!mbar_wait(full0 + 8 * s, (f / TC_STAGES) & 1, &s_fail)) {
+          if (!mbar_wait(tma0 + 8 * s, (f / TC_STAGES) & 1, &s_fail, budget) ||
+              !mbar_wait(full0 + 8 * s, (f / TC_STAGES) & 1, &s_fail, budget)) {
             if (!s_fail) flag_failure(&s_fail, err, 3);
             ok = false;
             break;
@@ -265,7 +280,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // loads of fill f + 3 (so each load has three stages of MMA time to arrive)
     auto fill = [&](unsigned f, u64 (&w)[4]) -> bool {
       const unsigned s = f % TC_STAGES;
-      if (f >= TC_STAGES && !mbar_wait(empty0 + 8 * s, ((f / TC_STAGES) - 1) & 1, &s_fail)) {
+      if (f >= TC_STAGES &&
+          !mbar_wait(empty0 + 8 * s, ((f / TC_STAGES) - 1) & 1, &s_fail, budget)) {
         if (!s_fail) flag_failure(&s_fail, err, 4);
         return false;
       }
@@ -306,7 +322,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     const unsigned mrow = 32 * quarter + lane;
     for (unsigned t = 0; t < my_tiles; ++t) {
       const size_t j0 = (size_t)(blockIdx.x + t * gridDim.x) * TC_N;
-      const bool got = mbar_wait(acc_full, t & 1, &s_fail);
+      const bool got = mbar_wait(acc_full, t & 1, &s_fail, budget);
       if (!epi_all(got)) {
         if (!s_fail) flag_failure(&s_fail, err, 5);
         break;
@@ -501,7 +517,7 @@ void make_alimb_tmap(const uint8_t* alimb, size_t W, void* tmap_out) {
 size_t tensor_map_bytes() { return sizeof(CUtensorMap); }
 
 void subset_sum_hash_tc(const void* tmap, const u64* cw, u64* H, u32* leaves, unsigned m,
-                        size_t two_n, int* err, cudaStream_t st) {
+                        size_t two_n, int* err, cudaStream_t st, uint64_t wait_cycles) {
   if (two_n % TC_N) throw ShapeError("hash: 2n must be a multiple of 256");
   if (m == 0 || m > 8192) throw ShapeError("hash: 1 <= m <= 8192");
   LGS_CUDA(cudaFuncSetAttribute(hash_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -511,8 +527,10 @@ void subset_sum_hash_tc(const void* tmap, const u64* cw, u64* H, u32* leaves, un
   LGS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const size_t ntiles = two_n / TC_N;
   const unsigned grid = (unsigned)std::min<size_t>(ntiles, (size_t)std::max(sms, 1));
+  const long long budget =
+      wait_cycles ? (long long)std::min<uint64_t>(wait_cycles, (uint64_t)WAIT_CYCLES) : WAIT_CYCLES;
   hash_tc_kernel<<<grid, NTHREADS, SMEM_BYTES, st>>>(*(const CUtensorMap*)tmap, cw, H, leaves, m,
-                                                     two_n, err);
+                                                     two_n, err, budget);
   LGS_LAUNCH_CHECK();
 }
 

@@ -33,8 +33,9 @@ void rs_dft_rows(const u64* in, size_t ld_in, size_t n_in, u64* out, size_t ld_o
 void alimb_from_a(const u64* A, uint8_t* alimb, size_t W, cudaStream_t st);
 void make_alimb_tmap(const uint8_t* alimb, size_t W, void* tmap_out);
 size_t tensor_map_bytes();
+// wait_cycles: clock budget of the kernel's bounded waits (0 = the default, about 2 s).
 void subset_sum_hash_tc(const void* tmap, const u64* cw, u64* H, u32* leaves, unsigned m,
-                        size_t two_n, int* err, cudaStream_t st);
+                        size_t two_n, int* err, cudaStream_t st, uint64_t wait_cycles = 0);
 // Dense tcgen05 kind::i8 throughput (TOP/s) of back-to-back M128 N256 K32 MMAs on every SM.
 double i8_tensor_peak_tops(unsigned iters, int* err, cudaStream_t st);
 
@@ -53,6 +54,11 @@ void merkle_leaves_contig(const u64* data, unsigned words, size_t nleaves, u32* 
                           cudaStream_t st);
 void gather_u64(const u64* src, const uint64_t* idx, size_t count, unsigned words, u64* dst,
                 cudaStream_t st);
+
+// Timeline marks inside multi-kernel helpers (profile level 2, bench.py --mode timeline): an
+// event node named "<branch>/<what>" when a prove is being enqueued with timeline marks on this
+// host thread, nothing otherwise.
+void tl_mark(const char* what, cudaStream_t st);
 
 // sumcheck.cu
 size_t sumcheck_partials_elems(unsigned k, unsigned d);
@@ -73,6 +79,9 @@ struct GatherSeg {
 };
 void gather_segments(const GatherSeg* segs_dev, unsigned nseg, cudaStream_t st);
 void new_eq_dev(const ef2* point, unsigned k, ef2* out, cudaStream_t st);
+// MlPoly::fold of the np (1..8) lowest variables: 2^k EF in, 2^(k-np) EF out.
+void mle_fold_dev(const ef2* in, unsigned k, const ef2* point, unsigned np, ef2* out,
+                  cudaStream_t st);
 void combine_eq_dev(const ef2* points, unsigned npts, unsigned k, const ef2* gamma, ef2* out,
                     cudaStream_t st);
 size_t eqdot_partials_elems(unsigned k);

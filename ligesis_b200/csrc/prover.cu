@@ -3,6 +3,7 @@
 // open (pcs/src/basefold.rs:648-856).  Every challenge of the pre-drawn oracle is known before
 // the first kernel runs, so `prove` uploads one parameter block, enqueues the whole dataflow on
 // the context stream, and reads back one staging buffer from which the proof is assembled.
+#include <functional>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -43,7 +44,9 @@ void bf_commit(lgs_ctx* c, const u64* poly, int is_ef, size_t len, unsigned li,
   else
     ntt_batch(tT, rows, rows, cT, L, logL, cols, scr, c->tw.as<u64>(), st);
   transpose_u64(cT, out->codes, cols, L, 1, st);
+  tl_mark("bf_dft_end", st);
   merkle_leaves_contig(out->codes, (unsigned)cols, L, out->nodes, st);
+  tl_mark("bf_leaves_end", st);
   merkle_build_from_leaves(out->nodes, L, st);
   out->poly = poly;
   out->is_ef = is_ef;
@@ -292,11 +295,17 @@ void ctx_init(lgs_ctx* c, int device) {
   LGS_CUDA(cudaStreamSynchronize(c->st));
 }
 
-void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lgs_pk* pk) {
+void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lgs_pk* pk,
+               bool commit_only) {
   Shape s{log_m, log_n};
-  if (!s.eval_ok())
+  if (commit_only) {
+    if (log_m > 13 || log_n < 7)
+      throw ShapeError("commit-only key: needs log_m <= 13 and log_n >= 7");
+  } else if (!s.eval_ok()) {
     throw ShapeError("batched LigeSIS needs the {A, B_I, a} var counts within LOG_INTERLEAVE");
+  }
   pk->shape = s;
+  pk->commit_only = commit_only;
   const size_t W = s.W(), len = (size_t)DIGEST_ROWS * W;
   c->arena.begin();
   pk->A.alloc(len * 8, c->st);
@@ -308,6 +317,10 @@ void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lg
   pk->alimb.detach(release_stream(c->device));
   alimb_from_a(pk->A.as<u64>(), pk->alimb.as<uint8_t>(), W, c->st);
   make_alimb_tmap(pk->alimb.as<uint8_t>(), W, pk->tmap);
+  if (commit_only) {
+    LGS_CUDA(cudaStreamSynchronize(c->st));
+    return;
+  }
   const unsigned li = s.li(s.na());
   const size_t L = (len >> li) << CODE_RATE;
   pk->a_codes.alloc(L * ((size_t)1 << li) * 8, c->st);
@@ -387,7 +400,7 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
   {
     StageTimer t(c->prof, c->hs, "subset_sum_hash");  // H and its Merkle leaf hashes
     subset_sum_hash_tc(pk->tmap, cd->cw.as<u64>(), cd->H.as<u64>(), cd->nodes.as<u32>(),
-                       (unsigned)m, two_n, c->err.as<int>(), c->hs);
+                       (unsigned)m, two_n, c->err.as<int>(), c->hs, c->wait_cycles);
   }
   {
     StageTimer t(c->prof, c->hs, "merkle_h");
@@ -538,6 +551,15 @@ const ProveGraph* prove_graph(lgs_ctx* c, const Shape& s, F&& enqueue) {
   g->up = c->up.p;
   g->down = c->down.p;
   return g;
+}
+
+namespace {
+thread_local std::function<void(const std::string&, cudaStream_t)>* t_tl_hook = nullptr;
+thread_local const char* t_tl_branch = "";
+}  // namespace
+
+void tl_mark(const char* what, cudaStream_t st) {
+  if (t_tl_hook) (*t_tl_hook)(std::string(t_tl_branch) + "/" + what, st);
 }
 
 void note_prove_need(lgs_ctx* c, const Shape& s, size_t need) {
@@ -807,7 +829,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   if (tl)
     for (int i = 0; i < lgs_ctx::TL_MAX; ++i)
       if (!c->tl_ev[i]) LGS_CUDA(cudaEventCreate(&c->tl_ev[i]));
-  auto mark = [&](const char* name, cudaStream_t where) {
+  auto mark = [&](const std::string& name, cudaStream_t where) {
     if (!tl || ntl >= (unsigned)lgs_ctx::TL_MAX) return;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     LGS_CUDA(cudaStreamIsCapturing(where, &cs));
@@ -818,7 +840,16 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     if (c->tl_names.size() <= ntl) c->tl_names.resize(ntl + 1);
     c->tl_names[ntl++] = name;
   };
+  std::function<void(const std::string&, cudaStream_t)> hook = mark;
+  struct HookScope {  // tl_mark() reaches `mark` only while this prove is enqueued
+    HookScope(std::function<void(const std::string&, cudaStream_t)>* h, bool on) {
+      t_tl_hook = on ? h : nullptr;
+      t_tl_branch = "";
+    }
+    ~HookScope() { t_tl_hook = nullptr; }
+  };
   auto enqueue = [&]() {
+  HookScope hook_scope(&hook, tl);
   ntl = 0;
   mark("start", st);
   h2d(d_up, h_up, blob, st);
@@ -855,6 +886,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   const unsigned br_b = (unsigned)brs.size();
   // B: the Basefold commitment to B_I (pcs/src/ligesis.rs:411-416)
   {
+    t_tl_branch = "B";
     cudaStream_t b = branch(true);
     bf_commit(c, bi, 0, WS, li_bi, CODE_RATE, &bi_st, b);
     mark("B_bi_commit_end", b);
@@ -862,17 +894,20 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   // C: binary check, factors [B_I, B_I - 1, eq_alpha1] (pcs/src/ligesis.rs:419-429); the
   // longest branch, so it is the third high-priority one
   {
+    t_tl_branch = "C";
     cudaStream_t b = branch(true);
     ef2* p0 = ar.get<ef2>(WS);
     ef2* p2 = ar.get<ef2>(WS);
     lift_bf(bi, p0, WS, 0, b);
     new_eq_dev(d_fields + fp.alpha1, nb, p2, b);
+    tl_mark("inputs_end", b);
     sumcheck_binary_dev(p0, p2, nb, d_fields + fp.ch_bin, (ef2*)(stage + S_sc_r[0]),
                         (ef2*)(stage + S_sc_f[0]), partials_for(nb, 3), b);
     mark("C_binary_sc_end", b);
   }
   // D: hash and recon bilinear sumchecks (pcs/src/ligesis.rs:435-485)
   {
+    t_tl_branch = "D";
     cudaStream_t b = branch();
     ef2* g1 = ar.get<ef2>(W);
     ef2* g2 = ar.get<ef2>(W);
@@ -882,6 +917,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     g2_build(bi, W, S, eq_r2, g2, b);
     d2d(g2b, g2, W * sizeof(ef2), b);
     v_build(eqz1, W, v, b);
+    tl_mark("inputs_end", b);
     ef2* ph[2] = {g1, g2};
     ef2* part = partials_for(log_w, 2);
     sumcheck_prove_dev(ph, 2, log_w, d_fields + fp.ch_hash, (ef2*)(stage + S_sc_r[1]),
@@ -893,11 +929,13 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   }
   // F: Stage A point reduction of B_I (pcs/src/ligesis.rs:510-516)
   {
+    t_tl_branch = "F";
     cudaStream_t b = branch();
     ef2* gbi = ar.get<ef2>(WS);
     ef2* bie = ar.get<ef2>(WS);
     combine_eq_dev(d_prm + P_bipts, 3, nb, d_fields + fp.gamma_bi, gbi, b);
     lift_bf(bi, bie, WS, 0, b);
+    tl_mark("inputs_end", b);
     ef2* pb[2] = {bie, gbi};
     sumcheck_prove_dev(pb, 2, nb, d_fields + fp.ch_bi, (ef2*)(stage + S_sc_r[5]),
                        (ef2*)(stage + S_sc_f[5]), partials_for(nb, 2), b);
@@ -911,6 +949,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   const unsigned br_a1 = (unsigned)brs.size();
   // A1: y = a(z2) and the Basefold commitment to a-bar (pcs/src/ligesis.rs:379-384)
   {
+    t_tl_branch = "A1";
     cudaStream_t b = branch(true);
     eq_dot_dev(a_vec, 0, d_prm + P_z2, log_n, (ef2*)(stage + S_y), partials_for(log_n, 1), b);
     bf_commit(c, (const u64*)a_vec, 1, n, li_a, CODE_RATE, &a_st, b);
@@ -918,6 +957,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   }
   // A2: RS(a-bar), y4, the recon table sumcheck and y5 (pcs/src/ligesis.rs:387, 458, 487-497)
   {
+    t_tl_branch = "A2";
     cudaStream_t b = branch();
     u64* t1 = ar.get<u64>(2 * n);
     u64* t2 = ar.get<u64>(2 * two_n);
@@ -925,6 +965,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     transpose_u64((const u64*)a_vec, t1, n, 2, 1, b);
     ntt_batch(t1, n, n, t2, two_n, ilog2(two_n), 2, scr, c->tw.as<u64>(), b);
     transpose_u64(t2, (u64*)ra, 2, two_n, 1, b);
+    tl_mark("rs_end", b);
     y4_dev(eq_r2, ra, d_idx, S, (ef2*)(stage + S_y4), b);
     ef2* sel = ar.get<ef2>(two_n);
     ef2* rac = ar.get<ef2>(two_n);
@@ -938,6 +979,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   }
   // E: RS-link sumcheck (pcs/src/ligesis.rs:499-502); r3 is pre-drawn, so w needs no wait
   {
+    t_tl_branch = "E";
     cudaStream_t b = branch();
     ef2* w = ar.get<ef2>(n);
     ef2* ac = ar.get<ef2>(n);
@@ -950,6 +992,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   }
   // G: Stage A point reduction of a-bar (pcs/src/ligesis.rs:518-522)
   {
+    t_tl_branch = "G";
     cudaStream_t b = branch();
     ef2* ga = ar.get<ef2>(n);
     ef2* ac = ar.get<ef2>(n);
@@ -964,6 +1007,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   // (2^R values) and the batch challenges r_0.., round t's l0 = MLE(m)(r_0, .., r_{t-1}, 0,
   // zp[t+1], .., zp[R-1]): the sequential rounds collapse to R independent evaluations.
   {
+    t_tl_branch = "H";
     cudaStream_t b = branch();
     const int poly_slot[3] = {PT_A, PT_BI, PT_AVEC};
     for (int ch = 0; ch < 3; ++ch)
@@ -972,6 +1016,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     eq_dot_multi_dev((const EqDotTask*)(d_up + U_tasks), 3 * R, R, part, b);
     mark("H_basefold_msgs_end", b);
   }
+  t_tl_branch = "main";
   // join: main waits for every branch
   for (size_t i = 0; i < brs.size(); ++i) LGS_CUDA(cudaEventRecord(c->ev_done[i], brs[i]));
   LGS_CUDA(cudaStreamWaitEvent(st, c->ev_done[br_a1], 0));

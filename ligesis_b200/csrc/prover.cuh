@@ -262,11 +262,12 @@ struct lgs_ctx {
   // Profile level 2: event-record nodes at the prove's branch boundaries (captured into its
   // graph), read back as "tl:<mark>" = ms since the prove's start.
   int prof_level = 0;
-  static constexpr int TL_MAX = 32;
+  static constexpr int TL_MAX = 96;
   cudaEvent_t tl_ev[TL_MAX] = {};
   std::vector<std::string> tl_names;
   unsigned tl_count = 0;  // marks recorded inside the prove's graph
   lgs::DevMem err;  // device error word of bounded-wait kernels (0 = ok)
+  uint64_t wait_cycles = 0;  // budget of those waits in clock cycles (0 = default; lgs_set_wait_budget)
   // Pinned host memory: every transfer of a call is asynchronous, so the host enqueues a whole
   // commit or prove without waiting for the device and synchronises once at the end.
   lgs::PinnedBuf up;    // the parameter blob of one prove (one host-to-device copy)
@@ -283,6 +284,7 @@ struct lgs_ctx {
 
 struct lgs_pk {
   lgs::Shape shape;
+  bool commit_only = false;  // lgs_setup_commit_only: no Basefold commitment of A, no prove
   lgs::DevMem A;      // 32 x W canonical u64, row-major (the flat A-bar of subset_sum.rs:73-79)
   lgs::DevMem alimb;  // 256 x W bytes: byte l of A[r][k] at row 8r + l
   alignas(64) unsigned char tmap[128];  // TMA descriptor of alimb (CUtensorMap)
@@ -321,7 +323,10 @@ namespace lgs {
 // The prover's stages (prover.cu).  commit_dev with finish = false only enqueues: commit_finish
 // (or any later synchronisation of the context followed by commit_finish) completes it.
 void ctx_init(lgs_ctx* c, int device);
-void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lgs_pk* pk);
+// commit_only: any shape the commit kernels take (log_n >= 7, log_m <= 13); the key then holds
+// only A and its limbs, and cannot be used by prove.
+void setup_dev(lgs_ctx* c, unsigned log_m, unsigned log_n, const u64* A_host, lgs_pk* pk,
+               bool commit_only = false);
 void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device, lgs_commit_data* cd,
                 bool finish = true);
 void commit_finish(lgs_ctx* c, lgs_commit_data* cd);

@@ -479,6 +479,7 @@ void sumcheck_run(ef2* const* polys, unsigned k, const ef2* ch, ef2* rounds_out,
     fold = 1;
     ++t;
   }
+  tl_mark("sc_passes_end", st);
   // the tail also sums the multi-CTA rounds' partials, and completes their g(1) along the
   // claim chain
   sc_tail_kernel<D, BIN><<<1, SC_TAIL_THREADS, 0, st>>>(P, (unsigned)len, fold, ch, t, k,

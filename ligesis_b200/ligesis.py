@@ -318,6 +318,19 @@ class Ligesis:
         return pk, vk
 
     @staticmethod
+    def setup_commit_only(log_m: int, log_n: int, hash_: SubsetSumHash,
+                          ctx: Context | None = None) -> ProvingKey:
+        """A key for `commit` alone, at any shape the commit takes (log_m <= 13, log_n >= 7):
+        setup's shared-domain assertion (pcs/src/ligesis.rs:246-251) binds only the prove, so
+        square shapes such as 2^12 x 2^12 are committed through this key.  It cannot prove."""
+        ctx = ctx or Context.default()
+        if hash_.width != ETA << log_m:
+            raise ValueError("the hash width must be 64 * 2^log_m")
+        h = vp()
+        check(load().lgs_setup_commit_only(ctx.handle, log_m, log_n, ptr64(hash_.a), C.byref(h)))
+        return ProvingKey(h, hash_, b"", log_m, log_n, ctx)
+
+    @staticmethod
     def commit(pk: ProvingKey, f: MlPoly) -> tuple[LigesisCommit, CommitData]:
         """Enqueues the commit (lgs_commit_async) and returns at once: the root is read when
         first used, and a prove on the same context runs after the commit on the device."""

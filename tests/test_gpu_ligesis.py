@@ -208,3 +208,27 @@ def test_bad_shapes_and_lengths_are_rejected(lgs):
     pk, vk = L.Ligesis.setup(3, 10, g)
     with pytest.raises(L.LgsError):
         L.Ligesis.commit(pk, L.MlPoly(g.field_elements(1 << 12)))
+
+
+@pytest.mark.parametrize("log_m,log_n", [(7, 7), (9, 8), (10, 10)])
+def test_commit_only_square_shapes_match_oracle(lgs, orc, log_m, log_n):
+    """Ligesis::commit at shapes setup's shared-domain window rejects (the square shapes of the
+    mu = 20/24/26 commit benchmarks run this way): codeword, digest H and root equal the
+    oracle's; the key cannot prove."""
+    f, A, z, fields, ints = ligesis_inputs(log_m, log_n, seed=500 + log_m + log_n)
+    with pytest.raises(L.ShapeError):
+        L.Ligesis.setup_with_hash(log_m, log_n, L.SubsetSumHash(64 << log_m, a=A))
+    pk = L.Ligesis.setup_commit_only(log_m, log_n, L.SubsetSumHash(64 << log_m, a=A))
+    commit, data = L.Ligesis.commit(pk, L.MlPoly(f))
+    orc.set_threads(None)
+    try:
+        cm = orc.Commitment(orc.Key(log_m, log_n, A, commit_only=True), f)
+    finally:
+        orc.set_threads(1)
+    assert commit.root == cm.root
+    assert np.array_equal(data.codeword(), cm.codeword())
+    assert np.array_equal(data.digest(), cm.digest())
+    o = L.RandomOracle(0, length=8)
+    o.fields, o.ints = np.ascontiguousarray(fields), np.ascontiguousarray(ints)
+    with pytest.raises(L.ShapeError):
+        L.Ligesis.prove(pk, data, z, o)

@@ -274,3 +274,14 @@ def test_basefold_tampered_message_is_rejected(orc):
     wrong_pt = np.array(pt, dtype=np.uint64).copy()
     wrong_pt[0, 0] ^= np.uint64(1)
     assert not orc.basefold_verify(cm.root, wrong_pt, pf, fields, ints)
+
+
+def test_commit_only_key_commits_like_setup_key(orc):
+    """The oracle's commit-only key gives the same commitment as setup's key where both exist."""
+    from tests.helpers import ligesis_inputs
+
+    f, A, _, _, _ = ligesis_inputs(3, 10, seed=44)
+    full = orc.Commitment(orc.Key(3, 10, A), f)
+    only = orc.Commitment(orc.Key(3, 10, A, commit_only=True), f)
+    assert full.root == only.root
+    assert np.array_equal(full.digest(), only.digest())
