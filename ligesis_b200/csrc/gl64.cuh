@@ -233,11 +233,55 @@ GL_HD ef2 ef_sub(ef2 a, ef2 b) { return ef_make(gl_sub(a.c0, b.c0), gl_sub(a.c1,
 GL_HD ef2 ef_scale(ef2 a, u64 s) { return ef_make(gl_mul(a.c0, s), gl_mul(a.c1, s)); }
 // 7 * x: x*8 - x through the 128-bit path (x < p, so x*8 < 2^67).
 GL_HD u64 gl_mul7(u64 x) { return gl_sub(gl_reduce(x << 3, x >> 61), x); }
+#ifdef __CUDA_ARCH__
+// (w0 + w1 2^32 + w2 2^64 + w3 2^96) = a * b, the 128-bit product on 32-bit multiply-adds.
+__device__ __forceinline__ void gl_mul_wide(u64 a, u64 b, uint32_t (&r)[4]) {
+  const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32);
+  const uint32_t b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+  asm("mul.lo.u32 %0, %4, %6;\n\t"
+      "mul.hi.u32 %1, %4, %6;\n\t"
+      "mad.lo.cc.u32 %1, %4, %7, %1;\n\t"
+      "madc.hi.u32 %2, %4, %7, 0;\n\t"
+      "mad.lo.cc.u32 %1, %5, %6, %1;\n\t"
+      "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+      "madc.hi.u32 %3, %5, %7, 0;\n\t"
+      "mad.lo.cc.u32 %2, %5, %7, %2;\n\t"
+      "addc.u32 %3, %3, 0;"
+      : "=&r"(r[0]), "=&r"(r[1]), "=&r"(r[2]), "=&r"(r[3])
+      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+}
+#endif
 GL_HD ef2 ef_mul(ef2 a, ef2 b) {
+#ifdef __CUDA_ARCH__
+  // Schoolbook with one reduction per coordinate: c1 = a0 b1 + a1 b0 and c0 = a0 b0 + 7 a1 b1 are
+  // summed unreduced (below 2^129 and 2^131) in five 32-bit words, then brought into the field.
+  Acc160 w1, w0;
+  uint32_t t[4];
+  gl_mul_wide(a.c0, b.c1, t);
+  w1.w[0] = t[0], w1.w[1] = t[1], w1.w[2] = t[2], w1.w[3] = t[3], w1.w[4] = 0;
+  gl_mac(w1, a.c1, b.c0);
+  gl_mul_wide(a.c1, b.c1, t);  // 7 t = 8 t - t, exact in five words
+  asm("{\n\t.reg .u32 s0, s1, s2, s3, s4;\n\t"
+      "shl.b32 s0, %5, 3;\n\t"
+      "shf.l.clamp.b32 s1, %5, %6, 3;\n\t"
+      "shf.l.clamp.b32 s2, %6, %7, 3;\n\t"
+      "shf.l.clamp.b32 s3, %7, %8, 3;\n\t"
+      "shr.b32 s4, %8, 29;\n\t"
+      "sub.cc.u32 %0, s0, %5;\n\t"
+      "subc.cc.u32 %1, s1, %6;\n\t"
+      "subc.cc.u32 %2, s2, %7;\n\t"
+      "subc.cc.u32 %3, s3, %8;\n\t"
+      "subc.u32 %4, s4, 0;\n\t}"
+      : "=r"(w0.w[0]), "=r"(w0.w[1]), "=r"(w0.w[2]), "=r"(w0.w[3]), "=r"(w0.w[4])
+      : "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(t[3]));
+  gl_mac(w0, a.c0, b.c0);
+  return ef_make(gl_acc_reduce(w0), gl_acc_reduce(w1));
+#else
   // Karatsuba: c0 = a0 b0 + 7 a1 b1, c1 = (a0 + a1)(b0 + b1) - a0 b0 - a1 b1
   u64 p0 = gl_mul(a.c0, b.c0), p1 = gl_mul(a.c1, b.c1);
   u64 pm = gl_mul(gl_add(a.c0, a.c1), gl_add(b.c0, b.c1));
   return ef_make(gl_add(p0, gl_mul7(p1)), gl_sub(gl_sub(pm, p0), p1));
+#endif
 }
 // (1 - r) a + r b = a + r (b - a)
 GL_HD ef2 ef_lerp(ef2 a, ef2 b, ef2 r) { return ef_add(a, ef_mul(r, ef_sub(b, a))); }
