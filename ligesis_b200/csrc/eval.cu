@@ -50,6 +50,24 @@ __device__ void eq_table_smem(const ef2* p, unsigned b, ef2* tab) {
     tab[j] = ef_mul(half_tabs[j & (n1 - 1)], half_tabs[32 + (j >> b1)]);
   __syncthreads();
 }
+// The two half tables of an eq table over p[0 .. b) (b <= 10): lo[j] over the low
+// b1 = min(b, 5) variables, hi[j] over the next b2 = b - b1, so that
+// eq(p[0 .. b), j) = lo[j mod 2^b1] hi[j >> b1].  Every thread of the CTA must call it; both
+// tables are complete when it returns (it ends with a barrier).
+__device__ void eq_halves(const ef2* p, unsigned b, ef2* lo, ef2* hi) {
+  const unsigned b1 = b < 5 ? b : 5, b2 = b - b1;
+  const unsigned n1 = 1u << b1, n2 = 1u << b2;
+  for (unsigned j = threadIdx.x; j < n1 + n2; j += blockDim.x) {
+    const bool h = j >= n1;
+    const unsigned idx = h ? j - n1 : j, nb = h ? b2 : b1;
+    const ef2* pp = h ? p + b1 : p;
+    ef2 acc = ef_one();
+    for (unsigned t = 0; t < nb; ++t)
+      acc = ef_mul(acc, ((idx >> t) & 1) ? pp[t] : ef_sub(ef_one(), pp[t]));
+    (h ? hi : lo)[idx] = acc;
+  }
+  __syncthreads();
+}
 // prod_{t in [b, k)} (bit t of idx ? p[t] : 1 - p[t]), by a whole warp: lane l multiplies the
 // terms t = b + l, b + l + 32, and a shuffle tree multiplies the lanes' products (the field
 // product does not depend on the order, so every lane gets the same element).  One thread alone
@@ -106,20 +124,26 @@ void gather_segments(const GatherSeg* segs_dev, unsigned nseg, cudaStream_t st) 
 
 // ---- eq tables ----------------------------------------------------------------------------
 // MlPoly::new_eq (utils/src/poly.rs:44-53): point[0] is the lowest index bit.
+// Entry j of a 2^b tile = lo[j mod 2^b1] * H[j >> b1] with H = (the tile's high factor) * hi:
+// one F_p2 product per entry.
 __global__ void new_eq_kernel(const ef2* __restrict__ point, unsigned k, ef2* __restrict__ out) {
   __shared__ ef2 p[64];
-  __shared__ ef2 tab[1 << EQ_TILE_LOG];
-  __shared__ ef2 hi;
+  __shared__ ef2 lo[32], hi[32];
+  __shared__ ef2 hfac;
   if (threadIdx.x < k) p[threadIdx.x] = point[threadIdx.x];
   __syncthreads();
   const unsigned b = k < EQ_TILE_LOG ? k : EQ_TILE_LOG;
+  const unsigned b1 = b < 5 ? b : 5;
   const size_t base = (size_t)blockIdx.x << b;
   if (threadIdx.x < 32) {
     const ef2 h = eq_high_warp(p, b, k, base);
-    if (threadIdx.x == 0) hi = h;
+    if (threadIdx.x == 0) hfac = h;
   }
-  eq_table_smem(p, b, tab);  // ends with a barrier, so hi is visible
-  for (unsigned j = threadIdx.x; j < (1u << b); j += blockDim.x) out[base + j] = ef_mul(hi, tab[j]);
+  eq_halves(p, b, lo, hi);  // ends with a barrier, so hfac is visible
+  if (threadIdx.x < (1u << (b - b1))) hi[threadIdx.x] = ef_mul(hi[threadIdx.x], hfac);
+  __syncthreads();
+  for (unsigned j = threadIdx.x; j < (1u << b); j += blockDim.x)
+    out[base + j] = ef_mul(lo[j & ((1u << b1) - 1)], hi[j >> b1]);
 }
 void new_eq_dev(const ef2* point, unsigned k, ef2* out, cudaStream_t st) {
   if (k > 40) throw ShapeError("new_eq: too many variables");
@@ -161,39 +185,36 @@ void mle_fold_dev(const ef2* in, unsigned k, const ef2* point, unsigned np, ef2*
   LGS_LAUNCH_CHECK();
 }
 
-// combine_eq (pcs/src/ligesis.rs:159-171): out = sum_j gamma^j eq_{points[j]}.
+// combine_eq (pcs/src/ligesis.rs:159-171): out = sum_j gamma^j eq_{points[j]}.  Per tile and
+// point, gamma^j times the tile's high eq factor is folded into the upper half table, so an
+// entry costs one F_p2 product per point.
 __global__ void combine_eq_kernel(const ef2* __restrict__ points, unsigned npts, unsigned k,
                                   const ef2* __restrict__ gamma, ef2* __restrict__ out) {
   __shared__ ef2 p[4 * 64];
-  __shared__ ef2 tab[1 << EQ_TILE_LOG];
-  __shared__ ef2 coef;
-  constexpr unsigned PER = (1u << EQ_TILE_LOG) / 256;  // entries per thread (blockDim 256)
+  __shared__ ef2 lo[4][32], hi[4][32];
+  __shared__ ef2 coef[4];
   for (unsigned i = threadIdx.x; i < npts * k; i += blockDim.x) p[i] = points[i];
   __syncthreads();
   const unsigned b = k < EQ_TILE_LOG ? k : EQ_TILE_LOG;
+  const unsigned b1 = b < 5 ? b : 5, n2 = 1u << (b - b1);
   const size_t base = (size_t)blockIdx.x << b;
-  ef2 acc[PER];
-#pragma unroll
-  for (unsigned q = 0; q < PER; ++q) acc[q] = ef_zero();
-  ef2 g = ef_one();
-  for (unsigned j = 0; j < npts; ++j) {
-    if (threadIdx.x < 32) {
+  if (threadIdx.x < 32) {
+    ef2 g = ef_one();
+    for (unsigned j = 0; j < npts; ++j) {
       const ef2 h = eq_high_warp(p + j * k, b, k, base);
-      if (threadIdx.x == 0) coef = ef_mul(g, h);
+      if (threadIdx.x == 0) coef[j] = ef_mul(g, h);
+      g = ef_mul(g, *gamma);
     }
-    eq_table_smem(p + j * k, b, tab);  // ends with a barrier, so coef is visible
-#pragma unroll
-    for (unsigned q = 0; q < PER; ++q) {
-      unsigned i = threadIdx.x + q * 256;
-      if (i < (1u << b)) acc[q] = ef_add(acc[q], ef_mul(coef, tab[i]));
-    }
-    __syncthreads();
-    g = ef_mul(g, *gamma);
   }
-#pragma unroll
-  for (unsigned q = 0; q < PER; ++q) {
-    unsigned i = threadIdx.x + q * 256;
-    if (i < (1u << b)) out[base + i] = acc[q];
+  for (unsigned j = 0; j < npts; ++j) eq_halves(p + j * k, b, lo[j], hi[j]);
+  for (unsigned i = threadIdx.x; i < npts * n2; i += blockDim.x)
+    hi[i / n2][i % n2] = ef_mul(hi[i / n2][i % n2], coef[i / n2]);
+  __syncthreads();
+  for (unsigned i = threadIdx.x; i < (1u << b); i += blockDim.x) {
+    const unsigned a = i & ((1u << b1) - 1), u = i >> b1;
+    ef2 acc = ef_mul(lo[0][a], hi[0][u]);
+    for (unsigned j = 1; j < npts; ++j) acc = ef_add(acc, ef_mul(lo[j][a], hi[j][u]));
+    out[base + i] = acc;
   }
 }
 void combine_eq_dev(const ef2* points, unsigned npts, unsigned k, const ef2* gamma, ef2* out,
@@ -209,20 +230,36 @@ template <bool BF>
 __global__ void eq_dot_kernel(const void* __restrict__ vec, const ef2* __restrict__ point,
                               unsigned k, ef2* __restrict__ partials) {
   __shared__ ef2 p[64];
-  __shared__ ef2 tab[1 << EQ_TILE_LOG];
+  __shared__ ef2 lo[32], hi[32];
   __shared__ ef2 red[32];
   if (threadIdx.x < k) p[threadIdx.x] = point[threadIdx.x];
   __syncthreads();
   const unsigned b = k < EQ_TILE_LOG ? k : EQ_TILE_LOG;
+  const unsigned b1 = b < 5 ? b : 5;
   const size_t base = (size_t)blockIdx.x << b;
-  eq_table_smem(p, b, tab);
+  eq_halves(p, b, lo, hi);
   ef2 acc = ef_zero();
-  for (unsigned j = threadIdx.x; j < (1u << b); j += blockDim.x) {
-    if (BF) {
-      u64 x = ((const u64*)vec)[base + j];
-      acc = ef_add(acc, ef_scale(tab[j], x));
-    } else {
-      acc = ef_add(acc, ef_mul(((const ef2*)vec)[base + j], tab[j]));
+  if (b1 == 5 && (blockDim.x & 31) == 0) {
+    // a thread's entries share their low five bits (blockDim is a multiple of 32):
+    // sum_i vec[i] eq(i) = lo[a] * sum_i vec[i] hi[i >> 5], one product per entry
+    for (unsigned j = threadIdx.x; j < (1u << b); j += blockDim.x) {
+      if (BF) {
+        const u64 x = ((const u64*)vec)[base + j];
+        acc = ef_add(acc, ef_scale(hi[j >> 5], x));
+      } else {
+        acc = ef_add(acc, ef_mul(((const ef2*)vec)[base + j], hi[j >> 5]));
+      }
+    }
+    acc = ef_mul(acc, lo[threadIdx.x & 31]);
+  } else {
+    for (unsigned j = threadIdx.x; j < (1u << b); j += blockDim.x) {
+      const ef2 e = ef_mul(lo[j & ((1u << b1) - 1)], hi[j >> b1]);
+      if (BF) {
+        const u64 x = ((const u64*)vec)[base + j];
+        acc = ef_add(acc, ef_scale(e, x));
+      } else {
+        acc = ef_add(acc, ef_mul(((const ef2*)vec)[base + j], e));
+      }
     }
   }
   acc = block_sum(acc, red);
@@ -332,17 +369,25 @@ void gemv_eq_rows(const u64* const* fref, const ef2* eq, size_t m, size_t n, ef2
 __global__ void eq_dot_multi_kernel(const EqDotTask* __restrict__ tasks, unsigned k,
                                     ef2* __restrict__ partials) {
   __shared__ ef2 p[64];
-  __shared__ ef2 tab[1 << EQ_TILE_LOG];
+  __shared__ ef2 lo[32], hi[32];
   __shared__ ef2 red[32];
   const EqDotTask task = tasks[blockIdx.y];
   if (threadIdx.x < k) p[threadIdx.x] = task.point[threadIdx.x];
   __syncthreads();
   const unsigned b = k < EQ_TILE_LOG ? k : EQ_TILE_LOG;
+  const unsigned b1 = b < 5 ? b : 5;
   const size_t base = (size_t)blockIdx.x << b;
-  eq_table_smem(p, b, tab);
+  eq_halves(p, b, lo, hi);
   ef2 acc = ef_zero();
-  for (unsigned j = threadIdx.x; j < (1u << b); j += blockDim.x)
-    acc = ef_add(acc, ef_mul(task.vec[base + j], tab[j]));
+  if (b1 == 5 && (blockDim.x & 31) == 0) {  // one product per entry (see eq_dot_kernel)
+    for (unsigned j = threadIdx.x; j < (1u << b); j += blockDim.x)
+      acc = ef_add(acc, ef_mul(task.vec[base + j], hi[j >> 5]));
+    acc = ef_mul(acc, lo[threadIdx.x & 31]);
+  } else {
+    for (unsigned j = threadIdx.x; j < (1u << b); j += blockDim.x)
+      acc = ef_add(acc, ef_mul(task.vec[base + j],
+                               ef_mul(lo[j & ((1u << b1) - 1)], hi[j >> b1])));
+  }
   acc = block_sum(acc, red);
   if (threadIdx.x < 32) {
     const ef2 h = eq_high_warp(p, b, k, base);

@@ -212,27 +212,27 @@ __global__ void __launch_bounds__(SC_THREADS, 2)
   const size_t qlen = len >> 2;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < qlen;
        i += (size_t)gridDim.x * blockDim.x) {
-    ef2 e[4][S];
+    // The two pairs of round t one after the other (fewer values live at once): pair m is
+    // (i + m qlen, i + (m + 2) qlen), folded with r_t into element i + m qlen.
+    ef2 y[2][S];
 #pragma unroll
-    for (int j = 0; j < S; ++j) {
-      const ef2* p = P.p[j];
+    for (int m = 0; m < 2; ++m) {
+      ef2 lo[S], hi[S];
 #pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        const size_t x = i + m * qlen;
-        e[m][j] = fold ? ef_lerp(p[x], p[x + len], ra) : p[x];
+      for (int j = 0; j < S; ++j) {
+        const ef2* p = P.p[j];
+        const size_t x = i + m * qlen, xh = x + 2 * qlen;
+        lo[j] = fold ? ef_lerp(p[x], p[x + len], ra) : p[x];
+        hi[j] = fold ? ef_lerp(p[xh], p[xh + len], ra) : p[xh];
+      }
+      add_pair<D, BIN>(lo, hi, s0, skip1);
+#pragma unroll
+      for (int j = 0; j < S; ++j) {
+        y[m][j] = ef_lerp(lo[j], hi[j], rb);
+        P.p[j][i + m * qlen] = y[m][j];
       }
     }
-    add_pair<D, BIN>(e[0], e[2], s0, skip1);
-    add_pair<D, BIN>(e[1], e[3], s0, skip1);
-    ef2 y0[S], y1[S];
-#pragma unroll
-    for (int j = 0; j < S; ++j) {
-      y0[j] = ef_lerp(e[0][j], e[2][j], rb);
-      y1[j] = ef_lerp(e[1][j], e[3][j], rb);
-      P.p[j][i] = y0[j];
-      P.p[j][i + qlen] = y1[j];
-    }
-    add_pair<D, BIN>(y0, y1, s1, true);
+    add_pair<D, BIN>(y[0], y[1], s1, true);
   }
   block_reduce<D>(s0, red);
   if (threadIdx.x == 0)
