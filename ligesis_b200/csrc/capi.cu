@@ -500,6 +500,17 @@ lgs_status lgs_basefold_verify(const uint8_t root[32], const uint64_t* point, si
 
 // ---- measurement ----------------------------------------------------------------------------
 
+namespace {
+// Waits for the context's streams and folds the stage events they recorded into the totals
+// (an asynchronous commit's stages are otherwise folded in only by a later call).
+void profile_settle(lgs_ctx* ctx) {
+  CtxDevice dg(ctx);
+  LGS_CUDA(cudaStreamSynchronize(ctx->st));
+  LGS_CUDA(cudaStreamSynchronize(ctx->hs));
+  ctx->prof.flush();
+}
+}  // namespace
+
 lgs_status lgs_profile(lgs_ctx* ctx, int enable) {
   return guarded([&] {
     need(ctx != nullptr, "lgs_profile: null context");
@@ -515,6 +526,7 @@ lgs_status lgs_profile(lgs_ctx* ctx, int enable) {
 lgs_status lgs_profile_names(lgs_ctx* ctx, char* buf, size_t cap, size_t* needed) {
   return guarded([&] {
     need(ctx && needed, "lgs_profile_names: null argument");
+    profile_settle(ctx);
     std::string all;
     for (auto& t : ctx->prof.totals) all += t.first + "\n";
     *needed = all.size() + 1;
@@ -536,6 +548,7 @@ lgs_status lgs_set_wait_budget(lgs_ctx* ctx, uint64_t cycles) {
 lgs_status lgs_profile_get(lgs_ctx* ctx, const char* stage, double* total_ms, uint64_t* count) {
   return guarded([&] {
     need(ctx && stage && total_ms && count, "lgs_profile_get: null argument");
+    profile_settle(ctx);
     *total_ms = 0;
     *count = 0;
     for (auto& t : ctx->prof.totals)

@@ -12,10 +12,8 @@
 //         DFT over k2 (N2 = 64: 8 warps on 32 columns the same way; smaller N2: one thread per
 //         column, in registers); reads Z and writes X in 256-byte runs per warp.
 // Inside a radix-8 the twiddles are 8th roots of unity, powers of two (2^120 is the order-8 root
-// of the reference's generator), so they are shifts; so are the twiddles between the two radix-8
-// digits of a 64-point DFT (64th roots, 2^39 is the order-64 root): each warp applies the shifts
-// of its digit through a warp-uniform switch.  Only the w_4096 and four-step twiddles use the
-// carry-chain multiplication.
+// of the reference's generator), so they are shifts; the twiddles between the radix-8 digits
+// are per-warp constants or table entries and use the carry-chain multiplication.
 #include "kernels.cuh"
 
 namespace lgs {
@@ -76,34 +74,6 @@ template <> struct RootLog<2> { static constexpr unsigned E = 48; };
 template <> struct RootLog<3> { static constexpr unsigned E = 120; };
 template <> struct RootLog<4> { static constexpr unsigned E = 156; };
 template <> struct RootLog<5> { static constexpr unsigned E = 78; };
-template <> struct RootLog<6> { static constexpr unsigned E = 39; };
-
-// v[j] *= w_64^(j W) for j = 1..7: the twiddles between the two radix-8 digits of a 64-point
-// DFT, powers of two (w_64 = g_6 = 2^39), so shifts.  W is the warp's digit: the warp-uniform
-// switch below picks the compile-time shift amounts of its case.
-template <unsigned W>
-__device__ __forceinline__ void tw64_row(u64* v) {
-  constexpr unsigned E = RootLog<6>::E;
-  v[1] = rot<(E * 1 * W) % 192>(v[1]);
-  v[2] = rot<(E * 2 * W) % 192>(v[2]);
-  v[3] = rot<(E * 3 * W) % 192>(v[3]);
-  v[4] = rot<(E * 4 * W) % 192>(v[4]);
-  v[5] = rot<(E * 5 * W) % 192>(v[5]);
-  v[6] = rot<(E * 6 * W) % 192>(v[6]);
-  v[7] = rot<(E * 7 * W) % 192>(v[7]);
-}
-__device__ __forceinline__ void tw64_warp(u64* v, unsigned w) {
-  switch (w) {
-    case 1: tw64_row<1>(v); break;
-    case 2: tw64_row<2>(v); break;
-    case 3: tw64_row<3>(v); break;
-    case 4: tw64_row<4>(v); break;
-    case 5: tw64_row<5>(v); break;
-    case 6: tw64_row<6>(v); break;
-    case 7: tw64_row<7>(v); break;
-    default: break;
-  }
-}
 
 // Natural-order R-point DFTs (R = 2, 4, 8) on registers v[0], v[ST], ..., v[(R-1) ST];
 // radix-2 DIT on the bit-reversed inputs.  ZH: the upper half of the inputs is zero.
@@ -244,6 +214,9 @@ __global__ void __launch_bounds__(PA_THREADS, 1)
   u64* ex = sm + PA_COLS * PA_CS + grp * 2048;  // [jb][w][lane]
   const size_t row = blockIdx.y;
   const unsigned k2_0 = blockIdx.x * PA_COLS;
+  u64 t64[8];  // w_64^(j w) = w_4096^(64 j w), the same for the whole warp
+#pragma unroll
+  for (int j = 1; j < 8; ++j) t64[j] = __ldg(tw4096 + 64 * j * w);
 
   // phase 1 inputs of this thread's four rounds, loaded up front
   constexpr int NB1 = HALF ? 4 : 8;
@@ -266,7 +239,8 @@ __global__ void __launch_bounds__(PA_THREADS, 1)
 #pragma unroll
     for (int b1 = 0; b1 < 8; ++b1) v[b1] = b1 < NB1 ? pre[i][b1 < NB1 ? b1 : 0] : 0;
     dft_r8<1, HALF>(v);
-    tw64_warp(v, w);
+#pragma unroll
+    for (int j = 1; j < 8; ++j) v[j] = gl_mul(v[j], t64[j]);
 #pragma unroll
     for (int j = 0; j < 8; ++j) ex[(j * 8 + w) * 32 + lane] = v[j];
     group_sync(grp);
@@ -290,7 +264,8 @@ __global__ void __launch_bounds__(PA_THREADS, 1)
 #pragma unroll
     for (int a1 = 0; a1 < 8; ++a1) v[a1] = s[8 * a1];
     dft_r8<1, false>(v);
-    tw64_warp(v, w);
+#pragma unroll
+    for (int j = 1; j < 8; ++j) v[j] = gl_mul(v[j], t64[j]);
 #pragma unroll
     for (int j = 0; j < 8; ++j) ex[(j * 8 + w) * 32 + lane] = v[j];
     group_sync(grp);
@@ -321,7 +296,8 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
   for (int kb = 0; kb < 8; ++kb) v[kb] = gl_mul(v[kb], __ldg(t4 + (w + 8 * kb) * 4096 + j1));
   dft_r8<1, false>(v);
-  tw64_warp(v, w);
+#pragma unroll
+  for (int j = 1; j < 8; ++j) v[j] = gl_mul(v[j], __ldg(tw4096 + 64 * j * w));
 #pragma unroll
   for (int j = 0; j < 8; ++j) ex[(j * 8 + w) * 32 + lane] = v[j];
   __syncthreads();

@@ -74,15 +74,27 @@ struct LigesisProof {
 inline std::vector<u64> hash_columns(const std::vector<u64>& A, size_t W,
                                      const std::vector<u64>& cw, size_t m, size_t two_n) {
   std::vector<u64> H(C * two_n, 0);
+  // The same sums with A read column-wise: AT[i][r] = A[r][i], so the C additions of one set
+  // bit touch one contiguous run (the reference reads A[r][i] across its rows).
+  std::vector<u64> AT(W * C);
+  for (unsigned r = 0; r < C; ++r)
+    for (size_t i = 0; i < W; ++i) AT[i * C + r] = A[r * W + i];
   parallel_ranges(two_n, [&](size_t lo, size_t hi) {  // columns are independent
-    std::vector<u64> acc(C);
+    u64 acc[C];
     for (size_t j = lo; j < hi; ++j) {
-      std::fill(acc.begin(), acc.end(), 0);
+      for (unsigned r = 0; r < C; ++r) acc[r] = 0;
       for (size_t i = 0; i < m; ++i) {
         u64 v = cw[i * two_n + j];
-        for (unsigned k = 0; k < ETA; ++k)
-          if ((v >> k) & 1)
-            for (unsigned r = 0; r < C; ++r) acc[r] = add(acc[r], A[r * W + ETA * i + k]);
+        while (v) {
+          const unsigned k = (unsigned)__builtin_ctzll(v);
+          v &= v - 1;
+          const u64* a = &AT[(ETA * i + k) * C];
+          for (unsigned r = 0; r < C; ++r) {  // add() without branches
+            u64 t = acc[r] + a[r];
+            t += (u64)(t < a[r]) * EPS;
+            acc[r] = t - (u64)(t >= P) * P;
+          }
+        }
       }
       for (unsigned r = 0; r < C; ++r) H[r * two_n + j] = acc[r];
     }
