@@ -19,7 +19,7 @@ namespace lgs {
 
 namespace {
 constexpr unsigned SC_THREADS = 256;
-constexpr unsigned SC_TAIL_THREADS = 512;
+constexpr unsigned SC_TAIL_THREADS = 128;
 
 __device__ __forceinline__ ef2 shfl_xor_ef(ef2 v, int m) {
   ef2 r;
@@ -299,12 +299,26 @@ __device__ void interp_weights(ef2 r, ef2 (&L)[D + 1]) {
   }
 }
 
-// Remaining rounds t0..k-1 in one CTA, in shared memory.  On entry the vectors hold `len`
-// entries (len <= TAIL); if `fold`, they hold 2*len entries still to be folded with
-// challenge t0 - 1.  A round's sums go per warp to shared memory (no block reduction per round);
-// the accumulation and the fold of an index are done by the same thread, so one barrier per
-// round suffices, and none once a single warp holds all pairs.  g(1) of every round after the
-// first is filled in at the end along the claim chain (see the chain below).
+// Remaining rounds t0..k-1 in one CTA of SC_TAIL_THREADS (NT) threads.  On entry the vectors hold
+// `len` entries (len <= TAIL); if `fold`, they hold 2*len entries still to be folded with
+// challenge t0 - 1.  The high variable is bound first (pairs i, i + half), so a thread that owns
+// the indices congruent to its id modulo NT owns both members of every pair while half >= NT:
+//   phase A  rounds with half >= NT: each thread folds its own slice of shared memory, no
+//            barrier (at most three rounds: TAIL = 8 NT);
+//   hand-over one barrier; warp 0 continues alone;
+//   phase B  rounds with 32 <= half < NT: the same with lane l owning l mod 32;
+//   phase C  half < 32: one entry per lane, the partner's through a shuffle.
+// No round waits for a reduction: each round's sums go to shared memory per warp (phase A) or
+// per lane (B, C) and are added up once at the end.  g(1) of every round after the first is
+// filled in along the claim chain (see the chain below).
+template <int D, bool BIN>
+struct TailSmem {
+  static constexpr int S = Fac<D, BIN>::S;
+  ef2 sv[S][Fac<D, BIN>::TAIL];
+  ef2 wsum[3][SC_TAIL_THREADS / 32][D + 1];  // phase A: per-warp sums of its (<= 3) rounds
+  ef2 lsum[8][D + 1][32];                     // phases B and C: per-lane sums (<= 7 rounds)
+};
+
 template <int D, bool BIN>
 __global__ void __launch_bounds__(SC_TAIL_THREADS)
     sc_tail_kernel(Polys<Fac<D, BIN>::S> P, unsigned len, int fold, const ef2* __restrict__ ch,
@@ -312,51 +326,54 @@ __global__ void __launch_bounds__(SC_TAIL_THREADS)
                    ef2* __restrict__ final_out, const ef2* __restrict__ partials,
                    size_t stride) {
   constexpr int S = Fac<D, BIN>::S;
-  constexpr unsigned NW = SC_TAIL_THREADS / 32;
-  constexpr unsigned MAXR = 11;  // log2(TAIL) + 1 rounds at most
-  __shared__ ef2 sv[S][Fac<D, BIN>::TAIL];
-  __shared__ ef2 acc[MAXR][NW][D + 1];
+  constexpr unsigned NT = SC_TAIL_THREADS, NW = NT / 32;
+  extern __shared__ __align__(16) unsigned char tail_smem_raw[];
+  TailSmem<D, BIN>& sm = *reinterpret_cast<TailSmem<D, BIN>*>(tail_smem_raw);
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // The multi-CTA rounds 0..t0-1: round t's sums over the CTAs that ran it (one warp per round);
-  // the claim chain at the end reads them, after the barriers below.
+  // the claim chain at the end reads them, after the hand-over barrier below.
   for (unsigned t = warp; t < t0; t += NW) {
     const size_t half = (size_t)1 << (k - 1 - t);
     const unsigned nb =
         (unsigned)min((size_t)SC_MAX_BLOCKS, (half + SC_THREADS - 1) / SC_THREADS);
-    ef2 s[D + 1];
+    ef2 sr[D + 1];
 #pragma unroll
-    for (int q = 0; q <= D; ++q) s[q] = ef_zero();
+    for (int q = 0; q <= D; ++q) sr[q] = ef_zero();
     const ef2* src = partials + (size_t)t * stride;
     for (unsigned b = lane; b < nb; b += 32)
 #pragma unroll
-      for (int q = 0; q <= D; ++q) s[q] = ef_add(s[q], src[(size_t)b * (D + 1) + q]);
+      for (int q = 0; q <= D; ++q) sr[q] = ef_add(sr[q], src[(size_t)b * (D + 1) + q]);
 #pragma unroll
     for (int q = 0; q <= D; ++q)
 #pragma unroll
-      for (int m = 16; m; m >>= 1) s[q] = ef_add(s[q], shfl_xor_ef(s[q], m));
+      for (int m = 16; m; m >>= 1) sr[q] = ef_add(sr[q], shfl_xor_ef(sr[q], m));
     if (lane == 0)
 #pragma unroll
-      for (int q = 0; q <= D; ++q) rounds_out[(size_t)t * (D + 1) + q] = s[q];
+      for (int q = 0; q <= D; ++q) rounds_out[(size_t)t * (D + 1) + q] = sr[q];
   }
+  // load, folding with the previous challenge; thread i loads the indices it owns in phase A
   {
     const ef2 r = fold ? ch[t0 - 1] : ef_zero();
-    for (unsigned i = threadIdx.x; i < len; i += blockDim.x)
+    for (unsigned i = threadIdx.x; i < len; i += NT)
 #pragma unroll
       for (int j = 0; j < S; ++j)
-        sv[j][i] = fold ? ef_lerp(P.p[j][i], P.p[j][i + len], r) : P.p[j][i];
+        sm.sv[j][i] = fold ? ef_lerp(P.p[j][i], P.p[j][i + len], r) : P.p[j][i];
   }
-  __syncthreads();
-  // one round over `half` pairs: sums of the thread's pairs, then the fold of the same indices
-  auto round = [&](unsigned t, unsigned half) {
+  unsigned L = len, t = t0, ra = 0;
+  // phase A
+  for (; L >= 2 * NT && t < k; ++t, ++ra, L >>= 1) {
+    const unsigned half = L >> 1;
+    const ef2 r = ch[t];
     ef2 s[D + 1];
 #pragma unroll
     for (int q = 0; q <= D; ++q) s[q] = ef_zero();
-    const bool skip1 = t > 0;
-    for (unsigned i = threadIdx.x; i < half; i += blockDim.x) {
+    for (unsigned i = threadIdx.x; i < half; i += NT) {
       ef2 lo[S], hi[S];
 #pragma unroll
-      for (int j = 0; j < S; ++j) lo[j] = sv[j][i], hi[j] = sv[j][i + half];
-      add_pair<D, BIN>(lo, hi, s, skip1);
+      for (int j = 0; j < S; ++j) lo[j] = sm.sv[j][i], hi[j] = sm.sv[j][i + half];
+      add_pair<D, BIN>(lo, hi, s, t > 0);
+#pragma unroll
+      for (int j = 0; j < S; ++j) sm.sv[j][i] = ef_lerp(lo[j], hi[j], r);
     }
 #pragma unroll
     for (int q = 0; q <= D; ++q)
@@ -364,55 +381,86 @@ __global__ void __launch_bounds__(SC_TAIL_THREADS)
       for (int m = 16; m; m >>= 1) s[q] = ef_add(s[q], shfl_xor_ef(s[q], m));
     if (lane == 0)
 #pragma unroll
-      for (int q = 0; q <= D; ++q) acc[t - t0][warp][q] = s[q];
+      for (int q = 0; q <= D; ++q) sm.wsum[ra][warp][q] = s[q];
+  }
+  __syncthreads();  // hand-over: every fold and partial-round sum is visible
+  if (warp != 0) return;
+  unsigned rb = 0;
+  // phase B
+  for (; L >= 64 && t < k; ++t, ++rb, L >>= 1) {
+    const unsigned half = L >> 1;
     const ef2 r = ch[t];
-    for (unsigned i = threadIdx.x; i < half; i += blockDim.x)
+    ef2 s[D + 1];
 #pragma unroll
-      for (int j = 0; j < S; ++j) sv[j][i] = ef_lerp(sv[j][i], sv[j][i + half], r);
-  };
-  unsigned t = t0;
-  for (; t < k && (len >> 1) > 32; ++t, len >>= 1) {
-    round(t, len >> 1);
-    __syncthreads();
-  }
-  if (warp == 0) {
-    for (unsigned tt = t, l = len; tt < k; ++tt, l >>= 1) {
-      round(tt, l >> 1);
-      __syncwarp();
+    for (int q = 0; q <= D; ++q) s[q] = ef_zero();
+    for (unsigned i = lane; i < half; i += 32) {
+      ef2 lo[S], hi[S];
+#pragma unroll
+      for (int j = 0; j < S; ++j) lo[j] = sm.sv[j][i], hi[j] = sm.sv[j][i + half];
+      add_pair<D, BIN>(lo, hi, s, t > 0);
+#pragma unroll
+      for (int j = 0; j < S; ++j) sm.sv[j][i] = ef_lerp(lo[j], hi[j], r);
     }
-  } else {
-    for (unsigned tt = t; tt < k; ++tt)
-      if (lane == 0)
 #pragma unroll
-        for (int q = 0; q <= D; ++q) acc[tt - t0][warp][q] = ef_zero();
+    for (int q = 0; q <= D; ++q) sm.lsum[rb][q][lane] = s[q];
   }
-  __syncthreads();
-  // this kernel's rounds: sums over the warps (g(1) only for round 0)
-  for (unsigned i = threadIdx.x; i < (k - t0) * (D + 1); i += blockDim.x) {
-    const unsigned tt = i / (D + 1), q = i % (D + 1);
-    if (q == 1 && t0 + tt > 0) continue;
-    ef2 v = ef_zero();
+  __syncwarp();
+  // phase C
+  ef2 v[S];
 #pragma unroll
-    for (unsigned w = 0; w < NW; ++w) v = ef_add(v, acc[tt][w][q]);
-    rounds_out[(size_t)(t0 + tt) * (D + 1) + q] = v;
+  for (int j = 0; j < S; ++j) v[j] = lane < L ? sm.sv[j][lane] : ef_zero();
+  for (; L > 1 && t < k; ++t, ++rb, L >>= 1) {
+    const unsigned half = L >> 1;
+    const ef2 r = ch[t];
+    ef2 hi[S];
+#pragma unroll
+    for (int j = 0; j < S; ++j)
+      hi[j] = ef_make(__shfl_down_sync(0xffffffffu, v[j].c0, half),
+                      __shfl_down_sync(0xffffffffu, v[j].c1, half));
+    ef2 s[D + 1];
+#pragma unroll
+    for (int q = 0; q <= D; ++q) s[q] = ef_zero();
+    if (lane < half) {
+      add_pair<D, BIN>(v, hi, s, t > 0);
+#pragma unroll
+      for (int j = 0; j < S; ++j) v[j] = ef_lerp(v[j], hi[j], r);
+    }
+#pragma unroll
+    for (int q = 0; q <= D; ++q) sm.lsum[rb][q][lane] = s[q];
   }
-  if (threadIdx.x == 0) {
+  __syncwarp();
+  // this kernel's round sums (g(1) only for round 0): lane x adds up one (round, q) pair
+  const unsigned nra = ra, nrb = rb;
+  for (unsigned x = lane; x < (nra + nrb) * (D + 1); x += 32) {
+    const unsigned rr = x / (D + 1), q = x % (D + 1);
+    const unsigned tt = t0 + rr;
+    if (q == 1 && tt > 0) continue;
+    ef2 acc = ef_zero();
+    if (rr < nra) {
+#pragma unroll
+      for (unsigned w = 0; w < NW; ++w) acc = ef_add(acc, sm.wsum[rr][w][q]);
+    } else {
+      for (unsigned l = 0; l < 32; ++l) acc = ef_add(acc, sm.lsum[rr - nra][q][l]);
+    }
+    rounds_out[(size_t)tt * (D + 1) + q] = acc;
+  }
+  __threadfence_block();  // the chain below reads these sums from other lanes
+  if (lane == 0) {
     if (BIN) {
-      final_out[0] = sv[0][0];
-      final_out[1] = ef_sub(sv[0][0], ef_one());
+      final_out[0] = v[0];
+      final_out[1] = ef_sub(v[0], ef_one());
 #pragma unroll
-      for (int j = 1; j < S; ++j) final_out[j + 1] = sv[j][0];
+      for (int j = 1; j < S; ++j) final_out[j + 1] = v[j];
     } else {
 #pragma unroll
-      for (int j = 0; j < S; ++j) final_out[j] = sv[j][0];
+      for (int j = 0; j < S; ++j) final_out[j] = v[j];
     }
   }
-  __syncthreads();
+  __syncwarp();
   // The claim chain: g_t(1) = claim_t - g_t(0) for t >= 1, claim_{t+1} = g_t(r_t).  With
   // g_t(r) = sum_q L_q(r) g_t(q), claim_{t+1} = A_t + L_1(r_t) claim_t, A_t collecting the other
   // terms (and A_0 = g_0(r_0), whose g(1) is summed), so lane t prepares its round's A_t and
   // L_1(r_t) in parallel and the claim moves from lane to lane with one product per round.
-  if (warp != 0) return;
   ef2 claim = ef_zero();
   for (unsigned c0 = 0; c0 < k; c0 += 32) {
     const unsigned tt = c0 + lane;
@@ -482,7 +530,10 @@ void sumcheck_run(ef2* const* polys, unsigned k, const ef2* ch, ef2* rounds_out,
   tl_mark("sc_passes_end", st);
   // the tail also sums the multi-CTA rounds' partials, and completes their g(1) along the
   // claim chain
-  sc_tail_kernel<D, BIN><<<1, SC_TAIL_THREADS, 0, st>>>(P, (unsigned)len, fold, ch, t, k,
+  constexpr size_t tail_smem = sizeof(TailSmem<D, BIN>);
+  LGS_CUDA(cudaFuncSetAttribute(sc_tail_kernel<D, BIN>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tail_smem));
+  sc_tail_kernel<D, BIN><<<1, SC_TAIL_THREADS, tail_smem, st>>>(P, (unsigned)len, fold, ch, t, k,
                                                         rounds_out, final_out, partials, stride);
   LGS_LAUNCH_CHECK();
 }
