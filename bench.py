@@ -301,8 +301,11 @@ def run_ours(args) -> None:
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
+    from ligesis_b200 import autotune
+
     lib = L.load()
     ctx = L.Context(local)
+    tuned = autotune.apply(ctx, LOG_M, LOG_N)  # launch choices from the committed tuning cache
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=torch.device("cuda", local))
 
     f, A, z, fields, ints = bench_inputs(rank)
@@ -468,7 +471,8 @@ def run_ours(args) -> None:
         "metric": metric_for(LOG_M, LOG_N), "value": round(value, 3), "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dev_ms, 3),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (mod p)",
-        "data": "synthetic (seeded uniform Goldilocks)", "config": _config(world),
+        "data": "synthetic (seeded uniform Goldilocks)",
+        "config": {**_config(world), "tuning": tuned or "built-in defaults"},
         "e2e": {"value": round(e2e_ms / world, 3), "unit": "ms",
                 "h2d_bytes_per_step": int(f.nbytes), "d2h_bytes_per_step": len(proof.data) + 32},
         "stages_ms": {k: round(v, 4) for k, v in stages.items()},
@@ -806,9 +810,21 @@ def run_sumcheck(args) -> None:
         del pristine, work, out
 
 
+def run_autotune(args) -> None:
+    """Times candidate launch choices of the commit + prove step and records the fastest in
+    ligesis_b200/tuning.json (see ligesis_b200/autotune.py)."""
+    from ligesis_b200 import autotune
+
+    entry = autotune.tune(args.log_m, args.log_n, steps=args.steps, warmup=args.warmup)
+    print(json.dumps({"mode": "autotune", "log_m": args.log_m, "log_n": args.log_n, **entry}),
+          flush=True)
+
+
 def run_timeline(args) -> None:
     """The prove's replayed graph with timeline event nodes (profile level 2): for each branch
-    boundary, ms from the prove's start, averaged over `--steps` proves of one commitment."""
+    boundary, ms from the prove's start, averaged over `--steps` proves of one commitment.  With
+    --overlap each prove follows a fresh commit of the same polynomial, as in the bench step, so
+    the commit's hash and tree run beside it."""
     import numpy as np
     import torch
 
@@ -825,18 +841,28 @@ def run_timeline(args) -> None:
     oracle = L.RandomOracle(0, length=8)
     oracle.fields, oracle.ints = g.ext_elements(4096), g.ints(4096)
     pk, _ = L.Ligesis.setup_with_hash(lm, ln, L.SubsetSumHash(64 << lm, a=A), ctx)
+    from ligesis_b200 import autotune
+
+    if args.overlap:
+        autotune.apply(ctx, lm, ln)
     f_dev = torch.from_numpy(f.view(np.int64)).to("cuda:0")
     commit, data = L.Ligesis.commit_device(pk, f_dev.data_ptr(), f.size)
     import ctypes as C
 
+    def one():
+        nonlocal commit, data
+        if args.overlap:
+            del data
+            commit, data = L.Ligesis.commit_device(pk, f_dev.data_ptr(), f.size)
+        oracle.restart()
+        L.Ligesis.prove(pk, data, z, oracle)
+
     L._lib.check(lib.lgs_profile(ctx.handle, 2))
     for _ in range(3):  # eager, capture, first replay
-        oracle.restart()
-        L.Ligesis.prove(pk, data, z, oracle)
+        one()
     L._lib.check(lib.lgs_profile(ctx.handle, 2))
     for _ in range(args.steps):
-        oracle.restart()
-        L.Ligesis.prove(pk, data, z, oracle)
+        one()
     need = C.c_size_t()
     L._lib.check(lib.lgs_profile_names(ctx.handle, None, 0, C.byref(need)))
     buf = C.create_string_buffer(need.value)
@@ -1097,10 +1123,13 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch-serve", action="store_true",
                     help="line mode: leave out the batched and served measurements")
+    ap.add_argument("--overlap", action="store_true",
+                    help="timeline mode: a fresh commit before every prove (as in the step)")
     ap.add_argument("--connections", type=int, default=0,
                     help="CUDA_DEVICE_MAX_CONNECTIONS for this process (0: the driver default)")
     ap.add_argument("--mode", choices=["line", "batch", "serve", "commit", "timeline", "basefold",
-                                       "logup", "witness", "sumcheck"], default="line")
+                                       "logup", "witness", "sumcheck", "autotune"],
+                    default="line")
     ap.add_argument("--log-m", type=int, default=LOG_M)
     ap.add_argument("--log-n", type=int, default=LOG_N)
     ap.add_argument("--lanes", type=int, default=12)
@@ -1143,6 +1172,9 @@ def main() -> None:
         return
     if args.mode == "sumcheck":
         run_sumcheck(args)
+        return
+    if args.mode == "autotune":
+        run_autotune(args)
         return
     if args.impl == "reference":
         run_reference(args)

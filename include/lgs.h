@@ -253,6 +253,14 @@ lgs_status lgs_profile_get(lgs_ctx* ctx, const char* stage, double* total_ms, ui
 /* Names of the stages with totals since lgs_profile(ctx, 1|2), one per line ("tl:<mark>" for
  * timeline marks); *needed receives the buffer size that holds them all (with the NUL). */
 lgs_status lgs_profile_names(lgs_ctx* ctx, char* buf, size_t cap, size_t* needed);
+/* Launch choices of this context's kernels, picked by the autotuner (ligesis_b200/autotune.py;
+ * no counterpart in the reference, which has no kernels).  0 restores the built-in default.
+ *   "hash_ctas"        persistent CTAs of the subset-sum hash (default one per SM); fewer leave
+ *                      SMs to the prove that runs beside the commit's hash
+ *   "sumcheck_blocks"  grid cap of the multi-CTA sumcheck passes (at most 296)
+ * Results do not depend on them.  Unknown names: LGS_ERR_BAD_ARG. */
+lgs_status lgs_tune(lgs_ctx* ctx, const char* name, uint64_t value);
+lgs_status lgs_tune_get(lgs_ctx* ctx, const char* name, uint64_t* value);
 /* Clock-cycle budget of the bounded device waits in the kernels this context launches (the
  * subset-sum hash's pipeline waits; no counterpart in the reference, whose code has no device
  * waits).  0 restores the default of about 2 s.  A budget shorter than the awaited event makes

@@ -74,6 +74,8 @@ _SIGS = {
     "lgs_profile_get": (C.c_int, [vp, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "lgs_launch_count": (C.c_uint64, []),
     "lgs_set_wait_budget": (C.c_int, [vp, C.c_uint64]),
+    "lgs_tune": (C.c_int, [vp, C.c_char_p, C.c_uint64]),
+    "lgs_tune_get": (C.c_int, [vp, C.c_char_p, C.POINTER(C.c_uint64)]),
     "lgs_profile_names": (C.c_int, [vp, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "lgs_sumcheck_prove_dev": (C.c_int, [vp, vp, C.c_uint, C.c_uint, vp, vp, vp]),
     "lgs_new_eq_dev": (C.c_int, [vp, vp, C.c_uint, vp]),
@@ -187,6 +189,19 @@ class Context:
         s = vp()
         check(self._lib.lgs_ctx_stream(self.handle, C.byref(s)))
         return int(s.value or 0)
+
+    def tune(self, **params: int) -> None:
+        """Launch choices of this context's kernels (lgs_tune): hash_ctas, sumcheck_blocks."""
+        for name, value in params.items():
+            check(self._lib.lgs_tune(self.handle, name.encode(), int(value)))
+
+    def tuning(self, *names: str) -> dict:
+        out = {}
+        for name in names or ("hash_ctas", "sumcheck_blocks"):
+            v = C.c_uint64()
+            check(self._lib.lgs_tune_get(self.handle, name.encode(), C.byref(v)))
+            out[name] = int(v.value)
+        return out
 
     def set_wait_budget(self, cycles: int) -> None:
         """Clock-cycle budget of the bounded device waits of this context's kernels (0 = the

@@ -1,0 +1,137 @@
+"""Autotuner for the launch choices of the commit + prove step (lgs_tune), with a JSON cache.
+
+The step runs the commit's subset-sum hash (a persistent tensor-core kernel, one CTA per SM by
+default) beside the prove's DAG of sumcheck, eq-table and Basefold kernels, so two choices trade
+against each other:
+
+* ``hash_ctas``: how many SMs the hash occupies; fewer leave SMs to the prove's latency-bound
+  branches while the hash runs.
+* ``sumcheck_blocks``: the grid cap of the multi-CTA sumcheck passes.
+
+``tune`` times candidate settings on the device (CUDA events on the context's stream, f already
+in HBM, the same step the bench times), keeps the fastest, and records it per GPU name and
+shape in the cache (``tuning.json`` beside this file unless a path is given).  ``apply`` sets a
+context from the cache.  Every setting computes the same commitment and proof bytes; ``tune``
+checks that too.
+"""
+from __future__ import annotations
+
+import json
+import time
+from pathlib import Path
+
+import numpy as np
+
+CACHE = Path(__file__).with_name("tuning.json")
+PARAMS = ("hash_ctas", "sumcheck_blocks")
+
+
+def _device_name(device: int = 0) -> str:
+    import torch
+
+    return torch.cuda.get_device_name(device)
+
+
+def shape_key(log_m: int, log_n: int) -> str:
+    return f"{log_m}x{log_n}"
+
+
+def load(path: Path | None = None) -> dict:
+    p = Path(path or CACHE)
+    return json.loads(p.read_text()) if p.exists() else {}
+
+
+def lookup(log_m: int, log_n: int, device: int = 0, path: Path | None = None) -> dict | None:
+    entry = load(path).get(_device_name(device), {}).get(shape_key(log_m, log_n))
+    return {k: entry[k] for k in PARAMS if k in entry} if entry else None
+
+
+def apply(ctx, log_m: int, log_n: int, path: Path | None = None) -> dict | None:
+    """Sets ctx's launch choices from the cache; returns them (None: no entry, defaults kept)."""
+    best = lookup(log_m, log_n, ctx.device, path)
+    if best:
+        ctx.tune(**best)
+    return best
+
+
+def tune(log_m: int, log_n: int, steps: int = 10, warmup: int = 3, device: int = 0,
+         hash_ctas=None, sumcheck_blocks=None, path: Path | None = None,
+         save: bool = True) -> dict:
+    """Coordinate search: hash_ctas first (sumcheck_blocks at its default), then
+    sumcheck_blocks at the best hash_ctas.  Returns the cache entry it wrote."""
+    import torch
+
+    import ligesis_b200 as L
+    from ligesis_b200 import rng
+
+    torch.cuda.set_device(device)
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    hash_ctas = list(hash_ctas or [sms - d for d in (0, 8, 16, 24, 32, 40, 48, 56)])
+    sumcheck_blocks = list(sumcheck_blocks or [296, 222, 148, 74])
+    ctx = L.Context(device)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=torch.device("cuda", device))
+    mu = log_m + log_n
+    f = rng.field_elements(1, 1 << mu)
+    A = rng.field_elements(2, 32 * (64 << log_m)).reshape(32, 64 << log_m)
+    z = rng.ext_elements(3, mu)
+    g = rng.SeededRng(4)
+    oracle = L.RandomOracle(0, length=8)
+    oracle.fields, oracle.ints = g.ext_elements(4096), g.ints(4096)
+    pk, _ = L.Ligesis.setup_with_hash(log_m, log_n, L.SubsetSumHash(64 << log_m, a=A), ctx)
+    f_dev = torch.from_numpy(f.view(np.int64)).to(f"cuda:{device}")
+
+    def step():
+        oracle.restart()
+        commit, data = L.Ligesis.commit_device(pk, f_dev.data_ptr(), f.size)
+        proof = L.Ligesis.prove(pk, data, z, oracle)
+        return commit, proof
+
+    ref = None
+
+    def measure(setting: dict) -> float:
+        nonlocal ref
+        ctx.tune(**setting)
+        prev = None
+        for _ in range(warmup):
+            prev = step()
+        c, p = prev
+        out = (c.root, p.data)
+        if ref is None:
+            ref = out
+        if out != ref:
+            raise RuntimeError(f"setting {setting} changed the commitment or proof")
+        del prev, c, p
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            last = step()
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        del last
+        return e0.elapsed_time(e1) / steps
+
+    trials = []
+    best = {"hash_ctas": 0, "sumcheck_blocks": 0}
+    best_ms = measure(best)
+    trials.append({**best, "ms": round(best_ms, 4)})
+    for h in hash_ctas:
+        s = {"hash_ctas": h, "sumcheck_blocks": 0}
+        ms = measure(s)
+        trials.append({**s, "ms": round(ms, 4)})
+        if ms < best_ms:
+            best, best_ms = s, ms
+    for b in sumcheck_blocks:
+        s = {"hash_ctas": best["hash_ctas"], "sumcheck_blocks": b}
+        ms = measure(s)
+        trials.append({**s, "ms": round(ms, 4)})
+        if ms < best_ms:
+            best, best_ms = s, ms
+    ctx.tune(hash_ctas=0, sumcheck_blocks=0)
+    entry = {**best, "ms": round(best_ms, 4), "default_ms": trials[0]["ms"],
+             "steps": steps, "when": time.strftime("%Y-%m-%d"), "trials": trials}
+    if save:
+        cache = load(path)
+        cache.setdefault(_device_name(device), {})[shape_key(log_m, log_n)] = entry
+        Path(path or CACHE).write_text(json.dumps(cache, indent=1) + "\n")
+    return entry

@@ -538,6 +538,38 @@ lgs_status lgs_profile_names(lgs_ctx* ctx, char* buf, size_t cap, size_t* needed
   });
 }
 
+lgs_status lgs_tune(lgs_ctx* ctx, const char* name, uint64_t value) {
+  return guarded([&] {
+    need(ctx && name, "lgs_tune: null argument");
+    const std::string n(name);
+    if (n == "hash_ctas") {
+      need(value <= 4096, "lgs_tune: hash_ctas above 4096");
+      ctx->hash_ctas = (unsigned)value;
+    } else if (n == "sumcheck_blocks") {
+      need(value <= SC_MAX_BLOCKS, "lgs_tune: sumcheck_blocks above the partial-sum slots");
+      ctx->sumcheck_blocks = (unsigned)value;
+      // captured prove graphs hold the old launch shapes: drop them (recaptured on next use)
+      CtxDevice dg(ctx);
+      LGS_CUDA(cudaStreamSynchronize(ctx->st));
+      for (auto& g : ctx->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+      ctx->graphs.clear();
+    } else {
+      throw std::invalid_argument("lgs_tune: unknown parameter " + n);
+    }
+  });
+}
+
+lgs_status lgs_tune_get(lgs_ctx* ctx, const char* name, uint64_t* value) {
+  return guarded([&] {
+    need(ctx && name && value, "lgs_tune_get: null argument");
+    const std::string n(name);
+    if (n == "hash_ctas") *value = ctx->hash_ctas;
+    else if (n == "sumcheck_blocks") *value = ctx->sumcheck_blocks;
+    else throw std::invalid_argument("lgs_tune_get: unknown parameter " + n);
+  });
+}
+
 lgs_status lgs_set_wait_budget(lgs_ctx* ctx, uint64_t cycles) {
   return guarded([&] {
     need(ctx != nullptr, "lgs_set_wait_budget: null context");

@@ -517,7 +517,8 @@ void make_alimb_tmap(const uint8_t* alimb, size_t W, void* tmap_out) {
 size_t tensor_map_bytes() { return sizeof(CUtensorMap); }
 
 void subset_sum_hash_tc(const void* tmap, const u64* cw, u64* H, u32* leaves, unsigned m,
-                        size_t two_n, int* err, cudaStream_t st, uint64_t wait_cycles) {
+                        size_t two_n, int* err, cudaStream_t st, uint64_t wait_cycles,
+                        unsigned max_ctas) {
   if (two_n % TC_N) throw ShapeError("hash: 2n must be a multiple of 256");
   if (m == 0 || m > 8192) throw ShapeError("hash: 1 <= m <= 8192");
   LGS_CUDA(cudaFuncSetAttribute(hash_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -526,7 +527,9 @@ void subset_sum_hash_tc(const void* tmap, const u64* cw, u64* H, u32* leaves, un
   LGS_CUDA(cudaGetDevice(&dev));
   LGS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const size_t ntiles = two_n / TC_N;
-  const unsigned grid = (unsigned)std::min<size_t>(ntiles, (size_t)std::max(sms, 1));
+  const size_t ctas = max_ctas ? std::min<size_t>(max_ctas, (size_t)std::max(sms, 1))
+                              : (size_t)std::max(sms, 1);
+  const unsigned grid = (unsigned)std::min<size_t>(ntiles, ctas);
   const long long budget =
       wait_cycles ? (long long)std::min<uint64_t>(wait_cycles, (uint64_t)WAIT_CYCLES) : WAIT_CYCLES;
   hash_tc_kernel<<<grid, NTHREADS, SMEM_BYTES, st>>>(*(const CUtensorMap*)tmap, cw, H, leaves, m,

@@ -34,8 +34,10 @@ void alimb_from_a(const u64* A, uint8_t* alimb, size_t W, cudaStream_t st);
 void make_alimb_tmap(const uint8_t* alimb, size_t W, void* tmap_out);
 size_t tensor_map_bytes();
 // wait_cycles: clock budget of the kernel's bounded waits (0 = the default, about 2 s).
+// max_ctas: persistent CTAs (0 = one per SM); fewer leave SMs to concurrent work.
 void subset_sum_hash_tc(const void* tmap, const u64* cw, u64* H, u32* leaves, unsigned m,
-                        size_t two_n, int* err, cudaStream_t st, uint64_t wait_cycles = 0);
+                        size_t two_n, int* err, cudaStream_t st, uint64_t wait_cycles = 0,
+                        unsigned max_ctas = 0);
 // Dense tcgen05 kind::i8 throughput (TOP/s) of back-to-back M128 N256 K32 MMAs on every SM.
 double i8_tensor_peak_tops(unsigned iters, int* err, cudaStream_t st);
 
@@ -62,11 +64,12 @@ void tl_mark(const char* what, cudaStream_t st);
 
 // sumcheck.cu
 size_t sumcheck_partials_elems(unsigned k, unsigned d);
+// max_blocks: grid cap of the multi-CTA passes (0 or above SC_MAX_BLOCKS: SC_MAX_BLOCKS).
 void sumcheck_prove_dev(ef2* const* polys, unsigned d, unsigned k, const ef2* ch, ef2* rounds_out,
-                        ef2* final_out, ef2* partials, cudaStream_t st);
+                        ef2* final_out, ef2* partials, cudaStream_t st, unsigned max_blocks = 0);
 // The 3-factor sumcheck of [b, b - 1, eq] storing only b and eq (both folded in place).
 void sumcheck_binary_dev(ef2* b, ef2* eq, unsigned k, const ef2* ch, ef2* rounds_out,
-                         ef2* final_out, ef2* partials, cudaStream_t st);
+                         ef2* final_out, ef2* partials, cudaStream_t st, unsigned max_blocks = 0);
 
 // eval.cu
 void canon_u64(u64* p, size_t n, cudaStream_t st);  // p[i] = p[i] mod p, in place

@@ -400,7 +400,7 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
   {
     StageTimer t(c->prof, c->hs, "subset_sum_hash");  // H and its Merkle leaf hashes
     subset_sum_hash_tc(pk->tmap, cd->cw.as<u64>(), cd->H.as<u64>(), cd->nodes.as<u32>(),
-                       (unsigned)m, two_n, c->err.as<int>(), c->hs, c->wait_cycles);
+                       (unsigned)m, two_n, c->err.as<int>(), c->hs, c->wait_cycles, c->hash_ctas);
   }
   {
     StageTimer t(c->prof, c->hs, "merkle_h");
@@ -902,7 +902,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     new_eq_dev(d_fields + fp.alpha1, nb, p2, b);
     tl_mark("inputs_end", b);
     sumcheck_binary_dev(p0, p2, nb, d_fields + fp.ch_bin, (ef2*)(stage + S_sc_r[0]),
-                        (ef2*)(stage + S_sc_f[0]), partials_for(nb, 3), b);
+                        (ef2*)(stage + S_sc_f[0]), partials_for(nb, 3), b, c->sumcheck_blocks);
     mark("C_binary_sc_end", b);
   }
   // D: hash and recon bilinear sumchecks (pcs/src/ligesis.rs:435-485)
@@ -921,10 +921,10 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     ef2* ph[2] = {g1, g2};
     ef2* part = partials_for(log_w, 2);
     sumcheck_prove_dev(ph, 2, log_w, d_fields + fp.ch_hash, (ef2*)(stage + S_sc_r[1]),
-                       (ef2*)(stage + S_sc_f[1]), part, b);
+                       (ef2*)(stage + S_sc_f[1]), part, b, c->sumcheck_blocks);
     ef2* pr[2] = {v, g2b};
     sumcheck_prove_dev(pr, 2, log_w, d_fields + fp.ch_recon, (ef2*)(stage + S_sc_r[2]),
-                       (ef2*)(stage + S_sc_f[2]), part, b);
+                       (ef2*)(stage + S_sc_f[2]), part, b, c->sumcheck_blocks);
     mark("D_hash_recon_sc_end", b);
   }
   // F: Stage A point reduction of B_I (pcs/src/ligesis.rs:510-516)
@@ -938,7 +938,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     tl_mark("inputs_end", b);
     ef2* pb[2] = {bie, gbi};
     sumcheck_prove_dev(pb, 2, nb, d_fields + fp.ch_bi, (ef2*)(stage + S_sc_r[5]),
-                       (ef2*)(stage + S_sc_f[5]), partials_for(nb, 2), b);
+                       (ef2*)(stage + S_sc_f[5]), partials_for(nb, 2), b, c->sumcheck_blocks);
     mark("F_bi_batch_sc_end", b);
   }
   // -- a-bar = eq_{z1}^T F and everything that needs it (pcs/src/ligesis.rs:365-387)
@@ -973,7 +973,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     d2d(rac, ra, two_n * sizeof(ef2), b);
     ef2* pt[2] = {sel, rac};
     sumcheck_prove_dev(pt, 2, log_n + 1, d_fields + fp.ch_table, (ef2*)(stage + S_sc_r[3]),
-                       (ef2*)(stage + S_sc_f[3]), partials_for(log_n + 1, 2), b);
+                       (ef2*)(stage + S_sc_f[3]), partials_for(log_n + 1, 2), b, c->sumcheck_blocks);
     eq_dot_dev(ra, 0, d_prm + P_r3, log_n + 1, (ef2*)(stage + S_y5), partials_for(log_n + 1, 1), b);
     mark("A2_rs_abar_table_sc_end", b);
   }
@@ -987,7 +987,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     d2d(ac, a_vec, n * sizeof(ef2), b);
     ef2* pw[2] = {ac, w};
     sumcheck_prove_dev(pw, 2, log_n, d_fields + fp.ch_rs, (ef2*)(stage + S_sc_r[4]),
-                       (ef2*)(stage + S_sc_f[4]), partials_for(log_n, 2), b);
+                       (ef2*)(stage + S_sc_f[4]), partials_for(log_n, 2), b, c->sumcheck_blocks);
     mark("E_rslink_sc_end", b);
   }
   // G: Stage A point reduction of a-bar (pcs/src/ligesis.rs:518-522)
@@ -1000,7 +1000,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
     d2d(ac, a_vec, n * sizeof(ef2), b);
     ef2* pa[2] = {ac, ga};
     sumcheck_prove_dev(pa, 2, log_n, d_fields + fp.ch_a, (ef2*)(stage + S_sc_r[6]),
-                       (ef2*)(stage + S_sc_f[6]), partials_for(log_n, 2), b);
+                       (ef2*)(stage + S_sc_f[6]), partials_for(log_n, 2), b, c->sumcheck_blocks);
     mark("G_a_batch_sc_end", b);
   }
   // H: Stage B reduction messages (pcs/src/basefold.rs:746-769).  With m = poly.fold(point[0..li])

@@ -268,6 +268,9 @@ struct lgs_ctx {
   unsigned tl_count = 0;  // marks recorded inside the prove's graph
   lgs::DevMem err;  // device error word of bounded-wait kernels (0 = ok)
   uint64_t wait_cycles = 0;  // budget of those waits in clock cycles (0 = default; lgs_set_wait_budget)
+  // Launch choices the autotuner sets (lgs_tune): 0 = the built-in default.
+  unsigned hash_ctas = 0;        // persistent CTAs of the subset-sum hash (default: one per SM)
+  unsigned sumcheck_blocks = 0;  // grid cap of the multi-CTA sumcheck passes (<= SC_MAX_BLOCKS)
   // Pinned host memory: every transfer of a call is asynchronous, so the host enqueues a whole
   // commit or prove without waiting for the device and synchronises once at the end.
   lgs::PinnedBuf up;    // the parameter blob of one prove (one host-to-device copy)

@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(SC_TAIL_THREADS)
     sc_tail_kernel(Polys<Fac<D, BIN>::S> P, unsigned len, int fold, const ef2* __restrict__ ch,
                    unsigned t0, unsigned k, ef2* __restrict__ rounds_out,
                    ef2* __restrict__ final_out, const ef2* __restrict__ partials,
-                   size_t stride) {
+                   size_t stride, unsigned cap) {
   constexpr int S = Fac<D, BIN>::S;
   constexpr unsigned NT = SC_TAIL_THREADS, NW = NT / 32;
   extern __shared__ __align__(16) unsigned char tail_smem_raw[];
@@ -334,8 +334,7 @@ __global__ void __launch_bounds__(SC_TAIL_THREADS)
   // the claim chain at the end reads them, after the hand-over barrier below.
   for (unsigned t = warp; t < t0; t += NW) {
     const size_t half = (size_t)1 << (k - 1 - t);
-    const unsigned nb =
-        (unsigned)min((size_t)SC_MAX_BLOCKS, (half + SC_THREADS - 1) / SC_THREADS);
+    const unsigned nb = (unsigned)min((size_t)cap, (half + SC_THREADS - 1) / SC_THREADS);
     ef2 sr[D + 1];
 #pragma unroll
     for (int q = 0; q <= D; ++q) sr[q] = ef_zero();
@@ -494,7 +493,8 @@ __global__ void __launch_bounds__(SC_TAIL_THREADS)
 
 template <int D, bool BIN>
 void sumcheck_run(ef2* const* polys, unsigned k, const ef2* ch, ef2* rounds_out, ef2* final_out,
-                  ef2* partials, cudaStream_t st) {
+                  ef2* partials, cudaStream_t st, unsigned max_blocks) {
+  const size_t cap = (max_blocks && max_blocks < SC_MAX_BLOCKS) ? max_blocks : SC_MAX_BLOCKS;
   constexpr int S = Fac<D, BIN>::S;
   Polys<S> P;
   for (int j = 0; j < S; ++j) P.p[j] = polys[j];
@@ -504,8 +504,8 @@ void sumcheck_run(ef2* const* polys, unsigned k, const ef2* ch, ef2* rounds_out,
   int fold = 0;
   while (t < k && len > Fac<D, BIN>::TAIL) {
     if (!(BIN && t == 0) && t + 1 < k && (len >> 1) > Fac<D, BIN>::TAIL) {  // two rounds
-      const unsigned nb_t = (unsigned)std::min<size_t>(SC_MAX_BLOCKS, cdiv(len >> 1, SC_THREADS));
-      const unsigned nb_t1 = (unsigned)std::min<size_t>(SC_MAX_BLOCKS, cdiv(len >> 2, SC_THREADS));
+      const unsigned nb_t = (unsigned)std::min<size_t>(cap, cdiv(len >> 1, SC_THREADS));
+      const unsigned nb_t1 = (unsigned)std::min<size_t>(cap, cdiv(len >> 2, SC_THREADS));
       sc_round2_kernel<D, BIN><<<nb_t1, SC_THREADS, 0, st>>>(
           P, len, fold, fold ? ch + (t - 1) : ch, ch + t, partials + (size_t)t * stride,
           partials + (size_t)(t + 1) * stride, nb_t);
@@ -516,7 +516,7 @@ void sumcheck_run(ef2* const* polys, unsigned k, const ef2* ch, ef2* rounds_out,
       continue;
     }
     size_t half = len >> 1;
-    unsigned blocks = (unsigned)std::min<size_t>(SC_MAX_BLOCKS, cdiv(half, SC_THREADS));
+    unsigned blocks = (unsigned)std::min<size_t>(cap, cdiv(half, SC_THREADS));
     if (BIN && t == 0)
       sc_bin_round0_kernel<<<blocks, SC_THREADS, 0, st>>>(P.p[0], P.p[S - 1], half, partials);
     else
@@ -534,7 +534,8 @@ void sumcheck_run(ef2* const* polys, unsigned k, const ef2* ch, ef2* rounds_out,
   LGS_CUDA(cudaFuncSetAttribute(sc_tail_kernel<D, BIN>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tail_smem));
   sc_tail_kernel<D, BIN><<<1, SC_TAIL_THREADS, tail_smem, st>>>(P, (unsigned)len, fold, ch, t, k,
-                                                        rounds_out, final_out, partials, stride);
+                                                        rounds_out, final_out, partials, stride,
+                                                                 (unsigned)cap);
   LGS_LAUNCH_CHECK();
 }
 }  // namespace
@@ -544,22 +545,22 @@ size_t sumcheck_partials_elems(unsigned k, unsigned d) {
 }
 
 void sumcheck_prove_dev(ef2* const* polys, unsigned d, unsigned k, const ef2* ch, ef2* rounds_out,
-                        ef2* final_out, ef2* partials, cudaStream_t st) {
+                        ef2* final_out, ef2* partials, cudaStream_t st, unsigned max_blocks) {
   if (k == 0) throw ShapeError("sumcheck: zero variables");
   if (k > 40) throw ShapeError("sumcheck: too many variables");
   switch (d) {
-    case 1: sumcheck_run<1, false>(polys, k, ch, rounds_out, final_out, partials, st); break;
-    case 2: sumcheck_run<2, false>(polys, k, ch, rounds_out, final_out, partials, st); break;
-    case 3: sumcheck_run<3, false>(polys, k, ch, rounds_out, final_out, partials, st); break;
+    case 1: sumcheck_run<1, false>(polys, k, ch, rounds_out, final_out, partials, st, max_blocks); break;
+    case 2: sumcheck_run<2, false>(polys, k, ch, rounds_out, final_out, partials, st, max_blocks); break;
+    case 3: sumcheck_run<3, false>(polys, k, ch, rounds_out, final_out, partials, st, max_blocks); break;
     default: throw ShapeError("sumcheck: 1 to 3 factors supported");
   }
 }
 
 void sumcheck_binary_dev(ef2* b, ef2* eq, unsigned k, const ef2* ch, ef2* rounds_out,
-                         ef2* final_out, ef2* partials, cudaStream_t st) {
+                         ef2* final_out, ef2* partials, cudaStream_t st, unsigned max_blocks) {
   if (k == 0 || k > 40) throw ShapeError("sumcheck: variable count out of range");
   ef2* polys[2] = {b, eq};
-  sumcheck_run<3, true>(polys, k, ch, rounds_out, final_out, partials, st);
+  sumcheck_run<3, true>(polys, k, ch, rounds_out, final_out, partials, st, max_blocks);
 }
 
 }  // namespace lgs

@@ -232,3 +232,26 @@ def test_commit_only_square_shapes_match_oracle(lgs, orc, log_m, log_n):
     o.fields, o.ints = np.ascontiguousarray(fields), np.ascontiguousarray(ints)
     with pytest.raises(L.ShapeError):
         L.Ligesis.prove(pk, data, z, o)
+
+
+def test_tuned_launch_choices_give_the_same_proof(lgs, orc):
+    """lgs_tune changes only how kernels are launched: fewer hash CTAs and a smaller sumcheck
+    grid give the oracle's commitment and proof; unknown names are refused."""
+    log_m, log_n = 5, 13
+    f, A, z, fields, ints = ligesis_inputs(log_m, log_n, seed=91)
+    ctx = L.Context(0)
+    pk, _ = L.Ligesis.setup_with_hash(log_m, log_n, L.SubsetSumHash(64 << log_m, a=A), ctx)
+    key = orc.Key(log_m, log_n, A)
+    want, _ = orc.prove(key, orc.Commitment(key, f), z, fields, ints)
+    for h, b in [(0, 0), (40, 148), (7, 16), (148, 296)]:
+        ctx.tune(hash_ctas=h, sumcheck_blocks=b)
+        assert ctx.tuning() == {"hash_ctas": h, "sumcheck_blocks": b}
+        for _ in range(3):  # eager, captured, replayed
+            commit, data = L.Ligesis.commit(pk, L.MlPoly(f))
+            o = L.RandomOracle(0, length=8)
+            o.fields, o.ints = np.ascontiguousarray(fields), np.ascontiguousarray(ints)
+            assert L.Ligesis.prove(pk, data, z, o).data == want, (h, b)
+    with pytest.raises(L.LgsError, match="unknown parameter"):
+        ctx.tune(nonsense=1)
+    with pytest.raises(L.LgsError):
+        ctx.tune(sumcheck_blocks=297)
