@@ -321,7 +321,8 @@ def run_ours(args) -> None:
     def step_device():
         oracle.restart()
         t0 = time.perf_counter()
-        commit, data = L.Ligesis.commit_device(pk, f_dev.data_ptr(), f.size)
+        # f is already in HBM and stays there: the commitment reads it in place (no copy)
+        commit, data = L.Ligesis.commit_device(pk, f_dev.data_ptr(), f.size, lend=True)
         t1 = time.perf_counter()
         proof = L.Ligesis.prove(pk, data, z, oracle)
         t2 = time.perf_counter()

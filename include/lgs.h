@@ -66,8 +66,11 @@ lgs_status lgs_commit_device(lgs_ctx* ctx, const lgs_pk* pk, const uint64_t* f_d
 /* Ligesis::commit without waiting for the device: the work is enqueued on the context's stream
  * and *out is at once usable by lgs_prove on the same context (stream order), so the prove's
  * host-side planning overlaps the commit's device work.  f is host memory (f_on_device = 0; read
- * before the call returns) or device memory of the context's device (f_on_device = 1; must stay
- * unchanged until the commit is done).  lgs_commit_root waits for the commit and returns the
+ * before the call returns) or device memory of the context's device (f_on_device = 1; copied,
+ * must stay unchanged until the commit is done; f_on_device = 2: lent, not copied: the
+ * commitment reads the caller's buffer until lgs_commit_data_free, so it must stay allocated
+ * and unchanged until then, as the reference's commit owns f).  lgs_commit_root waits for the
+ * commit and returns the
  * LigesisCommit root (and reports a failed bounded device wait).  The same computation as
  * lgs_commit, so the root and every later proof are identical. */
 lgs_status lgs_commit_async(lgs_ctx* ctx, const lgs_pk* pk, const uint64_t* f, size_t len,
@@ -258,6 +261,8 @@ lgs_status lgs_profile_names(lgs_ctx* ctx, char* buf, size_t cap, size_t* needed
  *   "hash_ctas"        persistent CTAs of the subset-sum hash (default one per SM); fewer leave
  *                      SMs to the prove that runs beside the commit's hash
  *   "sumcheck_blocks"  grid cap of the multi-CTA sumcheck passes (at most 296)
+ *   "hash_groups"      commits of host polynomials: digest the codeword in this many row
+ *                      groups (1..8) as their RS encoding finishes, under the upload
  * Results do not depend on them.  Unknown names: LGS_ERR_BAD_ARG. */
 lgs_status lgs_tune(lgs_ctx* ctx, const char* name, uint64_t value);
 lgs_status lgs_tune_get(lgs_ctx* ctx, const char* name, uint64_t* value);

@@ -197,7 +197,7 @@ class Context:
 
     def tuning(self, *names: str) -> dict:
         out = {}
-        for name in names or ("hash_ctas", "sumcheck_blocks"):
+        for name in names or ("hash_ctas", "sumcheck_blocks", "hash_groups"):
             v = C.c_uint64()
             check(self._lib.lgs_tune_get(self.handle, name.encode(), C.byref(v)))
             out[name] = int(v.value)

@@ -1,18 +1,21 @@
 """Autotuner for the launch choices of the commit + prove step (lgs_tune), with a JSON cache.
 
 The step runs the commit's subset-sum hash (a persistent tensor-core kernel, one CTA per SM by
-default) beside the prove's DAG of sumcheck, eq-table and Basefold kernels, so two choices trade
-against each other:
+default) beside the prove's DAG of sumcheck, eq-table and Basefold kernels, so these choices
+trade against each other:
 
 * ``hash_ctas``: how many SMs the hash occupies; fewer leave SMs to the prove's latency-bound
   branches while the hash runs.
 * ``sumcheck_blocks``: the grid cap of the multi-CTA sumcheck passes.
+* ``hash_groups``: for a polynomial uploaded from host memory, in how many row groups the digest
+  is built as the groups' RS encodings finish (under the rest of the upload).
 
-``tune`` times candidate settings on the device (CUDA events on the context's stream, f already
-in HBM, the same step the bench times), keeps the fastest, and records it per GPU name and
-shape in the cache (``tuning.json`` beside this file unless a path is given).  ``apply`` sets a
-context from the cache.  Every setting computes the same commitment and proof bytes; ``tune``
-checks that too.
+``tune`` times candidate settings on the device (CUDA events on the context's stream): the first
+two with f already in HBM (the step the bench's ``value`` times), ``hash_groups`` with f in
+page-locked host memory (the step ``e2e`` times).  It keeps the fastest and records it per GPU
+name and shape in the cache (``tuning.json`` beside this file unless a path is given).
+``apply`` sets a context from the cache.  Every setting computes the same commitment and proof
+bytes; ``tune`` checks that too.
 """
 from __future__ import annotations
 
@@ -23,7 +26,7 @@ from pathlib import Path
 import numpy as np
 
 CACHE = Path(__file__).with_name("tuning.json")
-PARAMS = ("hash_ctas", "sumcheck_blocks")
+PARAMS = ("hash_ctas", "sumcheck_blocks", "hash_groups")
 
 
 def _device_name(device: int = 0) -> str:
@@ -55,10 +58,11 @@ def apply(ctx, log_m: int, log_n: int, path: Path | None = None) -> dict | None:
 
 
 def tune(log_m: int, log_n: int, steps: int = 10, warmup: int = 3, device: int = 0,
-         hash_ctas=None, sumcheck_blocks=None, path: Path | None = None,
+         hash_ctas=None, sumcheck_blocks=None, hash_groups=None, path: Path | None = None,
          save: bool = True) -> dict:
     """Coordinate search: hash_ctas first (sumcheck_blocks at its default), then
-    sumcheck_blocks at the best hash_ctas.  Returns the cache entry it wrote."""
+    sumcheck_blocks at the best hash_ctas, then hash_groups on the host-input step.  Returns the
+    cache entry it wrote."""
     import torch
 
     import ligesis_b200 as L
@@ -68,6 +72,7 @@ def tune(log_m: int, log_n: int, steps: int = 10, warmup: int = 3, device: int =
     sms = torch.cuda.get_device_properties(device).multi_processor_count
     hash_ctas = list(hash_ctas or [sms - d for d in (0, 8, 16, 24, 32, 40, 48, 56)])
     sumcheck_blocks = list(sumcheck_blocks or [296, 222, 148, 74])
+    hash_groups = list(hash_groups or [1, 2, 4, 8])
     ctx = L.Context(device)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=torch.device("cuda", device))
     mu = log_m + log_n
@@ -79,10 +84,15 @@ def tune(log_m: int, log_n: int, steps: int = 10, warmup: int = 3, device: int =
     oracle.fields, oracle.ints = g.ext_elements(4096), g.ints(4096)
     pk, _ = L.Ligesis.setup_with_hash(log_m, log_n, L.SubsetSumHash(64 << log_m, a=A), ctx)
     f_dev = torch.from_numpy(f.view(np.int64)).to(f"cuda:{device}")
+    f_pin = torch.from_numpy(f.view(np.int64)).pin_memory().numpy().view(np.uint64)
+    host_input = False
 
     def step():
         oracle.restart()
-        commit, data = L.Ligesis.commit_device(pk, f_dev.data_ptr(), f.size)
+        if host_input:
+            commit, data = L.Ligesis.commit(pk, L.MlPoly(f_pin))
+        else:
+            commit, data = L.Ligesis.commit_device(pk, f_dev.data_ptr(), f.size, lend=True)
         proof = L.Ligesis.prove(pk, data, z, oracle)
         return commit, proof
 
@@ -127,9 +137,20 @@ def tune(log_m: int, log_n: int, steps: int = 10, warmup: int = 3, device: int =
         trials.append({**s, "ms": round(ms, 4)})
         if ms < best_ms:
             best, best_ms = s, ms
-    ctx.tune(hash_ctas=0, sumcheck_blocks=0)
+    host_input = True
+    best_e2e, e2e_trials = None, []
+    for gcount in hash_groups:
+        s = {**best, "hash_groups": gcount}
+        ms = measure(s)
+        e2e_trials.append({**s, "ms": round(ms, 4)})
+        if best_e2e is None or ms < best_e2e[1]:
+            best_e2e = (gcount, ms)
+    best["hash_groups"] = best_e2e[0]
+    ctx.tune(hash_ctas=0, sumcheck_blocks=0, hash_groups=0)
     entry = {**best, "ms": round(best_ms, 4), "default_ms": trials[0]["ms"],
-             "steps": steps, "when": time.strftime("%Y-%m-%d"), "trials": trials}
+             "e2e_ms": round(best_e2e[1], 4), "e2e_one_group_ms": e2e_trials[0]["ms"],
+             "steps": steps, "when": time.strftime("%Y-%m-%d"), "trials": trials,
+             "e2e_trials": e2e_trials}
     if save:
         cache = load(path)
         cache.setdefault(_device_name(device), {})[shape_key(log_m, log_n)] = entry

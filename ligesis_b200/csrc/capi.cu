@@ -144,6 +144,8 @@ void lgs_ctx_destroy(lgs_ctx* ctx) {
     if (ctx->ring_ev[i]) cudaEventDestroy(ctx->ring_ev[i]);
   for (int i = 0; i < lgs_ctx::ROW_BLOCKS; ++i)
     if (ctx->ev_rows[i]) cudaEventDestroy(ctx->ev_rows[i]);
+  for (int i = 0; i < lgs_ctx::ROW_BLOCKS; ++i)
+    if (ctx->ev_rs[i]) cudaEventDestroy(ctx->ev_rs[i]);
   for (int i = 0; i < lgs_ctx::TL_MAX; ++i)
     if (ctx->tl_ev[i]) cudaEventDestroy(ctx->tl_ev[i]);
   for (auto& g : ctx->graphs)
@@ -253,8 +255,10 @@ lgs_status lgs_commit_async(lgs_ctx* ctx, const lgs_pk* pk, const uint64_t* f, s
     need(ctx && pk && f && out, "lgs_commit_async: null argument");
     need(len == pk->shape.m() * pk->shape.n(),
          "lgs_commit_async: f must hold 2^(log_m+log_n) values");
+    need(f_on_device >= 0 && f_on_device <= 2, "lgs_commit_async: f_on_device must be 0, 1 or 2");
     CtxDevice dg(ctx);
     auto* cd = new lgs_commit_data;
+    if (f_on_device == 2) cd->f_lent = f;
     try {
       commit_dev(ctx, pk, f, f_on_device != 0, cd, false);
     } catch (...) {
@@ -545,6 +549,9 @@ lgs_status lgs_tune(lgs_ctx* ctx, const char* name, uint64_t value) {
     if (n == "hash_ctas") {
       need(value <= 4096, "lgs_tune: hash_ctas above 4096");
       ctx->hash_ctas = (unsigned)value;
+    } else if (n == "hash_groups") {
+      need(value <= lgs_ctx::ROW_BLOCKS, "lgs_tune: hash_groups above the upload's row blocks");
+      ctx->hash_groups = (unsigned)value;
     } else if (n == "sumcheck_blocks") {
       need(value <= SC_MAX_BLOCKS, "lgs_tune: sumcheck_blocks above the partial-sum slots");
       ctx->sumcheck_blocks = (unsigned)value;
@@ -566,6 +573,7 @@ lgs_status lgs_tune_get(lgs_ctx* ctx, const char* name, uint64_t* value) {
     const std::string n(name);
     if (n == "hash_ctas") *value = ctx->hash_ctas;
     else if (n == "sumcheck_blocks") *value = ctx->sumcheck_blocks;
+    else if (n == "hash_groups") *value = ctx->hash_groups;
     else throw std::invalid_argument("lgs_tune_get: unknown parameter " + n);
   });
 }

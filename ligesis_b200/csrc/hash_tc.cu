@@ -152,7 +152,8 @@ __device__ __forceinline__ uint32_t nib_expand(uint32_t nib) {
 __global__ void __launch_bounds__(NTHREADS, 1)
     hash_tc_kernel(const __grid_constant__ CUtensorMap tmap_a, const u64* __restrict__ cw,
                    u64* __restrict__ H, u32* __restrict__ leaves, unsigned m, size_t two_n,
-                   int* __restrict__ err, long long budget) {
+                   int* __restrict__ err, long long budget, unsigned c0, unsigned nck,
+                   int mode) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint32_t* Ss = (uint32_t*)(smem + TC_STAGES * STAGE_BYTES);
@@ -164,7 +165,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   const uint32_t drain = smem_u32(&bars[2 * TC_STAGES + 2]);
   const uint32_t tma0 = smem_u32(&bars[2 * TC_STAGES + 3]);
   const unsigned tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const unsigned nchunks = (m + 1) / 2;
+  // K chunks (pairs of codeword rows) c0 .. c0 + nck - 1 of this launch; mode bit 0: add the
+  // partial digest to H (else write it), bit 1: hash the leaves of the finished H.
   const unsigned ntiles = (unsigned)(two_n / TC_N);
   const unsigned my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   __shared__ volatile int s_fail;
@@ -192,14 +194,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_holder;
-  const unsigned nfill = my_tiles * nchunks;
+  const unsigned nfill = my_tiles * nck;
 
   if (warp == 0) {
     // ---- TMA producer: A-limb tiles ----
     if (lane == 0) {
       unsigned issued = 0;
       for (unsigned f = 0; f < nfill; ++f) {
-        const unsigned s = f % TC_STAGES, c = f % nchunks;
+        const unsigned s = f % TC_STAGES, c = c0 + f % nck;
         if (f >= TC_STAGES &&
             !mbar_wait(empty0 + 8 * s, ((f / TC_STAGES) - 1) & 1, &s_fail, budget)) {
           if (!s_fail) flag_failure(&s_fail, err, 1);
@@ -235,7 +237,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         }
-        for (unsigned c = 0; c < nchunks; ++c, ++f) {
+        for (unsigned c = 0; c < nck; ++c, ++f) {
           const unsigned s = f % TC_STAGES;
           if (!mbar_wait(tma0 + 8 * s, (f / TC_STAGES) & 1, &s_fail, budget) ||
               !mbar_wait(full0 + 8 * s, (f / TC_STAGES) & 1, &s_fail, budget)) {
@@ -266,7 +268,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     const unsigned pt = tid - 64;
     auto load_fill = [&](unsigned f, u64 (&w)[4]) {
       if (f >= nfill) return;
-      const unsigned tl = f / nchunks, c = f % nchunks;
+      const unsigned tl = f / nck, c = c0 + f % nck;
       const size_t j0 = (size_t)(blockIdx.x + tl * gridDim.x) * TC_N;
       const bool two = 2 * c + 1 < m;
 #pragma unroll
@@ -351,7 +353,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           const u64 b = (u64)hi4.x + ((u64)hi4.y << 8) + ((u64)hi4.z << 16) + ((u64)hi4.w << 24);
           const u64 lo = a + (b << 32);
           const u64 hi = (b >> 32) + (lo < a ? 1 : 0);
-          H[(size_t)r * two_n + j0 + EPI_COLS * q + col] = gl_reduce(lo, hi);
+          u64* hp = H + (size_t)r * two_n + j0 + EPI_COLS * q + col;
+          const u64 v = gl_reduce(lo, hi);
+          *hp = (mode & 1) ? gl_add(__ldcg(hp), v) : v;
         }
       }
       // accumulators drained: the MMAs of the next tile may start
@@ -360,6 +364,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       __threadfence_block();
       epi_sync();
       // leaf hash of each 256-byte column (C = 32 canonical u64, little-endian), from L2
+      if (!(mode & 2)) continue;  // a partial digest: no leaves yet
 #pragma unroll 1
       for (unsigned col = et; col < (unsigned)TC_N; col += NEPI) {
         const u64* hc = H + j0 + col;
@@ -518,9 +523,12 @@ size_t tensor_map_bytes() { return sizeof(CUtensorMap); }
 
 void subset_sum_hash_tc(const void* tmap, const u64* cw, u64* H, u32* leaves, unsigned m,
                         size_t two_n, int* err, cudaStream_t st, uint64_t wait_cycles,
-                        unsigned max_ctas) {
+                        unsigned max_ctas, unsigned row0, unsigned rows, int mode) {
   if (two_n % TC_N) throw ShapeError("hash: 2n must be a multiple of 256");
   if (m == 0 || m > 8192) throw ShapeError("hash: 1 <= m <= 8192");
+  if (rows == 0) rows = m - row0;
+  if (row0 % 2 || (rows % 2 && row0 + rows != m) || row0 + rows > m || mode < 0 || mode > 3)
+    throw ShapeError("hash: row range must start and end on chunks of two rows");
   LGS_CUDA(cudaFuncSetAttribute(hash_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 SMEM_BYTES));
   int dev = 0, sms = 0;
@@ -533,7 +541,8 @@ void subset_sum_hash_tc(const void* tmap, const u64* cw, u64* H, u32* leaves, un
   const long long budget =
       wait_cycles ? (long long)std::min<uint64_t>(wait_cycles, (uint64_t)WAIT_CYCLES) : WAIT_CYCLES;
   hash_tc_kernel<<<grid, NTHREADS, SMEM_BYTES, st>>>(*(const CUtensorMap*)tmap, cw, H, leaves, m,
-                                                     two_n, err, budget);
+                                                     two_n, err, budget, row0 / 2,
+                                                     (rows + 1) / 2, mode);
   LGS_LAUNCH_CHECK();
 }
 

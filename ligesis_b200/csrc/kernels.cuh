@@ -35,9 +35,13 @@ void make_alimb_tmap(const uint8_t* alimb, size_t W, void* tmap_out);
 size_t tensor_map_bytes();
 // wait_cycles: clock budget of the kernel's bounded waits (0 = the default, about 2 s).
 // max_ctas: persistent CTAs (0 = one per SM); fewer leave SMs to concurrent work.
+// Rows [row0, row0 + rows) of the codeword only (rows = 0: to the end; both even except at the
+// end): H is linear in the rows, so mode 0 writes the rows' partial digest, mode 1 adds it to H,
+// and modes 2 and 3 (write, add) also hash the finished H's leaves.
 void subset_sum_hash_tc(const void* tmap, const u64* cw, u64* H, u32* leaves, unsigned m,
                         size_t two_n, int* err, cudaStream_t st, uint64_t wait_cycles = 0,
-                        unsigned max_ctas = 0);
+                        unsigned max_ctas = 0, unsigned row0 = 0, unsigned rows = 0,
+                        int mode = 2);
 // Dense tcgen05 kind::i8 throughput (TOP/s) of back-to-back M128 N256 K32 MMAs on every SM.
 double i8_tensor_peak_tops(unsigned iters, int* err, cudaStream_t st);
 

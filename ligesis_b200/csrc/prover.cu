@@ -279,8 +279,10 @@ void ctx_init(lgs_ctx* c, int device) {
     LGS_CUDA(cudaEventCreateWithFlags(&c->ev_done[i], cudaEventDisableTiming));
   }
   LGS_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
-  for (int i = 0; i < lgs_ctx::ROW_BLOCKS; ++i)
+  for (int i = 0; i < lgs_ctx::ROW_BLOCKS; ++i) {
     LGS_CUDA(cudaEventCreateWithFlags(&c->ev_rows[i], cudaEventDisableTiming));
+    LGS_CUDA(cudaEventCreateWithFlags(&c->ev_rs[i], cudaEventDisableTiming));
+  }
   for (int i = 0; i < lgs_ctx::RING; ++i)
     LGS_CUDA(cudaEventCreateWithFlags(&c->ring_ev[i], cudaEventDisableTiming));
   c->tail.reserve(64);
@@ -343,7 +345,7 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
   HostClock hc(c->prof);
   cd->shape = s;
   c->arena.begin();
-  cd->f.acquire(m * n * 8, c->device, c->st);
+  if (!cd->f_lent) cd->f.acquire(m * n * 8, c->device, c->st);
   cd->cw.acquire(m * two_n * 8, c->device, c->st);
   cd->H.acquire(DIGEST_ROWS * two_n * 8, c->device, c->st);
   cd->nodes.acquire((2 * two_n - 1) * 32, c->device, c->st);
@@ -351,7 +353,8 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
   u64* scr = logN > 12 ? c->arena.get<u64>(m * two_n) : nullptr;
   const bool rows_path = rs_dft_supported(logN, n);
   hc.lap("host_commit_alloc");
-  if (!f_on_device && rows_path && m >= 2) {
+  bool hashed = false;  // the digest was built row group by row group under the upload
+  if (!f_on_device && !cd->f_lent && rows_path && m >= 2) {
     // Host rows: the upload of row block b + 1 overlaps the RS encoding of block b.  Page-locked
     // f is copied by the DMA engine on a side stream; pageable f goes through the pinned ring on
     // the context stream, where the host-side staging of the next block is the slower part.
@@ -364,6 +367,12 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
       LGS_CUDA(cudaEventRecord(c->ev_fork, c->st));  // cd->f exists on the context stream
       LGS_CUDA(cudaStreamWaitEvent(cp, c->ev_fork, 0));
     }
+    // H is linear in the rows: with hash_groups = G > 1 the hash stream digests each group of
+    // nb / G row blocks as soon as their RS encoding is done (write, then add; the last group
+    // also hashes the leaves), so most of the hash runs under the rest of the upload.
+    unsigned groups = c->hash_groups ? std::min(c->hash_groups, nb) : 1;
+    if (rows * (nb / groups) % 2) groups = 1;  // a group must hold whole pairs of rows
+    const unsigned per = nb / groups;
     for (unsigned b = 0; b < nb; ++b) {
       const size_t off = (size_t)b * rows * n;
       if (pinned) {
@@ -375,9 +384,20 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
       }
       rs_dft_rows(cd->f.as<u64>() + off, n, n, cd->cw.as<u64>() + (size_t)b * rows * two_n,
                   two_n, logN, rows, scr + (size_t)b * rows * two_n, c->rs_tw.as<u64>(), c->st);
+      if (groups > 1 && (b + 1) % per == 0) {
+        const unsigned g = b / per;
+        LGS_CUDA(cudaEventRecord(c->ev_rs[b], c->st));
+        LGS_CUDA(cudaStreamWaitEvent(c->hs, c->ev_rs[b], 0));
+        StageTimer th(c->prof, c->hs, "subset_sum_hash_rows");
+        subset_sum_hash_tc(pk->tmap, cd->cw.as<u64>(), cd->H.as<u64>(), cd->nodes.as<u32>(),
+                           (unsigned)m, two_n, c->err.as<int>(), c->hs, c->wait_cycles,
+                           c->hash_ctas, (unsigned)(g * per * rows), (unsigned)(per * rows),
+                           g == 0 ? 0 : (g + 1 == groups ? 3 : 1));
+        hashed = true;
+      }
     }
   } else {
-    {
+    if (!cd->f_lent) {
       StageTimer t(c->prof, c->st, "commit_upload");
       if (f_on_device)
         d2d(cd->f.p, f, m * n * 8, c->st);
@@ -386,18 +406,17 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
     }
     StageTimer t(c->prof, c->st, "rs_encode");
     if (rows_path)
-      rs_dft_rows(cd->f.as<u64>(), n, n, cd->cw.as<u64>(), two_n, logN, m, scr,
-                  c->rs_tw.as<u64>(), c->st);
+      rs_dft_rows(cd->fdev(), n, n, cd->cw.as<u64>(), two_n, logN, m, scr, c->rs_tw.as<u64>(),
+                  c->st);
     else
-      ntt_batch(cd->f.as<u64>(), n, n, cd->cw.as<u64>(), two_n, logN, m, scr, c->tw.as<u64>(),
-                c->st);
+      ntt_batch(cd->fdev(), n, n, cd->cw.as<u64>(), two_n, logN, m, scr, c->tw.as<u64>(), c->st);
   }
   hc.lap("host_commit_rs");
   // The hash and the tree need only the codeword: they run on the hash stream, and a prove
   // enqueued next on the context stream runs beside them (its gather waits for cd->done).
   LGS_CUDA(cudaEventRecord(c->ev_cw, c->st));
   LGS_CUDA(cudaStreamWaitEvent(c->hs, c->ev_cw, 0));
-  {
+  if (!hashed) {
     StageTimer t(c->prof, c->hs, "subset_sum_hash");  // H and its Merkle leaf hashes
     subset_sum_hash_tc(pk->tmap, cd->cw.as<u64>(), cd->H.as<u64>(), cd->nodes.as<u32>(),
                        (unsigned)m, two_n, c->err.as<int>(), c->hs, c->wait_cycles, c->hash_ctas);
@@ -789,7 +808,7 @@ void prove_dev(lgs_ctx* c, const lgs_pk* pk, const lgs_commit_data* cd, const u6
   std::memcpy(h_up + U_idx, idx.data(), S * 8);
   const u64* const* d_ptrs = (const u64* const*)(d_up + U_ptrs);
   {
-    const u64* pt[PT_N] = {cd->f.as<u64>(), cd->cw.as<u64>(), pk->A.as<u64>(), bi,
+    const u64* pt[PT_N] = {cd->fdev(), cd->cw.as<u64>(), pk->A.as<u64>(), bi,
                            (const u64*)a_vec};
     std::memcpy(h_up + U_ptrs, pt, sizeof(pt));
   }

@@ -255,6 +255,7 @@ struct lgs_ctx {
   cudaEvent_t ev_fork = nullptr;
   static constexpr int ROW_BLOCKS = 8;  // row blocks of a host upload pipelined with RS encoding
   cudaEvent_t ev_rows[ROW_BLOCKS] = {};
+  cudaEvent_t ev_rs[ROW_BLOCKS] = {};  // RS encoding of row block b done (host-rows commit)
   lgs::DevMem tw;
   lgs::DevMem rs_tw;  // twiddles of the row RS encoding (rs_dft.cu)
   lgs::Arena arena;
@@ -271,6 +272,7 @@ struct lgs_ctx {
   // Launch choices the autotuner sets (lgs_tune): 0 = the built-in default.
   unsigned hash_ctas = 0;        // persistent CTAs of the subset-sum hash (default: one per SM)
   unsigned sumcheck_blocks = 0;  // grid cap of the multi-CTA sumcheck passes (<= SC_MAX_BLOCKS)
+  unsigned hash_groups = 0;      // host-rows commit: hash launches over row groups (0: default)
   // Pinned host memory: every transfer of a call is asynchronous, so the host enqueues a whole
   // commit or prove without waiting for the device and synchronises once at the end.
   lgs::PinnedBuf up;    // the parameter blob of one prove (one host-to-device copy)
@@ -297,10 +299,12 @@ struct lgs_pk {
 };
 
 struct lgs_commit_data {
+  const uint64_t* fdev() const { return f_lent ? f_lent : f.as<uint64_t>(); }
   lgs::Shape shape;
   cudaEvent_t done = nullptr;  // recorded after the commit's last copy (asynchronous commits)
   bool root_ready = false;
-  lgs::RecycledBuf f;      // m x n
+  lgs::RecycledBuf f;      // m x n (unused when the caller lends its device copy)
+  const uint64_t* f_lent = nullptr;  // the caller's device f, kept alive and unchanged by it
   lgs::RecycledBuf cw;     // m x 2n RS codeword F' (its bits are B)
   lgs::RecycledBuf H;      // 32 x 2n digest
   lgs::RecycledBuf nodes;  // column Merkle tree over H

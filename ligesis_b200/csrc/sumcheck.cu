@@ -19,7 +19,6 @@ namespace lgs {
 
 namespace {
 constexpr unsigned SC_THREADS = 256;
-constexpr unsigned SC_TAIL_THREADS = 128;
 
 __device__ __forceinline__ ef2 shfl_xor_ef(ef2 v, int m) {
   ef2 r;
@@ -150,42 +149,111 @@ struct Polys {
   ef2* p[S];
 };
 
-// One round over `half` pairs.  If `fold`, the vectors still hold 4*half entries from the
-// previous round and are folded with r first (results written back to [0, 2*half)).
+// ---- cooperative rounds: G lanes per pair ----------------------------------------------------
+// A pair's work is split over a group of G = 4 lanes (8 for three stored factors): lane r < 2S
+// loads (and folds with the previous challenge) one of the 2S values lo_j, hi_j, the group
+// exchanges them with shuffles, and lane r computes the round polynomial at one point q.  Each
+// lane's chain is then one fold and one product (two F_p2 products) instead of all of them:
+// used where there are too few pairs to fill the GPU, so a round's time is its chain's latency.
+constexpr unsigned SC_COOP_THREADS = 1024;
+
 template <int D, bool BIN>
-__global__ void __launch_bounds__(SC_THREADS)
-    sc_round_kernel(Polys<Fac<D, BIN>::S> P, size_t half, int fold, const ef2* __restrict__ rptr,
-                    ef2* __restrict__ partial) {
-  const bool skip1 = fold != 0;  // every round but the first: g(1) comes from the claim
+struct Coop {
+  static constexpr int S = Fac<D, BIN>::S;
+  static constexpr unsigned G = S <= 2 ? 4 : 8;
+};
+
+// The point lane role r evaluates (-1: none): 0..D, or 0, 2, 3 (up to D) once g(1) comes from
+// the claim.
+template <int D>
+__device__ __forceinline__ int coop_q(unsigned r, bool skip1) {
+  if (skip1) return r < (unsigned)D ? (r == 0 ? 0 : (int)r + 1) : -1;
+  return r <= (unsigned)D ? (int)r : -1;
+}
+
+// prod_j (lo_j + q (hi_j - lo_j)), with b (b - 1) for the first factor of the binary check.
+template <int D, bool BIN>
+__device__ __noinline__ ef2 pair_point(FacVals<Fac<D, BIN>::S> lo, FacVals<Fac<D, BIN>::S> hi,
+                                       int q) {
   constexpr int S = Fac<D, BIN>::S;
-  __shared__ ef2 red[(D + 1) * 32];
-  ef2 s[D + 1];
+  ef2 v[S];
 #pragma unroll
-  for (int q = 0; q <= D; ++q) s[q] = ef_zero();
-  const ef2 r = fold ? *rptr : ef_zero();
-  const size_t len = 2 * half;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < half;
-       i += (size_t)gridDim.x * blockDim.x) {
-    ef2 lo[S], hi[S];
-#pragma unroll
-    for (int j = 0; j < S; ++j) {
-      ef2* p = P.p[j];
-      if (fold) {
-        lo[j] = ef_lerp(p[i], p[i + len], r);
-        hi[j] = ef_lerp(p[i + half], p[i + half + len], r);
-        p[i] = lo[j];
-        p[i + half] = hi[j];
-      } else {
-        lo[j] = p[i];
-        hi[j] = p[i + half];
-      }
-    }
-    add_pair<D, BIN>(lo, hi, s, skip1);
+  for (int j = 0; j < S; ++j) {
+    const ef2 d = ef_sub(hi.v[j], lo.v[j]);
+    v[j] = lo.v[j];
+    for (int c = 0; c < q; ++c) v[j] = ef_add(v[j], d);
   }
-  block_reduce<D>(s, red);
-  if (threadIdx.x == 0)
+  ef2 p = BIN ? ef_mul(v[0], ef_sub(v[0], ef_one())) : v[0];
 #pragma unroll
-    for (int q = 0; q <= D; ++q) partial[(size_t)blockIdx.x * (D + 1) + q] = s[q];
+  for (int j = 1; j < S; ++j) p = ef_mul(p, v[j]);
+  return p;
+}
+
+template <int S>
+__device__ __forceinline__ ef2* factor(const Polys<S>& P, unsigned j) {
+  ef2* p = P.p[0];
+#pragma unroll
+  for (int x = 1; x < S; ++x)
+    if (j == (unsigned)x) p = P.p[x];
+  return p;
+}
+
+// Out-of-line F_p2 products for the tail's one-time code (its rounds, the claim chain): the tail
+// runs each instruction about once, so instruction fetch, not issue, bounds it, and one shared
+// copy of the product is far less code than one inlined copy per use.
+__device__ __noinline__ ef2 ef_mul_ol(ef2 a, ef2 b) { return ef_mul(a, b); }
+__device__ __noinline__ ef2 ef_lerp_ol(ef2 a, ef2 b, ef2 r) { return ef_lerp(a, b, r); }
+
+__device__ __forceinline__ ef2 shfl_ef(ef2 v, unsigned src) {
+  return ef_make(__shfl_sync(0xffffffffu, v.c0, src), __shfl_sync(0xffffffffu, v.c1, src));
+}
+
+// One round over `half` pairs, a group of G lanes per pair.  If `fold`, the vectors still hold
+// 4 half entries and are folded with *rptr first (results written back to [0, 2 half)); each
+// position is read and written by one lane only.  The CTA's sums go to partial[blockIdx.x].
+template <int D, bool BIN>
+__global__ void __launch_bounds__(SC_COOP_THREADS)
+    sc_coop_kernel(Polys<Fac<D, BIN>::S> P, size_t half, int fold, const ef2* __restrict__ rptr,
+                   ef2* __restrict__ partial) {
+  constexpr int S = Fac<D, BIN>::S;
+  constexpr unsigned G = Coop<D, BIN>::G, NWARP = SC_COOP_THREADS / 32;
+  __shared__ ef2 red[NWARP][G];
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned r = lane & (G - 1), gb = lane & ~(G - 1);
+  const bool skip1 = fold != 0;
+  const int q = coop_q<D>(r, skip1);
+  const ef2 rp = fold ? *rptr : ef_zero();
+  const size_t len = 2 * half, gpb = SC_COOP_THREADS / G;
+  const size_t stride = (size_t)gridDim.x * gpb;
+  ef2* const mine = factor<S>(P, r >> 1);
+  ef2 acc = ef_zero();
+  // warp-uniform loop: every lane takes part in the shuffles, idle groups with act = false
+  for (size_t w0 = (size_t)blockIdx.x * gpb + warp * (32 / G); w0 < half; w0 += stride) {
+    const size_t i = w0 + lane / G;
+    const bool act = i < half;
+    ef2 val = ef_zero();
+    if (act && r < 2 * S) {
+      const size_t x = i + (r & 1) * half;
+      val = fold ? ef_lerp(mine[x], mine[x + len], rp) : mine[x];
+      if (fold) mine[x] = val;
+    }
+    FacVals<S> lo, hi;
+#pragma unroll
+    for (int j = 0; j < S; ++j) lo.v[j] = shfl_ef(val, gb + 2 * j), hi.v[j] = shfl_ef(val, gb + 2 * j + 1);
+    if (act && q >= 0) acc = ef_add(acc, pair_point<D, BIN>(lo, hi, q));
+  }
+#pragma unroll
+  for (unsigned m = G; m < 32; m <<= 1) acc = ef_add(acc, shfl_xor_ef(acc, m));
+  if (lane < G) red[warp][lane] = acc;
+  __syncthreads();
+  if (threadIdx.x < G) {
+    ef2 sum = ef_zero();
+#pragma unroll 4
+    for (unsigned w = 0; w < NWARP; ++w) sum = ef_add(sum, red[w][threadIdx.x]);
+    const int qq = coop_q<D>(threadIdx.x, skip1);
+    if (qq >= 0) partial[(size_t)blockIdx.x * (D + 1) + qq] = sum;
+    if (skip1 && threadIdx.x == 0) partial[(size_t)blockIdx.x * (D + 1) + 1] = ef_zero();
+  }
 }
 
 // Rounds t and t+1 in one pass.  On entry the vectors hold 2*len entries still to be folded with
@@ -299,24 +367,42 @@ __device__ void interp_weights(ef2 r, ef2 (&L)[D + 1]) {
   }
 }
 
-// Remaining rounds t0..k-1 in one CTA of SC_TAIL_THREADS (NT) threads.  On entry the vectors hold
-// `len` entries (len <= TAIL); if `fold`, they hold 2*len entries still to be folded with
-// challenge t0 - 1.  The high variable is bound first (pairs i, i + half), so a thread that owns
-// the indices congruent to its id modulo NT owns both members of every pair while half >= NT:
-//   phase A  rounds with half >= NT: each thread folds its own slice of shared memory, no
-//            barrier (at most three rounds: TAIL = 8 NT);
-//   hand-over one barrier; warp 0 continues alone;
-//   phase B  rounds with 32 <= half < NT: the same with lane l owning l mod 32;
-//   phase C  half < 32: one entry per lane, the partner's through a shuffle.
-// No round waits for a reduction: each round's sums go to shared memory per warp (phase A) or
-// per lane (B, C) and are added up once at the end.  g(1) of every round after the first is
-// filled in along the claim chain (see the chain below).
+template <int D>
+__device__ void interp_weights_ol(ef2 r, ef2 (&L)[D + 1]) {
+  const u64 inv2 = 0x7FFFFFFF80000001ULL, inv6 = 0xD555555480000001ULL;
+  const ef2 r1 = ef_sub(r, ef_from(1)), r2 = ef_sub(r, ef_from(2));
+  if (D == 1) {
+    L[0] = ef_sub(ef_one(), r);
+    L[1] = r;
+  } else if (D == 2) {
+    L[0] = ef_scale(ef_mul_ol(r1, r2), inv2);
+    L[1] = ef_sub(ef_zero(), ef_mul_ol(r, r2));
+    L[D] = ef_scale(ef_mul_ol(r, r1), inv2);
+  } else {
+    const ef2 r3 = ef_sub(r, ef_from(3));
+    const ef2 r12 = ef_mul_ol(r1, r2), rr1 = ef_mul_ol(r, r1);
+    L[0] = ef_sub(ef_zero(), ef_scale(ef_mul_ol(r12, r3), inv6));
+    L[1] = ef_scale(ef_mul_ol(ef_mul_ol(r, r2), r3), inv2);
+    L[D - 1] = ef_sub(ef_zero(), ef_scale(ef_mul_ol(rr1, r3), inv2));
+    L[D] = ef_scale(ef_mul_ol(rr1, r2), inv6);
+  }
+}
+
+// Remaining rounds t0..k-1 in one CTA, with the cooperative pair groups above.  On entry the
+// vectors hold `len` entries (len <= TAIL); if `fold`, they hold 2 len entries still to be
+// folded with challenge t0 - 1.  The vectors live in shared memory; a round is one group step
+// per pair (the fold of round t is written in place by the lane that loaded lo_j, after every
+// read of that position) and one barrier.  Each round's sums are reduced within the warp and
+// kept per warp; they are added up once after the last round.  g(1) of every round after the
+// first is filled in along the claim chain at the end.
+constexpr unsigned SC_TAIL_THREADS = SC_COOP_THREADS;
+constexpr unsigned SC_TAIL_MAXR = 11;
+
 template <int D, bool BIN>
 struct TailSmem {
   static constexpr int S = Fac<D, BIN>::S;
   ef2 sv[S][Fac<D, BIN>::TAIL];
-  ef2 wsum[3][SC_TAIL_THREADS / 32][D + 1];  // phase A: per-warp sums of its (<= 3) rounds
-  ef2 lsum[8][D + 1][32];                     // phases B and C: per-lane sums (<= 7 rounds)
+  ef2 red[SC_TAIL_MAXR][SC_TAIL_THREADS / 32][Coop<D, BIN>::G];
 };
 
 template <int D, bool BIN>
@@ -326,12 +412,13 @@ __global__ void __launch_bounds__(SC_TAIL_THREADS)
                    ef2* __restrict__ final_out, const ef2* __restrict__ partials,
                    size_t stride, unsigned cap) {
   constexpr int S = Fac<D, BIN>::S;
-  constexpr unsigned NT = SC_TAIL_THREADS, NW = NT / 32;
+  constexpr unsigned G = Coop<D, BIN>::G, NW = SC_TAIL_THREADS / 32, GPB = SC_TAIL_THREADS / G;
   extern __shared__ __align__(16) unsigned char tail_smem_raw[];
   TailSmem<D, BIN>& sm = *reinterpret_cast<TailSmem<D, BIN>*>(tail_smem_raw);
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned r = lane & (G - 1), gb = lane & ~(G - 1);
   // The multi-CTA rounds 0..t0-1: round t's sums over the CTAs that ran it (one warp per round);
-  // the claim chain at the end reads them, after the hand-over barrier below.
+  // the claim chain at the end reads them, after the barriers below.
   for (unsigned t = warp; t < t0; t += NW) {
     const size_t half = (size_t)1 << (k - 1 - t);
     const unsigned nb = (unsigned)min((size_t)cap, (half + SC_THREADS - 1) / SC_THREADS);
@@ -350,144 +437,109 @@ __global__ void __launch_bounds__(SC_TAIL_THREADS)
 #pragma unroll
       for (int q = 0; q <= D; ++q) rounds_out[(size_t)t * (D + 1) + q] = sr[q];
   }
-  // load, folding with the previous challenge; thread i loads the indices it owns in phase A
   {
-    const ef2 r = fold ? ch[t0 - 1] : ef_zero();
-    for (unsigned i = threadIdx.x; i < len; i += NT)
+    const ef2 r0 = fold ? ch[t0 - 1] : ef_zero();
+    for (unsigned i = threadIdx.x; i < len; i += SC_TAIL_THREADS)
 #pragma unroll
       for (int j = 0; j < S; ++j)
-        sm.sv[j][i] = fold ? ef_lerp(P.p[j][i], P.p[j][i + len], r) : P.p[j][i];
+        sm.sv[j][i] = fold ? ef_lerp_ol(P.p[j][i], P.p[j][i + len], r0) : P.p[j][i];
   }
-  unsigned L = len, t = t0, ra = 0;
-  // phase A
-  for (; L >= 2 * NT && t < k; ++t, ++ra, L >>= 1) {
+  __syncthreads();
+  unsigned L = len, t = t0, rr = 0;
+  for (; t < k; ++t, ++rr, L >>= 1) {
     const unsigned half = L >> 1;
-    const ef2 r = ch[t];
-    ef2 s[D + 1];
-#pragma unroll
-    for (int q = 0; q <= D; ++q) s[q] = ef_zero();
-    for (unsigned i = threadIdx.x; i < half; i += NT) {
-      ef2 lo[S], hi[S];
-#pragma unroll
-      for (int j = 0; j < S; ++j) lo[j] = sm.sv[j][i], hi[j] = sm.sv[j][i + half];
-      add_pair<D, BIN>(lo, hi, s, t > 0);
-#pragma unroll
-      for (int j = 0; j < S; ++j) sm.sv[j][i] = ef_lerp(lo[j], hi[j], r);
-    }
-#pragma unroll
-    for (int q = 0; q <= D; ++q)
-#pragma unroll
-      for (int m = 16; m; m >>= 1) s[q] = ef_add(s[q], shfl_xor_ef(s[q], m));
-    if (lane == 0)
-#pragma unroll
-      for (int q = 0; q <= D; ++q) sm.wsum[ra][warp][q] = s[q];
-  }
-  __syncthreads();  // hand-over: every fold and partial-round sum is visible
-  if (warp != 0) return;
-  unsigned rb = 0;
-  // phase B
-  for (; L >= 64 && t < k; ++t, ++rb, L >>= 1) {
-    const unsigned half = L >> 1;
-    const ef2 r = ch[t];
-    ef2 s[D + 1];
-#pragma unroll
-    for (int q = 0; q <= D; ++q) s[q] = ef_zero();
-    for (unsigned i = lane; i < half; i += 32) {
-      ef2 lo[S], hi[S];
-#pragma unroll
-      for (int j = 0; j < S; ++j) lo[j] = sm.sv[j][i], hi[j] = sm.sv[j][i + half];
-      add_pair<D, BIN>(lo, hi, s, t > 0);
-#pragma unroll
-      for (int j = 0; j < S; ++j) sm.sv[j][i] = ef_lerp(lo[j], hi[j], r);
-    }
-#pragma unroll
-    for (int q = 0; q <= D; ++q) sm.lsum[rb][q][lane] = s[q];
-  }
-  __syncwarp();
-  // phase C
-  ef2 v[S];
-#pragma unroll
-  for (int j = 0; j < S; ++j) v[j] = lane < L ? sm.sv[j][lane] : ef_zero();
-  for (; L > 1 && t < k; ++t, ++rb, L >>= 1) {
-    const unsigned half = L >> 1;
-    const ef2 r = ch[t];
-    ef2 hi[S];
-#pragma unroll
-    for (int j = 0; j < S; ++j)
-      hi[j] = ef_make(__shfl_down_sync(0xffffffffu, v[j].c0, half),
-                      __shfl_down_sync(0xffffffffu, v[j].c1, half));
-    ef2 s[D + 1];
-#pragma unroll
-    for (int q = 0; q <= D; ++q) s[q] = ef_zero();
-    if (lane < half) {
-      add_pair<D, BIN>(v, hi, s, t > 0);
-#pragma unroll
-      for (int j = 0; j < S; ++j) v[j] = ef_lerp(v[j], hi[j], r);
-    }
-#pragma unroll
-    for (int q = 0; q <= D; ++q) sm.lsum[rb][q][lane] = s[q];
-  }
-  __syncwarp();
-  // this kernel's round sums (g(1) only for round 0): lane x adds up one (round, q) pair
-  const unsigned nra = ra, nrb = rb;
-  for (unsigned x = lane; x < (nra + nrb) * (D + 1); x += 32) {
-    const unsigned rr = x / (D + 1), q = x % (D + 1);
-    const unsigned tt = t0 + rr;
-    if (q == 1 && tt > 0) continue;
+    const int q = coop_q<D>(r, t > 0);
+    const ef2 rt = ch[t];
     ef2 acc = ef_zero();
-    if (rr < nra) {
+    for (unsigned w0 = warp * (32 / G); w0 < half; w0 += GPB) {  // warp-uniform
+      const unsigned i = w0 + lane / G;
+      const bool act = i < half;
+      ef2 val = ef_zero();
+      if (act && r < 2 * S) val = sm.sv[r >> 1][i + (r & 1) * half];
+      FacVals<S> lo, hi;
 #pragma unroll
-      for (unsigned w = 0; w < NW; ++w) acc = ef_add(acc, sm.wsum[rr][w][q]);
-    } else {
-      for (unsigned l = 0; l < 32; ++l) acc = ef_add(acc, sm.lsum[rr - nra][q][l]);
+      for (int j = 0; j < S; ++j)
+        lo.v[j] = shfl_ef(val, gb + 2 * j), hi.v[j] = shfl_ef(val, gb + 2 * j + 1);
+      if (act && q >= 0) acc = ef_add(acc, pair_point<D, BIN>(lo, hi, q));
+      if (act && r < 2 * S && (r & 1) == 0) {
+        const unsigned j = r >> 1;
+        ef2 l = lo.v[0], h = hi.v[0];
+#pragma unroll
+        for (int x = 1; x < S; ++x)
+          if (j == (unsigned)x) l = lo.v[x], h = hi.v[x];
+        sm.sv[j][i] = ef_lerp_ol(l, h, rt);
+      }
     }
-    rounds_out[(size_t)tt * (D + 1) + q] = acc;
+#pragma unroll
+    for (unsigned m = G; m < 32; m <<= 1) acc = ef_add(acc, shfl_xor_ef(acc, m));
+    if (lane < G) sm.red[rr][warp][lane] = acc;
+    __syncthreads();
   }
-  __threadfence_block();  // the chain below reads these sums from other lanes
+  // this kernel's round sums (g(1) only for round 0): lane x of warp 0 adds up one (round, role)
+  if (warp != 0) return;
+  for (unsigned x = lane; x < rr * G; x += 32) {
+    const unsigned ro = x / G, role = x % G, tt = t0 + ro;
+    const int qq = coop_q<D>(role, tt > 0);
+    if (qq < 0) continue;
+    ef2 acc = ef_zero();
+    for (unsigned w = 0; w < NW; ++w) acc = ef_add(acc, sm.red[ro][w][role]);
+    rounds_out[(size_t)tt * (D + 1) + qq] = acc;
+  }
   if (lane == 0) {
     if (BIN) {
-      final_out[0] = v[0];
-      final_out[1] = ef_sub(v[0], ef_one());
+      final_out[0] = sm.sv[0][0];
+      final_out[1] = ef_sub(sm.sv[0][0], ef_one());
 #pragma unroll
-      for (int j = 1; j < S; ++j) final_out[j + 1] = v[j];
+      for (int j = 1; j < S; ++j) final_out[j + 1] = sm.sv[j][0];
     } else {
 #pragma unroll
-      for (int j = 0; j < S; ++j) final_out[j] = v[j];
+      for (int j = 0; j < S; ++j) final_out[j] = sm.sv[j][0];
     }
   }
+  __threadfence_block();  // the chain below reads these sums from other lanes
   __syncwarp();
   // The claim chain: g_t(1) = claim_t - g_t(0) for t >= 1, claim_{t+1} = g_t(r_t).  With
   // g_t(r) = sum_q L_q(r) g_t(q), claim_{t+1} = A_t + L_1(r_t) claim_t, A_t collecting the other
-  // terms (and A_0 = g_0(r_0), whose g(1) is summed), so lane t prepares its round's A_t and
-  // L_1(r_t) in parallel and the claim moves from lane to lane with one product per round.
-  ef2 claim = ef_zero();
+  // terms (and A_0 = g_0(r_0), whose g(1) is summed): an affine map per round.  Lane t prepares
+  // round t's map and an inclusive scan of the compositions (five shuffle steps) gives every
+  // lane claim_{t+1}; claim_t is the previous lane's, and the last lane's carries to the next
+  // 32 rounds.
+  ef2 carry = ef_zero();
   for (unsigned c0 = 0; c0 < k; c0 += 32) {
     const unsigned tt = c0 + lane;
-    ef2 g[D + 1], L[D + 1], a = ef_zero(), w1 = ef_zero();
+    ef2 g[D + 1], Lw[D + 1], a = ef_zero(), w1 = ef_one();
     if (tt < k) {
 #pragma unroll
-      for (int q = 0; q <= D; ++q) g[q] = rounds_out[(size_t)tt * (D + 1) + q];
-      interp_weights<D>(ch[tt], L);
-#pragma unroll
-      for (int q = 0; q <= D; ++q)
-        if (q != 1) a = ef_add(a, ef_mul(L[q], g[q]));
+      for (int qv = 0; qv <= D; ++qv) g[qv] = rounds_out[(size_t)tt * (D + 1) + qv];
+      interp_weights_ol<D>(ch[tt], Lw);
+      for (int qv = 0; qv <= D; ++qv)
+        if (qv != 1) a = ef_add(a, ef_mul_ol(Lw[qv], g[qv]));
       if (tt == 0) {
-        a = ef_add(a, ef_mul(L[1], g[1]));
+        a = ef_add(a, ef_mul_ol(Lw[1], g[1]));
+        w1 = ef_zero();
       } else {
-        w1 = L[1];
-        a = ef_sub(a, ef_mul(L[1], g[0]));
+        w1 = Lw[1];
+        a = ef_sub(a, ef_mul_ol(Lw[1], g[0]));
       }
     }
-    ef2 mine = ef_zero();  // claim_tt
-    for (unsigned j = 0; j < 32 && c0 + j < k; ++j) {
-      ef2 next = ef_zero();
-      if (lane == j) {
-        mine = claim;
-        next = ef_add(a, ef_mul(w1, claim));
+    // inclusive scan: (a, w) after composing lanes c0 .. lane (later maps on the left)
+#pragma unroll
+    for (unsigned off = 1; off < 32; off <<= 1) {
+      const ef2 pa = ef_make(__shfl_up_sync(0xffffffffu, a.c0, off),
+                             __shfl_up_sync(0xffffffffu, a.c1, off));
+      const ef2 pw = ef_make(__shfl_up_sync(0xffffffffu, w1.c0, off),
+                             __shfl_up_sync(0xffffffffu, w1.c1, off));
+      if (lane >= off) {
+        a = ef_add(a, ef_mul_ol(w1, pa));
+        w1 = ef_mul_ol(w1, pw);
       }
-      claim = ef_make(__shfl_sync(0xffffffffu, next.c0, j), __shfl_sync(0xffffffffu, next.c1, j));
     }
-    if (tt < k && tt > 0) rounds_out[(size_t)tt * (D + 1) + 1] = ef_sub(mine, g[0]);
+    const ef2 incl = ef_add(a, ef_mul_ol(w1, carry));  // claim_{tt + 1}
+    ef2 excl = ef_make(__shfl_up_sync(0xffffffffu, incl.c0, 1),
+                       __shfl_up_sync(0xffffffffu, incl.c1, 1));
+    if (lane == 0) excl = carry;  // claim_tt
+    if (tt < k && tt > 0) rounds_out[(size_t)tt * (D + 1) + 1] = ef_sub(excl, g[0]);
+    carry = shfl_ef(incl, 31);
   }
 }
 
@@ -520,7 +572,7 @@ void sumcheck_run(ef2* const* polys, unsigned k, const ef2* ch, ef2* rounds_out,
     if (BIN && t == 0)
       sc_bin_round0_kernel<<<blocks, SC_THREADS, 0, st>>>(P.p[0], P.p[S - 1], half, partials);
     else
-      sc_round_kernel<D, BIN><<<blocks, SC_THREADS, 0, st>>>(
+      sc_coop_kernel<D, BIN><<<blocks, SC_COOP_THREADS, 0, st>>>(
           P, half, fold, fold ? ch + (t - 1) : ch, partials + (size_t)t * stride);
     LGS_LAUNCH_CHECK();
     len = half;

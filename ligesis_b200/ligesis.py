@@ -344,12 +344,15 @@ class Ligesis:
         return LigesisCommit(data=data), data
 
     @staticmethod
-    def commit_device(pk: ProvingKey, f_dev_ptr: int, length: int):
+    def commit_device(pk: ProvingKey, f_dev_ptr: int, length: int, lend: bool = False):
         """commit with f already in device memory (e.g. a torch uint64/int64 CUDA tensor); f must
-        stay unchanged until the commitment's root has been read or a prove has returned."""
+        stay unchanged until the commitment's root has been read or a prove has returned.  With
+        lend=True f is not copied: the commitment reads the caller's buffer for as long as it
+        lives (as the reference's commit owns its MlPoly), so the buffer must stay allocated and
+        unchanged until the CommitData is released."""
         h = vp()
-        check(load().lgs_commit_async(pk.ctx.handle, pk.handle, vp(f_dev_ptr), length, 1,
-                                      C.byref(h)))
+        check(load().lgs_commit_async(pk.ctx.handle, pk.handle, vp(f_dev_ptr), length,
+                                      2 if lend else 1, C.byref(h)))
         data = CommitData(h, pk)
         return LigesisCommit(data=data), data
 

@@ -235,23 +235,45 @@ def test_commit_only_square_shapes_match_oracle(lgs, orc, log_m, log_n):
 
 
 def test_tuned_launch_choices_give_the_same_proof(lgs, orc):
-    """lgs_tune changes only how kernels are launched: fewer hash CTAs and a smaller sumcheck
-    grid give the oracle's commitment and proof; unknown names are refused."""
+    """lgs_tune changes only how kernels are launched: fewer hash CTAs, a smaller sumcheck grid
+    and the digest built in row groups under the upload (the host polynomial here takes that
+    path) give the oracle's commitment and proof; unknown names are refused."""
     log_m, log_n = 5, 13
     f, A, z, fields, ints = ligesis_inputs(log_m, log_n, seed=91)
     ctx = L.Context(0)
     pk, _ = L.Ligesis.setup_with_hash(log_m, log_n, L.SubsetSumHash(64 << log_m, a=A), ctx)
     key = orc.Key(log_m, log_n, A)
     want, _ = orc.prove(key, orc.Commitment(key, f), z, fields, ints)
-    for h, b in [(0, 0), (40, 148), (7, 16), (148, 296)]:
-        ctx.tune(hash_ctas=h, sumcheck_blocks=b)
-        assert ctx.tuning() == {"hash_ctas": h, "sumcheck_blocks": b}
+    for h, b, g in [(0, 0, 0), (40, 148, 2), (7, 16, 8), (148, 296, 4)]:
+        ctx.tune(hash_ctas=h, sumcheck_blocks=b, hash_groups=g)
+        assert ctx.tuning() == {"hash_ctas": h, "sumcheck_blocks": b, "hash_groups": g}
         for _ in range(3):  # eager, captured, replayed
             commit, data = L.Ligesis.commit(pk, L.MlPoly(f))
             o = L.RandomOracle(0, length=8)
             o.fields, o.ints = np.ascontiguousarray(fields), np.ascontiguousarray(ints)
-            assert L.Ligesis.prove(pk, data, z, o).data == want, (h, b)
+            assert L.Ligesis.prove(pk, data, z, o).data == want, (h, b, g)
     with pytest.raises(L.LgsError, match="unknown parameter"):
         ctx.tune(nonsense=1)
     with pytest.raises(L.LgsError):
         ctx.tune(sumcheck_blocks=297)
+
+
+def test_lent_device_polynomial_gives_the_same_commitment(lgs, orc):
+    """commit_device(lend=True) reads the caller's device buffer in place (f_on_device = 2):
+    the root and the proof equal the oracle's, as with the copying forms."""
+    import torch
+
+    log_m, log_n = 5, 13
+    f, A, z, fields, ints = ligesis_inputs(log_m, log_n, seed=93)
+    pk, _ = L.Ligesis.setup_with_hash(log_m, log_n, L.SubsetSumHash(64 << log_m, a=A))
+    f_dev = torch.from_numpy(f.view(np.int64).copy()).cuda()
+    key = orc.Key(log_m, log_n, A)
+    cm = orc.Commitment(key, f)
+    want, _ = orc.prove(key, cm, z, fields, ints)
+    for lend in (False, True):
+        commit, data = L.Ligesis.commit_device(pk, f_dev.data_ptr(), f.size, lend=lend)
+        o = L.RandomOracle(0, length=8)
+        o.fields, o.ints = np.ascontiguousarray(fields), np.ascontiguousarray(ints)
+        assert L.Ligesis.prove(pk, data, z, o).data == want, lend
+        assert commit.root == cm.root, lend
+    assert np.array_equal(f_dev.cpu().numpy().view(np.uint64), f)  # only read
