@@ -57,7 +57,8 @@ def apply(ctx, log_m: int, log_n: int, path: Path | None = None) -> dict | None:
     return best
 
 
-def tune(log_m: int, log_n: int, steps: int = 10, warmup: int = 3, device: int = 0,
+def tune(log_m: int, log_n: int, steps: int = 10, warmup: int = 3, repeats: int = 3,
+         device: int = 0,
          hash_ctas=None, sumcheck_blocks=None, hash_groups=None, path: Path | None = None,
          save: bool = True) -> dict:
     """Coordinate search: hash_ctas first (sumcheck_blocks at its default), then
@@ -111,15 +112,19 @@ def tune(log_m: int, log_n: int, steps: int = 10, warmup: int = 3, device: int =
         if out != ref:
             raise RuntimeError(f"setting {setting} changed the commitment or proof")
         del prev, c, p
-        torch.cuda.synchronize(device)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(steps):
-            last = step()
-        e1.record(stream)
-        torch.cuda.synchronize(device)
-        del last
-        return e0.elapsed_time(e1) / steps
+        best_ms = None
+        for _ in range(repeats):  # the fastest of `repeats` runs: timing noise only adds
+            torch.cuda.synchronize(device)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                last = step()
+            e1.record(stream)
+            torch.cuda.synchronize(device)
+            del last
+            ms = e0.elapsed_time(e1) / steps
+            best_ms = ms if best_ms is None else min(best_ms, ms)
+        return best_ms
 
     trials = []
     best = {"hash_ctas": 0, "sumcheck_blocks": 0}
