@@ -435,7 +435,9 @@ def run_ours(args) -> None:
         a = ntt_bytes / (stages["rs_encode"] * 1e-3) / 1e9
         others["rs_encode"] = {"bound": "hbm", "achieved": round(a, 1), "unit": "GB/s",
                                "peak": peaks["hbm_gbs"], "frac": round(a / peaks["hbm_gbs"], 4),
-                               "traffic": ncu_traffic("rs_encode")}
+                               "traffic": ncu_traffic("rs_encode"),
+                               "alu_floor": rs_alu_floor(lib, ctx, LOG_M, LOG_N,
+                                                         stages["rs_encode"])}
     if "subset_sum_hash" in stages:
         a = hash_ops / (stages["subset_sum_hash"] * 1e-3) / 1e12
         others["subset_sum_hash"] = {"bound": "tensor", "achieved": round(a, 1),
@@ -508,7 +510,34 @@ def _keys_for(mus, ctx):
     return keys
 
 
-def batch_stats(lanes: int, reps: int = 3) -> dict:
+def rs_alu_floor(lib, ctx, log_m: int, log_n: int, measured_ms: float) -> dict:
+    """The RS encoding's arithmetic floor: its radix-8 DFTs and twiddle multiplications (counted
+    from the kernels' structure, rs_dft.cu) at the device-wide rates of lgs_rs_alu_rates, which
+    run the same arithmetic with no memory traffic."""
+    import ctypes as C
+    import math
+
+    r8, mul = C.c_double(), C.c_double()
+    import ligesis_b200 as L
+
+    L._lib.check(lib.lgs_rs_alu_rates(ctx.handle, 4096, C.byref(r8), C.byref(mul)))
+    N = 2 << log_n
+    n2 = N >> 12
+    # pass A: four radix-8 stages (the first on a half-zero input, 8 of its 12 butterflies),
+    # 7 + 8 + 7 twiddle products per 8 values; pass B: log8(N2) stages, 15 products per 8
+    # values when N2 = 64 (one per value otherwise)
+    r8_per = (2.0 / 3.0 + 3.0) / 8.0 + (math.log2(n2) / 3.0) / 8.0
+    mul_per = 22.0 / 8.0 + (15.0 / 8.0 if n2 == 64 else 1.0)
+    values = float(1 << log_m) * N
+    floor_ms = values * (r8_per / r8.value + mul_per / mul.value) * 1e3
+    return {"floor_ms": round(floor_ms, 4), "frac_of_floor": round(floor_ms / measured_ms, 4),
+            "radix8_per_s": round(r8.value, 1), "mul_per_s": round(mul.value, 1),
+            "radix8_per_value": round(r8_per, 4), "mul_per_value": round(mul_per, 4),
+            "note": "arithmetic only (registers, no loads, stores or exchanges): the time the "
+                    "encoding's butterflies and twiddle products take at full occupancy"}
+
+
+def batch_stats(lanes: int, reps: int = 5) -> dict:
     """96 polynomials of uneven size (mu = floor(14 + 8u)), each committed and opened at its own
     point: one at a time on one context versus all through the engine's lanes; host f in, proof
     out.  Each side is timed `reps` times and the best run counts; every proof of the engine must
@@ -560,10 +589,12 @@ def batch_stats(lanes: int, reps: int = 3) -> dict:
     plain()  # warm-up: arenas and pools of every shape
     t_plain, ref = best(plain)
     with ProverEngine(0, lanes=lanes) as eng:
+        tuning = eng.tuning
         eng.prepare(keys.values())
         batched(eng)
         t_batch, got = best(lambda: batched(eng))
     return {"jobs": len(jobs), "mu": [min(mus), max(mus)], "lanes": lanes,
+            "lane_tuning": tuning or "built-in defaults",
             "plain_proofs_per_s": round(len(jobs) / t_plain, 1),
             "batched_proofs_per_s": round(len(jobs) / t_batch, 1),
             "speedup": round(t_plain / t_batch, 2), "identical_proofs": got == ref,
@@ -824,6 +855,9 @@ def run_autotune(args) -> None:
     entry = autotune.tune(args.log_m, args.log_n, steps=args.steps, warmup=args.warmup)
     print(json.dumps({"mode": "autotune", "log_m": args.log_m, "log_n": args.log_n, **entry}),
           flush=True)
+    if args.engine:  # the engine lanes' launch choices on the batch workload
+        entry = autotune.tune_engine(lanes=args.lanes)
+        print(json.dumps({"mode": "autotune", "engine": args.lanes, **entry}), flush=True)
 
 
 def run_timeline(args) -> None:
@@ -1081,6 +1115,26 @@ def run_witness(args) -> None:
                 fn()
             torch.cuda.synchronize()
             res[label] = round((time.perf_counter() - t0) / args.steps * 1e3, 3)
+        # the contraction kernel alone (CUDA events around it, device operands)
+        import ctypes as C
+
+        lib = L.load()
+        L._lib.check(lib.lgs_profile(ctx.handle, 1))
+        for _ in range(args.steps):
+            ps.linear_witness(xd, wd, bd, sc, wt, ctx)
+        for stage in ("linear_witness_tc", "linear_witness_cores"):
+            tot, cnt = C.c_double(), C.c_uint64()
+            L._lib.check(lib.lgs_profile_get(ctx.handle, stage.encode(), C.byref(tot),
+                                             C.byref(cnt)))
+            if cnt.value:
+                res[stage + "_kernel_ms"] = round(tot.value / cnt.value, 4)
+        L._lib.check(lib.lgs_profile(ctx.handle, 0))
+        kern = res.get("linear_witness_tc_kernel_ms")
+        if kern:
+            # HBM bytes: the weights and activations read once, four outputs written
+            bytes_ = 8.0 * (inner * cols + n * inner + 4 * n * cols)
+            res["kernel_gbs"] = round(bytes_ / (kern * 1e-3) / 1e9, 1)
+            res["kernel_frac_hbm"] = round(res["kernel_gbs"] / _peaks()["hbm_gbs"], 4)
         res["products"] = n * inner * cols
         out[name] = res
     if args.layer:
@@ -1139,6 +1193,8 @@ def main() -> None:
     ap.add_argument("--log-m", type=int, default=LOG_M)
     ap.add_argument("--log-n", type=int, default=LOG_N)
     ap.add_argument("--lanes", type=int, default=12)
+    ap.add_argument("--engine", action="store_true",
+                    help="autotune mode: also tune the engine lanes on the batch workload")
     ap.add_argument("--mus", default="20,22,24", help="sumcheck mode: polynomial sizes")
     ap.add_argument("--sc-d", type=int, default=3, choices=[1, 2, 3],
                     help="sumcheck mode: factors in the product (the reference bench: 3)")

@@ -240,6 +240,12 @@ void lgs_engine_free_proof(uint8_t* proof);
 lgs_status lgs_engine_prepare(lgs_engine* e, const lgs_pk* const* pks, size_t npk);
 /* Jobs waiting for a lane, and the device bytes reserved by running jobs. */
 lgs_status lgs_engine_pending(lgs_engine* e, size_t* queued, size_t* running_bytes);
+/* lgs_tune on every lane (same names and limits).  Small jobs run side by side when their
+ * kernels leave SMs free: a lower hash_ctas / sumcheck_blocks cap trades one job's latency for
+ * the batch's throughput.  Call with no job queued or running (else LGS_ERR_BAD_ARG); a
+ * sumcheck_blocks change drops the lanes' captured prove graphs (lgs_engine_prepare again).
+ * No reference counterpart. */
+lgs_status lgs_engine_tune(lgs_engine* e, const char* name, uint64_t value);
 
 /* ---- measurement (no counterpart in the reference, whose benches use wall-clock timers,
  * pcs/benches/ligesis.rs:27-45) ---- */
@@ -263,6 +269,9 @@ lgs_status lgs_profile_names(lgs_ctx* ctx, char* buf, size_t cap, size_t* needed
  *   "sumcheck_blocks"  grid cap of the multi-CTA sumcheck passes (at most 296)
  *   "hash_groups"      commits of host polynomials: digest the codeword in this many row
  *                      groups (1..8) as their RS encoding finishes, under the upload
+ *   "witness_path"     lgs_linear_witness: 0 the int8 tensor cores whenever every activation
+ *                      fits 24 and every weight 16 signed bits (else the CUDA cores), 1 always
+ *                      the CUDA cores
  * Results do not depend on them.  Unknown names: LGS_ERR_BAD_ARG. */
 lgs_status lgs_tune(lgs_ctx* ctx, const char* name, uint64_t value);
 lgs_status lgs_tune_get(lgs_ctx* ctx, const char* name, uint64_t* value);
@@ -280,6 +289,12 @@ uint64_t lgs_launch_count(void);
  * back-to-back tcgen05.mma.kind::i8 M128 N256 K32 from shared memory (the hash's MMA shape);
  * *tops receives the best of three timed launches in TOP/s (2 ops per multiply-add). */
 lgs_status lgs_tensor_peak_i8(lgs_ctx* ctx, unsigned iters, double* tops);
+/* The arithmetic floor of the commitment's RS encoding: device-wide rates, per second, of the
+ * radix-8 DFT every stage of the encoding runs and of its twiddle multiplications, each from a
+ * kernel that keeps eight values per thread in registers for `iters` iterations (no memory
+ * traffic; best of three timed launches).  No reference counterpart. */
+lgs_status lgs_rs_alu_rates(lgs_ctx* ctx, unsigned iters, double* radix8_per_s,
+                            double* mul_per_s);
 
 /* ---- the individual device operations of the path (host buffers in and out) ---- */
 

@@ -107,6 +107,7 @@ _SIGS = {
     "lgs_lut_gather": (C.c_int, [vp, i64p, C.c_size_t, i64p, C.c_size_t, C.c_int64, C.c_int,
                                  i64p]),
     "lgs_tensor_peak_i8": (C.c_int, [vp, C.c_uint, C.POINTER(C.c_double)]),
+    "lgs_rs_alu_rates": (C.c_int, [vp, C.c_uint, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "lgs_dft": (C.c_int, [vp, u64p, C.c_size_t, C.c_size_t, C.c_uint, u64p]),
     "lgs_subset_sum_hash": (C.c_int, [vp, u64p, C.c_size_t, u64p, C.c_size_t, u64p]),
     "lgs_merkle_root": (C.c_int, [vp, u64p, C.c_size_t, C.c_uint, u8p]),

@@ -49,6 +49,15 @@ def lookup(log_m: int, log_n: int, device: int = 0, path: Path | None = None) ->
     return {k: entry[k] for k in PARAMS if k in entry} if entry else None
 
 
+def engine_key(lanes: int) -> str:
+    return f"engine{lanes}"
+
+
+def lookup_engine(lanes: int, device: int = 0, path: Path | None = None) -> dict | None:
+    entry = load(path).get(_device_name(device), {}).get(engine_key(lanes))
+    return {k: entry[k] for k in ("hash_ctas", "sumcheck_blocks") if k in entry} if entry else None
+
+
 def apply(ctx, log_m: int, log_n: int, path: Path | None = None) -> dict | None:
     """Sets ctx's launch choices from the cache; returns them (None: no entry, defaults kept)."""
     best = lookup(log_m, log_n, ctx.device, path)
@@ -159,5 +168,70 @@ def tune(log_m: int, log_n: int, steps: int = 10, warmup: int = 3, repeats: int 
     if save:
         cache = load(path)
         cache.setdefault(_device_name(device), {})[shape_key(log_m, log_n)] = entry
+        Path(path or CACHE).write_text(json.dumps(cache, indent=1) + "\n")
+    return entry
+
+
+def tune_engine(lanes: int = 12, jobs: int = 96, repeats: int = 3, device: int = 0,
+                hash_ctas=(0, 32, 64), sumcheck_blocks=(0, 37, 74, 148),
+                path: Path | None = None, save: bool = True) -> dict:
+    """Grid search of the engine lanes' launch choices on the batch workload (`jobs` polynomials
+    of mu = floor(14 + 8u), host f in, proof out): with many small jobs in flight, smaller
+    hash and sumcheck grids let kernels of different lanes share the SMs.  Keeps the setting
+    with the most proofs per second (best of `repeats` batches, host wall clock) and records it
+    per GPU name under "engine<lanes>"; every setting must give the same roots and proofs."""
+    import gc
+
+    import ligesis_b200 as L
+    from ligesis_b200 import rng
+    from ligesis_b200.engine import ProverEngine
+    from ligesis_b200.workloads import batch_mus, shape_for_mu
+
+    mus = batch_mus(jobs)
+    ctx = L.Context(device)
+    keys = {}
+    for mu in sorted(set(mus)):
+        lm, ln = shape_for_mu(mu)
+        A = rng.field_elements(100 + lm, 32 * (64 << lm)).reshape(32, 64 << lm)
+        keys[mu] = L.Ligesis.setup_with_hash(lm, ln, L.SubsetSumHash(64 << lm, a=A), ctx)[0]
+    work = [(keys[mu], rng.field_elements(1000 + i, 1 << mu), rng.ext_elements(2000 + i, mu))
+            for i, mu in enumerate(mus)]
+    oracles = [L.RandomOracle(3000 + i, length=1024) for i in range(len(work))]
+    trials, ref, best = [], None, None
+    with ProverEngine(device, lanes=lanes, tuned=False) as eng:
+        for h in hash_ctas:
+            for b in sumcheck_blocks:
+                eng.tune(hash_ctas=h, sumcheck_blocks=b)
+                eng.prepare(keys.values())
+
+                def batch():
+                    for o in oracles:
+                        o.restart()
+                    res = eng.run([(pk, f, z, o) for (pk, f, z), o in zip(work, oracles)])
+                    return [(r.commit.root, r.proof.data) for r in res]
+
+                out = batch()  # warm-up
+                if ref is None:
+                    ref = out
+                if out != ref:
+                    raise RuntimeError(f"engine setting {h}, {b} changed a root or proof")
+                t_best = None
+                for _ in range(repeats):
+                    gc.collect()
+                    gc.disable()
+                    t0 = time.perf_counter()
+                    batch()
+                    t = time.perf_counter() - t0
+                    gc.enable()
+                    t_best = t if t_best is None else min(t_best, t)
+                pps = round(len(work) / t_best, 1)
+                trials.append({"hash_ctas": h, "sumcheck_blocks": b, "pps": pps})
+                if best is None or pps > best["pps"]:
+                    best = trials[-1]
+    entry = {**best, "default_pps": trials[0]["pps"], "jobs": jobs, "lanes": lanes,
+             "when": time.strftime("%Y-%m-%d"), "trials": trials}
+    if save:
+        cache = load(path)
+        cache.setdefault(_device_name(device), {})[engine_key(lanes)] = entry
         Path(path or CACHE).write_text(json.dumps(cache, indent=1) + "\n")
     return entry

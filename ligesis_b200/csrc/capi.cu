@@ -181,6 +181,19 @@ lgs_status lgs_tensor_peak_i8(lgs_ctx* ctx, unsigned iters, double* tops) {
   });
 }
 
+lgs_status lgs_rs_alu_rates(lgs_ctx* ctx, unsigned iters, double* radix8_per_s,
+                            double* mul_per_s) {
+  return guarded([&] {
+    need(ctx && radix8_per_s && mul_per_s && iters >= 1 && iters <= (1u << 24),
+         "lgs_rs_alu_rates: bad argument");
+    CtxDevice dg(ctx);
+    DevMem sink(sizeof(u64), ctx->st);
+    *radix8_per_s = rs_alu_rate(0, iters, sink.as<u64>(), ctx->st);
+    *mul_per_s = rs_alu_rate(1, iters, sink.as<u64>(), ctx->st);
+    LGS_CUDA(cudaStreamSynchronize(ctx->st));
+  });
+}
+
 lgs_status lgs_ctx_stream(lgs_ctx* ctx, void** stream) {
   return guarded([&] {
     need(ctx && stream, "lgs_ctx_stream: null argument");
@@ -552,6 +565,9 @@ lgs_status lgs_tune(lgs_ctx* ctx, const char* name, uint64_t value) {
     } else if (n == "hash_groups") {
       need(value <= lgs_ctx::ROW_BLOCKS, "lgs_tune: hash_groups above the upload's row blocks");
       ctx->hash_groups = (unsigned)value;
+    } else if (n == "witness_path") {
+      need(value <= 1, "lgs_tune: witness_path is 0 (tensor cores) or 1 (CUDA cores)");
+      ctx->witness_path = (unsigned)value;
     } else if (n == "sumcheck_blocks") {
       need(value <= SC_MAX_BLOCKS, "lgs_tune: sumcheck_blocks above the partial-sum slots");
       ctx->sumcheck_blocks = (unsigned)value;
@@ -574,6 +590,7 @@ lgs_status lgs_tune_get(lgs_ctx* ctx, const char* name, uint64_t* value) {
     if (n == "hash_ctas") *value = ctx->hash_ctas;
     else if (n == "sumcheck_blocks") *value = ctx->sumcheck_blocks;
     else if (n == "hash_groups") *value = ctx->hash_groups;
+    else if (n == "witness_path") *value = ctx->witness_path;
     else throw std::invalid_argument("lgs_tune_get: unknown parameter " + n);
   });
 }

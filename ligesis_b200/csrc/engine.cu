@@ -269,6 +269,27 @@ lgs_status lgs_engine_prepare(lgs_engine* e, const lgs_pk* const* pks, size_t np
   return st;
 }
 
+lgs_status lgs_engine_tune(lgs_engine* e, const char* name, uint64_t value) {
+  if (!e || !name) return lgs::set_error(LGS_ERR_BAD_ARG, "lgs_engine_tune: null argument");
+  {
+    std::lock_guard<std::mutex> lk(e->mu);
+    if (!e->queue.empty() || e->in_use != 0 || e->preparing)
+      return lgs::set_error(LGS_ERR_BAD_ARG, "lgs_engine_tune: jobs are queued or running");
+    e->preparing = true;  // the workers stay idle while the lanes change
+  }
+  lgs_status st = LGS_OK;
+  for (lgs_ctx* lane : e->lanes) {
+    st = lgs_tune(lane, name, value);
+    if (st != LGS_OK) break;
+  }
+  {
+    std::lock_guard<std::mutex> lk(e->mu);
+    e->preparing = false;
+  }
+  e->cv_work.notify_all();
+  return st;
+}
+
 lgs_status lgs_engine_pending(lgs_engine* e, size_t* queued, size_t* running_bytes) {
   if (!e || !queued || !running_bytes) return lgs::set_error(LGS_ERR_BAD_ARG, "null argument");
   std::lock_guard<std::mutex> lk(e->mu);

@@ -29,6 +29,7 @@
 
 #include "blake3.cuh"
 #include "kernels.cuh"
+#include "tcgen05.cuh"
 
 namespace lgs {
 
@@ -49,87 +50,25 @@ constexpr int SS_WORDS = EPI_COLS * SS_PITCH;  // one staging buffer; two altern
 constexpr int SS_BYTES = 2 * SS_WORDS * 4;
 constexpr int NBARS = 3 * TC_STAGES + 3;  // full, empty, acc_full/acc_empty/drain, tma
 constexpr int SMEM_BYTES = TC_STAGES * STAGE_BYTES + SS_BYTES + 1024 /*align*/ + 128 /*barriers*/;
-constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s at 1.9 GHz (default budget)
+constexpr long long WAIT_CYCLES = tc::DRAIN_CYCLES;  // ~2 s at 1.9 GHz (default budget)
 // instruction descriptor: D = S32 (2 << 4), A = B = U8 (0), both K-major, N = 256, M = 128
-constexpr uint32_t IDESC = (2u << 4) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr uint32_t IDESC = tc::idesc_u8(128, 256);
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(done)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-// Bounded wait for the phase with the given parity to complete.  false after `budget` clock
-// cycles, or as soon as another role has flagged a failure (*fail != 0).
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* fail,
-                                          long long budget) {
-  const long long t0 = clock64();
-  while (true) {
-    if (mbar_test(bar, parity)) return true;
-    if (*fail) return false;
-    if (clock64() - t0 > budget) return false;
-  }
-}
-// Bounded wait that ignores the failure flag (draining work already issued).
-__device__ __forceinline__ bool mbar_wait_drain(uint32_t bar, uint32_t parity) {
-  const long long t0 = clock64();
-  while (!mbar_test(bar, parity))
-    if (clock64() - t0 > WAIT_CYCLES) return false;
-  return true;
-}
-__device__ __forceinline__ void flag_failure(volatile int* fail, int* err, int code) {
-  *fail = 1;
-  atomicExch(err, code);
-}
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
-  uint64_t d = (uint64_t)((addr >> 4) & 0x3FFFu);  // start address
-  d |= (uint64_t)1 << 16;                          // leading byte offset (unused: K fits the atom)
-  d |= (uint64_t)(1024 >> 4) << 32;                // stride byte offset: 8 rows x 128 B
-  d |= (uint64_t)1 << 46;                          // descriptor version (sm_100)
-  d |= (uint64_t)2 << 61;                          // SWIZZLE_128B
-  return d;
-}
+using tc::flag_failure;
+using tc::mbar_arrive;
+using tc::mbar_arrive_tx;
+using tc::mbar_init;
+using tc::mbar_test;
+using tc::mbar_wait;
+using tc::mbar_wait_drain;
+using tc::mma_commit;
+using tc::smem_u32;
+using tc::sw128_desc;
+using tc::tmem_ld16;
+using tc::tmem_wait_ld;
 __device__ __forceinline__ void mma_i8(uint32_t dtmem, uint64_t adesc, uint64_t bdesc,
                                        uint32_t accumulate) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-      " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(dtmem),
-      "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate)
-      : "memory");
-}
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-      : "memory");
-}
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
-      "%14,%15}, [%16];\n"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-}
-__device__ __forceinline__ void tmem_wait_ld() {
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+  tc::mma_i8(dtmem, adesc, bdesc, IDESC, accumulate);
 }
 __device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 // Barrier of the 128 epilogue threads that also ANDs their flags, so that they leave a loop

@@ -28,6 +28,9 @@ void build_rs_tables(u64* tables, const u64* tw, cudaStream_t st);
 bool rs_dft_supported(unsigned logN, size_t n_in);
 void rs_dft_rows(const u64* in, size_t ld_in, size_t n_in, u64* out, size_t ld_out,
                  unsigned logN, size_t rows, u64* z, const u64* tables, cudaStream_t st);
+// Device-wide rate of the encoding's arithmetic with no memory traffic, per second: op 0 radix-8
+// DFTs, op 1 Goldilocks multiplications.  sink: one u64 of device memory.
+double rs_alu_rate(int op, unsigned iters, u64* sink, cudaStream_t st);
 
 // hash_tc.cu (tcgen05): also writes the Merkle leaf hashes of H's columns into `leaves`.
 void alimb_from_a(const u64* A, uint8_t* alimb, size_t W, cudaStream_t st);

@@ -273,6 +273,7 @@ struct lgs_ctx {
   unsigned hash_ctas = 0;        // persistent CTAs of the subset-sum hash (default: one per SM)
   unsigned sumcheck_blocks = 0;  // grid cap of the multi-CTA sumcheck passes (<= SC_MAX_BLOCKS)
   unsigned hash_groups = 0;      // host-rows commit: hash launches over row groups (0: default)
+  unsigned witness_path = 0;     // linear witness: 0 tensor cores when the operands fit, 1 CUDA cores
   // Pinned host memory: every transfer of a call is asynchronous, so the host enqueues a whole
   // commit or prove without waiting for the device and synchronises once at the end.
   lgs::PinnedBuf up;    // the parameter blob of one prove (one host-to-device copy)
@@ -370,6 +371,12 @@ int lookup_verify_host(const uint8_t* proof, size_t len, const u64* fields, size
                        u64* vals);
 // proofsys' rescaled linear-layer witness (witness.cu): Q, REM = floor_div(X W, divisor),
 // Y = Q + bias, Y_field = encode_i64(Y); row-major i64 arrays, on the host or (on_device) the device.
+// The layer's contraction on the int8 tensor cores (witness_tc.cu), on device operands; sets
+// *drange when an operand is outside its limb encoding (nothing usable is written then).
+void linear_witness_tc(lgs_ctx* c, const int64_t* dx, size_t rows, size_t inner,
+                       const int64_t* dw, size_t cols, bool w_transposed, const int64_t* db,
+                       int64_t divisor, int64_t* dq, int64_t* dr, int64_t* dy, uint64_t* df,
+                       int* derr, int* drange);
 void linear_witness_dev(lgs_ctx* c, const int64_t* x, size_t rows, size_t inner, const int64_t* w,
                         size_t cols, bool w_transposed, const int64_t* bias, int64_t divisor,
                         bool on_device, int64_t* q, int64_t* rem, int64_t* y, uint64_t* y_field);

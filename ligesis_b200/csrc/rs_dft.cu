@@ -363,7 +363,61 @@ void launch_b(const u64* z, u64* out, size_t ld_out, size_t rows, const u64* t4,
   LGS_LAUNCH_CHECK();
 }
 
+// ---- the arithmetic floor of the encoding: its operations with no memory traffic -------------
+// op 0: one radix-8 DFT (dft_r8, as every stage of both passes) per iteration; op 1: eight
+// independent twiddle multiplications (gl_mul) per iteration.  Eight values per thread, a
+// checksum to `sink` so nothing is optimised away.
+__global__ void __launch_bounds__(256) rs_alu_floor_kernel(unsigned iters, int op, u64* sink) {
+  const u64 seed = 0x9E3779B97F4A7C15ull * (blockIdx.x * blockDim.x + threadIdx.x + 1);
+  u64 v[8], t[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    v[j] = gl_canon(seed + 0x632BE59BD9B4E019ull * j);
+    t[j] = gl_canon(seed ^ (0xD1B54A32D192ED03ull * (j + 3)));
+  }
+  if (op == 0) {
+#pragma unroll 1
+    for (unsigned i = 0; i < iters; ++i) dft_r8<1, false>(v);
+  } else {
+#pragma unroll 1
+    for (unsigned i = 0; i < iters; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) v[j] = gl_mul(v[j], t[j]);
+  }
+  u64 acc = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) acc ^= v[j];
+  if (acc == 0x0123456789ABCDEFull) *sink = acc;  // practically never: keeps v live
+}
+
 }  // namespace
+
+double rs_alu_rate(int op, unsigned iters, u64* sink, cudaStream_t st) {
+  int dev = 0, sms = 0;
+  LGS_CUDA(cudaGetDevice(&dev));
+  LGS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  int per_sm = 1;
+  LGS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rs_alu_floor_kernel, 256, 0));
+  const unsigned blocks = (unsigned)(sms * std::max(1, per_sm));
+  cudaEvent_t e0, e1;
+  LGS_CUDA(cudaEventCreate(&e0));
+  LGS_CUDA(cudaEventCreate(&e1));
+  double best = 0.0;
+  for (int rep = 0; rep < 4; ++rep) {  // the first launch warms up; keep the best
+    LGS_CUDA(cudaEventRecord(e0, st));
+    rs_alu_floor_kernel<<<blocks, 256, 0, st>>>(iters, op, sink);
+    LGS_LAUNCH_CHECK();
+    LGS_CUDA(cudaEventRecord(e1, st));
+    LGS_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    LGS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    const double ops = (double)blocks * 256 * iters * (op == 0 ? 1.0 : 8.0);
+    if (rep > 0 && ms > 0) best = std::max(best, ops / (ms * 1e-3));
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return best;
+}
 
 size_t rs_table_offset(unsigned logN) {
   size_t off = 4096;

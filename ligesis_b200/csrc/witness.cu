@@ -17,6 +17,7 @@
 #include <cstring>
 
 #include "prover.cuh"
+#include "witness.cuh"
 
 namespace lgs {
 
@@ -26,55 +27,6 @@ constexpr int LW_TM = 32, LW_TN = 64, LW_K = 32;  // output tile rows x cols, K 
 constexpr size_t LW_XS_BYTES = (size_t)LW_K * (LW_TM + 1) * 8;
 constexpr size_t LW_WS_BYTES = (size_t)LW_K * (LW_TN + 1) * 8;
 constexpr size_t LW_SMEM = 2 * (LW_XS_BYTES + LW_WS_BYTES) + 4 * 8;
-
-// 128-bit accumulator as (hi:lo); a product of two i64 is added exactly.
-// (two's complement in two words, added modulo 2^128 like the reference's i128)
-struct Acc128 {
-  uint64_t lo, hi;
-};
-__device__ __forceinline__ void mac128(Acc128& a, int64_t x, int64_t y) {
-  const uint64_t pl = (uint64_t)x * (uint64_t)y;
-  const uint64_t ph = (uint64_t)__mul64hi(x, y);
-  a.lo += pl;
-  a.hi += ph + (a.lo < pl ? 1 : 0);
-}
-__device__ __forceinline__ void add128(Acc128& a, const Acc128& b) {
-  a.lo += b.lo;
-  a.hi += b.hi + (a.lo < b.lo ? 1 : 0);
-}
-__device__ __forceinline__ bool fits_i64(uint64_t hi, uint64_t lo) {
-  return (int64_t)hi == ((int64_t)lo >> 63);  // the high word extends the low word's sign
-}
-
-// Q, REM, Y, Y_field of one output from its exact sum; false when a value leaves the i64 range.
-__device__ __forceinline__ bool lw_finish(const Acc128& s, const int64_t* bias, size_t c,
-                                          int64_t d, size_t o, int64_t* q_out, int64_t* rem_out,
-                                          int64_t* y_out, uint64_t* yf_out) {
-  if (!fits_i64(s.hi, s.lo)) return false;  // checked_i128_to_i64 of the product
-  const int64_t v = (int64_t)s.lo;
-  int64_t q = v / d, rm = v % d;  // floor division: a negative remainder moves q down
-  if (rm < 0) {
-    q -= 1;
-    rm += d;
-  }
-  const int64_t b = bias ? bias[c] : 0;
-  const int64_t yy = (int64_t)((uint64_t)q + (uint64_t)b);
-  if (((q ^ yy) & (b ^ yy)) < 0) return false;  // signed overflow of q + bias
-  q_out[o] = q;
-  rem_out[o] = rm;
-  y_out[o] = yy;
-  if (yf_out) {  // encode_i64: y mod p, or -(|y| mod p)
-    uint64_t e;
-    if (yy >= 0) {
-      e = (uint64_t)yy % GL_P;
-    } else {
-      const uint64_t m = ((uint64_t)(-(yy + 1)) + 1) % GL_P;
-      e = m ? GL_P - m : 0;
-    }
-    yf_out[o] = e;
-  }
-  return true;
-}
 
 struct LwArgs {
   const int64_t* x;
@@ -416,8 +368,25 @@ void linear_witness_dev(lgs_ctx* c, const int64_t* x, size_t rows, size_t inner,
     dy = ar.get<int64_t>(no);
     df = y_field ? ar.get<uint64_t>(no) : nullptr;
   }
-  int* derr = ar.get<int>(1);  // error word
-  LGS_CUDA(cudaMemsetAsync(derr, 0, sizeof(int), st));
+  int* derr = ar.get<int>(2);  // error word, then the tensor path's operand-range flag
+  LGS_CUDA(cudaMemsetAsync(derr, 0, 2 * sizeof(int), st));
+  int herr = 0;
+  bool done = false;
+  if (c->witness_path == 0) {
+    // operands within the limb encodings (every integer GPT-2 layer): the tensor cores
+    linear_witness_tc(c, dx, rows, inner, dw, cols, w_transposed, db, divisor, dq, dr, dy, df,
+                      derr, derr + 1);
+    int flags[2] = {0, 0};
+    LGS_CUDA(cudaMemcpyAsync(flags, derr, sizeof(flags), cudaMemcpyDeviceToHost, st));
+    LGS_CUDA(cudaStreamSynchronize(st));
+    if (flags[0] >= 16)
+      throw DeviceTimeout("linear witness: a bounded device wait gave up (code " +
+                          std::to_string(flags[0]) + ")");
+    done = flags[1] == 0;  // else an operand needs more than its limbs: the CUDA-core kernel
+    if (done) herr = flags[0];
+    else LGS_CUDA(cudaMemsetAsync(derr, 0, 2 * sizeof(int), st));
+  }
+  if (!done) {
   // Few rows (GPT-2 runs 31 positions) leave most SMs idle: split K until there are about two
   // CTAs per SM, each with at least 128 values of K, and sum the exact partials afterwards.
   const size_t tiles = ((cols + LW_TN - 1) / LW_TN) * ((rows + LW_TM - 1) / LW_TM);
@@ -437,6 +406,7 @@ void linear_witness_dev(lgs_ctx* c, const int64_t* x, size_t rows, size_t inner,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LW_SMEM));
   LGS_CUDA(cudaFuncSetAttribute(linear_witness_kernel<false>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LW_SMEM));
+  StageTimer t(c->prof, st, "linear_witness_cores");
   if (split == 1) {
     linear_witness_kernel<true><<<grid, 256, LW_SMEM, st>>>(a);
     LGS_LAUNCH_CHECK();
@@ -448,8 +418,8 @@ void linear_witness_dev(lgs_ctx* c, const int64_t* x, size_t rows, size_t inner,
     linear_witness_finish_kernel<<<blocks, 256, 0, st>>>(a, (unsigned)split);
     LGS_LAUNCH_CHECK();
   }
-  int herr = 0;
   LGS_CUDA(cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  }
   if (!on_device) {
     LGS_CUDA(cudaMemcpyAsync(q, dq, no * 8, cudaMemcpyDeviceToHost, st));
     LGS_CUDA(cudaMemcpyAsync(rem, dr, no * 8, cudaMemcpyDeviceToHost, st));

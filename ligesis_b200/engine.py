@@ -38,6 +38,7 @@ _SIGS = {
     "lgs_engine_free_proof": (None, [C.POINTER(C.c_uint8)]),
     "lgs_engine_pending": (C.c_int, [vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     "lgs_engine_prepare": (C.c_int, [vp, C.POINTER(vp), C.c_size_t]),
+    "lgs_engine_tune": (C.c_int, [vp, C.c_char_p, C.c_uint64]),
 }
 
 
@@ -67,12 +68,19 @@ class JobResult:
 class ProverEngine:
     """`lanes` contexts on `device`; hbm_budget in bytes (0: 90% of free device memory)."""
 
-    def __init__(self, device: int = 0, lanes: int = 4, hbm_budget: int = 0):
+    def __init__(self, device: int = 0, lanes: int = 4, hbm_budget: int = 0, tuned: bool = True):
         lib = _lib()
         h = vp()
         check(lib.lgs_engine_create(int(device), int(lanes), int(hbm_budget), C.byref(h)))
         self.handle, self._lib = h, lib
         self._keep: dict[int, tuple] = {}
+        self.tuning = None
+        if tuned:  # the lanes' launch choices from the autotuner's cache, if it has them
+            from . import autotune
+
+            self.tuning = autotune.lookup_engine(lanes, device)
+            if self.tuning:
+                self.tune(**self.tuning)
 
     def submit(self, pk: ProvingKey, f, z, oracle: RandomOracle) -> int:
         """Queue one commit + prove of f (2^mu BF) at z, starting at the oracle's cursors.
@@ -120,6 +128,12 @@ class ProverEngine:
         pks = list(pks)
         arr = (vp * max(1, len(pks)))(*[pk.handle for pk in pks])
         check(self._lib.lgs_engine_prepare(self.handle, arr, len(pks)))
+
+    def tune(self, **params: int) -> None:
+        """lgs_tune on every lane (hash_ctas, sumcheck_blocks, hash_groups; 0 = default).
+        Call with no job queued or running; prepare again after a sumcheck_blocks change."""
+        for name, value in params.items():
+            check(self._lib.lgs_engine_tune(self.handle, name.encode(), int(value)))
 
     def pending(self) -> tuple[int, int]:
         q, b = C.c_size_t(), C.c_size_t()

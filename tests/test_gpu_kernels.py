@@ -126,3 +126,14 @@ def test_sumcheck_matches_oracle(lgs, orc, d, k):
     r_o, f_o, _ = orc.sumcheck_prove(polys, ch)
     assert np.array_equal(rounds, r_o)
     assert np.array_equal(finals, f_o)
+
+
+def test_rs_alu_rates_measure_the_encodings_arithmetic(lgs):
+    """lgs_rs_alu_rates (the RS encoding's arithmetic floor) runs and gives plausible rates: a
+    radix-8 DFT holds 12 butterflies, so it runs slower than a single multiplication."""
+    import ctypes as C
+
+    ctx = L.Context(0)
+    r8, mul = C.c_double(), C.c_double()
+    L._lib.check(L.load().lgs_rs_alu_rates(ctx.handle, 256, C.byref(r8), C.byref(mul)))
+    assert 1e9 < r8.value < mul.value < 1e14

@@ -159,9 +159,11 @@ def test_linear_witness_arithmetic_paths(lgs, orc, xb, wb, inner):
     """Operand sizes that select each exact path: fused multiply-adds of doubles (GPT-2's
     sizes), 64-bit products with 64-bit sums (40 + 8 and 40 + 15 bits), 32-bit products
     (28 + 28 bits), and 128-bit sums (wide operands whose results still fit an i64)."""
+    ctx = L.Context(0)
+    ctx.tune(witness_path=1)  # the CUDA-core kernel (the tensor cores would take 20 x 15 bits)
     x = _rand(xb + inner, (7, inner), xb)
     w = _rand(wb + inner, (inner, 9), wb)
-    got = ps.linear_witness(x, w, None, 3)
+    got = ps.linear_witness(x, w, None, 3, False, ctx)
     want = orc.linear_witness(x, w, None, 3)
     for g_, w_ in zip(got, want):
         assert np.array_equal(g_, w_)
