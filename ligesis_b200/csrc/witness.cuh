@@ -34,10 +34,17 @@ __device__ __forceinline__ bool lw_finish(const Acc128& s, const int64_t* bias, 
                                           int64_t* y_out, uint64_t* yf_out) {
   if (!fits_i64(s.hi, s.lo)) return false;  // checked_i128_to_i64 of the product
   const int64_t v = (int64_t)s.lo;
-  int64_t q = v / d, rm = v % d;  // floor division: a negative remainder moves q down
-  if (rm < 0) {
-    q -= 1;
-    rm += d;
+  int64_t q, rm;
+  if ((d & (d - 1)) == 0) {  // a power of two (the fixed-point scale): floor division is a shift
+    const int sh = __ffsll(d) - 1;
+    q = v >> sh;
+    rm = v & (d - 1);
+  } else {
+    q = v / d, rm = v % d;  // floor division: a negative remainder moves q down
+    if (rm < 0) {
+      q -= 1;
+      rm += d;
+    }
   }
   const int64_t b = bias ? bias[c] : 0;
   const int64_t yy = (int64_t)((uint64_t)q + (uint64_t)b);

@@ -17,8 +17,9 @@
 // N = NR <= 64 rows) over a K range, in chunks of 128 values of K:
 //   warps 0-7  load W and X from global memory, convert them to limbs in the 128-byte swizzled
 //              K-major tiles of a 2-stage pipeline (the weights are read from HBM exactly once)
-//   warp 8     TMEM allocation and one thread issuing the MMAs (M128 N=NR K32, 6 limb pairs,
-//              4 K steps per chunk) into four accumulators of NR columns
+//   warp 0     also allocates the TMEM and, once all warps have staged a chunk, one of its
+//              threads issues the chunk's MMAs (M128 N=NR K32, 6 limb pairs, 4 K steps) into
+//              four accumulators of NR columns
 //   warps 0-3  afterwards: drain the accumulators, recombine, finish the outputs.
 // When K is split over CTAs (to fill the GPU), each split adds its exact int64 sum into a zeroed
 // buffer and the last CTA of a tile (a counter per tile) finishes it.  Every wait is bounded.
@@ -35,7 +36,7 @@ constexpr int WT_KC = 128;       // K values per chunk (one 128-byte row of a li
 constexpr int WT_LX = 3, WT_LW = 2, WT_NG = WT_LX + WT_LW - 1;
 constexpr int WT_STAGES = 2;
 constexpr int WT_PROD = 256;     // producer threads (warps 0-7)
-constexpr int WT_THREADS = WT_PROD + 32;
+constexpr int WT_THREADS = WT_PROD;
 constexpr int WT_NR_MAX = 64;
 constexpr int64_t WT_OX = (int64_t)1 << 23, WT_OW = (int64_t)1 << 15;
 constexpr size_t WT_A_TILE = (size_t)WT_M * WT_KC;  // bytes of one W limb tile
@@ -63,6 +64,9 @@ struct WtArgs {
   int* err;                 // 1: a result leaves the i64 range; >= 16: a bounded wait gave up
   int* range;               // an operand outside the limb encodings
   long long budget;
+  const uint8_t* xl;        // the X limb tiles of every (row tile, chunk), x_limbs_kernel
+  const uint32_t* xsum;     // sum of x' per (row tile, chunk, row)
+  size_t chunks;            // chunks of 128 values of K in the whole inner dimension
 };
 
 // w' = w + 2^15 of a value in range, 0 for padding (outside the matrix); flags a value that
@@ -102,22 +106,119 @@ __device__ __forceinline__ void store_row(uint8_t* const (&tiles)[L], uint32_t r
   }
 }
 
-__device__ __forceinline__ void ld_pair(const int64_t* p, size_t k, size_t ke, bool row_ok,
-                                        bool vec, int64_t& a, int64_t& b) {
-  a = b = 0;
-  if (!row_ok || k >= ke) return;
-  if (vec && k + 1 < ke) {
-    const longlong2 v = __ldg((const longlong2*)(p + k));
-    a = v.x;
-    b = v.y;
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+// Group q (steps 2q, 2q + 1 of 16) of the W values this thread stages for the chunk at k0:
+//   w transposed (W[c][k]): step s is output column m = 8 s + warp, the values at K offsets
+//     2 lane, 2 lane + 1, 64 + 2 lane, 64 + 2 lane + 1 (two 16-byte loads when vec);
+//   else (W[k][c]): column m = 32 (warp % 4) + lane, K offsets 8 s + 4 (warp / 4) + 0..3.
+// Every address is clamped into the matrix (no branch, so the loads issue back to back);
+// store_w_group zeroes the values outside it.
+template <bool WT, bool VEC>
+__device__ __forceinline__ void load_w_group(const WtArgs& a, size_t c0, size_t k0, size_t ke,
+                                             unsigned warp, unsigned lane, int q,
+                                             int64_t (&v)[8]) {
+  if constexpr (WT) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const size_t c = min(c0 + 8 * (2 * q + i) + warp, a.cols - 1);
+      const int64_t* p = a.w + c * a.inner;
+      const size_t ka = k0 + 2 * lane, kb2 = k0 + 64 + 2 * lane;
+      if constexpr (VEC) {  // inner even: ke - 2 >= k0 is even: both 16-byte loads stay in the row
+        const longlong2 x = __ldg((const longlong2*)(p + min(ka, ke - 2)));
+        const longlong2 y = __ldg((const longlong2*)(p + min(kb2, ke - 2)));
+        v[4 * i] = x.x, v[4 * i + 1] = x.y, v[4 * i + 2] = y.x, v[4 * i + 3] = y.y;
+      } else {
+        v[4 * i] = __ldg(p + min(ka, ke - 1));
+        v[4 * i + 1] = __ldg(p + min(ka + 1, ke - 1));
+        v[4 * i + 2] = __ldg(p + min(kb2, ke - 1));
+        v[4 * i + 3] = __ldg(p + min(kb2 + 1, ke - 1));
+      }
+    }
   } else {
-    a = __ldg(p + k);
-    if (k + 1 < ke) b = __ldg(p + k + 1);
+    const size_t c = min(c0 + 32 * (warp & 3) + lane, a.cols - 1);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const size_t kk = k0 + 8 * (2 * q + i) + 4 * (warp >> 2);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) v[4 * i + j] = __ldg(a.w + min(kk + j, ke - 1) * a.cols + c);
+    }
+  }
+}
+template <bool WT>
+__device__ __forceinline__ void store_w_group(const WtArgs& a, uint8_t* const (&tiles)[WT_LW],
+                                              size_t c0, size_t k0, size_t ke, unsigned warp,
+                                              unsigned lane, int q, const int64_t (&v)[8],
+                                              bool& bad) {
+  if constexpr (WT) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const unsigned m = 8 * (2 * q + i) + warp;
+      const bool ok = c0 + m < a.cols;
+      const size_t ka = k0 + 2 * lane, kb2 = k0 + 64 + 2 * lane;
+      const uint32_t e0 = w_enc(v[4 * i], ok && ka < ke, bad);
+      const uint32_t e1 = w_enc(v[4 * i + 1], ok && ka + 1 < ke, bad);
+      const uint32_t e2 = w_enc(v[4 * i + 2], ok && kb2 < ke, bad);
+      const uint32_t e3 = w_enc(v[4 * i + 3], ok && kb2 + 1 < ke, bad);
+      store_row<WT_LW>(tiles, m, e0, e1, e2, e3);
+    }
+  } else {
+    const unsigned m = 32 * (warp & 3) + lane;
+    const bool ok = c0 + m < a.cols;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const unsigned kk = 8 * (2 * q + i) + 4 * (warp >> 2);
+      uint32_t w0 = 0, w1 = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const uint32_t e = w_enc(v[4 * i + j], ok && k0 + kk + j < ke, bad);
+        w0 |= (e & 255u) << (8 * j);
+        w1 |= ((e >> 8) & 255u) << (8 * j);
+      }
+      *(uint32_t*)(tiles[0] + tc::sw128_off(m, kk)) = w0;
+      *(uint32_t*)(tiles[1] + tc::sw128_off(m, kk)) = w1;
+    }
   }
 }
 
-__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+// The X side of every chunk, once per launch: for row tile blockIdx.y and the chunk of K values
+// [128 blockIdx.x, 128 blockIdx.x + 128), the three limb tiles exactly as the main kernel's
+// shared memory holds them (rows below nrv data, row nrv all ones in limb 0, the rest zero), and
+// each data row's sum of x' over the chunk.  A value outside 24 bits sets *range.
+__global__ void __launch_bounds__(256) x_limbs_kernel(const WtArgs a, uint8_t* __restrict__ xl,
+                                                      uint32_t* __restrict__ xsum) {
+  const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nr = a.nr;
+  const size_t chunks = gridDim.x, chunk = blockIdx.x, tile = blockIdx.y;
+  const size_t r0 = tile * a.nrv, k0 = chunk * WT_KC;
+  uint8_t* base = xl + (tile * chunks + chunk) * (size_t)(WT_LX * nr * WT_KC);
+  uint8_t* const tiles[WT_LX] = {base, base + nr * WT_KC, base + 2 * nr * WT_KC};
+  bool bad = false;
+  for (unsigned r = warp; r < nr; r += 8) {
+    const size_t gr = r0 + r;
+    const bool data = r < a.nrv && gr < a.rows;
+    uint32_t e[4] = {0, 0, 0, 0};
+    if (data) {
+      const int64_t* p = a.x + gr * a.inner;
+      const size_t ks[4] = {k0 + 2 * lane, k0 + 2 * lane + 1, k0 + 64 + 2 * lane,
+                            k0 + 64 + 2 * lane + 1};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const bool valid = ks[i] < a.inner;
+        e[i] = x_enc(valid ? __ldg(p + ks[i]) : 0, valid, bad);
+      }
+      const unsigned part = __reduce_add_sync(0xffffffffu, e[0] + e[1] + e[2] + e[3]);
+      if (lane == 0) xsum[(tile * chunks + chunk) * nr + r] = part;
+    } else {
+      if (r == a.nrv) e[0] = e[1] = e[2] = e[3] = 1;
+      if (lane == 0) xsum[(tile * chunks + chunk) * nr + r] = 0;
+    }
+    store_row<WT_LX>(tiles, r, e[0], e[1], e[2], e[3]);
+  }
+  if (bad) atomicExch(a.range, 1);
+}
 
+// WT: W is cols x inner (else inner x cols); VEC: W rows start 16-byte aligned (16-byte loads).
+template <bool WT, bool VEC>
 __global__ void __launch_bounds__(WT_THREADS, 2) linear_witness_tc_kernel(const WtArgs a) {
   extern __shared__ uint8_t wt_smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)wt_smem_raw + 1023) & ~(uintptr_t)1023);
@@ -125,10 +226,11 @@ __global__ void __launch_bounds__(WT_THREADS, 2) linear_witness_tc_kernel(const 
   const size_t stage_bytes = wt_stage_bytes(nr);
   unsigned long long* sx = (unsigned long long*)(smem + WT_STAGES * stage_bytes);
   uint64_t* bars = (uint64_t*)(sx + WT_NR_MAX);
-  uint32_t* tmem_holder = (uint32_t*)(bars + 2 * WT_STAGES + 2);
+  uint32_t* tmem_holder = (uint32_t*)(bars + 3 * WT_STAGES + 2);
   const uint32_t full0 = tc::smem_u32(&bars[0]), empty0 = tc::smem_u32(&bars[WT_STAGES]);
-  const uint32_t accf = tc::smem_u32(&bars[2 * WT_STAGES]);
-  const uint32_t drain = tc::smem_u32(&bars[2 * WT_STAGES + 1]);
+  const uint32_t xbar0 = tc::smem_u32(&bars[2 * WT_STAGES]);  // the X tiles' bulk copies
+  const uint32_t accf = tc::smem_u32(&bars[3 * WT_STAGES]);
+  const uint32_t drain = tc::smem_u32(&bars[3 * WT_STAGES + 1]);
   __shared__ volatile int s_fail;
   __shared__ int s_last;
   const unsigned tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -142,13 +244,13 @@ __global__ void __launch_bounds__(WT_THREADS, 2) linear_witness_tc_kernel(const 
     for (int s = 0; s < WT_STAGES; ++s) {
       tc::mbar_init(full0 + 8 * s, WT_PROD);
       tc::mbar_init(empty0 + 8 * s, 1);
+      tc::mbar_init(xbar0 + 8 * s, 1);
     }
     tc::mbar_init(accf, 1);
     tc::mbar_init(drain, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (tid < WT_NR_MAX) sx[tid] = 0;
-  if (warp == 8) {
+  if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      tc::smem_u32(tmem_holder)),
                  "r"(tcols)
@@ -159,122 +261,106 @@ __global__ void __launch_bounds__(WT_THREADS, 2) linear_witness_tc_kernel(const 
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_holder;
+  unsigned x_issued = 0;  // thread 0: X tile copies issued
 
-  if (warp == 8) {
-    // ---- MMA issuer: per chunk 4 K steps x 6 limb pairs; pair (i, j) into accumulator i + j
-    if (lane == 0) {
-      const uint32_t idesc = tc::idesc_u8(WT_M, nr);
-      bool ok = true;
-      for (unsigned t = 0; t < nchunks && ok; ++t) {
-        const unsigned s = t % WT_STAGES;
-        if (!tc::mbar_wait(full0 + 8 * s, (t / WT_STAGES) & 1, &s_fail, a.budget)) {
-          if (!s_fail) tc::flag_failure(&s_fail, a.err, 16);
-          ok = false;
-          break;
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t sa = tc::smem_u32(smem + s * stage_bytes);
-        const uint32_t sb = sa + (uint32_t)(WT_LW * WT_A_TILE);
-#pragma unroll
-        for (int ks = 0; ks < 4; ++ks)
-#pragma unroll
-          for (int i = 0; i < WT_LX; ++i)
-#pragma unroll
-            for (int j = 0; j < WT_LW; ++j) {
-              // the first pair of each accumulator in the first K step overwrites it
-              const bool first = t == 0 && ks == 0 && (j == 1 || i == 0) && !(i == 2 && j == 0);
-              tc::mma_i8(tmem + (uint32_t)((i + j) * nr),
-                         tc::sw128_desc(sa + (uint32_t)(j * WT_A_TILE) + 32 * ks),
-                         tc::sw128_desc(sb + (uint32_t)(i * nr * WT_KC) + 32 * ks), idesc,
-                         first ? 0u : 1u);
-            }
-        tc::mma_commit(empty0 + 8 * s);
-      }
-      if (ok) tc::mma_commit(accf);
-      // every MMA issued so far has completed once this arrives: wait before the TMEM is freed
-      tc::mma_commit(drain);
-      if (!tc::mbar_wait_drain(drain, 0)) atomicExch(a.err, 17);
-    }
-  } else {
-    // ---- producers: W tile (128 output columns) and X tile (nr rows) of each chunk as limbs
+  {
+    // ---- producers: the W tile (128 output columns) of each chunk as limbs, in eight groups of
+    // eight values per thread; the loads run three groups ahead of the stores (a ring of four
+    // register buffers, across chunk boundaries).  Thread 0 also fetches the chunk's X limb
+    // tiles (made once per launch by x_limbs_kernel) with one bulk copy.
     bool bad = false;
-    const bool wvec = a.wt && (a.inner % 2 == 0) && (((uintptr_t)a.w & 15) == 0);
-    const bool xvec = (a.inner % 2 == 0) && (((uintptr_t)a.x & 15) == 0);
+    const size_t xt_bytes = (size_t)WT_LX * nr * WT_KC;
+    int64_t b0[8], b1[8], b2[8], b3[8];
+    load_w_group<WT, VEC>(a, c0, kb, ke, warp, lane, 0, b0);
+    load_w_group<WT, VEC>(a, c0, kb, ke, warp, lane, 1, b1);
+    load_w_group<WT, VEC>(a, c0, kb, ke, warp, lane, 2, b2);
     for (unsigned t = 0; t < nchunks; ++t) {
       const unsigned s = t % WT_STAGES;
-      if (t >= WT_STAGES &&
-          !tc::mbar_wait(empty0 + 8 * s, ((t / WT_STAGES) - 1) & 1, &s_fail, a.budget)) {
-        if (!s_fail) tc::flag_failure(&s_fail, a.err, 18);
-        break;
+      const size_t k0 = kb + (size_t)t * WT_KC, k1 = k0 + WT_KC;
+      const bool more = t + 1 < nchunks;
+      if (t >= WT_STAGES) {  // one lane waits, so the warp decides as one (it shuffles below)
+        bool ok = true;
+        if (lane == 0) ok = tc::mbar_wait(empty0 + 8 * s, ((t / WT_STAGES) - 1) & 1, &s_fail,
+                                          a.budget);
+        if (!__shfl_sync(0xffffffffu, ok, 0)) {
+          if (lane == 0 && !s_fail) tc::flag_failure(&s_fail, a.err, 18);
+          break;
+        }
       }
       uint8_t* st = smem + s * stage_bytes;
       uint8_t* const wt_tiles[WT_LW] = {st, st + WT_A_TILE};
-      uint8_t* xb = st + WT_LW * WT_A_TILE;
-      uint8_t* const x_tiles[WT_LX] = {xb, xb + nr * WT_KC, xb + 2 * nr * WT_KC};
-      const size_t k0 = kb + (size_t)t * WT_KC;
-      if (a.wt) {  // W[c][k]: warp `warp` stages rows m = 8 step + warp
-#pragma unroll 4
-        for (int step = 0; step < WT_M / 8; ++step) {
-          const unsigned m = 8 * step + warp;
-          const size_t c = c0 + m;
-          const bool ok = c < a.cols;
-          const int64_t* p = a.w + (ok ? c : 0) * a.inner;
-          int64_t v0, v1, v2, v3;
-          ld_pair(p, k0 + 2 * lane, ke, ok, wvec, v0, v1);
-          ld_pair(p, k0 + 64 + 2 * lane, ke, ok, wvec, v2, v3);
-          const uint32_t e0 = w_enc(v0, ok && k0 + 2 * lane < ke, bad);
-          const uint32_t e1 = w_enc(v1, ok && k0 + 2 * lane + 1 < ke, bad);
-          const uint32_t e2 = w_enc(v2, ok && k0 + 64 + 2 * lane < ke, bad);
-          const uint32_t e3 = w_enc(v3, ok && k0 + 64 + 2 * lane + 1 < ke, bad);
-          store_row<WT_LW>(wt_tiles, m, e0, e1, e2, e3);
-        }
-      } else {  // W[k][c]: lane = output column, four consecutive k per thread
-        const unsigned m = 32 * (warp & 3) + lane;
-        const size_t c = c0 + m;
-        const bool ok = c < a.cols;
-#pragma unroll 4
-        for (int step = 0; step < WT_KC / 8; ++step) {
-          const unsigned kk = 8 * step + 4 * (warp >> 2);
-          uint32_t w0 = 0, w1 = 0;
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const size_t k = k0 + kk + i;
-            const bool valid = ok && k < ke;
-            const int64_t v = valid ? __ldg(a.w + k * a.cols + c) : 0;
-            const uint32_t e = w_enc(v, valid, bad);
-            w0 |= (e & 255u) << (8 * i);
-            w1 |= ((e >> 8) & 255u) << (8 * i);
-          }
-          *(uint32_t*)(wt_tiles[0] + tc::sw128_off(m, kk)) = w0;
-          *(uint32_t*)(wt_tiles[1] + tc::sw128_off(m, kk)) = w1;
-        }
+      if (tid == 0) {
+        const uint32_t bar = xbar0 + 8 * s;
+        tc::mbar_arrive_tx(bar, (uint32_t)xt_bytes);
+        x_issued = t + 1;
+        const uint8_t* src = a.xl + (blockIdx.y * a.chunks + kb / WT_KC + t) * xt_bytes;
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+            "[%3];" ::"r"(tc::smem_u32(st + WT_LW * WT_A_TILE)),
+            "l"(src), "r"((uint32_t)xt_bytes), "r"(bar)
+            : "memory");
       }
-      // X tile: rows below nrv are data, row nrv is ones (limb 0), the rest zero
-      for (unsigned r = warp; r < nr; r += 8) {
-        const size_t gr = r0 + r;
-        const bool data = r < a.nrv && gr < a.rows;
-        uint32_t e0 = 0, e1 = 0, e2 = 0, e3 = 0;
-        if (data) {
-          const int64_t* p = a.x + gr * a.inner;
-          int64_t v0, v1, v2, v3;
-          ld_pair(p, k0 + 2 * lane, ke, true, xvec, v0, v1);
-          ld_pair(p, k0 + 64 + 2 * lane, ke, true, xvec, v2, v3);
-          e0 = x_enc(v0, k0 + 2 * lane < ke, bad);
-          e1 = x_enc(v1, k0 + 2 * lane + 1 < ke, bad);
-          e2 = x_enc(v2, k0 + 64 + 2 * lane < ke, bad);
-          e3 = x_enc(v3, k0 + 64 + 2 * lane + 1 < ke, bad);
-          const unsigned part = __reduce_add_sync(0xffffffffu, e0 + e1 + e2 + e3);
-          if (lane == 0) sx[r] += part;
-        } else if (r == a.nrv) {
-          e0 = e1 = e2 = e3 = 1;
-        }
-        store_row<WT_LX>(x_tiles, r, e0, e1, e2, e3);
-      }
+      load_w_group<WT, VEC>(a, c0, k0, ke, warp, lane, 3, b3);
+      store_w_group<WT>(a, wt_tiles, c0, k0, ke, warp, lane, 0, b0, bad);
+      load_w_group<WT, VEC>(a, c0, k0, ke, warp, lane, 4, b0);
+      store_w_group<WT>(a, wt_tiles, c0, k0, ke, warp, lane, 1, b1, bad);
+      load_w_group<WT, VEC>(a, c0, k0, ke, warp, lane, 5, b1);
+      store_w_group<WT>(a, wt_tiles, c0, k0, ke, warp, lane, 2, b2, bad);
+      load_w_group<WT, VEC>(a, c0, k0, ke, warp, lane, 6, b2);
+      store_w_group<WT>(a, wt_tiles, c0, k0, ke, warp, lane, 3, b3, bad);
+      load_w_group<WT, VEC>(a, c0, k0, ke, warp, lane, 7, b3);
+      store_w_group<WT>(a, wt_tiles, c0, k0, ke, warp, lane, 4, b0, bad);
+      if (more) load_w_group<WT, VEC>(a, c0, k1, ke, warp, lane, 0, b0);
+      store_w_group<WT>(a, wt_tiles, c0, k0, ke, warp, lane, 5, b1, bad);
+      if (more) load_w_group<WT, VEC>(a, c0, k1, ke, warp, lane, 1, b1);
+      store_w_group<WT>(a, wt_tiles, c0, k0, ke, warp, lane, 6, b2, bad);
+      if (more) load_w_group<WT, VEC>(a, c0, k1, ke, warp, lane, 2, b2);
+      store_w_group<WT>(a, wt_tiles, c0, k0, ke, warp, lane, 7, b3, bad);
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       tc::mbar_arrive(full0 + 8 * s);
+      if (warp == 0) {
+        // MMA issue: once every producer has staged the chunk, 4 K steps x 6 limb pairs, pair
+        // (i, j) into accumulator i + j; the commit frees the stage
+        bool ok = true;
+        if (lane == 0)
+          ok = tc::mbar_wait(full0 + 8 * s, (t / WT_STAGES) & 1, &s_fail, a.budget) &&
+               tc::mbar_wait(xbar0 + 8 * s, (t / WT_STAGES) & 1, &s_fail, a.budget);
+        if (!__shfl_sync(0xffffffffu, ok, 0)) {
+          if (lane == 0 && !s_fail) tc::flag_failure(&s_fail, a.err, 16);
+          break;
+        }
+        if (lane == 0) {
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t idesc = tc::idesc_u8(WT_M, nr);
+          const uint32_t sa = tc::smem_u32(st);
+          const uint32_t sb = sa + (uint32_t)(WT_LW * WT_A_TILE);
+#pragma unroll
+          for (int ks = 0; ks < 4; ++ks)
+#pragma unroll
+            for (int i = 0; i < WT_LX; ++i)
+#pragma unroll
+              for (int j = 0; j < WT_LW; ++j) {
+                // the first pair of each accumulator in the first K step overwrites it
+                const bool first = t == 0 && ks == 0 && (j == 1 || i == 0);
+                tc::mma_i8(tmem + (uint32_t)((i + j) * nr),
+                           tc::sw128_desc(sa + (uint32_t)(j * WT_A_TILE) + 32 * ks),
+                           tc::sw128_desc(sb + (uint32_t)(i * nr * WT_KC) + 32 * ks), idesc,
+                           first ? 0u : 1u);
+              }
+          tc::mma_commit(empty0 + 8 * s);
+          if (t + 1 == nchunks) tc::mma_commit(accf);
+        }
+        __syncwarp();
+      }
     }
     if (bad) atomicExch(a.range, 1);
-    // every producer's sum of x' is in shared memory before the epilogue reads it
+    // this CTA's sums of x' per row, from the per-chunk sums
+    if (tid < nr) {
+      unsigned long long sum = 0;
+      for (unsigned t = 0; t < nchunks; ++t)
+        sum += a.xsum[(blockIdx.y * a.chunks + kb / WT_KC + t) * nr + tid];
+      sx[tid] = sum;
+    }
     asm volatile("bar.sync 2, 256;" ::: "memory");
     if (warp < 4) {
       // ---- epilogue (warps 0-3; TMEM lanes 32 warp .. 32 warp + 31 = output columns)
@@ -363,9 +449,19 @@ __global__ void __launch_bounds__(WT_THREADS, 2) linear_witness_tc_kernel(const 
       }
     }
   }
+  if (tid == 0) {
+    // only the newest copy of each stage can still be in flight (an older one was consumed
+    // before its stage was refilled): wait for those before the CTA may exit
+    for (unsigned g = x_issued > WT_STAGES ? x_issued - WT_STAGES : 0; g < x_issued; ++g)
+      if (!tc::mbar_wait_drain(xbar0 + 8 * (g % WT_STAGES), (g / WT_STAGES) & 1))
+        atomicExch(a.err, 20);
+    // every MMA issued so far has completed once this arrives: wait before the TMEM is freed
+    tc::mma_commit(drain);
+    if (!tc::mbar_wait_drain(drain, 0)) atomicExch(a.err, 17);
+  }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 8) {
+  if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tcols)
                  : "memory");
@@ -384,21 +480,27 @@ void linear_witness_tc(lgs_ctx* c, const int64_t* dx, size_t rows, size_t inner,
   const unsigned nrv = (unsigned)((rows + ntr - 1) / ntr);
   const unsigned nr = (nrv + 1 + 15) / 16 * 16;
   const size_t smem = wt_smem_bytes(nr);
-  auto k = linear_witness_tc_kernel;
+  const bool vec = w_transposed && (inner % 2 == 0) && (((uintptr_t)dw & 15) == 0);
+  auto k = w_transposed ? (vec ? linear_witness_tc_kernel<true, true>
+                               : linear_witness_tc_kernel<true, false>)
+                        : linear_witness_tc_kernel<false, false>;
   LGS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // two CTAs per SM need the largest shared-memory carveout
+  LGS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                (int)cudaSharedmemCarveoutMaxShared));
   int per_sm = 1, nsm = 148;
   LGS_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
   LGS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, WT_THREADS, smem));
   const size_t slots = (size_t)std::max(1, per_sm) * nsm;
   const size_t mt = (cols + WT_M - 1) / WT_M, tiles = mt * ntr;
   const size_t chunks = (inner + WT_KC - 1) / WT_KC;
-  // K splits: the fewest that minimise (waves of CTAs) x (chunks per CTA), and enough that no
-  // CTA sums more than WT_KMAX values of K
+  // K splits: the fewest that minimise (waves of CTAs) x (chunks per CTA + about one chunk of
+  // fixed cost per CTA), and enough that no CTA sums more than WT_KMAX values of K
   const size_t min_split = (inner + WT_KMAX - 1) / WT_KMAX;
   size_t split = min_split, best = SIZE_MAX;
   for (size_t sp = min_split; sp <= std::min<size_t>(chunks, 64); ++sp) {
     const size_t per = (chunks + sp - 1) / sp;
-    const size_t cost = ((tiles * sp + slots - 1) / slots) * per;
+    const size_t cost = ((tiles * sp + slots - 1) / slots) * (per + 1);
     if (cost < best) best = cost, split = sp;
   }
   const size_t kchunk = (chunks + split - 1) / split * WT_KC;
@@ -414,8 +516,17 @@ void linear_witness_tc(lgs_ctx* c, const int64_t* dx, size_t rows, size_t inner,
     LGS_CUDA(cudaMemsetAsync(a.acc, 0, rows * cols * 8, st));
     LGS_CUDA(cudaMemsetAsync(a.count, 0, tiles * 4, st));
   }
-  const dim3 grid((unsigned)mt, (unsigned)ntr, (unsigned)split);
+  // the X limb tiles and x' sums of every (row tile, chunk); 16-byte aligned arena blocks
+  const size_t xt_bytes = (size_t)WT_LX * nr * WT_KC;
+  uint8_t* xl = ar.get<uint8_t>(ntr * chunks * xt_bytes);
+  uint32_t* xsum = ar.get<uint32_t>(ntr * chunks * nr);
+  a.xl = xl;
+  a.xsum = xsum;
+  a.chunks = chunks;
   StageTimer t(c->prof, st, "linear_witness_tc");
+  x_limbs_kernel<<<dim3((unsigned)chunks, (unsigned)ntr), 256, 0, st>>>(a, xl, xsum);
+  LGS_LAUNCH_CHECK();
+  const dim3 grid((unsigned)mt, (unsigned)ntr, (unsigned)split);
   k<<<grid, WT_THREADS, smem, st>>>(a);
   LGS_LAUNCH_CHECK();
 }
