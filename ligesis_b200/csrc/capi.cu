@@ -131,6 +131,7 @@ void lgs_ctx_destroy(lgs_ctx* ctx) {
   ctx->arena.mem.release();
   ctx->tw.release();
   ctx->rs_tw.release();
+  ctx->hash_scr.release();
   ctx->err.release();
   if (ctx->st) cudaStreamSynchronize(ctx->st);
   for (int i = 0; i < lgs_ctx::NSIDE; ++i) {
@@ -667,8 +668,10 @@ lgs_status lgs_subset_sum_hash(lgs_ctx* ctx, const uint64_t* A, size_t m, const 
     alimb_from_a(dA, dL, W, ctx->st);
     alignas(64) unsigned char tmap[128];
     make_alimb_tmap(dL, W, tmap);
+    const unsigned splits = subset_sum_hash_splits(cp, (unsigned)m, ctx->hash_ctas);
+    u64* slices = splits > 1 ? ctx->arena.get<u64>((size_t)splits * DIGEST_ROWS * cp) : nullptr;
     subset_sum_hash_tc(tmap, dC, dH, dN, (unsigned)m, cp, ctx->err.as<int>(), ctx->st,
-                       ctx->wait_cycles);
+                       ctx->wait_cycles, ctx->hash_ctas, 0, 0, 2, slices);
     LGS_CUDA(cudaMemcpy2DAsync(H, cols * 8, dH, cp * 8, cols * 8, DIGEST_ROWS,
                                cudaMemcpyDeviceToHost, ctx->st));
     int err = 0;

@@ -35,6 +35,7 @@ namespace lgs {
 
 namespace {
 constexpr int TC_N = 256;
+constexpr int H_ROWS = 32;  // digest rows (C)
 constexpr int TC_KB = 128;
 constexpr int TC_STAGES = 3;
 constexpr int A_TILE = 256 * TC_KB;
@@ -92,7 +93,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     hash_tc_kernel(const __grid_constant__ CUtensorMap tmap_a, const u64* __restrict__ cw,
                    u64* __restrict__ H, u32* __restrict__ leaves, unsigned m, size_t two_n,
                    int* __restrict__ err, long long budget, unsigned c0, unsigned nck,
-                   int mode) {
+                   int mode, unsigned splits) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint32_t* Ss = (uint32_t*)(smem + TC_STAGES * STAGE_BYTES);
@@ -106,8 +107,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   const unsigned tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   // K chunks (pairs of codeword rows) c0 .. c0 + nck - 1 of this launch; mode bit 0: add the
   // partial digest to H (else write it), bit 1: hash the leaves of the finished H.
-  const unsigned ntiles = (unsigned)(two_n / TC_N);
-  const unsigned my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  // Work units: (tile, split) with unit u = tile + ntiles * split; split sp sums the K chunks
+  // c0 + sp nck .. c0 + sp nck + nck - 1 into its own digest slice H + sp * 32 * two_n (the
+  // host sums the slices when splits > 1).  "tiles" below are units.
+  const unsigned ntiles = (unsigned)(two_n / TC_N), nunits = ntiles * splits;
+  const unsigned my_tiles = blockIdx.x < nunits ? (nunits - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  auto unit_tile = [&](unsigned t) { return (blockIdx.x + t * gridDim.x) % ntiles; };
+  auto unit_split = [&](unsigned t) { return (blockIdx.x + t * gridDim.x) / ntiles; };
   __shared__ volatile int s_fail;
 
   if (tid == 0) {
@@ -140,7 +146,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     if (lane == 0) {
       unsigned issued = 0;
       for (unsigned f = 0; f < nfill; ++f) {
-        const unsigned s = f % TC_STAGES, c = c0 + f % nck;
+        const unsigned s = f % TC_STAGES, c = c0 + unit_split(f / nck) * nck + f % nck;
         if (f >= TC_STAGES &&
             !mbar_wait(empty0 + 8 * s, ((f / TC_STAGES) - 1) & 1, &s_fail, budget)) {
           if (!s_fail) flag_failure(&s_fail, err, 1);
@@ -207,8 +213,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     const unsigned pt = tid - 64;
     auto load_fill = [&](unsigned f, u64 (&w)[4]) {
       if (f >= nfill) return;
-      const unsigned tl = f / nck, c = c0 + f % nck;
-      const size_t j0 = (size_t)(blockIdx.x + tl * gridDim.x) * TC_N;
+      const unsigned tl = f / nck, c = c0 + unit_split(tl) * nck + f % nck;
+      const size_t j0 = (size_t)unit_tile(tl) * TC_N;
       const bool two = 2 * c + 1 < m;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
@@ -262,7 +268,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     const uint32_t lane_off = (uint32_t)(32 * quarter) << 16;
     const unsigned mrow = 32 * quarter + lane;
     for (unsigned t = 0; t < my_tiles; ++t) {
-      const size_t j0 = (size_t)(blockIdx.x + t * gridDim.x) * TC_N;
+      const size_t j0 = (size_t)unit_tile(t) * TC_N;
+      u64* const Hs = H + (size_t)unit_split(t) * H_ROWS * two_n;  // this split's slice
       const bool got = mbar_wait(acc_full, t & 1, &s_fail, budget);
       if (!epi_all(got)) {
         if (!s_fail) flag_failure(&s_fail, err, 5);
@@ -292,7 +299,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           const u64 b = (u64)hi4.x + ((u64)hi4.y << 8) + ((u64)hi4.z << 16) + ((u64)hi4.w << 24);
           const u64 lo = a + (b << 32);
           const u64 hi = (b >> 32) + (lo < a ? 1 : 0);
-          u64* hp = H + (size_t)r * two_n + j0 + EPI_COLS * q + col;
+          u64* hp = Hs + (size_t)r * two_n + j0 + EPI_COLS * q + col;
           const u64 v = gl_reduce(lo, hi);
           *hp = (mode & 1) ? gl_add(__ldcg(hp), v) : v;
         }
@@ -460,9 +467,65 @@ void make_alimb_tmap(const uint8_t* alimb, size_t W, void* tmap_out) {
 
 size_t tensor_map_bytes() { return sizeof(CUtensorMap); }
 
+namespace {
+// Sums the split slices of the digest (H = sum of slices, plus the old H in mode bit 0) and, in
+// mode bit 1, hashes each finished column as its Merkle leaf, one thread per column.
+__global__ void __launch_bounds__(256) hash_combine_kernel(const u64* __restrict__ Hp,
+                                                           unsigned splits, u64* __restrict__ H,
+                                                           u32* __restrict__ leaves, size_t two_n,
+                                                           int mode) {
+  const size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= two_n) return;
+  u64 v[H_ROWS];
+#pragma unroll
+  for (int r = 0; r < H_ROWS; ++r) {
+    u64 acc = (mode & 1) ? H[(size_t)r * two_n + j] : 0;
+    for (unsigned sp = 0; sp < splits; ++sp)
+      acc = gl_add(acc, __ldcs(Hp + ((size_t)sp * H_ROWS + r) * two_n + j));
+    H[(size_t)r * two_n + j] = acc;
+    v[r] = acc;
+  }
+  if (!(mode & 2)) return;
+  u32 cv[8];
+  b3_init(cv);
+#pragma unroll
+  for (int blk = 0; blk < 4; ++blk) {
+    u32 wd[16];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      wd[2 * q] = (u32)v[blk * 8 + q];
+      wd[2 * q + 1] = (u32)(v[blk * 8 + q] >> 32);
+    }
+    const u32 flags = (blk == 0 ? B3_CHUNK_START : 0) | (blk == 3 ? (B3_CHUNK_END | B3_ROOT) : 0);
+    b3_compress(cv, wd, 64, flags);
+  }
+  uint4* lp = (uint4*)(leaves + j * 8);
+  lp[0] = make_uint4(cv[0], cv[1], cv[2], cv[3]);
+  lp[1] = make_uint4(cv[4], cv[5], cv[6], cv[7]);
+}
+
+unsigned hash_ctas_for(unsigned max_ctas) {
+  int dev = 0, sms = 0;
+  LGS_CUDA(cudaGetDevice(&dev));
+  LGS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  return max_ctas ? std::min<unsigned>(max_ctas, (unsigned)std::max(sms, 1))
+                  : (unsigned)std::max(sms, 1);
+}
+}  // namespace
+
+unsigned subset_sum_hash_splits(size_t two_n, unsigned rows, unsigned max_ctas) {
+  const size_t ntiles = two_n / TC_N, ctas = hash_ctas_for(max_ctas);
+  const unsigned nck = (rows + 1) / 2;
+  unsigned sp = 1;
+  // halve the K chunks of a unit while that still leaves CTAs idle and units of >= 8 chunks
+  while (ntiles * sp * 2 <= ctas && nck % (sp * 2) == 0 && nck / (sp * 2) >= 8) sp *= 2;
+  return sp;
+}
+
 void subset_sum_hash_tc(const void* tmap, const u64* cw, u64* H, u32* leaves, unsigned m,
                         size_t two_n, int* err, cudaStream_t st, uint64_t wait_cycles,
-                        unsigned max_ctas, unsigned row0, unsigned rows, int mode) {
+                        unsigned max_ctas, unsigned row0, unsigned rows, int mode,
+                        u64* split_scratch) {
   if (two_n % TC_N) throw ShapeError("hash: 2n must be a multiple of 256");
   if (m == 0 || m > 8192) throw ShapeError("hash: 1 <= m <= 8192");
   if (rows == 0) rows = m - row0;
@@ -470,18 +533,26 @@ void subset_sum_hash_tc(const void* tmap, const u64* cw, u64* H, u32* leaves, un
     throw ShapeError("hash: row range must start and end on chunks of two rows");
   LGS_CUDA(cudaFuncSetAttribute(hash_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 SMEM_BYTES));
-  int dev = 0, sms = 0;
-  LGS_CUDA(cudaGetDevice(&dev));
-  LGS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  const size_t ntiles = two_n / TC_N;
-  const size_t ctas = max_ctas ? std::min<size_t>(max_ctas, (size_t)std::max(sms, 1))
-                              : (size_t)std::max(sms, 1);
-  const unsigned grid = (unsigned)std::min<size_t>(ntiles, ctas);
+  const size_t ntiles = two_n / TC_N, ctas = hash_ctas_for(max_ctas);
+  const unsigned nck = (rows + 1) / 2;
+  // Few column tiles (square shapes): split K over CTAs into digest slices, summed afterwards
+  const unsigned splits = split_scratch ? subset_sum_hash_splits(two_n, rows, max_ctas) : 1;
+  const unsigned grid = (unsigned)std::min<size_t>(ntiles * splits, ctas);
   const long long budget =
       wait_cycles ? (long long)std::min<uint64_t>(wait_cycles, (uint64_t)WAIT_CYCLES) : WAIT_CYCLES;
-  hash_tc_kernel<<<grid, NTHREADS, SMEM_BYTES, st>>>(*(const CUtensorMap*)tmap, cw, H, leaves, m,
-                                                     two_n, err, budget, row0 / 2,
-                                                     (rows + 1) / 2, mode);
+  if (splits == 1) {
+    hash_tc_kernel<<<grid, NTHREADS, SMEM_BYTES, st>>>(*(const CUtensorMap*)tmap, cw, H, leaves,
+                                                       m, two_n, err, budget, row0 / 2, nck, mode,
+                                                       1u);
+    LGS_LAUNCH_CHECK();
+    return;
+  }
+  hash_tc_kernel<<<grid, NTHREADS, SMEM_BYTES, st>>>(*(const CUtensorMap*)tmap, cw, split_scratch,
+                                                     leaves, m, two_n, err, budget, row0 / 2,
+                                                     nck / splits, 0, splits);
+  LGS_LAUNCH_CHECK();
+  hash_combine_kernel<<<(unsigned)cdiv(two_n, 256), 256, 0, st>>>(split_scratch, splits, H,
+                                                                 leaves, two_n, mode);
   LGS_LAUNCH_CHECK();
 }
 

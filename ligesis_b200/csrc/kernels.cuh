@@ -44,7 +44,11 @@ size_t tensor_map_bytes();
 void subset_sum_hash_tc(const void* tmap, const u64* cw, u64* H, u32* leaves, unsigned m,
                         size_t two_n, int* err, cudaStream_t st, uint64_t wait_cycles = 0,
                         unsigned max_ctas = 0, unsigned row0 = 0, unsigned rows = 0,
-                        int mode = 2);
+                        int mode = 2, u64* split_scratch = nullptr);
+// When the codeword has fewer 256-column tiles than CTAs, the hash splits its K rows over CTAs
+// into this many digest slices (a power of two); split_scratch must then hold splits x 32 x two_n
+// values (splits == 1: none needed).
+unsigned subset_sum_hash_splits(size_t two_n, unsigned rows, unsigned max_ctas = 0);
 // Dense tcgen05 kind::i8 throughput (TOP/s) of back-to-back M128 N256 K32 MMAs on every SM.
 double i8_tensor_peak_tops(unsigned iters, int* err, cudaStream_t st);
 

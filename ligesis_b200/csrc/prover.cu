@@ -417,9 +417,18 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
   LGS_CUDA(cudaEventRecord(c->ev_cw, c->st));
   LGS_CUDA(cudaStreamWaitEvent(c->hs, c->ev_cw, 0));
   if (!hashed) {
+    // digest slices of a split hash (few column tiles) live on the hash stream only
+    const unsigned splits = subset_sum_hash_splits(two_n, (unsigned)m, c->hash_ctas);
+    u64* slices = nullptr;
+    if (splits > 1) {
+      const size_t bytes = (size_t)splits * DIGEST_ROWS * two_n * 8;
+      if (c->hash_scr.bytes < bytes) c->hash_scr.alloc(bytes, c->hs);
+      slices = c->hash_scr.as<u64>();
+    }
     StageTimer t(c->prof, c->hs, "subset_sum_hash");  // H and its Merkle leaf hashes
     subset_sum_hash_tc(pk->tmap, cd->cw.as<u64>(), cd->H.as<u64>(), cd->nodes.as<u32>(),
-                       (unsigned)m, two_n, c->err.as<int>(), c->hs, c->wait_cycles, c->hash_ctas);
+                       (unsigned)m, two_n, c->err.as<int>(), c->hs, c->wait_cycles, c->hash_ctas,
+                       0, 0, 2, slices);
   }
   {
     StageTimer t(c->prof, c->hs, "merkle_h");

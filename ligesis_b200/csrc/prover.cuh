@@ -258,6 +258,7 @@ struct lgs_ctx {
   cudaEvent_t ev_rs[ROW_BLOCKS] = {};  // RS encoding of row block b done (host-rows commit)
   lgs::DevMem tw;
   lgs::DevMem rs_tw;  // twiddles of the row RS encoding (rs_dft.cu)
+  lgs::DevMem hash_scr;  // digest slices of a split subset-sum hash (used on hs only)
   lgs::Arena arena;
   lgs::Profiler prof;
   // Profile level 2: event-record nodes at the prove's branch boundaries (captured into its

@@ -72,6 +72,23 @@ def test_subset_sum_hash_many_tiles_per_cta(lgs, orc, m, cols):
     assert np.array_equal(got, orc.hash_columns(A, cw))
 
 
+@pytest.mark.parametrize("m,cols,hash_ctas", [(1000, 512, 0), (999, 300, 0), (2048, 256, 0),
+                                               (4096, 1024, 0), (512, 1024, 37)])
+def test_subset_sum_hash_split_over_k(lgs, orc, m, cols, hash_ctas):
+    """Few column tiles and many rows (the square commit shapes): the K rows are split over CTAs
+    into digest slices that a second kernel sums and hashes; also with a CTA cap and an odd row
+    count (which keeps a single slice)."""
+    A = rng.field_elements(2200 + m, 32 * 64 * m).reshape(32, 64 * m)
+    cw = rng.field_elements(3200 + m, m * cols).reshape(m, cols)
+    from ligesis_b200._lib import Context, check, load, ptr64
+
+    ctx = Context(0)
+    ctx.tune(hash_ctas=hash_ctas)
+    got = np.zeros((32, cols), dtype=np.uint64)
+    check(load().lgs_subset_sum_hash(ctx.handle, ptr64(A), m, ptr64(cw), cols, ptr64(got)))
+    assert np.array_equal(got, orc.hash_columns(A, cw))
+
+
 def test_subset_sum_hash_extremes(lgs, orc):
     # every bit set and every limb 0xff-heavy: the largest int32 limb sums the kernel sees
     m, cols = 128, 256
