@@ -537,7 +537,7 @@ def rs_alu_floor(lib, ctx, log_m: int, log_n: int, measured_ms: float) -> dict:
                     "encoding's butterflies and twiddle products take at full occupancy"}
 
 
-def batch_stats(lanes: int, reps: int = 5) -> dict:
+def batch_stats(lanes: int, reps: int = 7) -> dict:
     """96 polynomials of uneven size (mu = floor(14 + 8u)), each committed and opened at its own
     point: one at a time on one context versus all through the engine's lanes; host f in, proof
     out.  Each side is timed `reps` times and the best run counts; every proof of the engine must

@@ -14,7 +14,8 @@
 //   warp 1      TMEM allocation, and one thread issuing tcgen05.mma.kind::i8 (M128 N256 K32)
 //   warps 2-5   B producers: expand 2 x 256 codeword words (loaded three stages ahead) into the
 //               256 x 128-byte K-major SWIZZLE_128B bit tile
-//   warps 6-9   epilogue: tcgen05.ld the int32 limb sums, recombine mod p, write H, release the
+//   warps 6-13  epilogue, two sets of four warps taking alternate 8-column steps: tcgen05.ld
+//               the int32 limb sums, recombine mod p, write H, release the
 //               accumulators; then hash each 256-byte column leaf with BLAKE3 (reading H back
 //               from L2) while the MMAs of the next tile run.
 // Every mbarrier wait is bounded by a clock budget and watches a CTA-wide failure flag; on a
@@ -42,13 +43,13 @@ constexpr int A_TILE = 256 * TC_KB;
 constexpr int B_TILE = TC_N * TC_KB;
 constexpr int STAGE_BYTES = A_TILE + B_TILE;
 constexpr int NPROD = 128;
-constexpr int NEPI = 128;
-constexpr int NTHREADS = 320;
+constexpr int NEPI = 256;  // epilogue threads: two sets of four warps, one per TMEM lane quarter
+constexpr int NTHREADS = 64 + NPROD + NEPI;
 constexpr int TMEM_COLS = 512;
-constexpr int EPI_COLS = 16;     // accumulator columns drained per epilogue step
+constexpr int EPI_COLS = 8;      // accumulator columns a set drains per epilogue step
 constexpr int SS_PITCH = 260;    // u32 per drained column (256 limb rows + pad, 16-byte rows)
-constexpr int SS_WORDS = EPI_COLS * SS_PITCH;  // one staging buffer; two alternate
-constexpr int SS_BYTES = 2 * SS_WORDS * 4;
+constexpr int SS_WORDS = EPI_COLS * SS_PITCH;  // one staging buffer; two alternate per set
+constexpr int SS_BYTES = 4 * SS_WORDS * 4;
 constexpr int NBARS = 3 * TC_STAGES + 3;  // full, empty, acc_full/acc_empty/drain, tma
 constexpr int SMEM_BYTES = TC_STAGES * STAGE_BYTES + SS_BYTES + 1024 /*align*/ + 128 /*barriers*/;
 constexpr long long WAIT_CYCLES = tc::DRAIN_CYCLES;  // ~2 s at 1.9 GHz (default budget)
@@ -66,18 +67,23 @@ using tc::mma_commit;
 using tc::smem_u32;
 using tc::sw128_desc;
 using tc::tmem_ld16;
+using tc::tmem_ld8;
 using tc::tmem_wait_ld;
 __device__ __forceinline__ void mma_i8(uint32_t dtmem, uint64_t adesc, uint64_t bdesc,
                                        uint32_t accumulate) {
   tc::mma_i8(dtmem, adesc, bdesc, IDESC, accumulate);
 }
-__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
-// Barrier of the 128 epilogue threads that also ANDs their flags, so that they leave a loop
+// All epilogue threads (barrier 1); one set's 128 threads (barriers 2 and 3).
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+__device__ __forceinline__ void set_sync(unsigned set) {
+  asm volatile("bar.sync %0, 128;" ::"r"(2 + set) : "memory");
+}
+// Barrier of the 256 epilogue threads that also ANDs their flags, so that they leave a loop
 // together (a lone warp left behind would wait at the next named barrier for good).
 __device__ __forceinline__ bool epi_all(bool ok) {
   uint32_t r;
   asm volatile(
-      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.and.pred q, 1, 128, p;\n"
+      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.and.pred q, 1, 256, p;\n"
       " selp.u32 %0, 1, 0, q;\n}\n"
       : "=r"(r)
       : "r"((uint32_t)ok)
@@ -263,8 +269,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       if (f + 2 >= nfill || !fill(f + 2, w2)) break;
     }
   } else {
-    // ---- epilogue (128 threads, warps 6-9; TMEM lane quarter = warp % 4) ----
-    const unsigned et = tid - 192, quarter = warp & 3;
+    // ---- epilogue (256 threads, warps 6-13; TMEM lane quarter = warp % 4).  Two sets of four
+    // warps drain alternate 8-column steps, each through its own pair of staging buffers.
+    const unsigned et = tid - (64 + NPROD), quarter = warp & 3, set = et >> 7, st_t = et & 127;
     const uint32_t lane_off = (uint32_t)(32 * quarter) << 16;
     const unsigned mrow = 32 * quarter + lane;
     for (unsigned t = 0; t < my_tiles; ++t) {
@@ -276,23 +283,24 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      // Step q stages its columns in buffer q & 1: the step before last read that buffer before
-      // the previous step's barrier, so one barrier per step suffices.
-      for (int q = 0; q < TC_N / EPI_COLS; ++q) {
-        uint32_t* Sb = Ss + (q & 1) * SS_WORDS;
-        uint32_t r0[16], r1[16];
-        tmem_ld16(tmem + lane_off + EPI_COLS * q, r0);
-        tmem_ld16(tmem + lane_off + 256 + EPI_COLS * q, r1);
+      // The set's step k stages its columns in buffer k & 1: the step before last read that
+      // buffer before the previous step's barrier, so one barrier per step suffices.
+      for (int k = 0; k < TC_N / EPI_COLS / 2; ++k) {
+        const unsigned q = 2 * k + set;  // column group of this step
+        uint32_t* Sb = Ss + (2 * set + (k & 1)) * SS_WORDS;
+        uint32_t r0[8], r1[8];
+        tmem_ld8(tmem + lane_off + EPI_COLS * q, r0);
+        tmem_ld8(tmem + lane_off + 256 + EPI_COLS * q, r1);
         tmem_wait_ld();
 #pragma unroll
         for (int cc = 0; cc < EPI_COLS; ++cc) {
           Sb[cc * SS_PITCH + mrow] = r0[cc];
           Sb[cc * SS_PITCH + 128 + mrow] = r1[cc];
         }
-        epi_sync();
+        set_sync(set);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const unsigned idx = et + NEPI * i, col = idx & (EPI_COLS - 1), r = idx >> 4;
+        for (int i = 0; i < 2; ++i) {
+          const unsigned idx = st_t + 128 * i, col = idx & (EPI_COLS - 1), r = idx >> 3;
           const uint4 lo4 = *(const uint4*)&Sb[col * SS_PITCH + 8 * r];
           const uint4 hi4 = *(const uint4*)&Sb[col * SS_PITCH + 8 * r + 4];
           const u64 a = (u64)lo4.x + ((u64)lo4.y << 8) + ((u64)lo4.z << 16) + ((u64)lo4.w << 24);
