@@ -488,19 +488,23 @@ void linear_witness_tc(lgs_ctx* c, const int64_t* dx, size_t rows, size_t inner,
   // two CTAs per SM need the largest shared-memory carveout
   LGS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
                                 (int)cudaSharedmemCarveoutMaxShared));
-  int per_sm = 1, nsm = 148;
+  // resident CTAs per SM: the launch bounds cap registers for two; shared memory decides
+  int nsm = 148, smem_sm = 0;
   LGS_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
-  LGS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, WT_THREADS, smem));
-  const size_t slots = (size_t)std::max(1, per_sm) * nsm;
+  LGS_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor,
+                                  c->device));
+  const size_t per_sm = 2 * (smem + 1024) <= (size_t)smem_sm ? 2 : 1;
+  const size_t slots = per_sm * nsm;
   const size_t mt = (cols + WT_M - 1) / WT_M, tiles = mt * ntr;
   const size_t chunks = (inner + WT_KC - 1) / WT_KC;
-  // K splits: the fewest that minimise (waves of CTAs) x (chunks per CTA + about one chunk of
-  // fixed cost per CTA), and enough that no CTA sums more than WT_KMAX values of K
+  // K splits: the fewest that minimise (waves of CTAs) x (chunks per CTA + the fixed cost of a
+  // CTA, about three chunks with the split epilogue's atomics and finish), and enough that no
+  // CTA sums more than WT_KMAX values of K
   const size_t min_split = (inner + WT_KMAX - 1) / WT_KMAX;
   size_t split = min_split, best = SIZE_MAX;
   for (size_t sp = min_split; sp <= std::min<size_t>(chunks, 64); ++sp) {
     const size_t per = (chunks + sp - 1) / sp;
-    const size_t cost = ((tiles * sp + slots - 1) / slots) * (per + 1);
+    const size_t cost = ((tiles * sp + slots - 1) / slots) * (per + 3);
     if (cost < best) best = cost, split = sp;
   }
   const size_t kchunk = (chunks + split - 1) / split * WT_KC;
