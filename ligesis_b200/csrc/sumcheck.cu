@@ -4,11 +4,11 @@
 // lo = P[i], hi = P[i + half] (the HIGH variable is bound first), then folds every factor with
 // the round challenge r_t: P[i] = P[i] + r_t (P[i + half] - P[i]).  All challenges come from the
 // pre-drawn oracle (utils/src/oracle.rs:10-64), so no round depends on the host: the fold of
-// round t-1 is fused into the evaluation pass of round t (each thread owns the quadruple
-// i, i + half, i + 2 half, i + 3 half, so the in-place fold has no races), per-CTA partial sums
-// go to a scratch array, and a last kernel reduces them into the round polynomials.  Once the
-// vectors are short (1024 entries, 512 for three stored factors), one CTA loads them into shared
-// memory and finishes the remaining rounds there.
+// round t-1 is fused into the evaluation pass of round t, large rounds run two at a time in one
+// pass (each thread owns four entries, so the in-place fold has no races), and per-CTA partial
+// sums go to a scratch array.  Once the vectors are short (1024 entries, 512 for three stored
+// factors), one CTA loads them into shared memory, finishes the remaining rounds there, adds up
+// the earlier rounds' partials and fills in every round's g(1) along the claim chain.
 //
 // Binary variant (the B_I check of pcs/src/ligesis.rs:423-428, factors [b, b - 1, eq]): the
 // middle factor is always the first minus one (folding is affine), so only b and eq are stored
