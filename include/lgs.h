@@ -272,6 +272,9 @@ lgs_status lgs_profile_names(lgs_ctx* ctx, char* buf, size_t cap, size_t* needed
  *   "witness_path"     lgs_linear_witness: 0 the int8 tensor cores whenever every activation
  *                      fits 24 and every weight 16 signed bits (else the CUDA cores), 1 always
  *                      the CUDA cores
+ *   "witness_ctas"     lgs_linear_witness on the tensor cores: the resident CTAs its work plan
+ *                      assumes (whole waves of output tiles, the remaining tiles split over K
+ *                      to fill the last wave); 0 the GPU's own count
  * Results do not depend on them.  Unknown names: LGS_ERR_BAD_ARG. */
 lgs_status lgs_tune(lgs_ctx* ctx, const char* name, uint64_t value);
 lgs_status lgs_tune_get(lgs_ctx* ctx, const char* name, uint64_t* value);

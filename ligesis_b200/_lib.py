@@ -192,7 +192,8 @@ class Context:
         return int(s.value or 0)
 
     def tune(self, **params: int) -> None:
-        """Launch choices of this context's kernels (lgs_tune): hash_ctas, sumcheck_blocks."""
+        """Launch choices of this context's kernels (lgs_tune): hash_ctas, sumcheck_blocks,
+        hash_groups, witness_path, witness_ctas."""
         for name, value in params.items():
             check(self._lib.lgs_tune(self.handle, name.encode(), int(value)))
 

@@ -569,6 +569,9 @@ lgs_status lgs_tune(lgs_ctx* ctx, const char* name, uint64_t value) {
     } else if (n == "witness_path") {
       need(value <= 1, "lgs_tune: witness_path is 0 (tensor cores) or 1 (CUDA cores)");
       ctx->witness_path = (unsigned)value;
+    } else if (n == "witness_ctas") {
+      need(value <= 65536, "lgs_tune: witness_ctas above 65536");
+      ctx->witness_ctas = (unsigned)value;
     } else if (n == "sumcheck_blocks") {
       need(value <= SC_MAX_BLOCKS, "lgs_tune: sumcheck_blocks above the partial-sum slots");
       ctx->sumcheck_blocks = (unsigned)value;
@@ -592,6 +595,7 @@ lgs_status lgs_tune_get(lgs_ctx* ctx, const char* name, uint64_t* value) {
     else if (n == "sumcheck_blocks") *value = ctx->sumcheck_blocks;
     else if (n == "hash_groups") *value = ctx->hash_groups;
     else if (n == "witness_path") *value = ctx->witness_path;
+    else if (n == "witness_ctas") *value = ctx->witness_ctas;
     else throw std::invalid_argument("lgs_tune_get: unknown parameter " + n);
   });
 }

@@ -63,6 +63,27 @@ def test_tensor_path_matches_oracle(lgs, orc, rows, inner, cols, wt):
     _check(out["r"], orc.linear_witness(x, w, b, 1 << 12, wt))
 
 
+@pytest.mark.parametrize("rows,inner,cols,wt,ctas", [
+    (31, 768, 1300, True, 8),     # one wave of whole tiles, three tiles split in two after it
+    (70, 300, 700, False, 5),     # two row tiles, ragged K and columns, the tail split in two
+    (64, 2000, 1000, True, 3),    # one tail tile split in three
+    (3, 20000, 700, True, 4),     # every tile split by the int32 bound
+])
+def test_tensor_path_whole_waves_and_split_tail(lgs, orc, rows, inner, cols, wt, ctas):
+    """The work plan with fewer resident CTAs than tiles (witness_ctas caps what it assumes):
+    whole tiles in full waves, the remaining tiles split over K into one more wave."""
+    ctx = L.Context(0)
+    ctx.tune(witness_ctas=ctas)
+    x = _rand(rows + 7, (rows, inner), -(1 << 22), 1 << 22)
+    w = _rand(cols + 8, (cols, inner) if wt else (inner, cols), -(1 << 15), 1 << 15)
+    b = _rand(cols + 9, cols, -(1 << 40), 1 << 40)
+    out = {}
+    tc, cores = _paths(ctx, lambda: out.setdefault("r", ps.linear_witness(x, w, b, 3 << 11, wt,
+                                                                          ctx)))
+    assert (tc, cores) == (1, 0)
+    _check(out["r"], orc.linear_witness(x, w, b, 3 << 11, wt))
+
+
 @pytest.mark.parametrize("wt", [False, True])
 def test_tensor_path_at_the_encoding_bounds(lgs, orc, wt):
     """Every activation and weight at an end of its range, in sign patterns, with an odd
