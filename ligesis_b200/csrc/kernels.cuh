@@ -36,6 +36,8 @@ double rs_alu_rate(int op, unsigned iters, u64* sink, cudaStream_t st);
 void alimb_from_a(const u64* A, uint8_t* alimb, size_t W, cudaStream_t st);
 void make_alimb_tmap(const uint8_t* alimb, size_t W, void* tmap_out);
 size_t tensor_map_bytes();
+void make_i64_tmap(const int64_t* base, size_t rows, size_t inner, unsigned box_rows,
+                   void* tmap_out);
 // wait_cycles: clock budget of the kernel's bounded waits (0 = the default, about 2 s).
 // max_ctas: persistent CTAs (0 = one per SM); fewer leave SMs to concurrent work.
 // Rows [row0, row0 + rows) of the codeword only (rows = 0: to the end; both even except at the

@@ -23,18 +23,23 @@ __device__ __forceinline__ void mbar_arrive_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
                : "memory");
 }
+// A waiting thread sleeps in try_wait until the phase completes or this many nanoseconds pass
+// (then the wait loops below check their budget and the failure flag), so waiting roles leave
+// the issue slots to the working ones.
+constexpr uint32_t SUSPEND_NS = 100000;
+
 __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
   uint32_t done;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
       " selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(done)
-      : "r"(bar), "r"(parity)
+      : "r"(bar), "r"(parity), "r"(SUSPEND_NS)
       : "memory");
   return done != 0;
 }
 // Bounded wait for the phase with the given parity to complete.  false after `budget` clock
-// cycles, or as soon as another role has flagged a failure (*fail != 0).
+// cycles, or once another role has flagged a failure (*fail != 0; seen within one suspension).
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* fail,
                                           long long budget) {
   const long long t0 = clock64();
@@ -106,6 +111,18 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
                  "=r"(r[6]), "=r"(r[7])
                : "r"(taddr));
+}
+// 4 consecutive 32-bit accumulator columns of this warp's 32 TMEM lanes.
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&r)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr));
+}
+// One 32-bit accumulator column of this warp's 32 TMEM lanes.
+__device__ __forceinline__ uint32_t tmem_ld1(uint32_t taddr) {
+  uint32_t r;
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(r) : "r"(taddr));
+  return r;
 }
 __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");

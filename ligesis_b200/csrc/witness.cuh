@@ -28,12 +28,11 @@ __device__ __forceinline__ bool fits_i64(uint64_t hi, uint64_t lo) {
   return (int64_t)hi == ((int64_t)lo >> 63);  // the high word extends the low word's sign
 }
 
-// Q, REM, Y, Y_field of one output from its exact sum; false when a value leaves the i64 range.
-__device__ __forceinline__ bool lw_finish(const Acc128& s, const int64_t* bias, size_t c,
-                                          int64_t d, size_t o, int64_t* q_out, int64_t* rem_out,
-                                          int64_t* y_out, uint64_t* yf_out) {
-  if (!fits_i64(s.hi, s.lo)) return false;  // checked_i128_to_i64 of the product
-  const int64_t v = (int64_t)s.lo;
+// Q, REM, Y, Y_field of one output from its exact sum v (in the i64 range) and its column's
+// bias b; false when Q + bias leaves the i64 range.
+__device__ __forceinline__ bool lw_finish_i64(int64_t v, int64_t b, int64_t d, size_t o,
+                                              int64_t* q_out, int64_t* rem_out, int64_t* y_out,
+                                              uint64_t* yf_out) {
   int64_t q, rm;
   if ((d & (d - 1)) == 0) {  // a power of two (the fixed-point scale): floor division is a shift
     const int sh = __ffsll(d) - 1;
@@ -46,23 +45,24 @@ __device__ __forceinline__ bool lw_finish(const Acc128& s, const int64_t* bias, 
       rm += d;
     }
   }
-  const int64_t b = bias ? bias[c] : 0;
   const int64_t yy = (int64_t)((uint64_t)q + (uint64_t)b);
   if (((q ^ yy) & (b ^ yy)) < 0) return false;  // signed overflow of q + bias
   q_out[o] = q;
   rem_out[o] = rm;
   y_out[o] = yy;
-  if (yf_out) {  // encode_i64: y mod p, or -(|y| mod p)
-    uint64_t e;
-    if (yy >= 0) {
-      e = (uint64_t)yy % GL_P;
-    } else {
-      const uint64_t m = ((uint64_t)(-(yy + 1)) + 1) % GL_P;
-      e = m ? GL_P - m : 0;
-    }
-    yf_out[o] = e;
-  }
+  // encode_i64: y mod p, or -(|y| mod p).  |y| <= 2^63 < p, so no reduction is left: y itself,
+  // or p - |y| (|y| >= 1 for y < 0).
+  if (yf_out) yf_out[o] = yy >= 0 ? (uint64_t)yy : GL_P - ((uint64_t)(-(yy + 1)) + 1);
   return true;
+}
+
+// The same from a 128-bit sum, reading the bias of column c; false when a value leaves the i64
+// range (checked_i128_to_i64 of the product, or Q + bias).
+__device__ __forceinline__ bool lw_finish(const Acc128& s, const int64_t* bias, size_t c,
+                                          int64_t d, size_t o, int64_t* q_out, int64_t* rem_out,
+                                          int64_t* y_out, uint64_t* yf_out) {
+  if (!fits_i64(s.hi, s.lo)) return false;
+  return lw_finish_i64((int64_t)s.lo, bias ? bias[c] : 0, d, o, q_out, rem_out, y_out, yf_out);
 }
 
 }  // namespace lgs

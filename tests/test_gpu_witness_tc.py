@@ -106,8 +106,9 @@ def test_tensor_path_at_the_encoding_bounds(lgs, orc, wt):
     _check(out["r"], orc.linear_witness(x, w, None, 4097, wt))
 
 
+@pytest.mark.parametrize("wt", [False, True])
 @pytest.mark.parametrize("which", ["x", "w"])
-def test_operand_outside_the_limbs_takes_the_cuda_cores(lgs, orc, which):
+def test_operand_outside_the_limbs_takes_the_cuda_cores(lgs, orc, which, wt):
     ctx = L.Context(0)
     x = _rand(1, (31, 768), -(1 << 20), 1 << 20)
     w = _rand(2, (768, 300), -(1 << 15), 1 << 15)
@@ -115,11 +116,13 @@ def test_operand_outside_the_limbs_takes_the_cuda_cores(lgs, orc, which):
         x[17, 500] = 1 << 23
     else:
         w[700, 299] = -(1 << 15) - 1
+    if wt:
+        w = np.ascontiguousarray(w.T)
     out = {}
     tc, cores = _paths(ctx, lambda: out.setdefault("r", ps.linear_witness(x, w, None, 1 << 12,
-                                                                          False, ctx)))
+                                                                          wt, ctx)))
     assert (tc, cores) == (1, 1)
-    _check(out["r"], orc.linear_witness(x, w, None, 1 << 12))
+    _check(out["r"], orc.linear_witness(x, w, None, 1 << 12, wt))
 
 
 def test_device_arrays_both_paths_agree(lgs, orc):
