@@ -19,10 +19,10 @@
 // adding its exact int64 sum into a zeroed buffer and the last to arrive (a counter per tile)
 // finishing the tile.  x_limbs_kernel converts X once per launch into the limb tiles of every
 // (row tile, chunk) and zeroes the split buffers.  Two kernels take the units:
-//   linear_witness_tp_kernel (W transposed, the vocabulary head's layout): persistent, one CTA
-//     per SM, warp-specialised: W arrives by TMA into a ring of raw boxes, eight warps convert
-//     it to limbs, one thread issues the MMAs into two alternating accumulator sets in TMEM,
-//     and eight warps finish each unit while the next one streams
+//   linear_witness_tp_kernel (rows of W an even number of values, 16-byte aligned: every GPT-2
+//     layer): persistent, one CTA per SM, warp-specialised: W arrives by TMA into a ring of raw
+//     boxes, eight warps convert it to limbs, one thread issues the MMAs into two alternating
+//     accumulator sets in TMEM, and eight warps finish each unit while the next one streams
 //   linear_witness_tc_kernel (the other layouts): one CTA per unit, its eight warps loading W
 //     through registers into limbs, warp 0 issuing the MMAs, warps 0-3 finishing the unit.
 // Every wait is bounded.
@@ -498,9 +498,9 @@ __device__ __forceinline__ bool wt_epilogue(const WtArgs& a, const WtUnit& w, ui
   return !over;
 }
 
-// One CTA per unit, two per SM (the layouts the persistent kernel below does not take: W as
-// inner x cols, or W transposed with odd rows or rows not 16-byte aligned).  WT: W is cols x
-// inner (else inner x cols).
+// One CTA per unit, two per SM (the layouts the persistent kernel below does not take: rows of
+// W with an odd number of values, or not 16-byte aligned).  WT: W is cols x inner (else inner x
+// cols).
 template <bool WT>
 __global__ void __launch_bounds__(WT_THREADS, 2) linear_witness_tc_kernel(const WtArgs a) {
   extern __shared__ uint8_t wt_smem_raw[];
@@ -600,10 +600,11 @@ __global__ void __launch_bounds__(WT_THREADS, 2) linear_witness_tc_kernel(const 
   }
 }
 
-// ---- The persistent kernel for W transposed (cols x inner, inner even, rows 16-byte aligned) --
+// ---- The persistent kernel (rows of W an even number of values, 16-byte aligned) --------------
 // One CTA per SM walks the work units u = blockIdx.x, + gridDim.x, ... with its warps in roles:
-//   warp 8      TMA: W's chunk of each unit as eight boxes of 16 values of K x 128 columns
-//               (16 KB, 128-byte swizzle, zeros outside the matrix) into a ring of nraw boxes
+//   warp 8      TMA: W's chunk of each unit as eight boxes of 16 KB (128 rows of W x 16 values
+//               of K when W is transposed, else 128 rows of K x 16 columns; 128-byte swizzle,
+//               zeros outside the matrix) into a ring of nraw boxes
 //   warps 0-7   convert each box to limbs in the limb stage of its chunk (2 stages); thread 0
 //               also fetches the chunk's X limb tiles with one bulk copy
 //   warp 9      TMEM allocation; one thread issues each chunk's MMAs into the unit's accumulator
@@ -636,6 +637,51 @@ __device__ __forceinline__ bool warp_wait(uint32_t bar, uint32_t parity, volatil
   return __all_sync(0xffffffffu, tc::mbar_wait(bar, parity, fail, budget));
 }
 
+// One raw box of W (box b of its chunk) into the stage's two limb tiles, by warps 0-7.
+//   WT: the box is 128 rows of W (output columns) x 16 values of K.  Lane (r8, qd) takes rows
+//       8 warp + r8 and + 64, values 4 qd .. 4 qd + 3 (16-byte chunks 2 qd and 2 qd + 1 of the
+//       row, swizzled by r8); the limb words go to row m, K byte 16 b + 4 qd.
+//   else: the box is 128 rows of K x 16 output columns (16 b ..).  Lane (c8, q4) takes columns
+//       c8 and c8 + 8, rows 4 kq .. 4 kq + 3 with kq = 4 warp + q4 (8-byte loads; a load's lanes
+//       read 8 columns of 4 rows, two per swizzle pattern); the limb words go to row 16 b +
+//       column, K byte 4 kq.
+// Either way a limb store's 32 lanes hit 32 different banks.  acc collects the range check.
+template <bool WT>
+__device__ __forceinline__ void wp_convert(const uint8_t* box, uint8_t* const (&tiles)[WT_LW],
+                                           int b, unsigned warp, unsigned lane, uint64_t& acc) {
+  if constexpr (WT) {
+    const unsigned r8 = lane >> 2, qd = lane & 3;
+    const uint32_t row = (8 * warp + r8) * 128;
+    const uint32_t rd0 = row + (((2 * qd) ^ r8) << 4), rd1 = row + (((2 * qd + 1) ^ r8) << 4);
+    const uint32_t wr = row + (((uint32_t)b ^ r8) << 4) + 4 * qd;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const longlong2 v0 = *(const longlong2*)(box + rd0 + 8192 * h);
+      const longlong2 v1 = *(const longlong2*)(box + rd1 + 8192 * h);
+      const uint32_t e0 = w_word(v0.x, acc), e1 = w_word(v0.y, acc);
+      const uint32_t e2 = w_word(v1.x, acc), e3 = w_word(v1.y, acc);
+      store_limbs(tiles, wr + 8192 * h, pair_limbs(e0, e1), pair_limbs(e2, e3));
+    }
+  } else {
+    const unsigned c8 = lane >> 2, kq = 4 * warp + (lane & 3);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const unsigned cl = c8 + 8 * h;
+      uint32_t e[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const unsigned k = 4 * kq + j;
+        e[j] = w_word(*(const int64_t*)(box + k * 128 + ((((cl >> 1) ^ k) & 7) << 4) +
+                                        (cl & 1) * 8),
+                      acc);
+      }
+      store_limbs(tiles, tc::sw128_off(16 * b + cl, 4 * kq), pair_limbs(e[0], e[1]),
+                  pair_limbs(e[2], e[3]));
+    }
+  }
+}
+
+template <bool WT>
 __global__ void __launch_bounds__(WP_THREADS, 1)
     linear_witness_tp_kernel(const __grid_constant__ CUtensorMap tmap_w, const WtArgs a,
                              unsigned nraw) {
@@ -692,12 +738,7 @@ __global__ void __launch_bounds__(WP_THREADS, 1)
   const uint32_t tmem = *tmem_holder;
 
   if (warp < 8) {
-    // ---- converters: lane (r8, qd) takes rows m = 8 warp + r8 and m + 64 of each box, values
-    // 4 qd .. 4 qd + 3 of K (16-byte chunks 2 qd and 2 qd + 1 of the row, swizzled by r8); the
-    // limb words go to row m, K byte 16 box + 4 qd of the stage's two W tiles
-    const unsigned r8 = lane >> 2, qd = lane & 3;
-    const uint32_t row = (8 * warp + r8) * 128;
-    const uint32_t rd0 = row + (((2 * qd) ^ r8) << 4), rd1 = row + (((2 * qd + 1) ^ r8) << 4);
+    // ---- converters (wp_convert)
     uint64_t acc = 0;
     unsigned rawi = 0, limi = 0, x_issued = 0;
     bool ok = true;
@@ -734,16 +775,7 @@ __global__ void __launch_bounds__(WP_THREADS, 1)
             ok = false;
             break;
           }
-          const uint8_t* box = raw + (size_t)slot * WP_BOX;
-          const uint32_t wr = row + (((uint32_t)b ^ r8) << 4) + 4 * qd;
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const longlong2 v0 = *(const longlong2*)(box + rd0 + 8192 * h);
-            const longlong2 v1 = *(const longlong2*)(box + rd1 + 8192 * h);
-            const uint32_t e0 = w_word(v0.x, acc), e1 = w_word(v0.y, acc);
-            const uint32_t e2 = w_word(v1.x, acc), e3 = w_word(v1.y, acc);
-            store_limbs(tiles, wr + 8192 * h, pair_limbs(e0, e1), pair_limbs(e2, e3));
-          }
+          wp_convert<WT>(raw + (size_t)slot * WP_BOX, tiles, b, warp, lane, acc);
           __syncwarp();
           if (lane == 0) tc::mbar_arrive(raw_empty(slot));
         }
@@ -761,7 +793,8 @@ __global__ void __launch_bounds__(WP_THREADS, 1)
     }
   }
   else if (warp == WP_LOAD_WARP) {
-    // ---- TMA: box (16 values of K from kb + 128 t + 16 b) x (128 rows of W from c0)
+    // ---- TMA: W transposed: box (16 values of K from kb + 128 t + 16 b) x (128 rows of W from
+    // c0); else (16 columns from c0 + 16 b) x (128 rows of K from kb + 128 t)
     if (lane == 0) {
       unsigned rawi = 0;
       bool ok = true;
@@ -778,7 +811,8 @@ __global__ void __launch_bounds__(WP_THREADS, 1)
             }
             const uint32_t bar = raw_full(slot);
             tc::mbar_arrive_tx(bar, WP_BOX);
-            const int x = (int)(w.kb + (size_t)t * WT_KC + 16 * b), y = (int)w.c0;
+            const int x = WT ? (int)(w.kb + (size_t)t * WT_KC + 16 * b) : (int)(w.c0 + 16 * b);
+            const int y = WT ? (int)w.c0 : (int)(w.kb + (size_t)t * WT_KC);
             asm volatile(
                 "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
                 "[%0], [%1, {%2, %3}], [%4];" ::"r"(tc::smem_u32(raw + (size_t)slot * WP_BOX)),
@@ -895,9 +929,11 @@ void linear_witness_tc(lgs_ctx* c, const int64_t* dx, size_t rows, size_t inner,
   const size_t ntr = (rows + WT_NR_MAX - 2) / (WT_NR_MAX - 1);
   const unsigned nrv = (unsigned)((rows + ntr - 1) / ntr);
   const unsigned nr = (nrv + 1 + 15) / 16 * 16;
-  // W transposed with 16-byte aligned rows: the persistent kernel (its weights arrive by TMA);
-  // otherwise one CTA per unit, two per SM
-  const bool persistent = w_transposed && (inner % 2 == 0) && (((uintptr_t)dw & 15) == 0);
+  // W's rows an even number of values and 16-byte aligned: the persistent kernel (its weights
+  // arrive by TMA); otherwise one CTA per unit, two per SM
+  const bool persistent =
+      (w_transposed ? inner % 2 == 0 : cols % 2 == 0) && (((uintptr_t)dw & 15) == 0);
+  auto kp = w_transposed ? linear_witness_tp_kernel<true> : linear_witness_tp_kernel<false>;
   int nsm = 148, smem_sm = 0, smem_optin = 0;
   LGS_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
   LGS_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor,
@@ -913,9 +949,12 @@ void linear_witness_tc(lgs_ctx* c, const int64_t* dx, size_t rows, size_t inner,
     const size_t fixed = wp_fixed_bytes(nr);
     nraw = (unsigned)std::min<size_t>(WP_RAW_MAX, ((size_t)smem_optin - fixed - 1024) / WP_BOX);
     smem = fixed + (size_t)nraw * WP_BOX;
-    LGS_CUDA(cudaFuncSetAttribute(linear_witness_tp_kernel,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    make_i64_tmap(dw, cols, inner, WT_M, &tm);
+    LGS_CUDA(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // boxes of 128 rows x 16 values: rows of W (transposed) or rows of K
+    if (w_transposed)
+      make_i64_tmap(dw, cols, inner, WT_M, &tm);
+    else
+      make_i64_tmap(dw, inner, cols, WT_KC, &tm);
     slots = c->witness_ctas ? c->witness_ctas : (size_t)nsm;
     fixed_cost = 1;  // a unit's start and epilogue overlap the neighbouring units' streams
   } else {
@@ -1006,7 +1045,7 @@ void linear_witness_tc(lgs_ctx* c, const int64_t* dx, size_t rows, size_t inner,
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    LGS_CUDA(cudaLaunchKernelEx(&cfg, linear_witness_tp_kernel, tm, a, nraw));
+    LGS_CUDA(cudaLaunchKernelEx(&cfg, kp, tm, a, nraw));
   } else {
     k<<<(unsigned)units, WT_THREADS, smem, st>>>(a);
   }
