@@ -410,6 +410,12 @@ __device__ __forceinline__ uint64_t wt_produce(const WtArgs& a, WtCta& s) {
   return acc;
 }
 
+__device__ __noinline__ bool lw_finish_ol(int64_t v, int64_t b, int64_t d, size_t o,
+                                          int64_t* q_out, int64_t* rem_out, int64_t* y_out,
+                                          uint64_t* yf_out) {
+  return lw_finish_i64(v, b, d, o, q_out, rem_out, y_out, yf_out);
+}
+
 // The epilogue of one unit by the 128 x halves threads of 4 x halves warps (TMEM lane quarter
 // q = warp % 4 holds output columns 32 q .. 32 q + 31 of the tile; half h of the warps of a
 // quarter takes the row groups 4 h, 4 (h + halves), ...; leader: one of the threads) once its four
@@ -477,21 +483,28 @@ __device__ __forceinline__ bool wt_epilogue(const WtArgs& a, const WtUnit& w, ui
     epi_bar(128 * halves);
     if (*s_last) {
       __threadfence();
+      // this thread's groups of four rows (4 h, 4 (h + halves), ...), four groups' loads in
+      // flight at once; the finish out of line, so that this rarely run code stays small
 #pragma unroll 1
-      for (unsigned blk = 4 * h; blk < a.nrv; blk += 4 * halves) {  // four rows' loads at a time
-        int64_t val[4];
+      for (unsigned blk = 4 * h; blk < a.nrv; blk += 16 * halves) {
+        int64_t val[16];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const unsigned r = blk + i;
-          val[i] = r < a.nrv ? (int64_t)__ldcg(tacc + (size_t)r * WT_M + m) : 0;
-        }
+        for (int g = 0; g < 4; ++g)
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const unsigned r = blk + i;
-          const size_t gr = w.r0 + r;
-          if (r >= a.nrv || gr >= a.rows || !col_ok) continue;
-          over |= !lw_finish_i64(val[i], bias, a.d, gr * a.cols + c, a.q, a.rem, a.y, a.yf);
-        }
+          for (int i = 0; i < 4; ++i) {
+            const unsigned r = blk + 4 * halves * g + i;
+            val[4 * g + i] = r < a.nrv ? (int64_t)__ldcg(tacc + (size_t)r * WT_M + m) : 0;
+          }
+#pragma unroll
+        for (int g = 0; g < 4; ++g)
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const unsigned r = blk + 4 * halves * g + i;
+            const size_t gr = w.r0 + r;
+            if (r >= a.nrv || gr >= a.rows || !col_ok) continue;
+            over |= !lw_finish_ol(val[4 * g + i], bias, a.d, gr * a.cols + c, a.q, a.rem, a.y,
+                                  a.yf);
+          }
       }
     }
   }
