@@ -63,6 +63,27 @@ def test_tensor_path_matches_oracle(lgs, orc, rows, inner, cols, wt):
     _check(out["r"], orc.linear_witness(x, w, b, 1 << 12, wt))
 
 
+@pytest.mark.parametrize("rows,inner,cols,wt", [
+    (63, 512, 300, True),     # N = 64: two accumulator sets fill all 512 TMEM columns
+    (63, 512, 300, False),
+    (7, 256, 10, False),      # fewer columns than one 16-column box
+    (5, 2, 200, True),        # K of two values: one chunk, mostly past the matrix
+    (31, 20000, 300, False),  # K split by the int32 bound, weights as inner x cols
+    (40, 1000, 2, True),      # two output columns
+])
+def test_persistent_kernel_edges(lgs, orc, rows, inner, cols, wt):
+    """Shapes at the edges of the persistent kernel's boxes, tiles and TMEM."""
+    ctx = L.Context(0)
+    x = _rand(rows + 11, (rows, inner), -(1 << 23), 1 << 23)
+    w = _rand(cols + 12, (cols, inner) if wt else (inner, cols), -(1 << 15), 1 << 15)
+    b = _rand(cols + 13, cols, -(1 << 35), 1 << 35)
+    out = {}
+    tc, cores = _paths(ctx, lambda: out.setdefault("r", ps.linear_witness(x, w, b, 1 << 12, wt,
+                                                                          ctx)))
+    assert (tc, cores) == (1, 0)
+    _check(out["r"], orc.linear_witness(x, w, b, 1 << 12, wt))
+
+
 @pytest.mark.parametrize("rows,inner,cols,wt,ctas", [
     (31, 768, 1300, True, 8),     # one wave of whole tiles, three tiles split in two after it
     (70, 300, 700, False, 5),     # two row tiles, ragged K and columns, the tail split in two
