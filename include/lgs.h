@@ -272,6 +272,9 @@ lgs_status lgs_profile_names(lgs_ctx* ctx, char* buf, size_t cap, size_t* needed
  *   "witness_path"     lgs_linear_witness: 0 the int8 tensor cores whenever every activation
  *                      fits 24 and every weight 16 signed bits (else the CUDA cores), 1 always
  *                      the CUDA cores
+ *   "upload_block_bytes" commits of host polynomials: the least bytes per row block of the
+ *                      upload pipelined with the RS encoding (0: 1 MB; an engine's lanes
+ *                      start at 4 MB)
  *   "witness_ctas"     lgs_linear_witness on the tensor cores: the resident CTAs its work plan
  *                      assumes (whole waves of output tiles, the remaining tiles split over K
  *                      to fill the last wave); 0 the GPU's own count

@@ -569,6 +569,9 @@ lgs_status lgs_tune(lgs_ctx* ctx, const char* name, uint64_t value) {
     } else if (n == "witness_path") {
       need(value <= 1, "lgs_tune: witness_path is 0 (tensor cores) or 1 (CUDA cores)");
       ctx->witness_path = (unsigned)value;
+    } else if (n == "upload_block_bytes") {
+      need(value <= ((uint64_t)1 << 40), "lgs_tune: upload_block_bytes above 2^40");
+      ctx->upload_block = (size_t)value;
     } else if (n == "witness_ctas") {
       need(value <= 65536, "lgs_tune: witness_ctas above 65536");
       ctx->witness_ctas = (unsigned)value;
@@ -596,6 +599,7 @@ lgs_status lgs_tune_get(lgs_ctx* ctx, const char* name, uint64_t* value) {
     else if (n == "hash_groups") *value = ctx->hash_groups;
     else if (n == "witness_path") *value = ctx->witness_path;
     else if (n == "witness_ctas") *value = ctx->witness_ctas;
+    else if (n == "upload_block_bytes") *value = ctx->upload_block;
     else throw std::invalid_argument("lgs_tune_get: unknown parameter " + n);
   });
 }

@@ -131,6 +131,9 @@ lgs_status lgs_engine_create(int device, unsigned lanes, size_t hbm_budget, lgs_
       e->lanes.push_back(c);
       lgs::ctx_init(c, device);
       c->copy_pool = false;  // the lanes already copy in parallel
+      // larger upload blocks than a lone context: fewer calls per job, the lanes' jobs
+      // overlapping each other's uploads instead of their own blocks
+      c->upload_block = (size_t)4 << 20;
     }
     for (unsigned i = 0; i < lanes; ++i) e->workers.emplace_back(worker_main, e, (size_t)i);
   } catch (...) {

@@ -359,7 +359,13 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
     // f is copied by the DMA engine on a side stream; pageable f goes through the pinned ring on
     // the context stream, where the host-side staging of the next block is the slower part.
     StageTimer t(c->prof, c->st, "upload_and_rs_encode");
-    const unsigned nb = (unsigned)std::min<size_t>(lgs_ctx::ROW_BLOCKS, m);
+    // enough row blocks that the upload of each overlaps the encoding of the one before, but
+    // none smaller than upload_block (1 MB by default: a block costs a few calls and two
+    // launches, which a smaller block's overlap does not pay back; engine lanes use 4 MB, their
+    // jobs overlapping each other instead)
+    const size_t min_block = c->upload_block ? c->upload_block : ((size_t)1 << 20);
+    unsigned nb = (unsigned)std::min<size_t>(lgs_ctx::ROW_BLOCKS, m);
+    while (nb > 1 && m * n * 8 / nb < min_block) nb >>= 1;
     const size_t rows = m / nb;  // m and nb are powers of two
     const bool pinned = host_is_pinned(f);
     cudaStream_t cp = c->side[0];

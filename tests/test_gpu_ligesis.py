@@ -277,3 +277,16 @@ def test_lent_device_polynomial_gives_the_same_commitment(lgs, orc):
         assert L.Ligesis.prove(pk, data, z, o).data == want, lend
         assert commit.root == cm.root, lend
     assert np.array_equal(f_dev.cpu().numpy().view(np.uint64), f)  # only read
+
+
+@pytest.mark.parametrize("block", [1, 0, 1 << 30])
+def test_upload_row_blocks_give_the_same_root(lgs, orc, block):
+    """A host polynomial is uploaded and encoded in row blocks of at least upload_block_bytes
+    (8, 2 and 1 blocks of a 2 MiB polynomial here); the commitment must not depend on it."""
+    log_m, log_n = 5, 13
+    f, A, _, _, _ = ligesis_inputs(log_m, log_n, seed=71)
+    ctx = L.Context(0)
+    ctx.tune(upload_block_bytes=block)
+    pk, _ = L.Ligesis.setup_with_hash(log_m, log_n, L.SubsetSumHash(64 << log_m, a=A), ctx)
+    commit, _ = L.Ligesis.commit(pk, L.MlPoly(f))
+    assert commit.root == orc.Commitment(orc.Key(log_m, log_n, A), f).root
