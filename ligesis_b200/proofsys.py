@@ -56,12 +56,16 @@ def linear_witness(x, w, bias, divisor: int, w_transposed: bool = False,
         if (w.shape[1] if w_transposed else w.shape[0]) != inner:
             raise ValueError("linear witness: inner dimensions differ")
         dev = x.device
+        xc, wc = x.contiguous(), w.contiguous()
+        bc = None if bias is None else bias.contiguous()
         q = torch.empty((rows, cols), dtype=torch.int64, device=dev)
         rem, y, yf = torch.empty_like(q), torch.empty_like(q), torch.empty_like(q)
-        torch.cuda.synchronize(dev)
-        check(load().lgs_linear_witness(ctx.handle, _ptr(x.contiguous()), rows, inner,
-                                        _ptr(w.contiguous()), cols, int(w_transposed),
-                                        None if bias is None else _ptr(bias.contiguous()),
+        # the context's stream waits for the operands' producer (torch's current stream), in
+        # stream order; the call returns once its own stream has finished
+        torch.cuda.ExternalStream(ctx.stream_ptr, device=dev).wait_stream(
+            torch.cuda.current_stream(dev))
+        check(load().lgs_linear_witness(ctx.handle, _ptr(xc), rows, inner, _ptr(wc), cols,
+                                        int(w_transposed), None if bc is None else _ptr(bc),
                                         int(divisor), 1, _ptr(q), _ptr(rem), _ptr(y),
                                         C.cast(C.c_void_p(yf.data_ptr()), C.POINTER(C.c_uint64))))
         return q, rem, y, yf
