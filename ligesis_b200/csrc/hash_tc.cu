@@ -470,12 +470,13 @@ void make_alimb_tmap(const uint8_t* alimb, size_t W, void* tmap_out) {
   CUresult r = encode_fn()(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)alimb, dims, strides, box,
                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  if (r != CUDA_SUCCESS)
+    throw CudaError("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
 }
 
-// The TMA descriptor of a row-major rows x inner matrix of 64-bit integers (inner even, base 16-byte
-// aligned): boxes of box_rows rows x 16 values (128 bytes), 128-byte swizzle, zeros outside the
-// matrix.
+// The TMA descriptor of a row-major rows x inner matrix of 64-bit integers (inner even, base
+// 16-byte aligned): boxes of box_rows rows x 16 values (128 bytes), 128-byte swizzle, zeros
+// outside the matrix.
 void make_i64_tmap(const int64_t* base, size_t rows, size_t inner, unsigned box_rows,
                    void* tmap_out) {
   if (inner % 2 || ((uintptr_t)base & 15)) throw ShapeError("TMA: int64 matrix misaligned");
@@ -487,7 +488,8 @@ void make_i64_tmap(const int64_t* base, size_t rows, size_t inner, unsigned box_
   CUresult r = encode_fn()(tm, CU_TENSOR_MAP_DATA_TYPE_INT64, 2, (void*)base, dims, strides, box,
                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  if (r != CUDA_SUCCESS)
+    throw CudaError("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
 }
 
 size_t tensor_map_bytes() { return sizeof(CUtensorMap); }

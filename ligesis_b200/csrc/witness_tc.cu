@@ -942,10 +942,6 @@ void linear_witness_tc(lgs_ctx* c, const int64_t* dx, size_t rows, size_t inner,
   const size_t ntr = (rows + WT_NR_MAX - 2) / (WT_NR_MAX - 1);
   const unsigned nrv = (unsigned)((rows + ntr - 1) / ntr);
   const unsigned nr = (nrv + 1 + 15) / 16 * 16;
-  // W's rows an even number of values and 16-byte aligned: the persistent kernel (its weights
-  // arrive by TMA); otherwise one CTA per unit, two per SM
-  const bool persistent =
-      (w_transposed ? inner % 2 == 0 : cols % 2 == 0) && (((uintptr_t)dw & 15) == 0);
   auto kp = w_transposed ? linear_witness_tp_kernel<true> : linear_witness_tp_kernel<false>;
   int nsm = 148, smem_sm = 0, smem_optin = 0;
   LGS_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
@@ -953,14 +949,21 @@ void linear_witness_tc(lgs_ctx* c, const int64_t* dx, size_t rows, size_t inner,
                                   c->device));
   LGS_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
                                   c->device));
+  // as many 16 KB boxes of weights in flight as shared memory holds beside the limb stages
+  const size_t fixed = wp_fixed_bytes(nr);
+  const unsigned nraw =
+      (size_t)smem_optin > fixed + 1024
+          ? (unsigned)std::min<size_t>(WP_RAW_MAX, ((size_t)smem_optin - fixed - 1024) / WP_BOX)
+          : 0;
+  // W's rows an even number of values and 16-byte aligned, and room for a ring of at least two
+  // boxes: the persistent kernel (its weights arrive by TMA); otherwise one CTA per unit, two
+  // per SM
+  const bool persistent = (w_transposed ? inner % 2 == 0 : cols % 2 == 0) &&
+                          (((uintptr_t)dw & 15) == 0) && nraw >= 2;
   size_t smem, slots, fixed_cost;
-  unsigned nraw = 0;
-  CUtensorMap tm;  // encoded before the first launch, so the launches follow back to back
+  CUtensorMap tm{};  // encoded before the first launch, so the launches follow back to back
   auto k = w_transposed ? linear_witness_tc_kernel<true> : linear_witness_tc_kernel<false>;
   if (persistent) {
-    // as many 16 KB boxes of weights in flight as shared memory holds beside the limb stages
-    const size_t fixed = wp_fixed_bytes(nr);
-    nraw = (unsigned)std::min<size_t>(WP_RAW_MAX, ((size_t)smem_optin - fixed - 1024) / WP_BOX);
     smem = fixed + (size_t)nraw * WP_BOX;
     LGS_CUDA(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // boxes of 128 rows x 16 values: rows of W (transposed) or rows of K
@@ -983,10 +986,10 @@ void linear_witness_tc(lgs_ctx* c, const int64_t* dx, size_t rows, size_t inner,
   }
   const size_t mt = (cols + WT_M - 1) / WT_M, tiles = mt * ntr;
   const size_t chunks = (inner + WT_KC - 1) / WT_KC;
-  // K splits: the fewest that minimise (waves of units) x (chunks per unit + the fixed cost of a
-  // unit), and enough that no unit sums more than WT_KMAX values of K.  Either one split for every tile, or (more tiles
-  // than resident CTAs) whole waves of tiles with the fewest splits and the remaining tiles
-  // split apart to fill one last wave.
+  // K splits: the fewest that minimise (waves of units) x (chunks per unit + the fixed cost of
+  // a unit), and enough that no unit sums more than WT_KMAX values of K.  Either one split for
+  // every tile, or (more tiles than resident CTAs) whole waves of tiles with the fewest splits
+  // and the remaining tiles split apart to fill one last wave.
   const size_t min_split = (inner + WT_KMAX - 1) / WT_KMAX;
   auto best_split = [&](size_t n, size_t& cost) {
     size_t split = min_split;
@@ -1008,8 +1011,9 @@ void linear_witness_tc(lgs_ctx* c, const int64_t* dx, size_t rows, size_t inner,
   WtArgs a{dx, dw, db, rows, inner, cols, nr, nrv, w_transposed ? 1 : 0, divisor, dq, dr, dy, df};
   a.err = derr;
   a.range = drange;
-  a.budget = c->wait_cycles ? (long long)std::min<uint64_t>(c->wait_cycles, (uint64_t)tc::DRAIN_CYCLES)
-                            : tc::DRAIN_CYCLES;
+  a.budget = c->wait_cycles
+                 ? (long long)std::min<uint64_t>(c->wait_cycles, (uint64_t)tc::DRAIN_CYCLES)
+                 : tc::DRAIN_CYCLES;
   const size_t sps[2] = {sp_a, sp_b};
   for (int g = 0; g < 2; ++g) {
     a.kch[g] = (chunks + sps[g] - 1) / sps[g] * WT_KC;
