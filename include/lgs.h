@@ -275,6 +275,9 @@ lgs_status lgs_profile_names(lgs_ctx* ctx, char* buf, size_t cap, size_t* needed
  *   "upload_block_bytes" commits of host polynomials: the least bytes per row block of the
  *                      upload pipelined with the RS encoding (0: 1 MB; an engine's lanes
  *                      start at 4 MB)
+ *   "upload_tail_rows" commits of host polynomials: rows of the last of those row blocks, whose
+ *                      RS encoding the prove waits for after the upload (0, or a whole equal
+ *                      share or more: equal blocks)
  *   "witness_ctas"     lgs_linear_witness on the tensor cores: the resident CTAs its work plan
  *                      assumes (whole waves of output tiles, the remaining tiles split over K
  *                      to fill the last wave); 0 the GPU's own count

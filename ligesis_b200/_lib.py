@@ -193,7 +193,7 @@ class Context:
 
     def tune(self, **params: int) -> None:
         """Launch choices of this context's kernels (lgs_tune): hash_ctas, sumcheck_blocks,
-        hash_groups, witness_path, witness_ctas."""
+        hash_groups, witness_path, witness_ctas, upload_block_bytes, upload_tail_rows."""
         for name, value in params.items():
             check(self._lib.lgs_tune(self.handle, name.encode(), int(value)))
 

@@ -572,6 +572,9 @@ lgs_status lgs_tune(lgs_ctx* ctx, const char* name, uint64_t value) {
     } else if (n == "upload_block_bytes") {
       need(value <= ((uint64_t)1 << 40), "lgs_tune: upload_block_bytes above 2^40");
       ctx->upload_block = (size_t)value;
+    } else if (n == "upload_tail_rows") {
+      need(value <= 65536, "lgs_tune: upload_tail_rows above 65536");
+      ctx->upload_tail = (size_t)value;
     } else if (n == "witness_ctas") {
       need(value <= 65536, "lgs_tune: witness_ctas above 65536");
       ctx->witness_ctas = (unsigned)value;
@@ -600,6 +603,7 @@ lgs_status lgs_tune_get(lgs_ctx* ctx, const char* name, uint64_t* value) {
     else if (n == "witness_path") *value = ctx->witness_path;
     else if (n == "witness_ctas") *value = ctx->witness_ctas;
     else if (n == "upload_block_bytes") *value = ctx->upload_block;
+    else if (n == "upload_tail_rows") *value = ctx->upload_tail;
     else throw std::invalid_argument("lgs_tune_get: unknown parameter " + n);
   });
 }

@@ -366,7 +366,22 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
     const size_t min_block = c->upload_block ? c->upload_block : ((size_t)1 << 20);
     unsigned nb = (unsigned)std::min<size_t>(lgs_ctx::ROW_BLOCKS, m);
     while (nb > 1 && m * n * 8 / nb < min_block) nb >>= 1;
-    const size_t rows = m / nb;  // m and nb are powers of two
+    const size_t share = m / nb;  // m and nb are powers of two
+    // Row block b holds rows [brow[b], brow[b + 1]): equal blocks, or with upload_tail_rows
+    // below an equal share a last block of that many rows (even, at least 2) and the rest in
+    // even sizes.  The prove waits for the last block's RS encoding after its upload lands, but
+    // a short block does not shorten that wait in proportion (the encoding's grid is over rows),
+    // and on B200 at 2^7 x 2^17 a 4-row tail made the host-input step slower (3.58 vs 3.51 ms).
+    size_t brow[lgs_ctx::ROW_BLOCKS + 1];
+    brow[0] = 0;
+    if (nb > 1 && share >= 4 && c->upload_tail && c->upload_tail < share) {
+      const size_t tail = std::max<size_t>(2, c->upload_tail & ~(size_t)1);
+      const size_t pairs = (m - tail) / 2, each = pairs / (nb - 1), extra = pairs % (nb - 1);
+      for (unsigned b = 0; b + 1 < nb; ++b) brow[b + 1] = brow[b] + 2 * (each + (b < extra));
+    } else {
+      for (unsigned b = 0; b + 1 < nb; ++b) brow[b + 1] = (size_t)(b + 1) * share;
+    }
+    brow[nb] = m;
     const bool pinned = host_is_pinned(f);
     cudaStream_t cp = c->side[0];
     if (pinned) {
@@ -374,13 +389,18 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
       LGS_CUDA(cudaStreamWaitEvent(cp, c->ev_fork, 0));
     }
     // H is linear in the rows: with hash_groups = G > 1 the hash stream digests each group of
-    // nb / G row blocks as soon as their RS encoding is done (write, then add; the last group
-    // also hashes the leaves), so most of the hash runs under the rest of the upload.
+    // row blocks as soon as their RS encoding is done (write, then add; the last group also
+    // hashes the leaves), so most of the hash runs under the rest of the upload.  Group g ends
+    // with block (g + 1) nb / G - 1, which leaves no group empty for any G <= nb.
     unsigned groups = c->hash_groups ? std::min(c->hash_groups, nb) : 1;
-    if (rows * (nb / groups) % 2) groups = 1;  // a group must hold whole pairs of rows
-    const unsigned per = nb / groups;
+    for (unsigned g = 1; g < groups; ++g)  // a group must hold whole pairs of rows
+      if (brow[(size_t)g * nb / groups] % 2) {
+        groups = 1;
+        break;
+      }
+    unsigned g = 0;  // the next group to hash
     for (unsigned b = 0; b < nb; ++b) {
-      const size_t off = (size_t)b * rows * n;
+      const size_t rows = brow[b + 1] - brow[b], off = brow[b] * n;
       if (pinned) {
         h2d(cd->f.as<u64>() + off, f + off, rows * n * 8, cp);
         LGS_CUDA(cudaEventRecord(c->ev_rows[b], cp));
@@ -388,18 +408,19 @@ void commit_dev(lgs_ctx* c, const lgs_pk* pk, const u64* f, bool f_on_device,
       } else {
         h2d_staged(c, cd->f.as<u64>() + off, f + off, rows * n * 8, c->st);
       }
-      rs_dft_rows(cd->f.as<u64>() + off, n, n, cd->cw.as<u64>() + (size_t)b * rows * two_n,
-                  two_n, logN, rows, scr + (size_t)b * rows * two_n, c->rs_tw.as<u64>(), c->st);
-      if (groups > 1 && (b + 1) % per == 0) {
-        const unsigned g = b / per;
+      rs_dft_rows(cd->f.as<u64>() + off, n, n, cd->cw.as<u64>() + brow[b] * two_n, two_n, logN,
+                  (unsigned)rows, scr + brow[b] * two_n, c->rs_tw.as<u64>(), c->st);
+      if (groups > 1 && b + 1 == (size_t)(g + 1) * nb / groups) {
+        const size_t r0 = brow[(size_t)g * nb / groups];
         LGS_CUDA(cudaEventRecord(c->ev_rs[b], c->st));
         LGS_CUDA(cudaStreamWaitEvent(c->hs, c->ev_rs[b], 0));
         StageTimer th(c->prof, c->hs, "subset_sum_hash_rows");
         subset_sum_hash_tc(pk->tmap, cd->cw.as<u64>(), cd->H.as<u64>(), cd->nodes.as<u32>(),
                            (unsigned)m, two_n, c->err.as<int>(), c->hs, c->wait_cycles,
-                           c->hash_ctas, (unsigned)(g * per * rows), (unsigned)(per * rows),
+                           c->hash_ctas, (unsigned)r0, (unsigned)(brow[b + 1] - r0),
                            g == 0 ? 0 : (g + 1 == groups ? 3 : 1));
         hashed = true;
+        ++g;
       }
     }
   } else {

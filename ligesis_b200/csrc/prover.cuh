@@ -277,6 +277,7 @@ struct lgs_ctx {
   unsigned witness_path = 0;     // linear witness: 0 tensor cores when the operands fit, 1 CUDA cores
   unsigned witness_ctas = 0;     // linear witness: resident CTAs its work plan assumes (0: the GPU's)
   size_t upload_block = 0;       // host-rows commit: least bytes per row block (0: 1 MB)
+  size_t upload_tail = 0;        // host-rows commit: rows of the last row block (0: equal)
   // Pinned host memory: every transfer of a call is asynchronous, so the host enqueues a whole
   // commit or prove without waiting for the device and synchronises once at the end.
   lgs::PinnedBuf up;    // the parameter blob of one prove (one host-to-device copy)

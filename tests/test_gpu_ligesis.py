@@ -279,14 +279,21 @@ def test_lent_device_polynomial_gives_the_same_commitment(lgs, orc):
     assert np.array_equal(f_dev.cpu().numpy().view(np.uint64), f)  # only read
 
 
-@pytest.mark.parametrize("block", [1, 0, 1 << 30])
-def test_upload_row_blocks_give_the_same_root(lgs, orc, block):
+@pytest.mark.parametrize("block,tail,groups", [
+    (1, 0, 0), (0, 0, 0), (1 << 30, 0, 0),  # 8, 2 and 1 equal blocks
+    (1, 2, 0), (1, 1 << 16, 0),  # a 2-row last block; a tail above a share: equal blocks
+    (1, 3, 3), (1, 0, 8), (0, 6, 2), (1, 0, 3),  # hash groups at the block boundaries
+])
+def test_upload_row_blocks_give_the_same_root(lgs, orc, block, tail, groups):
     """A host polynomial is uploaded and encoded in row blocks of at least upload_block_bytes
-    (8, 2 and 1 blocks of a 2 MiB polynomial here); the commitment must not depend on it."""
+    (8, 2 and 1 blocks of a 2 MiB polynomial here), the last one upload_tail_rows long, and
+    hashed in hash_groups groups of whole blocks (3 groups over 8 blocks end with blocks 1, 4
+    and 7); the commitment must not depend on any of it."""
     log_m, log_n = 5, 13
     f, A, _, _, _ = ligesis_inputs(log_m, log_n, seed=71)
     ctx = L.Context(0)
-    ctx.tune(upload_block_bytes=block)
+    ctx.tune(upload_block_bytes=block, upload_tail_rows=tail, hash_groups=groups)
+    assert ctx.tuning("upload_tail_rows") == {"upload_tail_rows": tail}
     pk, _ = L.Ligesis.setup_with_hash(log_m, log_n, L.SubsetSumHash(64 << log_m, a=A), ctx)
     commit, _ = L.Ligesis.commit(pk, L.MlPoly(f))
     assert commit.root == orc.Commitment(orc.Key(log_m, log_n, A), f).root
