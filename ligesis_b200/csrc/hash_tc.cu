@@ -5,7 +5,9 @@
 // Exactness: A's canonical 64-bit entries are split into byte limbs, Alimb[8r + l][k] = byte l of
 // A[r][k], and B[64 i + b][j] = bit b of the RS codeword word F'[i][j].  S_l = Alimb_l * B is an
 // exact int32 sum (terms <= 255, at most 64 * 2^13 of them), and H[r][j] = sum_l 2^(8l) S_l mod p
-// is recombined exactly in 128-bit arithmetic.
+// is recombined exactly in 128-bit arithmetic.  K is stored permuted inside each aligned group of
+// 32 (the same permutation in A's limb columns and B's rows, so the products are unchanged): it
+// lets the producers spread a word's bits into bytes with a shift and a mask per 4 bytes.
 //
 // Persistent CTAs (one per SM) walk the 256-column tiles.  A tile is all 256 limb rows (two
 // M = 128 accumulators in TMEM, 2 x 256 columns = the SM's 512 TMEM columns) by 256 codeword
@@ -90,8 +92,13 @@ __device__ __forceinline__ bool epi_all(bool ok) {
       : "memory");
   return r != 0;
 }
-__device__ __forceinline__ uint32_t nib_expand(uint32_t nib) {
-  return (nib * 0x00204081u) & 0x01010101u;
+// 16 bytes of 0/1 from bits 0-3 and 8-11, 16-19, 24-27 of x: byte k of word p is bit 8k + p.
+// Applied to x and x >> 4, the 32 bits of a codeword word land in 32 K positions in the order
+// alimb_kernel stores A's limb columns, two instructions per word instead of a nibble multiply
+// per word.
+__device__ __forceinline__ uint4 bit_spread(uint32_t x) {
+  constexpr uint32_t M = 0x01010101u;
+  return make_uint4(x & M, (x >> 1) & M, (x >> 2) & M, (x >> 3) & M);
 }
 }  // namespace
 
@@ -242,16 +249,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const unsigned j = pt + h * NPROD;
-        const u64 a = w[2 * h], b = w[2 * h + 1];
+        const uint32_t x4[4] = {(uint32_t)w[2 * h], (uint32_t)(w[2 * h] >> 32),
+                                (uint32_t)w[2 * h + 1], (uint32_t)(w[2 * h + 1] >> 32)};
 #pragma unroll
-        for (int kc = 0; kc < 8; ++kc) {
-          const uint32_t b16 = (uint32_t)((kc < 4 ? (a >> (16 * kc)) : (b >> (16 * (kc - 4)))) & 0xFFFFu);
-          uint4 v;
-          v.x = nib_expand(b16 & 15u);
-          v.y = nib_expand((b16 >> 4) & 15u);
-          v.z = nib_expand((b16 >> 8) & 15u);
-          v.w = nib_expand((b16 >> 12) & 15u);
-          *(uint4*)(bt + j * TC_KB + ((kc ^ (j & 7)) << 4)) = v;
+        for (int q = 0; q < 4; ++q) {  // 32 bits -> chunks 2q, 2q + 1 (bit_spread's order)
+          const uint32_t x = x4[q];
+          const uint4 v0 = bit_spread(x), v1 = bit_spread(x >> 4);
+          *(uint4*)(bt + j * TC_KB + (((2 * q) ^ (j & 7)) << 4)) = v0;
+          *(uint4*)(bt + j * TC_KB + (((2 * q + 1) ^ (j & 7)) << 4)) = v1;
         }
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -427,14 +432,18 @@ double i8_tensor_peak_tops(unsigned iters, int* err, cudaStream_t st) {
   return best;
 }
 
-// Alimb[8r + l][k] = byte l of A[r][k] (the 256 x W limb matrix the TMA descriptor covers).
+// Alimb[8r + l][kperm(k)] = byte l of A[r][k] (the 256 x W limb matrix the TMA descriptor
+// covers), with the K order of the B tiles the hash's producers write: inside each aligned group
+// of 32 columns, bit t of a codeword word sits at position 16 ((t >> 2) & 1) + 4 (t & 3) + (t >> 3).
 __global__ void alimb_kernel(const u64* __restrict__ A, uint8_t* __restrict__ alimb, size_t W) {
   size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned r = blockIdx.y;
   if (k >= W) return;
   u64 v = A[(size_t)r * W + k];
+  const unsigned t = (unsigned)(k & 31);
+  const size_t kp = (k & ~(size_t)31) | (16 * ((t >> 2) & 1) + 4 * (t & 3) + (t >> 3));
 #pragma unroll
-  for (int l = 0; l < 8; ++l) alimb[(size_t)(r * 8 + l) * W + k] = (uint8_t)(v >> (8 * l));
+  for (int l = 0; l < 8; ++l) alimb[(size_t)(r * 8 + l) * W + kp] = (uint8_t)(v >> (8 * l));
 }
 
 void alimb_from_a(const u64* A, uint8_t* alimb, size_t W, cudaStream_t st) {
