@@ -231,7 +231,7 @@ class ClockSampler:
 # DRAM bytes (read + write) per launch of the two commit stages at mu = 24, from one ncu capture
 # each (`bench.py --mode commit --steps 3` under ncu --set full; profiles/rs_encode_mu24.md and
 # profiles/hash_tc_mu24.md): rs_encode = rs_pass_a + rs_pass_b.
-NCU_TRAFFIC_MU24 = {"rs_encode": 842.0e6, "subset_sum_hash": 326.6e6}
+NCU_TRAFFIC_MU24 = {"rs_encode": 842.0e6, "subset_sum_hash": 326.3e6}
 
 
 def ncu_traffic(stage: str) -> float:
