@@ -20,7 +20,8 @@ def _entries():
             yield gpu, key, entry
 
 
-@pytest.mark.parametrize("gpu,key,entry", list(_entries()), ids=lambda v: v if isinstance(v, str) else "")
+@pytest.mark.parametrize("gpu,key,entry", list(_entries()),
+                         ids=lambda v: v if isinstance(v, str) else "")
 def test_cached_settings_are_valid_and_timed(gpu, key, entry):
     if key.startswith("engine"):
         assert int(key[len("engine"):]) > 0
